@@ -1,0 +1,628 @@
+/*
+ * CPU oracle: plain-C restatement of the reference pressure-Poisson path.
+ * TEST INFRASTRUCTURE ONLY (the parity checker); see oracle.h.
+ *
+ * Every function states the reference file:line it follows. Operation
+ * order is kept where it decides the rounding (SpMV pair sums, residual
+ * accumulation, sequential dot products, coarse-operator sums).
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define IDX(i, j, k) (((size_t)(i) * ny + (size_t)(j)) * nz + (size_t)(k))
+
+/* ------------------------------------------------------------------ */
+/* Scalar operators                                                    */
+/* ------------------------------------------------------------------ */
+
+/* scalar_operators.cpp:49-72: four passes; each pair sum is formed first
+ * and then subtracted. Out-of-domain neighbours are the (zero) halo. */
+void orc_spmv(const orc_mat *A, const double *x, double *y) {
+  const int nx = A->nx, ny = A->ny, nz = A->nz;
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        size_t p = IDX(i, j, k);
+        double xw = i > 0 ? x[IDX(i - 1, j, k)] : 0.0, xe = i < nx - 1 ? x[IDX(i + 1, j, k)] : 0.0;
+        double xs = j > 0 ? x[IDX(i, j - 1, k)] : 0.0, xn = j < ny - 1 ? x[IDX(i, j + 1, k)] : 0.0;
+        double xb = k > 0 ? x[IDX(i, j, k - 1)] : 0.0, xt = k < nz - 1 ? x[IDX(i, j, k + 1)] : 0.0;
+        double v = A->c[p] * x[p];
+        v -= (A->w[p] * xw + A->e[p] * xe);
+        v -= (A->s[p] * xs + A->n[p] * xn);
+        v -= (A->b[p] * xb + A->t[p] * xt);
+        y[p] = v;
+      }
+}
+
+/* scalar_operators.cpp:22-46 */
+void orc_resid(const orc_mat *A, const double *x, const double *b, double *r) {
+  const int nx = A->nx, ny = A->ny, nz = A->nz;
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        size_t p = IDX(i, j, k);
+        double xw = i > 0 ? x[IDX(i - 1, j, k)] : 0.0, xe = i < nx - 1 ? x[IDX(i + 1, j, k)] : 0.0;
+        double xs = j > 0 ? x[IDX(i, j - 1, k)] : 0.0, xn = j < ny - 1 ? x[IDX(i, j + 1, k)] : 0.0;
+        double xb = k > 0 ? x[IDX(i, j, k - 1)] : 0.0, xt = k < nz - 1 ? x[IDX(i, j, k + 1)] : 0.0;
+        double v = b[p] - A->c[p] * x[p];
+        v += A->w[p] * xw + A->e[p] * xe;
+        v += A->s[p] * xs + A->n[p] * xn;
+        v += A->b[p] * xb + A->t[p] * xt;
+        r[p] = v;
+      }
+}
+
+/* scalar.h:296-298 */
+double orc_dot(size_t n, const double *x, const double *y) {
+  double d = 0.0;
+  for (size_t p = 0; p < n; ++p) d += x[p] * y[p];
+  return d;
+}
+
+/* scalar.h:317-326: d += x*y/dV/dV, then d/N/N */
+double orc_dot_voldiv_avg(size_t n, const double *x, const double *y, double dV) {
+  double d = 0.0;
+  for (size_t p = 0; p < n; ++p) d += x[p] * y[p] / dV / dV;
+  return d / (double)n / (double)n;
+}
+
+/* scalar_minmax.cpp:155-165 */
+double orc_max_abs_voldiv(size_t n, const double *x, double dV) {
+  double v = fabs(x[0] / dV);
+  for (size_t p = 0; p < n; ++p)
+    if (fabs(x[p] / dV) > v) v = fabs(x[p] / dV);
+  return v;
+}
+
+/* ------------------------------------------------------------------ */
+/* Krylov solvers                                                      */
+/* ------------------------------------------------------------------ */
+
+/* staleness window of cg.cpp:39-45,138-160 / bicgs.cpp:58-64,195-217 */
+typedef struct { double *v; int n; } stale_win;
+
+static void stale_init(stale_win *w, int n, double res0) {
+  w->n = n > 0 ? n : 0;
+  w->v = NULL;
+  if (w->n) {
+    w->v = (double *)malloc(sizeof(double) * w->n);
+    for (int q = 0; q < w->n; ++q) w->v[q] = 1.0e24; /* boil::unreal */
+    w->v[w->n - 1] = res0;
+  }
+}
+/* returns 1 when stale (breaks), else rotates the window */
+static int stale_step(stale_win *w, double res) {
+  if (!w->n) return 0;
+  int stale = 1;
+  for (int q = 0; q < w->n; ++q)
+    if (res < w->v[q]) { stale = 0; break; }
+  if (stale) return 1;
+  memmove(w->v, w->v + 1, sizeof(double) * (w->n - 1));
+  w->v[w->n - 1] = res;
+  return 0;
+}
+
+/* cg.cpp:10-182 with Diagonal (preconditioner_form.cpp:4-13,
+ * preconditioner_solve.cpp:4-11) */
+int orc_cg(const orc_mat *A, double *x, const double *b, int mini, int maxit,
+           double res_rat, double res_tol, double scale, int stalecount,
+           double dV, orc_stats *st, double *hist) {
+  const size_t N = (size_t)A->nx * A->ny * A->nz;
+  double *p = calloc(N, sizeof(double)), *q = calloc(N, sizeof(double));
+  double *r = calloc(N, sizeof(double)), *z = calloc(N, sizeof(double));
+  double *Mc = calloc(N, sizeof(double));
+  for (size_t c = 0; c < N; ++c) Mc[c] = 1.0 / A->c[c];
+  orc_resid(A, x, b, r);
+  double res = sqrt(orc_dot_voldiv_avg(N, r, r, dV)) / scale;
+  double res0 = res;
+  stale_win win;
+  stale_init(&win, stalecount, res);
+  orc_stats s = {0, 0, 0, res0, res, 0};
+  if (res < res_tol) {
+    s.converged = 1; s.status = 4;
+    free(p); free(q); free(r); free(z); free(Mc); free(win.v);
+    if (st) *st = s;
+    return 1;
+  }
+  double rho = 0, rho_old = 0, alfa, beta, pq;
+  int converged = 0, i, broke = 0;
+  s.status = 1;
+  for (i = 0; i < maxit; ++i) {
+    for (size_t c = 0; c < N; ++c) z[c] = r[c] * Mc[c];
+    rho = orc_dot(N, r, z);
+    if (i == 0) {
+      memcpy(p, z, N * sizeof(double));
+    } else {
+      beta = rho / rho_old;
+      for (size_t c = 0; c < N; ++c) p[c] = z[c] + beta * p[c];
+    }
+    orc_spmv(A, p, q);
+    pq = orc_dot(N, p, q);
+    alfa = rho / pq;
+    for (size_t c = 0; c < N; ++c) x[c] += alfa * p[c];
+    for (size_t c = 0; c < N; ++c) r[c] -= alfa * q[c];
+    res = sqrt(orc_dot_voldiv_avg(N, r, r, dV)) / scale;
+    if (hist) hist[i] = res;
+    if (res < res_tol && i >= mini - 1) { converged = 1; broke = 1; s.status = 0; break; }
+    if (res < res0 * res_rat && i >= mini - 1) { converged = 1; broke = 1; s.status = 0; break; }
+    if (stale_step(&win, res)) { broke = 1; s.status = 2; break; }
+    rho_old = rho;
+  }
+  s.converged = converged;
+  s.iterations = broke ? i + 1 : maxit;
+  s.printed = i + 1;
+  s.res = res;
+  if (st) *st = s;
+  free(p); free(q); free(r); free(z); free(Mc); free(win.v);
+  return converged;
+}
+
+/* bicgs.cpp:9-229 with Diagonal */
+int orc_bicgs(const orc_mat *A, double *x, const double *b, int mini, int maxit,
+              double res_rat, double res_tol, double scale, int stalecount,
+              double dV, orc_stats *st, double *hist) {
+  const size_t N = (size_t)A->nx * A->ny * A->nz;
+  double *p = calloc(N, sizeof(double)), *r = calloc(N, sizeof(double));
+  double *s = calloc(N, sizeof(double)), *t = calloc(N, sizeof(double));
+  double *v = calloc(N, sizeof(double)), *p_ = calloc(N, sizeof(double));
+  double *r_ = calloc(N, sizeof(double)), *s_ = calloc(N, sizeof(double));
+  double *Mc = calloc(N, sizeof(double));
+  for (size_t c = 0; c < N; ++c) Mc[c] = 1.0 / A->c[c];
+  orc_resid(A, x, b, r);
+  double res = sqrt(orc_dot_voldiv_avg(N, r, r, dV)) / scale;
+  double res0 = res;
+  stale_win win;
+  stale_init(&win, stalecount, res);
+  orc_stats so = {0, 0, 0, res0, res, 0};
+  int converged = 0, i, broke = 0;
+  if (res < res_tol) {
+    so.converged = 1; so.status = 4;
+    goto done_early;
+  }
+  memcpy(r_, r, N * sizeof(double));
+  double alfa = 0, beta, omega = 0, rho = 0, rho_old = 0, r_v, ss, ts, tt;
+  so.status = 1;
+  for (i = 0; i < maxit; ++i) {
+    rho = orc_dot(N, r_, r);
+    if (sqrt(fabs(rho)) < res_tol) { broke = 1; so.status = 3; break; }
+    if (i == 0) {
+      memcpy(p, r, N * sizeof(double));
+    } else {
+      beta = (rho / rho_old) * (alfa / omega);
+      for (size_t c = 0; c < N; ++c) p[c] = r[c] + beta * p[c];
+      double bo = beta * omega;
+      for (size_t c = 0; c < N; ++c) p[c] -= bo * v[c];
+    }
+    for (size_t c = 0; c < N; ++c) p_[c] = p[c] * Mc[c];
+    orc_spmv(A, p_, v);
+    r_v = orc_dot(N, r_, v);
+    alfa = rho / r_v;
+    for (size_t c = 0; c < N; ++c) s[c] = r[c] - alfa * v[c];
+    ss = orc_dot(N, s, s);
+    if (sqrt(ss) < res_tol) {
+      for (size_t c = 0; c < N; ++c) x[c] += alfa * p_[c];
+      broke = 1; so.status = 3;
+      break;
+    }
+    for (size_t c = 0; c < N; ++c) s_[c] = s[c] * Mc[c];
+    orc_spmv(A, s_, t);
+    ts = orc_dot(N, t, s);
+    tt = orc_dot(N, t, t);
+    omega = ts / tt;
+    for (size_t c = 0; c < N; ++c) x[c] += alfa * p_[c];
+    for (size_t c = 0; c < N; ++c) x[c] += omega * s_[c];
+    for (size_t c = 0; c < N; ++c) r[c] = s[c] - omega * t[c];
+    res = sqrt(orc_dot_voldiv_avg(N, r, r, dV)) / scale;
+    if (hist) hist[i] = res;
+    if (res < res_tol && i >= mini - 1) { converged = 1; broke = 1; so.status = 0; break; }
+    if (res < res0 * res_rat && i >= mini - 1) { converged = 1; broke = 1; so.status = 0; break; }
+    if (omega >= -res_tol && omega <= res_tol) { broke = 1; so.status = 3; break; }
+    if (stale_step(&win, res)) { broke = 1; so.status = 2; break; }
+    rho_old = rho;
+  }
+  so.converged = converged;
+  so.iterations = broke ? i + 1 : maxit;
+  so.printed = i + 1;
+  so.res = res;
+done_early:
+  if (st) *st = so;
+  free(p); free(r); free(s); free(t); free(v); free(p_); free(r_); free(s_); free(Mc);
+  free(win.v);
+  return converged || so.status == 4;
+}
+
+/* ------------------------------------------------------------------ */
+/* Additive-correction multigrid                                       */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+  int nx, ny, nz;     /* interior cells of this level                 */
+  int CI, CJ, CK;     /* ratio to the finer level (level 0: 1,1,1)    */
+  double dV;          /* cell volume (uniform)                        */
+  orc_mat A;
+  double *phi, *fnew; /* level unknown and rhs                        */
+  uint8_t *aflag;
+} orc_level;
+
+struct orc_ac {
+  int nlevels;
+  orc_level L[64];
+  double *fold;       /* last "good" fine solution                    */
+  double *res;        /* fine residual scratch                        */
+  /* cycle parameters (additive.cpp:11-19) */
+  double resrat_val, restol_val;
+};
+
+/* Domain::factor (domain_factor.cpp:4-21): first factor = smallest prime */
+static int first_factor(int n) {
+  int m = n - 1;
+  for (;;) {
+    if (m <= 0) return n;
+    if (n % m == 0) return n / m;
+    m--;
+    if (m == 0) return n;
+    if (m == 1) return n;
+  }
+}
+
+static void alloc_level(orc_level *lv) {
+  size_t N = (size_t)lv->nx * lv->ny * lv->nz;
+  double **arr[7] = {&lv->A.c, &lv->A.w, &lv->A.e, &lv->A.s, &lv->A.n, &lv->A.b, &lv->A.t};
+  for (int q = 0; q < 7; ++q) *arr[q] = calloc(N, sizeof(double));
+  lv->phi = calloc(N, sizeof(double));
+  lv->fnew = calloc(N, sizeof(double));
+  lv->aflag = calloc(N, 1);
+  lv->A.nx = lv->nx; lv->A.ny = lv->ny; lv->A.nz = lv->nz;
+}
+
+/* additive.cpp:8-48 + domain_coarsen.cpp:6-112 + additive_coarsen_flag.cpp */
+orc_ac *orc_ac_create(const orc_mat *A, const uint8_t *aflag, double h) {
+  orc_ac *ac = calloc(1, sizeof(orc_ac));
+  ac->resrat_val = 1.0e-18; /* boil::atto */
+  ac->restol_val = 1.0e-18;
+  orc_level *L0 = &ac->L[0];
+  L0->nx = A->nx; L0->ny = A->ny; L0->nz = A->nz;
+  L0->CI = L0->CJ = L0->CK = 1;
+  alloc_level(L0);
+  size_t N0 = (size_t)A->nx * A->ny * A->nz;
+  memcpy(L0->A.c, A->c, N0 * 8); memcpy(L0->A.w, A->w, N0 * 8);
+  memcpy(L0->A.e, A->e, N0 * 8); memcpy(L0->A.s, A->s, N0 * 8);
+  memcpy(L0->A.n, A->n, N0 * 8); memcpy(L0->A.b, A->b, N0 * 8);
+  memcpy(L0->A.t, A->t, N0 * 8);
+  memcpy(L0->aflag, aflag, N0);
+  const int dummy_z = (A->nz == 1);
+  double hx = h, hy = h, hz = h;
+  L0->dV = hx * hy * hz;
+  ac->fold = calloc(N0, sizeof(double));
+  ac->res = calloc(N0, sizeof(double));
+  int l = 1;
+  for (; l < 64; ++l) {
+    orc_level *f = &ac->L[l - 1];
+    int n[3] = {f->nx, f->ny, f->nz};
+    int fac[3] = {2, 2, 2}, ok[3];
+    for (int d = 0; d < 3; ++d) {
+      if (!(d == 2 && dummy_z)) fac[d] = first_factor(n[d]);
+      ok[d] = !((n[d] % fac[d]) != 0 || (n[d] + 6) <= 10 || n[d] == fac[d]);
+    }
+    if (!ok[0] && !ok[1] && !ok[2]) break;
+    orc_level *c = &ac->L[l];
+    c->CI = ok[0] ? fac[0] : 1; c->CJ = ok[1] ? fac[1] : 1; c->CK = ok[2] ? fac[2] : 1;
+    c->nx = n[0] / c->CI; c->ny = n[1] / c->CJ; c->nz = n[2] / c->CK;
+    hx *= c->CI; hy *= c->CJ; hz *= c->CK;
+    c->dV = hx * hy * hz;
+    alloc_level(c);
+    /* OR of the fine active flags (additive_coarsen_flag.cpp:20-38) */
+    const int nyf = f->ny, nzf = f->nz;
+    for (int I = 0; I < c->nx; ++I)
+      for (int J = 0; J < c->ny; ++J)
+        for (int K = 0; K < c->nz; ++K) {
+          uint8_t v = 0;
+          for (int i = 0; i < c->CI; ++i)
+            for (int j = 0; j < c->CJ; ++j)
+              for (int k = 0; k < c->CK; ++k)
+                v |= f->aflag[((size_t)(I * c->CI + i) * nyf + (J * c->CJ + j)) * nzf + (K * c->CK + k)];
+          c->aflag[((size_t)I * c->ny + J) * c->nz + K] = v;
+        }
+  }
+  ac->nlevels = l;
+  return ac;
+}
+
+void orc_ac_destroy(orc_ac *ac) {
+  if (!ac) return;
+  for (int l = 0; l < ac->nlevels; ++l) {
+    orc_level *lv = &ac->L[l];
+    free(lv->A.c); free(lv->A.w); free(lv->A.e); free(lv->A.s);
+    free(lv->A.n); free(lv->A.b); free(lv->A.t);
+    free(lv->phi); free(lv->fnew); free(lv->aflag);
+  }
+  free(ac->fold); free(ac->res);
+  free(ac);
+}
+
+int orc_ac_nlevels(const orc_ac *ac) { return ac->nlevels; }
+
+void orc_ac_level_dims(const orc_ac *ac, int l, int *dims) {
+  dims[0] = ac->L[l].nx; dims[1] = ac->L[l].ny; dims[2] = ac->L[l].nz;
+}
+
+void orc_ac_level_matrix(const orc_ac *ac, int l, double *out7) {
+  const orc_level *lv = &ac->L[l];
+  size_t N = (size_t)lv->nx * lv->ny * lv->nz;
+  const double *arr[7] = {lv->A.c, lv->A.w, lv->A.e, lv->A.s, lv->A.n, lv->A.b, lv->A.t};
+  for (int q = 0; q < 7; ++q) memcpy(out7 + q * N, arr[q], N * 8);
+}
+
+/* additive_coarsen_system.cpp:4-140 (h fine, H coarse) */
+static void coarsen_system(const orc_level *h, orc_level *H) {
+  const int CI = H->CI, CJ = H->CJ, CK = H->CK;
+  const int nyf = h->ny, nzf = h->nz;
+#define F(arr, i, j, k) h->A.arr[((size_t)(i) * nyf + (size_t)(j)) * nzf + (size_t)(k)]
+  for (int I = 0; I < H->nx; ++I)
+    for (int J = 0; J < H->ny; ++J)
+      for (int K = 0; K < H->nz; ++K) {
+        size_t P = ((size_t)I * H->ny + J) * H->nz + K;
+        int i0 = I * CI, j0 = J * CJ, k0 = K * CK;
+        double c = 0.0;
+        for (int i = 0; i < CI; ++i)
+          for (int j = 0; j < CJ; ++j)
+            for (int k = 0; k < CK; ++k) c += F(c, i0 + i, j0 + j, k0 + k);
+        for (int j = 0; j < CJ; ++j)
+          for (int k = 0; k < CK; ++k) {
+            for (int i = 0; i < CI - 1; ++i) c -= F(e, i0 + i, j0 + j, k0 + k);
+            for (int i = 1; i < CI; ++i) c -= F(w, i0 + i, j0 + j, k0 + k);
+          }
+        double e = 0.0, w = 0.0;
+        for (int j = 0; j < CJ; ++j)
+          for (int k = 0; k < CK; ++k) {
+            e += F(e, i0 + CI - 1, j0 + j, k0 + k);
+            w += F(w, i0, j0 + j, k0 + k);
+          }
+        for (int i = 0; i < CI; ++i)
+          for (int k = 0; k < CK; ++k) {
+            for (int j = 0; j < CJ - 1; ++j) c -= F(n, i0 + i, j0 + j, k0 + k);
+            for (int j = 1; j < CJ; ++j) c -= F(s, i0 + i, j0 + j, k0 + k);
+          }
+        double n = 0.0, s = 0.0;
+        for (int i = 0; i < CI; ++i)
+          for (int k = 0; k < CK; ++k) {
+            n += F(n, i0 + i, j0 + CJ - 1, k0 + k);
+            s += F(s, i0 + i, j0, k0 + k);
+          }
+        for (int i = 0; i < CI; ++i)
+          for (int j = 0; j < CJ; ++j) {
+            for (int k = 0; k < CK - 1; ++k) c -= F(t, i0 + i, j0 + j, k0 + k);
+            for (int k = 1; k < CK; ++k) c -= F(b, i0 + i, j0 + j, k0 + k);
+          }
+        double t = 0.0, b = 0.0;
+        for (int i = 0; i < CI; ++i)
+          for (int j = 0; j < CJ; ++j) {
+            t += F(t, i0 + i, j0 + j, k0 + CK - 1);
+            b += F(b, i0 + i, j0 + j, k0);
+          }
+        H->A.c[P] = c; H->A.e[P] = e; H->A.w[P] = w; H->A.n[P] = n;
+        H->A.s[P] = s; H->A.t[P] = t; H->A.b[P] = b;
+      }
+#undef F
+}
+
+void orc_ac_coarsen_all(orc_ac *ac) {
+  for (int l = 1; l < ac->nlevels; ++l) coarsen_system(&ac->L[l - 1], &ac->L[l]);
+}
+
+/* additive_restriction.cpp:12-177 */
+static void restriction(const orc_level *h, orc_level *H) {
+  const int CI = H->CI, CJ = H->CJ, CK = H->CK;
+  const int nxf = h->nx, nyf = h->ny, nzf = h->nz;
+  double *D = malloc(sizeof(double) * CI * CJ * CK);
+#define FI(i, j, k) (((size_t)(i) * nyf + (size_t)(j)) * nzf + (size_t)(k))
+#define PHI(i, j, k) (((i) < 0 || (i) >= nxf || (j) < 0 || (j) >= nyf || (k) < 0 || (k) >= nzf) ? 0.0 : h->phi[FI(i, j, k)])
+#define DD(i, j, k) D[((i) * CJ + (j)) * CK + (k)]
+  for (int I = 0; I < H->nx; ++I)
+    for (int J = 0; J < H->ny; ++J)
+      for (int K = 0; K < H->nz; ++K) {
+        size_t P = ((size_t)I * H->ny + J) * H->nz + K;
+        int i0 = I * CI, j0 = J * CJ, k0 = K * CK;
+        double f = 0.0;
+        for (int i = 0; i < CI; ++i)
+          for (int j = 0; j < CJ; ++j)
+            for (int k = 0; k < CK; ++k) {
+              DD(i, j, k) = h->A.c[FI(i0 + i, j0 + j, k0 + k)];
+              f += h->fnew[FI(i0 + i, j0 + j, k0 + k)];
+            }
+        for (int j = 0; j < CJ; ++j)
+          for (int k = 0; k < CK; ++k) {
+            f += h->A.e[FI(i0 + CI - 1, j0 + j, k0 + k)] * PHI(i0 + CI, j0 + j, k0 + k);
+            f += h->A.w[FI(i0, j0 + j, k0 + k)] * PHI(i0 - 1, j0 + j, k0 + k);
+            for (int i = 0; i < CI - 1; ++i) DD(i, j, k) -= h->A.e[FI(i0 + i, j0 + j, k0 + k)];
+            for (int i = CI - 1; i > 0; --i) DD(i, j, k) -= h->A.w[FI(i0 + i, j0 + j, k0 + k)];
+          }
+        for (int i = 0; i < CI; ++i)
+          for (int k = 0; k < CK; ++k) {
+            f += h->A.n[FI(i0 + i, j0 + CJ - 1, k0 + k)] * PHI(i0 + i, j0 + CJ, k0 + k);
+            f += h->A.s[FI(i0 + i, j0, k0 + k)] * PHI(i0 + i, j0 - 1, k0 + k);
+            for (int j = 0; j < CJ - 1; ++j) DD(i, j, k) -= h->A.n[FI(i0 + i, j0 + j, k0 + k)];
+            for (int j = CJ - 1; j > 0; --j) DD(i, j, k) -= h->A.s[FI(i0 + i, j0 + j, k0 + k)];
+          }
+        for (int i = 0; i < CI; ++i)
+          for (int j = 0; j < CJ; ++j) {
+            f += h->A.t[FI(i0 + i, j0 + j, k0 + CK - 1)] * PHI(i0 + i, j0 + j, k0 + CK);
+            f += h->A.b[FI(i0 + i, j0 + j, k0)] * PHI(i0 + i, j0 + j, k0 - 1);
+            for (int k = 0; k < CK - 1; ++k) DD(i, j, k) -= h->A.t[FI(i0 + i, j0 + j, k0 + k)];
+            for (int k = CK - 1; k > 0; --k) DD(i, j, k) -= h->A.b[FI(i0 + i, j0 + j, k0 + k)];
+          }
+        for (int i = 0; i < CI; ++i)
+          for (int j = 0; j < CJ; ++j)
+            for (int k = 0; k < CK; ++k) f -= DD(i, j, k) * h->phi[FI(i0 + i, j0 + j, k0 + k)];
+        H->fnew[P] = f;
+      }
+#undef FI
+#undef PHI
+#undef DD
+  free(D);
+  const size_t NH = (size_t)H->nx * H->ny * H->nz;
+  for (size_t P = 0; P < NH; ++P)
+    if (!H->aflag[P]) H->fnew[P] = 0.0;
+  /* zero-mean normalisation over active coarse cells (:151-174) */
+  double sum = 0.0;
+  int ncell = 0;
+  for (size_t P = 0; P < NH; ++P)
+    if (H->aflag[P]) { sum += H->fnew[P]; ncell++; }
+  sum /= (double)ncell;
+  for (size_t P = 0; P < NH; ++P)
+    if (H->aflag[P]) H->fnew[P] -= sum;
+}
+
+/* additive_interpolation.cpp:12-64 (H coarse -> h fine) */
+static void interpolation(const orc_level *H, orc_level *h) {
+  const int CI = H->CI, CJ = H->CJ, CK = H->CK;
+  const int nyf = h->ny, nzf = h->nz;
+  for (int I = 0; I < H->nx; ++I)
+    for (int J = 0; J < H->ny; ++J)
+      for (int K = 0; K < H->nz; ++K) {
+        double v = H->phi[((size_t)I * H->ny + J) * H->nz + K];
+        for (int i = 0; i < CI; ++i)
+          for (int j = 0; j < CJ; ++j)
+            for (int k = 0; k < CK; ++k)
+              h->phi[((size_t)(I * CI + i) * nyf + (J * CJ + j)) * nzf + (K * CK + k)] += v;
+      }
+}
+
+/* additive_residual.cpp:4-30 with dt = 1 */
+static double residual(orc_ac *ac, double *linf) {
+  orc_level *h = &ac->L[0];
+  size_t N = (size_t)h->nx * h->ny * h->nz;
+  orc_resid(&h->A, h->phi, h->fnew, ac->res);
+  double r2 = sqrt(orc_dot_voldiv_avg(N, ac->res, ac->res, h->dV)) * 1.0;
+  if (linf) *linf = orc_max_abs_voldiv(N, ac->res, h->dV) * 1.0;
+  return r2;
+}
+
+/* call_smoother / call_solver (additive_cycle_functions.cpp:90-107):
+ * CG on level l with scale dti*scale = 1 */
+static void smooth(orc_ac *ac, int l, int mi, double res_rat, double res_tol, int ms) {
+  orc_level *lv = &ac->L[l];
+  orc_cg(&lv->A, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, 1.0, ms, lv->dV, NULL, NULL);
+}
+
+static void v_cycle(orc_ac *ac, int l, const int mv[3], const int ms[3]);
+
+/* additive_recursive.cpp:4-34 */
+static void v_cycle(orc_ac *ac, int l, const int mv[3], const int ms[3]) {
+  if (l != ac->nlevels - 1) {
+    smooth(ac, l, mv[0], ac->resrat_val, ac->restol_val, ms[0]);
+    restriction(&ac->L[l], &ac->L[l + 1]);
+    v_cycle(ac, l + 1, mv, ms);
+    smooth(ac, l, mv[2], ac->resrat_val, ac->restol_val, ms[2]);
+    if (l > 0) interpolation(&ac->L[l], &ac->L[l - 1]);
+  } else {
+    smooth(ac, l, 100, -1.0, ac->restol_val, -1);
+    interpolation(&ac->L[l], &ac->L[l - 1]);
+  }
+}
+
+/* additive_recursive.cpp:37-76 (f) and 79-118 (w) */
+static void fw_cycle(orc_ac *ac, int l, const int mv[3], const int ms[3], int w) {
+  if (l != ac->nlevels - 1) {
+    smooth(ac, l, mv[0], ac->resrat_val, ac->restol_val, ms[0]);
+    restriction(&ac->L[l], &ac->L[l + 1]);
+    fw_cycle(ac, l + 1, mv, ms, w);
+    smooth(ac, l, mv[1], ac->resrat_val, ac->restol_val, ms[1]);
+    restriction(&ac->L[l], &ac->L[l + 1]);
+    if (w) fw_cycle(ac, l + 1, mv, ms, w);
+    else v_cycle(ac, l + 1, mv, ms);
+    smooth(ac, l, mv[2], ac->resrat_val, ac->restol_val, ms[2]);
+    if (l > 0) interpolation(&ac->L[l], &ac->L[l - 1]);
+  } else {
+    smooth(ac, l, 100, -1.0, ac->restol_val, -1);
+    interpolation(&ac->L[l], &ac->L[l - 1]);
+  }
+}
+
+static void run_cycle(orc_ac *ac, int kind, int l, const int mv[3], const int ms[3]) {
+  if (kind == 1) v_cycle(ac, l, mv, ms);
+  else if (kind == 2) fw_cycle(ac, l, mv, ms, 0);
+  else if (kind == 4) fw_cycle(ac, l, mv, ms, 1);
+}
+
+/* additive_recursive.cpp:121-158 */
+static void full_cycle(orc_ac *ac, int l, int kind, const int mv[3], const int ms[3]) {
+  if (l != ac->nlevels - 1) {
+    restriction(&ac->L[l], &ac->L[l + 1]);
+    full_cycle(ac, l + 1, kind, mv, ms);
+    run_cycle(ac, kind, l, mv, ms);
+  } else {
+    smooth(ac, l, 100, -1.0, ac->restol_val, -1);
+    interpolation(&ac->L[l], &ac->L[l - 1]);
+  }
+}
+
+/* AC::cycle (additive_cycle.cpp:4-99), init_cycles and converged
+ * (additive_cycle_functions.cpp:12-87) */
+int orc_ac_cycle(orc_ac *ac, double *x, const double *b, int init, int loop,
+                 double toler, double factor, const int mv[3], const int ms[3],
+                 int max_cyc, int min_cyc, int stop_if_div, int priority_min_cyc,
+                 int *ncyc, double *res_hist, int *nhist) {
+  orc_level *L0 = &ac->L[0];
+  const size_t N0 = (size_t)L0->nx * L0->ny * L0->nz;
+  int nh = 0;
+  memcpy(L0->phi, x, N0 * 8);
+  memcpy(L0->fnew, b, N0 * 8);
+  orc_ac_coarsen_all(ac);
+  double linf;
+  double res_0 = residual(ac, &linf);
+  if (res_hist) res_hist[nh] = res_0;
+  nh++;
+  memcpy(ac->fold, L0->phi, N0 * 8);
+  int ret = 0, nc = 0;
+  if ((res_0 < toler && min_cyc == 0) || res_0 == 0.0) {
+    ret = 1; nc = 0;
+    goto out;
+  }
+  for (int l = 1; l < ac->nlevels; ++l) {
+    size_t N = (size_t)ac->L[l].nx * ac->L[l].ny * ac->L[l].nz;
+    memset(ac->L[l].phi, 0, N * 8);
+    memset(ac->L[l].fnew, 0, N * 8);
+  }
+  double res_m1;
+  if (init != -1) {
+    full_cycle(ac, 0, init, mv, ms);
+    res_m1 = residual(ac, NULL);
+    /* converged(...) at cycle 0: its result is not used by the reference */
+  } else {
+    res_m1 = residual(ac, NULL);
+  }
+  nc = max_cyc;
+  for (int c = 1; c <= max_cyc; ++c) {
+    run_cycle(ac, loop, 0, mv, ms);
+    double res1 = residual(ac, NULL);
+    if (res_hist) res_hist[nh] = res1;
+    nh++;
+    int con;
+    if (c >= min_cyc && (res1 / res_0 < factor || res1 < toler)) {
+      con = 0;
+    } else {
+      int check = stop_if_div;
+      if (priority_min_cyc && c < min_cyc) check = 0;
+      if (check && res1 >= res_m1) {
+        memcpy(L0->phi, ac->fold, N0 * 8);
+        con = 1;
+      } else {
+        con = 2;
+      }
+    }
+    res_m1 = res1;
+    if (con == 0) { ret = 1; nc = c; goto out; }
+    if (con == 1) { ret = 0; nc = c; goto out; }
+    memcpy(ac->fold, L0->phi, N0 * 8);
+  }
+  ret = 0;
+out:
+  memcpy(x, L0->phi, N0 * 8);
+  if (ncyc) *ncyc = nc;
+  if (nhist) *nhist = nh;
+  return ret;
+}

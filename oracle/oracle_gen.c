@@ -1,0 +1,37 @@
+/*
+ * Oracle-side entry to the shared seeded workload generator
+ * (psiboil_b200/csrc/problem_gen.h). TEST INFRASTRUCTURE ONLY.
+ *
+ * kind 0: single bubble n^3; 1: bubbles + solid cylinder; 2: batch member.
+ * params: n, nb, rmin, rmax, rc, ratio, index, n2d, s2lo, s2hi, s3lo, s3hi,
+ *         rhs stream.
+ * With solid == NULL only dims and hb (h, density ratio) are written;
+ * otherwise out receives rho, rhs, c, w, e, s, n, b, t, ci (N each).
+ */
+#include <stdlib.h>
+#include "problem_gen.h"
+
+int orc_gen_problem(int kind, const double *params, uint64_t seed, int *dims,
+                    uint8_t *solid, double *hb, double *out) {
+  pbg_problem_desc d;
+  int n = (int)params[0];
+  if (kind == 0) pbg_desc_single_bubble(&d, n, seed);
+  else if (kind == 1)
+    pbg_desc_bubbles_cylinder(&d, n, (int)params[1], params[2], params[3], params[4],
+                              params[5], seed);
+  else
+    pbg_desc_batch_member(&d, seed, (int)params[6], (int)params[7], (int)params[8],
+                          (int)params[9], (int)params[10], (int)params[11]);
+  dims[0] = d.nx; dims[1] = d.ny; dims[2] = d.nz;
+  hb[0] = d.h;
+  hb[1] = d.rho_liquid / d.rho_vapour;
+  if (!solid) return 0;
+  size_t N = pbg_ncells(&d);
+  double *rho = out, *b = out + N;
+  pbg_gen_fields(&d, rho, solid);
+  pbg_gen_rhs(&d, (uint64_t)params[12], solid, b);
+  double *m = out + 2 * N;
+  pbg_gen_assemble(d.nx, d.ny, d.nz, d.h, d.bc, rho, solid, m, m + N, m + 2 * N, m + 3 * N,
+                   m + 4 * N, m + 5 * N, m + 6 * N, m + 7 * N);
+  return 0;
+}

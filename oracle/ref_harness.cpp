@@ -1,0 +1,296 @@
+/*
+ * Fixture harness around the UNMODIFIED PSI-BOIL reference library.
+ *
+ * Test infrastructure only: it is the parity checker and the timed CPU
+ * baseline, never part of the product. It is linked against the reference
+ * built from its own sources by oracle/build_ref.py.
+ *
+ * What it does, with reference code doing the solving:
+ *  - builds a uniform Domain and a Pressure equation exactly as the
+ *    reference's application mains do (Tests/Bubble3d/main-bubble-3d.cpp:
+ *    Grid1D/Domain/Times, `new CG(d, Prec::di())`, `Pressure pr(...)`,
+ *    `AC multigrid(&pr)`);
+ *  - the `Fixture` subclass overrides `Pressure::discretize` with the
+ *    workload's harmonic-density face coefficients and voxel solid mask
+ *    (the face stage of psiboil_b200/csrc/problem_gen.h), then calls the
+ *    reference's own `Centered::create_system_bnd()` for the boundary
+ *    correction, sets `ci = 1/c`, scales solid cells by pico
+ *    (pressure_discretize.cpp:125-148) and clears `aflag` on solid cells;
+ *  - overrides `update_rhs` to load the seeded right-hand side;
+ *  - runs one of:
+ *      cg     `Centered::solve` -> `CG::solve` (Src/Solver/Linear/Krylov/cg.cpp)
+ *      bicgs  `Centered::solve` -> `BiCGS::solve` (bicgs.cpp)
+ *      ac     `AC::vcycle(ResRat)` (Src/Solver/Additive/additive_cycle.cpp)
+ *    with x0 = 0 and dt = 1, and writes the matrix, rhs, solution and a
+ *    text summary (iterations, cycles, residual history parsed from the
+ *    reference's own log lines, wall time of the solve call alone).
+ *
+ * Usage:
+ *   ref_harness --kind single|cyl|batch --n N [--nb NB --rmin R --rmax R
+ *               --rc R --ratio Q] [--index I --n2d M --s2 LO HI --s3 LO HI]
+ *               --seed S --solver cg|bicgs|ac --resrat RR --maxit M
+ *               [--maxcyc C --guard 0|1 --cycle V|F|W] --out PREFIX
+ */
+#include "Include/psi-boil.h"
+#include "problem_gen.h"
+
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+namespace {
+
+struct Args {
+  std::string kind = "single", solver = "cg", out = "ref", cycle = "V";
+  int n = 16, nb = 0, index = 0, n2d = 0, s2lo = 64, s2hi = 512, s3lo = 32, s3hi = 96;
+  double rmin = 4, rmax = 16, rc = 0, ratio = 1000;
+  unsigned long long seed = 1;
+  double resrat = 1e-8;
+  int maxit = 20000, maxcyc = 20, guard = 1, dump = 1;
+};
+
+Args parse(int argc, char **argv) {
+  Args a;
+  for (int q = 1; q < argc; ++q) {
+    std::string k = argv[q];
+    auto nxt = [&]() -> const char * {
+      if (q + 1 >= argc) { std::fprintf(stderr, "missing value for %s\n", k.c_str()); std::exit(2); }
+      return argv[++q];
+    };
+    if (k == "--kind") a.kind = nxt();
+    else if (k == "--n") a.n = std::atoi(nxt());
+    else if (k == "--nb") a.nb = std::atoi(nxt());
+    else if (k == "--rmin") a.rmin = std::atof(nxt());
+    else if (k == "--rmax") a.rmax = std::atof(nxt());
+    else if (k == "--rc") a.rc = std::atof(nxt());
+    else if (k == "--ratio") a.ratio = std::atof(nxt());
+    else if (k == "--index") a.index = std::atoi(nxt());
+    else if (k == "--n2d") a.n2d = std::atoi(nxt());
+    else if (k == "--s2") { a.s2lo = std::atoi(nxt()); a.s2hi = std::atoi(nxt()); }
+    else if (k == "--s3") { a.s3lo = std::atoi(nxt()); a.s3hi = std::atoi(nxt()); }
+    else if (k == "--seed") a.seed = std::strtoull(nxt(), nullptr, 10);
+    else if (k == "--solver") a.solver = nxt();
+    else if (k == "--resrat") a.resrat = std::atof(nxt());
+    else if (k == "--maxit") a.maxit = std::atoi(nxt());
+    else if (k == "--maxcyc") a.maxcyc = std::atoi(nxt());
+    else if (k == "--guard") a.guard = std::atoi(nxt());
+    else if (k == "--cycle") a.cycle = nxt();
+    else if (k == "--dump") a.dump = std::atoi(nxt());
+    else if (k == "--out") a.out = nxt();
+    else { std::fprintf(stderr, "unknown argument %s\n", k.c_str()); std::exit(2); }
+  }
+  return a;
+}
+
+/* Pressure equation whose matrix and rhs come from the seeded fixture. */
+class Fixture : public Pressure {
+ public:
+  Fixture(const Scalar &p, const Scalar &f, const Vector &u, Times &t,
+          Linear *sm, Matter *m, const pbg_problem_desc &d,
+          const std::vector<double> &rho, const std::vector<uint8_t> &solid,
+          const std::vector<double> &rhs)
+      : Pressure(p, f, u, t, sm, m), D(d), RHO(rho), SOLID(solid), RHS(rhs) {
+    ready = true;
+    discretize();
+    for (int i = 0; i < D.nx; ++i)
+      for (int j = 0; j < D.ny; ++j)
+        for (int k = 0; k < D.nz; ++k)
+          aflag[i + boil::BW][j + boil::BW][k + boil::BW] = SOLID[at(i, j, k)] ? 0 : 1;
+  }
+
+  size_t at(int i, int j, int k) const { return ((size_t)i * D.ny + j) * D.nz + k; }
+
+  void discretize(const Scalar *diff_eddy = NULL) override {
+    if (!ready) { Pressure::discretize(diff_eddy); return; }
+    const size_t N = pbg_ncells(&D);
+    std::vector<double> c(N), w(N), e(N), s(N), n(N), b(N), t(N);
+    pbg_gen_faces(D.nx, D.ny, D.nz, D.h, RHO.data(), SOLID.data(),
+                  c.data(), w.data(), e.data(), s.data(), n.data(), b.data(), t.data());
+    const int B = boil::BW;
+    for (int i = 0; i < D.nx; ++i)
+      for (int j = 0; j < D.ny; ++j)
+        for (int k = 0; k < D.nz; ++k) {
+          size_t p = at(i, j, k);
+          A.c[i + B][j + B][k + B] = c[p];
+          A.w[i + B][j + B][k + B] = w[p]; A.e[i + B][j + B][k + B] = e[p];
+          A.s[i + B][j + B][k + B] = s[p]; A.n[i + B][j + B][k + B] = n[p];
+          A.b[i + B][j + B][k + B] = b[p]; A.t[i + B][j + B][k + B] = t[p];
+        }
+    /* the reference's own boundary correction */
+    Centered::create_system_bnd();
+    for (int i = 0; i < D.nx; ++i)
+      for (int j = 0; j < D.ny; ++j)
+        for (int k = 0; k < D.nz; ++k) {
+          A.ci[i + B][j + B][k + B] = 1.0 / A.c[i + B][j + B][k + B];
+          if (SOLID[at(i, j, k)]) {
+            A.c[i + B][j + B][k + B] *= boil::pico;
+            A.w[i + B][j + B][k + B] = 0.0; A.e[i + B][j + B][k + B] = 0.0;
+            A.s[i + B][j + B][k + B] = 0.0; A.n[i + B][j + B][k + B] = 0.0;
+            A.b[i + B][j + B][k + B] = 0.0; A.t[i + B][j + B][k + B] = 0.0;
+          }
+        }
+  }
+
+  real update_rhs() override {
+    const int B = boil::BW;
+    for (int i = 0; i < D.nx; ++i)
+      for (int j = 0; j < D.ny; ++j)
+        for (int k = 0; k < D.nz; ++k)
+          fnew[i + B][j + B][k + B] = RHS[at(i, j, k)];
+    return 0.0;
+  }
+
+  /* interior dump of one reference array into the engine's layout */
+  void dump(const Scalar &s, std::vector<double> &out) const {
+    const int B = boil::BW;
+    out.resize(pbg_ncells(&D));
+    for (int i = 0; i < D.nx; ++i)
+      for (int j = 0; j < D.ny; ++j)
+        for (int k = 0; k < D.nz; ++k)
+          out[at(i, j, k)] = s[i + B][j + B][k + B];
+  }
+  void dump_matrix(std::ofstream &f) const {
+    std::vector<double> v;
+    const Scalar *arr[8] = {&A.c, &A.w, &A.e, &A.s, &A.n, &A.b, &A.t, &A.ci};
+    for (auto *s : arr) { dump(*s, v); f.write((const char *)v.data(), v.size() * sizeof(double)); }
+  }
+  void dump_phi(std::vector<double> &v) const { dump(phi, v); }
+  void dump_fnew(std::vector<double> &v) const { dump(fnew, v); }
+
+ private:
+  pbg_problem_desc D;
+  std::vector<double> RHO;
+  std::vector<uint8_t> SOLID;
+  std::vector<double> RHS;
+  bool ready = false;
+};
+
+pbg_problem_desc make_desc(const Args &a) {
+  pbg_problem_desc d;
+  if (a.kind == "single") pbg_desc_single_bubble(&d, a.n, a.seed);
+  else if (a.kind == "cyl") pbg_desc_bubbles_cylinder(&d, a.n, a.nb, a.rmin, a.rmax, a.rc, a.ratio, a.seed);
+  else if (a.kind == "batch") pbg_desc_batch_member(&d, a.seed, a.index, a.n2d, a.s2lo, a.s2hi, a.s3lo, a.s3hi);
+  else { std::fprintf(stderr, "unknown kind\n"); std::exit(2); }
+  return d;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+  Args a = parse(argc, argv);
+  pbg_problem_desc D = make_desc(a);
+  const size_t N = pbg_ncells(&D);
+  std::vector<double> rho(N), rhs(N);
+  std::vector<uint8_t> solid(N);
+  pbg_gen_fields(&D, rho.data(), solid.data());
+  pbg_gen_rhs(&D, 0, solid.data(), rhs.data());
+
+  std::ostringstream log;
+  std::streambuf *saved = std::cout.rdbuf(log.rdbuf());
+  std::cout.precision(17);
+
+  const double h = D.h;
+  Grid1D gx(Range<real>(0.0, D.nx * h), Range<real>(h, h), D.nx, Periodic::no());
+  Grid1D gy(Range<real>(0.0, D.ny * h), Range<real>(h, h), D.ny, Periodic::no());
+  Grid1D *gz = (D.nz > 1) ? new Grid1D(Range<real>(0.0, D.nz * h), Range<real>(h, h), D.nz, Periodic::no())
+                          : new Grid1D(h);
+  Domain d(gx, gy, *gz);
+  Times time(1, 1.0);
+
+  Linear *solver = nullptr;
+  if (a.solver == "bicgs") solver = new BiCGS(d, Prec::di());
+  else solver = new CG(d, Prec::di());
+
+  Vector uvw(d);
+  Scalar p(d), f(d);
+  const Dir dirs[6] = {Dir::imin(), Dir::imax(), Dir::jmin(), Dir::jmax(), Dir::kmin(), Dir::kmax()};
+  for (int q = 0; q < 6; ++q) {
+    if (D.nz == 1 && q >= 4) p.bc().add(BndCnd(dirs[q], BndType::pseudo()));
+    else if (D.bc[q] == PBG_BC_DIRICHLET) p.bc().add(BndCnd(dirs[q], BndType::dirichlet(), 0.0));
+    else p.bc().add(BndCnd(dirs[q], BndType::neumann()));
+  }
+  const Comp comps[3] = {Comp::u(), Comp::v(), Comp::w()};
+  for (int m = 0; m < 3; ++m)
+    for (int q = 0; q < 6; ++q) {
+      if (D.nz == 1 && q >= 4) uvw.bc(comps[m]).add(BndCnd(dirs[q], BndType::pseudo()));
+      else uvw.bc(comps[m]).add(BndCnd(dirs[q], BndType::wall()));
+    }
+  Matter fluid(d);
+  fluid.rho(1.0);
+
+  Fixture pr(p, f, uvw, time, solver, &fluid, D, rho, solid, rhs);
+
+  p = 0.0;
+  bool conv = false;
+  int ncyc = -1;
+  double secs = 0.0;
+  if (a.solver == "ac") {
+    AC mg(&pr);
+    mg.max_cycles(a.maxcyc);
+    mg.stop_if_diverging(a.guard != 0);
+    p = 0.0;
+    auto t0 = std::chrono::steady_clock::now();
+    if (a.cycle == "F") conv = mg.fcycle(ResRat(a.resrat), &ncyc);
+    else if (a.cycle == "W") conv = mg.wcycle(ResRat(a.resrat), &ncyc);
+    else conv = mg.vcycle(ResRat(a.resrat), &ncyc);
+    secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  } else {
+    auto t0 = std::chrono::steady_clock::now();
+    pr.solve(ResTol(boil::atto), ResRat(a.resrat), "refsolve", a.maxit);
+    secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  std::cout.rdbuf(saved);
+
+  /* parse the reference's own log lines */
+  int iters = -1;
+  double res_final = -1, ratio_final = -1;
+  std::vector<double> cycle_res;
+  double res0_ac = -1;
+  std::istringstream in(log.str());
+  std::string line;
+  while (std::getline(in, line)) {
+    size_t q;
+    if ((q = line.find("refsolve, residual = ")) != std::string::npos) {
+      std::sscanf(line.c_str() + q, "refsolve, residual = %lf, ratio = %lf, iterations = %d",
+                  &res_final, &ratio_final, &iters);
+    } else if (line.rfind("Initial res = ", 0) == 0) {
+      std::sscanf(line.c_str(), "Initial res = %lf", &res0_ac);
+    } else if (line.rfind("Cycle ", 0) == 0) {
+      int c;
+      double r;
+      if (std::sscanf(line.c_str(), "Cycle %d; res = %lf", &c, &r) == 2) cycle_res.push_back(r);
+    }
+  }
+  if (a.solver != "ac") conv = (ratio_final >= 0 && ratio_final < a.resrat);
+
+  if (a.dump) {
+    std::ofstream fa(a.out + ".A", std::ios::binary);
+    pr.dump_matrix(fa);
+    std::vector<double> v;
+    pr.dump_fnew(v);
+    std::ofstream fb(a.out + ".b", std::ios::binary);
+    fb.write((const char *)v.data(), v.size() * sizeof(double));
+    pr.dump_phi(v);
+    std::ofstream fx(a.out + ".x", std::ios::binary);
+    fx.write((const char *)v.data(), v.size() * sizeof(double));
+  }
+  std::ofstream fm(a.out + ".txt");
+  fm.precision(17);
+  fm << "nx " << D.nx << "\nny " << D.ny << "\nnz " << D.nz << "\n";
+  fm << "solver " << a.solver << "\nconverged " << (conv ? 1 : 0) << "\n";
+  fm << "iterations " << iters << "\nresidual " << res_final << "\nratio " << ratio_final << "\n";
+  fm << "cycles " << ncyc << "\nres0 " << res0_ac << "\n";
+  fm << "cycle_res";
+  for (double r : cycle_res) fm << " " << r;
+  fm << "\nseconds " << secs << "\n";
+  fm.close();
+  std::printf("{\"solver\": \"%s\", \"converged\": %d, \"iterations\": %d, \"cycles\": %d, "
+              "\"ratio\": %.17g, \"seconds\": %.6f, \"cells\": %zu}\n",
+              a.solver.c_str(), conv ? 1 : 0, iters, ncyc, ratio_final, secs, N);
+  return 0;
+}
