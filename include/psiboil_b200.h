@@ -1,0 +1,211 @@
+/*
+ * psiboil_b200: B200-native pressure-Poisson engine — C ABI.
+ *
+ * Plain pointers and sizes only; every function returns an int status
+ * (PBG_OK or a negative PBG_ERR_*) and never aborts. pbg_last_error()
+ * returns the message of the calling thread's last failure.
+ *
+ * The reference (PSI-BOIL) has no C ABI or plugin interface; its swap
+ * points are C++ virtuals. Each entry point below names the reference
+ * interface it stands in for:
+ *   - Linear::solve / Krylov::solve        Src/Solver/Linear/linear.h:46-56,
+ *                                          Src/Solver/Linear/Krylov/krylov.h:20-30
+ *   - CG::solve, BiCGS::solve              Src/Solver/Linear/Krylov/cg.cpp:10-182,
+ *                                          bicgs.cpp:9-229
+ *   - AC::AC, AC::cycle and the vcycle/fcycle/wcycle/fullcycle overloads and
+ *     setters                             Src/Solver/Additive/additive.h:26-142
+ *   - Matrix (c, w, e, s, n, b, t, ci)     Src/Matrix/matrix.h:23-54
+ *   - Pressure::discretize                 Src/Equation/Centered/Pressure/pressure_discretize.cpp:11-151
+ *   - Scalar::operator=(A_x), (y_m_A_x)    Src/Field/Scalar/scalar_operators.cpp:22-72
+ *   - Scalar::dot, dot_voldiv_avg          Src/Field/Scalar/scalar.h:296-326
+ *
+ * Array layout. Compact arrays hold interior cells only, index
+ * (i*ny + j)*nz + k with k fastest. Strided entry points take the
+ * reference's contiguous val[0][0] block directly: element (i,j,k) of the
+ * interior lives at base[offset + i*si + j*sj + k*sk]; for a PSI-BOIL
+ * Scalar with BW = 3 that is si = (nj+6)*(nk+6), sj = nk+6, sk = 1,
+ * offset = 3*(si+sj+sk).
+ *
+ * `where` says whether caller pointers are host (PBG_HOST) or device
+ * (PBG_DEVICE, on the session's device) memory.
+ */
+#ifndef PSIBOIL_B200_H
+#define PSIBOIL_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PBG_API_VERSION 1
+
+typedef struct pbg_session pbg_session;
+
+/* call status */
+enum {
+  PBG_OK = 0,
+  PBG_ERR_ARG = -1,
+  PBG_ERR_CUDA = -2,
+  PBG_ERR_STATE = -3,
+  PBG_ERR_NOMEM = -4,
+  PBG_ERR_UNSUPPORTED = -5,
+  PBG_ERR_ADMISSION = -6
+};
+
+/* solve status (pbg_result.status) */
+enum {
+  PBG_CONVERGED = 0,
+  PBG_MAXITER = 1,
+  PBG_STALE = 2,
+  PBG_BREAKDOWN = 3,
+  PBG_INITIAL = 4,   /* converged before the first iteration */
+  PBG_NAN = 5,
+  PBG_DIVERGED = 6   /* AC divergence guard restored the last good iterate */
+};
+
+enum { PBG_HOST = 0, PBG_DEVICE = 1 };
+enum { PBG_BC_NEUMANN_ = 0, PBG_BC_DIRICHLET_ = 1 };
+
+/* solvers */
+enum {
+  PBG_SOLVER_CG = 0,      /* CG with diagonal preconditioner (reference parity)   */
+  PBG_SOLVER_BICGS = 1,   /* BiCGStab with diagonal preconditioner (parity)       */
+  PBG_SOLVER_AC = 2,      /* additive-correction multigrid, CG smoother (parity)  */
+  PBG_SOLVER_ENGINE = 3   /* flexible CG + AC K-cycle (the engine's fast solver)  */
+};
+enum { PBG_FP64 = 0, PBG_MIXED = 1 };
+enum { PBG_CYCLE_NONE = -1, PBG_CYCLE_V = 1, PBG_CYCLE_F = 2, PBG_CYCLE_W = 4 };
+
+typedef struct {
+  int solver;
+  int precision;          /* PBG_FP64 or PBG_MIXED (engine only)                */
+  /* Linear::solve(A, x, b, MinIter, MaxIter, name, ResRat, ResTol, scale,
+   * stalecount, precform) */
+  int min_iter;
+  int max_iter;
+  double res_rat;         /* ResRat (default 0.01); < 0 disables              */
+  double res_tol;         /* ResTol (default 1e-15)                            */
+  double scale;
+  int stalecount;         /* <= 0: off; at most 64                              */
+  /* AC::cycle(init, loop, ResTol, ResRat, mv, ms, &ncyc) and setters */
+  int init_cycle;         /* PBG_CYCLE_NONE | V | F | W                         */
+  int loop_cycle;         /* PBG_CYCLE_V | F | W                                */
+  double toler;           /* ResTol of the cycle loop (< 0 disables)            */
+  double factor;          /* ResRat of the cycle loop (< 0 disables)            */
+  int max_cycles, min_cycles, stop_if_div, priority_min_cyc;
+  int mv[3], ms[3];
+  /* engine */
+  double tol;             /* target |b - A x| / |b| (FP64 true residual)        */
+  double inner_tol;       /* mixed: FP32 inner solve reduction per sweep         */
+  int max_sweeps;         /* mixed: refinement sweeps at most                    */
+} pbg_params;
+
+typedef struct {
+  int status;             /* PBG_CONVERGED ...                                   */
+  int converged;          /* the reference's bool return value                    */
+  int iterations;         /* Krylov iterations performed (engine: all sweeps)    */
+  int cycles;             /* AC cycles (the reference's *ncyc)                    */
+  int sweeps;             /* refinement sweeps (engine)                           */
+  int levels;             /* multigrid levels                                     */
+  double res0, res;       /* reference residual measure at start / end            */
+  double relres;          /* engine: FP64 |b - A x| / |b| at return               */
+  double seconds;         /* wall time of the call                                */
+} pbg_result;
+
+const char *pbg_last_error(void);
+int pbg_version(void);
+int pbg_device_count(int *count);
+
+/* Defaults of the reference: MinIter(1), MaxIter(20), ResRat(0.01),
+ * ResTol(1e-15), scale 1, stalecount -1 (linear.h:46-56, resrat.h,
+ * restol.h, maxiter.h); AC defaults of additive.cpp:11-19 (max_cyc 20,
+ * min_cyc 0, stop_if_div true, priority_min_cyc true, mv {20,20,20},
+ * ms {-1,-1,-1}); engine tol 1e-8, inner_tol 1e-4, max_sweeps 8. */
+void pbg_params_default(pbg_params *p, int solver);
+
+/* A session owns one grid (nx, ny, nz interior cells, nz == 1 for 2-D, uniform
+ * spacing h), its matrix, the multigrid hierarchies and all scratch on one
+ * device. bc: imin, imax, jmin, jmax, kmin, kmax (PBG_BC_NEUMANN_ |
+ * PBG_BC_DIRICHLET_), used by pbg_assemble_pressure. Stands in for the
+ * Centered/Pressure object plus its Linear solver (centered.h:62-200). */
+int pbg_session_create(int nx, int ny, int nz, double h, const int bc[6], int device,
+                       pbg_session **out);
+int pbg_session_destroy(pbg_session *s);
+int pbg_session_info(const pbg_session *s, long long *ncell, int *symmetric,
+                     long long *device_bytes);
+
+/* Upload the seven coefficient arrays of the reference's Matrix
+ * (matrix.h:23-54; sign convention A x = c x_P - sum a_nb x_nb), strided
+ * as described above. A matrix whose e/n/t equal the next cell's w/s/b bit
+ * for bit is stored in the symmetric four-array form. */
+int pbg_matrix_upload(pbg_session *s, const double *c, const double *w, const double *e,
+                      const double *sv, const double *n, const double *b, const double *t,
+                      long long si, long long sj, long long sk, long long offset, int where);
+/* Download the matrix in compact layout (any pointer may be NULL). */
+int pbg_matrix_download(pbg_session *s, double *c, double *w, double *e, double *sv, double *n,
+                        double *b, double *t, int where);
+/* Active-cell flags (the reference's ScalarInt aflag, centered.h:196; 1 =
+ * active), strided like the matrix. Default: all active. */
+int pbg_active_upload(pbg_session *s, const int *aflag, long long si, long long sj, long long sk,
+                      long long offset, int where);
+
+/* On-device assembly of the pressure matrix from cell densities and a solid
+ * mask (1 = solid), Pressure::discretize with a harmonic face density:
+ * A.w = dS/dx/rho_face, c = sum, faces touching solid cells zeroed, boundary
+ * correction (Neumann c -= a_bnd; Dirichlet a_bnd = 0), solid cells c *= 1e-12
+ * (pressure_discretize.cpp:24-148, centered_system_bnd.cpp). Also sets the
+ * active flags to !solid. Compact arrays. */
+int pbg_assemble_pressure(pbg_session *s, const double *rho, const uint8_t *solid, int where);
+
+/* Solve A x = b with x as initial guess and result (x updated in place,
+ * b read only), compact layout. The reference-parity solvers follow
+ * Linear::solve / AC::cycle semantics (x0 as given, residual measure
+ * sqrt(dot_voldiv_avg(r))/scale, stopping tests, return value). */
+int pbg_solve(pbg_session *s, double *x, const double *b, int where, const pbg_params *p,
+              pbg_result *r);
+/* Same with strided x and b (the reference's Scalar blocks). */
+int pbg_solve_strided(pbg_session *s, double *x, const double *b, long long si, long long sj,
+                      long long sk, long long offset, int where, const pbg_params *p,
+                      pbg_result *r);
+/* Residual history of the last solve: per iteration (Krylov), per cycle
+ * including the initial residual (AC), or per FCG iteration (engine). */
+int pbg_history(const pbg_session *s, double *out, int cap, int *count);
+
+/* Operators, compact layout: y = A x (scalar_operators.cpp:49-72),
+ * r = b - A x (:22-46), dots (scalar.h:296-326): out[0] = x.y,
+ * out[1] = sum x*y/dV/dV / N / N. */
+int pbg_spmv(pbg_session *s, const double *x, double *y, int where);
+int pbg_residual(pbg_session *s, const double *x, const double *b, double *r, int where);
+int pbg_dot(pbg_session *s, const double *x, const double *y, int where, double out[2]);
+
+/* Multigrid hierarchy sizes: count and per-level dims (3 ints per level).
+ * kind 0: the reference AC hierarchy (Domain::coarsen rule), kind 1: the
+ * engine's aggregation hierarchy. */
+int pbg_levels(pbg_session *s, int kind, int *count, int *dims, int cap);
+/* Coarse matrix of the reference AC hierarchy, level l (7 compact arrays
+ * c,w,e,s,n,b,t concatenated, AC::coarsen_system). */
+int pbg_ac_level_matrix(pbg_session *s, int level, double *out7, int where);
+
+/* Seeded workload generator (the same code the oracle uses): kind 0 single
+ * bubble n^3, 1 bubbles + solid cylinder, 2 member of the uneven batch.
+ * params: n, nb, rmin, rmax, rc, ratio, index, n2d, s2lo, s2hi, s3lo, s3hi,
+ * stream. With rho == NULL only dims/h are returned. */
+int pbg_generate(int kind, const double *params, uint64_t seed, int dims[3], double *h,
+                 double *rho, uint8_t *solid, double *b);
+
+/* Instrumentation (no reference counterpart): kernels launched by this
+ * library so far in the process; the session's CUDA stream (for events);
+ * the average device time of one launch of a hot kernel timed alone with
+ * CUDA events (which 0: the engine's fine-level smoothing sweep, precision
+ * PBG_FP64 | PBG_MIXED for FP32; which 1: the reference-order FP64 SpMV)
+ * and its algorithmic bytes per launch. */
+unsigned long long pbg_launch_count(void);
+int pbg_session_stream(pbg_session *s, void **stream);
+int pbg_bench_kernel(pbg_session *s, int which, int precision, int reps, double *ms,
+                     double *bytes_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

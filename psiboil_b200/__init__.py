@@ -1,0 +1,433 @@
+"""psiboil_b200 — B200-native pressure-Poisson engine for PSI-BOIL.
+
+Host-side mirror of the reference's solver interface over the engine's C ABI
+(include/psiboil_b200.h). The reference's swap points are C++ virtuals; this
+module keeps their names, argument meaning and return values:
+
+  CG(sess).solve(A, x, b, MinIter, MaxIter, name, ResRat, ResTol, scale,
+                 stalecount) -> bool     Linear::solve, Src/Solver/Linear/linear.h:46-56
+  BiCGS(sess).solve(...)                 BiCGS::solve,  Krylov/bicgs.cpp:9-229
+  AC(sess).vcycle(ResRat, ...) -> bool   AC::vcycle,    Src/Solver/Additive/additive.h:54-95
+  Engine(sess).solve(x, b, tol, precision)   the engine's flexible-CG + AC K-cycle
+
+Arrays are numpy arrays (host) or CUDA tensors (device, e.g. torch) in the
+compact layout index (i*ny + j)*nz + k; the strided entry points accept the
+reference's BW=3 Scalar blocks. Every compute call runs the CUDA library; if
+it cannot be loaded, importing a solver raises — there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpsiboil_b200.so")
+
+PBG_OK = 0
+HOST, DEVICE = 0, 1
+NEUMANN, DIRICHLET = 0, 1
+SOLVER_CG, SOLVER_BICGS, SOLVER_AC, SOLVER_ENGINE = 0, 1, 2, 3
+FP64, MIXED = 0, 1
+CYCLE_NONE, CYCLE_V, CYCLE_F, CYCLE_W = -1, 1, 2, 4
+STATUS = {0: "converged", 1: "maxiter", 2: "stale", 3: "breakdown", 4: "initial", 5: "nan",
+          6: "diverged"}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+_ll = ctypes.c_longlong
+
+
+class PbgError(RuntimeError):
+    """A C-ABI call returned an error status."""
+
+    def __init__(self, code, msg):
+        super().__init__("pbg error %d: %s" % (code, msg))
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("solver", ctypes.c_int), ("precision", ctypes.c_int),
+                ("min_iter", ctypes.c_int), ("max_iter", ctypes.c_int),
+                ("res_rat", ctypes.c_double), ("res_tol", ctypes.c_double),
+                ("scale", ctypes.c_double), ("stalecount", ctypes.c_int),
+                ("init_cycle", ctypes.c_int), ("loop_cycle", ctypes.c_int),
+                ("toler", ctypes.c_double), ("factor", ctypes.c_double),
+                ("max_cycles", ctypes.c_int), ("min_cycles", ctypes.c_int),
+                ("stop_if_div", ctypes.c_int), ("priority_min_cyc", ctypes.c_int),
+                ("mv", ctypes.c_int * 3), ("ms", ctypes.c_int * 3),
+                ("tol", ctypes.c_double), ("inner_tol", ctypes.c_double),
+                ("max_sweeps", ctypes.c_int)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("converged", ctypes.c_int),
+                ("iterations", ctypes.c_int), ("cycles", ctypes.c_int),
+                ("sweeps", ctypes.c_int), ("levels", ctypes.c_int),
+                ("res0", ctypes.c_double), ("res", ctypes.c_double),
+                ("relres", ctypes.c_double), ("seconds", ctypes.c_double)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["status_name"] = STATUS.get(self.status, str(self.status))
+        return d
+
+
+# exported symbols and their argument types
+_SIGS = {
+    "pbg_last_error": (ctypes.c_char_p, []),
+    "pbg_version": (ctypes.c_int, []),
+    "pbg_device_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
+    "pbg_params_default": (None, [ctypes.POINTER(Params), ctypes.c_int]),
+    "pbg_session_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                          ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                          ctypes.POINTER(_vp)]),
+    "pbg_session_destroy": (ctypes.c_int, [_vp]),
+    "pbg_session_info": (ctypes.c_int, [_vp, ctypes.POINTER(_ll), ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(_ll)]),
+    "pbg_matrix_upload": (ctypes.c_int, [_vp] + [_vp] * 7 + [_ll, _ll, _ll, _ll, ctypes.c_int]),
+    "pbg_matrix_download": (ctypes.c_int, [_vp] + [_vp] * 7 + [ctypes.c_int]),
+    "pbg_active_upload": (ctypes.c_int, [_vp, _vp, _ll, _ll, _ll, _ll, ctypes.c_int]),
+    "pbg_assemble_pressure": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
+    "pbg_solve": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.POINTER(Params),
+                                 ctypes.POINTER(Result)]),
+    "pbg_solve_strided": (ctypes.c_int, [_vp, _vp, _vp, _ll, _ll, _ll, _ll, ctypes.c_int,
+                                         ctypes.POINTER(Params), ctypes.POINTER(Result)]),
+    "pbg_history": (ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    "pbg_spmv": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
+    "pbg_residual": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int]),
+    "pbg_dot": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _dp]),
+    "pbg_levels": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
+    "pbg_ac_level_matrix": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
+    "pbg_launch_count": (ctypes.c_ulonglong, []),
+    "pbg_session_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "pbg_bench_kernel": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]),
+    "pbg_generate": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int),
+                                    _dp, _vp, _vp, _vp]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library (raises if it is missing: no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("psiboil_b200: %s not built (run __graft_entry__.build())" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(code):
+    if code != PBG_OK:
+        raise PbgError(code, lib().pbg_last_error().decode())
+
+
+def _ptr(a):
+    """(pointer, where) of a numpy array or a CUDA tensor."""
+    if a is None:
+        return None, HOST
+    if hasattr(a, "data_ptr") and getattr(a, "is_cuda", False):
+        return a.data_ptr(), DEVICE
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("arrays must be C-contiguous")
+        return a.ctypes.data, HOST
+    raise TypeError("expected a numpy array or a CUDA tensor, got %r" % type(a))
+
+
+def default_params(solver):
+    p = Params()
+    lib().pbg_params_default(ctypes.byref(p), solver)
+    return p
+
+
+def launch_count():
+    return int(lib().pbg_launch_count())
+
+
+def device_count():
+    n = ctypes.c_int(0)
+    rc = lib().pbg_device_count(ctypes.byref(n))
+    return n.value if rc == PBG_OK else 0
+
+
+class Session:
+    """One grid, its matrix, hierarchies and scratch on one GPU.
+
+    Stands in for the reference's Centered/Pressure equation object that owns
+    A, phi, fnew and aflag (Src/Equation/Centered/centered.h:62-200).
+    """
+
+    def __init__(self, nx, ny, nz, h, bc=None, device=0):
+        if bc is None:
+            bc = [NEUMANN] * 6
+            bc[5 if nz > 1 else 3] = DIRICHLET
+        self.dims = (int(nx), int(ny), int(nz))
+        self.h = float(h)
+        self.bc = list(bc)
+        self.device = device
+        arr = (ctypes.c_int * 6)(*bc)
+        hnd = _vp()
+        _check(lib().pbg_session_create(nx, ny, nz, h, arr, device, ctypes.byref(hnd)))
+        self._h = hnd
+
+    @property
+    def ncell(self):
+        return self.dims[0] * self.dims[1] * self.dims[2]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pbg_session_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- matrix -----------------------------------------------------------
+    def upload_matrix(self, A, strides=None, offset=0):
+        """A: mapping with c, w, e, s, n, b, t (the reference's Matrix)."""
+        ptrs = [_ptr(A[k]) for k in "cwesnbt"]
+        where = ptrs[0][1]
+        nx, ny, nz = self.dims
+        si, sj, sk = strides if strides else (ny * nz, nz, 1)
+        _check(lib().pbg_matrix_upload(self._h, *[p for p, _ in ptrs], si, sj, sk, offset, where))
+
+    def download_matrix(self):
+        out = {k: np.zeros(self.ncell) for k in "cwesnbt"}
+        _check(lib().pbg_matrix_download(self._h, *[out[k].ctypes.data for k in "cwesnbt"], HOST))
+        return out
+
+    def upload_active(self, aflag, strides=None, offset=0):
+        a = np.ascontiguousarray(aflag, dtype=np.int32)
+        nx, ny, nz = self.dims
+        si, sj, sk = strides if strides else (ny * nz, nz, 1)
+        _check(lib().pbg_active_upload(self._h, a.ctypes.data, si, sj, sk, offset, HOST))
+
+    def assemble_pressure(self, rho, solid):
+        """Pressure::discretize on the device (harmonic face density)."""
+        pr, where = _ptr(rho)
+        ps, where2 = _ptr(solid)
+        if where != where2:
+            raise ValueError("rho and solid must live in the same memory")
+        _check(lib().pbg_assemble_pressure(self._h, pr, ps, where))
+
+    def symmetric(self):
+        sym = ctypes.c_int(0)
+        _check(lib().pbg_session_info(self._h, None, ctypes.byref(sym), None))
+        return bool(sym.value)
+
+    # -- operators ---------------------------------------------------------
+    def spmv(self, x, y):
+        px, w = _ptr(x)
+        py, _ = _ptr(y)
+        _check(lib().pbg_spmv(self._h, px, py, w))
+        return y
+
+    def residual(self, x, b, r):
+        px, w = _ptr(x)
+        _check(lib().pbg_residual(self._h, px, _ptr(b)[0], _ptr(r)[0], w))
+        return r
+
+    def dot(self, x, y):
+        out = (ctypes.c_double * 2)()
+        px, w = _ptr(x)
+        _check(lib().pbg_dot(self._h, px, _ptr(y)[0], w, out))
+        return out[0], out[1]
+
+    def levels(self, kind=0):
+        cnt = ctypes.c_int(0)
+        dims = (ctypes.c_int * (3 * 64))()
+        _check(lib().pbg_levels(self._h, kind, ctypes.byref(cnt), dims, 64))
+        return [tuple(dims[3 * q:3 * q + 3]) for q in range(cnt.value)]
+
+    def ac_level_matrix(self, level):
+        nx, ny, nz = self.levels(0)[level]
+        n = nx * ny * nz
+        out = np.zeros(7 * n)
+        _check(lib().pbg_ac_level_matrix(self._h, level, out.ctypes.data, HOST))
+        return {k: out[q * n:(q + 1) * n] for q, k in enumerate("cwesnbt")}
+
+    # -- solve -------------------------------------------------------------
+    def solve(self, x, b, params, strides=None, offset=0):
+        px, where = _ptr(x)
+        pb, where2 = _ptr(b)
+        if where != where2:
+            raise ValueError("x and b must live in the same memory")
+        res = Result()
+        if strides is None:
+            _check(lib().pbg_solve(self._h, px, pb, where, ctypes.byref(params), ctypes.byref(res)))
+        else:
+            si, sj, sk = strides
+            _check(lib().pbg_solve_strided(self._h, px, pb, si, sj, sk, offset, where,
+                                           ctypes.byref(params), ctypes.byref(res)))
+        return res
+
+    def stream_handle(self):
+        h = _vp()
+        _check(lib().pbg_session_stream(self._h, ctypes.byref(h)))
+        return h.value or 0
+
+    def bench_kernel(self, which, precision=FP64, reps=20):
+        """(ms per launch, algorithmic bytes per launch) of a hot kernel timed alone."""
+        ms, by = ctypes.c_double(0), ctypes.c_double(0)
+        _check(lib().pbg_bench_kernel(self._h, which, precision, reps, ctypes.byref(ms), ctypes.byref(by)))
+        return ms.value, by.value
+
+    def history(self):
+        n = ctypes.c_int(0)
+        _check(lib().pbg_history(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(max(n.value, 1))
+        _check(lib().pbg_history(self._h, out.ctypes.data_as(_dp), n.value, ctypes.byref(n)))
+        return out[:n.value]
+
+
+# ---------------------------------------------------------------- solvers
+class _Krylov:
+    solver = SOLVER_CG
+
+    def __init__(self, session, prec="di"):
+        if prec not in ("di", "diagonal"):
+            raise NotImplementedError("only the diagonal preconditioner (Prec::di) is provided")
+        self.session = session
+        self.last = None
+
+    def solve(self, x, b, min_iter=1, max_iter=20, name=None, res_rat=0.01, res_tol=1.0e-15,
+              scale=1.0, stalecount=-1):
+        """Linear::solve(A, x, b, MinIter, MaxIter, name, ResRat, ResTol, scale,
+        stalecount): updates x in place, returns the converged flag."""
+        p = default_params(self.solver)
+        p.min_iter, p.max_iter = int(min_iter), int(max_iter)
+        p.res_rat, p.res_tol, p.scale, p.stalecount = res_rat, res_tol, scale, int(stalecount)
+        self.last = self.session.solve(x, b, p)
+        if name is not None:
+            r = self.last
+            print("%s, residual = %.17g, ratio = %.17g, iterations = %d" %
+                  (name, r.res, r.res / r.res0 if r.res0 else 0.0, r.iterations))
+        return bool(self.last.converged)
+
+
+class CG(_Krylov):
+    """CG with the diagonal preconditioner (Src/Solver/Linear/Krylov/cg.cpp)."""
+    solver = SOLVER_CG
+
+
+class BiCGS(_Krylov):
+    """BiCGStab with the diagonal preconditioner (Krylov/bicgs.cpp)."""
+    solver = SOLVER_BICGS
+
+
+class AC:
+    """Additive-correction multigrid with CG smoothers (Src/Solver/Additive)."""
+
+    def __init__(self, session):
+        self.session = session
+        self._max_cyc, self._min_cyc = 20, 0
+        self._stop_if_div, self._prio = True, True
+        self.mv = [20, 20, 20]
+        self.ms = [-1, -1, -1]
+        self.last = None
+
+    # setters of additive.h:97-142
+    def max_cycles(self, mc=None):
+        if mc is None:
+            return self._max_cyc
+        self._max_cyc = int(mc)
+
+    def min_cycles(self, mc=None):
+        if mc is None:
+            return self._min_cyc
+        self._min_cyc = int(mc)
+
+    def stop_if_diverging(self, s=None):
+        if s is None:
+            return self._stop_if_div
+        self._stop_if_div = bool(s)
+
+    def priority_min_cycle(self, s=None):
+        if s is None:
+            return self._prio
+        self._prio = bool(s)
+
+    def max_iter_array(self, mv):
+        self.mv = list(mv)
+
+    def stale_iter_array(self, ms):
+        self.ms = list(ms)
+
+    def cycle(self, x, b, init=CYCLE_NONE, loop=CYCLE_V, toler=-1.0, factor=-1.0, mv=None, ms=None):
+        """AC::cycle(init, loop, ResTol, ResRat, mv, ms, &ncyc) -> (bool, ncyc)."""
+        p = default_params(SOLVER_AC)
+        p.init_cycle, p.loop_cycle = init, loop
+        p.toler, p.factor = toler, factor
+        p.max_cycles, p.min_cycles = self._max_cyc, self._min_cyc
+        p.stop_if_div, p.priority_min_cyc = int(self._stop_if_div), int(self._prio)
+        for q in range(3):
+            p.mv[q] = (mv or self.mv)[q]
+            p.ms[q] = (ms or self.ms)[q]
+        self.last = self.session.solve(x, b, p)
+        return bool(self.last.converged), self.last.cycles
+
+    def vcycle(self, x, b, factor=-1.0, toler=-1.0):
+        return self.cycle(x, b, CYCLE_NONE, CYCLE_V, toler, factor)
+
+    def fcycle(self, x, b, factor=-1.0, toler=-1.0):
+        return self.cycle(x, b, CYCLE_NONE, CYCLE_F, toler, factor)
+
+    def wcycle(self, x, b, factor=-1.0, toler=-1.0):
+        return self.cycle(x, b, CYCLE_NONE, CYCLE_W, toler, factor)
+
+    def fullcycle(self, x, b, loop=CYCLE_V, factor=-1.0, toler=-1.0):
+        return self.cycle(x, b, CYCLE_V, loop, toler, factor)
+
+
+class Engine:
+    """Flexible CG + AC K-cycle; FP64 or mixed (FP32 inner, FP64 refinement)."""
+
+    def __init__(self, session):
+        self.session = session
+        self.last = None
+
+    def solve(self, x, b, tol=1.0e-8, precision=FP64, inner_tol=1.0e-4, max_iter=500,
+              max_sweeps=8):
+        p = default_params(SOLVER_ENGINE)
+        p.precision, p.tol, p.inner_tol = precision, tol, inner_tol
+        p.max_iter, p.max_sweeps = max_iter, max_sweeps
+        self.last = self.session.solve(x, b, p)
+        return bool(self.last.converged)
+
+
+def generate(kind, seed, n=16, nb=0, rmin=4.0, rmax=16.0, rc=0.0, ratio=1000.0, index=0, n2d=0,
+             s2=(64, 512), s3=(32, 96), stream=0):
+    """Seeded workload (psiboil_b200/csrc/problem_gen.h): returns
+    (dims, h, rho, solid, b)."""
+    params = (ctypes.c_double * 13)(n, nb, rmin, rmax, rc, ratio, index, n2d, s2[0], s2[1],
+                                    s3[0], s3[1], stream)
+    dims = (ctypes.c_int * 3)()
+    h = ctypes.c_double(0.0)
+    _check(lib().pbg_generate(kind, params, seed, dims, ctypes.byref(h), None, None, None))
+    N = dims[0] * dims[1] * dims[2]
+    rho = np.zeros(N)
+    solid = np.zeros(N, dtype=np.uint8)
+    b = np.zeros(N)
+    _check(lib().pbg_generate(kind, params, seed, dims, ctypes.byref(h), rho.ctypes.data_as(_dp),
+                              solid.ctypes.data, b.ctypes.data))
+    return tuple(dims), h.value, rho, solid, b
+
+
+KIND_SINGLE, KIND_CYL, KIND_BATCH = 0, 1, 2

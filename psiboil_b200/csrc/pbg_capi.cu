@@ -1,0 +1,733 @@
+// C ABI of the engine: sessions, uploads, on-device pressure assembly and
+// the solver entry points. No torch types; plain pointers and sizes.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/psiboil_b200.h"
+#include "pbg_engine.cuh"
+#include "pbg_ref_kernels.cuh"
+#include "problem_gen.h"
+
+using namespace pbg;
+
+static thread_local std::string g_err;
+namespace pbg {
+unsigned long long g_launch_count = 0;
+}
+
+struct pbg_session {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int nx = 0, ny = 0, nz = 0;
+  double h = 0.0;
+  int bc[6] = {0, 0, 0, 0, 0, 0};
+  Mat64 A;
+  bool have_matrix = false;
+  DBuf<uint8_t> aflag;
+  RedPool red;
+  DBuf<KrylovState> kst;
+  KrylovState *hkst = nullptr;
+  RefKrylovWork rkw;
+  std::unique_ptr<RefAC> refac;
+  bool refac_dirty = true;
+  std::unique_ptr<Engine> eng;
+  bool eng_dirty = true, eng_mixed = false;
+  DBuf<double> dx, db, dscal, hist;
+  DBuf<unsigned long long> dlinf;
+  double *hbuf = nullptr;          // pinned: 64 doubles
+  double *px = nullptr, *pb = nullptr;  // pinned staging (ncell each)
+  std::vector<double> hhist;
+  int nhist = 0;
+  long long ncell() const { return (long long)nx * ny * nz; }
+};
+
+namespace {
+
+int fail(int code, const std::string &m) {
+  g_err = m;
+  return code;
+}
+
+template <typename F>
+int guard(pbg_session *s, F &&f) {
+  try {
+    if (s) PBG_CUDA(cudaSetDevice(s->device));
+    return f();
+  } catch (const CudaError &e) {
+    return fail(PBG_ERR_CUDA, e.what());
+  } catch (const std::bad_alloc &) {
+    return fail(PBG_ERR_NOMEM, "host allocation failed");
+  } catch (const std::exception &e) {
+    return fail(PBG_ERR_STATE, e.what());
+  }
+}
+
+// (i,j,k) interior of a strided array -> compact
+template <typename T, typename U>
+void gather(const T *src, U *dst, int nx, int ny, int nz, long long si, long long sj, long long sk,
+            long long off) {
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k)
+        dst[((size_t)i * ny + j) * nz + k] = (U)src[off + i * si + j * sj + k * sk];
+}
+
+__global__ void k_gather(const double *__restrict__ src, double *__restrict__ dst, int nx, int ny,
+                         int nz, long long si, long long sj, long long sk, long long off) {
+  const long long N = (long long)nx * ny * nz;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    Pos q = pos_of(p, ny, nz);
+    dst[p] = src[off + q.i * si + q.j * sj + q.k * sk];
+  }
+}
+__global__ void k_scatter(const double *__restrict__ src, double *__restrict__ dst, int nx, int ny,
+                          int nz, long long si, long long sj, long long sk, long long off) {
+  const long long N = (long long)nx * ny * nz;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    Pos q = pos_of(p, ny, nz);
+    dst[off + q.i * si + q.j * sj + q.k * sk] = src[p];
+  }
+}
+
+__device__ __forceinline__ double harm_d(double a, double b) {
+  return __ddiv_rn(__dmul_rn(__dmul_rn(a, b), 2.0), __dadd_rn(a, b));
+}
+
+// On-device fixture assembly, bit-identical to pbg_gen_assemble (see
+// problem_gen.h for the reference lines each step follows). Writes the
+// symmetric storage c, w, s, b and the active flags.
+__global__ void k_assemble(int nx, int ny, int nz, double h, int4 bc03, int2 bc45,
+                           const double *__restrict__ rho, const uint8_t *__restrict__ solid,
+                           double *__restrict__ C, double *__restrict__ W, double *__restrict__ S,
+                           double *__restrict__ B, uint8_t *__restrict__ aflag) {
+  const long long N = (long long)nx * ny * nz, SI = (long long)ny * nz, SJ = nz;
+  const int bc[6] = {bc03.x, bc03.y, bc03.z, bc03.w, bc45.x, bc45.y};
+  const double hx = __ddiv_rn(__dmul_rn(h, h), h);
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    Pos q = pos_of(p, ny, nz);
+    const double rp = rho[p];
+    const uint8_t sp = solid[p];
+    double a[6];
+    a[0] = __ddiv_rn(hx, q.i > 0 ? harm_d(rho[p - SI], rp) : rp);
+    a[1] = __ddiv_rn(hx, q.i < nx - 1 ? harm_d(rp, rho[p + SI]) : rp);
+    a[2] = __ddiv_rn(hx, q.j > 0 ? harm_d(rho[p - SJ], rp) : rp);
+    a[3] = __ddiv_rn(hx, q.j < ny - 1 ? harm_d(rp, rho[p + SJ]) : rp);
+    if (nz > 1) {
+      a[4] = __ddiv_rn(hx, q.k > 0 ? harm_d(rho[p - 1], rp) : rp);
+      a[5] = __ddiv_rn(hx, q.k < nz - 1 ? harm_d(rp, rho[p + 1]) : rp);
+    } else {
+      a[4] = 0.0;
+      a[5] = 0.0;
+    }
+    double c = a[0];
+    for (int f = 1; f < 6; ++f) c = __dadd_rn(c, a[f]);
+    if (q.i > 0 && solid[p - SI] != sp) a[0] = 0.0;
+    if (q.i < nx - 1 && solid[p + SI] != sp) a[1] = 0.0;
+    if (q.j > 0 && solid[p - SJ] != sp) a[2] = 0.0;
+    if (q.j < ny - 1 && solid[p + SJ] != sp) a[3] = 0.0;
+    if (q.k > 0 && solid[p - 1] != sp) a[4] = 0.0;
+    if (q.k < nz - 1 && solid[p + 1] != sp) a[5] = 0.0;
+    if (!sp) {
+      c = a[0];
+      for (int f = 1; f < 6; ++f) c = __dadd_rn(c, a[f]);
+    }
+    const bool onb[6] = {q.i == 0, q.i == nx - 1, q.j == 0, q.j == ny - 1, q.k == 0, q.k == nz - 1};
+    for (int f = 0; f < 6; ++f) {  // Neumann sides first, in face order
+      if (bc[f] != PBG_BC_NEUMANN || (nz == 1 && f >= 4) || !onb[f]) continue;
+      c = __dsub_rn(c, a[f]);
+      a[f] = 0.0;
+    }
+    for (int f = 0; f < 6; ++f)
+      if (bc[f] == PBG_BC_DIRICHLET && onb[f]) a[f] = 0.0;
+    if (sp) {
+      c = __dmul_rn(c, 1.0e-12);
+      for (int f = 0; f < 6; ++f) a[f] = 0.0;
+    }
+    C[p] = c;
+    W[p] = a[0];
+    S[p] = a[2];
+    B[p] = a[4];
+    aflag[p] = sp ? 0 : 1;
+  }
+}
+
+void ensure_staging(pbg_session *s) {
+  if (!s->px) {
+    PBG_CUDA(cudaMallocHost((void **)&s->px, sizeof(double) * s->ncell()));
+    PBG_CUDA(cudaMallocHost((void **)&s->pb, sizeof(double) * s->ncell()));
+  }
+  if (s->dx.n == 0) { s->dx.alloc(s->ncell()); s->db.alloc(s->ncell()); }
+}
+
+void invalidate(pbg_session *s) {
+  s->refac_dirty = true;
+  s->eng_dirty = true;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *pbg_last_error(void) { return g_err.c_str(); }
+int pbg_version(void) { return PBG_API_VERSION; }
+
+int pbg_device_count(int *count) {
+  if (!count) return fail(PBG_ERR_ARG, "count is NULL");
+  cudaError_t e = cudaGetDeviceCount(count);
+  if (e != cudaSuccess) { *count = 0; return fail(PBG_ERR_CUDA, cudaGetErrorString(e)); }
+  return PBG_OK;
+}
+
+void pbg_params_default(pbg_params *p, int solver) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->solver = solver;
+  p->precision = PBG_FP64;
+  p->min_iter = 1;
+  p->max_iter = 20;
+  p->res_rat = 0.01;
+  p->res_tol = 1.0e-15;
+  p->scale = 1.0;
+  p->stalecount = -1;
+  p->init_cycle = PBG_CYCLE_NONE;
+  p->loop_cycle = PBG_CYCLE_V;
+  p->toler = -1.0;
+  p->factor = 0.01;
+  p->max_cycles = 20;
+  p->min_cycles = 0;
+  p->stop_if_div = 1;
+  p->priority_min_cyc = 1;
+  for (int q = 0; q < 3; ++q) { p->mv[q] = 20; p->ms[q] = -1; }
+  p->tol = 1.0e-8;
+  p->inner_tol = 1.0e-4;
+  p->max_sweeps = 8;
+  if (solver == PBG_SOLVER_ENGINE) p->max_iter = 500;
+}
+
+int pbg_session_create(int nx, int ny, int nz, double h, const int bc[6], int device,
+                       pbg_session **out) {
+  if (!out) return fail(PBG_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  if (nx < 1 || ny < 1 || nz < 1 || !(h > 0.0))
+    return fail(PBG_ERR_ARG, "grid dimensions must be >= 1 and h > 0");
+  if ((long long)nx * ny * nz > (1LL << 31))
+    return fail(PBG_ERR_ARG, "more than 2^31 cells in one session");
+  auto s = std::make_unique<pbg_session>();
+  s->device = device;
+  s->nx = nx; s->ny = ny; s->nz = nz; s->h = h;
+  if (bc) for (int f = 0; f < 6; ++f) s->bc[f] = bc[f];
+  int rc = guard(s.get(), [&]() -> int {
+    PBG_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    s->red.init();
+    s->kst.alloc(1);
+    PBG_CUDA(cudaMallocHost((void **)&s->hkst, sizeof(KrylovState)));
+    PBG_CUDA(cudaMallocHost((void **)&s->hbuf, 64 * sizeof(double)));
+    s->aflag.alloc(s->ncell());
+    PBG_CUDA(cudaMemset(s->aflag.p, 1, s->ncell()));
+    s->dscal.alloc(8);
+    s->dlinf.alloc(1);
+    s->hist.alloc(kHistMax);
+    return PBG_OK;
+  });
+  if (rc != PBG_OK) return rc;
+  *out = s.release();
+  return PBG_OK;
+}
+
+int pbg_session_destroy(pbg_session *s) {
+  if (!s) return PBG_OK;
+  int rc = guard(s, [&]() -> int {
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    s->eng.reset();
+    s->refac.reset();
+    if (s->hkst) cudaFreeHost(s->hkst);
+    if (s->hbuf) cudaFreeHost(s->hbuf);
+    if (s->px) cudaFreeHost(s->px);
+    if (s->pb) cudaFreeHost(s->pb);
+    s->hkst = nullptr; s->hbuf = s->px = s->pb = nullptr;
+    return PBG_OK;
+  });
+  cudaStream_t st = s->stream;
+  delete s;
+  if (st) cudaStreamDestroy(st);
+  return rc;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int pbg_session_info(const pbg_session *s, long long *ncell, int *symmetric, long long *device_bytes) {
+  if (!s) return fail(PBG_ERR_ARG, "session is NULL");
+  if (ncell) *ncell = s->ncell();
+  if (symmetric) *symmetric = s->A.sym ? 1 : 0;
+  if (device_bytes) {
+    size_t b = s->A.c.bytes() + s->A.w.bytes() + s->A.e.bytes() + s->A.s.bytes() + s->A.n.bytes() +
+               s->A.b.bytes() + s->A.t.bytes() + s->aflag.bytes() + s->dx.bytes() + s->db.bytes();
+    *device_bytes = (long long)b;
+  }
+  return PBG_OK;
+}
+
+int pbg_matrix_upload(pbg_session *s, const double *c, const double *w, const double *e,
+                      const double *sv, const double *n, const double *b, const double *t,
+                      long long si, long long sj, long long sk, long long offset, int where) {
+  if (!s || !c || !w || !e || !sv || !n || !b || !t) return fail(PBG_ERR_ARG, "NULL argument");
+  return guard(s, [&]() -> int {
+    const long long N = s->ncell();
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    const double *src[7] = {c, w, e, sv, n, b, t};
+    std::vector<std::vector<double>> h(7, std::vector<double>(N));
+    if (where == PBG_HOST) {
+      for (int q = 0; q < 7; ++q) gather(src[q], h[q].data(), nx, ny, nz, si, sj, sk, offset);
+    } else {
+      DBuf<double> tmp(N);
+      for (int q = 0; q < 7; ++q) {
+        k_gather<<<grid_for(N), kThreads, 0, s->stream>>>(src[q], tmp.p, nx, ny, nz, si, sj, sk, offset); note_launch();
+        PBG_CUDA(cudaMemcpyAsync(h[q].data(), tmp.p, N * 8, cudaMemcpyDeviceToHost, s->stream));
+      }
+      PBG_CUDA(cudaStreamSynchronize(s->stream));
+    }
+    // symmetry: e(i) == w(i+1), n(j) == s(j+1), t(k) == b(k+1) bit for bit,
+    // and the outermost e / n / t are zero
+    const long long SI = (long long)ny * nz, SJ = nz;
+    bool sym = true;
+    for (int i = 0; i < nx && sym; ++i)
+      for (int j = 0; j < ny && sym; ++j)
+        for (int k = 0; k < nz && sym; ++k) {
+          long long p = ((long long)i * ny + j) * nz + k;
+          double ee = i < nx - 1 ? h[1][p + SI] : 0.0;
+          double nn = j < ny - 1 ? h[3][p + SJ] : 0.0;
+          double tt = k < nz - 1 ? h[5][p + 1] : 0.0;
+          if (std::memcmp(&ee, &h[2][p], 8) || std::memcmp(&nn, &h[4][p], 8) ||
+              std::memcmp(&tt, &h[6][p], 8))
+            sym = false;
+        }
+    Mat64 &A = s->A;
+    A.nx = nx; A.ny = ny; A.nz = nz; A.sym = sym;
+    A.c.alloc(N); A.w.alloc(N); A.s.alloc(N); A.b.alloc(N);
+    if (sym) { A.e.release(); A.n.release(); A.t.release(); }
+    else { A.e.alloc(N); A.n.alloc(N); A.t.alloc(N); }
+    DBuf<double> *dst[7] = {&A.c, &A.w, &A.e, &A.s, &A.n, &A.b, &A.t};
+    for (int q = 0; q < 7; ++q)
+      if (dst[q]->p) PBG_CUDA(cudaMemcpyAsync(dst[q]->p, h[q].data(), N * 8, cudaMemcpyHostToDevice, s->stream));
+    PBG_CUDA(cudaStreamSynchronize(s->stream));
+    s->have_matrix = true;
+    invalidate(s);
+    return PBG_OK;
+  });
+}
+
+int pbg_matrix_download(pbg_session *s, double *c, double *w, double *e, double *sv, double *n,
+                        double *b, double *t, int where) {
+  if (!s) return fail(PBG_ERR_ARG, "session is NULL");
+  if (!s->have_matrix) return fail(PBG_ERR_STATE, "no matrix");
+  return guard(s, [&]() -> int {
+    const long long N = s->ncell();
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    const long long SI = (long long)ny * nz, SJ = nz;
+    std::vector<double> h(7 * N, 0.0);
+    const Mat64 &A = s->A;
+    const double *src[7] = {A.c.p, A.w.p, A.e.p, A.s.p, A.n.p, A.b.p, A.t.p};
+    for (int q = 0; q < 7; ++q)
+      if (src[q]) PBG_CUDA(cudaMemcpyAsync(&h[q * N], src[q], N * 8, cudaMemcpyDeviceToHost, s->stream));
+    PBG_CUDA(cudaStreamSynchronize(s->stream));
+    if (A.sym)
+      for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+          for (int k = 0; k < nz; ++k) {
+            long long p = ((long long)i * ny + j) * nz + k;
+            h[2 * N + p] = i < nx - 1 ? h[1 * N + p + SI] : 0.0;
+            h[4 * N + p] = j < ny - 1 ? h[3 * N + p + SJ] : 0.0;
+            h[6 * N + p] = k < nz - 1 ? h[5 * N + p + 1] : 0.0;
+          }
+    double *dst[7] = {c, w, e, sv, n, b, t};
+    for (int q = 0; q < 7; ++q) {
+      if (!dst[q]) continue;
+      if (where == PBG_HOST) std::memcpy(dst[q], &h[q * N], N * 8);
+      else PBG_CUDA(cudaMemcpyAsync(dst[q], &h[q * N], N * 8, cudaMemcpyHostToDevice, s->stream));
+    }
+    PBG_CUDA(cudaStreamSynchronize(s->stream));
+    return PBG_OK;
+  });
+}
+
+int pbg_active_upload(pbg_session *s, const int *aflag, long long si, long long sj, long long sk,
+                      long long offset, int where) {
+  if (!s || !aflag) return fail(PBG_ERR_ARG, "NULL argument");
+  if (where != PBG_HOST) return fail(PBG_ERR_UNSUPPORTED, "active flags are uploaded from host memory");
+  return guard(s, [&]() -> int {
+    std::vector<uint8_t> h(s->ncell());
+    for (int i = 0; i < s->nx; ++i)
+      for (int j = 0; j < s->ny; ++j)
+        for (int k = 0; k < s->nz; ++k)
+          h[((size_t)i * s->ny + j) * s->nz + k] = aflag[offset + i * si + j * sj + k * sk] ? 1 : 0;
+    PBG_CUDA(cudaMemcpy(s->aflag.p, h.data(), h.size(), cudaMemcpyHostToDevice));
+    invalidate(s);
+    return PBG_OK;
+  });
+}
+
+int pbg_assemble_pressure(pbg_session *s, const double *rho, const uint8_t *solid, int where) {
+  if (!s || !rho || !solid) return fail(PBG_ERR_ARG, "NULL argument");
+  return guard(s, [&]() -> int {
+    const long long N = s->ncell();
+    DBuf<double> drho;
+    DBuf<uint8_t> dsol;
+    const double *r = rho;
+    const uint8_t *so = solid;
+    if (where == PBG_HOST) {
+      drho.alloc(N); dsol.alloc(N);
+      PBG_CUDA(cudaMemcpyAsync(drho.p, rho, N * 8, cudaMemcpyHostToDevice, s->stream));
+      PBG_CUDA(cudaMemcpyAsync(dsol.p, solid, N, cudaMemcpyHostToDevice, s->stream));
+      r = drho.p; so = dsol.p;
+    }
+    Mat64 &A = s->A;
+    A.nx = s->nx; A.ny = s->ny; A.nz = s->nz; A.sym = true;
+    if (A.c.n != (size_t)N) { A.c.alloc(N); A.w.alloc(N); A.s.alloc(N); A.b.alloc(N); }
+    A.e.release(); A.n.release(); A.t.release();
+    k_assemble<<<grid_for(N), kThreads, 0, s->stream>>>(
+        s->nx, s->ny, s->nz, s->h, make_int4(s->bc[0], s->bc[1], s->bc[2], s->bc[3]),
+        make_int2(s->bc[4], s->bc[5]), r, so, A.c.p, A.w.p, A.s.p, A.b.p, s->aflag.p); note_launch();
+    PBG_CUDA(cudaGetLastError());
+    PBG_CUDA(cudaStreamSynchronize(s->stream));
+    s->have_matrix = true;
+    invalidate(s);
+    return PBG_OK;
+  });
+}
+
+}  // extern "C"
+
+namespace {
+
+void ensure_refac(pbg_session *s) {
+  if (!s->refac) s->refac = std::make_unique<RefAC>();
+  if (s->refac_dirty) {
+    s->refac->build(s->A.view(), s->aflag.p, s->h, s->stream);
+    PBG_CUDA(cudaStreamSynchronize(s->stream));
+    s->refac_dirty = false;
+  }
+}
+
+void ensure_engine(pbg_session *s, bool mixed) {
+  if (!s->eng) s->eng = std::make_unique<Engine>();
+  if (s->eng_dirty || (mixed && !s->eng->have32)) {
+    const Mat64 &A = s->A;
+    EMat<double> m{A.nx, A.ny, A.nz, A.c.p, A.w.p, A.s.p, A.b.p};
+    s->eng->build(m, s->stream, mixed || s->eng_mixed);
+    s->eng_mixed = s->eng_mixed || mixed;
+    s->eng_dirty = false;
+  }
+}
+
+int solve_device(pbg_session *s, double *xd, const double *bd, const pbg_params *p, pbg_result *r) {
+  pbg_result out;
+  std::memset(&out, 0, sizeof(out));
+  const double dV = (s->h * s->h) * s->h;
+  s->nhist = 0;
+  if (p->solver == PBG_SOLVER_CG || p->solver == PBG_SOLVER_BICGS) {
+    KrylovParams pr;
+    pr.mini = p->min_iter; pr.maxit = p->max_iter;
+    pr.stalecount = p->stalecount > kStaleMax ? kStaleMax : p->stalecount;
+    pr.hist_cap = kHistMax;
+    pr.res_rat = p->res_rat; pr.res_tol = p->res_tol; pr.scale = p->scale; pr.dV = dV;
+    RefKrylovResult rr = ref_krylov_solve(s->A.view(), xd, bd, pr, p->solver == PBG_SOLVER_BICGS ? 1 : 0,
+                                          s->rkw, s->red, s->kst.p, s->hkst, s->hist.p, s->stream);
+    out.status = rr.status;
+    out.converged = rr.converged;
+    out.iterations = rr.iterations;
+    out.res0 = rr.res0;
+    out.res = rr.res;
+    out.levels = 1;
+    int nh = rr.iterations < kHistMax ? rr.iterations : kHistMax;
+    s->hhist.resize(nh);
+    if (nh) PBG_CUDA(cudaMemcpy(s->hhist.data(), s->hist.p, nh * 8, cudaMemcpyDeviceToHost));
+    s->nhist = nh;
+  } else if (p->solver == PBG_SOLVER_AC) {
+    ensure_refac(s);
+    RefACParams pa;
+    pa.init = p->init_cycle; pa.loop = p->loop_cycle;
+    pa.toler = p->toler; pa.factor = p->factor;
+    pa.max_cyc = p->max_cycles; pa.min_cyc = p->min_cycles;
+    pa.stop_if_div = p->stop_if_div; pa.priority_min_cyc = p->priority_min_cyc;
+    for (int q = 0; q < 3; ++q) { pa.mv[q] = p->mv[q]; pa.ms[q] = p->ms[q] > kStaleMax ? kStaleMax : p->ms[q]; }
+    pa.resrat_val = 1.0e-18;  // AC defaults (additive.cpp:17-18): atto
+    pa.restol_val = 1.0e-18;
+    RefACCtx cx;
+    cx.s = s->stream; cx.w = &s->rkw; cx.red = &s->red; cx.st = s->kst.p;
+    cx.dscal = s->dscal.p; cx.dmean = s->dscal.p + 4; cx.hbuf = s->hbuf; cx.dlinf = s->dlinf.p;
+    for (int q = 0; q < 3; ++q) { cx.mv[q] = pa.mv[q]; cx.ms[q] = pa.ms[q]; }
+    cx.resrat_val = pa.resrat_val; cx.restol_val = pa.restol_val;
+    s->hhist.assign(p->max_cycles + 2, 0.0);
+    RefACResult ar = s->refac->cycle(xd, bd, pa, cx, s->hhist.data(), (int)s->hhist.size());
+    s->nhist = ar.nhist < (int)s->hhist.size() ? ar.nhist : (int)s->hhist.size();
+    out.converged = ar.converged;
+    out.cycles = ar.cycles;
+    out.status = ar.converged ? PBG_CONVERGED : (ar.diverged ? PBG_DIVERGED : PBG_MAXITER);
+    out.res0 = ar.res0;
+    out.res = ar.res;
+    out.levels = s->refac->nlevels();
+  } else if (p->solver == PBG_SOLVER_ENGINE) {
+    if (!s->A.sym) return fail(PBG_ERR_UNSUPPORTED, "the engine solver needs a symmetric matrix");
+    const bool mixed = p->precision == PBG_MIXED;
+    ensure_engine(s, mixed);
+    EngineResult er = mixed ? s->eng->solve_mixed(xd, bd, p->tol, p->inner_tol, p->max_sweeps,
+                                                  p->max_iter, s->red, s->stream, s->hist.p)
+                            : s->eng->solve_fp64(xd, bd, p->tol, p->max_iter, s->red, s->stream,
+                                                 s->hist.p);
+    out.status = er.status;
+    out.converged = er.converged;
+    out.iterations = er.iterations;
+    out.sweeps = er.sweeps;
+    out.relres = er.relres;
+    out.res = er.relres;
+    out.levels = s->eng->nlevels();
+    int nh = er.iterations < kHistMax ? er.iterations : kHistMax;
+    s->hhist.resize(nh);
+    if (nh) PBG_CUDA(cudaMemcpy(s->hhist.data(), s->hist.p, nh * 8, cudaMemcpyDeviceToHost));
+    s->nhist = nh;
+  } else {
+    return fail(PBG_ERR_ARG, "unknown solver");
+  }
+  if (r) *r = out;
+  return PBG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pbg_solve_strided(pbg_session *s, double *x, const double *b, long long si, long long sj,
+                      long long sk, long long offset, int where, const pbg_params *p,
+                      pbg_result *r) {
+  if (!s || !x || !b || !p) return fail(PBG_ERR_ARG, "NULL argument");
+  if (!s->have_matrix) return fail(PBG_ERR_STATE, "no matrix uploaded or assembled");
+  if (p->solver == PBG_SOLVER_ENGINE && !(p->tol > 0.0))
+    return fail(PBG_ERR_ARG, "engine tolerance must be > 0");
+  return guard(s, [&]() -> int {
+    auto t0 = std::chrono::steady_clock::now();
+    const long long N = s->ncell();
+    const bool compact = (si == (long long)s->ny * s->nz && sj == s->nz && sk == 1 && offset == 0);
+    int rc;
+    if (where == PBG_DEVICE && compact) {
+      rc = solve_device(s, x, b, p, r);
+    } else {
+      ensure_staging(s);
+      if (where == PBG_HOST) {
+        if (compact) {
+          std::memcpy(s->px, x, N * 8);
+          std::memcpy(s->pb, b, N * 8);
+        } else {
+          gather(x, s->px, s->nx, s->ny, s->nz, si, sj, sk, offset);
+          gather(b, s->pb, s->nx, s->ny, s->nz, si, sj, sk, offset);
+        }
+        PBG_CUDA(cudaMemcpyAsync(s->dx.p, s->px, N * 8, cudaMemcpyHostToDevice, s->stream));
+        PBG_CUDA(cudaMemcpyAsync(s->db.p, s->pb, N * 8, cudaMemcpyHostToDevice, s->stream));
+      } else {
+        k_gather<<<grid_for(N), kThreads, 0, s->stream>>>(x, s->dx.p, s->nx, s->ny, s->nz, si, sj, sk, offset); note_launch();
+        k_gather<<<grid_for(N), kThreads, 0, s->stream>>>(b, s->db.p, s->nx, s->ny, s->nz, si, sj, sk, offset); note_launch();
+      }
+      rc = solve_device(s, s->dx.p, s->db.p, p, r);
+      if (rc == PBG_OK) {
+        if (where == PBG_HOST) {
+          PBG_CUDA(cudaMemcpyAsync(s->px, s->dx.p, N * 8, cudaMemcpyDeviceToHost, s->stream));
+          PBG_CUDA(cudaStreamSynchronize(s->stream));
+          if (compact) std::memcpy(x, s->px, N * 8);
+          else
+            for (int i = 0; i < s->nx; ++i)
+              for (int j = 0; j < s->ny; ++j)
+                for (int k = 0; k < s->nz; ++k)
+                  x[offset + i * si + j * sj + k * sk] = s->px[((size_t)i * s->ny + j) * s->nz + k];
+        } else {
+          k_scatter<<<grid_for(N), kThreads, 0, s->stream>>>(s->dx.p, x, s->nx, s->ny, s->nz, si, sj, sk, offset); note_launch();
+        }
+      }
+    }
+    PBG_CUDA(cudaStreamSynchronize(s->stream));
+    if (r) r->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+  });
+}
+
+int pbg_solve(pbg_session *s, double *x, const double *b, int where, const pbg_params *p,
+              pbg_result *r) {
+  if (!s) return fail(PBG_ERR_ARG, "session is NULL");
+  return pbg_solve_strided(s, x, b, (long long)s->ny * s->nz, s->nz, 1, 0, where, p, r);
+}
+
+int pbg_history(const pbg_session *s, double *out, int cap, int *count) {
+  if (!s) return fail(PBG_ERR_ARG, "session is NULL");
+  int n = s->nhist < cap ? s->nhist : cap;
+  if (out && n > 0) std::memcpy(out, s->hhist.data(), n * 8);
+  if (count) *count = s->nhist;
+  return PBG_OK;
+}
+
+static int op_run(pbg_session *s, int op, const double *x, const double *b, double *y, int where,
+                  double *out2) {
+  if (!s) return fail(PBG_ERR_ARG, "session is NULL");
+  if (op != 2 && !s->have_matrix) return fail(PBG_ERR_STATE, "no matrix");
+  return guard(s, [&]() -> int {
+    const long long N = s->ncell();
+    const double *dxp = x, *dbp = b;
+    double *dyp = y;
+    DBuf<double> t1, t2, t3;
+    if (where == PBG_HOST) {
+      t1.alloc(N);
+      PBG_CUDA(cudaMemcpyAsync(t1.p, x, N * 8, cudaMemcpyHostToDevice, s->stream));
+      dxp = t1.p;
+      if (b) { t2.alloc(N); PBG_CUDA(cudaMemcpyAsync(t2.p, b, N * 8, cudaMemcpyHostToDevice, s->stream)); dbp = t2.p; }
+      if (y) { t3.alloc(N); dyp = t3.p; }
+    }
+    const int g = grid_for(N);
+    if (op == 0) { k_spmv_ref<<<g, kThreads, 0, s->stream>>>(s->A.view(), dxp, dyp); note_launch(); }
+    else if (op == 1) { k_resid_ref<<<g, kThreads, 0, s->stream>>>(s->A.view(), dxp, dbp, dyp); note_launch(); }
+    else {
+      k_dot2<<<g, kThreads, 0, s->stream>>>(N, dxp, dbp, (s->h * s->h) * s->h, s->red.slot_part(0),
+                                           s->red.slot_count(0), s->dscal.p); note_launch();
+      PBG_CUDA(cudaMemcpyAsync(s->hbuf, s->dscal.p, 16, cudaMemcpyDeviceToHost, s->stream));
+    }
+    PBG_CUDA(cudaGetLastError());
+    if (where == PBG_HOST && y) PBG_CUDA(cudaMemcpyAsync(y, dyp, N * 8, cudaMemcpyDeviceToHost, s->stream));
+    PBG_CUDA(cudaStreamSynchronize(s->stream));
+    if (op == 2) {
+      double n = (double)N;
+      out2[0] = s->hbuf[0];
+      out2[1] = s->hbuf[1] / n / n;
+    }
+    return PBG_OK;
+  });
+}
+
+int pbg_spmv(pbg_session *s, const double *x, double *y, int where) {
+  if (!x || !y) return fail(PBG_ERR_ARG, "NULL argument");
+  return op_run(s, 0, x, nullptr, y, where, nullptr);
+}
+int pbg_residual(pbg_session *s, const double *x, const double *b, double *r, int where) {
+  if (!x || !b || !r) return fail(PBG_ERR_ARG, "NULL argument");
+  return op_run(s, 1, x, b, r, where, nullptr);
+}
+int pbg_dot(pbg_session *s, const double *x, const double *y, int where, double out[2]) {
+  if (!x || !y || !out) return fail(PBG_ERR_ARG, "NULL argument");
+  return op_run(s, 2, x, y, nullptr, where, out);
+}
+
+int pbg_levels(pbg_session *s, int kind, int *count, int *dims, int cap) {
+  if (!s || !count) return fail(PBG_ERR_ARG, "NULL argument");
+  if (!s->have_matrix) return fail(PBG_ERR_STATE, "no matrix");
+  return guard(s, [&]() -> int {
+    std::vector<int> d;
+    if (kind == 0) {
+      ensure_refac(s);
+      for (auto &l : s->refac->L) { d.push_back(l.nx); d.push_back(l.ny); d.push_back(l.nz); }
+    } else {
+      ensure_engine(s, false);
+      for (auto &l : s->eng->L) { d.push_back(l.nx); d.push_back(l.ny); d.push_back(l.nz); }
+    }
+    *count = (int)d.size() / 3;
+    if (dims) for (int q = 0; q < (int)d.size() && q < 3 * cap; ++q) dims[q] = d[q];
+    return PBG_OK;
+  });
+}
+
+int pbg_ac_level_matrix(pbg_session *s, int level, double *out7, int where) {
+  if (!s || !out7) return fail(PBG_ERR_ARG, "NULL argument");
+  if (!s->have_matrix) return fail(PBG_ERR_STATE, "no matrix");
+  return guard(s, [&]() -> int {
+    ensure_refac(s);
+    if (level < 1 || level >= s->refac->nlevels()) return fail(PBG_ERR_ARG, "level out of range");
+    s->refac->coarsen_all(s->stream);
+    const RefACLevel &L = s->refac->L[level];
+    const long long n = (long long)L.nx * L.ny * L.nz;
+    const double *src[7] = {L.A.c.p, L.A.w.p, L.A.e.p, L.A.s.p, L.A.n.p, L.A.b.p, L.A.t.p};
+    for (int q = 0; q < 7; ++q)
+      PBG_CUDA(cudaMemcpyAsync(out7 + q * n, src[q], n * 8,
+                               where == PBG_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                               s->stream));
+    PBG_CUDA(cudaStreamSynchronize(s->stream));
+    return PBG_OK;
+  });
+}
+
+int pbg_generate(int kind, const double *params, uint64_t seed, int dims[3], double *h,
+                 double *rho, uint8_t *solid, double *b) {
+  if (!params || !dims || !h) return fail(PBG_ERR_ARG, "NULL argument");
+  pbg_problem_desc d;
+  int n = (int)params[0];
+  if (kind == 0) pbg_desc_single_bubble(&d, n, seed);
+  else if (kind == 1)
+    pbg_desc_bubbles_cylinder(&d, n, (int)params[1], params[2], params[3], params[4], params[5], seed);
+  else if (kind == 2)
+    pbg_desc_batch_member(&d, seed, (int)params[6], (int)params[7], (int)params[8], (int)params[9],
+                          (int)params[10], (int)params[11]);
+  else return fail(PBG_ERR_ARG, "unknown kind");
+  dims[0] = d.nx; dims[1] = d.ny; dims[2] = d.nz;
+  *h = d.h;
+  if (!rho) return PBG_OK;
+  if (!solid || !b) return fail(PBG_ERR_ARG, "rho, solid and b go together");
+  pbg_gen_fields(&d, rho, solid);
+  pbg_gen_rhs(&d, (uint64_t)params[12], solid, b);
+  return PBG_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+unsigned long long pbg_launch_count(void) { return __atomic_load_n(&pbg::g_launch_count, __ATOMIC_RELAXED); }
+
+int pbg_session_stream(pbg_session *s, void **stream) {
+  if (!s || !stream) return fail(PBG_ERR_ARG, "NULL argument");
+  *stream = (void *)s->stream;
+  return PBG_OK;
+}
+
+int pbg_bench_kernel(pbg_session *s, int which, int precision, int reps, double *ms,
+                     double *bytes_per_launch) {
+  if (!s || !ms || reps < 1) return fail(PBG_ERR_ARG, "bad argument");
+  if (!s->have_matrix) return fail(PBG_ERR_STATE, "no matrix");
+  return guard(s, [&]() -> int {
+    const long long N = s->ncell();
+    if (which == 0) {
+      if (!s->A.sym) return fail(PBG_ERR_UNSUPPORTED, "engine needs a symmetric matrix");
+      ensure_engine(s, precision == 1);
+      *ms = s->eng->bench_sweep(precision, reps, s->stream);
+      if (bytes_per_launch) *bytes_per_launch = (double)N * (precision == 1 ? 28.0 : 56.0);
+      return PBG_OK;
+    }
+    if (which == 1) {
+      ensure_staging(s);
+      PBG_CUDA(cudaMemsetAsync(s->dx.p, 0, N * 8, s->stream));
+      cudaEvent_t e0, e1;
+      PBG_CUDA(cudaEventCreate(&e0));
+      PBG_CUDA(cudaEventCreate(&e1));
+      const int g = grid_for(N);
+      k_spmv_ref<<<g, kThreads, 0, s->stream>>>(s->A.view(), s->dx.p, s->db.p); note_launch();
+      PBG_CUDA(cudaEventRecord(e0, s->stream));
+      for (int q = 0; q < reps; ++q) {
+        k_spmv_ref<<<g, kThreads, 0, s->stream>>>(s->A.view(), (q & 1) ? s->db.p : s->dx.p,
+                                                  (q & 1) ? s->dx.p : s->db.p); note_launch();
+      }
+      PBG_CUDA(cudaEventRecord(e1, s->stream));
+      PBG_CUDA(cudaEventSynchronize(e1));
+      float t = 0.f;
+      PBG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      *ms = (double)t / reps;
+      if (bytes_per_launch) *bytes_per_launch = (double)N * (s->A.sym ? 48.0 : 72.0);
+      return PBG_OK;
+    }
+    return fail(PBG_ERR_ARG, "unknown kernel id");
+  });
+}
+
+}  // extern "C"

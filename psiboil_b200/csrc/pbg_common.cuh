@@ -1,0 +1,178 @@
+// Common device/host definitions of the B200 pressure-Poisson engine.
+//
+// Cell layout on the device: interior cells only, index = (i*ny + j)*nz + k
+// (k fastest), the interior of the reference's val[i][j][k] block
+// (PSI-BOIL Src/Global/global_malloc.cpp:35-56). Out-of-domain neighbours
+// contribute nothing: their coefficients are zero after the boundary
+// correction (Src/Equation/Centered/centered_system_bnd.cpp), which is what
+// the reference's zero-valued halo multiplies.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <stdexcept>
+#include <string>
+
+namespace pbg {
+
+constexpr int kThreads = 256;          // threads per block of the streaming kernels
+constexpr int kMaxBlocks = 148 * 8;    // grid cap: 8 blocks of 256 per SM on 148 SMs
+constexpr int kStaleMax = 64;          // longest Krylov staleness window kept on device
+constexpr int kHistMax = 4096;         // residual history entries kept on device
+
+struct CudaError : std::runtime_error {
+  explicit CudaError(const std::string &s) : std::runtime_error(s) {}
+};
+
+#define PBG_CUDA(call)                                                              \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess)                                                          \
+      throw ::pbg::CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));   \
+  } while (0)
+
+// Kernel launches issued by this library (a process-wide counter, read
+// through pbg_launch_count); used to report the launches of a timed region.
+extern unsigned long long g_launch_count;
+inline void note_launch() { __atomic_add_fetch(&g_launch_count, 1ULL, __ATOMIC_RELAXED); }
+
+inline int grid_for(long long n, int threads = kThreads, int cap = kMaxBlocks) {
+  long long b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > cap) b = cap;
+  return (int)b;
+}
+
+// ---------------------------------------------------------------------------
+// Matrix views. General storage keeps all seven arrays (the reference's
+// Matrix, Src/Matrix/matrix.h:23-54). Symmetric storage keeps c, w, s, b and
+// reads e(i) = w(i+1), n(j) = s(j+1), t(k) = b(k+1); it is chosen only when
+// the uploaded arrays satisfy those identities bit for bit, so the stencil
+// value is unchanged.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct MatView {
+  int nx, ny, nz;
+  const T *c, *w, *e, *s, *n, *b, *t;   // e, n, t == nullptr: symmetric storage
+  __host__ __device__ long long ncell() const { return (long long)nx * ny * nz; }
+};
+
+// Position of a cell from its linear index.
+struct Pos { int i, j, k; };
+__device__ __forceinline__ Pos pos_of(long long p, int ny, int nz) {
+  long long nynz = (long long)ny * nz;
+  int i = (int)(p / nynz);
+  long long rem = p - (long long)i * nynz;
+  int j = (int)(rem / nz);
+  int k = (int)(rem - (long long)j * nz);
+  return {i, j, k};
+}
+
+// The six neighbour coefficients of cell p (zero outside the domain).
+template <typename T>
+struct Nb { T w, e, s, n, b, t; };
+
+template <typename T>
+__device__ __forceinline__ Nb<T> coeffs(const MatView<T> &A, long long p, Pos q) {
+  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
+  Nb<T> o;
+  o.w = A.w[p];
+  o.s = A.s[p];
+  o.b = A.b[p];
+  if (A.e) {
+    o.e = A.e[p];
+    o.n = A.n[p];
+    o.t = A.t[p];
+  } else {
+    o.e = (q.i < A.nx - 1) ? A.w[p + SI] : T(0);
+    o.n = (q.j < A.ny - 1) ? A.s[p + SJ] : T(0);
+    o.t = (q.k < A.nz - 1) ? A.b[p + 1] : T(0);
+  }
+  return o;
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic grid reduction: each block reduces its values (fixed warp
+// order), writes one partial per value, and the last block to arrive sums
+// the partials in block order and runs the finalize step. No spin waits: the
+// "last block" is found with one atomic counter that the last block resets.
+// ---------------------------------------------------------------------------
+struct RedScratch {
+  double *part;        // [kRedSlots][kMaxBlocks] partial sums
+  unsigned *count;     // [kRedSlots] arrival counters (zero between uses)
+};
+constexpr int kRedVals = 4;   // values reduced by one kernel at most
+
+template <int NV>
+__device__ __forceinline__ void warp_sum(double (&v)[NV]) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] += __shfl_down_sync(0xffffffffu, v[q], off);
+}
+
+// Returns true in thread 0 of the last block; out[] then holds the totals.
+template <int NV>
+__device__ bool grid_reduce(double (&v)[NV], double *part, unsigned *count, double (&out)[NV]) {
+  __shared__ double sm[NV][kThreads / 32];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  warp_sum<NV>(v);
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) sm[q][wid] = v[q];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double s = 0.0;
+      for (int w = 0; w < nw; ++w) s += sm[q][w];
+      part[q * kMaxBlocks + blockIdx.x] = s;
+    }
+    __threadfence();
+    unsigned prev = atomicAdd(count, 1u);
+    last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  double acc[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) acc[q] = 0.0;
+  for (int bl = threadIdx.x; bl < (int)gridDim.x; bl += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[q] += __ldcg(&part[q * kMaxBlocks + bl]);
+  warp_sum<NV>(acc);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) sm[q][wid] = acc[q];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double s = 0.0;
+      for (int w = 0; w < nw; ++w) s += sm[q][w];
+      out[q] = s;
+    }
+    *count = 0u;
+    return true;
+  }
+  return false;
+}
+
+// Status words shared by all solvers (also the C-ABI result codes).
+enum SolveStatus : int {
+  ST_RUNNING = -1,
+  ST_CONVERGED = 0,
+  ST_MAXITER = 1,
+  ST_STALE = 2,
+  ST_BREAKDOWN = 3,
+  ST_INITIAL = 4,     // converged before the first iteration
+  ST_NAN = 5,
+  ST_DIVERGED = 6,
+};
+
+}  // namespace pbg

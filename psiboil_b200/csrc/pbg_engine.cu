@@ -1,0 +1,339 @@
+// Host side of the engine solver (hierarchy set-up, K-cycle recursion,
+// flexible CG and the mixed-precision refinement loop).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "pbg_engine.cuh"
+#include "pbg_engine_kernels.cuh"
+
+namespace pbg {
+
+template <typename T>
+void EWork<T>::ensure(const std::vector<ELevel> &lv) {
+  if (L.size() == lv.size() && x0.n == (size_t)lv[0].ncell()) return;
+  L.clear();
+  L.resize(lv.size());
+  for (size_t l = 0; l < lv.size(); ++l) {
+    size_t n = (size_t)lv[l].ncell();
+    Lv &v = L[l];
+    v.b.alloc(n); v.x.alloc(n); v.xa.alloc(n); v.xb.alloc(n);
+    if (l > 0) { v.z1.alloc(n); v.z2.alloc(n); v.q1.alloc(n); v.r1.alloc(n); v.v.alloc(n); }
+  }
+  size_t n0 = (size_t)lv[0].ncell();
+  x0.alloc(n0); r0.alloc(n0); z0.alloc(n0); pA.alloc(n0); pB.alloc(n0); q0.alloc(n0);
+  ks.alloc(lv.size());
+  fs.alloc(1);
+  PBG_CUDA(cudaMemset(fs.p, 0, sizeof(FcgScal)));
+}
+
+template struct EWork<double>;
+template struct EWork<float>;
+
+Engine::~Engine() {
+  if (hsc) cudaFreeHost(hsc);
+}
+
+template <> EMat<double> Engine::mat<double>(int l) const { return L[l].m64; }
+template <> EMat<float> Engine::mat<float>(int l) const { return L[l].m32; }
+
+// Dense inverse of the coarsest operator by Cholesky. A pivot below
+// 1e-10 x the largest diagonal (a solid-only aggregate, or the constant
+// mode of an all-Neumann problem) is skipped: that unknown is held at zero,
+// which gives a generalised inverse for a consistent singular system.
+static void dense_spd_inverse(int n, std::vector<double> &A) {
+  std::vector<double> Lm((size_t)n * n, 0.0);
+  std::vector<char> skip(n, 0);
+  double dmax = 0.0;
+  for (int i = 0; i < n; ++i) dmax = std::fmax(dmax, A[(size_t)i * n + i]);
+  for (int j = 0; j < n; ++j) {
+    double d = A[(size_t)j * n + j];
+    for (int k = 0; k < j; ++k) d -= Lm[(size_t)j * n + k] * Lm[(size_t)j * n + k];
+    if (!(d > 1e-10 * dmax)) { skip[j] = 1; continue; }
+    double ljj = std::sqrt(d);
+    Lm[(size_t)j * n + j] = ljj;
+    for (int i = j + 1; i < n; ++i) {
+      double v = A[(size_t)i * n + j];
+      for (int k = 0; k < j; ++k) v -= Lm[(size_t)i * n + k] * Lm[(size_t)j * n + k];
+      Lm[(size_t)i * n + j] = v / ljj;
+    }
+  }
+  std::vector<double> inv((size_t)n * n, 0.0), y(n);
+  for (int c = 0; c < n; ++c) {
+    for (int i = 0; i < n; ++i) {  // L y = e_c
+      if (skip[i]) { y[i] = 0.0; continue; }
+      double v = (i == c) ? 1.0 : 0.0;
+      for (int k = 0; k < i; ++k) v -= Lm[(size_t)i * n + k] * y[k];
+      y[i] = v / Lm[(size_t)i * n + i];
+    }
+    for (int i = n - 1; i >= 0; --i) {  // L^T x = y
+      if (skip[i]) { y[i] = 0.0; continue; }
+      double v = y[i];
+      for (int k = i + 1; k < n; ++k) v -= Lm[(size_t)k * n + i] * y[k];
+      y[i] = v / Lm[(size_t)i * n + i];
+    }
+    for (int i = 0; i < n; ++i) inv[(size_t)i * n + c] = y[i];
+  }
+  A.swap(inv);
+}
+
+void Engine::build(const EMat<double> &A0, cudaStream_t s, bool mixed) {
+  L.clear();
+  L.emplace_back();
+  L[0].nx = A0.nx; L[0].ny = A0.ny; L[0].nz = A0.nz;
+  L[0].m64 = A0;
+  while (L.back().ncell() > opt.coarse_max &&
+         (L.back().nx > 1 || L.back().ny > 1 || L.back().nz > 1)) {
+    const ELevel &f = L.back();
+    ELevel c;
+    c.nx = f.nx > 1 ? (f.nx + 1) / 2 : 1;
+    c.ny = f.ny > 1 ? (f.ny + 1) / 2 : 1;
+    c.nz = f.nz > 1 ? (f.nz + 1) / 2 : 1;
+    long long n = c.ncell();
+    c.c64.alloc(n); c.w64.alloc(n); c.s64.alloc(n); c.b64.alloc(n);
+    k_galerkin<<<grid_for(n), kThreads, 0, s>>>(f.m64, c.nx, c.ny, c.nz, c.c64.p, c.w64.p, c.s64.p,
+                                                 c.b64.p); note_launch();
+    PBG_CUDA(cudaGetLastError());
+    c.m64 = {c.nx, c.ny, c.nz, c.c64.p, c.w64.p, c.s64.p, c.b64.p};
+    L.push_back(std::move(c));
+  }
+  // dense inverse of the coarsest level
+  const ELevel &cl = L.back();
+  const int n = (int)cl.ncell();
+  ncoarse = n;
+  std::vector<double> hc(n), hw(n), hs(n), hb(n);
+  PBG_CUDA(cudaMemcpyAsync(hc.data(), cl.m64.c, n * 8, cudaMemcpyDeviceToHost, s));
+  PBG_CUDA(cudaMemcpyAsync(hw.data(), cl.m64.w, n * 8, cudaMemcpyDeviceToHost, s));
+  PBG_CUDA(cudaMemcpyAsync(hs.data(), cl.m64.s, n * 8, cudaMemcpyDeviceToHost, s));
+  PBG_CUDA(cudaMemcpyAsync(hb.data(), cl.m64.b, n * 8, cudaMemcpyDeviceToHost, s));
+  PBG_CUDA(cudaStreamSynchronize(s));
+  std::vector<double> D((size_t)n * n, 0.0);
+  const int SI = cl.ny * cl.nz, SJ = cl.nz;
+  for (int i = 0; i < cl.nx; ++i)
+    for (int j = 0; j < cl.ny; ++j)
+      for (int k = 0; k < cl.nz; ++k) {
+        int p = (i * cl.ny + j) * cl.nz + k;
+        D[(size_t)p * n + p] = hc[p];
+        if (i > 0) { D[(size_t)p * n + p - SI] = -hw[p]; D[(size_t)(p - SI) * n + p] = -hw[p]; }
+        if (j > 0) { D[(size_t)p * n + p - SJ] = -hs[p]; D[(size_t)(p - SJ) * n + p] = -hs[p]; }
+        if (k > 0) { D[(size_t)p * n + p - 1] = -hb[p]; D[(size_t)(p - 1) * n + p] = -hb[p]; }
+      }
+  dense_spd_inverse(n, D);
+  Ainv.alloc((size_t)n * n);
+  PBG_CUDA(cudaMemcpy(Ainv.p, D.data(), D.size() * 8, cudaMemcpyHostToDevice));
+  have32 = false;
+  if (mixed) {
+    for (auto &lv : L) {
+      long long m = lv.ncell();
+      lv.c32.alloc(m); lv.w32.alloc(m); lv.s32.alloc(m); lv.b32.alloc(m);
+      const double *src[4] = {lv.m64.c, lv.m64.w, lv.m64.s, lv.m64.b};
+      float *dst[4] = {lv.c32.p, lv.w32.p, lv.s32.p, lv.b32.p};
+      for (int q = 0; q < 4; ++q) { k_to_float<<<grid_for(m), kThreads, 0, s>>>(m, src[q], dst[q]); note_launch(); }
+      lv.m32 = {lv.nx, lv.ny, lv.nz, lv.c32.p, lv.w32.p, lv.s32.p, lv.b32.p};
+    }
+    PBG_CUDA(cudaGetLastError());
+    have32 = true;
+  }
+  if (!hsc) PBG_CUDA(cudaMallocHost((void **)&hsc, 64 * sizeof(double)));
+  if (dsc.n < 8) dsc.alloc(8);
+  PBG_CUDA(cudaStreamSynchronize(s));
+}
+
+template <typename T>
+void Engine::precond(int l, const T *r, T *z, bool dots, const T *u, double *out2, EWork<T> &w,
+                     RedPool &red, const int *stop, cudaStream_t s) {
+  const int last = (int)L.size() - 1;
+  const T om = (T)opt.omega;
+  if (l == last) {
+    k_dense_solve<T><<<(ncoarse * 32 + kThreads - 1) / kThreads, kThreads, 0, s>>>(ncoarse, Ainv.p, r, z, stop); note_launch();
+    if (dots) {  // a level-0 problem small enough to be the coarsest
+      EMat<T> A = mat<T>(l);
+      PBG_CUDA(cudaMemcpyAsync(w.L[l].xa.p, z, sizeof(T) * A.ncell(), cudaMemcpyDeviceToDevice, s));
+      // z = xa + omega (r - A xa)/c would change z; use omega = 0 to keep z and get the dots
+      k_jac_dots<T><<<grid_for(A.ncell()), kThreads, 0, s>>>(A, r, w.L[l].xa.p, z, T(0), u, out2,
+                                                            red.slot_part(0), red.slot_count(0), stop); note_launch();
+    }
+    return;
+  }
+  EMat<T> A = mat<T>(l);
+  const long long N = A.ncell();
+  const int g = grid_for(N);
+  auto &v = w.L[l];
+  const ELevel &H = L[l + 1];
+  k_jac0<T><<<g, kThreads, 0, s>>>(A, r, v.xa.p, om, stop); note_launch();
+  k_jac<T><<<g, kThreads, 0, s>>>(A, r, v.xa.p, v.xb.p, om, stop); note_launch();
+  k_resid_restrict<T><<<grid_for(H.ncell()), kThreads, 0, s>>>(A, r, v.xb.p, H.nx, H.ny, H.nz,
+                                                               w.L[l + 1].b.p, stop); note_launch();
+  if (l + 1 == last) {
+    k_dense_solve<T><<<(ncoarse * 32 + kThreads - 1) / kThreads, kThreads, 0, s>>>(
+        ncoarse, Ainv.p, w.L[l + 1].b.p, w.L[l + 1].x.p, stop); note_launch();
+  } else {
+    kcycle<T>(l + 1, w, red, stop, s);
+  }
+  k_prolong_jac<T><<<g, kThreads, 0, s>>>(A, r, v.xb.p, H.ny, H.nz, w.L[l + 1].x.p, v.xa.p, om, stop); note_launch();
+  if (dots) {
+    k_jac_dots<T><<<g, kThreads, 0, s>>>(A, r, v.xa.p, z, om, u, out2, red.slot_part(0),
+                                         red.slot_count(0), stop); note_launch();
+  } else {
+    k_jac<T><<<g, kThreads, 0, s>>>(A, r, v.xa.p, z, om, stop); note_launch();
+  }
+}
+
+template <typename T>
+void Engine::kcycle(int l, EWork<T> &w, RedPool &red, const int *stop, cudaStream_t s) {
+  EMat<T> A = mat<T>(l);
+  const long long N = A.ncell();
+  const int g = grid_for(N);
+  auto &v = w.L[l];
+  KScal *ks = w.ks.p + l;
+  precond<T>(l, v.b.p, v.z1.p, false, nullptr, nullptr, w, red, stop, s);
+  k_kc_q1<T><<<g, kThreads, 0, s>>>(A, v.z1.p, v.b.p, v.q1.p, ks, red.slot_part(0), red.slot_count(0), stop); note_launch();
+  k_kc_r1<T><<<g, kThreads, 0, s>>>(N, v.b.p, v.q1.p, v.r1.p, ks, stop); note_launch();
+  precond<T>(l, v.r1.p, v.z2.p, false, nullptr, nullptr, w, red, stop, s);
+  k_kc_q2<T><<<g, kThreads, 0, s>>>(A, v.z2.p, v.q1.p, v.r1.p, v.v.p, ks, red.slot_part(0),
+                                    red.slot_count(0), stop); note_launch();
+  k_kc_x<T><<<g, kThreads, 0, s>>>(N, v.z1.p, v.z2.p, v.x.p, ks, stop); note_launch();
+}
+
+// Flexible CG on level 0 for A e = b (e starts at zero); returns iterations.
+template <typename T>
+int Engine::fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red, cudaStream_t s,
+                double *hist, FcgScal *hfs) {
+  EMat<T> A = mat<T>(0);
+  const long long N = A.ncell();
+  const int g = grid_for(N);
+  FcgScal *fs = w.fs.p;
+  const int *stop = &fs->done;
+  PBG_CUDA(cudaMemsetAsync(w.q0.p, 0, sizeof(T) * N, s));
+  k_fcg_init<T><<<g, kThreads, 0, s>>>(N, b, w.x0.p, w.r0.p, fs, tol, maxit, red.slot_part(0),
+                                       red.slot_count(0)); note_launch();
+  PBG_CUDA(cudaGetLastError());
+  int enq = 0, chunk = 4;
+  for (;;) {
+    PBG_CUDA(cudaMemcpyAsync(hfs, fs, sizeof(FcgScal), cudaMemcpyDeviceToHost, s));
+    PBG_CUDA(cudaStreamSynchronize(s));
+    if (hfs->done || enq >= maxit) break;
+    int cnt = chunk;
+    if (enq + cnt > maxit) cnt = maxit - enq;
+    for (int c = 0; c < cnt; ++c) {
+      precond<T>(0, w.r0.p, w.z0.p, true, w.q0.p, &fs->zr, w, red, stop, s);
+      k_fcg_pq<T><<<g, kThreads, 0, s>>>(A, w.z0.p, w.pA.p, w.pB.p, w.q0.p, fs, red.slot_part(0),
+                                         red.slot_count(0)); note_launch();
+      k_fcg_xr<T><<<g, kThreads, 0, s>>>(N, w.x0.p, w.r0.p, w.pA.p, w.pB.p, w.q0.p, fs, hist,
+                                         red.slot_part(0), red.slot_count(0)); note_launch();
+    }
+    PBG_CUDA(cudaGetLastError());
+    enq += cnt;
+    if (chunk < 16) chunk *= 2;
+  }
+  return hfs->iter;
+}
+
+EngineResult Engine::solve_fp64(double *x, const double *b, double tol, int maxit, RedPool &red,
+                                cudaStream_t s, double *hist) {
+  w64.ensure(L);
+  const EMat<double> A = L[0].m64;
+  const long long N = A.ncell();
+  const int g = grid_for(N);
+  FcgScal *hfs = (FcgScal *)hsc;
+  double *rhs = w64.L[0].b.p;
+  EngineResult res{ST_RUNNING, 0, 0, 0, 0.0};
+  k_true_resid<double><<<g, kThreads, 0, s>>>(A, x, b, nullptr, rhs, dsc.p, red.slot_part(0), red.slot_count(0)); note_launch();
+  PBG_CUDA(cudaMemcpyAsync(hsc + 32, dsc.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  PBG_CUDA(cudaStreamSynchronize(s));
+  double rr = hsc[32], bb = hsc[33];
+  if (!(bb > 0.0)) { res.status = ST_INITIAL; res.converged = 1; return res; }
+  double rel = std::sqrt(rr / bb);
+  for (int sweep = 0; sweep < 4 && rel > tol; ++sweep) {
+    double itol = std::fmin(0.9 * tol / rel, 0.5);
+    int its = fcg<double>(w64, rhs, itol, maxit - res.iterations, red, s, hist, hfs);
+    res.iterations += its;
+    res.sweeps++;
+    k_add_corr<double><<<g, kThreads, 0, s>>>(N, x, w64.x0.p); note_launch();
+    k_true_resid<double><<<g, kThreads, 0, s>>>(A, x, b, nullptr, rhs, dsc.p, red.slot_part(0), red.slot_count(0)); note_launch();
+    PBG_CUDA(cudaMemcpyAsync(hsc + 32, dsc.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    PBG_CUDA(cudaStreamSynchronize(s));
+    rel = std::sqrt(hsc[32] / bb);
+    if (hfs->status == ST_NAN || hfs->status == ST_BREAKDOWN) { res.status = hfs->status; break; }
+    if (res.iterations >= maxit) break;
+  }
+  res.relres = rel;
+  if (rel <= tol) { res.converged = 1; res.status = ST_CONVERGED; }
+  else if (res.status == ST_RUNNING) res.status = (rel == rel) ? ST_MAXITER : ST_NAN;
+  return res;
+}
+
+EngineResult Engine::solve_mixed(double *x, const double *b, double tol, double inner_tol,
+                                 int max_sweeps, int inner_maxit, RedPool &red, cudaStream_t s,
+                                 double *hist) {
+  w32.ensure(L);
+  const EMat<double> A = L[0].m64;
+  const long long N = A.ncell();
+  const int g = grid_for(N);
+  FcgScal *hfs = (FcgScal *)hsc;
+  float *rhs = w32.L[0].b.p;
+  EngineResult res{ST_RUNNING, 0, 0, 0, 0.0};
+  k_true_resid<float><<<g, kThreads, 0, s>>>(A, x, b, nullptr, rhs, dsc.p, red.slot_part(0), red.slot_count(0)); note_launch();
+  PBG_CUDA(cudaMemcpyAsync(hsc + 32, dsc.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  PBG_CUDA(cudaStreamSynchronize(s));
+  double rr = hsc[32], bb = hsc[33];
+  if (!(bb > 0.0)) { res.status = ST_INITIAL; res.converged = 1; return res; }
+  double rel = std::sqrt(rr / bb);
+  for (int sweep = 0; sweep < max_sweeps && rel > tol; ++sweep) {
+    // solve no further than the outer target needs in the last sweep
+    double itol = std::fmax(inner_tol, 0.9 * tol / rel);
+    // history slots this sweep may fill: it < kHistMax in k_fcg_xr, so the
+    // offset pointer is passed only while offset + kHistMax stays in bounds
+    double *h = (hist && res.iterations == 0) ? hist : nullptr;
+    int its = fcg<float>(w32, rhs, itol, inner_maxit, red, s, h, hfs);
+    res.iterations += its;
+    res.sweeps++;
+    k_add_corr<float><<<g, kThreads, 0, s>>>(N, x, w32.x0.p); note_launch();
+    k_true_resid<float><<<g, kThreads, 0, s>>>(A, x, b, nullptr, rhs, dsc.p, red.slot_part(0), red.slot_count(0)); note_launch();
+    PBG_CUDA(cudaMemcpyAsync(hsc + 32, dsc.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    PBG_CUDA(cudaStreamSynchronize(s));
+    double nrel = std::sqrt(hsc[32] / bb);
+    if (!(nrel == nrel)) { rel = nrel; res.status = ST_NAN; break; }
+    if (hfs->status == ST_BREAKDOWN && nrel >= rel) { rel = nrel; res.status = ST_BREAKDOWN; break; }
+    rel = nrel;
+  }
+  res.relres = rel;
+  if (rel <= tol) { res.converged = 1; res.status = ST_CONVERGED; }
+  else if (res.status == ST_RUNNING) res.status = ST_MAXITER;
+  return res;
+}
+
+template <typename T>
+static double time_sweeps(const EMat<T> &A, const T *r, T *xa, T *xb, T om, int reps, cudaStream_t s) {
+  cudaEvent_t e0, e1;
+  PBG_CUDA(cudaEventCreate(&e0));
+  PBG_CUDA(cudaEventCreate(&e1));
+  const int g = grid_for(A.ncell());
+  k_jac<T><<<g, kThreads, 0, s>>>(A, r, xa, xb, om, nullptr); note_launch();
+  PBG_CUDA(cudaEventRecord(e0, s));
+  for (int q = 0; q < reps; ++q) {
+    k_jac<T><<<g, kThreads, 0, s>>>(A, r, (q & 1) ? xb : xa, (q & 1) ? xa : xb, om, nullptr); note_launch();
+  }
+  PBG_CUDA(cudaEventRecord(e1, s));
+  PBG_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  PBG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return (double)ms / reps;
+}
+
+double Engine::bench_sweep(int precision, int reps, cudaStream_t s) {
+  if (precision == 0) {
+    w64.ensure(L);
+    PBG_CUDA(cudaMemsetAsync(w64.r0.p, 0, sizeof(double) * L[0].ncell(), s));
+    PBG_CUDA(cudaMemsetAsync(w64.L[0].xa.p, 0, sizeof(double) * L[0].ncell(), s));
+    return time_sweeps<double>(L[0].m64, w64.r0.p, w64.L[0].xa.p, w64.L[0].xb.p, 0.8, reps, s);
+  }
+  w32.ensure(L);
+  PBG_CUDA(cudaMemsetAsync(w32.r0.p, 0, sizeof(float) * L[0].ncell(), s));
+  PBG_CUDA(cudaMemsetAsync(w32.L[0].xa.p, 0, sizeof(float) * L[0].ncell(), s));
+  return time_sweeps<float>(L[0].m32, w32.r0.p, w32.L[0].xa.p, w32.L[0].xb.p, 0.8f, reps, s);
+}
+
+}  // namespace pbg

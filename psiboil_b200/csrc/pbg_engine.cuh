@@ -1,0 +1,99 @@
+// Engine solver: flexible CG + additive-correction K-cycle, FP64 and mixed.
+#pragma once
+
+#include <vector>
+
+#include "pbg_common.cuh"
+#include "pbg_session.h"
+
+namespace pbg {
+
+// Symmetric 7-point operator: c, w, s, b (east/north/top from the next cell).
+template <typename T>
+struct EMat {
+  int nx, ny, nz;
+  const T *c, *w, *s, *b;
+  __host__ __device__ long long ncell() const { return (long long)nx * ny * nz; }
+};
+
+// Scalars of one K-cycle visit on a coarse level.
+struct KScal {
+  double zb, zq, a1, beta, a2, pad[3];
+};
+
+// Scalars of one flexible-CG solve.
+struct FcgScal {
+  double zr, zq;          // written together by k_jac_dots (z.r, z.q_old)
+  double pr, pq, beta, alpha, rr, rr0, tol;
+  int iter, maxit, done, converged, status, pad;
+};
+
+// One aggregation level of the engine hierarchy.
+struct ELevel {
+  int nx = 0, ny = 0, nz = 0;
+  DBuf<double> c64, w64, s64, b64;     // level >= 1 (level 0 borrows the session's)
+  DBuf<float> c32, w32, s32, b32;      // mixed precision copies
+  EMat<double> m64{};
+  EMat<float> m32{};
+  long long ncell() const { return (long long)nx * ny * nz; }
+};
+
+// Per-precision work vectors of every level.
+template <typename T>
+struct EWork {
+  struct Lv {
+    DBuf<T> b, x, z1, z2, q1, r1, v, xa, xb;
+  };
+  std::vector<Lv> L;
+  DBuf<T> x0, r0, z0, pA, pB, q0;      // outer FCG on level 0
+  DBuf<KScal> ks;                      // one per level
+  DBuf<FcgScal> fs;
+  void ensure(const std::vector<ELevel> &lv);
+};
+
+struct EngineOpts {
+  double omega = 0.8;        // damped-Jacobi weight
+  int coarse_max = 512;      // coarsest level size (dense direct solve)
+};
+
+struct EngineResult {
+  int status, converged, iterations, sweeps;
+  double relres;             // FP64 true residual |b - A x| / |b|
+};
+
+class Engine {
+ public:
+  std::vector<ELevel> L;
+  DBuf<double> Ainv;           // dense inverse of the coarsest operator
+  int ncoarse = 0;
+  bool have32 = false;
+  EngineOpts opt;
+  EWork<double> w64;
+  EWork<float> w32;
+  DBuf<double> r64, xtmp, dsc; // FP64 refinement residual, scratch, scalars
+  double *hsc = nullptr;       // pinned host scalars
+
+  ~Engine();
+  void build(const EMat<double> &A0, cudaStream_t s, bool mixed);
+  // Plain FP64: FCG + FP64 K-cycle to |r|/|b| <= tol.
+  EngineResult solve_fp64(double *x, const double *b, double tol, int maxit, RedPool &red,
+                          cudaStream_t s, double *hist);
+  // Mixed: FP32 FCG + FP32 K-cycle to inner_tol inside FP64 refinement.
+  EngineResult solve_mixed(double *x, const double *b, double tol, double inner_tol,
+                           int max_sweeps, int inner_maxit, RedPool &red, cudaStream_t s,
+                           double *hist);
+  int nlevels() const { return (int)L.size(); }
+  // Average duration (ms) of the fine-level smoothing sweep, `reps` launches
+  // back to back between CUDA events on stream s; precision 0 FP64, 1 FP32.
+  double bench_sweep(int precision, int reps, cudaStream_t s);
+
+ private:
+  template <typename T> void precond(int l, const T *r, T *z, bool dots, const T *u, double *out2,
+                                     EWork<T> &w, RedPool &red, const int *stop, cudaStream_t s);
+  template <typename T> void kcycle(int l, EWork<T> &w, RedPool &red, const int *stop, cudaStream_t s);
+  template <typename T> EMat<T> mat(int l) const;
+  template <typename T> int fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red,
+                                cudaStream_t s, double *hist, FcgScal *hfs);
+};
+
+}  // namespace pbg

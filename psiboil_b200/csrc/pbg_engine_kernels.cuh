@@ -1,0 +1,390 @@
+// Engine kernels: flexible CG preconditioned by an additive-correction
+// (piecewise-constant aggregation, Galerkin coarse operator) K-cycle.
+// Templated on the storage/arithmetic type T (double for the plain FP64
+// path, float inside the mixed-precision refinement); every global sum is
+// accumulated in double.
+//
+// Matrices are symmetric 7-point operators stored as c, w, s, b; the east,
+// north and top coefficients of cell p are w, s, b of the next cell in that
+// direction (zero on the last plane).
+#pragma once
+#include "pbg_engine.cuh"
+
+namespace pbg {
+
+template <typename T>
+__device__ __forceinline__ T ax_at(const EMat<T> &A, long long p, Pos q, const T *__restrict__ x) {
+  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
+  T v = A.c[p] * x[p];
+  if (q.i > 0) v -= A.w[p] * x[p - SI];
+  if (q.i < A.nx - 1) v -= A.w[p + SI] * x[p + SI];
+  if (q.j > 0) v -= A.s[p] * x[p - SJ];
+  if (q.j < A.ny - 1) v -= A.s[p + SJ] * x[p + SJ];
+  if (q.k > 0) v -= A.b[p] * x[p - 1];
+  if (q.k < A.nz - 1) v -= A.b[p + 1] * x[p + 1];
+  return v;
+}
+
+// same with x given by a functor (values formed on the fly)
+template <typename T, typename XF>
+__device__ __forceinline__ T ax_f(const EMat<T> &A, long long p, Pos q, XF x) {
+  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
+  T v = A.c[p] * x(p);
+  if (q.i > 0) v -= A.w[p] * x(p - SI);
+  if (q.i < A.nx - 1) v -= A.w[p + SI] * x(p + SI);
+  if (q.j > 0) v -= A.s[p] * x(p - SJ);
+  if (q.j < A.ny - 1) v -= A.s[p + SJ] * x(p + SJ);
+  if (q.k > 0) v -= A.b[p] * x(p - 1);
+  if (q.k < A.nz - 1) v -= A.b[p + 1] * x(p + 1);
+  return v;
+}
+
+#define GRID_LOOP(p, N)                                                          \
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < (N); \
+       p += (long long)gridDim.x * blockDim.x)
+
+// ---------------------------------------------------------------- smoothers
+// x = omega r / c   (first damped-Jacobi sweep from a zero guess)
+template <typename T>
+__global__ void k_jac0(EMat<T> A, const T *__restrict__ r, T *__restrict__ x, T omega,
+                       const int *stop) {
+  if (stop && *stop) return;
+  const long long N = A.ncell();
+  GRID_LOOP(p, N) x[p] = omega * r[p] / A.c[p];
+}
+
+// xo = xi + omega (r - A xi) / c
+template <typename T>
+__global__ void k_jac(EMat<T> A, const T *__restrict__ r, const T *__restrict__ xi,
+                      T *__restrict__ xo, T omega, const int *stop) {
+  if (stop && *stop) return;
+  const long long N = A.ncell();
+  GRID_LOOP(p, N) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    T ax = ax_at(A, p, q, xi);
+    xo[p] = xi[p] + omega * (r[p] - ax) / A.c[p];
+  }
+}
+
+// coarse rhs = block sums of the fine residual r - A x (restriction by the
+// transpose of piecewise-constant prolongation)
+template <typename T>
+__global__ void k_resid_restrict(EMat<T> A, const T *__restrict__ r, const T *__restrict__ x,
+                                 int Hnx, int Hny, int Hnz, T *__restrict__ rH, const int *stop) {
+  if (stop && *stop) return;
+  const int fx = A.nx > 1 ? 2 : 1, fy = A.ny > 1 ? 2 : 1, fz = A.nz > 1 ? 2 : 1;
+  const long long NH = (long long)Hnx * Hny * Hnz;
+  GRID_LOOP(P, NH) {
+    Pos Q = pos_of(P, Hny, Hnz);
+    T sum = 0;
+    for (int a = 0; a < fx; ++a) {
+      int i = Q.i * fx + a;
+      if (i >= A.nx) break;
+      for (int bb = 0; bb < fy; ++bb) {
+        int j = Q.j * fy + bb;
+        if (j >= A.ny) break;
+        for (int cc = 0; cc < fz; ++cc) {
+          int k = Q.k * fz + cc;
+          if (k >= A.nz) break;
+          long long p = ((long long)i * A.ny + j) * A.nz + k;
+          sum += r[p] - ax_at(A, p, Pos{i, j, k}, x);
+        }
+      }
+    }
+    rH[P] = sum;
+  }
+}
+
+// x' = xi + P e (prolongation of the coarse correction), then one sweep:
+// xo = x' + omega (r - A x') / c
+template <typename T>
+__global__ void k_prolong_jac(EMat<T> A, const T *__restrict__ r, const T *__restrict__ xi,
+                              int Hny, int Hnz, const T *__restrict__ eH, T *__restrict__ xo,
+                              T omega, const int *stop) {
+  if (stop && *stop) return;
+  const int fx = A.nx > 1 ? 2 : 1, fy = A.ny > 1 ? 2 : 1, fz = A.nz > 1 ? 2 : 1;
+  const long long N = A.ncell();
+  const long long nynz = (long long)A.ny * A.nz;
+  auto xp = [&](long long s) -> T {
+    int i = (int)(s / nynz);
+    long long rem = s - (long long)i * nynz;
+    int j = (int)(rem / A.nz), k = (int)(rem - (long long)j * A.nz);
+    return xi[s] + eH[((long long)(i / fx) * Hny + j / fy) * Hnz + k / fz];
+  };
+  GRID_LOOP(p, N) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    T xc = xp(p);
+    T ax = ax_f(A, p, q, xp);
+    xo[p] = xc + omega * (r[p] - ax) / A.c[p];
+  }
+}
+
+// Last post-smoothing sweep of a preconditioner application with fused dot
+// products for the Krylov step that consumes z:
+//   z = xi + omega (r - A xi) / c;   d0 = z.r, d1 = z.u (u optional)
+template <typename T>
+__global__ void k_jac_dots(EMat<T> A, const T *__restrict__ r, const T *__restrict__ xi,
+                           T *__restrict__ z, T omega, const T *__restrict__ u, double *out2,
+                           double *part, unsigned *count, const int *stop) {
+  if (stop && *stop) return;
+  const long long N = A.ncell();
+  double v[2] = {0.0, 0.0};
+  GRID_LOOP(p, N) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    T ax = ax_at(A, p, q, xi);
+    T zz = xi[p] + omega * (r[p] - ax) / A.c[p];
+    z[p] = zz;
+    v[0] += (double)zz * (double)r[p];
+    if (u) v[1] += (double)zz * (double)u[p];
+  }
+  double o[2];
+  if (grid_reduce<2>(v, part, count, o)) { out2[0] = o[0]; out2[1] = o[1]; }
+}
+
+
+// ---------------------------------------------------------------- K-cycle
+// Two flexible-CG steps on a coarse level (Notay's K-cycle), with the
+// level's own cycle as the preconditioner:
+//   z1 = M b; q1 = A z1; a1 = z1.b / z1.q1; r1 = b - a1 q1
+//   z2 = M r1; v = A z2; beta = z2.q1 / z1.q1; p2 = z2 - beta z1
+//   a2 = p2.r1 / p2.q2;  x = a1 z1 + a2 p2
+// p2.q2 = z2.v - 2 beta z2.q1 + beta^2 z1.q1 and z1.r1 = z1.b - a1 z1.q1
+// use the symmetry of A, so that q2 is never formed.
+template <typename T>
+__global__ void k_kc_q1(EMat<T> A, const T *__restrict__ z1, const T *__restrict__ b,
+                        T *__restrict__ q1, KScal *ks, double *part, unsigned *count,
+                        const int *stop) {
+  if (stop && *stop) return;
+  const long long N = A.ncell();
+  double v[2] = {0.0, 0.0};
+  GRID_LOOP(p, N) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    T qq = ax_at(A, p, q, z1);
+    q1[p] = qq;
+    v[0] += (double)z1[p] * (double)b[p];
+    v[1] += (double)z1[p] * (double)qq;
+  }
+  double o[2];
+  if (grid_reduce<2>(v, part, count, o)) {
+    ks->zb = o[0];
+    ks->zq = o[1];
+    ks->a1 = (o[1] > 0.0 && o[1] == o[1]) ? o[0] / o[1] : 0.0;
+  }
+}
+
+template <typename T>
+__global__ void k_kc_r1(long long N, const T *__restrict__ b, const T *__restrict__ q1,
+                        T *__restrict__ r1, const KScal *ks, const int *stop) {
+  if (stop && *stop) return;
+  const T a1 = (T)ks->a1;
+  GRID_LOOP(p, N) r1[p] = b[p] - a1 * q1[p];
+}
+
+template <typename T>
+__global__ void k_kc_q2(EMat<T> A, const T *__restrict__ z2, const T *__restrict__ q1,
+                        const T *__restrict__ r1, T *__restrict__ vv, KScal *ks, double *part,
+                        unsigned *count, const int *stop) {
+  if (stop && *stop) return;
+  const long long N = A.ncell();
+  double v[3] = {0.0, 0.0, 0.0};
+  GRID_LOOP(p, N) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    T av = ax_at(A, p, q, z2);
+    vv[p] = av;
+    double zz = (double)z2[p];
+    v[0] += zz * (double)q1[p];
+    v[1] += zz * (double)r1[p];
+    v[2] += zz * (double)av;
+  }
+  double o[3];
+  if (grid_reduce<3>(v, part, count, o)) {
+    const double zq = ks->zq;
+    double beta = zq > 0.0 ? o[0] / zq : 0.0;
+    double z1r1 = ks->zb - ks->a1 * zq;
+    double pr = o[1] - beta * z1r1;
+    double pq = o[2] - 2.0 * beta * o[0] + beta * beta * zq;
+    double a2 = (pq > 0.0 && pq == pq && pr == pr) ? pr / pq : 0.0;
+    ks->beta = beta;
+    ks->a2 = a2;
+  }
+}
+
+template <typename T>
+__global__ void k_kc_x(long long N, const T *__restrict__ z1, const T *__restrict__ z2,
+                       T *__restrict__ x, const KScal *ks, const int *stop) {
+  if (stop && *stop) return;
+  const T c1 = (T)(ks->a1 - ks->a2 * ks->beta), c2 = (T)ks->a2;
+  GRID_LOOP(p, N) x[p] = c1 * z1[p] + c2 * z2[p];
+}
+
+// Coarsest level: z = Ainv r with the dense FP64 inverse (one warp per row).
+template <typename T>
+__global__ void k_dense_solve(int n, const double *__restrict__ Ainv, const T *__restrict__ r,
+                              T *__restrict__ z, const int *stop) {
+  if (stop && *stop) return;
+  const int lane = threadIdx.x & 31;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= n) return;
+  double acc = 0.0;
+  for (int c = lane; c < n; c += 32) acc += Ainv[(long long)row * n + c] * (double)r[c];
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+  if (lane == 0) z[row] = (T)acc;
+}
+
+// ---------------------------------------------------------------- outer FCG
+// Flexible CG with one-vector orthogonalisation (FCG(1)):
+//   beta = z.q_old / p_old.q_old;  p = z - beta p_old;  q = A p
+//   alpha = p.r / p.q;  x += alpha p;  r -= alpha q
+// p.r = z.r - beta p_old.r, with z.r and z.q_old from the last smoothing
+// sweep (k_jac_dots) and p_old.r from the previous update (k_fcg_xr).
+// p is double-buffered by iteration parity; each thread forms p at its
+// neighbours from z and p_old.
+template <typename T>
+__global__ void k_fcg_pq(EMat<T> A, const T *__restrict__ z, T *pA, T *pB, T *__restrict__ qv,
+                         FcgScal *fs, double *part, unsigned *count) {
+  if (fs->done) return;
+  const int it = fs->iter;
+  const T *pold = (it & 1) ? pB : pA;
+  T *pnew = (it & 1) ? pA : pB;
+  const double betad = (it == 0 || !(fs->pq > 0.0)) ? 0.0 : fs->zq / fs->pq;
+  const T beta = (T)betad;
+  auto pv = [&](long long s) -> T { return it == 0 ? z[s] : z[s] - beta * pold[s]; };
+  const long long N = A.ncell();
+  double v[1] = {0.0};
+  GRID_LOOP(p, N) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    T pp = pv(p);
+    T qq = ax_f(A, p, q, pv);
+    pnew[p] = pp;
+    qv[p] = qq;
+    v[0] += (double)pp * (double)qq;
+  }
+  double o[1];
+  if (grid_reduce<1>(v, part, count, o)) {
+    double pr = fs->zr - betad * (it == 0 ? 0.0 : fs->pr);
+    fs->beta = betad;
+    fs->pq = o[0];
+    fs->alpha = (o[0] > 0.0 && o[0] == o[0]) ? pr / o[0] : 0.0;
+    if (!(o[0] > 0.0) || !(o[0] == o[0])) { fs->done = 1; fs->status = ST_BREAKDOWN; }
+  }
+}
+
+template <typename T>
+__global__ void k_fcg_xr(long long N, T *__restrict__ x, T *__restrict__ r, const T *pA,
+                         const T *pB, const T *__restrict__ qv, FcgScal *fs, double *hist,
+                         double *part, unsigned *count) {
+  if (fs->done) return;
+  const int it = fs->iter;
+  const T *pp = (it & 1) ? pA : pB;
+  const T alpha = (T)fs->alpha;
+  double v[2] = {0.0, 0.0};
+  GRID_LOOP(p, N) {
+    T pv = pp[p];
+    x[p] += alpha * pv;
+    T rv = r[p] - alpha * qv[p];
+    r[p] = rv;
+    v[0] += (double)rv * (double)rv;
+    v[1] += (double)pv * (double)rv;
+  }
+  double o[2];
+  if (grid_reduce<2>(v, part, count, o)) {
+    fs->rr = o[0];
+    fs->pr = o[1];
+    double rel = sqrt(o[0] / fs->rr0);
+    if (hist && it < kHistMax) hist[it] = rel;
+    fs->iter = it + 1;
+    if (rel <= fs->tol) { fs->done = 1; fs->converged = 1; fs->status = ST_CONVERGED; }
+    else if (!(rel == rel)) { fs->done = 1; fs->status = ST_NAN; }
+    else if (it + 1 >= fs->maxit) { fs->done = 1; fs->status = ST_MAXITER; }
+  }
+}
+
+// r = b, x = 0 (T), rr0 = |b|^2; fs set up for a new solve
+template <typename T>
+__global__ void k_fcg_init(long long N, const T *__restrict__ b, T *__restrict__ x,
+                           T *__restrict__ r, FcgScal *fs, double tol, int maxit, double *part,
+                           unsigned *count) {
+  double v[1] = {0.0};
+  GRID_LOOP(p, N) {
+    T bv = b[p];
+    r[p] = bv;
+    x[p] = 0;
+    v[0] += (double)bv * (double)bv;
+  }
+  double o[1];
+  if (grid_reduce<1>(v, part, count, o)) {
+    fs->rr0 = o[0];
+    fs->rr = o[0];
+    fs->tol = tol;
+    fs->maxit = maxit;
+    fs->iter = 0;
+    fs->pq = 0.0;
+    fs->pr = 0.0;
+    fs->zq = 0.0;
+    fs->zr = 0.0;
+    fs->converged = 0;
+    if (!(o[0] > 0.0)) { fs->done = 1; fs->converged = 1; fs->status = ST_INITIAL; }
+    else if (maxit <= 0) { fs->done = 1; fs->status = ST_MAXITER; }
+    else { fs->done = 0; fs->status = ST_RUNNING; }
+  }
+}
+
+// ---------------------------------------------------------------- refinement
+// x64 += e (T), elementwise
+template <typename T>
+__global__ void k_add_corr(long long N, double *__restrict__ x, const T *__restrict__ e) {
+  GRID_LOOP(p, N) x[p] += (double)e[p];
+}
+
+// r = b - A x in FP64, r32 = (T) r, out[0] = |r|^2, out[1] = |b|^2
+template <typename T>
+__global__ void k_true_resid(EMat<double> A, const double *__restrict__ x, const double *__restrict__ b,
+                             double *__restrict__ r, T *__restrict__ rT, double *out, double *part,
+                             unsigned *count) {
+  const long long N = A.ncell();
+  double v[2] = {0.0, 0.0};
+  GRID_LOOP(p, N) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    double rv = b[p] - ax_at(A, p, q, x);
+    if (r) r[p] = rv;
+    if (rT) rT[p] = (T)rv;
+    v[0] += rv * rv;
+    v[1] += b[p] * b[p];
+  }
+  double o[2];
+  if (grid_reduce<2>(v, part, count, o)) { out[0] = o[0]; out[1] = o[1]; }
+}
+
+// ---------------------------------------------------------------- hierarchy
+// Galerkin coarse operator P^T A P for piecewise-constant aggregation by 2
+// in every direction with more than one cell (last block partial on odd
+// sizes): c_H = sum c - 2 sum(internal couplings), w_H / s_H / b_H = sum of
+// the couplings across the block's west / south / bottom face.
+__global__ void k_galerkin(EMat<double> A, int Hnx, int Hny, int Hnz, double *__restrict__ cH,
+                           double *__restrict__ wH, double *__restrict__ sH, double *__restrict__ bH) {
+  const int fx = A.nx > 1 ? 2 : 1, fy = A.ny > 1 ? 2 : 1, fz = A.nz > 1 ? 2 : 1;
+  const long long NH = (long long)Hnx * Hny * Hnz;
+  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
+  GRID_LOOP(P, NH) {
+    Pos Q = pos_of(P, Hny, Hnz);
+    double c = 0.0, w = 0.0, s = 0.0, b = 0.0;
+    const int i0 = Q.i * fx, j0 = Q.j * fy, k0 = Q.k * fz;
+    for (int a = 0; a < fx && i0 + a < A.nx; ++a)
+      for (int bb = 0; bb < fy && j0 + bb < A.ny; ++bb)
+        for (int cc = 0; cc < fz && k0 + cc < A.nz; ++cc) {
+          const long long p = ((long long)(i0 + a) * A.ny + (j0 + bb)) * A.nz + (k0 + cc);
+          c += A.c[p];
+          if (a == 0) w += A.w[p]; else c -= 2.0 * A.w[p];
+          if (bb == 0) s += A.s[p]; else c -= 2.0 * A.s[p];
+          if (cc == 0) b += A.b[p]; else c -= 2.0 * A.b[p];
+        }
+    (void)SI; (void)SJ;
+    cH[P] = c; wH[P] = w; sH[P] = s; bH[P] = b;
+  }
+}
+
+__global__ void k_to_float(long long N, const double *__restrict__ a, float *__restrict__ o) {
+  GRID_LOOP(p, N) o[p] = (float)a[p];
+}
+
+}  // namespace pbg

@@ -1,0 +1,922 @@
+// Reference-parity kernels: the reference's per-element arithmetic, in the
+// reference's operation order, with explicit round-to-nearest intrinsics so
+// that the compiler cannot contract a multiply and an add into one FMA.
+// Only the order of the global sums differs from the reference (a tree
+// instead of a sequential i,j,k sum).
+#include "pbg_ref_kernels.cuh"
+
+namespace pbg {
+
+// ---------------------------------------------------------------------------
+// Stencil helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double ld0(const double *x, long long p, bool ok) {
+  return ok ? x[p] : 0.0;
+}
+
+// y = A x at cell p, order of Scalar::operator=(const A_x&)
+// (Src/Field/Scalar/scalar_operators.cpp:49-72):
+//   y = c x;  y -= (w xw + e xe);  y -= (s xs + n xn);  y -= (b xb + t xt)
+template <typename XF>
+__device__ __forceinline__ double ref_ax(const MatView<double> &A, long long p, Pos q, XF xv) {
+  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
+  Nb<double> a = coeffs(A, p, q);
+  double xw = q.i > 0 ? xv(p - SI) : 0.0, xe = q.i < A.nx - 1 ? xv(p + SI) : 0.0;
+  double xs = q.j > 0 ? xv(p - SJ) : 0.0, xn = q.j < A.ny - 1 ? xv(p + SJ) : 0.0;
+  double xb = q.k > 0 ? xv(p - 1) : 0.0, xt = q.k < A.nz - 1 ? xv(p + 1) : 0.0;
+  double v = __dmul_rn(A.c[p], xv(p));
+  v = __dsub_rn(v, __dadd_rn(__dmul_rn(a.w, xw), __dmul_rn(a.e, xe)));
+  v = __dsub_rn(v, __dadd_rn(__dmul_rn(a.s, xs), __dmul_rn(a.n, xn)));
+  v = __dsub_rn(v, __dadd_rn(__dmul_rn(a.b, xb), __dmul_rn(a.t, xt)));
+  return v;
+}
+
+// r = b - A x at cell p, order of Scalar::operator=(const y_m_A_x&)
+// (scalar_operators.cpp:22-46):
+//   r = b - c x;  r += w xw + e xe;  r += s xs + n xn;  r += b xb + t xt
+__device__ __forceinline__ double ref_bmax(const MatView<double> &A, long long p, Pos q,
+                                           const double *x, double bp) {
+  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
+  Nb<double> a = coeffs(A, p, q);
+  double xw = ld0(x, p - SI, q.i > 0), xe = ld0(x, p + SI, q.i < A.nx - 1);
+  double xs = ld0(x, p - SJ, q.j > 0), xn = ld0(x, p + SJ, q.j < A.ny - 1);
+  double xb = ld0(x, p - 1, q.k > 0), xt = ld0(x, p + 1, q.k < A.nz - 1);
+  double v = __dsub_rn(bp, __dmul_rn(A.c[p], x[p]));
+  v = __dadd_rn(v, __dadd_rn(__dmul_rn(a.w, xw), __dmul_rn(a.e, xe)));
+  v = __dadd_rn(v, __dadd_rn(__dmul_rn(a.s, xs), __dmul_rn(a.n, xn)));
+  v = __dadd_rn(v, __dadd_rn(__dmul_rn(a.b, xb), __dmul_rn(a.t, xt)));
+  return v;
+}
+
+// element of Scalar::dot_voldiv_avg: x*y/dV/dV (scalar.h:317-326)
+__device__ __forceinline__ double voldiv(double x, double y, double dV) {
+  return __ddiv_rn(__ddiv_rn(__dmul_rn(x, y), dV), dV);
+}
+
+// res = sqrt(d/N/N)/scale (cg.cpp:68 and :115)
+__device__ __forceinline__ double res_of(double d, const KrylovState *st) {
+  return __ddiv_rn(__dsqrt_rn(__ddiv_rn(__ddiv_rn(d, st->ncell), st->ncell)), st->scale);
+}
+
+// ---------------------------------------------------------------------------
+// Plain operators (parity tests and building blocks)
+// ---------------------------------------------------------------------------
+__global__ void k_spmv_ref(MatView<double> A, const double *__restrict__ x, double *__restrict__ y) {
+  const long long N = A.ncell();
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    y[p] = ref_ax(A, p, q, [&](long long r) { return x[r]; });
+  }
+}
+
+__global__ void k_resid_ref(MatView<double> A, const double *__restrict__ x,
+                            const double *__restrict__ b, double *__restrict__ r) {
+  const long long N = A.ncell();
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    r[p] = ref_bmax(A, p, q, x, b[p]);
+  }
+}
+
+// out[0] = sum x*y, out[1] = sum x*y/dV/dV (deterministic tree order)
+__global__ void k_dot2(long long N, const double *__restrict__ x, const double *__restrict__ y,
+                       double dV, double *part, unsigned *count, double *out) {
+  double v[2] = {0.0, 0.0};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    v[0] += __dmul_rn(x[p], y[p]);
+    v[1] += voldiv(x[p], y[p], dV);
+  }
+  double o[2];
+  if (grid_reduce<2>(v, part, count, o)) { out[0] = o[0]; out[1] = o[1]; }
+}
+
+// ---------------------------------------------------------------------------
+// CG with the diagonal preconditioner, CG::solve (cg.cpp:10-182),
+// Diagonal::form/solve (preconditioner_form.cpp:4-13,
+// preconditioner_solve.cpp:4-11): Mc = 1/c, z = r*Mc.
+//
+// Per iteration two kernels:
+//   k_cg_pq : p = z + beta p (p = z at i = 0), q = A p, pq = p.q, alfa
+//   k_cg_xr : x += alfa p, r -= alfa q, res, convergence, next rho = r.z
+// p is double-buffered (read p_old, write p_new) so that each thread can
+// form p at its six neighbours from z and p_old without a grid barrier.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double mc_of(const double *c, long long p) { return __ddiv_rn(1.0, c[p]); }
+
+__device__ void stale_init_dev(KrylovState *st, double res0) {
+  int n = st->stalecount > kStaleMax ? kStaleMax : st->stalecount;
+  for (int q = 0; q < n; ++q) st->stale[q] = 1.0e24;  // boil::unreal
+  if (n > 0) st->stale[n - 1] = res0;
+}
+
+// true when stale (cg.cpp:138-160); otherwise rotates the window
+__device__ bool stale_step_dev(KrylovState *st, double res) {
+  int n = st->stalecount > kStaleMax ? kStaleMax : st->stalecount;
+  if (n <= 0) return false;
+  bool stale = true;
+  for (int q = 0; q < n; ++q)
+    if (res < st->stale[q]) { stale = false; break; }
+  if (stale) return true;
+  for (int q = 0; q < n - 1; ++q) st->stale[q] = st->stale[q + 1];
+  st->stale[n - 1] = res;
+  return false;
+}
+
+__global__ void k_cg_init(MatView<double> A, const double *__restrict__ x,
+                          const double *__restrict__ b, double *__restrict__ r,
+                          KrylovState *st, double *part, unsigned *count) {
+  const long long N = A.ncell();
+  const double dV = st->dV;
+  double v[2] = {0.0, 0.0};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    double rv = ref_bmax(A, p, q, x, b[p]);
+    r[p] = rv;
+    v[0] += voldiv(rv, rv, dV);
+    v[1] += __dmul_rn(rv, __dmul_rn(rv, mc_of(A.c, p)));
+  }
+  double o[2];
+  if (grid_reduce<2>(v, part, count, o)) {
+    double res = res_of(o[0], st);
+    st->res0 = res;
+    st->res = res;
+    st->rho = o[1];
+    st->iter = 0;
+    st->iterations = 0;
+    st->converged = 0;
+    st->pending_x = 0;
+    stale_init_dev(st, res);
+    if (res < st->res_tol) {  // cg.cpp:83
+      st->done = 1;
+      st->converged = 1;
+      st->status = ST_INITIAL;
+    } else if (st->maxit <= 0) {
+      st->done = 1;
+      st->status = ST_MAXITER;
+    } else {
+      st->done = 0;
+      st->status = ST_RUNNING;
+    }
+  }
+}
+
+__global__ void k_cg_pq(MatView<double> A, const double *__restrict__ r, double *pA, double *pB,
+                        double *__restrict__ qv, KrylovState *st, double *part, unsigned *count) {
+  if (st->done) return;
+  const int it = st->iter;
+  const double *pold = (it & 1) ? pB : pA;
+  double *pnew = (it & 1) ? pA : pB;
+  const double beta = it == 0 ? 0.0 : __ddiv_rn(st->rho, st->rho_old);
+  const long long N = A.ncell();
+  auto pv = [&](long long s) {
+    double z = __dmul_rn(r[s], mc_of(A.c, s));
+    return it == 0 ? z : __dadd_rn(z, __dmul_rn(beta, pold[s]));
+  };
+  double v[1] = {0.0};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    double pp = pv(p);
+    double qq = ref_ax(A, p, q, pv);
+    pnew[p] = pp;
+    qv[p] = qq;
+    v[0] += __dmul_rn(pp, qq);
+  }
+  double o[1];
+  if (grid_reduce<1>(v, part, count, o)) {
+    st->beta = beta;
+    st->pq = o[0];
+    st->alfa = __ddiv_rn(st->rho, o[0]);
+  }
+}
+
+__global__ void k_cg_xr(long long N, const double *__restrict__ c, double *__restrict__ x,
+                        double *__restrict__ r, const double *pA, const double *pB,
+                        const double *__restrict__ qv, KrylovState *st, double *hist,
+                        double *part, unsigned *count) {
+  if (st->done) return;
+  const int it = st->iter;
+  const double *p_ = (it & 1) ? pA : pB;  // the buffer k_cg_pq wrote
+  const double alfa = st->alfa, dV = st->dV;
+  double v[2] = {0.0, 0.0};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    x[p] = __dadd_rn(x[p], __dmul_rn(alfa, p_[p]));
+    double rv = __dsub_rn(r[p], __dmul_rn(alfa, qv[p]));
+    r[p] = rv;
+    v[0] += voldiv(rv, rv, dV);
+    v[1] += __dmul_rn(rv, __dmul_rn(rv, mc_of(c, p)));
+  }
+  double o[2];
+  if (grid_reduce<2>(v, part, count, o)) {
+    double res = res_of(o[0], st);
+    st->res = res;
+    if (hist && it < st->hist_cap) hist[it] = res;
+    const bool minok = it >= st->mini - 1;
+    if ((res < st->res_tol && minok) || (res < st->res0 * st->res_rat && minok)) {
+      st->done = 1; st->converged = 1; st->status = ST_CONVERGED; st->iterations = it + 1;
+    } else if (stale_step_dev(st, res)) {
+      st->done = 1; st->status = ST_STALE; st->iterations = it + 1;
+    } else if (!(res == res)) {
+      st->done = 1; st->status = ST_NAN; st->iterations = it + 1;
+    } else {
+      st->rho_old = st->rho;
+      st->rho = o[1];
+      st->iter = it + 1;
+      st->iterations = it + 1;
+      if (it + 1 >= st->maxit) { st->done = 1; st->status = ST_MAXITER; }
+    }
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// BiCGStab with the diagonal preconditioner, BiCGS::solve (bicgs.cpp:9-229).
+// One iteration:
+//   k_bi_rho   rho = r~.r; breakdown test; beta                     (:91-99)
+//   k_bi_p     p = r (i=0) | p = r + beta p; p -= (beta omega) v; p^ = p Mc
+//   k_bi_v     v = A p^; r~.v; alfa                                 (:124-133)
+//   k_bi_s     s = r - alfa v; s.s; early exit test; s^ = s Mc      (:137-159)
+//   k_bi_t     t = A s^; t.s, t.t; omega                           (:163-175)
+//   k_bi_xr    x += alfa p^; x += omega s^; r = s - omega t; res; tests
+// The early exit of :146-150 (x += alfa p^, break) is carried by
+// pending_x, which k_bi_xr applies and clears.
+// ---------------------------------------------------------------------------
+__global__ void k_bi_init(MatView<double> A, const double *__restrict__ x, const double *__restrict__ b,
+                          double *__restrict__ r, double *__restrict__ rt, KrylovState *st,
+                          double *part, unsigned *count) {
+  const long long N = A.ncell();
+  const double dV = st->dV;
+  double v[1] = {0.0};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    double rv = ref_bmax(A, p, q, x, b[p]);
+    r[p] = rv;
+    rt[p] = rv;
+    v[0] += voldiv(rv, rv, dV);
+  }
+  double o[1];
+  if (grid_reduce<1>(v, part, count, o)) {
+    double res = res_of(o[0], st);
+    st->res0 = res;
+    st->res = res;
+    st->iter = 0;
+    st->iterations = 0;
+    st->converged = 0;
+    st->pending_x = 0;
+    stale_init_dev(st, res);
+    if (res < st->res_tol) {
+      st->done = 1; st->converged = 1; st->status = ST_INITIAL;
+    } else if (st->maxit <= 0) {
+      st->done = 1; st->status = ST_MAXITER;
+    } else {
+      st->done = 0; st->status = ST_RUNNING;
+    }
+  }
+}
+
+__global__ void k_bi_rho(long long N, const double *__restrict__ rt, const double *__restrict__ r,
+                         KrylovState *st, double *part, unsigned *count) {
+  if (st->done) return;
+  double v[1] = {0.0};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x)
+    v[0] += __dmul_rn(rt[p], r[p]);
+  double o[1];
+  if (grid_reduce<1>(v, part, count, o)) {
+    const int it = st->iter;
+    st->rho = o[0];
+    if (__dsqrt_rn(fabs(o[0])) < st->res_tol) {
+      st->done = 1; st->status = ST_BREAKDOWN; st->iterations = it + 1;
+    } else if (it > 0) {
+      st->beta = __dmul_rn(__ddiv_rn(o[0], st->rho_old), __ddiv_rn(st->alfa, st->omega));
+    }
+  }
+}
+
+__global__ void k_bi_p(long long N, const double *__restrict__ c, const double *__restrict__ r,
+                       double *__restrict__ pv, const double *__restrict__ v, double *__restrict__ ph,
+                       const KrylovState *st) {
+  if (st->done) return;
+  const int it = st->iter;
+  const double beta = st->beta, bo = __dmul_rn(st->beta, st->omega);
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    double pp;
+    if (it == 0) pp = r[p];
+    else {
+      pp = __dadd_rn(r[p], __dmul_rn(beta, pv[p]));
+      pp = __dsub_rn(pp, __dmul_rn(bo, v[p]));
+    }
+    pv[p] = pp;
+    ph[p] = __dmul_rn(pp, mc_of(c, p));
+  }
+}
+
+// y = A x and up to two dots with y: mode 0 -> rt.y (alfa), mode 1 -> y.s, y.y (omega)
+__global__ void k_bi_spmv(MatView<double> A, const double *__restrict__ x, double *__restrict__ y,
+                          const double *__restrict__ o1, int mode, KrylovState *st,
+                          double *part, unsigned *count) {
+  if (st->done) return;
+  const long long N = A.ncell();
+  double v[2] = {0.0, 0.0};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    double yv = ref_ax(A, p, q, [&](long long s) { return x[s]; });
+    y[p] = yv;
+    if (mode == 0) v[0] += __dmul_rn(o1[p], yv);
+    else { v[0] += __dmul_rn(yv, o1[p]); v[1] += __dmul_rn(yv, yv); }
+  }
+  double o[2];
+  if (grid_reduce<2>(v, part, count, o)) {
+    if (mode == 0) st->alfa = __ddiv_rn(st->rho, o[0]);
+    else { st->aux0 = o[0]; st->aux1 = o[1]; st->omega = __ddiv_rn(o[0], o[1]); }
+  }
+}
+
+__global__ void k_bi_s(long long N, const double *__restrict__ c, const double *__restrict__ r,
+                       const double *__restrict__ v, double *__restrict__ s, double *__restrict__ sh,
+                       KrylovState *st, double *part, unsigned *count) {
+  if (st->done) return;
+  const double alfa = st->alfa;
+  double a[1] = {0.0};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    double sv = __dsub_rn(r[p], __dmul_rn(alfa, v[p]));
+    s[p] = sv;
+    sh[p] = __dmul_rn(sv, mc_of(c, p));
+    a[0] += __dmul_rn(sv, sv);
+  }
+  double o[1];
+  if (grid_reduce<1>(a, part, count, o)) {
+    if (__dsqrt_rn(o[0]) < st->res_tol) {
+      st->pending_x = 1;  // x += alfa p^, then stop (bicgs.cpp:146-150)
+      st->done = 1; st->status = ST_BREAKDOWN; st->iterations = st->iter + 1;
+    }
+  }
+}
+
+__global__ void k_bi_xr(long long N, double *__restrict__ x, double *__restrict__ r,
+                        const double *__restrict__ ph, const double *__restrict__ sh,
+                        const double *__restrict__ s, const double *__restrict__ t,
+                        KrylovState *st, double *hist, double *part, unsigned *count) {
+  const int pend = st->pending_x;
+  if (st->done && !pend) return;
+  const double alfa = st->alfa, omega = st->omega, dV = st->dV;
+  double v[1] = {0.0};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    double xv = __dadd_rn(x[p], __dmul_rn(alfa, ph[p]));
+    if (pend) { x[p] = xv; continue; }
+    x[p] = __dadd_rn(xv, __dmul_rn(omega, sh[p]));
+    double rv = __dsub_rn(s[p], __dmul_rn(omega, t[p]));
+    r[p] = rv;
+    v[0] += voldiv(rv, rv, dV);
+  }
+  double o[1];
+  if (grid_reduce<1>(v, part, count, o)) {
+    if (pend) { st->pending_x = 0; return; }
+    const int it = st->iter;
+    double res = res_of(o[0], st);
+    st->res = res;
+    if (hist && it < st->hist_cap) hist[it] = res;
+    const bool minok = it >= st->mini - 1;
+    if ((res < st->res_tol && minok) || (res < st->res0 * st->res_rat && minok)) {
+      st->done = 1; st->converged = 1; st->status = ST_CONVERGED; st->iterations = it + 1;
+    } else if (omega >= -st->res_tol && omega <= st->res_tol) {  // bicgs.cpp:189
+      st->done = 1; st->status = ST_BREAKDOWN; st->iterations = it + 1;
+    } else if (stale_step_dev(st, res)) {
+      st->done = 1; st->status = ST_STALE; st->iterations = it + 1;
+    } else if (!(res == res)) {
+      st->done = 1; st->status = ST_NAN; st->iterations = it + 1;
+    } else {
+      st->rho_old = st->rho;
+      st->iter = it + 1;
+      st->iterations = it + 1;
+      if (it + 1 >= st->maxit) { st->done = 1; st->status = ST_MAXITER; }
+    }
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Additive-correction multigrid, reference form (Src/Solver/Additive).
+// Coarse cell (I,J,K) covers fine cells I*CI..I*CI+CI-1 (likewise J, K),
+// the index map of additive_coarsen_system.cpp:30-36.
+// ---------------------------------------------------------------------------
+struct FineCell {
+  const MatView<double> &A;
+  __device__ FineCell(const MatView<double> &a) : A(a) {}
+  __device__ long long at(int i, int j, int k) const {
+    return ((long long)i * A.ny + j) * A.nz + k;
+  }
+  __device__ double c(int i, int j, int k) const { return A.c[at(i, j, k)]; }
+  __device__ double w(int i, int j, int k) const { return A.w[at(i, j, k)]; }
+  __device__ double s(int i, int j, int k) const { return A.s[at(i, j, k)]; }
+  __device__ double b(int i, int j, int k) const { return A.b[at(i, j, k)]; }
+  __device__ double e(int i, int j, int k) const {
+    return A.e ? A.e[at(i, j, k)] : (i < A.nx - 1 ? A.w[at(i + 1, j, k)] : 0.0);
+  }
+  __device__ double n(int i, int j, int k) const {
+    return A.n ? A.n[at(i, j, k)] : (j < A.ny - 1 ? A.s[at(i, j + 1, k)] : 0.0);
+  }
+  __device__ double t(int i, int j, int k) const {
+    return A.t ? A.t[at(i, j, k)] : (k < A.nz - 1 ? A.b[at(i, j, k + 1)] : 0.0);
+  }
+};
+
+struct CoarseOut { int nx, ny, nz; double *c, *w, *e, *s, *n, *b, *t; };
+
+// AC::coarsen_system (additive_coarsen_system.cpp:4-140), one thread per
+// coarse cell, the reference's summation order.
+__global__ void k_ac_coarsen(MatView<double> A, CoarseOut H, int CI, int CJ, int CK) {
+  FineCell f(A);
+  const long long NH = (long long)H.nx * H.ny * H.nz;
+  for (long long P = blockIdx.x * (long long)blockDim.x + threadIdx.x; P < NH;
+       P += (long long)gridDim.x * blockDim.x) {
+    Pos Q = pos_of(P, H.ny, H.nz);
+    const int i0 = Q.i * CI, j0 = Q.j * CJ, k0 = Q.k * CK;
+    double c = 0.0;
+    for (int i = 0; i < CI; ++i)
+      for (int j = 0; j < CJ; ++j)
+        for (int k = 0; k < CK; ++k) c = __dadd_rn(c, f.c(i0 + i, j0 + j, k0 + k));
+    for (int j = 0; j < CJ; ++j)
+      for (int k = 0; k < CK; ++k) {
+        for (int i = 0; i < CI - 1; ++i) c = __dsub_rn(c, f.e(i0 + i, j0 + j, k0 + k));
+        for (int i = 1; i < CI; ++i) c = __dsub_rn(c, f.w(i0 + i, j0 + j, k0 + k));
+      }
+    double e = 0.0, w = 0.0;
+    for (int j = 0; j < CJ; ++j)
+      for (int k = 0; k < CK; ++k) {
+        e = __dadd_rn(e, f.e(i0 + CI - 1, j0 + j, k0 + k));
+        w = __dadd_rn(w, f.w(i0, j0 + j, k0 + k));
+      }
+    for (int i = 0; i < CI; ++i)
+      for (int k = 0; k < CK; ++k) {
+        for (int j = 0; j < CJ - 1; ++j) c = __dsub_rn(c, f.n(i0 + i, j0 + j, k0 + k));
+        for (int j = 1; j < CJ; ++j) c = __dsub_rn(c, f.s(i0 + i, j0 + j, k0 + k));
+      }
+    double n = 0.0, s = 0.0;
+    for (int i = 0; i < CI; ++i)
+      for (int k = 0; k < CK; ++k) {
+        n = __dadd_rn(n, f.n(i0 + i, j0 + CJ - 1, k0 + k));
+        s = __dadd_rn(s, f.s(i0 + i, j0, k0 + k));
+      }
+    for (int i = 0; i < CI; ++i)
+      for (int j = 0; j < CJ; ++j) {
+        for (int k = 0; k < CK - 1; ++k) c = __dsub_rn(c, f.t(i0 + i, j0 + j, k0 + k));
+        for (int k = 1; k < CK; ++k) c = __dsub_rn(c, f.b(i0 + i, j0 + j, k0 + k));
+      }
+    double t = 0.0, b = 0.0;
+    for (int i = 0; i < CI; ++i)
+      for (int j = 0; j < CJ; ++j) {
+        t = __dadd_rn(t, f.t(i0 + i, j0 + j, k0 + CK - 1));
+        b = __dadd_rn(b, f.b(i0 + i, j0 + j, k0));
+      }
+    H.c[P] = c; H.w[P] = w; H.e[P] = e; H.s[P] = s; H.n[P] = n; H.b[P] = b; H.t[P] = t;
+  }
+}
+
+// AC::coarsen_flag (additive_coarsen_flag.cpp:4-41): OR over the block
+__global__ void k_ac_flag(int fny, int fnz, const uint8_t *__restrict__ af, int Hnx, int Hny, int Hnz,
+                          uint8_t *__restrict__ aH, int CI, int CJ, int CK) {
+  const long long NH = (long long)Hnx * Hny * Hnz;
+  for (long long P = blockIdx.x * (long long)blockDim.x + threadIdx.x; P < NH;
+       P += (long long)gridDim.x * blockDim.x) {
+    Pos Q = pos_of(P, Hny, Hnz);
+    uint8_t v = 0;
+    for (int i = 0; i < CI; ++i)
+      for (int j = 0; j < CJ; ++j)
+        for (int k = 0; k < CK; ++k)
+          v |= af[((long long)(Q.i * CI + i) * fny + (Q.j * CJ + j)) * fnz + (Q.k * CK + k)];
+    aH[P] = v;
+  }
+}
+
+// AC::restriction (additive_restriction.cpp:12-177): coarse rhs = block sum
+// of the fine residual in the reference's order (D = c minus the block's
+// internal couplings, taken e, w, n, s, t, b), zero on inactive coarse cells;
+// the block also sums the active values and counts them for the zero-mean
+// step (:151-174), finished by k_ac_submean.
+__global__ void k_ac_restrict(MatView<double> A, const double *__restrict__ phi,
+                              const double *__restrict__ fnew, int Hnx, int Hny, int Hnz,
+                              double *__restrict__ fH, const uint8_t *__restrict__ aH,
+                              int CI, int CJ, int CK, double *mean_out, double *part,
+                              unsigned *count) {
+  FineCell f(A);
+  auto ph = [&](int i, int j, int k) -> double {
+    return (i < 0 || i >= A.nx || j < 0 || j >= A.ny || k < 0 || k >= A.nz) ? 0.0 : phi[f.at(i, j, k)];
+  };
+  const long long NH = (long long)Hnx * Hny * Hnz;
+  double v[2] = {0.0, 0.0};
+  for (long long P = blockIdx.x * (long long)blockDim.x + threadIdx.x; P < NH;
+       P += (long long)gridDim.x * blockDim.x) {
+    Pos Q = pos_of(P, Hny, Hnz);
+    const int i0 = Q.i * CI, j0 = Q.j * CJ, k0 = Q.k * CK;
+    double F = 0.0;
+    for (int i = 0; i < CI; ++i)
+      for (int j = 0; j < CJ; ++j)
+        for (int k = 0; k < CK; ++k) F = __dadd_rn(F, fnew[f.at(i0 + i, j0 + j, k0 + k)]);
+    for (int j = 0; j < CJ; ++j)
+      for (int k = 0; k < CK; ++k) {
+        F = __dadd_rn(F, __dmul_rn(f.e(i0 + CI - 1, j0 + j, k0 + k), ph(i0 + CI, j0 + j, k0 + k)));
+        F = __dadd_rn(F, __dmul_rn(f.w(i0, j0 + j, k0 + k), ph(i0 - 1, j0 + j, k0 + k)));
+      }
+    for (int i = 0; i < CI; ++i)
+      for (int k = 0; k < CK; ++k) {
+        F = __dadd_rn(F, __dmul_rn(f.n(i0 + i, j0 + CJ - 1, k0 + k), ph(i0 + i, j0 + CJ, k0 + k)));
+        F = __dadd_rn(F, __dmul_rn(f.s(i0 + i, j0, k0 + k), ph(i0 + i, j0 - 1, k0 + k)));
+      }
+    for (int i = 0; i < CI; ++i)
+      for (int j = 0; j < CJ; ++j) {
+        F = __dadd_rn(F, __dmul_rn(f.t(i0 + i, j0 + j, k0 + CK - 1), ph(i0 + i, j0 + j, k0 + CK)));
+        F = __dadd_rn(F, __dmul_rn(f.b(i0 + i, j0 + j, k0), ph(i0 + i, j0 + j, k0 - 1)));
+      }
+    for (int i = 0; i < CI; ++i)
+      for (int j = 0; j < CJ; ++j)
+        for (int k = 0; k < CK; ++k) {
+          const int a = i0 + i, bb = j0 + j, cc = k0 + k;
+          double D = f.c(a, bb, cc);
+          if (i < CI - 1) D = __dsub_rn(D, f.e(a, bb, cc));
+          if (i > 0) D = __dsub_rn(D, f.w(a, bb, cc));
+          if (j < CJ - 1) D = __dsub_rn(D, f.n(a, bb, cc));
+          if (j > 0) D = __dsub_rn(D, f.s(a, bb, cc));
+          if (k < CK - 1) D = __dsub_rn(D, f.t(a, bb, cc));
+          if (k > 0) D = __dsub_rn(D, f.b(a, bb, cc));
+          F = __dsub_rn(F, __dmul_rn(D, phi[f.at(a, bb, cc)]));
+        }
+    if (!aH[P]) F = 0.0;
+    fH[P] = F;
+    if (aH[P]) { v[0] += F; v[1] += 1.0; }
+  }
+  double o[2];
+  if (grid_reduce<2>(v, part, count, o)) *mean_out = __ddiv_rn(o[0], o[1]);
+}
+
+__global__ void k_ac_submean(long long NH, double *__restrict__ fH, const uint8_t *__restrict__ aH,
+                             const double *mean) {
+  const double m = *mean;
+  for (long long P = blockIdx.x * (long long)blockDim.x + threadIdx.x; P < NH;
+       P += (long long)gridDim.x * blockDim.x)
+    if (aH[P]) fH[P] = __dsub_rn(fH[P], m);
+}
+
+// AC::interpolation (additive_interpolation.cpp:12-64): h.phi += H.phi
+__global__ void k_ac_interp(int nx, int ny, int nz, double *__restrict__ phi, int Hny, int Hnz,
+                            const double *__restrict__ phiH, int CI, int CJ, int CK) {
+  const long long N = (long long)nx * ny * nz;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    Pos q = pos_of(p, ny, nz);
+    long long P = ((long long)(q.i / CI) * Hny + q.j / CJ) * Hnz + q.k / CK;
+    phi[p] = __dadd_rn(phi[p], phiH[P]);
+  }
+}
+
+// AC::residual (additive_residual.cpp:4-30) with dt = 1: res = b - A phi,
+// out[0] = sqrt(dot_voldiv_avg(res,res)), linf via an order-free max of
+// |res/dV| (non-negative doubles order like their bit patterns).
+__global__ void k_ac_resnorm(MatView<double> A, const double *__restrict__ phi,
+                             const double *__restrict__ fnew, double dV, double *out,
+                             unsigned long long *linf_bits, double *part, unsigned *count) {
+  const long long N = A.ncell();
+  double v[1] = {0.0};
+  double mx = 0.0;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    double rv = ref_bmax(A, p, q, phi, fnew[p]);
+    v[0] += voldiv(rv, rv, dV);
+    mx = fmax(mx, fabs(__ddiv_rn(rv, dV)));
+  }
+  for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(linf_bits, (unsigned long long)__double_as_longlong(mx));
+  double o[1];
+  if (grid_reduce<1>(v, part, count, o)) {
+    double n = (double)N;
+    out[0] = __dsqrt_rn(__ddiv_rn(__ddiv_rn(o[0], n), n));
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Host drivers
+// ---------------------------------------------------------------------------
+__global__ void k_krylov_setup(KrylovState *st, KrylovParams pr, long long ncell) {
+  st->res_rat = pr.res_rat;
+  st->res_tol = pr.res_tol;
+  st->scale = pr.scale;
+  st->dV = pr.dV;
+  st->ncell = (double)ncell;
+  st->mini = pr.mini;
+  st->maxit = pr.maxit;
+  st->stalecount = pr.stalecount;
+  st->hist_cap = pr.hist_cap;
+  st->done = 0;
+  st->converged = 0;
+  st->status = ST_RUNNING;
+  st->iter = 0;
+  st->iterations = 0;
+  st->pending_x = 0;
+  st->rho = st->rho_old = st->alfa = st->beta = st->omega = st->pq = 0.0;
+}
+
+void RefKrylovWork::ensure(size_t n, bool bicgs) {
+  auto fit = [n](DBuf<double> &b) { if (b.n < n) b.alloc(n); };
+  fit(r); fit(q); fit(pA); fit(pB);
+  if (bicgs) { fit(rt); fit(ph); fit(v); fit(s); fit(sh); fit(t); }
+}
+
+void enqueue_ref_setup(const MatView<double> &A, double *x, const double *b, const KrylovParams &pr,
+                       int solver, RefKrylovWork &w, const RedPool &red, KrylovState *st,
+                       cudaStream_t s) {
+  const long long N = A.ncell();
+  const int g = grid_for(N);
+  w.ensure((size_t)N, solver == 1);
+  k_krylov_setup<<<1, 1, 0, s>>>(st, pr, N); note_launch();
+  if (solver == 0) {
+    PBG_CUDA(cudaMemsetAsync(w.pA.p, 0, sizeof(double) * N, s));
+    k_cg_init<<<g, kThreads, 0, s>>>(A, x, b, w.r.p, st, red.slot_part(0), red.slot_count(0)); note_launch();
+  } else {
+    PBG_CUDA(cudaMemsetAsync(w.pA.p, 0, sizeof(double) * N, s));
+    PBG_CUDA(cudaMemsetAsync(w.v.p, 0, sizeof(double) * N, s));
+    k_bi_init<<<g, kThreads, 0, s>>>(A, x, b, w.r.p, w.rt.p, st, red.slot_part(0), red.slot_count(0)); note_launch();
+  }
+  PBG_CUDA(cudaGetLastError());
+}
+
+void enqueue_ref_iters(const MatView<double> &A, double *x, int solver, int count,
+                       RefKrylovWork &w, const RedPool &red, KrylovState *st, double *hist,
+                       cudaStream_t s) {
+  const long long N = A.ncell();
+  const int g = grid_for(N);
+  double *P0 = red.slot_part(0), *P1 = red.slot_part(1);
+  unsigned *C0 = red.slot_count(0), *C1 = red.slot_count(1);
+  for (int it = 0; it < count; ++it) {
+    if (solver == 0) {
+      k_cg_pq<<<g, kThreads, 0, s>>>(A, w.r.p, w.pA.p, w.pB.p, w.q.p, st, P0, C0); note_launch();
+      k_cg_xr<<<g, kThreads, 0, s>>>(N, A.c, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1); note_launch();
+    } else {
+      k_bi_rho<<<g, kThreads, 0, s>>>(N, w.rt.p, w.r.p, st, P0, C0); note_launch();
+      k_bi_p<<<g, kThreads, 0, s>>>(N, A.c, w.r.p, w.pA.p, w.v.p, w.ph.p, st); note_launch();
+      k_bi_spmv<<<g, kThreads, 0, s>>>(A, w.ph.p, w.v.p, w.rt.p, 0, st, P1, C1); note_launch();
+      k_bi_s<<<g, kThreads, 0, s>>>(N, A.c, w.r.p, w.v.p, w.s.p, w.sh.p, st, P0, C0); note_launch();
+      k_bi_spmv<<<g, kThreads, 0, s>>>(A, w.sh.p, w.t.p, w.s.p, 1, st, P1, C1); note_launch();
+      k_bi_xr<<<g, kThreads, 0, s>>>(N, x, w.r.p, w.ph.p, w.sh.p, w.s.p, w.t.p, st, hist, P0, C0); note_launch();
+    }
+  }
+  PBG_CUDA(cudaGetLastError());
+}
+
+// Full solve with host polling of the device status every chunk.
+RefKrylovResult ref_krylov_solve(const MatView<double> &A, double *x, const double *b,
+                                 const KrylovParams &pr, int solver, RefKrylovWork &w,
+                                 const RedPool &red, KrylovState *st, KrylovState *hst,
+                                 double *hist, cudaStream_t s) {
+  enqueue_ref_setup(A, x, b, pr, solver, w, red, st, s);
+  int enq = 0, chunk = 8;
+  for (;;) {
+    PBG_CUDA(cudaMemcpyAsync(hst, st, sizeof(KrylovState), cudaMemcpyDeviceToHost, s));
+    PBG_CUDA(cudaStreamSynchronize(s));
+    if (hst->done || enq >= pr.maxit) break;
+    int cnt = chunk;
+    if (enq + cnt > pr.maxit) cnt = pr.maxit - enq;
+    enqueue_ref_iters(A, x, solver, cnt, w, red, st, hist, s);
+    enq += cnt;
+    if (chunk < 256) chunk *= 2;
+  }
+  RefKrylovResult r;
+  r.converged = hst->converged;
+  r.status = hst->status;
+  r.iterations = hst->iterations;
+  r.res0 = hst->res0;
+  r.res = hst->res;
+  return r;
+}
+
+// ----------------------------- reference AC ---------------------------------
+static int first_factor(int n) {  // Domain::factor (domain_factor.cpp:4-21)
+  int m = n - 1;
+  for (;;) {
+    if (m <= 0) return n;
+    if (n % m == 0) return n / m;
+    m--;
+    if (m == 0 || m == 1) return n;
+  }
+}
+
+void RefAC::build(const MatView<double> &A0, const uint8_t *aflag0, double h, cudaStream_t s) {
+  L.clear();
+  L.emplace_back();
+  RefACLevel &l0 = L.back();
+  l0.nx = A0.nx; l0.ny = A0.ny; l0.nz = A0.nz;
+  l0.CI = l0.CJ = l0.CK = 1;
+  double hx = h, hy = h, hz = h;
+  l0.dV = hx * hy * hz;
+  const long long N0 = A0.ncell();
+  l0.phi.alloc(N0); l0.fnew.alloc(N0); l0.aflag.alloc(N0);
+  PBG_CUDA(cudaMemcpyAsync(l0.aflag.p, aflag0, N0, cudaMemcpyDeviceToDevice, s));
+  fold.alloc(N0);
+  A0v = A0;
+  // Domain::coarsen (domain_coarsen.cpp:6-112): factor = smallest prime
+  // factor, coarsen a direction while interior % factor == 0, interior > 4
+  // and interior != factor; stop when no direction coarsens.
+  for (int lev = 1; lev < 64; ++lev) {
+    const RefACLevel &f = L.back();
+    int n[3] = {f.nx, f.ny, f.nz}, fac[3], ok[3];
+    for (int d = 0; d < 3; ++d) {
+      fac[d] = (d == 2 && A0.nz == 1) ? 2 : first_factor(n[d]);
+      ok[d] = !((n[d] % fac[d]) != 0 || (n[d] + 6) <= 10 || n[d] == fac[d]);
+    }
+    if (!ok[0] && !ok[1] && !ok[2]) break;
+    RefACLevel c;
+    c.CI = ok[0] ? fac[0] : 1; c.CJ = ok[1] ? fac[1] : 1; c.CK = ok[2] ? fac[2] : 1;
+    c.nx = n[0] / c.CI; c.ny = n[1] / c.CJ; c.nz = n[2] / c.CK;
+    hx *= c.CI; hy *= c.CJ; hz *= c.CK;
+    c.dV = hx * hy * hz;
+    const long long NH = (long long)c.nx * c.ny * c.nz;
+    c.A.nx = c.nx; c.A.ny = c.ny; c.A.nz = c.nz; c.A.sym = false;
+    DBuf<double> *arr[7] = {&c.A.c, &c.A.w, &c.A.e, &c.A.s, &c.A.n, &c.A.b, &c.A.t};
+    for (auto *a : arr) a->alloc(NH);
+    c.phi.alloc(NH); c.fnew.alloc(NH); c.aflag.alloc(NH);
+    k_ac_flag<<<grid_for(NH), kThreads, 0, s>>>(f.ny, f.nz, f.aflag.p, c.nx, c.ny, c.nz, c.aflag.p,
+                                                 c.CI, c.CJ, c.CK); note_launch();
+    L.push_back(std::move(c));
+  }
+  PBG_CUDA(cudaGetLastError());
+}
+
+MatView<double> RefAC::view(int l) const { return l == 0 ? A0v : L[l].A.view(); }
+
+void RefAC::coarsen_all(cudaStream_t s) {
+  for (size_t l = 1; l < L.size(); ++l) {
+    RefACLevel &c = L[l];
+    CoarseOut H{c.nx, c.ny, c.nz, c.A.c.p, c.A.w.p, c.A.e.p, c.A.s.p, c.A.n.p, c.A.b.p, c.A.t.p};
+    long long NH = (long long)c.nx * c.ny * c.nz;
+    k_ac_coarsen<<<grid_for(NH), kThreads, 0, s>>>(view((int)l - 1), H, c.CI, c.CJ, c.CK); note_launch();
+  }
+  PBG_CUDA(cudaGetLastError());
+}
+
+double RefAC::residual(RedPool &red, double *dscal, unsigned long long *dlinf, double *hbuf,
+                       cudaStream_t s, double *linf) {
+  const RefACLevel &l0 = L[0];
+  PBG_CUDA(cudaMemsetAsync(dlinf, 0, sizeof(unsigned long long), s));
+  k_ac_resnorm<<<grid_for(A0v.ncell()), kThreads, 0, s>>>(A0v, l0.phi.p, l0.fnew.p, l0.dV, dscal,
+                                                          dlinf, red.slot_part(2), red.slot_count(2)); note_launch();
+  PBG_CUDA(cudaGetLastError());
+  PBG_CUDA(cudaMemcpyAsync(hbuf, dscal, sizeof(double), cudaMemcpyDeviceToHost, s));
+  PBG_CUDA(cudaMemcpyAsync(hbuf + 1, dlinf, sizeof(double), cudaMemcpyDeviceToHost, s));
+  PBG_CUDA(cudaStreamSynchronize(s));
+  if (linf) *linf = hbuf[1];
+  return hbuf[0];
+}
+
+void RefAC::smooth(int l, int mi, double res_rat, double res_tol, int ms, RefKrylovWork &w,
+                   RedPool &red, KrylovState *st, cudaStream_t s) {
+  KrylovParams pr;
+  pr.mini = 1; pr.maxit = mi; pr.stalecount = ms;
+  pr.res_rat = res_rat; pr.res_tol = res_tol; pr.scale = 1.0; pr.dV = L[l].dV; pr.hist_cap = 0;
+  MatView<double> A = view(l);
+  enqueue_ref_setup(A, L[l].phi.p, L[l].fnew.p, pr, 0, w, red, st, s);
+  enqueue_ref_iters(A, L[l].phi.p, 0, mi, w, red, st, nullptr, s);
+}
+
+void RefAC::restrict_to(int l, RedPool &red, double *dmean, cudaStream_t s) {
+  RefACLevel &f = L[l], &c = L[l + 1];
+  long long NH = (long long)c.nx * c.ny * c.nz;
+  int g = grid_for(NH);
+  k_ac_restrict<<<g, kThreads, 0, s>>>(view(l), f.phi.p, f.fnew.p, c.nx, c.ny, c.nz, c.fnew.p,
+                                        c.aflag.p, c.CI, c.CJ, c.CK, dmean, red.slot_part(3),
+                                        red.slot_count(3)); note_launch();
+  k_ac_submean<<<g, kThreads, 0, s>>>(NH, c.fnew.p, c.aflag.p, dmean); note_launch();
+  PBG_CUDA(cudaGetLastError());
+}
+
+void RefAC::interp_from(int l, cudaStream_t s) {
+  RefACLevel &c = L[l], &f = L[l - 1];
+  long long N = (long long)f.nx * f.ny * f.nz;
+  k_ac_interp<<<grid_for(N), kThreads, 0, s>>>(f.nx, f.ny, f.nz, f.phi.p, c.ny, c.nz, c.phi.p, c.CI,
+                                               c.CJ, c.CK); note_launch();
+  PBG_CUDA(cudaGetLastError());
+}
+
+
+// AC::cycle and its recursions (additive_cycle.cpp:4-99,
+// additive_cycle_functions.cpp:12-107, additive_recursive.cpp:4-158).
+void RefAC::run(int kind, int l, RefACCtx &cx) {
+  if (kind == 1) v_cycle(l, cx);
+  else if (kind == 2 || kind == 4) fw_cycle(l, cx, kind == 4);
+}
+
+void RefAC::v_cycle(int l, RefACCtx &cx) {
+  const int last = (int)L.size() - 1;
+  if (l != last) {
+    smooth(l, cx.mv[0], cx.resrat_val, cx.restol_val, cx.ms[0], *cx.w, *cx.red, cx.st, cx.s);
+    restrict_to(l, *cx.red, cx.dmean, cx.s);
+    v_cycle(l + 1, cx);
+    smooth(l, cx.mv[2], cx.resrat_val, cx.restol_val, cx.ms[2], *cx.w, *cx.red, cx.st, cx.s);
+    if (l > 0) interp_from(l, cx.s);
+  } else {
+    smooth(l, 100, -1.0, cx.restol_val, -1, *cx.w, *cx.red, cx.st, cx.s);
+    if (l > 0) interp_from(l, cx.s);
+  }
+}
+
+void RefAC::fw_cycle(int l, RefACCtx &cx, bool w) {
+  const int last = (int)L.size() - 1;
+  if (l != last) {
+    smooth(l, cx.mv[0], cx.resrat_val, cx.restol_val, cx.ms[0], *cx.w, *cx.red, cx.st, cx.s);
+    restrict_to(l, *cx.red, cx.dmean, cx.s);
+    fw_cycle(l + 1, cx, w);
+    smooth(l, cx.mv[1], cx.resrat_val, cx.restol_val, cx.ms[1], *cx.w, *cx.red, cx.st, cx.s);
+    restrict_to(l, *cx.red, cx.dmean, cx.s);
+    if (w) fw_cycle(l + 1, cx, w);
+    else v_cycle(l + 1, cx);
+    smooth(l, cx.mv[2], cx.resrat_val, cx.restol_val, cx.ms[2], *cx.w, *cx.red, cx.st, cx.s);
+    if (l > 0) interp_from(l, cx.s);
+  } else {
+    smooth(l, 100, -1.0, cx.restol_val, -1, *cx.w, *cx.red, cx.st, cx.s);
+    if (l > 0) interp_from(l, cx.s);
+  }
+}
+
+void RefAC::full_cycle(int l, int kind, RefACCtx &cx) {
+  const int last = (int)L.size() - 1;
+  if (l != last) {
+    restrict_to(l, *cx.red, cx.dmean, cx.s);
+    full_cycle(l + 1, kind, cx);
+    run(kind, l, cx);
+  } else {
+    smooth(l, 100, -1.0, cx.restol_val, -1, *cx.w, *cx.red, cx.st, cx.s);
+    if (l > 0) interp_from(l, cx.s);
+  }
+}
+
+RefACResult RefAC::cycle(double *x, const double *b, const RefACParams &pa, RefACCtx &cx,
+                         double *res_hist, int hist_cap) {
+  RefACLevel &l0 = L[0];
+  const long long N0 = A0v.ncell();
+  cudaStream_t s = cx.s;
+  PBG_CUDA(cudaMemcpyAsync(l0.phi.p, x, sizeof(double) * N0, cudaMemcpyDeviceToDevice, s));
+  PBG_CUDA(cudaMemcpyAsync(l0.fnew.p, b, sizeof(double) * N0, cudaMemcpyDeviceToDevice, s));
+  coarsen_all(s);  // rebuilt on every call (additive_cycle_functions.cpp:25-26)
+  RefACResult out{};
+  int nh = 0;
+  double linf0;
+  double res_0 = residual(*cx.red, cx.dscal, cx.dlinf, cx.hbuf, s, &linf0);
+  if (res_hist && nh < hist_cap) res_hist[nh] = res_0;
+  nh++;
+  PBG_CUDA(cudaMemcpyAsync(fold.p, l0.phi.p, sizeof(double) * N0, cudaMemcpyDeviceToDevice, s));
+  out.res0 = res_0;
+  if ((res_0 < pa.toler && pa.min_cyc == 0) || res_0 == 0.0) {
+    out.converged = 1; out.cycles = 0; out.res = res_0;
+  } else {
+    for (size_t l = 1; l < L.size(); ++l) {
+      long long n = (long long)L[l].nx * L[l].ny * L[l].nz;
+      PBG_CUDA(cudaMemsetAsync(L[l].phi.p, 0, sizeof(double) * n, s));
+      PBG_CUDA(cudaMemsetAsync(L[l].fnew.p, 0, sizeof(double) * n, s));
+    }
+    if (pa.init != -1) full_cycle(0, pa.init, cx);
+    double res_m1 = residual(*cx.red, cx.dscal, cx.dlinf, cx.hbuf, s, nullptr);
+    out.cycles = pa.max_cyc;
+    out.converged = 0;
+    out.res = res_m1;
+    for (int c = 1; c <= pa.max_cyc; ++c) {
+      run(pa.loop, 0, cx);
+      double res1 = residual(*cx.red, cx.dscal, cx.dlinf, cx.hbuf, s, nullptr);
+      if (res_hist && nh < hist_cap) res_hist[nh] = res1;
+      nh++;
+      out.res = res1;
+      int con;
+      if (c >= pa.min_cyc && (res1 / res_0 < pa.factor || res1 < pa.toler)) {
+        con = 0;
+      } else {
+        bool check = pa.stop_if_div != 0;
+        if (pa.priority_min_cyc && c < pa.min_cyc) check = false;
+        if (check && res1 >= res_m1) {
+          PBG_CUDA(cudaMemcpyAsync(l0.phi.p, fold.p, sizeof(double) * N0, cudaMemcpyDeviceToDevice, s));
+          con = 1;
+        } else {
+          con = 2;
+        }
+      }
+      res_m1 = res1;
+      if (con == 0) { out.converged = 1; out.cycles = c; break; }
+      if (con == 1) { out.converged = 0; out.cycles = c; out.diverged = 1; break; }
+      PBG_CUDA(cudaMemcpyAsync(fold.p, l0.phi.p, sizeof(double) * N0, cudaMemcpyDeviceToDevice, s));
+    }
+  }
+  PBG_CUDA(cudaMemcpyAsync(x, l0.phi.p, sizeof(double) * N0, cudaMemcpyDeviceToDevice, s));
+  PBG_CUDA(cudaStreamSynchronize(s));
+  out.nhist = nh;
+  return out;
+}
+
+}  // namespace pbg

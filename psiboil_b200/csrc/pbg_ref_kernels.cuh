@@ -1,0 +1,102 @@
+// Reference-parity solvers: host drivers and the kernels the C-ABI calls
+// directly. See pbg_ref_kernels.cu.
+#pragma once
+
+#include <vector>
+
+#include "pbg_common.cuh"
+#include "pbg_session.h"
+
+namespace pbg {
+
+struct KrylovParams {
+  int mini, maxit, stalecount, hist_cap;
+  double res_rat, res_tol, scale, dV;
+};
+
+struct RefKrylovWork {
+  DBuf<double> r, q, pA, pB, rt, ph, v, s, sh, t;
+  void ensure(size_t n, bool bicgs);
+};
+
+struct RefKrylovResult {
+  int converged, status, iterations;
+  double res0, res;
+};
+
+__global__ void k_spmv_ref(MatView<double> A, const double *__restrict__ x, double *__restrict__ y);
+__global__ void k_resid_ref(MatView<double> A, const double *__restrict__ x,
+                            const double *__restrict__ b, double *__restrict__ r);
+__global__ void k_dot2(long long N, const double *__restrict__ x, const double *__restrict__ y,
+                       double dV, double *part, unsigned *count, double *out);
+
+void enqueue_ref_setup(const MatView<double> &A, double *x, const double *b, const KrylovParams &pr,
+                       int solver, RefKrylovWork &w, const RedPool &red, KrylovState *st,
+                       cudaStream_t s);
+void enqueue_ref_iters(const MatView<double> &A, double *x, int solver, int count,
+                       RefKrylovWork &w, const RedPool &red, KrylovState *st, double *hist,
+                       cudaStream_t s);
+RefKrylovResult ref_krylov_solve(const MatView<double> &A, double *x, const double *b,
+                                 const KrylovParams &pr, int solver, RefKrylovWork &w,
+                                 const RedPool &red, KrylovState *st, KrylovState *hst,
+                                 double *hist, cudaStream_t s);
+
+struct RefACLevel {
+  int nx = 0, ny = 0, nz = 0, CI = 1, CJ = 1, CK = 1;
+  double dV = 0;
+  Mat64 A;                 // coarse levels: general storage
+  DBuf<double> phi, fnew;
+  DBuf<uint8_t> aflag;
+};
+
+struct RefACParams {
+  int init, loop;          // -1 none, 1 V, 2 F, 4 W
+  double toler, factor;
+  int max_cyc, min_cyc, stop_if_div, priority_min_cyc;
+  int mv[3], ms[3];
+  double resrat_val, restol_val;
+};
+
+struct RefACResult {
+  int converged, cycles, diverged, nhist;
+  double res0, res;
+};
+
+struct RefACCtx {
+  cudaStream_t s;
+  RefKrylovWork *w;
+  RedPool *red;
+  KrylovState *st;
+  double *dscal, *dmean, *hbuf;
+  unsigned long long *dlinf;
+  int mv[3], ms[3];
+  double resrat_val, restol_val;
+};
+
+class RefAC {
+ public:
+  std::vector<RefACLevel> L;
+  DBuf<double> fold;
+  MatView<double> A0v{};
+
+  void build(const MatView<double> &A0, const uint8_t *aflag0, double h, cudaStream_t s);
+  MatView<double> view(int l) const;
+  void coarsen_all(cudaStream_t s);
+  RefACResult cycle(double *x, const double *b, const RefACParams &pa, RefACCtx &cx,
+                    double *res_hist, int hist_cap);
+  int nlevels() const { return (int)L.size(); }
+
+ private:
+  double residual(RedPool &red, double *dscal, unsigned long long *dlinf, double *hbuf,
+                  cudaStream_t s, double *linf);
+  void smooth(int l, int mi, double res_rat, double res_tol, int ms, RefKrylovWork &w,
+              RedPool &red, KrylovState *st, cudaStream_t s);
+  void restrict_to(int l, RedPool &red, double *dmean, cudaStream_t s);
+  void interp_from(int l, cudaStream_t s);
+  void run(int kind, int l, RefACCtx &cx);
+  void v_cycle(int l, RefACCtx &cx);
+  void fw_cycle(int l, RefACCtx &cx, bool w);
+  void full_cycle(int l, int kind, RefACCtx &cx);
+};
+
+}  // namespace pbg

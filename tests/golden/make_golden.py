@@ -1,0 +1,68 @@
+"""Generate the golden fixtures from the compiled reference (PSI-BOIL).
+
+Runs oracle/_ref/ref_harness (the unmodified reference library built from
+its sources by oracle/build_ref.py, driven by the fixture harness) on small
+seeded problems and stores its matrix, right-hand side, solutions,
+iteration/cycle counts and residual histories under tests/golden/*.npz.
+Only needed where the reference sources exist; the fixtures are committed.
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import oracle_py as O  # noqa: E402
+
+CASES = [
+    # name, kind, problem kwargs, runs
+    ("single16", O.KIND_SINGLE, dict(n=16), ["cg", "bicgs", "ac"]),
+    ("single12", O.KIND_SINGLE, dict(n=12), ["cg", "ac_w", "ac_f", "ac_noguard"]),
+    ("cyl24", O.KIND_CYL, dict(n=24, nb=3, rmin=2.0, rmax=4.0, rc=5.0), ["cg", "ac"]),
+    ("odd15", O.KIND_BATCH, dict(index=40, n2d=0, s3=(15, 16)), ["cg", "ac"]),
+    ("flat2d", O.KIND_BATCH, dict(index=1, n2d=8, s2=(24, 40)), ["cg", "bicgs", "ac"]),
+]
+
+
+def main():
+    O.build()
+    if not O.harness_available():
+        raise SystemExit("oracle/_ref/ref_harness missing: run python oracle/build_ref.py")
+    for name, kind, kw, runs in CASES:
+        P = O.Problem(kind, 7, **kw)
+        out = dict(dims=np.array(P.dims), h=np.array(P.h), kind=np.array(kind), seed=np.array(7))
+        for k, v in kw.items():
+            out["arg_" + k] = np.array(v)
+        for run in runs:
+            solver = "ac" if run.startswith("ac") else run
+            extra = {}
+            if run == "ac_w":
+                extra = dict(cycle="W")
+            elif run == "ac_f":
+                extra = dict(cycle="F")
+            elif run == "ac_noguard":
+                extra = dict(guard=0, maxcyc=6)
+            meta, arr = O.run_reference(P, solver, resrat=1e-8, **extra)
+            if "A" not in out:
+                for k in "cwesnbt":
+                    out["A_" + k] = arr["A"][k]
+                out["ci"] = arr["ci"]
+                out["b"] = arr["b"]
+            out[run + "_x"] = arr["x"]
+            out[run + "_iterations"] = np.array(meta["iterations"])
+            out[run + "_converged"] = np.array(meta["converged"])
+            out[run + "_cycles"] = np.array(meta["cycles"])
+            if solver == "ac":
+                out[run + "_hist"] = np.array([meta["res0"]] + meta["cycle_res"])
+            print(name, run, P.dims, {k: meta[k] for k in ("iterations", "cycles", "converged")})
+            out["A"] = True
+        del out["A"]
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,77 @@
+"""The engine's fast solver (flexible CG + AC K-cycle) in FP64 and mixed
+precision. Checked with the oracle: the FP64 true residual |b - A x| / |b|
+<= 1e-8 (recomputed on the CPU), and the error against the tight oracle
+solution (CG to 1e-13) stays within what the residual bound allows."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CASES = [(0, dict(n=16)), (0, dict(n=64)), (1, dict(n=40, nb=6, rmin=2.0, rmax=5.0, rc=8.0)),
+         (2, dict(index=2, n2d=4, s2=(40, 90))), (2, dict(index=9, n2d=4, s3=(21, 33)))]
+
+
+def true_relres(oracle, P, x):
+    r = oracle.resid(P, x, P.b)
+    return float(np.linalg.norm(r) / np.linalg.norm(P.b))
+
+
+@pytest.mark.parametrize("kind,kw", CASES)
+@pytest.mark.parametrize("precision", [0, 1])
+def test_engine_reaches_1e8(engine, oracle, kind, kw, precision):
+    P = oracle.Problem(kind, 3, **kw)
+    x = np.zeros(P.N)
+    with engine.Session(*P.dims, P.h) as s:
+        s.assemble_pressure(P.rho, P.solid)
+        E = engine.Engine(s)
+        ok = E.solve(x, P.b.copy(), tol=1e-8, precision=precision)
+        r = E.last
+    assert ok and r.status == 0
+    rel = true_relres(oracle, P, x)
+    assert rel <= 1e-8 * 1.0001, rel
+    assert abs(rel - r.relres) <= 1e-3 * rel + 1e-15
+    xt, _ = oracle.cg(P, res_rat=1e-13, maxit=100000)
+    err = np.linalg.norm(x - xt) / np.linalg.norm(xt)
+    assert err < 1e-4, err
+    if precision == 1:
+        assert r.sweeps >= 2
+
+
+def test_engine_warm_start(engine, oracle):
+    P = oracle.Problem(0, 5, n=24)
+    with engine.Session(*P.dims, P.h) as s:
+        s.assemble_pressure(P.rho, P.solid)
+        E = engine.Engine(s)
+        x = np.zeros(P.N)
+        E.solve(x, P.b.copy(), precision=1)
+        cold = E.last.iterations
+        x2 = x.copy()
+        E.solve(x2, P.b.copy(), precision=1)
+        assert E.last.status in (0, 4) and E.last.iterations <= 1
+        x3 = x + 1e-3 * np.random.default_rng(0).standard_normal(P.N) * np.abs(x).max()
+        E.solve(x3, P.b.copy(), precision=1)
+        assert E.last.converged and E.last.iterations < cold
+    assert true_relres(oracle, P, x3) <= 1e-8 * 1.0001
+
+
+def test_engine_rejects_nonsymmetric(engine, oracle):
+    P = oracle.Problem(0, 5, n=8)
+    A = {k: v.copy() for k, v in P.A.items()}
+    A["e"][0] *= 1.5
+    with engine.Session(*P.dims, P.h) as s:
+        s.upload_matrix(A)
+        assert not s.symmetric()
+        with pytest.raises(engine.PbgError):
+            engine.Engine(s).solve(np.zeros(P.N), P.b.copy())
+
+
+def test_device_arrays(engine, oracle):
+    torch = pytest.importorskip("torch")
+    P = oracle.Problem(0, 2, n=20)
+    with engine.Session(*P.dims, P.h) as s:
+        s.assemble_pressure(torch.from_numpy(P.rho).cuda(), torch.from_numpy(P.solid).cuda())
+        xd = torch.zeros(P.N, dtype=torch.float64, device="cuda")
+        bd = torch.from_numpy(P.b).cuda()
+        engine.Engine(s).solve(xd, bd, precision=1)
+        x = xd.cpu().numpy()
+    assert true_relres(oracle, P, x) <= 1e-8 * 1.0001

@@ -1,0 +1,165 @@
+"""Reference-parity path on the GPU, checked against the oracle and the
+reference's golden outputs. Tolerances: bit-exact for the assembled matrix,
+SpMV, residual and AC coarse operators (same per-element operation order);
+solutions of CG / BiCGS / AC within 1e-10 relative (only the order of the
+global sums differs) and iteration / cycle counts within 2."""
+import numpy as np
+import pytest
+
+from golden_util import NAMES, load, problem_of
+
+pytestmark = pytest.mark.gpu
+RTOL_X = 1e-10
+
+
+def relerr(x, ref):
+    return float(np.abs(x - ref).max() / max(np.abs(ref).max(), 1e-300))
+
+
+def session_for(engine, P, assemble=True):
+    s = engine.Session(*P.dims, P.h)
+    if assemble:
+        s.assemble_pressure(P.rho, P.solid)
+    else:
+        s.upload_matrix(P.A)
+        s.upload_active((1 - P.solid).astype(np.int32))
+    return s
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_assembly_bit_exact(engine, oracle, name):
+    P = problem_of(load(name), oracle)
+    with session_for(engine, P) as s:
+        assert s.symmetric()
+        M = s.download_matrix()
+    for k in "cwesnbt":
+        assert np.array_equal(M[k], P.A[k]), k
+
+
+def test_upload_reference_layout(engine, oracle):
+    """The reference's BW=3 Scalar blocks go in unchanged (strided upload)."""
+    P = problem_of(load("cyl24"), oracle)
+    nx, ny, nz = P.dims
+    B = 3
+    si, sj = (ny + 2 * B) * (nz + 2 * B), nz + 2 * B
+    off = B * (si + sj + 1)
+    pad = {}
+    for k in "cwesnbt":
+        a = np.full((nx + 2 * B) * si, np.nan)
+        v = a.reshape(nx + 2 * B, ny + 2 * B, nz + 2 * B)
+        v[B:B + nx, B:B + ny, B:B + nz] = P.A[k].reshape(nx, ny, nz)
+        pad[k] = a
+    with engine.Session(*P.dims, P.h) as s:
+        s.upload_matrix(pad, strides=(si, sj, 1), offset=off)
+        assert s.symmetric()
+        M = s.download_matrix()
+        for k in "cwesnbt":
+            assert np.array_equal(M[k], P.A[k])
+        # strided solve on reference-layout x and b
+        bpad = np.zeros_like(pad["c"])
+        bpad.reshape(nx + 2 * B, ny + 2 * B, nz + 2 * B)[B:B + nx, B:B + ny, B:B + nz] = P.b.reshape(nx, ny, nz)
+        xpad = np.zeros_like(bpad)
+        s.upload_active((1 - P.solid).astype(np.int32))
+        p = engine.default_params(engine.SOLVER_CG)
+        p.max_iter, p.res_rat, p.res_tol = 20000, 1e-8, 1e-18
+        r = s.solve(xpad, bpad, p, strides=(si, sj, 1), offset=off)
+    x = xpad.reshape(nx + 2 * B, ny + 2 * B, nz + 2 * B)[B:B + nx, B:B + ny, B:B + nz].ravel()
+    g = load("cyl24")
+    assert relerr(x, g["cg_x"]) <= RTOL_X
+    assert abs(r.iterations - int(g["cg_iterations"])) <= 2
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_spmv_and_residual_bit_exact(engine, oracle, name):
+    P = problem_of(load(name), oracle)
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(P.N)
+    for assemble in (True, False):
+        with session_for(engine, P, assemble) as s:
+            y = s.spmv(x, np.zeros(P.N))
+            r = s.residual(x, P.b, np.zeros(P.N))
+        assert np.array_equal(y, oracle.spmv(P, x))
+        assert np.array_equal(r, oracle.resid(P, x, P.b))
+
+
+def test_dots(engine, oracle):
+    P = problem_of(load("single16"), oracle)
+    rng = np.random.default_rng(4)
+    x, y = rng.standard_normal(P.N), rng.standard_normal(P.N)
+    with session_for(engine, P) as s:
+        d, dv = s.dot(x, y)
+    assert abs(d - oracle.dot(x, y)) <= 1e-12 * np.abs(x * y).sum()
+    ref = oracle.dot_voldiv_avg(x, y, P.dV)
+    assert abs(dv - ref) <= 1e-12 * abs(ref) + 1e-300
+
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("solver", ["cg", "bicgs"])
+def test_krylov_parity(engine, oracle, name, solver):
+    g = load(name)
+    if solver + "_x" not in g:
+        pytest.skip("no golden run")
+    P = problem_of(g, oracle)
+    x = np.zeros(P.N)
+    with session_for(engine, P) as s:
+        K = engine.CG(s) if solver == "cg" else engine.BiCGS(s)
+        ok = K.solve(x, P.b.copy(), min_iter=1, max_iter=20000, res_rat=1e-8, res_tol=1e-18)
+        it = K.last.iterations
+    assert ok == bool(g[solver + "_converged"])
+    assert abs(it - int(g[solver + "_iterations"])) <= 2
+    assert relerr(x, g[solver + "_x"]) <= RTOL_X
+
+
+AC_RUNS = {"ac": dict(loop=1), "ac_w": dict(loop=4), "ac_f": dict(loop=2),
+           "ac_noguard": dict(loop=1, guard=False, max_cyc=6)}
+
+
+@pytest.mark.parametrize("name,run", [(n, r) for n in NAMES for r in AC_RUNS if r + "_x" in load(n)])
+def test_ac_parity(engine, oracle, name, run):
+    g = load(name)
+    P = problem_of(g, oracle)
+    cfg = AC_RUNS[run]
+    x = np.zeros(P.N)
+    with session_for(engine, P) as s:
+        ac = engine.AC(s)
+        ac.stop_if_diverging(cfg.get("guard", True))
+        ac.max_cycles(cfg.get("max_cyc", 20))
+        ok, ncyc = ac.cycle(x, P.b.copy(), loop=cfg["loop"], factor=1e-8)
+        hist = s.history()
+    assert abs(ncyc - int(g[run + "_cycles"])) <= 2
+    assert ok == bool(g[run + "_converged"])
+    n = min(len(hist), len(g[run + "_hist"]))
+    np.testing.assert_allclose(hist[:n], g[run + "_hist"][:n], rtol=1e-10)
+    assert relerr(x, g[run + "_x"]) <= RTOL_X
+
+
+@pytest.mark.parametrize("name", ["single16", "cyl24", "odd15", "flat2d"])
+def test_ac_hierarchy_and_coarse_operators(engine, oracle, name):
+    P = problem_of(load(name), oracle)
+    ac = oracle.AC(P)
+    with session_for(engine, P) as s:
+        lv = s.levels(0)
+        assert lv == [ac.level_dims(l) for l in range(ac.nlevels)]
+        for l in range(1, len(lv)):
+            M = s.ac_level_matrix(l)
+            R = ac.level_matrix(l)
+            for k in "cwesnbt":
+                assert np.array_equal(M[k], R[k]), (l, k)
+
+
+@pytest.mark.slow
+def test_config0_64_cg_and_ac(engine, oracle):
+    """The 64^3 one-bubble case: CG (566 its in the reference) and AC V-cycles."""
+    P = oracle.Problem(oracle.KIND_SINGLE, 1, n=64)
+    xo, st = oracle.cg(P)
+    x = np.zeros(P.N)
+    with session_for(engine, P) as s:
+        K = engine.CG(s)
+        K.solve(x, P.b.copy(), max_iter=20000, res_rat=1e-8, res_tol=1e-18)
+        assert abs(K.last.iterations - st["iterations"]) <= 2
+        assert relerr(x, xo) <= RTOL_X
+        xa = np.zeros(P.N)
+        ok, ncyc = engine.AC(s).vcycle(xa, P.b.copy(), factor=1e-8)
+    xr, sr = oracle.AC(P).cycle(factor=1e-8)
+    assert ncyc == sr["cycles"] and ok == bool(sr["converged"])
+    assert relerr(xa, xr) <= RTOL_X

@@ -1,0 +1,73 @@
+"""The CPU oracle against the reference's own outputs (golden fixtures made
+by tests/golden/make_golden.py from the compiled reference)."""
+import numpy as np
+import pytest
+
+from golden_util import NAMES, load, problem_of
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_fixture_matrix_and_rhs_bit_exact(oracle, name):
+    g = load(name)
+    P = problem_of(g, oracle)
+    assert P.dims == tuple(g["dims"])
+    for k in "cwesnbt":
+        assert np.array_equal(P.A[k], g["A_" + k]), k
+    assert np.array_equal(P.ci, g["ci"])
+    assert np.array_equal(P.b, g["b"])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_cg_bit_exact(oracle, name):
+    g = load(name)
+    P = problem_of(g, oracle)
+    x, st = oracle.cg(P, res_rat=1e-8, maxit=20000)
+    assert st["printed"] == int(g["cg_iterations"])
+    assert st["converged"] == int(g["cg_converged"])
+    assert np.array_equal(x, g["cg_x"])
+
+
+@pytest.mark.parametrize("name", [n for n in NAMES if "bicgs_x" in load(n)])
+def test_bicgs_bit_exact(oracle, name):
+    g = load(name)
+    P = problem_of(g, oracle)
+    x, st = oracle.cg(P, res_rat=1e-8, maxit=20000, solver="bicgs")
+    assert st["printed"] == int(g["bicgs_iterations"])
+    assert np.array_equal(x, g["bicgs_x"])
+
+
+AC_RUNS = {"ac": dict(loop=1), "ac_w": dict(loop=4), "ac_f": dict(loop=2),
+           "ac_noguard": dict(loop=1, stop_if_div=0, max_cyc=6)}
+
+
+@pytest.mark.parametrize("name,run", [(n, r) for n in NAMES for r in AC_RUNS if r + "_x" in load(n)])
+def test_ac_bit_exact(oracle, name, run):
+    g = load(name)
+    P = problem_of(g, oracle)
+    ac = oracle.AC(P)
+    x, st = ac.cycle(factor=1e-8, **AC_RUNS[run])
+    assert st["cycles"] == int(g[run + "_cycles"])
+    assert st["converged"] == int(g[run + "_converged"])
+    # residual values: the reference's cell volume is a product of node-coordinate
+    # differences (Domain::dV, domain_surfaces_volumes.cpp:60-61), uniform only to
+    # rounding when 1/n is not a binary fraction; solutions stay bit-exact.
+    np.testing.assert_allclose(st["hist"], g[run + "_hist"], rtol=1e-13, atol=0)
+    assert np.array_equal(x, g[run + "_x"])
+
+
+def test_mt64_matches_standard_engine(oracle):
+    # the 10000th draw of a default-seeded mt19937_64 is fixed by the C++ standard
+    import ctypes
+    import subprocess, tempfile, os
+    src = r'''
+    #include <stdio.h>
+    #include "problem_gen.h"
+    int main(){ pbg_mt64 g; pbg_mt64_seed(&g, 5489ULL); unsigned long long v=0;
+      for(int i=0;i<10000;++i) v=pbg_mt64_next(&g); printf("%llu\n", v); return 0; }
+    '''
+    d = tempfile.mkdtemp()
+    c = os.path.join(d, "t.c")
+    open(c, "w").write(src)
+    exe = os.path.join(d, "t")
+    subprocess.check_call(["gcc", "-std=c99", "-I", oracle.PROBLEM_GEN_DIR, c, "-o", exe, "-lm"])
+    assert subprocess.check_output([exe]).strip() == b"9981545732273789042"
