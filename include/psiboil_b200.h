@@ -99,6 +99,10 @@ typedef struct {
   double tol;             /* target |b - A x| / |b| (FP64 true residual)        */
   double inner_tol;       /* mixed: FP32 inner solve reduction per sweep         */
   int max_sweeps;         /* mixed: refinement sweeps at most                    */
+  /* reference-parity solvers: 1 = add every global sum in the reference's
+   * sequential i,j,k order (bit-for-bit reference results, one thread per
+   * cell and a serial sum per dot product); 0 = deterministic tree sums */
+  int exact_sums;
 } pbg_params;
 
 typedef struct {

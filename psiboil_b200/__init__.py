@@ -56,7 +56,7 @@ class Params(ctypes.Structure):
                 ("stop_if_div", ctypes.c_int), ("priority_min_cyc", ctypes.c_int),
                 ("mv", ctypes.c_int * 3), ("ms", ctypes.c_int * 3),
                 ("tol", ctypes.c_double), ("inner_tol", ctypes.c_double),
-                ("max_sweeps", ctypes.c_int)]
+                ("max_sweeps", ctypes.c_int), ("exact_sums", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):
@@ -301,10 +301,11 @@ class Session:
 class _Krylov:
     solver = SOLVER_CG
 
-    def __init__(self, session, prec="di"):
+    def __init__(self, session, prec="di", exact_sums=False):
         if prec not in ("di", "diagonal"):
             raise NotImplementedError("only the diagonal preconditioner (Prec::di) is provided")
         self.session = session
+        self.exact_sums = exact_sums
         self.last = None
 
     def solve(self, x, b, min_iter=1, max_iter=20, name=None, res_rat=0.01, res_tol=1.0e-15,
@@ -314,6 +315,7 @@ class _Krylov:
         p = default_params(self.solver)
         p.min_iter, p.max_iter = int(min_iter), int(max_iter)
         p.res_rat, p.res_tol, p.scale, p.stalecount = res_rat, res_tol, scale, int(stalecount)
+        p.exact_sums = int(self.exact_sums)
         self.last = self.session.solve(x, b, p)
         if name is not None:
             r = self.last
@@ -335,8 +337,9 @@ class BiCGS(_Krylov):
 class AC:
     """Additive-correction multigrid with CG smoothers (Src/Solver/Additive)."""
 
-    def __init__(self, session):
+    def __init__(self, session, exact_sums=False):
         self.session = session
+        self.exact_sums = exact_sums
         self._max_cyc, self._min_cyc = 20, 0
         self._stop_if_div, self._prio = True, True
         self.mv = [20, 20, 20]
@@ -380,6 +383,7 @@ class AC:
         for q in range(3):
             p.mv[q] = (mv or self.mv)[q]
             p.ms[q] = (ms or self.ms)[q]
+        p.exact_sums = int(self.exact_sums)
         self.last = self.session.solve(x, b, p)
         return bool(self.last.converged), self.last.cycles
 

@@ -36,7 +36,7 @@ struct pbg_session {
   bool refac_dirty = true;
   std::unique_ptr<Engine> eng;
   bool eng_dirty = true, eng_mixed = false;
-  DBuf<double> dx, db, dscal, hist;
+  DBuf<double> dx, db, dscal, hist, seq;
   DBuf<unsigned long long> dlinf;
   double *hbuf = nullptr;          // pinned: 64 doubles
   double *px = nullptr, *pb = nullptr;  // pinned staging (ncell each)
@@ -428,6 +428,13 @@ void ensure_engine(pbg_session *s, bool mixed) {
   }
 }
 
+// Scratch of the exact-order reductions (2 terms per cell), when requested.
+double *exact_terms(pbg_session *s, const pbg_params *p) {
+  if (!p->exact_sums) return nullptr;
+  if (s->seq.n < (size_t)(2 * s->ncell())) s->seq.alloc(2 * s->ncell());
+  return s->seq.p;
+}
+
 int solve_device(pbg_session *s, double *xd, const double *bd, const pbg_params *p, pbg_result *r) {
   pbg_result out;
   std::memset(&out, 0, sizeof(out));
@@ -439,6 +446,7 @@ int solve_device(pbg_session *s, double *xd, const double *bd, const pbg_params 
     pr.stalecount = p->stalecount > kStaleMax ? kStaleMax : p->stalecount;
     pr.hist_cap = kHistMax;
     pr.res_rat = p->res_rat; pr.res_tol = p->res_tol; pr.scale = p->scale; pr.dV = dV;
+    pr.seq = exact_terms(s, p);
     RefKrylovResult rr = ref_krylov_solve(s->A.view(), xd, bd, pr, p->solver == PBG_SOLVER_BICGS ? 1 : 0,
                                           s->rkw, s->red, s->kst.p, s->hkst, s->hist.p, s->stream);
     out.status = rr.status;
@@ -466,6 +474,7 @@ int solve_device(pbg_session *s, double *xd, const double *bd, const pbg_params 
     cx.dscal = s->dscal.p; cx.dmean = s->dscal.p + 4; cx.hbuf = s->hbuf; cx.dlinf = s->dlinf.p;
     for (int q = 0; q < 3; ++q) { cx.mv[q] = pa.mv[q]; cx.ms[q] = pa.ms[q]; }
     cx.resrat_val = pa.resrat_val; cx.restol_val = pa.restol_val;
+    s->refac->seq = exact_terms(s, p);
     s->hhist.assign(p->max_cycles + 2, 0.0);
     RefACResult ar = s->refac->cycle(xd, bd, pa, cx, s->hhist.data(), (int)s->hhist.size());
     s->nhist = ar.nhist < (int)s->hhist.size() ? ar.nhist : (int)s->hhist.size();

@@ -38,6 +38,12 @@ struct CudaError : std::runtime_error {
 extern unsigned long long g_launch_count;
 inline void note_launch() { __atomic_add_fetch(&g_launch_count, 1ULL, __ATOMIC_RELAXED); }
 
+// Grid of an exact-order reduction: one thread per element.
+inline int grid_exact(long long n, int threads = kThreads) {
+  long long b = (n + threads - 1) / threads;
+  return (int)(b < 1 ? 1 : b);
+}
+
 inline int grid_for(long long n, int threads = kThreads, int cap = kMaxBlocks) {
   long long b = (n + threads - 1) / threads;
   if (b < 1) b = 1;
@@ -114,10 +120,40 @@ __device__ __forceinline__ void warp_sum(double (&v)[NV]) {
 }
 
 // Returns true in thread 0 of the last block; out[] then holds the totals.
+//
+// Exact-order mode (seq != nullptr): the launch has one thread per element
+// (thread p holds element p's term in v), every term is stored in
+// seq[q*n + p], and the last block's thread 0 adds them in index order —
+// the reference's sequential i,j,k summation (Src/Field/Scalar/scalar.h:296-326)
+// reproduced to the bit. Used by the reference-parity solvers on request.
 template <int NV>
-__device__ bool grid_reduce(double (&v)[NV], double *part, unsigned *count, double (&out)[NV]) {
+__device__ bool grid_reduce(double (&v)[NV], double *part, unsigned *count, double (&out)[NV],
+                            double *seq = nullptr, long long n = 0) {
   __shared__ double sm[NV][kThreads / 32];
   __shared__ bool last;
+  if (seq) {
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p < n)
+#pragma unroll
+      for (int q = 0; q < NV; ++q) seq[q * n + p] = v[q];
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned prev = atomicAdd(count, 1u);
+      last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return false;
+    __threadfence();
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double s = 0.0;
+      for (long long e = 0; e < n; ++e) s = __dadd_rn(s, __ldcg(&seq[q * n + e]));
+      out[q] = s;
+    }
+    *count = 0u;
+    return true;
+  }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   warp_sum<NV>(v);
   if (lane == 0)

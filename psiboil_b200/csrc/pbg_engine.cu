@@ -12,6 +12,7 @@ namespace pbg {
 template <typename T>
 void EWork<T>::ensure(const std::vector<ELevel> &lv) {
   if (L.size() == lv.size() && x0.n == (size_t)lv[0].ncell()) return;
+  drop_graph();
   L.clear();
   L.resize(lv.size());
   for (size_t l = 0; l < lv.size(); ++l) {
@@ -25,6 +26,13 @@ void EWork<T>::ensure(const std::vector<ELevel> &lv) {
   ks.alloc(lv.size());
   fs.alloc(1);
   PBG_CUDA(cudaMemset(fs.p, 0, sizeof(FcgScal)));
+}
+
+template <typename T>
+void EWork<T>::drop_graph() {
+  if (iter_graph) cudaGraphExecDestroy(iter_graph);
+  iter_graph = nullptr;
+  iter_nodes = 0;
 }
 
 template struct EWork<double>;
@@ -78,6 +86,10 @@ static void dense_spd_inverse(int n, std::vector<double> &A) {
 }
 
 void Engine::build(const EMat<double> &A0, cudaStream_t s, bool mixed) {
+  w64.drop_graph();
+  w32.drop_graph();
+  w64.L.clear();
+  w32.L.clear();
   L.clear();
   L.emplace_back();
   L[0].nx = A0.nx; L[0].ny = A0.ny; L[0].nz = A0.nz;
@@ -196,6 +208,9 @@ void Engine::kcycle(int l, EWork<T> &w, RedPool &red, const int *stop, cudaStrea
 }
 
 // Flexible CG on level 0 for A e = b (e starts at zero); returns iterations.
+// One iteration (the preconditioner's K-cycle over all levels plus the two
+// FCG kernels) is captured once into a CUDA graph and replayed; every kernel
+// in it returns at once when the device-side done flag is set.
 template <typename T>
 int Engine::fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red, cudaStream_t s,
                 double *hist, FcgScal *hfs) {
@@ -204,9 +219,24 @@ int Engine::fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red, cu
   const int g = grid_for(N);
   FcgScal *fs = w.fs.p;
   const int *stop = &fs->done;
-  PBG_CUDA(cudaMemsetAsync(w.q0.p, 0, sizeof(T) * N, s));
-  k_fcg_init<T><<<g, kThreads, 0, s>>>(N, b, w.x0.p, w.r0.p, fs, tol, maxit, red.slot_part(0),
+  if (!w.iter_graph) {
+    cudaGraph_t graph;
+    const unsigned long long before = g_launch_count;
+    PBG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    precond<T>(0, w.r0.p, w.z0.p, true, w.q0.p, &fs->zr, w, red, stop, s);
+    k_fcg_pq<T><<<g, kThreads, 0, s>>>(A, w.z0.p, w.pA.p, w.pB.p, w.q0.p, fs, red.slot_part(0),
                                        red.slot_count(0)); note_launch();
+    k_fcg_xr<T><<<g, kThreads, 0, s>>>(N, w.x0.p, w.r0.p, w.pA.p, w.pB.p, w.q0.p, fs,
+                                       red.slot_part(0), red.slot_count(0)); note_launch();
+    PBG_CUDA(cudaStreamEndCapture(s, &graph));
+    w.iter_nodes = (size_t)(g_launch_count - before);
+    __atomic_sub_fetch(&g_launch_count, (unsigned long long)w.iter_nodes, __ATOMIC_RELAXED);
+    PBG_CUDA(cudaGraphInstantiate(&w.iter_graph, graph, 0));
+    cudaGraphDestroy(graph);
+  }
+  PBG_CUDA(cudaMemsetAsync(w.q0.p, 0, sizeof(T) * N, s));
+  k_fcg_init<T><<<g, kThreads, 0, s>>>(N, b, w.x0.p, w.r0.p, fs, tol, maxit, hist,
+                                       red.slot_part(0), red.slot_count(0)); note_launch();
   PBG_CUDA(cudaGetLastError());
   int enq = 0, chunk = 4;
   for (;;) {
@@ -215,14 +245,8 @@ int Engine::fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red, cu
     if (hfs->done || enq >= maxit) break;
     int cnt = chunk;
     if (enq + cnt > maxit) cnt = maxit - enq;
-    for (int c = 0; c < cnt; ++c) {
-      precond<T>(0, w.r0.p, w.z0.p, true, w.q0.p, &fs->zr, w, red, stop, s);
-      k_fcg_pq<T><<<g, kThreads, 0, s>>>(A, w.z0.p, w.pA.p, w.pB.p, w.q0.p, fs, red.slot_part(0),
-                                         red.slot_count(0)); note_launch();
-      k_fcg_xr<T><<<g, kThreads, 0, s>>>(N, w.x0.p, w.r0.p, w.pA.p, w.pB.p, w.q0.p, fs, hist,
-                                         red.slot_part(0), red.slot_count(0)); note_launch();
-    }
-    PBG_CUDA(cudaGetLastError());
+    for (int c = 0; c < cnt; ++c) PBG_CUDA(cudaGraphLaunch(w.iter_graph, s));
+    __atomic_add_fetch(&g_launch_count, (unsigned long long)(cnt * w.iter_nodes), __ATOMIC_RELAXED);
     enq += cnt;
     if (chunk < 16) chunk *= 2;
   }

@@ -26,6 +26,7 @@ struct FcgScal {
   double zr, zq;          // written together by k_jac_dots (z.r, z.q_old)
   double pr, pq, beta, alpha, rr, rr0, tol;
   int iter, maxit, done, converged, status, pad;
+  double *hist;           // per-iteration |r|/|r0| (kHistMax entries) or null
 };
 
 // One aggregation level of the engine hierarchy.
@@ -48,7 +49,11 @@ struct EWork {
   DBuf<T> x0, r0, z0, pA, pB, q0;      // outer FCG on level 0
   DBuf<KScal> ks;                      // one per level
   DBuf<FcgScal> fs;
+  cudaGraphExec_t iter_graph = nullptr;  // one captured FCG iteration
+  size_t iter_nodes = 0;
   void ensure(const std::vector<ELevel> &lv);
+  void drop_graph();
+  ~EWork() { drop_graph(); }
 };
 
 struct EngineOpts {

@@ -271,7 +271,7 @@ __global__ void k_fcg_pq(EMat<T> A, const T *__restrict__ z, T *pA, T *pB, T *__
 
 template <typename T>
 __global__ void k_fcg_xr(long long N, T *__restrict__ x, T *__restrict__ r, const T *pA,
-                         const T *pB, const T *__restrict__ qv, FcgScal *fs, double *hist,
+                         const T *pB, const T *__restrict__ qv, FcgScal *fs,
                          double *part, unsigned *count) {
   if (fs->done) return;
   const int it = fs->iter;
@@ -291,7 +291,7 @@ __global__ void k_fcg_xr(long long N, T *__restrict__ x, T *__restrict__ r, cons
     fs->rr = o[0];
     fs->pr = o[1];
     double rel = sqrt(o[0] / fs->rr0);
-    if (hist && it < kHistMax) hist[it] = rel;
+    if (fs->hist && it < kHistMax) fs->hist[it] = rel;
     fs->iter = it + 1;
     if (rel <= fs->tol) { fs->done = 1; fs->converged = 1; fs->status = ST_CONVERGED; }
     else if (!(rel == rel)) { fs->done = 1; fs->status = ST_NAN; }
@@ -302,8 +302,8 @@ __global__ void k_fcg_xr(long long N, T *__restrict__ x, T *__restrict__ r, cons
 // r = b, x = 0 (T), rr0 = |b|^2; fs set up for a new solve
 template <typename T>
 __global__ void k_fcg_init(long long N, const T *__restrict__ b, T *__restrict__ x,
-                           T *__restrict__ r, FcgScal *fs, double tol, int maxit, double *part,
-                           unsigned *count) {
+                           T *__restrict__ r, FcgScal *fs, double tol, int maxit, double *hist,
+                           double *part, unsigned *count) {
   double v[1] = {0.0};
   GRID_LOOP(p, N) {
     T bv = b[p];
@@ -315,6 +315,7 @@ __global__ void k_fcg_init(long long N, const T *__restrict__ b, T *__restrict__
   if (grid_reduce<1>(v, part, count, o)) {
     fs->rr0 = o[0];
     fs->rr = o[0];
+    fs->hist = hist;
     fs->tol = tol;
     fs->maxit = maxit;
     fs->iter = 0;

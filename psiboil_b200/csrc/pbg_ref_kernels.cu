@@ -140,7 +140,7 @@ __global__ void k_cg_init(MatView<double> A, const double *__restrict__ x,
     v[1] += __dmul_rn(rv, __dmul_rn(rv, mc_of(A.c, p)));
   }
   double o[2];
-  if (grid_reduce<2>(v, part, count, o)) {
+  if (grid_reduce<2>(v, part, count, o, st->seq, N)) {
     double res = res_of(o[0], st);
     st->res0 = res;
     st->res = res;
@@ -187,7 +187,7 @@ __global__ void k_cg_pq(MatView<double> A, const double *__restrict__ r, double 
     v[0] += __dmul_rn(pp, qq);
   }
   double o[1];
-  if (grid_reduce<1>(v, part, count, o)) {
+  if (grid_reduce<1>(v, part, count, o, st->seq, N)) {
     st->beta = beta;
     st->pq = o[0];
     st->alfa = __ddiv_rn(st->rho, o[0]);
@@ -212,7 +212,7 @@ __global__ void k_cg_xr(long long N, const double *__restrict__ c, double *__res
     v[1] += __dmul_rn(rv, __dmul_rn(rv, mc_of(c, p)));
   }
   double o[2];
-  if (grid_reduce<2>(v, part, count, o)) {
+  if (grid_reduce<2>(v, part, count, o, st->seq, N)) {
     double res = res_of(o[0], st);
     st->res = res;
     if (hist && it < st->hist_cap) hist[it] = res;
@@ -261,7 +261,7 @@ __global__ void k_bi_init(MatView<double> A, const double *__restrict__ x, const
     v[0] += voldiv(rv, rv, dV);
   }
   double o[1];
-  if (grid_reduce<1>(v, part, count, o)) {
+  if (grid_reduce<1>(v, part, count, o, st->seq, N)) {
     double res = res_of(o[0], st);
     st->res0 = res;
     st->res = res;
@@ -288,7 +288,7 @@ __global__ void k_bi_rho(long long N, const double *__restrict__ rt, const doubl
        p += (long long)gridDim.x * blockDim.x)
     v[0] += __dmul_rn(rt[p], r[p]);
   double o[1];
-  if (grid_reduce<1>(v, part, count, o)) {
+  if (grid_reduce<1>(v, part, count, o, st->seq, N)) {
     const int it = st->iter;
     st->rho = o[0];
     if (__dsqrt_rn(fabs(o[0])) < st->res_tol) {
@@ -334,7 +334,7 @@ __global__ void k_bi_spmv(MatView<double> A, const double *__restrict__ x, doubl
     else { v[0] += __dmul_rn(yv, o1[p]); v[1] += __dmul_rn(yv, yv); }
   }
   double o[2];
-  if (grid_reduce<2>(v, part, count, o)) {
+  if (grid_reduce<2>(v, part, count, o, st->seq, N)) {
     if (mode == 0) st->alfa = __ddiv_rn(st->rho, o[0]);
     else { st->aux0 = o[0]; st->aux1 = o[1]; st->omega = __ddiv_rn(o[0], o[1]); }
   }
@@ -354,7 +354,7 @@ __global__ void k_bi_s(long long N, const double *__restrict__ c, const double *
     a[0] += __dmul_rn(sv, sv);
   }
   double o[1];
-  if (grid_reduce<1>(a, part, count, o)) {
+  if (grid_reduce<1>(a, part, count, o, st->seq, N)) {
     if (__dsqrt_rn(o[0]) < st->res_tol) {
       st->pending_x = 1;  // x += alfa p^, then stop (bicgs.cpp:146-150)
       st->done = 1; st->status = ST_BREAKDOWN; st->iterations = st->iter + 1;
@@ -380,7 +380,7 @@ __global__ void k_bi_xr(long long N, double *__restrict__ x, double *__restrict_
     v[0] += voldiv(rv, rv, dV);
   }
   double o[1];
-  if (grid_reduce<1>(v, part, count, o)) {
+  if (grid_reduce<1>(v, part, count, o, st->seq, N)) {
     if (pend) { st->pending_x = 0; return; }
     const int it = st->iter;
     double res = res_of(o[0], st);
@@ -508,7 +508,7 @@ __global__ void k_ac_restrict(MatView<double> A, const double *__restrict__ phi,
                               const double *__restrict__ fnew, int Hnx, int Hny, int Hnz,
                               double *__restrict__ fH, const uint8_t *__restrict__ aH,
                               int CI, int CJ, int CK, double *mean_out, double *part,
-                              unsigned *count) {
+                              unsigned *count, double *seq) {
   FineCell f(A);
   auto ph = [&](int i, int j, int k) -> double {
     return (i < 0 || i >= A.nx || j < 0 || j >= A.ny || k < 0 || k >= A.nz) ? 0.0 : phi[f.at(i, j, k)];
@@ -556,7 +556,7 @@ __global__ void k_ac_restrict(MatView<double> A, const double *__restrict__ phi,
     if (aH[P]) { v[0] += F; v[1] += 1.0; }
   }
   double o[2];
-  if (grid_reduce<2>(v, part, count, o)) *mean_out = __ddiv_rn(o[0], o[1]);
+  if (grid_reduce<2>(v, part, count, o, seq, NH)) *mean_out = __ddiv_rn(o[0], o[1]);
 }
 
 __global__ void k_ac_submean(long long NH, double *__restrict__ fH, const uint8_t *__restrict__ aH,
@@ -584,7 +584,8 @@ __global__ void k_ac_interp(int nx, int ny, int nz, double *__restrict__ phi, in
 // |res/dV| (non-negative doubles order like their bit patterns).
 __global__ void k_ac_resnorm(MatView<double> A, const double *__restrict__ phi,
                              const double *__restrict__ fnew, double dV, double *out,
-                             unsigned long long *linf_bits, double *part, unsigned *count) {
+                             unsigned long long *linf_bits, double *part, unsigned *count,
+                             double *seq) {
   const long long N = A.ncell();
   double v[1] = {0.0};
   double mx = 0.0;
@@ -598,7 +599,7 @@ __global__ void k_ac_resnorm(MatView<double> A, const double *__restrict__ phi,
   for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, off));
   if ((threadIdx.x & 31) == 0) atomicMax(linf_bits, (unsigned long long)__double_as_longlong(mx));
   double o[1];
-  if (grid_reduce<1>(v, part, count, o)) {
+  if (grid_reduce<1>(v, part, count, o, seq, N)) {
     double n = (double)N;
     out[0] = __dsqrt_rn(__ddiv_rn(__ddiv_rn(o[0], n), n));
   }
@@ -618,6 +619,7 @@ __global__ void k_krylov_setup(KrylovState *st, KrylovParams pr, long long ncell
   st->maxit = pr.maxit;
   st->stalecount = pr.stalecount;
   st->hist_cap = pr.hist_cap;
+  st->seq = pr.seq;
   st->done = 0;
   st->converged = 0;
   st->status = ST_RUNNING;
@@ -637,7 +639,7 @@ void enqueue_ref_setup(const MatView<double> &A, double *x, const double *b, con
                        int solver, RefKrylovWork &w, const RedPool &red, KrylovState *st,
                        cudaStream_t s) {
   const long long N = A.ncell();
-  const int g = grid_for(N);
+  const int g = pr.seq ? grid_exact(N) : grid_for(N);
   w.ensure((size_t)N, solver == 1);
   k_krylov_setup<<<1, 1, 0, s>>>(st, pr, N); note_launch();
   if (solver == 0) {
@@ -653,9 +655,9 @@ void enqueue_ref_setup(const MatView<double> &A, double *x, const double *b, con
 
 void enqueue_ref_iters(const MatView<double> &A, double *x, int solver, int count,
                        RefKrylovWork &w, const RedPool &red, KrylovState *st, double *hist,
-                       cudaStream_t s) {
+                       cudaStream_t s, bool exact) {
   const long long N = A.ncell();
-  const int g = grid_for(N);
+  const int g = exact ? grid_exact(N) : grid_for(N);
   double *P0 = red.slot_part(0), *P1 = red.slot_part(1);
   unsigned *C0 = red.slot_count(0), *C1 = red.slot_count(1);
   for (int it = 0; it < count; ++it) {
@@ -687,7 +689,7 @@ RefKrylovResult ref_krylov_solve(const MatView<double> &A, double *x, const doub
     if (hst->done || enq >= pr.maxit) break;
     int cnt = chunk;
     if (enq + cnt > pr.maxit) cnt = pr.maxit - enq;
-    enqueue_ref_iters(A, x, solver, cnt, w, red, st, hist, s);
+    enqueue_ref_iters(A, x, solver, cnt, w, red, st, hist, s, pr.seq != nullptr);
     enq += cnt;
     if (chunk < 256) chunk *= 2;
   }
@@ -768,8 +770,9 @@ double RefAC::residual(RedPool &red, double *dscal, unsigned long long *dlinf, d
                        cudaStream_t s, double *linf) {
   const RefACLevel &l0 = L[0];
   PBG_CUDA(cudaMemsetAsync(dlinf, 0, sizeof(unsigned long long), s));
-  k_ac_resnorm<<<grid_for(A0v.ncell()), kThreads, 0, s>>>(A0v, l0.phi.p, l0.fnew.p, l0.dV, dscal,
-                                                          dlinf, red.slot_part(2), red.slot_count(2)); note_launch();
+  const int g = seq ? grid_exact(A0v.ncell()) : grid_for(A0v.ncell());
+  k_ac_resnorm<<<g, kThreads, 0, s>>>(A0v, l0.phi.p, l0.fnew.p, l0.dV, dscal, dlinf,
+                                      red.slot_part(2), red.slot_count(2), seq); note_launch();
   PBG_CUDA(cudaGetLastError());
   PBG_CUDA(cudaMemcpyAsync(hbuf, dscal, sizeof(double), cudaMemcpyDeviceToHost, s));
   PBG_CUDA(cudaMemcpyAsync(hbuf + 1, dlinf, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -783,18 +786,19 @@ void RefAC::smooth(int l, int mi, double res_rat, double res_tol, int ms, RefKry
   KrylovParams pr;
   pr.mini = 1; pr.maxit = mi; pr.stalecount = ms;
   pr.res_rat = res_rat; pr.res_tol = res_tol; pr.scale = 1.0; pr.dV = L[l].dV; pr.hist_cap = 0;
+  pr.seq = seq;
   MatView<double> A = view(l);
   enqueue_ref_setup(A, L[l].phi.p, L[l].fnew.p, pr, 0, w, red, st, s);
-  enqueue_ref_iters(A, L[l].phi.p, 0, mi, w, red, st, nullptr, s);
+  enqueue_ref_iters(A, L[l].phi.p, 0, mi, w, red, st, nullptr, s, seq != nullptr);
 }
 
 void RefAC::restrict_to(int l, RedPool &red, double *dmean, cudaStream_t s) {
   RefACLevel &f = L[l], &c = L[l + 1];
   long long NH = (long long)c.nx * c.ny * c.nz;
-  int g = grid_for(NH);
+  int g = seq ? grid_exact(NH) : grid_for(NH);
   k_ac_restrict<<<g, kThreads, 0, s>>>(view(l), f.phi.p, f.fnew.p, c.nx, c.ny, c.nz, c.fnew.p,
                                         c.aflag.p, c.CI, c.CJ, c.CK, dmean, red.slot_part(3),
-                                        red.slot_count(3)); note_launch();
+                                        red.slot_count(3), seq); note_launch();
   k_ac_submean<<<g, kThreads, 0, s>>>(NH, c.fnew.p, c.aflag.p, dmean); note_launch();
   PBG_CUDA(cudaGetLastError());
 }

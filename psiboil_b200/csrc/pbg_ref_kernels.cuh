@@ -12,6 +12,7 @@ namespace pbg {
 struct KrylovParams {
   int mini, maxit, stalecount, hist_cap;
   double res_rat, res_tol, scale, dV;
+  double *seq = nullptr;   // exact-order reduction terms (2 x ncell), null: tree
 };
 
 struct RefKrylovWork {
@@ -35,7 +36,7 @@ void enqueue_ref_setup(const MatView<double> &A, double *x, const double *b, con
                        cudaStream_t s);
 void enqueue_ref_iters(const MatView<double> &A, double *x, int solver, int count,
                        RefKrylovWork &w, const RedPool &red, KrylovState *st, double *hist,
-                       cudaStream_t s);
+                       cudaStream_t s, bool exact);
 RefKrylovResult ref_krylov_solve(const MatView<double> &A, double *x, const double *b,
                                  const KrylovParams &pr, int solver, RefKrylovWork &w,
                                  const RedPool &red, KrylovState *st, KrylovState *hst,
@@ -77,6 +78,7 @@ class RefAC {
  public:
   std::vector<RefACLevel> L;
   DBuf<double> fold;
+  double *seq = nullptr;   // exact-order reduction terms, or null
   MatView<double> A0v{};
 
   void build(const MatView<double> &A0, const uint8_t *aflag0, double h, cudaStream_t s);

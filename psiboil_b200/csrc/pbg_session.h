@@ -46,6 +46,7 @@ struct KrylovState {
   // running values
   double rho, rho_old, alfa, beta, omega, pq, res, res0, rr0, aux0, aux1;
   int iter, done, converged, status, iterations, pending_x, pad0, pad1;
+  double *seq;   // exact-order reduction terms (null: tree reduction)
   double stale[kStaleMax];
 };
 

@@ -1,8 +1,19 @@
 """Reference-parity path on the GPU, checked against the oracle and the
-reference's golden outputs. Tolerances: bit-exact for the assembled matrix,
-SpMV, residual and AC coarse operators (same per-element operation order);
-solutions of CG / BiCGS / AC within 1e-10 relative (only the order of the
-global sums differs) and iteration / cycle counts within 2."""
+reference's golden outputs.
+
+Tolerances: bit-exact for the assembled matrix, SpMV, residual and AC
+coarse operators (same per-element operation order). Solvers run in two
+reduction modes:
+  exact_sums=True  every global sum in the reference's sequential order:
+                   CG, BiCGS and AC solutions, iteration / cycle counts and
+                   residual histories bit-for-bit equal to the reference;
+  exact_sums=False deterministic tree sums (the fast default): CG and AC
+                   solutions within 1e-10 relative and counts within 2;
+                   BiCGStab's iterates depend on the rounding of its dot
+                   products far more (an emulation of the tree order on the
+                   CPU moves them by 6e-8..2e-7), so BiCGS is held to 1e-6
+                   relative and counts within 6 in that mode.
+"""
 import numpy as np
 import pytest
 
@@ -95,19 +106,27 @@ def test_dots(engine, oracle):
 
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("solver", ["cg", "bicgs"])
-def test_krylov_parity(engine, oracle, name, solver):
+@pytest.mark.parametrize("exact", [True, False])
+def test_krylov_parity(engine, oracle, name, solver, exact):
     g = load(name)
     if solver + "_x" not in g:
         pytest.skip("no golden run")
     P = problem_of(g, oracle)
     x = np.zeros(P.N)
     with session_for(engine, P) as s:
-        K = engine.CG(s) if solver == "cg" else engine.BiCGS(s)
+        K = (engine.CG if solver == "cg" else engine.BiCGS)(s, exact_sums=exact)
         ok = K.solve(x, P.b.copy(), min_iter=1, max_iter=20000, res_rat=1e-8, res_tol=1e-18)
         it = K.last.iterations
     assert ok == bool(g[solver + "_converged"])
-    assert abs(it - int(g[solver + "_iterations"])) <= 2
-    assert relerr(x, g[solver + "_x"]) <= RTOL_X
+    if exact:
+        assert it == int(g[solver + "_iterations"])
+        assert np.array_equal(x, g[solver + "_x"])
+    elif solver == "cg":
+        assert abs(it - int(g[solver + "_iterations"])) <= 2
+        assert relerr(x, g[solver + "_x"]) <= RTOL_X
+    else:
+        assert abs(it - int(g[solver + "_iterations"])) <= 6
+        assert relerr(x, g[solver + "_x"]) <= 1e-6
 
 
 AC_RUNS = {"ac": dict(loop=1), "ac_w": dict(loop=4), "ac_f": dict(loop=2),
@@ -115,22 +134,30 @@ AC_RUNS = {"ac": dict(loop=1), "ac_w": dict(loop=4), "ac_f": dict(loop=2),
 
 
 @pytest.mark.parametrize("name,run", [(n, r) for n in NAMES for r in AC_RUNS if r + "_x" in load(n)])
-def test_ac_parity(engine, oracle, name, run):
+@pytest.mark.parametrize("exact", [True, False])
+def test_ac_parity(engine, oracle, name, run, exact):
     g = load(name)
     P = problem_of(g, oracle)
     cfg = AC_RUNS[run]
     x = np.zeros(P.N)
     with session_for(engine, P) as s:
-        ac = engine.AC(s)
+        ac = engine.AC(s, exact_sums=exact)
         ac.stop_if_diverging(cfg.get("guard", True))
         ac.max_cycles(cfg.get("max_cyc", 20))
         ok, ncyc = ac.cycle(x, P.b.copy(), loop=cfg["loop"], factor=1e-8)
         hist = s.history()
-    assert abs(ncyc - int(g[run + "_cycles"])) <= 2
     assert ok == bool(g[run + "_converged"])
-    n = min(len(hist), len(g[run + "_hist"]))
-    np.testing.assert_allclose(hist[:n], g[run + "_hist"][:n], rtol=1e-10)
-    assert relerr(x, g[run + "_x"]) <= RTOL_X
+    if exact:
+        assert ncyc == int(g[run + "_cycles"])
+        assert np.array_equal(x, g[run + "_x"])
+        # the reference prints residuals computed with per-cell volumes
+        # (exact on binary-fraction spacings)
+        np.testing.assert_allclose(hist, g[run + "_hist"], rtol=1e-13)
+    else:
+        assert abs(ncyc - int(g[run + "_cycles"])) <= 2
+        n = min(len(hist), len(g[run + "_hist"]))
+        np.testing.assert_allclose(hist[:n], g[run + "_hist"][:n], rtol=1e-10)
+        assert relerr(x, g[run + "_x"]) <= RTOL_X
 
 
 @pytest.mark.parametrize("name", ["single16", "cyl24", "odd15", "flat2d"])
@@ -152,14 +179,15 @@ def test_config0_64_cg_and_ac(engine, oracle):
     """The 64^3 one-bubble case: CG (566 its in the reference) and AC V-cycles."""
     P = oracle.Problem(oracle.KIND_SINGLE, 1, n=64)
     xo, st = oracle.cg(P)
-    x = np.zeros(P.N)
-    with session_for(engine, P) as s:
-        K = engine.CG(s)
-        K.solve(x, P.b.copy(), max_iter=20000, res_rat=1e-8, res_tol=1e-18)
-        assert abs(K.last.iterations - st["iterations"]) <= 2
-        assert relerr(x, xo) <= RTOL_X
-        xa = np.zeros(P.N)
-        ok, ncyc = engine.AC(s).vcycle(xa, P.b.copy(), factor=1e-8)
     xr, sr = oracle.AC(P).cycle(factor=1e-8)
-    assert ncyc == sr["cycles"] and ok == bool(sr["converged"])
-    assert relerr(xa, xr) <= RTOL_X
+    with session_for(engine, P) as s:
+        for exact in (False, True):
+            x = np.zeros(P.N)
+            K = engine.CG(s, exact_sums=exact)
+            K.solve(x, P.b.copy(), max_iter=20000, res_rat=1e-8, res_tol=1e-18)
+            assert abs(K.last.iterations - st["iterations"]) <= (0 if exact else 2)
+            assert relerr(x, xo) <= (0.0 if exact else RTOL_X)
+            xa = np.zeros(P.N)
+            ok, ncyc = engine.AC(s, exact_sums=exact).vcycle(xa, P.b.copy(), factor=1e-8)
+            assert ncyc == sr["cycles"] and ok == bool(sr["converged"])
+            assert relerr(xa, xr) <= (0.0 if exact else RTOL_X)
