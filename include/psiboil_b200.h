@@ -138,6 +138,10 @@ int pbg_session_create(int nx, int ny, int nz, double h, const int bc[6], int de
 int pbg_session_destroy(pbg_session *s);
 int pbg_session_info(const pbg_session *s, long long *ncell, int *symmetric,
                      long long *device_bytes);
+/* Cell volume used by the reference-parity residual measure
+ * sqrt(dot_voldiv_avg(r, r))/scale (scalar.h:317-326); default h*h*h.
+ * Domain::dV of the level (domain_surfaces_volumes.cpp:60-61). */
+int pbg_session_set_cell_volume(pbg_session *s, double dV);
 
 /* Upload the seven coefficient arrays of the reference's Matrix
  * (matrix.h:23-54; sign convention A x = c x_P - sum a_nb x_nb), strided

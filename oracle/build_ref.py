@@ -111,6 +111,20 @@ def build(ref, jobs):
         subprocess.check_call(["g++"] + CXXFLAGS + flags +
                               ["-I", os.path.join(REPO, "psiboil_b200", "csrc"),
                                harness, lib, "-o", exe])
+    # the same harness with the engine's Krylov classes plugged in through
+    # include/psiboil_b200_psiboil.hpp (needs the built engine library)
+    englib = os.path.join(REPO, "psiboil_b200", "libpsiboil_b200.so")
+    exe_gpu = os.path.join(OUT, "ref_harness_gpu")
+    if os.path.exists(englib):
+        deps_gpu = deps + [englib, os.path.join(REPO, "include", "psiboil_b200_psiboil.hpp")]
+        if not os.path.exists(exe_gpu) or max(os.path.getmtime(d) for d in deps_gpu) > os.path.getmtime(exe_gpu):
+            cuda = "/usr/local/cuda"
+            subprocess.check_call(["g++"] + CXXFLAGS + flags + ["-DPBG_WITH_ENGINE",
+                                  "-I", os.path.join(REPO, "psiboil_b200", "csrc"),
+                                  "-I", os.path.join(REPO, "include"),
+                                  harness, lib, englib, "-L", os.path.join(cuda, "lib64"), "-lcudart",
+                                  "-Wl,-rpath,$ORIGIN/../../psiboil_b200",
+                                  "-o", exe_gpu])
     print("reference built: %d sources -> %s" % (len(files), exe))
     return exe
 

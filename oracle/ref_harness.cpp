@@ -33,6 +33,9 @@
  */
 #include "Include/psi-boil.h"
 #include "problem_gen.h"
+#ifdef PBG_WITH_ENGINE
+#include "psiboil_b200_psiboil.hpp"
+#endif
 
 #include <chrono>
 #include <cstdio>
@@ -51,7 +54,7 @@ struct Args {
   double rmin = 4, rmax = 16, rc = 0, ratio = 1000;
   unsigned long long seed = 1;
   double resrat = 1e-8;
-  int maxit = 20000, maxcyc = 20, guard = 1, dump = 1, repeat = 1;
+  int maxit = 20000, maxcyc = 20, guard = 1, dump = 1, repeat = 1, gpu = 0, exact = 1;
 };
 
 Args parse(int argc, char **argv) {
@@ -82,6 +85,8 @@ Args parse(int argc, char **argv) {
     else if (k == "--cycle") a.cycle = nxt();
     else if (k == "--dump") a.dump = std::atoi(nxt());
     else if (k == "--repeat") a.repeat = std::atoi(nxt());
+    else if (k == "--gpu") a.gpu = std::atoi(nxt());
+    else if (k == "--exact") a.exact = std::atoi(nxt());
     else if (k == "--out") a.out = nxt();
     else { std::fprintf(stderr, "unknown argument %s\n", k.c_str()); std::exit(2); }
   }
@@ -204,6 +209,12 @@ int main(int argc, char **argv) {
   Times time(1, 1.0);
 
   Linear *solver = nullptr;
+#ifdef PBG_WITH_ENGINE
+  /* the drop-in: the engine's Krylov classes behind the reference's virtual */
+  if (a.gpu && a.solver == "bicgs") solver = new pbg_psiboil::GpuBiCGS(d, Prec::di(), a.exact != 0);
+  else if (a.gpu) solver = new pbg_psiboil::GpuCG(d, Prec::di(), a.exact != 0);
+  else
+#endif
   if (a.solver == "bicgs") solver = new BiCGS(d, Prec::di());
   else solver = new CG(d, Prec::di());
 

@@ -84,6 +84,7 @@ _SIGS = {
     "pbg_session_destroy": (ctypes.c_int, [_vp]),
     "pbg_session_info": (ctypes.c_int, [_vp, ctypes.POINTER(_ll), ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(_ll)]),
+    "pbg_session_set_cell_volume": (ctypes.c_int, [_vp, ctypes.c_double]),
     "pbg_matrix_upload": (ctypes.c_int, [_vp] + [_vp] * 7 + [_ll, _ll, _ll, _ll, ctypes.c_int]),
     "pbg_matrix_download": (ctypes.c_int, [_vp] + [_vp] * 7 + [ctypes.c_int]),
     "pbg_active_upload": (ctypes.c_int, [_vp, _vp, _ll, _ll, _ll, _ll, ctypes.c_int]),

@@ -23,7 +23,7 @@ struct pbg_session {
   int device = 0;
   cudaStream_t stream = nullptr;
   int nx = 0, ny = 0, nz = 0;
-  double h = 0.0;
+  double h = 0.0, dV = 0.0;
   int bc[6] = {0, 0, 0, 0, 0, 0};
   Mat64 A;
   bool have_matrix = false;
@@ -222,6 +222,7 @@ int pbg_session_create(int nx, int ny, int nz, double h, const int bc[6], int de
   auto s = std::make_unique<pbg_session>();
   s->device = device;
   s->nx = nx; s->ny = ny; s->nz = nz; s->h = h;
+  s->dV = (h * h) * h;
   if (bc) for (int f = 0; f < 6; ++f) s->bc[f] = bc[f];
   int rc = guard(s.get(), [&]() -> int {
     PBG_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
@@ -273,6 +274,12 @@ int pbg_session_info(const pbg_session *s, long long *ncell, int *symmetric, lon
                s->A.b.bytes() + s->A.t.bytes() + s->aflag.bytes() + s->dx.bytes() + s->db.bytes();
     *device_bytes = (long long)b;
   }
+  return PBG_OK;
+}
+
+int pbg_session_set_cell_volume(pbg_session *s, double dV) {
+  if (!s || !(dV > 0.0)) return fail(PBG_ERR_ARG, "bad cell volume");
+  s->dV = dV;
   return PBG_OK;
 }
 
@@ -438,7 +445,7 @@ double *exact_terms(pbg_session *s, const pbg_params *p) {
 int solve_device(pbg_session *s, double *xd, const double *bd, const pbg_params *p, pbg_result *r) {
   pbg_result out;
   std::memset(&out, 0, sizeof(out));
-  const double dV = (s->h * s->h) * s->h;
+  const double dV = s->dV;
   s->nhist = 0;
   if (p->solver == PBG_SOLVER_CG || p->solver == PBG_SOLVER_BICGS) {
     KrylovParams pr;

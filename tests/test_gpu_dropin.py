@@ -1,0 +1,56 @@
+"""Drop-in through the reference's own Krylov virtual.
+
+oracle/_ref/ref_harness_gpu is the reference harness built with
+include/psiboil_b200_psiboil.hpp: `new pbg_psiboil::GpuCG(d, Prec::di())`
+replaces `new CG(d, Prec::di())`, so the reference's Centered::solve and the
+reference's own AC multigrid (its cycle logic, restriction, coarse
+operators on the CPU) call the engine's GPU CG through Linear::solve. With
+exact-order sums the results equal the reference's own, bit for bit.
+"""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from golden_util import load
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "oracle", "_ref", "ref_harness_gpu")
+
+
+def run(args):
+    out = os.path.join(tempfile.mkdtemp(prefix="pbg_dropin_"), "r")
+    subprocess.run([EXE] + args + ["--out", out], check=True, capture_output=True, timeout=600)
+    x = np.fromfile(out + ".x", dtype=np.float64)
+    meta = {}
+    for line in open(out + ".txt"):
+        p = line.split()
+        if len(p) >= 2:
+            meta[p[0]] = p[1:]
+    return x, meta
+
+
+@pytest.mark.skipif(not os.path.exists(EXE), reason="GPU-backed reference harness not built")
+@pytest.mark.parametrize("solver,key", [("cg", "cg"), ("bicgs", "bicgs"), ("ac", "ac")])
+def test_reference_with_gpu_krylov_is_bit_exact(solver, key):
+    g = load("single16")
+    x, meta = run(["--kind", "single", "--n", "16", "--seed", "7", "--solver", solver,
+                   "--resrat", "1e-8", "--gpu", "1", "--exact", "1"])
+    assert np.array_equal(x, g[key + "_x"])
+    if solver == "ac":
+        assert int(meta["cycles"][0]) == int(g["ac_cycles"])
+    else:
+        assert int(meta["iterations"][0]) == int(g[key + "_iterations"])
+
+
+@pytest.mark.skipif(not os.path.exists(EXE), reason="GPU-backed reference harness not built")
+def test_reference_ac_with_gpu_krylov_tree_sums():
+    g = load("cyl24")
+    x, meta = run(["--kind", "cyl", "--n", "24", "--nb", "3", "--rmin", "2.0", "--rmax", "4.0",
+                   "--rc", "5.0", "--seed", "7", "--solver", "ac", "--resrat", "1e-8",
+                   "--gpu", "1", "--exact", "0"])
+    assert abs(int(meta["cycles"][0]) - int(g["ac_cycles"])) <= 2
+    assert np.abs(x - g["ac_x"]).max() <= 1e-8 * np.abs(g["ac_x"]).max()

