@@ -428,7 +428,7 @@ void ensure_engine(pbg_session *s, bool mixed) {
   if (!s->eng) s->eng = std::make_unique<Engine>();
   if (s->eng_dirty || (mixed && !s->eng->have32)) {
     const Mat64 &A = s->A;
-    EMat<double> m{A.nx, A.ny, A.nz, A.c.p, A.w.p, A.s.p, A.b.p};
+    EMat<double> m = make_emat<double>(A.nx, A.ny, A.nz, A.c.p, A.w.p, A.s.p, A.b.p, nullptr);
     s->eng->build(m, s->stream, mixed || s->eng_mixed);
     s->eng_mixed = s->eng_mixed || mixed;
     s->eng_dirty = false;

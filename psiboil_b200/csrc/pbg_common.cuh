@@ -65,6 +65,29 @@ struct MatView {
   __host__ __device__ long long ncell() const { return (long long)nx * ny * nz; }
 };
 
+// Unsigned division by a run-time constant with a multiply-high and a shift
+// (Granlund & Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994): for d >= 1 take s = ceil(log2 d) and
+// m = floor(2^32 (2^s - d) / d) + 1; then n / d = (umulhi(n, m) + n) >> s
+// for every n < 2^31 (the sum stays below 2^32). Cell counts are capped
+// at 2^31 per session.
+struct FastDiv {
+  uint32_t d, m, s;
+  FastDiv() : d(1), m(1), s(0) {}
+  explicit FastDiv(uint32_t dv) : d(dv) {
+    s = 0;
+    while ((1ull << s) < dv) ++s;
+    m = (uint32_t)((((1ull << 32) * ((1ull << s) - dv)) / dv) + 1);
+  }
+  __host__ __device__ __forceinline__ uint32_t div(uint32_t n) const {
+#ifdef __CUDA_ARCH__
+    return (__umulhi(n, m) + n) >> s;
+#else
+    return (uint32_t)((((uint64_t)n * m) >> 32) + n) >> s;
+#endif
+  }
+};
+
 // Position of a cell from its linear index.
 struct Pos { int i, j, k; };
 __device__ __forceinline__ Pos pos_of(long long p, int ny, int nz) {
@@ -75,6 +98,23 @@ __device__ __forceinline__ Pos pos_of(long long p, int ny, int nz) {
   int k = (int)(rem - (long long)j * nz);
   return {i, j, k};
 }
+
+// Grid geometry with precomputed divisors (cells < 2^31).
+struct Geo {
+  int nx, ny, nz;
+  uint32_t n, nynz;
+  FastDiv dnynz, dnz;
+  Geo() = default;
+  Geo(int x, int y, int z)
+      : nx(x), ny(y), nz(z), n((uint32_t)x * y * z), nynz((uint32_t)y * z), dnynz((uint32_t)y * z),
+        dnz((uint32_t)z) {}
+  __device__ __forceinline__ Pos pos(uint32_t p) const {
+    uint32_t i = dnynz.div(p);
+    uint32_t rem = p - i * nynz;
+    uint32_t j = dnz.div(rem);
+    return {(int)i, (int)j, (int)(rem - j * (uint32_t)nz)};
+  }
+};
 
 // The six neighbour coefficients of cell p (zero outside the domain).
 template <typename T>

@@ -6,6 +6,7 @@
 
 #include "pbg_engine.cuh"
 #include "pbg_engine_kernels.cuh"
+#include "pbg_bottom.cuh"
 
 namespace pbg {
 
@@ -13,6 +14,7 @@ template <typename T>
 void EWork<T>::ensure(const std::vector<ELevel> &lv) {
   if (L.size() == lv.size() && x0.n == (size_t)lv[0].ncell()) return;
   drop_graph();
+  bot.release();
   L.clear();
   L.resize(lv.size());
   for (size_t l = 0; l < lv.size(); ++l) {
@@ -90,10 +92,18 @@ void Engine::build(const EMat<double> &A0, cudaStream_t s, bool mixed) {
   w32.drop_graph();
   w64.L.clear();
   w32.L.clear();
+  w64.bot.release();
+  w32.bot.release();
   L.clear();
   L.emplace_back();
-  L[0].nx = A0.nx; L[0].ny = A0.ny; L[0].nz = A0.nz;
-  L[0].m64 = A0;
+  {
+    ELevel &l0 = L[0];
+    l0.nx = A0.nx; l0.ny = A0.ny; l0.nz = A0.nz;
+    long long n0 = l0.ncell();
+    l0.d64.alloc(n0);
+    k_inverse<<<grid_for(n0), kThreads, 0, s>>>(n0, A0.c, l0.d64.p); note_launch();
+    l0.m64 = make_emat<double>(A0.nx, A0.ny, A0.nz, A0.c, A0.w, A0.s, A0.b, l0.d64.p);
+  }
   while (L.back().ncell() > opt.coarse_max &&
          (L.back().nx > 1 || L.back().ny > 1 || L.back().nz > 1)) {
     const ELevel &f = L.back();
@@ -102,11 +112,12 @@ void Engine::build(const EMat<double> &A0, cudaStream_t s, bool mixed) {
     c.ny = f.ny > 1 ? (f.ny + 1) / 2 : 1;
     c.nz = f.nz > 1 ? (f.nz + 1) / 2 : 1;
     long long n = c.ncell();
-    c.c64.alloc(n); c.w64.alloc(n); c.s64.alloc(n); c.b64.alloc(n);
-    k_galerkin<<<grid_for(n), kThreads, 0, s>>>(f.m64, c.nx, c.ny, c.nz, c.c64.p, c.w64.p, c.s64.p,
-                                                 c.b64.p); note_launch();
+    c.c64.alloc(n); c.w64.alloc(n); c.s64.alloc(n); c.b64.alloc(n); c.d64.alloc(n);
+    k_galerkin<<<grid_for(n), kThreads, 0, s>>>(f.m64, Geo(c.nx, c.ny, c.nz), c.c64.p, c.w64.p,
+                                                 c.s64.p, c.b64.p); note_launch();
+    k_inverse<<<grid_for(n), kThreads, 0, s>>>(n, c.c64.p, c.d64.p); note_launch();
     PBG_CUDA(cudaGetLastError());
-    c.m64 = {c.nx, c.ny, c.nz, c.c64.p, c.w64.p, c.s64.p, c.b64.p};
+    c.m64 = make_emat<double>(c.nx, c.ny, c.nz, c.c64.p, c.w64.p, c.s64.p, c.b64.p, c.d64.p);
     L.push_back(std::move(c));
   }
   // dense inverse of the coarsest level
@@ -137,11 +148,11 @@ void Engine::build(const EMat<double> &A0, cudaStream_t s, bool mixed) {
   if (mixed) {
     for (auto &lv : L) {
       long long m = lv.ncell();
-      lv.c32.alloc(m); lv.w32.alloc(m); lv.s32.alloc(m); lv.b32.alloc(m);
-      const double *src[4] = {lv.m64.c, lv.m64.w, lv.m64.s, lv.m64.b};
-      float *dst[4] = {lv.c32.p, lv.w32.p, lv.s32.p, lv.b32.p};
-      for (int q = 0; q < 4; ++q) { k_to_float<<<grid_for(m), kThreads, 0, s>>>(m, src[q], dst[q]); note_launch(); }
-      lv.m32 = {lv.nx, lv.ny, lv.nz, lv.c32.p, lv.w32.p, lv.s32.p, lv.b32.p};
+      lv.c32.alloc(m); lv.w32.alloc(m); lv.s32.alloc(m); lv.b32.alloc(m); lv.d32.alloc(m);
+      const double *src[5] = {lv.m64.c, lv.m64.w, lv.m64.s, lv.m64.b, lv.m64.dinv};
+      float *dst[5] = {lv.c32.p, lv.w32.p, lv.s32.p, lv.b32.p, lv.d32.p};
+      for (int q = 0; q < 5; ++q) { k_to_float<<<grid_for(m), kThreads, 0, s>>>(m, src[q], dst[q]); note_launch(); }
+      lv.m32 = make_emat<float>(lv.nx, lv.ny, lv.nz, lv.c32.p, lv.w32.p, lv.s32.p, lv.b32.p, lv.d32.p);
     }
     PBG_CUDA(cudaGetLastError());
     have32 = true;
@@ -151,60 +162,124 @@ void Engine::build(const EMat<double> &A0, cudaStream_t s, bool mixed) {
   PBG_CUDA(cudaStreamSynchronize(s));
 }
 
+// Shared-memory bytes the bottom solver needs when it starts at level l.
+template <typename T>
+static size_t bottom_smem(const Engine &E, int l) {
+  size_t b = bot_level_bytes<T>(E.L[l].ncell(), false);
+  for (int m = l + 1; m < (int)E.L.size(); ++m) b += bot_level_bytes<T>(E.L[m].ncell(), true);
+  return b + (size_t)E.ncoarse * E.ncoarse * sizeof(double);
+}
+
+// First level handled by the shared-memory bottom solver: the first level
+// below level 0 whose work set (and that of every coarser level) fits the
+// shared-memory budget and the solver's level table; L.size() if none.
+template <typename T>
+int Engine::bottom_level() const {
+  const int last = (int)L.size() - 1;
+  for (int l = 1; l < last; ++l)
+    if (last - l < kBotMaxLevels && bottom_smem<T>(*this, l) <= kBotSmemMax) return l;
+  return (int)L.size();
+}
+
+// Level table of the bottom solver, uploaded once per work set (before any
+// graph capture: it allocates).
+template <typename T>
+static void ensure_bottom(const Engine &E, EWork<T> &w) {
+  const int first = E.bottom_level<T>();
+  if (w.bot.p || first >= (int)E.L.size()) return;
+  BotCtx<T> C;
+  memset(&C, 0, sizeof(C));
+  C.first = first;
+  C.last = (int)E.L.size() - 1;
+  uint32_t off = 0;
+  for (int l = first; l <= C.last; ++l) {
+    BotLevel<T> &B = C.L[l - first];
+    B.A = E.template mat<T>(l);
+    B.ks = w.ks.p + l;
+    auto &v = w.L[l];
+    B.gb = v.b.p; B.gz1 = v.z1.p; B.gz2 = v.z2.p;
+    B.off = off;
+    B.smem_matrix = l > first ? 1 : 0;
+    off += (uint32_t)bot_level_bytes<T>(E.L[l].ncell(), l > first);
+  }
+  C.ainv_off = off;
+  off += (uint32_t)((size_t)E.ncoarse * E.ncoarse * sizeof(double));
+  C.smem_bytes = off;
+  C.Ainv = E.Ainv.p;
+  C.ncoarse = E.ncoarse;
+  C.omega = (T)E.opt.omega;
+  PBG_CUDA(cudaFuncSetAttribute(k_bottom<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)off));
+  w.bot.alloc(sizeof(C));
+  w.bot_smem = off;
+  PBG_CUDA(cudaMemcpy(w.bot.p, &C, sizeof(C), cudaMemcpyHostToDevice));
+}
+
+template <typename T>
+static void launch_bottom(EWork<T> &w, const int *stop, cudaStream_t s) {
+  if (!w.bot.p) throw CudaError("bottom solver table not prepared");
+  k_bottom<T><<<1, kBotThreads, w.bot_smem, s>>>((const BotCtx<T> *)w.bot.p, stop); note_launch();
+}
+
+// Preconditioner M r -> z on level l. kc: the K-cycle's second application,
+// whose right-hand side r1 = b - a1 q1 is formed (and stored) by k_jac2.
 template <typename T>
 void Engine::precond(int l, const T *r, T *z, bool dots, const T *u, double *out2, EWork<T> &w,
-                     RedPool &red, const int *stop, cudaStream_t s) {
+                     RedPool &red, const int *stop, cudaStream_t s, bool kc) {
   const int last = (int)L.size() - 1;
   const T om = (T)opt.omega;
+  auto &v = w.L[l];
   if (l == last) {
     k_dense_solve<T><<<(ncoarse * 32 + kThreads - 1) / kThreads, kThreads, 0, s>>>(ncoarse, Ainv.p, r, z, stop); note_launch();
     if (dots) {  // a level-0 problem small enough to be the coarsest
       EMat<T> A = mat<T>(l);
-      PBG_CUDA(cudaMemcpyAsync(w.L[l].xa.p, z, sizeof(T) * A.ncell(), cudaMemcpyDeviceToDevice, s));
-      // z = xa + omega (r - A xa)/c would change z; use omega = 0 to keep z and get the dots
-      k_jac_dots<T><<<grid_for(A.ncell()), kThreads, 0, s>>>(A, r, w.L[l].xa.p, z, T(0), u, out2,
+      PBG_CUDA(cudaMemcpyAsync(v.xa.p, z, sizeof(T) * A.ncell(), cudaMemcpyDeviceToDevice, s));
+      // omega = 0 keeps z and computes the dot products
+      k_jac_dots<T><<<grid_for(A.ncell()), kThreads, 0, s>>>(A, r, v.xa.p, z, T(0), u, out2,
                                                             red.slot_part(0), red.slot_count(0), stop); note_launch();
     }
     return;
   }
   EMat<T> A = mat<T>(l);
-  const long long N = A.ncell();
-  const int g = grid_for(N);
-  auto &v = w.L[l];
+  const int g = grid_for(A.ncell());
   const ELevel &H = L[l + 1];
-  k_jac0<T><<<g, kThreads, 0, s>>>(A, r, v.xa.p, om, stop); note_launch();
-  k_jac<T><<<g, kThreads, 0, s>>>(A, r, v.xa.p, v.xb.p, om, stop); note_launch();
-  k_resid_restrict<T><<<grid_for(H.ncell()), kThreads, 0, s>>>(A, r, v.xb.p, H.nx, H.ny, H.nz,
-                                                               w.L[l + 1].b.p, stop); note_launch();
+  auto &vh = w.L[l + 1];
+  const T *rr = kc ? v.r1.p : r;
+  k_jac2<T><<<g, kThreads, 0, s>>>(A, r, v.b.p, v.q1.p, kc ? w.ks.p + l : nullptr, v.r1.p, v.xb.p,
+                                   om, stop); note_launch();
+  k_resid_restrict<T><<<grid_for(H.ncell()), kThreads, 0, s>>>(A, rr, v.xb.p, Geo(H.nx, H.ny, H.nz),
+                                                               vh.b.p, stop); note_launch();
+  const T *eH, *z2H = nullptr;
+  const KScal *ksH = nullptr;
   if (l + 1 == last) {
     k_dense_solve<T><<<(ncoarse * 32 + kThreads - 1) / kThreads, kThreads, 0, s>>>(
-        ncoarse, Ainv.p, w.L[l + 1].b.p, w.L[l + 1].x.p, stop); note_launch();
+        ncoarse, Ainv.p, vh.b.p, vh.x.p, stop); note_launch();
+    eH = vh.x.p;
   } else {
-    kcycle<T>(l + 1, w, red, stop, s);
+    if (l + 1 >= bottom_level<T>()) launch_bottom<T>(w, stop, s);
+    else kcycle<T>(l + 1, w, red, stop, s);
+    eH = vh.z1.p; z2H = vh.z2.p; ksH = w.ks.p + l + 1;
   }
-  k_prolong_jac<T><<<g, kThreads, 0, s>>>(A, r, v.xb.p, H.ny, H.nz, w.L[l + 1].x.p, v.xa.p, om, stop); note_launch();
+  k_prolong_jac<T><<<g, kThreads, 0, s>>>(A, rr, v.xb.p, H.ny, H.nz, eH, z2H, ksH, v.xa.p, om,
+                                          stop); note_launch();
   if (dots) {
-    k_jac_dots<T><<<g, kThreads, 0, s>>>(A, r, v.xa.p, z, om, u, out2, red.slot_part(0),
+    k_jac_dots<T><<<g, kThreads, 0, s>>>(A, rr, v.xa.p, z, om, u, out2, red.slot_part(0),
                                          red.slot_count(0), stop); note_launch();
   } else {
-    k_jac<T><<<g, kThreads, 0, s>>>(A, r, v.xa.p, z, om, stop); note_launch();
+    k_jac<T><<<g, kThreads, 0, s>>>(A, rr, v.xa.p, z, om, stop); note_launch();
   }
 }
 
 template <typename T>
 void Engine::kcycle(int l, EWork<T> &w, RedPool &red, const int *stop, cudaStream_t s) {
   EMat<T> A = mat<T>(l);
-  const long long N = A.ncell();
-  const int g = grid_for(N);
+  const int g = grid_for(A.ncell());
   auto &v = w.L[l];
   KScal *ks = w.ks.p + l;
-  precond<T>(l, v.b.p, v.z1.p, false, nullptr, nullptr, w, red, stop, s);
+  precond<T>(l, v.b.p, v.z1.p, false, nullptr, nullptr, w, red, stop, s, false);
   k_kc_q1<T><<<g, kThreads, 0, s>>>(A, v.z1.p, v.b.p, v.q1.p, ks, red.slot_part(0), red.slot_count(0), stop); note_launch();
-  k_kc_r1<T><<<g, kThreads, 0, s>>>(N, v.b.p, v.q1.p, v.r1.p, ks, stop); note_launch();
-  precond<T>(l, v.r1.p, v.z2.p, false, nullptr, nullptr, w, red, stop, s);
+  precond<T>(l, nullptr, v.z2.p, false, nullptr, nullptr, w, red, stop, s, true);
   k_kc_q2<T><<<g, kThreads, 0, s>>>(A, v.z2.p, v.q1.p, v.r1.p, v.v.p, ks, red.slot_part(0),
                                     red.slot_count(0), stop); note_launch();
-  k_kc_x<T><<<g, kThreads, 0, s>>>(N, v.z1.p, v.z2.p, v.x.p, ks, stop); note_launch();
 }
 
 // Flexible CG on level 0 for A e = b (e starts at zero); returns iterations.
@@ -220,14 +295,21 @@ int Engine::fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red, cu
   FcgScal *fs = w.fs.p;
   const int *stop = &fs->done;
   if (!w.iter_graph) {
-    cudaGraph_t graph;
+    ensure_bottom<T>(*this, w);
+    cudaGraph_t graph = nullptr;
     const unsigned long long before = g_launch_count;
     PBG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    precond<T>(0, w.r0.p, w.z0.p, true, w.q0.p, &fs->zr, w, red, stop, s);
-    k_fcg_pq<T><<<g, kThreads, 0, s>>>(A, w.z0.p, w.pA.p, w.pB.p, w.q0.p, fs, red.slot_part(0),
-                                       red.slot_count(0)); note_launch();
-    k_fcg_xr<T><<<g, kThreads, 0, s>>>(N, w.x0.p, w.r0.p, w.pA.p, w.pB.p, w.q0.p, fs,
-                                       red.slot_part(0), red.slot_count(0)); note_launch();
+    try {
+      precond<T>(0, w.r0.p, w.z0.p, true, w.q0.p, &fs->zr, w, red, stop, s, false);
+      k_fcg_pq<T><<<g, kThreads, 0, s>>>(A, w.z0.p, w.pA.p, w.pB.p, w.q0.p, fs, red.slot_part(0),
+                                         red.slot_count(0)); note_launch();
+      k_fcg_xr<T><<<g, kThreads, 0, s>>>(N, w.x0.p, w.r0.p, w.pA.p, w.pB.p, w.q0.p, fs,
+                                         red.slot_part(0), red.slot_count(0)); note_launch();
+    } catch (...) {
+      cudaStreamEndCapture(s, &graph);  // leave the stream usable
+      if (graph) cudaGraphDestroy(graph);
+      throw;
+    }
     PBG_CUDA(cudaStreamEndCapture(s, &graph));
     w.iter_nodes = (size_t)(g_launch_count - before);
     __atomic_sub_fetch(&g_launch_count, (unsigned long long)w.iter_nodes, __ATOMIC_RELAXED);

@@ -8,13 +8,25 @@
 
 namespace pbg {
 
-// Symmetric 7-point operator: c, w, s, b (east/north/top from the next cell).
+// Symmetric 7-point operator: c, w, s, b (east/north/top from the next cell)
+// and the inverse diagonal dinv = 1/c used by the smoother.
 template <typename T>
 struct EMat {
   int nx, ny, nz;
-  const T *c, *w, *s, *b;
+  Geo g;
+  const T *c, *w, *s, *b, *dinv;
   __host__ __device__ long long ncell() const { return (long long)nx * ny * nz; }
 };
+
+template <typename T>
+inline EMat<T> make_emat(int nx, int ny, int nz, const T *c, const T *w, const T *s, const T *b,
+                         const T *dinv) {
+  EMat<T> m;
+  m.nx = nx; m.ny = ny; m.nz = nz;
+  m.g = Geo(nx, ny, nz);
+  m.c = c; m.w = w; m.s = s; m.b = b; m.dinv = dinv;
+  return m;
+}
 
 // Scalars of one K-cycle visit on a coarse level.
 struct KScal {
@@ -33,7 +45,8 @@ struct FcgScal {
 struct ELevel {
   int nx = 0, ny = 0, nz = 0;
   DBuf<double> c64, w64, s64, b64;     // level >= 1 (level 0 borrows the session's)
-  DBuf<float> c32, w32, s32, b32;      // mixed precision copies
+  DBuf<double> d64;                    // inverse diagonal (every level)
+  DBuf<float> c32, w32, s32, b32, d32; // mixed precision copies
   EMat<double> m64{};
   EMat<float> m32{};
   long long ncell() const { return (long long)nx * ny * nz; }
@@ -49,6 +62,8 @@ struct EWork {
   DBuf<T> x0, r0, z0, pA, pB, q0;      // outer FCG on level 0
   DBuf<KScal> ks;                      // one per level
   DBuf<FcgScal> fs;
+  DBuf<char> bot;                      // level table of the bottom solver
+  size_t bot_smem = 0;                 // its dynamic shared memory
   cudaGraphExec_t iter_graph = nullptr;  // one captured FCG iteration
   size_t iter_nodes = 0;
   void ensure(const std::vector<ELevel> &lv);
@@ -58,7 +73,7 @@ struct EWork {
 
 struct EngineOpts {
   double omega = 0.8;        // damped-Jacobi weight
-  int coarse_max = 512;      // coarsest level size (dense direct solve)
+  int coarse_max = 64;       // coarsest level size (dense direct solve)
 };
 
 struct EngineResult {
@@ -88,15 +103,17 @@ class Engine {
                            int max_sweeps, int inner_maxit, RedPool &red, cudaStream_t s,
                            double *hist);
   int nlevels() const { return (int)L.size(); }
+  template <typename T> int bottom_level() const;
+  template <typename T> EMat<T> mat(int l) const;
   // Average duration (ms) of the fine-level smoothing sweep, `reps` launches
   // back to back between CUDA events on stream s; precision 0 FP64, 1 FP32.
   double bench_sweep(int precision, int reps, cudaStream_t s);
 
  private:
   template <typename T> void precond(int l, const T *r, T *z, bool dots, const T *u, double *out2,
-                                     EWork<T> &w, RedPool &red, const int *stop, cudaStream_t s);
+                                     EWork<T> &w, RedPool &red, const int *stop, cudaStream_t s,
+                                     bool kc);
   template <typename T> void kcycle(int l, EWork<T> &w, RedPool &red, const int *stop, cudaStream_t s);
-  template <typename T> EMat<T> mat(int l) const;
   template <typename T> int fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red,
                                 cudaStream_t s, double *hist, FcgScal *hfs);
 };

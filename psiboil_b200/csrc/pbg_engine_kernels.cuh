@@ -12,70 +12,92 @@
 
 namespace pbg {
 
-template <typename T>
-__device__ __forceinline__ T ax_at(const EMat<T> &A, long long p, Pos q, const T *__restrict__ x) {
-  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
-  T v = A.c[p] * x[p];
-  if (q.i > 0) v -= A.w[p] * x[p - SI];
-  if (q.i < A.nx - 1) v -= A.w[p + SI] * x[p + SI];
-  if (q.j > 0) v -= A.s[p] * x[p - SJ];
-  if (q.j < A.ny - 1) v -= A.s[p + SJ] * x[p + SJ];
-  if (q.k > 0) v -= A.b[p] * x[p - 1];
-  if (q.k < A.nz - 1) v -= A.b[p + 1] * x[p + 1];
-  return v;
-}
-
-// same with x given by a functor (values formed on the fly)
+// Off-diagonal part sum_nb a_nb x_nb of cell p (x given by a functor).
 template <typename T, typename XF>
-__device__ __forceinline__ T ax_f(const EMat<T> &A, long long p, Pos q, XF x) {
-  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
-  T v = A.c[p] * x(p);
-  if (q.i > 0) v -= A.w[p] * x(p - SI);
-  if (q.i < A.nx - 1) v -= A.w[p + SI] * x(p + SI);
-  if (q.j > 0) v -= A.s[p] * x(p - SJ);
-  if (q.j < A.ny - 1) v -= A.s[p + SJ] * x(p + SJ);
-  if (q.k > 0) v -= A.b[p] * x(p - 1);
-  if (q.k < A.nz - 1) v -= A.b[p + 1] * x(p + 1);
+__device__ __forceinline__ T offdiag(const EMat<T> &A, uint32_t p, Pos q, XF x) {
+  const uint32_t SI = A.g.nynz, SJ = (uint32_t)A.nz;
+  T v = 0;
+  if (q.i > 0) v += A.w[p] * x(p - SI);
+  if (q.i < A.nx - 1) v += A.w[p + SI] * x(p + SI);
+  if (q.j > 0) v += A.s[p] * x(p - SJ);
+  if (q.j < A.ny - 1) v += A.s[p + SJ] * x(p + SJ);
+  if (q.k > 0) v += A.b[p] * x(p - 1);
+  if (q.k < A.nz - 1) v += A.b[p + 1] * x(p + 1);
   return v;
 }
 
-#define GRID_LOOP(p, N)                                                          \
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < (N); \
-       p += (long long)gridDim.x * blockDim.x)
+// (A x)_p = c x_p - sum_nb a_nb x_nb
+template <typename T>
+__device__ __forceinline__ T ax_at(const EMat<T> &A, uint32_t p, Pos q, const T *__restrict__ x) {
+  return A.c[p] * x[p] - offdiag(A, p, q, [&](uint32_t s) { return x[s]; });
+}
+
+template <typename T, typename XF>
+__device__ __forceinline__ T ax_f(const EMat<T> &A, uint32_t p, Pos q, XF x) {
+  return A.c[p] * x(p) - offdiag(A, p, q, x);
+}
+
+#define GRID_LOOP(p, N)                                                       \
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < (uint32_t)(N); \
+       p += gridDim.x * blockDim.x)
 
 // ---------------------------------------------------------------- smoothers
-// x = omega r / c   (first damped-Jacobi sweep from a zero guess)
+// Damped Jacobi with the stored inverse diagonal:
+//   x' = x + w (D^-1 (r + sum_nb a_nb x_nb) - x)   (= x + w D^-1 (r - A x))
+
+// x = w D^-1 r   (first sweep from a zero guess)
 template <typename T>
-__global__ void k_jac0(EMat<T> A, const T *__restrict__ r, T *__restrict__ x, T omega,
+__global__ void __launch_bounds__(kThreads, 8) k_jac0(EMat<T> A, const T *__restrict__ r, T *__restrict__ x, T omega,
                        const int *stop) {
   if (stop && *stop) return;
-  const long long N = A.ncell();
-  GRID_LOOP(p, N) x[p] = omega * r[p] / A.c[p];
+  GRID_LOOP(p, A.g.n) x[p] = omega * r[p] * A.dinv[p];
 }
 
-// xo = xi + omega (r - A xi) / c
 template <typename T>
-__global__ void k_jac(EMat<T> A, const T *__restrict__ r, const T *__restrict__ xi,
+__global__ void __launch_bounds__(kThreads, 8) k_jac(EMat<T> A, const T *__restrict__ r, const T *__restrict__ xi,
                       T *__restrict__ xo, T omega, const int *stop) {
   if (stop && *stop) return;
-  const long long N = A.ncell();
-  GRID_LOOP(p, N) {
-    Pos q = pos_of(p, A.ny, A.nz);
-    T ax = ax_at(A, p, q, xi);
-    xo[p] = xi[p] + omega * (r[p] - ax) / A.c[p];
+  GRID_LOOP(p, A.g.n) {
+    Pos q = A.g.pos(p);
+    T on = offdiag(A, p, q, [&](uint32_t s) { return xi[s]; });
+    T xp = xi[p];
+    xo[p] = xp + omega * ((r[p] + on) * A.dinv[p] - xp);
+  }
+}
+
+// Two damped-Jacobi sweeps from a zero guess in one pass:
+//   x1 = w D^-1 r;  x2 = x1 + w (D^-1 (r + sum_nb a_nb x1_nb) - x1)
+// with x1 at the neighbours formed from r and D^-1 there. When ks is set the
+// right-hand side is the K-cycle residual r = b2 - a1 q2, formed on the fly
+// and stored to r_out for the later passes of the same cycle.
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 8)
+    k_jac2(EMat<T> A, const T *__restrict__ r, const T *__restrict__ b2, const T *__restrict__ q2,
+           const KScal *ks, T *__restrict__ r_out, T *__restrict__ xo, T omega, const int *stop) {
+  if (stop && *stop) return;
+  const T a1 = ks ? (T)ks->a1 : T(0);
+  auto rv = [&](uint32_t s) -> T { return ks ? b2[s] - a1 * q2[s] : r[s]; };
+  auto x1 = [&](uint32_t s) -> T { return omega * rv(s) * A.dinv[s]; };
+  GRID_LOOP(p, A.g.n) {
+    Pos q = A.g.pos(p);
+    const T rp = rv(p);
+    if (ks) r_out[p] = rp;
+    const T d = A.dinv[p];
+    const T xp = omega * rp * d;
+    const T on = offdiag(A, p, q, x1);
+    xo[p] = xp + omega * ((rp + on) * d - xp);
   }
 }
 
 // coarse rhs = block sums of the fine residual r - A x (restriction by the
 // transpose of piecewise-constant prolongation)
 template <typename T>
-__global__ void k_resid_restrict(EMat<T> A, const T *__restrict__ r, const T *__restrict__ x,
-                                 int Hnx, int Hny, int Hnz, T *__restrict__ rH, const int *stop) {
+__global__ void __launch_bounds__(kThreads, 8) k_resid_restrict(EMat<T> A, const T *__restrict__ r, const T *__restrict__ x,
+                                 Geo H, T *__restrict__ rH, const int *stop) {
   if (stop && *stop) return;
   const int fx = A.nx > 1 ? 2 : 1, fy = A.ny > 1 ? 2 : 1, fz = A.nz > 1 ? 2 : 1;
-  const long long NH = (long long)Hnx * Hny * Hnz;
-  GRID_LOOP(P, NH) {
-    Pos Q = pos_of(P, Hny, Hnz);
+  GRID_LOOP(P, H.n) {
+    Pos Q = H.pos(P);
     T sum = 0;
     for (int a = 0; a < fx; ++a) {
       int i = Q.i * fx + a;
@@ -86,7 +108,7 @@ __global__ void k_resid_restrict(EMat<T> A, const T *__restrict__ r, const T *__
         for (int cc = 0; cc < fz; ++cc) {
           int k = Q.k * fz + cc;
           if (k >= A.nz) break;
-          long long p = ((long long)i * A.ny + j) * A.nz + k;
+          uint32_t p = ((uint32_t)i * A.ny + j) * A.nz + k;
           sum += r[p] - ax_at(A, p, Pos{i, j, k}, x);
         }
       }
@@ -95,44 +117,51 @@ __global__ void k_resid_restrict(EMat<T> A, const T *__restrict__ r, const T *__
   }
 }
 
-// x' = xi + P e (prolongation of the coarse correction), then one sweep:
-// xo = x' + omega (r - A x') / c
+// x' = xi + P e (prolongation of the coarse correction), then one sweep.
+// e is the coarse array eH, or — after a K-cycle — e = c1 z1H + c2 z2H with
+// c1 = a1 - a2 beta, c2 = a2 from the coarse level's scalars ksH.
 template <typename T>
-__global__ void k_prolong_jac(EMat<T> A, const T *__restrict__ r, const T *__restrict__ xi,
-                              int Hny, int Hnz, const T *__restrict__ eH, T *__restrict__ xo,
-                              T omega, const int *stop) {
+__global__ void __launch_bounds__(kThreads, 8)
+    k_prolong_jac(EMat<T> A, const T *__restrict__ r, const T *__restrict__ xi, int Hny, int Hnz,
+                  const T *__restrict__ eH, const T *__restrict__ z2H, const KScal *ksH,
+                  T *__restrict__ xo, T omega, const int *stop) {
   if (stop && *stop) return;
-  const int fx = A.nx > 1 ? 2 : 1, fy = A.ny > 1 ? 2 : 1, fz = A.nz > 1 ? 2 : 1;
-  const long long N = A.ncell();
-  const long long nynz = (long long)A.ny * A.nz;
-  auto xp = [&](long long s) -> T {
-    int i = (int)(s / nynz);
-    long long rem = s - (long long)i * nynz;
-    int j = (int)(rem / A.nz), k = (int)(rem - (long long)j * A.nz);
-    return xi[s] + eH[((long long)(i / fx) * Hny + j / fy) * Hnz + k / fz];
+  const int sx = A.nx > 1 ? 1 : 0, sy = A.ny > 1 ? 1 : 0, sz = A.nz > 1 ? 1 : 0;
+  const uint32_t HnYZ = (uint32_t)Hny * Hnz;
+  T c1 = 1, c2 = 0;
+  if (ksH) { c1 = (T)(ksH->a1 - ksH->a2 * ksH->beta); c2 = (T)ksH->a2; }
+  auto e = [&](int i, int j, int k) -> T {
+    const uint32_t P = (uint32_t)(i >> sx) * HnYZ + (uint32_t)(j >> sy) * Hnz + (uint32_t)(k >> sz);
+    return ksH ? c1 * eH[P] + c2 * z2H[P] : eH[P];
   };
-  GRID_LOOP(p, N) {
-    Pos q = pos_of(p, A.ny, A.nz);
-    T xc = xp(p);
-    T ax = ax_f(A, p, q, xp);
-    xo[p] = xc + omega * (r[p] - ax) / A.c[p];
+  GRID_LOOP(p, A.g.n) {
+    Pos q = A.g.pos(p);
+    const uint32_t SI = A.g.nynz, SJ = (uint32_t)A.nz;
+    T on = 0;
+    if (q.i > 0) on += A.w[p] * (xi[p - SI] + e(q.i - 1, q.j, q.k));
+    if (q.i < A.nx - 1) on += A.w[p + SI] * (xi[p + SI] + e(q.i + 1, q.j, q.k));
+    if (q.j > 0) on += A.s[p] * (xi[p - SJ] + e(q.i, q.j - 1, q.k));
+    if (q.j < A.ny - 1) on += A.s[p + SJ] * (xi[p + SJ] + e(q.i, q.j + 1, q.k));
+    if (q.k > 0) on += A.b[p] * (xi[p - 1] + e(q.i, q.j, q.k - 1));
+    if (q.k < A.nz - 1) on += A.b[p + 1] * (xi[p + 1] + e(q.i, q.j, q.k + 1));
+    T xp = xi[p] + e(q.i, q.j, q.k);
+    xo[p] = xp + omega * ((r[p] + on) * A.dinv[p] - xp);
   }
 }
 
 // Last post-smoothing sweep of a preconditioner application with fused dot
-// products for the Krylov step that consumes z:
-//   z = xi + omega (r - A xi) / c;   d0 = z.r, d1 = z.u (u optional)
+// products for the Krylov step that consumes z:  d0 = z.r, d1 = z.u
 template <typename T>
-__global__ void k_jac_dots(EMat<T> A, const T *__restrict__ r, const T *__restrict__ xi,
+__global__ void __launch_bounds__(kThreads, 8) k_jac_dots(EMat<T> A, const T *__restrict__ r, const T *__restrict__ xi,
                            T *__restrict__ z, T omega, const T *__restrict__ u, double *out2,
                            double *part, unsigned *count, const int *stop) {
   if (stop && *stop) return;
-  const long long N = A.ncell();
   double v[2] = {0.0, 0.0};
-  GRID_LOOP(p, N) {
-    Pos q = pos_of(p, A.ny, A.nz);
-    T ax = ax_at(A, p, q, xi);
-    T zz = xi[p] + omega * (r[p] - ax) / A.c[p];
+  GRID_LOOP(p, A.g.n) {
+    Pos q = A.g.pos(p);
+    T on = offdiag(A, p, q, [&](uint32_t s) { return xi[s]; });
+    T xp = xi[p];
+    T zz = xp + omega * ((r[p] + on) * A.dinv[p] - xp);
     z[p] = zz;
     v[0] += (double)zz * (double)r[p];
     if (u) v[1] += (double)zz * (double)u[p];
@@ -140,7 +169,6 @@ __global__ void k_jac_dots(EMat<T> A, const T *__restrict__ r, const T *__restri
   double o[2];
   if (grid_reduce<2>(v, part, count, o)) { out2[0] = o[0]; out2[1] = o[1]; }
 }
-
 
 // ---------------------------------------------------------------- K-cycle
 // Two flexible-CG steps on a coarse level (Notay's K-cycle), with the
@@ -151,14 +179,13 @@ __global__ void k_jac_dots(EMat<T> A, const T *__restrict__ r, const T *__restri
 // p2.q2 = z2.v - 2 beta z2.q1 + beta^2 z1.q1 and z1.r1 = z1.b - a1 z1.q1
 // use the symmetry of A, so that q2 is never formed.
 template <typename T>
-__global__ void k_kc_q1(EMat<T> A, const T *__restrict__ z1, const T *__restrict__ b,
+__global__ void __launch_bounds__(kThreads, 8) k_kc_q1(EMat<T> A, const T *__restrict__ z1, const T *__restrict__ b,
                         T *__restrict__ q1, KScal *ks, double *part, unsigned *count,
                         const int *stop) {
   if (stop && *stop) return;
-  const long long N = A.ncell();
   double v[2] = {0.0, 0.0};
-  GRID_LOOP(p, N) {
-    Pos q = pos_of(p, A.ny, A.nz);
+  GRID_LOOP(p, A.g.n) {
+    Pos q = A.g.pos(p);
     T qq = ax_at(A, p, q, z1);
     q1[p] = qq;
     v[0] += (double)z1[p] * (double)b[p];
@@ -173,7 +200,7 @@ __global__ void k_kc_q1(EMat<T> A, const T *__restrict__ z1, const T *__restrict
 }
 
 template <typename T>
-__global__ void k_kc_r1(long long N, const T *__restrict__ b, const T *__restrict__ q1,
+__global__ void __launch_bounds__(kThreads, 8) k_kc_r1(long long N, const T *__restrict__ b, const T *__restrict__ q1,
                         T *__restrict__ r1, const KScal *ks, const int *stop) {
   if (stop && *stop) return;
   const T a1 = (T)ks->a1;
@@ -181,14 +208,13 @@ __global__ void k_kc_r1(long long N, const T *__restrict__ b, const T *__restric
 }
 
 template <typename T>
-__global__ void k_kc_q2(EMat<T> A, const T *__restrict__ z2, const T *__restrict__ q1,
+__global__ void __launch_bounds__(kThreads, 8) k_kc_q2(EMat<T> A, const T *__restrict__ z2, const T *__restrict__ q1,
                         const T *__restrict__ r1, T *__restrict__ vv, KScal *ks, double *part,
                         unsigned *count, const int *stop) {
   if (stop && *stop) return;
-  const long long N = A.ncell();
   double v[3] = {0.0, 0.0, 0.0};
-  GRID_LOOP(p, N) {
-    Pos q = pos_of(p, A.ny, A.nz);
+  GRID_LOOP(p, A.g.n) {
+    Pos q = A.g.pos(p);
     T av = ax_at(A, p, q, z2);
     vv[p] = av;
     double zz = (double)z2[p];
@@ -210,7 +236,7 @@ __global__ void k_kc_q2(EMat<T> A, const T *__restrict__ z2, const T *__restrict
 }
 
 template <typename T>
-__global__ void k_kc_x(long long N, const T *__restrict__ z1, const T *__restrict__ z2,
+__global__ void __launch_bounds__(kThreads, 8) k_kc_x(long long N, const T *__restrict__ z1, const T *__restrict__ z2,
                        T *__restrict__ x, const KScal *ks, const int *stop) {
   if (stop && *stop) return;
   const T c1 = (T)(ks->a1 - ks->a2 * ks->beta), c2 = (T)ks->a2;
@@ -240,7 +266,7 @@ __global__ void k_dense_solve(int n, const double *__restrict__ Ainv, const T *_
 // p is double-buffered by iteration parity; each thread forms p at its
 // neighbours from z and p_old.
 template <typename T>
-__global__ void k_fcg_pq(EMat<T> A, const T *__restrict__ z, T *pA, T *pB, T *__restrict__ qv,
+__global__ void __launch_bounds__(kThreads, 8) k_fcg_pq(EMat<T> A, const T *__restrict__ z, T *pA, T *pB, T *__restrict__ qv,
                          FcgScal *fs, double *part, unsigned *count) {
   if (fs->done) return;
   const int it = fs->iter;
@@ -248,11 +274,10 @@ __global__ void k_fcg_pq(EMat<T> A, const T *__restrict__ z, T *pA, T *pB, T *__
   T *pnew = (it & 1) ? pA : pB;
   const double betad = (it == 0 || !(fs->pq > 0.0)) ? 0.0 : fs->zq / fs->pq;
   const T beta = (T)betad;
-  auto pv = [&](long long s) -> T { return it == 0 ? z[s] : z[s] - beta * pold[s]; };
-  const long long N = A.ncell();
+  auto pv = [&](uint32_t s) -> T { return it == 0 ? z[s] : z[s] - beta * pold[s]; };
   double v[1] = {0.0};
-  GRID_LOOP(p, N) {
-    Pos q = pos_of(p, A.ny, A.nz);
+  GRID_LOOP(p, A.g.n) {
+    Pos q = A.g.pos(p);
     T pp = pv(p);
     T qq = ax_f(A, p, q, pv);
     pnew[p] = pp;
@@ -270,7 +295,7 @@ __global__ void k_fcg_pq(EMat<T> A, const T *__restrict__ z, T *pA, T *pB, T *__
 }
 
 template <typename T>
-__global__ void k_fcg_xr(long long N, T *__restrict__ x, T *__restrict__ r, const T *pA,
+__global__ void __launch_bounds__(kThreads, 8) k_fcg_xr(long long N, T *__restrict__ x, T *__restrict__ r, const T *pA,
                          const T *pB, const T *__restrict__ qv, FcgScal *fs,
                          double *part, unsigned *count) {
   if (fs->done) return;
@@ -301,7 +326,7 @@ __global__ void k_fcg_xr(long long N, T *__restrict__ x, T *__restrict__ r, cons
 
 // r = b, x = 0 (T), rr0 = |b|^2; fs set up for a new solve
 template <typename T>
-__global__ void k_fcg_init(long long N, const T *__restrict__ b, T *__restrict__ x,
+__global__ void __launch_bounds__(kThreads, 8) k_fcg_init(long long N, const T *__restrict__ b, T *__restrict__ x,
                            T *__restrict__ r, FcgScal *fs, double tol, int maxit, double *hist,
                            double *part, unsigned *count) {
   double v[1] = {0.0};
@@ -333,19 +358,18 @@ __global__ void k_fcg_init(long long N, const T *__restrict__ b, T *__restrict__
 // ---------------------------------------------------------------- refinement
 // x64 += e (T), elementwise
 template <typename T>
-__global__ void k_add_corr(long long N, double *__restrict__ x, const T *__restrict__ e) {
+__global__ void __launch_bounds__(kThreads, 8) k_add_corr(long long N, double *__restrict__ x, const T *__restrict__ e) {
   GRID_LOOP(p, N) x[p] += (double)e[p];
 }
 
 // r = b - A x in FP64, r32 = (T) r, out[0] = |r|^2, out[1] = |b|^2
 template <typename T>
-__global__ void k_true_resid(EMat<double> A, const double *__restrict__ x, const double *__restrict__ b,
+__global__ void __launch_bounds__(kThreads, 8) k_true_resid(EMat<double> A, const double *__restrict__ x, const double *__restrict__ b,
                              double *__restrict__ r, T *__restrict__ rT, double *out, double *part,
                              unsigned *count) {
-  const long long N = A.ncell();
   double v[2] = {0.0, 0.0};
-  GRID_LOOP(p, N) {
-    Pos q = pos_of(p, A.ny, A.nz);
+  GRID_LOOP(p, A.g.n) {
+    Pos q = A.g.pos(p);
     double rv = b[p] - ax_at(A, p, q, x);
     if (r) r[p] = rv;
     if (rT) rT[p] = (T)rv;
@@ -361,31 +385,32 @@ __global__ void k_true_resid(EMat<double> A, const double *__restrict__ x, const
 // in every direction with more than one cell (last block partial on odd
 // sizes): c_H = sum c - 2 sum(internal couplings), w_H / s_H / b_H = sum of
 // the couplings across the block's west / south / bottom face.
-__global__ void k_galerkin(EMat<double> A, int Hnx, int Hny, int Hnz, double *__restrict__ cH,
+__global__ void k_galerkin(EMat<double> A, Geo H, double *__restrict__ cH,
                            double *__restrict__ wH, double *__restrict__ sH, double *__restrict__ bH) {
   const int fx = A.nx > 1 ? 2 : 1, fy = A.ny > 1 ? 2 : 1, fz = A.nz > 1 ? 2 : 1;
-  const long long NH = (long long)Hnx * Hny * Hnz;
-  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
-  GRID_LOOP(P, NH) {
-    Pos Q = pos_of(P, Hny, Hnz);
+  GRID_LOOP(P, H.n) {
+    Pos Q = H.pos(P);
     double c = 0.0, w = 0.0, s = 0.0, b = 0.0;
     const int i0 = Q.i * fx, j0 = Q.j * fy, k0 = Q.k * fz;
     for (int a = 0; a < fx && i0 + a < A.nx; ++a)
       for (int bb = 0; bb < fy && j0 + bb < A.ny; ++bb)
         for (int cc = 0; cc < fz && k0 + cc < A.nz; ++cc) {
-          const long long p = ((long long)(i0 + a) * A.ny + (j0 + bb)) * A.nz + (k0 + cc);
+          const uint32_t p = ((uint32_t)(i0 + a) * A.ny + (j0 + bb)) * A.nz + (k0 + cc);
           c += A.c[p];
           if (a == 0) w += A.w[p]; else c -= 2.0 * A.w[p];
           if (bb == 0) s += A.s[p]; else c -= 2.0 * A.s[p];
           if (cc == 0) b += A.b[p]; else c -= 2.0 * A.b[p];
         }
-    (void)SI; (void)SJ;
     cH[P] = c; wH[P] = w; sH[P] = s; bH[P] = b;
   }
 }
 
 __global__ void k_to_float(long long N, const double *__restrict__ a, float *__restrict__ o) {
   GRID_LOOP(p, N) o[p] = (float)a[p];
+}
+
+__global__ void k_inverse(long long N, const double *__restrict__ c, double *__restrict__ d) {
+  GRID_LOOP(p, N) d[p] = 1.0 / c[p];
 }
 
 }  // namespace pbg
