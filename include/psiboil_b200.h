@@ -213,6 +213,24 @@ int pbg_session_stream(pbg_session *s, void **stream);
 int pbg_bench_kernel(pbg_session *s, int which, int precision, int reps, double *ms,
                      double *bytes_per_launch);
 
+/* Dot products without allocating (no counterpart in the reference).
+ * For callers that cannot call cudaMalloc where they need a dot product —
+ * code recorded into a CUDA graph by stream capture, callers whose device
+ * memory belongs to another allocator or pool, time-step loops that must not
+ * take an allocation's latency or failure path. Same results as pbg_dot:
+ * out[0] = x.y, out[1] = sum x*y/dV/dV / n / n, written to `out` (two
+ * doubles in device memory); x and y are device arrays of n doubles, on
+ * `stream` (a cudaStream_t, NULL for the default stream) of the current
+ * device. No session is needed and nothing is allocated: the scratch is a
+ * fixed array of about 19 KB in the library's device memory, held on every
+ * GPU that loads the library until the process exits; n must not exceed
+ * 2^31 - 1. Every call on a device shares that array and it keeps the last
+ * call's contents; calls that overlap on the GPU race and must be
+ * serialised. The first call on a device looks the array up for that device
+ * (make it before any stream capture). */
+int pbg_dot_noalloc(const double *x, const double *y, long long n, double dV, double *out,
+                    void *stream);
+
 #ifdef __cplusplus
 }
 #endif

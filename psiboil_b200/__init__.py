@@ -103,6 +103,7 @@ _SIGS = {
     "pbg_launch_count": (ctypes.c_ulonglong, []),
     "pbg_session_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
     "pbg_bench_kernel": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]),
+    "pbg_dot_noalloc": (ctypes.c_int, [_vp, _vp, _ll, ctypes.c_double, _vp, _vp]),
     "pbg_generate": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int),
                                     _dp, _vp, _vp, _vp]),
 }
@@ -147,6 +148,17 @@ def default_params(solver):
     p = Params()
     lib().pbg_params_default(ctypes.byref(p), solver)
     return p
+
+
+def dot_noalloc(x, y, dV, out, stream=None):
+    """pbg_dot_noalloc on CUDA tensors: out (2 doubles, device) = (x.y,
+    sum x*y/dV/dV / n / n); allocates nothing."""
+    n = x.numel()
+    if y.numel() != n or out.numel() < 2:
+        raise ValueError("x and y must have the same length, out at least 2")
+    h = stream.cuda_stream if stream is not None else None
+    _check(lib().pbg_dot_noalloc(x.data_ptr(), y.data_ptr(), n, dV, out.data_ptr(), h))
+    return out
 
 
 def launch_count():

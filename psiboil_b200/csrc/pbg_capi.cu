@@ -17,6 +17,7 @@ using namespace pbg;
 static thread_local std::string g_err;
 namespace pbg {
 unsigned long long g_launch_count = 0;
+void set_last_error(const char *msg) { g_err = msg; }
 }
 
 struct pbg_session {
