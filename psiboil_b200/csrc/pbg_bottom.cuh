@@ -21,6 +21,10 @@ namespace pbg {
 constexpr int kBotThreads = 1024;
 constexpr int kBotMaxLevels = 8;
 constexpr size_t kBotSmemMax = 200 * 1024;   // dynamic shared memory budget
+// Largest first level: one block keeps up with the launched kernels only on
+// levels of a few hundred cells (a 4096-cell K-cycle call is ~10M thread
+// instructions, about 150 us on one SM).
+constexpr long long kBotMaxCells = 512;
 
 template <typename T>
 struct BotLevel {
@@ -276,10 +280,13 @@ template <typename T>
 __global__ void __launch_bounds__(kBotThreads, 1) k_bottom(const BotCtx<T> *__restrict__ ctx,
                                                            const int *stop) {
   extern __shared__ __align__(16) char bot_smem[];
-  __shared__ EMat<T> views[kBotMaxLevels];
-  __shared__ BotVec<T> vecs[kBotMaxLevels];
+  // raw storage (the view types have constructors, which shared variables
+  // do not run; thread 0 fills them)
+  __shared__ __align__(16) char views_raw[sizeof(EMat<T>) * kBotMaxLevels];
+  __shared__ __align__(16) char vecs_raw[sizeof(BotVec<T>) * kBotMaxLevels];
   if (stop && *stop) return;
-  Bottom<T> B(*ctx, bot_smem, views, vecs);
+  Bottom<T> B(*ctx, bot_smem, reinterpret_cast<EMat<T> *>(views_raw),
+              reinterpret_cast<BotVec<T> *>(vecs_raw));
   __syncthreads();
   B.load();
   B.template kcycle<0>();

@@ -1,12 +1,14 @@
 // Host side of the engine solver (hierarchy set-up, K-cycle recursion,
 // flexible CG and the mixed-precision refinement loop).
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
 #include "pbg_engine.cuh"
 #include "pbg_engine_kernels.cuh"
 #include "pbg_bottom.cuh"
+#include "pbg_vec.cuh"
 
 namespace pbg {
 
@@ -25,6 +27,7 @@ void EWork<T>::ensure(const std::vector<ELevel> &lv) {
   }
   size_t n0 = (size_t)lv[0].ncell();
   x0.alloc(n0); r0.alloc(n0); z0.alloc(n0); pA.alloc(n0); pB.alloc(n0); q0.alloc(n0);
+  q0b.alloc(n0);
   ks.alloc(lv.size());
   fs.alloc(1);
   PBG_CUDA(cudaMemset(fs.p, 0, sizeof(FcgScal)));
@@ -35,6 +38,18 @@ void EWork<T>::drop_graph() {
   if (iter_graph) cudaGraphExecDestroy(iter_graph);
   iter_graph = nullptr;
   iter_nodes = 0;
+}
+
+// Tuning knobs (environment): PBG_BLOCK_BOTTOM=1 enables the single-block
+// shared-memory solver for the coarse tail of the K-cycle (levels of at most
+// kBotMaxCells cells above a smaller dense level; measured slower than
+// launched kernels with the default 512-cell dense level); PBG_COARSE_MAX
+// sets the size of the dense coarsest level.
+EngineOpts::EngineOpts() {
+  const char *e = getenv("PBG_BLOCK_BOTTOM");
+  block_bottom = e && e[0] == '1';
+  const char *c = getenv("PBG_COARSE_MAX");
+  if (c && atoi(c) > 0) coarse_max = atoi(c);
 }
 
 template struct EWork<double>;
@@ -176,8 +191,11 @@ static size_t bottom_smem(const Engine &E, int l) {
 template <typename T>
 int Engine::bottom_level() const {
   const int last = (int)L.size() - 1;
+  if (!opt.block_bottom) return (int)L.size();
   for (int l = 1; l < last; ++l)
-    if (last - l < kBotMaxLevels && bottom_smem<T>(*this, l) <= kBotSmemMax) return l;
+    if (L[l].ncell() <= kBotMaxCells && last - l < kBotMaxLevels &&
+        bottom_smem<T>(*this, l) <= kBotSmemMax)
+      return l;
   return (int)L.size();
 }
 
@@ -244,8 +262,15 @@ void Engine::precond(int l, const T *r, T *z, bool dots, const T *u, double *out
   const ELevel &H = L[l + 1];
   auto &vh = w.L[l + 1];
   const T *rr = kc ? v.r1.p : r;
-  k_jac2<T><<<g, kThreads, 0, s>>>(A, r, v.b.p, v.q1.p, kc ? w.ks.p + l : nullptr, v.r1.p, v.xb.p,
-                                   om, stop); note_launch();
+  const bool vec = A.nz % VecTraits<T>::V == 0;
+  const int gv = grid_for(A.ncell() / VecTraits<T>::V, kThreads, kVecBlocks);
+  if (vec) {
+    kv_jac2<T><<<gv, kThreads, 0, s>>>(A, r, v.b.p, v.q1.p, kc ? w.ks.p + l : nullptr, v.r1.p,
+                                       v.xb.p, om, stop); note_launch();
+  } else {
+    k_jac2<T><<<g, kThreads, 0, s>>>(A, r, v.b.p, v.q1.p, kc ? w.ks.p + l : nullptr, v.r1.p, v.xb.p,
+                                     om, stop); note_launch();
+  }
   k_resid_restrict<T><<<grid_for(H.ncell()), kThreads, 0, s>>>(A, rr, v.xb.p, Geo(H.nx, H.ny, H.nz),
                                                                vh.b.p, stop); note_launch();
   const T *eH, *z2H = nullptr;
@@ -259,11 +284,23 @@ void Engine::precond(int l, const T *r, T *z, bool dots, const T *u, double *out
     else kcycle<T>(l + 1, w, red, stop, s);
     eH = vh.z1.p; z2H = vh.z2.p; ksH = w.ks.p + l + 1;
   }
-  k_prolong_jac<T><<<g, kThreads, 0, s>>>(A, rr, v.xb.p, H.ny, H.nz, eH, z2H, ksH, v.xa.p, om,
-                                          stop); note_launch();
-  if (dots) {
+  if (vec) {
+    kv_prolong_jac<T><<<gv, kThreads, 0, s>>>(A, rr, v.xb.p, H.ny, H.nz, eH, z2H, ksH, v.xa.p, om,
+                                              stop); note_launch();
+  } else {
+    k_prolong_jac<T><<<g, kThreads, 0, s>>>(A, rr, v.xb.p, H.ny, H.nz, eH, z2H, ksH, v.xa.p, om,
+                                            stop); note_launch();
+  }
+  if (dots && vec && l == 0) {
+    // u is the q of the previous FCG iteration, picked by parity on the device
+    kv_jac<T, true><<<gv, kThreads, 0, s>>>(A, rr, v.xa.p, z, om, w.q0.p, w.q0b.p, w.fs.p, out2,
+                                            red.slot_part(0), red.slot_count(0), stop); note_launch();
+  } else if (dots) {
     k_jac_dots<T><<<g, kThreads, 0, s>>>(A, rr, v.xa.p, z, om, u, out2, red.slot_part(0),
                                          red.slot_count(0), stop); note_launch();
+  } else if (vec) {
+    kv_jac<T, false><<<gv, kThreads, 0, s>>>(A, rr, v.xa.p, z, om, nullptr, nullptr, nullptr,
+                                             nullptr, nullptr, nullptr, stop); note_launch();
   } else {
     k_jac<T><<<g, kThreads, 0, s>>>(A, rr, v.xa.p, z, om, stop); note_launch();
   }
@@ -301,10 +338,18 @@ int Engine::fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red, cu
     PBG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     try {
       precond<T>(0, w.r0.p, w.z0.p, true, w.q0.p, &fs->zr, w, red, stop, s, false);
-      k_fcg_pq<T><<<g, kThreads, 0, s>>>(A, w.z0.p, w.pA.p, w.pB.p, w.q0.p, fs, red.slot_part(0),
-                                         red.slot_count(0)); note_launch();
-      k_fcg_xr<T><<<g, kThreads, 0, s>>>(N, w.x0.p, w.r0.p, w.pA.p, w.pB.p, w.q0.p, fs,
-                                         red.slot_part(0), red.slot_count(0)); note_launch();
+      if (A.nz % VecTraits<T>::V == 0 && (int)L.size() > 1) {
+        const int gv = grid_for(N / VecTraits<T>::V, kThreads, kVecBlocks);
+        kv_fcg_pq<T><<<gv, kThreads, 0, s>>>(A, w.z0.p, w.pA.p, w.pB.p, w.q0.p, w.q0b.p, fs,
+                                             red.slot_part(0), red.slot_count(0)); note_launch();
+        kv_fcg_xr<T><<<gv, kThreads, 0, s>>>(N, w.x0.p, w.r0.p, w.pA.p, w.pB.p, w.q0.p, w.q0b.p, fs,
+                                             red.slot_part(0), red.slot_count(0)); note_launch();
+      } else {
+        k_fcg_pq<T><<<g, kThreads, 0, s>>>(A, w.z0.p, w.pA.p, w.pB.p, w.q0.p, fs, red.slot_part(0),
+                                           red.slot_count(0)); note_launch();
+        k_fcg_xr<T><<<g, kThreads, 0, s>>>(N, w.x0.p, w.r0.p, w.pA.p, w.pB.p, w.q0.p, fs,
+                                           red.slot_part(0), red.slot_count(0)); note_launch();
+      }
     } catch (...) {
       cudaStreamEndCapture(s, &graph);  // leave the stream usable
       if (graph) cudaGraphDestroy(graph);
@@ -317,6 +362,7 @@ int Engine::fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red, cu
     cudaGraphDestroy(graph);
   }
   PBG_CUDA(cudaMemsetAsync(w.q0.p, 0, sizeof(T) * N, s));
+  PBG_CUDA(cudaMemsetAsync(w.q0b.p, 0, sizeof(T) * N, s));
   k_fcg_init<T><<<g, kThreads, 0, s>>>(N, b, w.x0.p, w.r0.p, fs, tol, maxit, hist,
                                        red.slot_part(0), red.slot_count(0)); note_launch();
   PBG_CUDA(cudaGetLastError());
@@ -409,17 +455,27 @@ EngineResult Engine::solve_mixed(double *x, const double *b, double tol, double 
   return res;
 }
 
+// Times the fine-level smoothing sweep the solver launches: the vectorised
+// kv_jac when the rows allow it, else the scalar k_jac.
 template <typename T>
 static double time_sweeps(const EMat<T> &A, const T *r, T *xa, T *xb, T om, int reps, cudaStream_t s) {
   cudaEvent_t e0, e1;
   PBG_CUDA(cudaEventCreate(&e0));
   PBG_CUDA(cudaEventCreate(&e1));
+  const bool vec = A.nz % VecTraits<T>::V == 0;
   const int g = grid_for(A.ncell());
-  k_jac<T><<<g, kThreads, 0, s>>>(A, r, xa, xb, om, nullptr); note_launch();
+  const int gv = grid_for(A.ncell() / VecTraits<T>::V, kThreads, kVecBlocks);
+  auto sweep = [&](const T *xi, T *xo) {
+    if (vec)
+      kv_jac<T, false><<<gv, kThreads, 0, s>>>(A, r, xi, xo, om, nullptr, nullptr, nullptr, nullptr,
+                                               nullptr, nullptr, nullptr);
+    else
+      k_jac<T><<<g, kThreads, 0, s>>>(A, r, xi, xo, om, nullptr);
+    note_launch();
+  };
+  sweep(xa, xb);
   PBG_CUDA(cudaEventRecord(e0, s));
-  for (int q = 0; q < reps; ++q) {
-    k_jac<T><<<g, kThreads, 0, s>>>(A, r, (q & 1) ? xb : xa, (q & 1) ? xa : xb, om, nullptr); note_launch();
-  }
+  for (int q = 0; q < reps; ++q) sweep((q & 1) ? xb : xa, (q & 1) ? xa : xb);
   PBG_CUDA(cudaEventRecord(e1, s));
   PBG_CUDA(cudaEventSynchronize(e1));
   float ms = 0.f;

@@ -59,7 +59,7 @@ struct EWork {
     DBuf<T> b, x, z1, z2, q1, r1, v, xa, xb;
   };
   std::vector<Lv> L;
-  DBuf<T> x0, r0, z0, pA, pB, q0;      // outer FCG on level 0
+  DBuf<T> x0, r0, z0, pA, pB, q0, q0b; // outer FCG on level 0 (q0/q0b: q by parity)
   DBuf<KScal> ks;                      // one per level
   DBuf<FcgScal> fs;
   DBuf<char> bot;                      // level table of the bottom solver
@@ -73,7 +73,9 @@ struct EWork {
 
 struct EngineOpts {
   double omega = 0.8;        // damped-Jacobi weight
-  int coarse_max = 64;       // coarsest level size (dense direct solve)
+  int coarse_max = 512;      // coarsest level size (dense direct solve)
+  bool block_bottom = false; // run the coarse K-cycle tail in one block (k_bottom)
+  EngineOpts();
 };
 
 struct EngineResult {
