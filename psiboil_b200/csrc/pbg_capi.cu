@@ -320,7 +320,8 @@ int pbg_matrix_upload(pbg_session *s, const double *c, const double *w, const do
         }
     Mat64 &A = s->A;
     A.nx = nx; A.ny = ny; A.nz = nz; A.sym = sym;
-    A.c.alloc(N); A.w.alloc(N); A.s.alloc(N); A.b.alloc(N);
+    // same-size uploads keep the buffers (the engine then refreshes in place)
+    if (A.c.n != (size_t)N) { A.c.alloc(N); A.w.alloc(N); A.s.alloc(N); A.b.alloc(N); }
     if (sym) { A.e.release(); A.n.release(); A.t.release(); }
     else { A.e.alloc(N); A.n.alloc(N); A.t.alloc(N); }
     DBuf<double> *dst[7] = {&A.c, &A.w, &A.e, &A.s, &A.n, &A.b, &A.t};
@@ -430,6 +431,11 @@ void ensure_engine(pbg_session *s, bool mixed) {
   if (s->eng_dirty || (mixed && !s->eng->have32)) {
     const Mat64 &A = s->A;
     EMat<double> m = make_emat<double>(A.nx, A.ny, A.nz, A.c.p, A.w.p, A.s.p, A.b.p, nullptr);
+    // same shape and buffers (a re-assembled matrix): numeric refresh only
+    if (s->eng->refresh(m, mixed, s->stream)) {
+      s->eng_dirty = false;
+      return;
+    }
     s->eng->build(m, s->stream, mixed || s->eng_mixed);
     s->eng_mixed = s->eng_mixed || mixed;
     s->eng_dirty = false;

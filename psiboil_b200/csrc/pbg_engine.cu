@@ -62,46 +62,6 @@ Engine::~Engine() {
 template <> EMat<double> Engine::mat<double>(int l) const { return L[l].m64; }
 template <> EMat<float> Engine::mat<float>(int l) const { return L[l].m32; }
 
-// Dense inverse of the coarsest operator by Cholesky. A pivot below
-// 1e-10 x the largest diagonal (a solid-only aggregate, or the constant
-// mode of an all-Neumann problem) is skipped: that unknown is held at zero,
-// which gives a generalised inverse for a consistent singular system.
-static void dense_spd_inverse(int n, std::vector<double> &A) {
-  std::vector<double> Lm((size_t)n * n, 0.0);
-  std::vector<char> skip(n, 0);
-  double dmax = 0.0;
-  for (int i = 0; i < n; ++i) dmax = std::fmax(dmax, A[(size_t)i * n + i]);
-  for (int j = 0; j < n; ++j) {
-    double d = A[(size_t)j * n + j];
-    for (int k = 0; k < j; ++k) d -= Lm[(size_t)j * n + k] * Lm[(size_t)j * n + k];
-    if (!(d > 1e-10 * dmax)) { skip[j] = 1; continue; }
-    double ljj = std::sqrt(d);
-    Lm[(size_t)j * n + j] = ljj;
-    for (int i = j + 1; i < n; ++i) {
-      double v = A[(size_t)i * n + j];
-      for (int k = 0; k < j; ++k) v -= Lm[(size_t)i * n + k] * Lm[(size_t)j * n + k];
-      Lm[(size_t)i * n + j] = v / ljj;
-    }
-  }
-  std::vector<double> inv((size_t)n * n, 0.0), y(n);
-  for (int c = 0; c < n; ++c) {
-    for (int i = 0; i < n; ++i) {  // L y = e_c
-      if (skip[i]) { y[i] = 0.0; continue; }
-      double v = (i == c) ? 1.0 : 0.0;
-      for (int k = 0; k < i; ++k) v -= Lm[(size_t)i * n + k] * y[k];
-      y[i] = v / Lm[(size_t)i * n + i];
-    }
-    for (int i = n - 1; i >= 0; --i) {  // L^T x = y
-      if (skip[i]) { y[i] = 0.0; continue; }
-      double v = y[i];
-      for (int k = i + 1; k < n; ++k) v -= Lm[(size_t)k * n + i] * y[k];
-      y[i] = v / Lm[(size_t)i * n + i];
-    }
-    for (int i = 0; i < n; ++i) inv[(size_t)i * n + c] = y[i];
-  }
-  A.swap(inv);
-}
-
 void Engine::build(const EMat<double> &A0, cudaStream_t s, bool mixed) {
   w64.drop_graph();
   w32.drop_graph();
@@ -114,9 +74,7 @@ void Engine::build(const EMat<double> &A0, cudaStream_t s, bool mixed) {
   {
     ELevel &l0 = L[0];
     l0.nx = A0.nx; l0.ny = A0.ny; l0.nz = A0.nz;
-    long long n0 = l0.ncell();
-    l0.d64.alloc(n0);
-    k_inverse<<<grid_for(n0), kThreads, 0, s>>>(n0, A0.c, l0.d64.p); note_launch();
+    l0.d64.alloc(l0.ncell());
     l0.m64 = make_emat<double>(A0.nx, A0.ny, A0.nz, A0.c, A0.w, A0.s, A0.b, l0.d64.p);
   }
   while (L.back().ncell() > opt.coarse_max &&
@@ -128,53 +86,72 @@ void Engine::build(const EMat<double> &A0, cudaStream_t s, bool mixed) {
     c.nz = f.nz > 1 ? (f.nz + 1) / 2 : 1;
     long long n = c.ncell();
     c.c64.alloc(n); c.w64.alloc(n); c.s64.alloc(n); c.b64.alloc(n); c.d64.alloc(n);
-    k_galerkin<<<grid_for(n), kThreads, 0, s>>>(f.m64, Geo(c.nx, c.ny, c.nz), c.c64.p, c.w64.p,
-                                                 c.s64.p, c.b64.p); note_launch();
-    k_inverse<<<grid_for(n), kThreads, 0, s>>>(n, c.c64.p, c.d64.p); note_launch();
-    PBG_CUDA(cudaGetLastError());
     c.m64 = make_emat<double>(c.nx, c.ny, c.nz, c.c64.p, c.w64.p, c.s64.p, c.b64.p, c.d64.p);
     L.push_back(std::move(c));
   }
-  // dense inverse of the coarsest level
-  const ELevel &cl = L.back();
-  const int n = (int)cl.ncell();
-  ncoarse = n;
-  std::vector<double> hc(n), hw(n), hs(n), hb(n);
-  PBG_CUDA(cudaMemcpyAsync(hc.data(), cl.m64.c, n * 8, cudaMemcpyDeviceToHost, s));
-  PBG_CUDA(cudaMemcpyAsync(hw.data(), cl.m64.w, n * 8, cudaMemcpyDeviceToHost, s));
-  PBG_CUDA(cudaMemcpyAsync(hs.data(), cl.m64.s, n * 8, cudaMemcpyDeviceToHost, s));
-  PBG_CUDA(cudaMemcpyAsync(hb.data(), cl.m64.b, n * 8, cudaMemcpyDeviceToHost, s));
-  PBG_CUDA(cudaStreamSynchronize(s));
-  std::vector<double> D((size_t)n * n, 0.0);
-  const int SI = cl.ny * cl.nz, SJ = cl.nz;
-  for (int i = 0; i < cl.nx; ++i)
-    for (int j = 0; j < cl.ny; ++j)
-      for (int k = 0; k < cl.nz; ++k) {
-        int p = (i * cl.ny + j) * cl.nz + k;
-        D[(size_t)p * n + p] = hc[p];
-        if (i > 0) { D[(size_t)p * n + p - SI] = -hw[p]; D[(size_t)(p - SI) * n + p] = -hw[p]; }
-        if (j > 0) { D[(size_t)p * n + p - SJ] = -hs[p]; D[(size_t)(p - SJ) * n + p] = -hs[p]; }
-        if (k > 0) { D[(size_t)p * n + p - 1] = -hb[p]; D[(size_t)(p - 1) * n + p] = -hb[p]; }
-      }
-  dense_spd_inverse(n, D);
-  Ainv.alloc((size_t)n * n);
-  PBG_CUDA(cudaMemcpy(Ainv.p, D.data(), D.size() * 8, cudaMemcpyHostToDevice));
+  ncoarse = (int)L.back().ncell();
+  Ainv.alloc((size_t)ncoarse * ncoarse);
+  Dtmp.alloc((size_t)ncoarse * ncoarse);
   have32 = false;
   if (mixed) {
     for (auto &lv : L) {
       long long m = lv.ncell();
       lv.c32.alloc(m); lv.w32.alloc(m); lv.s32.alloc(m); lv.b32.alloc(m); lv.d32.alloc(m);
-      const double *src[5] = {lv.m64.c, lv.m64.w, lv.m64.s, lv.m64.b, lv.m64.dinv};
-      float *dst[5] = {lv.c32.p, lv.w32.p, lv.s32.p, lv.b32.p, lv.d32.p};
-      for (int q = 0; q < 5; ++q) { k_to_float<<<grid_for(m), kThreads, 0, s>>>(m, src[q], dst[q]); note_launch(); }
       lv.m32 = make_emat<float>(lv.nx, lv.ny, lv.nz, lv.c32.p, lv.w32.p, lv.s32.p, lv.b32.p, lv.d32.p);
     }
-    PBG_CUDA(cudaGetLastError());
     have32 = true;
   }
   if (!hsc) PBG_CUDA(cudaMallocHost((void **)&hsc, 64 * sizeof(double)));
   if (dsc.n < 8) dsc.alloc(8);
+  compute(s);
   PBG_CUDA(cudaStreamSynchronize(s));
+}
+
+// Numeric set-up on the allocated hierarchy, all on the device: inverse
+// diagonals, Galerkin coarse operators, FP32 copies and the dense inverse of
+// the coarsest level. Used by build() and again after the fine matrix
+// changed in place: buffers, and so the captured iteration graphs, stay
+// valid. Enqueued on s, no host synchronisation.
+void Engine::compute(cudaStream_t s) {
+  auto out = [&](ELevel &lv) {
+    LevelOut o{const_cast<double *>(lv.m64.c),
+               const_cast<double *>(lv.m64.w), const_cast<double *>(lv.m64.s),
+               const_cast<double *>(lv.m64.b), lv.d64.p,
+               nullptr, nullptr, nullptr, nullptr, nullptr};
+    if (have32) { o.c32 = lv.c32.p; o.w32 = lv.w32.p; o.s32 = lv.s32.p; o.b32 = lv.b32.p; o.d32 = lv.d32.p; }
+    return o;
+  };
+  k_level_finish<<<grid_for(L[0].ncell()), kThreads, 0, s>>>(L[0].m64, out(L[0])); note_launch();
+  for (size_t l = 1; l < L.size(); ++l) {
+    ELevel &c = L[l];
+    k_galerkin<<<grid_for(c.ncell()), kThreads, 0, s>>>(L[l - 1].m64, Geo(c.nx, c.ny, c.nz), out(c));
+    note_launch();
+  }
+  // dense inverse of the coarsest operator: blocked Gauss-Jordan, out of place
+  const int n = ncoarse;
+  const size_t nn = (size_t)n * n;
+  PBG_CUDA(cudaMemsetAsync(Dtmp.p, 0, nn * sizeof(double), s));
+  k_dense_fill<<<grid_for(n), kThreads, 0, s>>>(L.back().m64, Dtmp.p); note_launch();
+  k_dense_dmax<<<1, 1024, 0, s>>>(n, Dtmp.p, dsc.p + 7); note_launch();
+  double *src = Dtmp.p, *dst = Ainv.p;
+  const int tiles = (n + kGjRows - 1) / kGjRows;
+  for (int k0 = 0; k0 < n; k0 += kGjB) {
+    k_gj_block<<<tiles, kGjRows * kGjB, 0, s>>>(n, k0, src, dst, dsc.p + 7, 1e-10); note_launch();
+    std::swap(src, dst);
+  }
+  if (src != Ainv.p)
+    PBG_CUDA(cudaMemcpyAsync(Ainv.p, src, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  PBG_CUDA(cudaGetLastError());
+}
+
+// Numeric refresh for a changed fine matrix of the same shape at the same
+// addresses; false if the hierarchy has to be built anew.
+bool Engine::refresh(const EMat<double> &A0, bool mixed, cudaStream_t s) {
+  if (L.empty() || (mixed && !have32) || L[0].nx != A0.nx || L[0].ny != A0.ny || L[0].nz != A0.nz ||
+      L[0].m64.c != A0.c || L[0].m64.w != A0.w || L[0].m64.s != A0.s || L[0].m64.b != A0.b)
+    return false;
+  compute(s);
+  return true;
 }
 
 // Shared-memory bytes the bottom solver needs when it starts at level l.

@@ -87,6 +87,7 @@ class Engine {
  public:
   std::vector<ELevel> L;
   DBuf<double> Ainv;           // dense inverse of the coarsest operator
+  DBuf<double> Dtmp;           // its Gauss-Jordan work copy
   int ncoarse = 0;
   bool have32 = false;
   EngineOpts opt;
@@ -97,6 +98,8 @@ class Engine {
 
   ~Engine();
   void build(const EMat<double> &A0, cudaStream_t s, bool mixed);
+  void compute(cudaStream_t s);
+  bool refresh(const EMat<double> &A0, bool mixed, cudaStream_t s);
   // Plain FP64: FCG + FP64 K-cycle to |r|/|b| <= tol.
   EngineResult solve_fp64(double *x, const double *b, double tol, int maxit, RedPool &red,
                           cudaStream_t s, double *hist);

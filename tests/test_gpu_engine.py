@@ -75,3 +75,31 @@ def test_device_arrays(engine, oracle):
         engine.Engine(s).solve(xd, bd, precision=1)
         x = xd.cpu().numpy()
     assert true_relres(oracle, P, x) <= 1e-8 * 1.0001
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_refresh_equals_fresh_build(engine, oracle, precision):
+    """A re-assembled matrix of the same shape reuses the hierarchy's buffers
+    (numeric refresh on the device, the dense coarsest inverse included) and
+    gives bit-for-bit the solution of a session built for that matrix."""
+    P1 = oracle.Problem(1, 3, n=32, nb=4, rmin=2.0, rmax=4.0, rc=6.0)
+    P2 = oracle.Problem(1, 8, n=32, nb=5, rmin=2.0, rmax=5.0, rc=7.0)
+    assert P1.dims == P2.dims
+    with engine.Session(*P1.dims, P1.h) as s:
+        E = engine.Engine(s)
+        s.assemble_pressure(P1.rho, P1.solid)
+        x1 = np.zeros(P1.N)
+        assert E.solve(x1, P1.b.copy(), precision=precision)
+        s.assemble_pressure(P2.rho, P2.solid)
+        xa = np.zeros(P2.N)
+        assert E.solve(xa, P2.b.copy(), precision=precision)
+        ita = E.last.iterations
+    with engine.Session(*P2.dims, P2.h) as s:
+        s.assemble_pressure(P2.rho, P2.solid)
+        E = engine.Engine(s)
+        xb = np.zeros(P2.N)
+        assert E.solve(xb, P2.b.copy(), precision=precision)
+        itb = E.last.iterations
+    assert ita == itb
+    assert np.array_equal(xa, xb)
+    assert true_relres(oracle, P2, xa) <= 1e-8 * 1.0001
