@@ -7,7 +7,6 @@
 
 #include "pbg_engine.cuh"
 #include "pbg_engine_kernels.cuh"
-#include "pbg_bottom.cuh"
 #include "pbg_vec.cuh"
 
 namespace pbg {
@@ -16,7 +15,6 @@ template <typename T>
 void EWork<T>::ensure(const std::vector<ELevel> &lv) {
   if (L.size() == lv.size() && x0.n == (size_t)lv[0].ncell()) return;
   drop_graph();
-  bot.release();
   L.clear();
   L.resize(lv.size());
   for (size_t l = 0; l < lv.size(); ++l) {
@@ -40,14 +38,9 @@ void EWork<T>::drop_graph() {
   iter_nodes = 0;
 }
 
-// Tuning knobs (environment): PBG_BLOCK_BOTTOM=1 enables the single-block
-// shared-memory solver for the coarse tail of the K-cycle (levels of at most
-// kBotMaxCells cells above a smaller dense level; measured slower than
-// launched kernels with the default 512-cell dense level); PBG_COARSE_MAX
-// sets the size of the dense coarsest level.
+// Tuning knob (environment): PBG_COARSE_MAX sets the size of the dense
+// coarsest level.
 EngineOpts::EngineOpts() {
-  const char *e = getenv("PBG_BLOCK_BOTTOM");
-  block_bottom = e && e[0] == '1';
   const char *c = getenv("PBG_COARSE_MAX");
   if (c && atoi(c) > 0) coarse_max = atoi(c);
 }
@@ -67,8 +60,6 @@ void Engine::build(const EMat<double> &A0, cudaStream_t s, bool mixed) {
   w32.drop_graph();
   w64.L.clear();
   w32.L.clear();
-  w64.bot.release();
-  w32.bot.release();
   L.clear();
   L.emplace_back();
   {
@@ -154,67 +145,6 @@ bool Engine::refresh(const EMat<double> &A0, bool mixed, cudaStream_t s) {
   return true;
 }
 
-// Shared-memory bytes the bottom solver needs when it starts at level l.
-template <typename T>
-static size_t bottom_smem(const Engine &E, int l) {
-  size_t b = bot_level_bytes<T>(E.L[l].ncell(), false);
-  for (int m = l + 1; m < (int)E.L.size(); ++m) b += bot_level_bytes<T>(E.L[m].ncell(), true);
-  return b + (size_t)E.ncoarse * E.ncoarse * sizeof(double);
-}
-
-// First level handled by the shared-memory bottom solver: the first level
-// below level 0 whose work set (and that of every coarser level) fits the
-// shared-memory budget and the solver's level table; L.size() if none.
-template <typename T>
-int Engine::bottom_level() const {
-  const int last = (int)L.size() - 1;
-  if (!opt.block_bottom) return (int)L.size();
-  for (int l = 1; l < last; ++l)
-    if (L[l].ncell() <= kBotMaxCells && last - l < kBotMaxLevels &&
-        bottom_smem<T>(*this, l) <= kBotSmemMax)
-      return l;
-  return (int)L.size();
-}
-
-// Level table of the bottom solver, uploaded once per work set (before any
-// graph capture: it allocates).
-template <typename T>
-static void ensure_bottom(const Engine &E, EWork<T> &w) {
-  const int first = E.bottom_level<T>();
-  if (w.bot.p || first >= (int)E.L.size()) return;
-  BotCtx<T> C;
-  memset(&C, 0, sizeof(C));
-  C.first = first;
-  C.last = (int)E.L.size() - 1;
-  uint32_t off = 0;
-  for (int l = first; l <= C.last; ++l) {
-    BotLevel<T> &B = C.L[l - first];
-    B.A = E.template mat<T>(l);
-    B.ks = w.ks.p + l;
-    auto &v = w.L[l];
-    B.gb = v.b.p; B.gz1 = v.z1.p; B.gz2 = v.z2.p;
-    B.off = off;
-    B.smem_matrix = l > first ? 1 : 0;
-    off += (uint32_t)bot_level_bytes<T>(E.L[l].ncell(), l > first);
-  }
-  C.ainv_off = off;
-  off += (uint32_t)((size_t)E.ncoarse * E.ncoarse * sizeof(double));
-  C.smem_bytes = off;
-  C.Ainv = E.Ainv.p;
-  C.ncoarse = E.ncoarse;
-  C.omega = (T)E.opt.omega;
-  PBG_CUDA(cudaFuncSetAttribute(k_bottom<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)off));
-  w.bot.alloc(sizeof(C));
-  w.bot_smem = off;
-  PBG_CUDA(cudaMemcpy(w.bot.p, &C, sizeof(C), cudaMemcpyHostToDevice));
-}
-
-template <typename T>
-static void launch_bottom(EWork<T> &w, const int *stop, cudaStream_t s) {
-  if (!w.bot.p) throw CudaError("bottom solver table not prepared");
-  k_bottom<T><<<1, kBotThreads, w.bot_smem, s>>>((const BotCtx<T> *)w.bot.p, stop); note_launch();
-}
-
 // Preconditioner M r -> z on level l. kc: the K-cycle's second application,
 // whose right-hand side r1 = b - a1 q1 is formed (and stored) by k_jac2.
 template <typename T>
@@ -257,8 +187,7 @@ void Engine::precond(int l, const T *r, T *z, bool dots, const T *u, double *out
         ncoarse, Ainv.p, vh.b.p, vh.x.p, stop); note_launch();
     eH = vh.x.p;
   } else {
-    if (l + 1 >= bottom_level<T>()) launch_bottom<T>(w, stop, s);
-    else kcycle<T>(l + 1, w, red, stop, s);
+    kcycle<T>(l + 1, w, red, stop, s);
     eH = vh.z1.p; z2H = vh.z2.p; ksH = w.ks.p + l + 1;
   }
   if (vec) {
@@ -309,7 +238,6 @@ int Engine::fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red, cu
   FcgScal *fs = w.fs.p;
   const int *stop = &fs->done;
   if (!w.iter_graph) {
-    ensure_bottom<T>(*this, w);
     cudaGraph_t graph = nullptr;
     const unsigned long long before = g_launch_count;
     PBG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));

@@ -62,8 +62,6 @@ struct EWork {
   DBuf<T> x0, r0, z0, pA, pB, q0, q0b; // outer FCG on level 0 (q0/q0b: q by parity)
   DBuf<KScal> ks;                      // one per level
   DBuf<FcgScal> fs;
-  DBuf<char> bot;                      // level table of the bottom solver
-  size_t bot_smem = 0;                 // its dynamic shared memory
   cudaGraphExec_t iter_graph = nullptr;  // one captured FCG iteration
   size_t iter_nodes = 0;
   void ensure(const std::vector<ELevel> &lv);
@@ -74,7 +72,6 @@ struct EWork {
 struct EngineOpts {
   double omega = 0.8;        // damped-Jacobi weight
   int coarse_max = 512;      // coarsest level size (dense direct solve)
-  bool block_bottom = false; // run the coarse K-cycle tail in one block (k_bottom)
   EngineOpts();
 };
 
@@ -108,7 +105,6 @@ class Engine {
                            int max_sweeps, int inner_maxit, RedPool &red, cudaStream_t s,
                            double *hist);
   int nlevels() const { return (int)L.size(); }
-  template <typename T> int bottom_level() const;
   template <typename T> EMat<T> mat(int l) const;
   // Average duration (ms) of the fine-level smoothing sweep, `reps` launches
   // back to back between CUDA events on stream s; precision 0 FP64, 1 FP32.
