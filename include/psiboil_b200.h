@@ -213,6 +213,56 @@ int pbg_session_stream(pbg_session *s, void **stream);
 int pbg_bench_kernel(pbg_session *s, int which, int precision, int reps, double *ms,
                      double *bytes_per_launch);
 
+/* ---------------------------------------------------------------------------
+ * Batched solves (no counterpart in the reference, which solves one pressure
+ * system per Pressure object and MPI rank): many independent problems of
+ * uneven 2-D / 3-D sizes solved together by the engine's solver (flexible CG
+ * + AC K-cycle; mixed FP32 inner / FP64 refinement, or plain FP64). Every
+ * problem keeps its matrix, hierarchy and solution resident on the device
+ * until removed; a solve starts from the stored solution (warm start) unless
+ * it is reset. Results do not depend on which problems share a solve.
+ * ------------------------------------------------------------------------- */
+typedef struct pbg_batch pbg_batch;
+
+typedef struct {
+  int precision;    /* PBG_MIXED or PBG_FP64                                  */
+  int slots;        /* problems in flight at once                             */
+  int threads;      /* launch shape: threads per CTA (multiple of 32, 64..512) */
+  int tile_cells;   /* cells per tile (>= threads)                            */
+  int grid;         /* CTAs per tile kernel                                    */
+  int kc_max;       /* levels 1..kc_max run a K-cycle, deeper levels one visit */
+} pbg_batch_config;
+
+void pbg_batch_config_default(pbg_batch_config *c);
+int pbg_batch_create(const pbg_batch_config *c, int device, pbg_batch **out);
+int pbg_batch_destroy(pbg_batch *b);
+/* Device bytes one problem of these dimensions takes (admission control). */
+int pbg_batch_problem_bytes(pbg_batch *b, int nx, int ny, int nz, long long *bytes);
+/* Add a problem (nx*ny*nz > 64 cells; nz == 1 for 2-D); its id. bc as for
+ * pbg_session_create; NULL: Neumann walls with a Dirichlet top (kmax in 3-D,
+ * jmax in 2-D). */
+int pbg_batch_add(pbg_batch *b, int nx, int ny, int nz, double h, const int bc[6], int *id);
+int pbg_batch_remove(pbg_batch *b, int id);
+/* Inputs as for a session: cell densities and solid mask (assembled on the
+ * device, pbg_assemble_pressure), right-hand side, initial guess (NULL:
+ * zero). */
+int pbg_batch_set_fields(pbg_batch *b, int id, const double *rho, const uint8_t *solid, int where);
+int pbg_batch_set_rhs(pbg_batch *b, int id, const double *rhs, int where);
+int pbg_batch_set_x(pbg_batch *b, int id, const double *x, int where);
+int pbg_batch_get_x(pbg_batch *b, int id, double *x, int where);
+/* Solve problems ids[0..n-1] to p->tol (FP64 |b - A x| / |b|; p->inner_tol,
+ * p->max_sweeps, p->max_iter as for the engine). Largest problems are
+ * started first; a problem enters as soon as a slot is free. res[i]
+ * (optional) gets the outcome; res[i].seconds is the time from the start of
+ * the call until problem i finished. */
+int pbg_batch_solve(pbg_batch *b, const int *ids, int n, const pbg_params *p, pbg_result *res);
+/* Pick the launch shape for this batch: time the solve of ids under each
+ * candidate shape and keep the fastest. With cache_path, the choice is read
+ * from / written to that JSON file (keyed by device and batch signature).
+ * best (optional) receives it; the batch keeps it. */
+int pbg_batch_autotune(pbg_batch *b, const int *ids, int n, const pbg_params *p,
+                       const char *cache_path, pbg_batch_config *best);
+
 /* Dot products without allocating (no counterpart in the reference).
  * For callers that cannot call cudaMalloc where they need a dot product —
  * code recorded into a CUDA graph by stream capture, callers whose device

@@ -108,6 +108,35 @@ _SIGS = {
                                     _dp, _vp, _vp, _vp]),
 }
 
+
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("slots", ctypes.c_int), ("threads", ctypes.c_int),
+                ("tile_cells", ctypes.c_int), ("grid", ctypes.c_int), ("kc_max", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_BCP = ctypes.POINTER(BatchConfig)
+_SIGS.update({
+    "pbg_batch_config_default": (None, [_BCP]),
+    "pbg_batch_create": (ctypes.c_int, [_BCP, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "pbg_batch_destroy": (ctypes.c_int, [_vp]),
+    "pbg_batch_problem_bytes": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                               ctypes.POINTER(_ll)]),
+    "pbg_batch_add": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "pbg_batch_remove": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "pbg_batch_set_fields": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int]),
+    "pbg_batch_set_rhs": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
+    "pbg_batch_set_x": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
+    "pbg_batch_get_x": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
+    "pbg_batch_solve": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                       ctypes.POINTER(Params), ctypes.POINTER(Result)]),
+    "pbg_batch_autotune": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                          ctypes.POINTER(Params), ctypes.c_char_p, _BCP]),
+})
+
 _lib = None
 
 
@@ -448,3 +477,118 @@ def generate(kind, seed, n=16, nb=0, rmin=4.0, rmax=16.0, rc=0.0, ratio=1000.0, 
 
 
 KIND_SINGLE, KIND_CYL, KIND_BATCH = 0, 1, 2
+
+
+def batch_config(precision=MIXED, slots=64, **shape):
+    c = BatchConfig()
+    lib().pbg_batch_config_default(ctypes.byref(c))
+    c.precision, c.slots = precision, slots
+    for k, v in shape.items():
+        setattr(c, k, v)
+    return c
+
+
+class Batch:
+    """Many independent pressure problems solved together (pbg_batch_*).
+
+    Each problem keeps its matrix, hierarchy and solution on the device;
+    solve() starts from the stored solution (warm start) unless reset."""
+
+    def __init__(self, precision=MIXED, slots=64, device=0, **shape):
+        self.config = batch_config(precision, slots, **shape)
+        h = _vp()
+        _check(lib().pbg_batch_create(ctypes.byref(self.config), device, ctypes.byref(h)))
+        self._h = h
+        self.dims = {}
+
+    def close(self):
+        if self._h:
+            lib().pbg_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def problem_bytes(self, nx, ny, nz):
+        v = _ll(0)
+        _check(lib().pbg_batch_problem_bytes(self._h, nx, ny, nz, ctypes.byref(v)))
+        return v.value
+
+    def add(self, dims, h, rho=None, solid=None, b=None, x=None, bc=None):
+        """A new problem; returns its id."""
+        if bc is None:  # Dirichlet top: kmax in 3-D, jmax in 2-D (as Session)
+            bc = [NEUMANN] * 6
+            bc[5 if dims[2] > 1 else 3] = DIRICHLET
+        cbc = (ctypes.c_int * 6)(*bc)
+        pid = ctypes.c_int(-1)
+        _check(lib().pbg_batch_add(self._h, dims[0], dims[1], dims[2], h, cbc, ctypes.byref(pid)))
+        i = pid.value
+        self.dims[i] = tuple(dims)
+        if rho is not None:
+            self.set_fields(i, rho, solid)
+        if b is not None:
+            self.set_rhs(i, b)
+        self.set_x(i, x)
+        return i
+
+    def remove(self, i):
+        _check(lib().pbg_batch_remove(self._h, i))
+        self.dims.pop(i, None)
+
+    def set_fields(self, i, rho, solid):
+        pr, wr = _ptr(rho)
+        ps, ws = _ptr(solid)
+        if wr != ws:
+            raise ValueError("rho and solid must live on the same side")
+        _check(lib().pbg_batch_set_fields(self._h, i, pr, ps, wr))
+
+    def set_rhs(self, i, b):
+        pb_, w = _ptr(b)
+        _check(lib().pbg_batch_set_rhs(self._h, i, pb_, w))
+
+    def set_x(self, i, x=None):
+        px, w = _ptr(x)
+        _check(lib().pbg_batch_set_x(self._h, i, px, w))
+
+    def get_x(self, i, out=None):
+        if out is None:
+            d = self.dims[i]
+            out = np.zeros(d[0] * d[1] * d[2])
+        p, w = _ptr(out)
+        _check(lib().pbg_batch_get_x(self._h, i, p, w))
+        return out
+
+    @staticmethod
+    def _params(tol, inner_tol, max_iter, max_sweeps):
+        p = default_params(SOLVER_ENGINE)
+        p.tol, p.inner_tol, p.max_iter, p.max_sweeps = tol, inner_tol, max_iter, max_sweeps
+        return p
+
+    def solve(self, ids, tol=1.0e-8, inner_tol=1.0e-4, max_iter=500, max_sweeps=8):
+        """Solve the problems `ids`; returns a list of Result (seconds = time
+        from the start of the call until that problem finished)."""
+        ids = list(ids)
+        arr = (ctypes.c_int * len(ids))(*ids)
+        res = (Result * len(ids))()
+        p = self._params(tol, inner_tol, max_iter, max_sweeps)
+        _check(lib().pbg_batch_solve(self._h, arr, len(ids), ctypes.byref(p), res))
+        return list(res)
+
+    def autotune(self, ids, cache=None, tol=1.0e-8, inner_tol=1.0e-4, max_iter=500, max_sweeps=8):
+        ids = list(ids)
+        arr = (ctypes.c_int * len(ids))(*ids)
+        p = self._params(tol, inner_tol, max_iter, max_sweeps)
+        best = BatchConfig()
+        _check(lib().pbg_batch_autotune(self._h, arr, len(ids), ctypes.byref(p),
+                                        cache.encode() if cache else None, ctypes.byref(best)))
+        self.config = best
+        return best

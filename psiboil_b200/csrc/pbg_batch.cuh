@@ -1,0 +1,705 @@
+// Batched engine, device side: many independent pressure problems of
+// uneven sizes (2-D and 3-D) solved together, each in a "slot".
+//
+// Work layout: every level of every occupied slot is cut into tiles of a
+// fixed number of cells; the tiles of all slots for level l form one flat
+// list (a contiguous range of the tile array). Every kernel below runs a
+// fixed grid that strides over the tile list of one level and processes the
+// cells of each tile, so one launch does the same phase for every problem,
+// whatever its size. The launch sequence of one outer iteration (captured
+// once as a CUDA graph) is that of the deepest hierarchy in the batch;
+// problems whose hierarchy ends earlier take their dense solve where it
+// ends and skip the deeper launches (per-slot filters at the top of each
+// tile).
+//
+// Per-problem state lives on the device (BState): an outer FP64 refinement
+// state machine (INIT -> RUN -> DONE) around the inner flexible CG in T.
+// Every decision of a slot is taken by the last tile of that slot to finish
+// a reduction, after all of the slot's tiles in that launch are done, so a
+// tile never sees its slot's state change during a launch.
+//
+// Reductions are per slot and deterministic: each tile writes a block
+// partial to its own entry, and the slot's last-arriving tile sums the
+// slot's partials in a fixed order (b_reduce). A problem's tiles, and so
+// every bit of its result, do not depend on which other problems share the
+// batch.
+//
+// Algorithm (per problem) = the engine's (pbg_engine_kernels.cuh): FCG(1)
+// on the finest level, preconditioned by the AC K-cycle (piecewise-constant
+// aggregation by 2, Galerkin coarse operators, damped Jacobi with two fused
+// pre-sweeps and two post-sweeps, two FCG steps per coarse level up to
+// kc_max, one visit below), dense inverse on the coarsest level; FP64 true
+// residual and correction in the outer loop.
+#pragma once
+#include <cstdint>
+
+#include "pbg_assemble.cuh"
+#include "pbg_engine.cuh"
+#include "pbg_engine_kernels.cuh"
+
+namespace pbg {
+
+constexpr int kBMaxLev = 12;    // levels per problem
+constexpr int kBDenseMax = 64;  // cells of the coarsest level (dense inverse in shared memory)
+constexpr int kBThreadsMax = 512;
+
+enum BPhase { BP_IDLE = 0, BP_INIT = 1, BP_RUN = 2, BP_DONE = 3 };
+
+// One level of a problem.
+template <typename T>
+struct BLev {
+  EMat<T> A;                              // operator in T (c, w, s, b, dinv)
+  double *c64, *w64, *s64, *b64;          // FP64 operator (level 0: the assembled matrix)
+  T *b, *x, *z1, *z2, *q1, *r1, *xa, *xb;
+};
+
+// Device descriptor of the problem in a slot (written by the host).
+template <typename T>
+struct BProb {
+  int nlev, ncoarse;
+  int nx, ny, nz;
+  int bc[6];
+  double h;
+  const double *rho;        // assembly inputs (device) or null: level-0 FP64 matrix given
+  const uint8_t *solid;
+  double *x;                // FP64 solution (in: initial guess, out: result)
+  const double *b;          // FP64 right-hand side
+  double *Ainv;             // ncoarse x ncoarse
+  T *x0, *r0, *z0, *pA, *pB, *q0;
+  BLev<T> L[kBMaxLev];
+};
+
+// Per-slot solver state (device). Read back by the host after a solve.
+struct BState {
+  int phase, setup;         // BPhase; setup: hierarchy (re)computation requested
+  int sweeps, iters, status, converged;
+  int max_sweeps, maxit, inner_maxit, mixed;
+  double tol, inner_tol, bb, rel, rel0;
+  FcgScal f;                // inner flexible CG (f.done: inner solve finished)
+  KScal ks[kBMaxLev];
+};
+
+struct BTile {
+  int slot;
+  uint32_t p0, n;           // cells [p0, p0 + n) of the slot's level
+};
+
+// Everything a batch kernel needs (device pointers), passed by value.
+template <typename T>
+struct BCtx {
+  const BProb<T> *prob;     // [S]
+  BState *st;               // [S]
+  const BTile *tiles;       // all levels
+  const int *lbeg;          // [kBMaxLev + 1]: tiles of level l are [lbeg[l], lbeg[l+1])
+  const int *tbeg, *tcnt;   // [kBMaxLev * S]: first tile and tile count of (level, slot)
+  double *part;             // [tiles * 4] per-tile partial sums
+  unsigned *cnt;            // [kBMaxLev * S] arrival counters (zero between launches)
+  int S;
+  int kc_max;               // levels 1..kc_max run a K-cycle, deeper ones one visit
+  T omega;
+};
+
+#define BTILE_LOOP(C, l, t) for (int t = (C).lbeg[l] + (int)blockIdx.x; t < (C).lbeg[(l) + 1]; t += (int)gridDim.x)
+#define BCELL_LOOP(T_, p) for (uint32_t p = (T_).p0 + threadIdx.x; p < (T_).p0 + (T_).n; p += blockDim.x)
+
+// Is slot s running its inner solve (this launch's work applies)?
+__device__ __forceinline__ bool b_running(const BState &S) { return S.phase == BP_RUN && !S.f.done; }
+
+// Block sum of v[0..K-1] in a fixed order (warp shuffles, then warps in
+// index order); the result is valid on thread 0. Ends with the CTA
+// synchronised, so sm can be reused at once.
+template <int K>
+__device__ __forceinline__ void b_block_sum(double (&v)[K], double (&sm)[K][kBThreadsMax / 32]) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  warp_sum<K>(v);
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < K; ++q) sm[q][wid] = v[q];
+  __syncthreads();
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+      double s = 0.0;
+      for (int w = 0; w < nw; ++w) s += sm[q][w];
+      v[q] = s;
+    }
+  __syncthreads();
+}
+
+// Per-slot segmented reduction of K values. Every tile of the slot writes
+// its block sum; the slot's last-arriving tile then sums the slot's tile
+// partials with the whole CTA (thread t takes tiles t, t + blockDim, ... in
+// order, then the fixed block order). The grouping depends only on the
+// slot's own tile count, so the bits do not depend on the other slots.
+// Returns true on thread 0 of that last tile, with out = the slot's sums.
+// Called by every thread of the CTA (it synchronises the CTA).
+template <int K, typename T>
+__device__ bool b_reduce(const BCtx<T> &C, int l, int t, int slot, double (&v)[K], double (&out)[K]) {
+  __shared__ double sm[K][kBThreadsMax / 32];
+  __shared__ int last;
+  b_block_sum<K>(v, sm);
+  const int key = l * C.S + slot;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < K; ++q) C.part[(size_t)t * 4 + q] = v[q];
+    __threadfence();
+    const unsigned prev = atomicAdd(&C.cnt[key], 1u);
+    last = prev == (unsigned)C.tcnt[key] - 1u;
+  }
+  __syncthreads();
+  const int is_last = last;
+  __syncthreads();  // `last` may be rewritten by this CTA's next tile
+  if (!is_last) return false;
+  __threadfence();
+  const int tb = C.tbeg[key], tn = C.tcnt[key];
+  double acc[K];
+#pragma unroll
+  for (int q = 0; q < K; ++q) acc[q] = 0.0;
+  for (int e = threadIdx.x; e < tn; e += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < K; ++q) acc[q] += __ldcg(&C.part[(size_t)(tb + e) * 4 + q]);
+  b_block_sum<K>(acc, sm);
+  if (threadIdx.x != 0) return false;
+#pragma unroll
+  for (int q = 0; q < K; ++q) out[q] = acc[q];
+  C.cnt[key] = 0u;
+  return true;
+}
+
+// ---------------------------------------------------------------- set-up
+// Level 0 of flagged slots: assemble the FP64 matrix from the fields (or
+// keep the uploaded one).
+template <typename T>
+__global__ void kb_assemble(BCtx<T> C) {
+  BTILE_LOOP(C, 0, t) {
+    const BTile tl = C.tiles[t];
+    if (!C.st[tl.slot].setup) continue;
+    const BProb<T> &P = C.prob[tl.slot];
+    if (!P.rho) continue;
+    const BLev<T> &V = P.L[0];
+    BCELL_LOOP(tl, p) {
+      double c, w, s, b;
+      const Pos q = V.A.g.pos(p);
+      assemble_cell(P.nx, P.ny, P.nz, P.h, P.bc, P.rho, P.solid, (long long)p, q, c, w, s, b);
+      V.c64[p] = c; V.w64[p] = w; V.s64[p] = s; V.b64[p] = b;
+    }
+  }
+}
+
+// Level l >= 1 of flagged slots: Galerkin operator from level l-1 (as
+// k_galerkin), FP64.
+template <typename T>
+__global__ void kb_galerkin(BCtx<T> C, int l) {
+  BTILE_LOOP(C, l, t) {
+    const BTile tl = C.tiles[t];
+    if (!C.st[tl.slot].setup) continue;
+    const BProb<T> &P = C.prob[tl.slot];
+    const BLev<T> &F = P.L[l - 1], &V = P.L[l];
+    const int fx = F.A.nx > 1 ? 2 : 1, fy = F.A.ny > 1 ? 2 : 1, fz = F.A.nz > 1 ? 2 : 1;
+    BCELL_LOOP(tl, P_) {
+      Pos Q = V.A.g.pos(P_);
+      double c = 0.0, w = 0.0, s = 0.0, b = 0.0;
+      const int i0 = Q.i * fx, j0 = Q.j * fy, k0 = Q.k * fz;
+      for (int a = 0; a < fx && i0 + a < F.A.nx; ++a)
+        for (int bb = 0; bb < fy && j0 + bb < F.A.ny; ++bb)
+          for (int cc = 0; cc < fz && k0 + cc < F.A.nz; ++cc) {
+            const uint32_t p = ((uint32_t)(i0 + a) * F.A.ny + (j0 + bb)) * F.A.nz + (k0 + cc);
+            c += F.c64[p];
+            if (a == 0) w += F.w64[p]; else c -= 2.0 * F.w64[p];
+            if (bb == 0) s += F.s64[p]; else c -= 2.0 * F.s64[p];
+            if (cc == 0) b += F.b64[p]; else c -= 2.0 * F.b64[p];
+          }
+      V.c64[P_] = c; V.w64[P_] = w; V.s64[P_] = s; V.b64[P_] = b;
+    }
+  }
+}
+
+// Level l of flagged slots: inverse diagonal, and the operator in T (FP32:
+// edge form with the diagonal excess, see kEdgeForm; FP64: the level's own
+// arrays).
+template <typename T>
+__global__ void kb_finish(BCtx<T> C, int l) {
+  BTILE_LOOP(C, l, t) {
+    const BTile tl = C.tiles[t];
+    if (!C.st[tl.slot].setup) continue;
+    const BLev<T> &V = C.prob[tl.slot].L[l];
+    const EMat<T> &A = V.A;
+    const uint32_t SI = A.g.nynz, SJ = (uint32_t)A.nz;
+    T *dinv = const_cast<T *>(A.dinv);
+    BCELL_LOOP(tl, p) {
+      const double c = V.c64[p];
+      dinv[p] = (T)(1.0 / c);
+      if constexpr (kEdgeForm<T>) {
+        const Pos q = A.g.pos(p);
+        double sum = 0.0;
+        if (q.i > 0) sum += V.w64[p];
+        if (q.i < A.nx - 1) sum += V.w64[p + SI];
+        if (q.j > 0) sum += V.s64[p];
+        if (q.j < A.ny - 1) sum += V.s64[p + SJ];
+        if (q.k > 0) sum += V.b64[p];
+        if (q.k < A.nz - 1) sum += V.b64[p + 1];
+        const_cast<T *>(A.c)[p] = (T)(c - sum);
+        const_cast<T *>(A.w)[p] = (T)V.w64[p];
+        const_cast<T *>(A.s)[p] = (T)V.s64[p];
+        const_cast<T *>(A.b)[p] = (T)V.b64[p];
+      }
+    }
+  }
+}
+
+// Dense inverse of every flagged slot's coarsest operator: one CTA per
+// slot, Gauss-Jordan in shared memory (the same exchange steps and pivot
+// skip as k_gj_block), then the setup flag is cleared.
+template <typename T>
+__global__ void kb_dense_inverse(BCtx<T> C, double rel_tol) {
+  __shared__ double D[kBDenseMax][kBDenseMax + 1];
+  __shared__ double rowk[kBDenseMax], colk[kBDenseMax];
+  __shared__ double dmax;
+  for (int slot = blockIdx.x; slot < C.S; slot += gridDim.x) {
+    BState &S = C.st[slot];
+    if (!S.setup) continue;
+    const BProb<T> &P = C.prob[slot];
+    const BLev<T> &V = P.L[P.nlev - 1];
+    const int n = P.ncoarse;
+    for (int e = threadIdx.x; e < kBDenseMax * kBDenseMax; e += blockDim.x) D[e / kBDenseMax][e % kBDenseMax] = 0.0;
+    __syncthreads();
+    const uint32_t SI = V.A.g.nynz, SJ = (uint32_t)V.A.nz;
+    for (int p = threadIdx.x; p < n; p += blockDim.x) {
+      Pos q = V.A.g.pos((uint32_t)p);
+      D[p][p] = V.c64[p];
+      if (q.i > 0) { D[p][p - SI] = -V.w64[p]; D[p - SI][p] = -V.w64[p]; }
+      if (q.j > 0) { D[p][p - SJ] = -V.s64[p]; D[p - SJ][p] = -V.s64[p]; }
+      if (q.k > 0) { D[p][p - 1] = -V.b64[p]; D[p - 1][p] = -V.b64[p]; }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = 0.0;
+      for (int i = 0; i < n; ++i) m = fmax(m, D[i][i]);
+      dmax = m;
+    }
+    __syncthreads();
+    const double thr = rel_tol * dmax;
+    for (int k = 0; k < n; ++k) {
+      if (threadIdx.x < n) { rowk[threadIdx.x] = D[k][threadIdx.x]; colk[threadIdx.x] = D[threadIdx.x][k]; }
+      __syncthreads();
+      const double akk = rowk[k];
+      const bool sk = !(akk > thr);
+      const double piv = sk ? 0.0 : 1.0 / akk;
+      for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int i = e / n, j = e - i * n;
+        double v;
+        if (sk) v = (i == k || j == k) ? 0.0 : D[i][j];
+        else if (i == k && j == k) v = piv;
+        else if (i == k) v = rowk[j] * piv;
+        else if (j == k) v = -colk[i] * piv;
+        else v = D[i][j] - colk[i] * rowk[j] * piv;
+        D[i][j] = v;
+      }
+      __syncthreads();
+    }
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) P.Ainv[e] = D[e / n][e % n];
+    __syncthreads();
+    if (threadIdx.x == 0) S.setup = 0;
+  }
+}
+
+// ---------------------------------------------------------------- outer loop
+// x += e for slots whose inner solve just finished.
+template <typename T>
+__global__ void kb_outer_corr(BCtx<T> C) {
+  BTILE_LOOP(C, 0, t) {
+    const BTile tl = C.tiles[t];
+    const BState &S = C.st[tl.slot];
+    if (!(S.phase == BP_RUN && S.f.done)) continue;
+    const BProb<T> &P = C.prob[tl.slot];
+    BCELL_LOOP(tl, p) P.x[p] += (double)P.x0[p];
+  }
+}
+
+// FP64 true residual r = b - A x for new slots and for slots whose inner
+// solve just finished; r0 = (T) r starts the next inner solve. The slot's
+// last tile runs the refinement decisions (as Engine::solve_mixed /
+// solve_fp64).
+template <typename T>
+__global__ void kb_outer_resid(BCtx<T> C) {
+  BTILE_LOOP(C, 0, t) {
+    const BTile tl = C.tiles[t];
+    BState &S = C.st[tl.slot];
+    if (!(S.phase == BP_INIT || (S.phase == BP_RUN && S.f.done))) continue;
+    const BProb<T> &P = C.prob[tl.slot];
+    const EMat<T> &A = P.L[0].A;
+    const BLev<T> &V = P.L[0];
+    double v[3] = {0.0, 0.0, 0.0};
+    BCELL_LOOP(tl, p) {
+      Pos q = A.g.pos(p);
+      const uint32_t SI = A.g.nynz, SJ = (uint32_t)A.nz;
+      const double *x = P.x;
+      double on = 0.0;
+      if (q.i > 0) on += V.w64[p] * x[p - SI];
+      if (q.i < A.nx - 1) on += V.w64[p + SI] * x[p + SI];
+      if (q.j > 0) on += V.s64[p] * x[p - SJ];
+      if (q.j < A.ny - 1) on += V.s64[p + SJ] * x[p + SJ];
+      if (q.k > 0) on += V.b64[p] * x[p - 1];
+      if (q.k < A.nz - 1) on += V.b64[p + 1] * x[p + 1];
+      const double bp = P.b[p];
+      const double r = bp - (V.c64[p] * x[p] - on);
+      const T rt = (T)r;
+      P.r0[p] = rt;
+      P.x0[p] = T(0);
+      P.q0[p] = T(0);
+      v[0] += r * r;
+      v[1] += bp * bp;
+      v[2] += (double)rt * (double)rt;
+    }
+    double o[3];
+    if (b_reduce<3>(C, 0, t, tl.slot, v, o)) {
+      const bool fresh = S.phase == BP_INIT;
+      if (fresh) {
+        S.bb = o[1];
+        S.sweeps = 0;
+        S.iters = 0;
+        S.converged = 0;
+        S.status = ST_RUNNING;
+        if (!(o[1] > 0.0)) {
+          S.rel = 0.0; S.rel0 = 0.0; S.converged = 1; S.status = ST_INITIAL; S.phase = BP_DONE;
+          continue;
+        }
+        S.rel = sqrt(o[0] / o[1]);
+        S.rel0 = S.rel;
+      } else {
+        const double nrel = sqrt(o[0] / S.bb);
+        S.iters += S.f.iter;
+        S.sweeps += 1;
+        if (!(nrel == nrel)) { S.rel = nrel; S.status = ST_NAN; S.phase = BP_DONE; continue; }
+        if (S.f.status == ST_BREAKDOWN && nrel >= S.rel) {
+          S.rel = nrel; S.status = ST_BREAKDOWN; S.phase = BP_DONE; continue;
+        }
+        S.rel = nrel;
+      }
+      if (S.rel <= S.tol) { S.converged = 1; S.status = ST_CONVERGED; S.phase = BP_DONE; continue; }
+      const int left = S.maxit - S.iters;
+      if (S.sweeps >= S.max_sweeps || left <= 0 || !(o[2] > 0.0)) {
+        S.status = ST_MAXITER; S.phase = BP_DONE; continue;
+      }
+      // next inner solve
+      const double itol = S.mixed ? fmax(S.inner_tol, 0.9 * S.tol / S.rel) : fmin(0.9 * S.tol / S.rel, 0.5);
+      FcgScal &f = S.f;
+      f.rr0 = o[2]; f.rr = o[2]; f.tol = itol;
+      f.maxit = left < S.inner_maxit ? left : S.inner_maxit;
+      f.iter = 0; f.pq = 0.0; f.pr = 0.0; f.zq = 0.0; f.zr = 0.0; f.beta = 0.0; f.alpha = 0.0;
+      f.converged = 0; f.status = ST_RUNNING; f.hist = nullptr;
+      f.done = 0;
+      S.phase = BP_RUN;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- K-cycle phases
+// Right-hand side of the preconditioner application on level l: the FCG
+// residual on level 0, the restricted b on coarse levels, or (kc) the
+// K-cycle residual r1.
+template <typename T>
+__device__ __forceinline__ const T *b_rhs(const BProb<T> &P, int l, bool kc) {
+  return l == 0 ? P.r0 : (kc ? P.L[l].r1 : P.L[l].b);
+}
+
+// Two damped-Jacobi sweeps from zero (k_jac2); kc: rhs b - a1 q1 formed and
+// stored to r1.
+template <typename T>
+__global__ void kb_jac2(BCtx<T> C, int l, int kc) {
+  BTILE_LOOP(C, l, t) {
+    const BTile tl = C.tiles[t];
+    const BState &S = C.st[tl.slot];
+    const BProb<T> &P = C.prob[tl.slot];
+    if (!b_running(S) || P.nlev - 1 <= l) continue;
+    const BLev<T> &V = P.L[l];
+    const EMat<T> &A = V.A;
+    const T om = C.omega;
+    const T a1 = kc ? (T)S.ks[l].a1 : T(0);
+    const T *r = l == 0 ? P.r0 : V.b;
+    auto rv = [&](uint32_t s) -> T { return kc ? V.b[s] - a1 * V.q1[s] : r[s]; };
+    auto x1 = [&](uint32_t s) -> T { return om * rv(s) * A.dinv[s]; };
+    BCELL_LOOP(tl, p) {
+      Pos q = A.g.pos(p);
+      const T rp = rv(p);
+      if (kc) V.r1[p] = rp;
+      const T d = A.dinv[p];
+      const T xp = om * rp * d;
+      const T on = offdiag(A, p, q, x1);
+      V.xb[p] = xp + om * ((rp + on) * d - xp);
+    }
+  }
+}
+
+// b on level l+1 = block sums of (rhs - A xb) on level l
+template <typename T>
+__global__ void kb_restrict(BCtx<T> C, int l, int kc) {
+  BTILE_LOOP(C, l + 1, t) {
+    const BTile tl = C.tiles[t];
+    const BState &S = C.st[tl.slot];
+    const BProb<T> &P = C.prob[tl.slot];
+    if (!b_running(S) || P.nlev - 1 <= l) continue;
+    const BLev<T> &V = P.L[l];
+    const EMat<T> &A = V.A;
+    const Geo &H = P.L[l + 1].A.g;
+    T *rH = P.L[l + 1].b;
+    const T *r = b_rhs(P, l, kc);
+    const int fx = A.nx > 1 ? 2 : 1, fy = A.ny > 1 ? 2 : 1, fz = A.nz > 1 ? 2 : 1;
+    BCELL_LOOP(tl, Pc) {
+      Pos Q = H.pos(Pc);
+      T sum = 0;
+      for (int a = 0; a < fx; ++a) {
+        const int i = Q.i * fx + a;
+        if (i >= A.nx) break;
+        for (int bb = 0; bb < fy; ++bb) {
+          const int j = Q.j * fy + bb;
+          if (j >= A.ny) break;
+          for (int cc = 0; cc < fz; ++cc) {
+            const int k = Q.k * fz + cc;
+            if (k >= A.nz) break;
+            const uint32_t p = ((uint32_t)i * A.ny + j) * A.nz + k;
+            sum += r[p] - ax_at(A, p, Pos{i, j, k}, V.xb);
+          }
+        }
+      }
+      rH[Pc] = sum;
+    }
+  }
+}
+
+// x = Ainv b on level L for slots whose coarsest level is L (one CTA per
+// slot, one warp per row, FP64 sums).
+template <typename T>
+__global__ void kb_dense(BCtx<T> C, int L) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int slot = blockIdx.x; slot < C.S; slot += gridDim.x) {
+    const BState &S = C.st[slot];
+    const BProb<T> &P = C.prob[slot];
+    if (!b_running(S) || P.nlev - 1 != L) continue;
+    const BLev<T> &V = P.L[L];
+    const int n = P.ncoarse;
+    for (int row = wid; row < n; row += nw) {
+      double acc = 0.0;
+      for (int col = lane; col < n; col += 32) acc += P.Ainv[row * n + col] * (double)V.b[col];
+      for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+      if (lane == 0) V.x[row] = (T)acc;
+    }
+  }
+}
+
+// x' = xb + P e, then one sweep (k_prolong_jac). e comes from level l+1:
+// the dense solution x (coarsest), z1 (single visit) or c1 z1 + c2 z2
+// (K-cycle, coefficients from the level's scalars).
+template <typename T>
+__global__ void kb_prolong_jac(BCtx<T> C, int l, int kc) {
+  BTILE_LOOP(C, l, t) {
+    const BTile tl = C.tiles[t];
+    const BState &S = C.st[tl.slot];
+    const BProb<T> &P = C.prob[tl.slot];
+    if (!b_running(S) || P.nlev - 1 <= l) continue;
+    const BLev<T> &V = P.L[l];
+    const BLev<T> &Hl = P.L[l + 1];
+    const EMat<T> &A = V.A;
+    const Geo &H = Hl.A.g;
+    const bool hdense = P.nlev - 1 == l + 1;
+    const bool two = !hdense && (l + 1) <= C.kc_max;
+    const T *eH = hdense ? Hl.x : Hl.z1;
+    const T *z2H = Hl.z2;
+    T c1 = 1, c2 = 0;
+    if (two) {
+      const KScal &k = S.ks[l + 1];
+      c1 = (T)(k.a1 - k.a2 * k.beta);
+      c2 = (T)k.a2;
+    }
+    const T *r = b_rhs(P, l, kc);
+    const T om = C.omega;
+    const int sx = A.nx > 1 ? 1 : 0, sy = A.ny > 1 ? 1 : 0, sz = A.nz > 1 ? 1 : 0;
+    auto e = [&](int i, int j, int k) -> T {
+      const uint32_t Pc = (uint32_t)(i >> sx) * H.nynz + (uint32_t)(j >> sy) * (uint32_t)H.nz + (uint32_t)(k >> sz);
+      return two ? c1 * eH[Pc] + c2 * z2H[Pc] : eH[Pc];
+    };
+    const T *xi = V.xb;
+    BCELL_LOOP(tl, p) {
+      Pos q = A.g.pos(p);
+      const uint32_t SI = A.g.nynz, SJ = (uint32_t)A.nz;
+      T on = 0;
+      if (q.i > 0) on += A.w[p] * (xi[p - SI] + e(q.i - 1, q.j, q.k));
+      if (q.i < A.nx - 1) on += A.w[p + SI] * (xi[p + SI] + e(q.i + 1, q.j, q.k));
+      if (q.j > 0) on += A.s[p] * (xi[p - SJ] + e(q.i, q.j - 1, q.k));
+      if (q.j < A.ny - 1) on += A.s[p + SJ] * (xi[p + SJ] + e(q.i, q.j + 1, q.k));
+      if (q.k > 0) on += A.b[p] * (xi[p - 1] + e(q.i, q.j, q.k - 1));
+      if (q.k < A.nz - 1) on += A.b[p + 1] * (xi[p + 1] + e(q.i, q.j, q.k + 1));
+      const T xp = xi[p] + e(q.i, q.j, q.k);
+      V.xa[p] = xp + om * ((r[p] + on) * A.dinv[p] - xp);
+    }
+  }
+}
+
+// Last sweep of a preconditioner application: z = xa + w D^-1 (rhs - A xa).
+// Level 0 writes z0 and reduces z.r0 and z.q0 (q of the previous FCG
+// iteration) into the slot's FCG scalars; coarse levels write z1 (first
+// application) or z2 (kc).
+template <typename T>
+__global__ void kb_jac(BCtx<T> C, int l, int kc) {
+  BTILE_LOOP(C, l, t) {
+    const BTile tl = C.tiles[t];
+    BState &S = C.st[tl.slot];
+    const BProb<T> &P = C.prob[tl.slot];
+    if (!b_running(S) || P.nlev - 1 <= l) continue;
+    const BLev<T> &V = P.L[l];
+    const EMat<T> &A = V.A;
+    const T *r = b_rhs(P, l, kc);
+    T *z = l == 0 ? P.z0 : (kc ? V.z2 : V.z1);
+    const T om = C.omega;
+    double v[2] = {0.0, 0.0};
+    BCELL_LOOP(tl, p) {
+      Pos q = A.g.pos(p);
+      const T on = offdiag(A, p, q, [&](uint32_t s) { return V.xa[s]; });
+      const T xp = V.xa[p];
+      const T zz = xp + om * ((r[p] + on) * A.dinv[p] - xp);
+      z[p] = zz;
+      if (l == 0) {
+        v[0] += (double)zz * (double)r[p];
+        v[1] += (double)zz * (double)P.q0[p];
+      }
+    }
+    if (l == 0) {
+      double o[2];
+      if (b_reduce<2>(C, 0, t, tl.slot, v, o)) { S.f.zr = o[0]; S.f.zq = o[1]; }
+    }
+  }
+}
+
+// K-cycle, first FCG step on level l: q1 = A z1, a1 = z1.b / z1.q1
+template <typename T>
+__global__ void kb_kc_q1(BCtx<T> C, int l) {
+  BTILE_LOOP(C, l, t) {
+    const BTile tl = C.tiles[t];
+    BState &S = C.st[tl.slot];
+    const BProb<T> &P = C.prob[tl.slot];
+    if (!b_running(S) || P.nlev - 1 <= l) continue;
+    const BLev<T> &V = P.L[l];
+    double v[2] = {0.0, 0.0};
+    BCELL_LOOP(tl, p) {
+      Pos q = V.A.g.pos(p);
+      const T qq = ax_at(V.A, p, q, V.z1);
+      V.q1[p] = qq;
+      v[0] += (double)V.z1[p] * (double)V.b[p];
+      v[1] += (double)V.z1[p] * (double)qq;
+    }
+    double o[2];
+    if (b_reduce<2>(C, l, t, tl.slot, v, o)) {
+      KScal &k = S.ks[l];
+      k.zb = o[0];
+      k.zq = o[1];
+      k.a1 = (o[1] > 0.0 && o[1] == o[1]) ? o[0] / o[1] : 0.0;
+    }
+  }
+}
+
+// K-cycle, second FCG step on level l (k_kc_q2): beta and a2 from
+// z2.q1, z2.r1 and z2.A z2.
+template <typename T>
+__global__ void kb_kc_q2(BCtx<T> C, int l) {
+  BTILE_LOOP(C, l, t) {
+    const BTile tl = C.tiles[t];
+    BState &S = C.st[tl.slot];
+    const BProb<T> &P = C.prob[tl.slot];
+    if (!b_running(S) || P.nlev - 1 <= l) continue;
+    const BLev<T> &V = P.L[l];
+    double v[3] = {0.0, 0.0, 0.0};
+    BCELL_LOOP(tl, p) {
+      Pos q = V.A.g.pos(p);
+      const T av = ax_at(V.A, p, q, V.z2);
+      const double zz = (double)V.z2[p];
+      v[0] += zz * (double)V.q1[p];
+      v[1] += zz * (double)V.r1[p];
+      v[2] += zz * (double)av;
+    }
+    double o[3];
+    if (b_reduce<3>(C, l, t, tl.slot, v, o)) {
+      KScal &k = S.ks[l];
+      const double zq = k.zq;
+      const double beta = zq > 0.0 ? o[0] / zq : 0.0;
+      const double z1r1 = k.zb - k.a1 * zq;
+      const double pr = o[1] - beta * z1r1;
+      const double pq = o[2] - 2.0 * beta * o[0] + beta * beta * zq;
+      k.beta = beta;
+      k.a2 = (pq > 0.0 && pq == pq && pr == pr) ? pr / pq : 0.0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- outer FCG (level 0)
+// p = z - beta p_old, q = A p, alpha = p.r / p.q (k_fcg_pq)
+template <typename T>
+__global__ void kb_fcg_pq(BCtx<T> C) {
+  BTILE_LOOP(C, 0, t) {
+    const BTile tl = C.tiles[t];
+    BState &S = C.st[tl.slot];
+    if (!b_running(S)) continue;
+    const BProb<T> &P = C.prob[tl.slot];
+    const EMat<T> &A = P.L[0].A;
+    FcgScal &f = S.f;
+    const int it = f.iter;
+    const T *pold = (it & 1) ? P.pB : P.pA;
+    T *pnew = (it & 1) ? P.pA : P.pB;
+    const double betad = (it == 0 || !(f.pq > 0.0)) ? 0.0 : f.zq / f.pq;
+    const T beta = (T)betad;
+    const T *z = P.z0;
+    auto pv = [&](uint32_t s) -> T { return it == 0 ? z[s] : z[s] - beta * pold[s]; };
+    double v[1] = {0.0};
+    BCELL_LOOP(tl, p) {
+      Pos q = A.g.pos(p);
+      const T pp = pv(p);
+      const T qq = ax_f(A, p, q, pv);
+      pnew[p] = pp;
+      P.q0[p] = qq;
+      v[0] += (double)pp * (double)qq;
+    }
+    double o[1];
+    if (b_reduce<1>(C, 0, t, tl.slot, v, o)) {
+      const double pr = f.zr - betad * (it == 0 ? 0.0 : f.pr);
+      f.beta = betad;
+      f.pq = o[0];
+      f.alpha = (o[0] > 0.0 && o[0] == o[0]) ? pr / o[0] : 0.0;
+      if (!(o[0] > 0.0) || !(o[0] == o[0])) { f.done = 1; f.status = ST_BREAKDOWN; }
+    }
+  }
+}
+
+// x += alpha p, r -= alpha q; inner convergence (k_fcg_xr)
+template <typename T>
+__global__ void kb_fcg_xr(BCtx<T> C) {
+  BTILE_LOOP(C, 0, t) {
+    const BTile tl = C.tiles[t];
+    BState &S = C.st[tl.slot];
+    if (!b_running(S)) continue;
+    const BProb<T> &P = C.prob[tl.slot];
+    FcgScal &f = S.f;
+    const int it = f.iter;
+    const T *pp = (it & 1) ? P.pA : P.pB;
+    const T alpha = (T)f.alpha;
+    double v[2] = {0.0, 0.0};
+    BCELL_LOOP(tl, p) {
+      const T pv = pp[p];
+      P.x0[p] += alpha * pv;
+      const T rv = P.r0[p] - alpha * P.q0[p];
+      P.r0[p] = rv;
+      v[0] += (double)rv * (double)rv;
+      v[1] += (double)pv * (double)rv;
+    }
+    double o[2];
+    if (b_reduce<2>(C, 0, t, tl.slot, v, o)) {
+      f.rr = o[0];
+      f.pr = o[1];
+      const double rel = sqrt(o[0] / f.rr0);
+      f.iter = it + 1;
+      if (rel <= f.tol) { f.done = 1; f.converged = 1; f.status = ST_CONVERGED; }
+      else if (!(rel == rel)) { f.done = 1; f.status = ST_NAN; }
+      else if (it + 1 >= f.maxit) { f.done = 1; f.status = ST_MAXITER; }
+    }
+  }
+}
+
+}  // namespace pbg

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/psiboil_b200.h"
+#include "pbg_assemble.cuh"
 #include "pbg_engine.cuh"
 #include "pbg_ref_kernels.cuh"
 #include "problem_gen.h"
@@ -96,66 +97,23 @@ __global__ void k_scatter(const double *__restrict__ src, double *__restrict__ d
   }
 }
 
-__device__ __forceinline__ double harm_d(double a, double b) {
-  return __ddiv_rn(__dmul_rn(__dmul_rn(a, b), 2.0), __dadd_rn(a, b));
-}
-
-// On-device fixture assembly, bit-identical to pbg_gen_assemble (see
-// problem_gen.h for the reference lines each step follows). Writes the
-// symmetric storage c, w, s, b and the active flags.
+// On-device fixture assembly (one thread per cell, assemble_cell).
 __global__ void k_assemble(int nx, int ny, int nz, double h, int4 bc03, int2 bc45,
                            const double *__restrict__ rho, const uint8_t *__restrict__ solid,
                            double *__restrict__ C, double *__restrict__ W, double *__restrict__ S,
                            double *__restrict__ B, uint8_t *__restrict__ aflag) {
-  const long long N = (long long)nx * ny * nz, SI = (long long)ny * nz, SJ = nz;
+  const long long N = (long long)nx * ny * nz;
   const int bc[6] = {bc03.x, bc03.y, bc03.z, bc03.w, bc45.x, bc45.y};
-  const double hx = __ddiv_rn(__dmul_rn(h, h), h);
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
        p += (long long)gridDim.x * blockDim.x) {
     Pos q = pos_of(p, ny, nz);
-    const double rp = rho[p];
-    const uint8_t sp = solid[p];
-    double a[6];
-    a[0] = __ddiv_rn(hx, q.i > 0 ? harm_d(rho[p - SI], rp) : rp);
-    a[1] = __ddiv_rn(hx, q.i < nx - 1 ? harm_d(rp, rho[p + SI]) : rp);
-    a[2] = __ddiv_rn(hx, q.j > 0 ? harm_d(rho[p - SJ], rp) : rp);
-    a[3] = __ddiv_rn(hx, q.j < ny - 1 ? harm_d(rp, rho[p + SJ]) : rp);
-    if (nz > 1) {
-      a[4] = __ddiv_rn(hx, q.k > 0 ? harm_d(rho[p - 1], rp) : rp);
-      a[5] = __ddiv_rn(hx, q.k < nz - 1 ? harm_d(rp, rho[p + 1]) : rp);
-    } else {
-      a[4] = 0.0;
-      a[5] = 0.0;
-    }
-    double c = a[0];
-    for (int f = 1; f < 6; ++f) c = __dadd_rn(c, a[f]);
-    if (q.i > 0 && solid[p - SI] != sp) a[0] = 0.0;
-    if (q.i < nx - 1 && solid[p + SI] != sp) a[1] = 0.0;
-    if (q.j > 0 && solid[p - SJ] != sp) a[2] = 0.0;
-    if (q.j < ny - 1 && solid[p + SJ] != sp) a[3] = 0.0;
-    if (q.k > 0 && solid[p - 1] != sp) a[4] = 0.0;
-    if (q.k < nz - 1 && solid[p + 1] != sp) a[5] = 0.0;
-    if (!sp) {
-      c = a[0];
-      for (int f = 1; f < 6; ++f) c = __dadd_rn(c, a[f]);
-    }
-    const bool onb[6] = {q.i == 0, q.i == nx - 1, q.j == 0, q.j == ny - 1, q.k == 0, q.k == nz - 1};
-    for (int f = 0; f < 6; ++f) {  // Neumann sides first, in face order
-      if (bc[f] != PBG_BC_NEUMANN || (nz == 1 && f >= 4) || !onb[f]) continue;
-      c = __dsub_rn(c, a[f]);
-      a[f] = 0.0;
-    }
-    for (int f = 0; f < 6; ++f)
-      if (bc[f] == PBG_BC_DIRICHLET && onb[f]) a[f] = 0.0;
-    if (sp) {
-      c = __dmul_rn(c, 1.0e-12);
-      for (int f = 0; f < 6; ++f) a[f] = 0.0;
-    }
+    double c, w, sv, b;
+    assemble_cell(nx, ny, nz, h, bc, rho, solid, p, q, c, w, sv, b);
     C[p] = c;
-    W[p] = a[0];
-    S[p] = a[2];
-    B[p] = a[4];
-    aflag[p] = sp ? 0 : 1;
+    W[p] = w;
+    S[p] = sv;
+    B[p] = b;
+    aflag[p] = solid[p] ? 0 : 1;
   }
 }
 

@@ -11,6 +11,172 @@
 
 namespace pbg {
 
+// ---------------------------------------------------------------- hierarchy set-up kernels
+// Output arrays of one level's numeric set-up: the FP64 operator, its
+// inverse diagonal and, in the mixed path (c32 != nullptr), the FP32
+// operator in edge form (c32 = diagonal excess, see kEdgeForm).
+struct LevelOut {
+  double *c, *w, *s, *b, *d;
+  float *c32, *w32, *s32, *b32, *d32;
+};
+
+// Inverse diagonal and FP32 copies of a level whose FP64 operator is set.
+__global__ void k_level_finish(EMat<double> A, LevelOut o) {
+  GRID_LOOP(p, A.g.n) {
+    const double c = A.c[p];
+    o.d[p] = 1.0 / c;
+    if (o.c32) {
+      const Pos q = A.g.pos(p);
+      const double sum = offdiag(A, p, q, [](uint32_t) { return 1.0; });
+      o.c32[p] = (float)(c - sum);
+      o.w32[p] = (float)A.w[p]; o.s32[p] = (float)A.s[p]; o.b32[p] = (float)A.b[p];
+      o.d32[p] = (float)(1.0 / c);
+    }
+  }
+}
+
+// Galerkin coarse operator P^T A P for piecewise-constant aggregation by 2
+// per direction (the sum over a block of every entry of A; each internal
+// coupling enters the block's diagonal twice), FP64.
+__global__ void k_galerkin(EMat<double> A, Geo H, LevelOut o) {
+  const int fx = A.nx > 1 ? 2 : 1, fy = A.ny > 1 ? 2 : 1, fz = A.nz > 1 ? 2 : 1;
+  GRID_LOOP(P, H.n) {
+    Pos Q = H.pos(P);
+    double c = 0.0, w = 0.0, s = 0.0, b = 0.0;
+    const int i0 = Q.i * fx, j0 = Q.j * fy, k0 = Q.k * fz;
+    for (int a = 0; a < fx && i0 + a < A.nx; ++a)
+      for (int bb = 0; bb < fy && j0 + bb < A.ny; ++bb)
+        for (int cc = 0; cc < fz && k0 + cc < A.nz; ++cc) {
+          const uint32_t p = ((uint32_t)(i0 + a) * A.ny + (j0 + bb)) * A.nz + (k0 + cc);
+          c += A.c[p];
+          if (a == 0) w += A.w[p]; else c -= 2.0 * A.w[p];
+          if (bb == 0) s += A.s[p]; else c -= 2.0 * A.s[p];
+          if (cc == 0) b += A.b[p]; else c -= 2.0 * A.b[p];
+        }
+    o.c[P] = c; o.w[P] = w; o.s[P] = s; o.b[P] = b;
+  }
+}
+
+// ---------------------------------------------------------------- dense coarsest
+// Dense n x n matrix of the coarsest symmetric 7-point operator (D zeroed
+// beforehand).
+__global__ void k_dense_fill(EMat<double> A, double *__restrict__ D) {
+  const uint32_t n = A.g.n, SI = A.g.nynz, SJ = (uint32_t)A.nz;
+  GRID_LOOP(p, n) {
+    Pos q = A.g.pos(p);
+    D[(size_t)p * n + p] = A.c[p];
+    if (q.i > 0) { D[(size_t)p * n + p - SI] = -A.w[p]; D[(size_t)(p - SI) * n + p] = -A.w[p]; }
+    if (q.j > 0) { D[(size_t)p * n + p - SJ] = -A.s[p]; D[(size_t)(p - SJ) * n + p] = -A.s[p]; }
+    if (q.k > 0) { D[(size_t)p * n + p - 1] = -A.b[p]; D[(size_t)(p - 1) * n + p] = -A.b[p]; }
+  }
+}
+
+// Largest diagonal entry, for the pivot threshold (one block of 1024).
+__global__ void k_dense_dmax(int n, const double *__restrict__ D, double *dmax) {
+  double m = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, D[(size_t)i * n + i]);
+  for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+  __shared__ double wm[32];
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) m = fmax(m, wm[q]);
+    *dmax = fmax(m, wm[0]);
+  }
+}
+
+constexpr int kGjB = 32;     // pivots per block step
+constexpr int kGjRows = 8;   // rows per CTA
+
+// One blocked Gauss-Jordan exchange on the pivots k0 .. k0+kb-1 (out of
+// place, A -> B). With A11 the pivot block, G = A11^-1 (by scalar
+// Gauss-Jordan in shared memory, every CTA redundantly):
+//   B11 = G, B12 = G A12, B21 = -A21 G, B22 = A22 - A21 G A12.
+// After the last block B = A^-1. A pivot not above rel_tol * dmax (a
+// solid-only aggregate, or the constant mode of an all-Neumann problem)
+// is skipped: its row and column become zero, i.e. that unknown is held at
+// zero, which gives a generalised inverse of a consistent singular system
+// (in a positive semi-definite matrix a zero Schur pivot has a zero row
+// and column, so nothing else changes).
+__global__ void __launch_bounds__(256) k_gj_block(int n, int k0, const double *__restrict__ A,
+                                                  double *__restrict__ B, const double *dmax,
+                                                  double rel_tol) {
+  __shared__ double G[kGjB][kGjB + 1];
+  __shared__ double U[kGjRows][kGjB + 1];
+  __shared__ double S[kGjRows][kGjB + 1];
+  __shared__ double rowk[kGjB], colk[kGjB];
+  const int kb = min(kGjB, n - k0);
+  const double thr = rel_tol * (*dmax);
+  for (int e = threadIdx.x; e < kGjB * kGjB; e += blockDim.x) {
+    const int r = e / kGjB, c = e % kGjB;
+    G[r][c] = (r < kb && c < kb) ? A[(size_t)(k0 + r) * n + k0 + c] : 0.0;
+  }
+  __syncthreads();
+  for (int k = 0; k < kb; ++k) {
+    if (threadIdx.x < kb) { rowk[threadIdx.x] = G[k][threadIdx.x]; colk[threadIdx.x] = G[threadIdx.x][k]; }
+    __syncthreads();
+    const double akk = rowk[k];
+    const bool sk = !(akk > thr);
+    const double piv = sk ? 0.0 : 1.0 / akk;
+    for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
+      const int i = e / kb, j = e - i * kb;
+      double v;
+      if (sk) v = (i == k || j == k) ? 0.0 : G[i][j];
+      else if (i == k && j == k) v = piv;
+      else if (i == k) v = rowk[j] * piv;
+      else if (j == k) v = -colk[i] * piv;
+      else v = G[i][j] - colk[i] * rowk[j] * piv;
+      G[i][j] = v;
+    }
+    __syncthreads();
+  }
+  const int ntile = (n + kGjRows - 1) / kGjRows;
+  for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
+    const int i0 = t * kGjRows;
+    // U: the row coefficients on the pivot rows; S: the rows' pivot-column entries
+    {
+      const int ii = threadIdx.x / kGjB, l = threadIdx.x % kGjB, i = i0 + ii;
+      if (ii < kGjRows) S[ii][l] = (i < n && l < kb) ? A[(size_t)i * n + k0 + l] : 0.0;
+    }
+    __syncthreads();
+    {
+      const int ii = threadIdx.x / kGjB, l = threadIdx.x % kGjB, i = i0 + ii;
+      if (ii < kGjRows) {
+        double u = 0.0;
+        if (i < n && l < kb) {
+          if (i >= k0 && i < k0 + kb) u = G[i - k0][l];
+          else
+            for (int m = 0; m < kb; ++m) u += S[ii][m] * G[m][l];
+        }
+        U[ii][l] = u;
+      }
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+      const bool jin = j >= k0 && j < k0 + kb;
+      double a[kGjB];
+#pragma unroll
+      for (int l = 0; l < kGjB; ++l) a[l] = (!jin && l < kb) ? A[(size_t)(k0 + l) * n + j] : 0.0;
+      for (int ii = 0; ii < kGjRows; ++ii) {
+        const int i = i0 + ii;
+        if (i >= n) break;
+        const bool iin = i >= k0 && i < k0 + kb;
+        double v;
+        if (jin) v = iin ? U[ii][j - k0] : -U[ii][j - k0];
+        else {
+          double acc = 0.0;
+#pragma unroll
+          for (int l = 0; l < kGjB; ++l) acc += U[ii][l] * a[l];
+          v = iin ? acc : A[(size_t)i * n + j] - acc;
+        }
+        B[(size_t)i * n + j] = v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+
 template <typename T>
 void EWork<T>::ensure(const std::vector<ELevel> &lv) {
   if (L.size() == lv.size() && x0.n == (size_t)lv[0].ncell()) return;
@@ -116,7 +282,8 @@ void Engine::compute(cudaStream_t s) {
   for (size_t l = 1; l < L.size(); ++l) {
     ELevel &c = L[l];
     k_galerkin<<<grid_for(c.ncell()), kThreads, 0, s>>>(L[l - 1].m64, Geo(c.nx, c.ny, c.nz), out(c));
-    note_launch();
+    k_level_finish<<<grid_for(c.ncell()), kThreads, 0, s>>>(c.m64, out(c));
+    note_launch(); note_launch();
   }
   // dense inverse of the coarsest operator: blocked Gauss-Jordan, out of place
   const int n = ncoarse;

@@ -290,7 +290,23 @@ __global__ void __launch_bounds__(kThreads, 4)
 // (A x)_m of lane m
 template <typename T>
 __device__ __forceinline__ T axv(const T c, const CoefV<T> &C, const HoodV<T> &X, int m) {
-  return c * X.c.v[m] - offd(C, X, m);
+  if constexpr (kEdgeForm<T>) {  // c holds the diagonal excess (ax_f)
+    constexpr int V = VecTraits<T>::V;
+    const T xp = X.c.v[m];
+    const T xl = m > 0 ? X.c.v[m - 1] : X.km;
+    const T xr = m < V - 1 ? X.c.v[m + 1] : X.kp;
+    const T bt = m < V - 1 ? C.b.v[m + 1] : C.bk;
+    T v = 0;
+    v += C.w.v[m] * (xp - X.w.v[m]);
+    v += C.we.v[m] * (xp - X.e.v[m]);
+    v += C.s.v[m] * (xp - X.s.v[m]);
+    v += C.sn.v[m] * (xp - X.n.v[m]);
+    v += C.b.v[m] * (xp - xl);
+    v += bt * (xp - xr);
+    return c * xp + v;
+  } else {
+    return c * X.c.v[m] - offd(C, X, m);
+  }
 }
 
 // FCG direction: p = z - beta p_old, q = A z - beta q_old (A p = A z - beta
