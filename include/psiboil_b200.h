@@ -263,6 +263,66 @@ int pbg_batch_solve(pbg_batch *b, const int *ids, int n, const pbg_params *p, pb
 int pbg_batch_autotune(pbg_batch *b, const int *ids, int n, const pbg_params *p,
                        const char *cache_path, pbg_batch_config *best);
 
+/* ---------------------------------------------------------------------------
+ * Serving (no counterpart in the reference): a request loop on one GPU. A
+ * session is one grid whose matrix, hierarchy and last solution stay on the
+ * device (the next request starts from that solution); sessions are admitted
+ * while their device bytes fit the HBM budget. Requests from any thread
+ * are queued; a worker thread admits them into the running batch as slots
+ * free up (continuous batching: requests that arrive while others are on
+ * the GPU join at the next outer iteration) and records each latency from
+ * submission to completion. One request per session is in flight at a
+ * time; a session's later requests wait for it in order. A result does not
+ * depend on the other requests in flight.
+ * ------------------------------------------------------------------------- */
+typedef struct pbg_server pbg_server;
+
+typedef struct {
+  int precision;          /* PBG_MIXED or PBG_FP64                             */
+  int slots;              /* requests in flight at once                        */
+  long long hbm_budget;   /* device bytes the sessions may take (0: 150 GB)    */
+  int iters_per_poll;     /* outer iterations between completion checks        */
+  int threads, tile_cells, grid, kc_max;   /* launch shape (pbg_batch_config)  */
+  double tol, inner_tol;  /* as pbg_params                                     */
+  int max_sweeps, max_iter;
+} pbg_server_config;
+
+typedef struct {
+  long long submitted, completed, queued, in_flight;
+  long long sessions, device_bytes;   /* admitted sessions and their bytes       */
+  unsigned long long kernel_launches;
+} pbg_server_stats;
+
+void pbg_server_config_default(pbg_server_config *c);
+int pbg_server_create(const pbg_server_config *c, int device, pbg_server **out);
+/* Stops the worker after the requests in flight (queued ones are dropped). */
+int pbg_server_destroy(pbg_server *s);
+/* PBG_ERR_ADMISSION if the session's device bytes do not fit the budget. */
+int pbg_server_open_session(pbg_server *s, int nx, int ny, int nz, double h, const int bc[6],
+                            int *sid);
+/* Waits for the session's requests, then frees its device memory. */
+int pbg_server_close_session(pbg_server *s, int sid);
+/* Queue a solve on session sid: new cell densities and solid mask (both
+ * NULL: matrix unchanged), right-hand side. Host inputs are copied at
+ * submission; device inputs are read when the request starts, so they must
+ * stay valid until pbg_server_wait returns for it. */
+int pbg_server_submit(pbg_server *s, int sid, const double *rho, const uint8_t *solid,
+                      const double *rhs, int where, long long *rid);
+/* Queue a solve whose inputs are made on the device when it starts: one
+ * bubble (centre in cell units, radius in cells, density 1 inside and
+ * `ratio` outside) and a uniform right-hand side in [-1, 1] from
+ * rhs_seed, made zero-mean over the cells and scaled by 1/h^2. */
+int pbg_server_submit_bubble(pbg_server *s, int sid, const double center[3], double radius,
+                             double ratio, unsigned long long rhs_seed, long long *rid);
+/* Wait for a request (timeout_s < 0: no limit); PBG_ERR_STATE on timeout.
+ * latency_s: submission to completion. A request's record is released by
+ * the first wait that returns it. */
+int pbg_server_wait(pbg_server *s, long long rid, double timeout_s, pbg_result *res,
+                    double *latency_s);
+/* The session's current solution (waits until it has no request in flight). */
+int pbg_server_get_x(pbg_server *s, int sid, double *x, int where);
+int pbg_server_stats_get(pbg_server *s, pbg_server_stats *st);
+
 /* Dot products without allocating (no counterpart in the reference).
  * For callers that cannot call cudaMalloc where they need a dot product —
  * code recorded into a CUDA graph by stream capture, callers whose device

@@ -137,6 +137,40 @@ _SIGS.update({
                                           ctypes.POINTER(Params), ctypes.c_char_p, _BCP]),
 })
 
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("slots", ctypes.c_int), ("hbm_budget", ctypes.c_longlong),
+                ("iters_per_poll", ctypes.c_int), ("threads", ctypes.c_int), ("tile_cells", ctypes.c_int),
+                ("grid", ctypes.c_int), ("kc_max", ctypes.c_int), ("tol", ctypes.c_double),
+                ("inner_tol", ctypes.c_double), ("max_sweeps", ctypes.c_int), ("max_iter", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong),
+                ("queued", ctypes.c_longlong), ("in_flight", ctypes.c_longlong),
+                ("sessions", ctypes.c_longlong), ("device_bytes", ctypes.c_longlong),
+                ("kernel_launches", ctypes.c_ulonglong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_SCP = ctypes.POINTER(ServerConfig)
+_SIGS.update({
+    "pbg_server_config_default": (None, [_SCP]),
+    "pbg_server_create": (ctypes.c_int, [_SCP, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "pbg_server_destroy": (ctypes.c_int, [_vp]),
+    "pbg_server_open_session": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "pbg_server_close_session": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "pbg_server_submit": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, ctypes.POINTER(_ll)]),
+    "pbg_server_submit_bubble": (ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double,
+                                                ctypes.c_ulonglong, ctypes.POINTER(_ll)]),
+    "pbg_server_wait": (ctypes.c_int, [_vp, _ll, ctypes.c_double, ctypes.POINTER(Result), _dp]),
+    "pbg_server_get_x": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
+    "pbg_server_stats_get": (ctypes.c_int, [_vp, ctypes.POINTER(ServerStats)]),
+})
+
 _lib = None
 
 
@@ -592,3 +626,86 @@ class Batch:
                                         cache.encode() if cache else None, ctypes.byref(best)))
         self.config = best
         return best
+
+
+class Server:
+    """The serving loop (pbg_server_*): resident sessions, a request queue
+    and a worker thread that batches requests continuously on one GPU."""
+
+    def __init__(self, precision=MIXED, slots=64, hbm_budget=0, device=0, **kw):
+        c = ServerConfig()
+        lib().pbg_server_config_default(ctypes.byref(c))
+        c.precision, c.slots, c.hbm_budget = precision, slots, hbm_budget
+        for k, v in kw.items():
+            setattr(c, k, v)
+        self.config = c
+        h = _vp()
+        _check(lib().pbg_server_create(ctypes.byref(c), device, ctypes.byref(h)))
+        self._h = h
+        self.dims = {}
+
+    def close(self):
+        if self._h:
+            lib().pbg_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def open_session(self, dims, h, bc=None):
+        if bc is None:
+            bc = [NEUMANN] * 6
+            bc[5 if dims[2] > 1 else 3] = DIRICHLET
+        sid = ctypes.c_int(-1)
+        _check(lib().pbg_server_open_session(self._h, dims[0], dims[1], dims[2], h,
+                                             (ctypes.c_int * 6)(*bc), ctypes.byref(sid)))
+        self.dims[sid.value] = tuple(dims)
+        return sid.value
+
+    def close_session(self, sid):
+        _check(lib().pbg_server_close_session(self._h, sid))
+        self.dims.pop(sid, None)
+
+    def submit(self, sid, rhs, rho=None, solid=None):
+        pb_, w = _ptr(rhs)
+        pr, _ = _ptr(rho)
+        ps, _ = _ptr(solid)
+        rid = _ll(-1)
+        _check(lib().pbg_server_submit(self._h, sid, pr, ps, pb_, w, ctypes.byref(rid)))
+        return rid.value
+
+    def submit_bubble(self, sid, center, radius, ratio, seed):
+        c = (ctypes.c_double * 3)(*center)
+        rid = _ll(-1)
+        _check(lib().pbg_server_submit_bubble(self._h, sid, c, radius, ratio, seed, ctypes.byref(rid)))
+        return rid.value
+
+    def wait(self, rid, timeout=-1.0):
+        """(Result, latency seconds) of a request."""
+        r = Result()
+        lat = ctypes.c_double(0.0)
+        _check(lib().pbg_server_wait(self._h, rid, timeout, ctypes.byref(r), ctypes.byref(lat)))
+        return r, lat.value
+
+    def get_x(self, sid, out=None):
+        if out is None:
+            d = self.dims[sid]
+            out = np.zeros(d[0] * d[1] * d[2])
+        p, w = _ptr(out)
+        _check(lib().pbg_server_get_x(self._h, sid, p, w))
+        return out
+
+    def stats(self):
+        st = ServerStats()
+        _check(lib().pbg_server_stats_get(self._h, ctypes.byref(st)))
+        return st.as_dict()
+

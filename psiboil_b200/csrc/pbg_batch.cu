@@ -283,6 +283,15 @@ class BatchEngine : public BatchEngineBase {
 
   double *device_x(int id) override { return get(id).d.x; }
   double *device_rhs(int id) override { return const_cast<double *>(get(id).d.b); }
+  double *device_rho(int id) override { return get(id).rho; }
+  uint8_t *device_solid(int id) override { return get(id).solid; }
+  void fields_changed(int id) override {
+    Prob &P = get(id);
+    if (P.slot >= 0) throw std::runtime_error("batch: problem is being solved");
+    P.assemble = true;
+    P.have_matrix = true;
+    P.need_setup = true;
+  }
 
   // ------------------------------------------------------------ slots
   int free_slots() const override { return S_ - active_; }

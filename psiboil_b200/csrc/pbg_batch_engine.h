@@ -60,6 +60,11 @@ class BatchEngineBase {
   virtual void get_x(int id, double *x, int where) = 0;
   virtual double *device_x(int id) = 0;
   virtual double *device_rhs(int id) = 0;
+  // The problem's own field buffers (for inputs made on the device); after
+  // writing them, fields_changed marks the matrix for re-assembly.
+  virtual double *device_rho(int id) = 0;
+  virtual uint8_t *device_solid(int id) = 0;
+  virtual void fields_changed(int id) = 0;
   // Attach a problem to a free slot for one solve; the slot, or -1 if none.
   virtual int attach(int id, const BatchSolveParams &p) = 0;
   virtual int free_slots() const = 0;
