@@ -231,6 +231,8 @@ typedef struct {
   int tile_cells;   /* cells per tile (>= threads)                            */
   int grid;         /* CTAs per tile kernel                                    */
   int kc_max;       /* levels 1..kc_max run a K-cycle, deeper levels one visit */
+  int tail_cells;   /* a problem's coarse levels of at most this many cells run
+                       their whole K-cycle in one CTA (0: none)                */
 } pbg_batch_config;
 
 void pbg_batch_config_default(pbg_batch_config *c);
@@ -282,7 +284,7 @@ typedef struct {
   int slots;              /* requests in flight at once                        */
   long long hbm_budget;   /* device bytes the sessions may take (0: 150 GB)    */
   int iters_per_poll;     /* outer iterations between completion checks        */
-  int threads, tile_cells, grid, kc_max;   /* launch shape (pbg_batch_config)  */
+  int threads, tile_cells, grid, kc_max, tail_cells;  /* as pbg_batch_config  */
   double tol, inner_tol;  /* as pbg_params                                     */
   int max_sweeps, max_iter;
 } pbg_server_config;

@@ -111,7 +111,8 @@ _SIGS = {
 
 class BatchConfig(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("slots", ctypes.c_int), ("threads", ctypes.c_int),
-                ("tile_cells", ctypes.c_int), ("grid", ctypes.c_int), ("kc_max", ctypes.c_int)]
+                ("tile_cells", ctypes.c_int), ("grid", ctypes.c_int), ("kc_max", ctypes.c_int),
+                ("tail_cells", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -141,7 +142,8 @@ _SIGS.update({
 class ServerConfig(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("slots", ctypes.c_int), ("hbm_budget", ctypes.c_longlong),
                 ("iters_per_poll", ctypes.c_int), ("threads", ctypes.c_int), ("tile_cells", ctypes.c_int),
-                ("grid", ctypes.c_int), ("kc_max", ctypes.c_int), ("tol", ctypes.c_double),
+                ("grid", ctypes.c_int), ("kc_max", ctypes.c_int), ("tail_cells", ctypes.c_int),
+                ("tol", ctypes.c_double),
                 ("inner_tol", ctypes.c_double), ("max_sweeps", ctypes.c_int), ("max_iter", ctypes.c_int)]
 
 

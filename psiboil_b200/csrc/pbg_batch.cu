@@ -62,6 +62,7 @@ class BatchEngine : public BatchEngineBase {
   int active_ = 0;
   bool tiles_dirty_ = true, setup_pending_ = false;
   int dmax_ = 0;
+  unsigned long long sig_ = 0;  // launch-sequence signature of the attached slots
 
   DBuf<BProb<T>> dprob_;
   DBuf<BState> dst_;
@@ -81,7 +82,7 @@ class BatchEngine : public BatchEngineBase {
     cudaGraphExec_t exec = nullptr;
     size_t nodes = 0;
   };
-  std::map<int, Graph> graphs_;
+  std::map<unsigned long long, Graph> graphs_;
   unsigned long long launches_ = 0;
 
  public:
@@ -123,6 +124,7 @@ class BatchEngine : public BatchEngineBase {
       throw std::invalid_argument("batch: tile_cells must be in [threads, 2^20]");
     if (s.grid < 1 || s.grid > 65535) throw std::invalid_argument("batch: grid must be in [1, 65535]");
     if (s.kc_max < 0) throw std::invalid_argument("batch: kc_max must be >= 0");
+    if (s.tail_cells < 0 || s.tail_cells > (1 << 20)) throw std::invalid_argument("batch: tail_cells must be in [0, 2^20]");
   }
 
   // ------------------------------------------------------------ problems
@@ -309,6 +311,7 @@ class BatchEngine : public BatchEngineBase {
     PBG_CUDA(cudaStreamSynchronize(stream));
     BProb<T> &d = hprob_[s];
     d = P.d;
+    d.tail = tail_level(P);
     d.rho = P.assemble ? P.rho : nullptr;
     d.solid = P.assemble ? P.solid : nullptr;
     BState &st = hst_[s];
@@ -334,13 +337,33 @@ class BatchEngine : public BatchEngineBase {
     return s;
   }
 
+  // First level (>= 1, not the coarsest) with at most tail_cells cells:
+  // its K-cycle and everything below runs in one CTA; kBMaxLev if none.
+  int tail_level(const Prob &P) const {
+    if (shape_.tail_cells <= 0) return kBMaxLev;
+    for (int l = 1; l < P.nlev - 1; ++l)
+      if ((long long)P.dims[l][0] * P.dims[l][1] * P.dims[l][2] <= shape_.tail_cells) return l;
+    return kBMaxLev;
+  }
+
   // ------------------------------------------------------------ tiles
   void rebuild_tiles() {
     std::vector<BTile> tiles;
     std::vector<int> lbeg(kBMaxLev + 1, 0), tbeg((size_t)kBMaxLev * S_, 0), tcnt((size_t)kBMaxLev * S_, 0);
     dmax_ = 0;
-    for (int s = 0; s < S_; ++s)
-      if (slot_pid_[s] >= 0) dmax_ = std::max(dmax_, get(slot_pid_[s]).nlev);
+    int dtile = 0;
+    unsigned dense_mask = 0, tail_mask = 0;
+    for (int s = 0; s < S_; ++s) {
+      if (slot_pid_[s] < 0) continue;
+      const Prob &P = get(slot_pid_[s]);
+      const int tl = tail_level(P);
+      dmax_ = std::max(dmax_, P.nlev);
+      dtile = std::max(dtile, std::min(P.nlev - 1, tl));
+      if (tl < kBMaxLev) tail_mask |= 1u << tl;
+      else dense_mask |= 1u << (P.nlev - 1);
+    }
+    sig_ = (unsigned long long)dtile | ((unsigned long long)dense_mask << 8) |
+           ((unsigned long long)tail_mask << 24) | ((unsigned long long)dmax_ << 40);
     const uint32_t tc = (uint32_t)shape_.tile_cells;
     for (int l = 0; l < kBMaxLev; ++l) {
       lbeg[l] = (int)tiles.size();
@@ -417,30 +440,35 @@ class BatchEngine : public BatchEngineBase {
     count(2 * D + 1);
   }
 
-  // Launch sequence of one preconditioner application on level l (the
-  // deepest hierarchy has D levels); counts the launches.
-  void seq_precond(const BCtx<T> &C, int l, int kc, int D, size_t &n) {
+  // Launch sequence of one preconditioner application on level l (tile
+  // kernels), with the dense solves and CTA-local tails of level l+1 and
+  // the tile K-cycle of level l+1 where some slot needs them; counts the
+  // launches.
+  void seq_precond(const BCtx<T> &C, int l, int kc, size_t &n) {
     const int G = shape_.grid, NT = shape_.threads;
+    const int dtile = (int)(sig_ & 0xff);
+    const unsigned dense_mask = (unsigned)((sig_ >> 8) & 0xffff), tail_mask = (unsigned)((sig_ >> 24) & 0xffff);
     kb_jac2<T><<<G, NT, 0, stream>>>(C, l, kc); ++n;
     kb_restrict<T><<<G, NT, 0, stream>>>(C, l, kc); ++n;
-    kb_dense<T><<<slot_grid(), NT, 0, stream>>>(C, l + 1); ++n;
-    if (l + 1 < D - 1) seq_kcycle(C, l + 1, D, n);
+    if (dense_mask & (1u << (l + 1))) { kb_dense<T><<<slot_grid(), NT, 0, stream>>>(C, l + 1); ++n; }
+    if (tail_mask & (1u << (l + 1))) { kb_tail<T><<<slot_grid(), NT, 0, stream>>>(C, l + 1); ++n; }
+    if (l + 1 < dtile) seq_kcycle(C, l + 1, n);
     kb_prolong_jac<T><<<G, NT, 0, stream>>>(C, l, kc); ++n;
     kb_jac<T><<<G, NT, 0, stream>>>(C, l, kc); ++n;
   }
 
-  void seq_kcycle(const BCtx<T> &C, int l, int D, size_t &n) {
+  void seq_kcycle(const BCtx<T> &C, int l, size_t &n) {
     const int G = shape_.grid, NT = shape_.threads;
-    seq_precond(C, l, 0, D, n);
+    seq_precond(C, l, 0, n);
     if (l <= shape_.kc_max) {
       kb_kc_q1<T><<<G, NT, 0, stream>>>(C, l); ++n;
-      seq_precond(C, l, 1, D, n);
+      seq_precond(C, l, 1, n);
       kb_kc_q2<T><<<G, NT, 0, stream>>>(C, l); ++n;
     }
   }
 
-  Graph &graph(int D) {
-    auto it = graphs_.find(D);
+  Graph &graph(unsigned long long key) {
+    auto it = graphs_.find(key);
     if (it != graphs_.end()) return it->second;
     const BCtx<T> C = ctx();
     const int G = shape_.grid, NT = shape_.threads;
@@ -450,7 +478,7 @@ class BatchEngine : public BatchEngineBase {
     try {
       kb_outer_corr<T><<<G, NT, 0, stream>>>(C); ++n;
       kb_outer_resid<T><<<G, NT, 0, stream>>>(C); ++n;
-      seq_precond(C, 0, 0, D, n);
+      seq_precond(C, 0, 0, n);
       kb_fcg_pq<T><<<G, NT, 0, stream>>>(C); ++n;
       kb_fcg_xr<T><<<G, NT, 0, stream>>>(C); ++n;
       PBG_CUDA(cudaGetLastError());
@@ -465,7 +493,7 @@ class BatchEngine : public BatchEngineBase {
     cudaError_t e = cudaGraphInstantiate(&gr.exec, g, 0);
     cudaGraphDestroy(g);
     PBG_CUDA(e);
-    return graphs_[D] = gr;
+    return graphs_[key] = gr;
   }
 
   void count(unsigned long long n) {
@@ -486,7 +514,7 @@ class BatchEngine : public BatchEngineBase {
       setup_launches(dmax_);
       setup_pending_ = false;
     }
-    Graph &g = graph(dmax_);
+    Graph &g = graph(sig_);
     for (int k = 0; k < iterations; ++k) PBG_CUDA(cudaGraphLaunch(g.exec, stream));
     count((unsigned long long)iterations * g.nodes);
   }

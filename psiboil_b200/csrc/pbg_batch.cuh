@@ -57,6 +57,7 @@ struct BLev {
 template <typename T>
 struct BProb {
   int nlev, ncoarse;
+  int tail;                 // first level run by the CTA-local tail (kBMaxLev: none)
   int nx, ny, nz;
   int bc[6];
   double h;
@@ -109,7 +110,7 @@ __device__ __forceinline__ bool b_running(const BState &S) { return S.phase == B
 // index order); the result is valid on thread 0. Ends with the CTA
 // synchronised, so sm can be reused at once.
 template <int K>
-__device__ __forceinline__ void b_block_sum(double (&v)[K], double (&sm)[K][kBThreadsMax / 32]) {
+__device__ __forceinline__ void b_block_sum(double (&v)[K], double (*sm)[kBThreadsMax / 32]) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   warp_sum<K>(v);
   if (lane == 0)
@@ -394,7 +395,10 @@ __global__ void kb_outer_resid(BCtx<T> C) {
   }
 }
 
-// ---------------------------------------------------------------- K-cycle phases
+// ---------------------------------------------------------------- K-cycle: cell arithmetic
+// One cell of each K-cycle phase, shared by the tile kernels and the
+// CTA-local tail (kb_tail), so both compute the same bits.
+
 // Right-hand side of the preconditioner application on level l: the FCG
 // residual on level 0, the restricted b on coarse levels, or (kc) the
 // K-cycle residual r1.
@@ -403,161 +407,213 @@ __device__ __forceinline__ const T *b_rhs(const BProb<T> &P, int l, bool kc) {
   return l == 0 ? P.r0 : (kc ? P.L[l].r1 : P.L[l].b);
 }
 
-// Two damped-Jacobi sweeps from zero (k_jac2); kc: rhs b - a1 q1 formed and
-// stored to r1.
+// Two damped-Jacobi sweeps from zero (k_jac2) into xb; kc: rhs b - a1 q1,
+// formed on the fly and stored to r1.
+template <typename T>
+__device__ __forceinline__ void cell_jac2(const BLev<T> &V, const T *r, uint32_t p, T a1, bool kc, T om) {
+  const EMat<T> &A = V.A;
+  auto rv = [&](uint32_t s) -> T { return kc ? V.b[s] - a1 * V.q1[s] : r[s]; };
+  auto x1 = [&](uint32_t s) -> T { return om * rv(s) * A.dinv[s]; };
+  const Pos q = A.g.pos(p);
+  const T rp = rv(p);
+  if (kc) V.r1[p] = rp;
+  const T d = A.dinv[p];
+  const T xp = om * rp * d;
+  const T on = offdiag(A, p, q, x1);
+  V.xb[p] = xp + om * ((rp + on) * d - xp);
+}
+
+// Row of the dense coarsest solve: one warp, FP64 sums (lane 0 writes).
+template <typename T>
+__device__ __forceinline__ void warp_dense_row(const double *Ainv, int n, const T *b, T *x, int row) {
+  const int lane = threadIdx.x & 31;
+  double acc = 0.0;
+  for (int col = lane; col < n; col += 32) acc += Ainv[row * n + col] * (double)b[col];
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+  if (lane == 0) x[row] = (T)acc;
+}
+
+// xa = xb + P e, then one sweep (k_prolong_jac); e from level l+1: eH
+// (dense solution or single visit) or c1 z1 + c2 z2 (two).
+template <typename T>
+__device__ __forceinline__ void cell_prolong_jac(const BLev<T> &V, const BLev<T> &Hl, const T *r, const T *eH,
+                                                 bool two, T c1, T c2, T om, uint32_t p) {
+  const EMat<T> &A = V.A;
+  const Geo &H = Hl.A.g;
+  const T *z2H = Hl.z2;
+  const int sx = A.nx > 1 ? 1 : 0, sy = A.ny > 1 ? 1 : 0, sz = A.nz > 1 ? 1 : 0;
+  auto e = [&](int i, int j, int k) -> T {
+    const uint32_t Pc = (uint32_t)(i >> sx) * H.nynz + (uint32_t)(j >> sy) * (uint32_t)H.nz + (uint32_t)(k >> sz);
+    return two ? c1 * eH[Pc] + c2 * z2H[Pc] : eH[Pc];
+  };
+  const T *xi = V.xb;
+  const Pos q = A.g.pos(p);
+  const uint32_t SI = A.g.nynz, SJ = (uint32_t)A.nz;
+  T on = 0;
+  if (q.i > 0) on += A.w[p] * (xi[p - SI] + e(q.i - 1, q.j, q.k));
+  if (q.i < A.nx - 1) on += A.w[p + SI] * (xi[p + SI] + e(q.i + 1, q.j, q.k));
+  if (q.j > 0) on += A.s[p] * (xi[p - SJ] + e(q.i, q.j - 1, q.k));
+  if (q.j < A.ny - 1) on += A.s[p + SJ] * (xi[p + SJ] + e(q.i, q.j + 1, q.k));
+  if (q.k > 0) on += A.b[p] * (xi[p - 1] + e(q.i, q.j, q.k - 1));
+  if (q.k < A.nz - 1) on += A.b[p + 1] * (xi[p + 1] + e(q.i, q.j, q.k + 1));
+  const T xp = xi[p] + e(q.i, q.j, q.k);
+  V.xa[p] = xp + om * ((r[p] + on) * A.dinv[p] - xp);
+}
+
+// z = xa + w D^-1 (rhs - A xa); returns z
+template <typename T>
+__device__ __forceinline__ T cell_jac(const BLev<T> &V, const T *r, T *z, T om, uint32_t p) {
+  const EMat<T> &A = V.A;
+  const Pos q = A.g.pos(p);
+  const T on = offdiag(A, p, q, [&](uint32_t s) { return V.xa[s]; });
+  const T xp = V.xa[p];
+  const T zz = xp + om * ((r[p] + on) * A.dinv[p] - xp);
+  z[p] = zz;
+  return zz;
+}
+
+// q1 = A z1; v += (z1.b, z1.q1)
+template <typename T>
+__device__ __forceinline__ void cell_q1(const BLev<T> &V, uint32_t p, double (&v)[2]) {
+  const Pos q = V.A.g.pos(p);
+  const T qq = ax_at(V.A, p, q, V.z1);
+  V.q1[p] = qq;
+  v[0] += (double)V.z1[p] * (double)V.b[p];
+  v[1] += (double)V.z1[p] * (double)qq;
+}
+
+// v += (z2.q1, z2.r1, z2.A z2)
+template <typename T>
+__device__ __forceinline__ void cell_q2(const BLev<T> &V, uint32_t p, double (&v)[3]) {
+  const Pos q = V.A.g.pos(p);
+  const T av = ax_at(V.A, p, q, V.z2);
+  const double zz = (double)V.z2[p];
+  v[0] += zz * (double)V.q1[p];
+  v[1] += zz * (double)V.r1[p];
+  v[2] += zz * (double)av;
+}
+
+// K-cycle scalars from the two steps' sums (k_kc_q1 / k_kc_q2)
+__device__ __forceinline__ void kc_after_q1(KScal &k, const double (&o)[2]) {
+  k.zb = o[0];
+  k.zq = o[1];
+  k.a1 = (o[1] > 0.0 && o[1] == o[1]) ? o[0] / o[1] : 0.0;
+}
+__device__ __forceinline__ void kc_after_q2(KScal &k, const double (&o)[3]) {
+  const double zq = k.zq;
+  const double beta = zq > 0.0 ? o[0] / zq : 0.0;
+  const double z1r1 = k.zb - k.a1 * zq;
+  const double pr = o[1] - beta * z1r1;
+  const double pq = o[2] - 2.0 * beta * o[0] + beta * beta * zq;
+  k.beta = beta;
+  k.a2 = (pq > 0.0 && pq == pq && pr == pr) ? pr / pq : 0.0;
+}
+
+// Does the tile-kernel K-cycle on level l apply to this slot? (Level l
+// exists, is not the coarsest, and is above the slot's CTA-local tail.)
+template <typename T>
+__device__ __forceinline__ bool b_tile_level(const BState &S, const BProb<T> &P, int l) {
+  return b_running(S) && l < P.nlev - 1 && l < P.tail;
+}
+
+// Coarse correction read by the prolongation on level l (from level l+1)
+template <typename T>
+__device__ __forceinline__ void b_coarse(const BProb<T> &P, const BState &S, int l, int kc_max,
+                                         const T *&eH, bool &two, T &c1, T &c2) {
+  const BLev<T> &Hl = P.L[l + 1];
+  const bool hdense = P.nlev - 1 == l + 1;
+  two = !hdense && (l + 1) <= kc_max;
+  eH = hdense ? Hl.x : Hl.z1;
+  c1 = 1;
+  c2 = 0;
+  if (two) {
+    const KScal &k = S.ks[l + 1];
+    c1 = (T)(k.a1 - k.a2 * k.beta);
+    c2 = (T)k.a2;
+  }
+}
+
+// ---------------------------------------------------------------- K-cycle: tile kernels
 template <typename T>
 __global__ void kb_jac2(BCtx<T> C, int l, int kc) {
   BTILE_LOOP(C, l, t) {
     const BTile tl = C.tiles[t];
     const BState &S = C.st[tl.slot];
     const BProb<T> &P = C.prob[tl.slot];
-    if (!b_running(S) || P.nlev - 1 <= l) continue;
-    const BLev<T> &V = P.L[l];
-    const EMat<T> &A = V.A;
-    const T om = C.omega;
+    if (!b_tile_level(S, P, l)) continue;
     const T a1 = kc ? (T)S.ks[l].a1 : T(0);
-    const T *r = l == 0 ? P.r0 : V.b;
-    auto rv = [&](uint32_t s) -> T { return kc ? V.b[s] - a1 * V.q1[s] : r[s]; };
-    auto x1 = [&](uint32_t s) -> T { return om * rv(s) * A.dinv[s]; };
-    BCELL_LOOP(tl, p) {
-      Pos q = A.g.pos(p);
-      const T rp = rv(p);
-      if (kc) V.r1[p] = rp;
-      const T d = A.dinv[p];
-      const T xp = om * rp * d;
-      const T on = offdiag(A, p, q, x1);
-      V.xb[p] = xp + om * ((rp + on) * d - xp);
-    }
+    const T *r = l == 0 ? P.r0 : P.L[l].b;
+    BCELL_LOOP(tl, p) cell_jac2(P.L[l], r, p, a1, kc != 0, C.omega);
   }
 }
 
-// b on level l+1 = block sums of (rhs - A xb) on level l
+// b on level l+1 = block sums of (rhs - A xb) on level l; eight lanes per
+// coarse cell of the tile (restrict_child, sum8)
 template <typename T>
 __global__ void kb_restrict(BCtx<T> C, int l, int kc) {
   BTILE_LOOP(C, l + 1, t) {
     const BTile tl = C.tiles[t];
     const BState &S = C.st[tl.slot];
     const BProb<T> &P = C.prob[tl.slot];
-    if (!b_running(S) || P.nlev - 1 <= l) continue;
-    const BLev<T> &V = P.L[l];
-    const EMat<T> &A = V.A;
-    const Geo &H = P.L[l + 1].A.g;
-    T *rH = P.L[l + 1].b;
-    const T *r = b_rhs(P, l, kc);
-    const int fx = A.nx > 1 ? 2 : 1, fy = A.ny > 1 ? 2 : 1, fz = A.nz > 1 ? 2 : 1;
-    BCELL_LOOP(tl, Pc) {
-      Pos Q = H.pos(Pc);
-      T sum = 0;
-      for (int a = 0; a < fx; ++a) {
-        const int i = Q.i * fx + a;
-        if (i >= A.nx) break;
-        for (int bb = 0; bb < fy; ++bb) {
-          const int j = Q.j * fy + bb;
-          if (j >= A.ny) break;
-          for (int cc = 0; cc < fz; ++cc) {
-            const int k = Q.k * fz + cc;
-            if (k >= A.nz) break;
-            const uint32_t p = ((uint32_t)i * A.ny + j) * A.nz + k;
-            sum += r[p] - ax_at(A, p, Pos{i, j, k}, V.xb);
-          }
-        }
-      }
-      rH[Pc] = sum;
+    if (!b_tile_level(S, P, l)) continue;
+    const T *r = b_rhs(P, l, kc != 0);
+    const BLev<T> &V = P.L[l], &H = P.L[l + 1];
+    const uint32_t total = tl.n * 8u;
+    for (uint32_t base = 0; base < total; base += blockDim.x) {
+      const uint32_t u = base + threadIdx.x;
+      const bool valid = u < total;
+      T v = valid ? restrict_child(V.A, r, V.xb, H.A.g, tl.p0 * 8u + u) : T(0);
+      v = sum8(v);
+      if (valid && (u & 7u) == 0u) H.b[tl.p0 + (u >> 3)] = v;
     }
   }
 }
 
-// x = Ainv b on level L for slots whose coarsest level is L (one CTA per
-// slot, one warp per row, FP64 sums).
+// x = Ainv b on level L for slots whose coarsest level is L and not inside
+// their tail (one CTA per slot, one warp per row).
 template <typename T>
 __global__ void kb_dense(BCtx<T> C, int L) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int slot = blockIdx.x; slot < C.S; slot += gridDim.x) {
     const BState &S = C.st[slot];
     const BProb<T> &P = C.prob[slot];
-    if (!b_running(S) || P.nlev - 1 != L) continue;
+    if (!b_running(S) || P.nlev - 1 != L || P.tail <= L) continue;
     const BLev<T> &V = P.L[L];
-    const int n = P.ncoarse;
-    for (int row = wid; row < n; row += nw) {
-      double acc = 0.0;
-      for (int col = lane; col < n; col += 32) acc += P.Ainv[row * n + col] * (double)V.b[col];
-      for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
-      if (lane == 0) V.x[row] = (T)acc;
-    }
+    for (int row = wid; row < P.ncoarse; row += nw) warp_dense_row(P.Ainv, P.ncoarse, V.b, V.x, row);
   }
 }
 
-// x' = xb + P e, then one sweep (k_prolong_jac). e comes from level l+1:
-// the dense solution x (coarsest), z1 (single visit) or c1 z1 + c2 z2
-// (K-cycle, coefficients from the level's scalars).
 template <typename T>
 __global__ void kb_prolong_jac(BCtx<T> C, int l, int kc) {
   BTILE_LOOP(C, l, t) {
     const BTile tl = C.tiles[t];
     const BState &S = C.st[tl.slot];
     const BProb<T> &P = C.prob[tl.slot];
-    if (!b_running(S) || P.nlev - 1 <= l) continue;
-    const BLev<T> &V = P.L[l];
-    const BLev<T> &Hl = P.L[l + 1];
-    const EMat<T> &A = V.A;
-    const Geo &H = Hl.A.g;
-    const bool hdense = P.nlev - 1 == l + 1;
-    const bool two = !hdense && (l + 1) <= C.kc_max;
-    const T *eH = hdense ? Hl.x : Hl.z1;
-    const T *z2H = Hl.z2;
-    T c1 = 1, c2 = 0;
-    if (two) {
-      const KScal &k = S.ks[l + 1];
-      c1 = (T)(k.a1 - k.a2 * k.beta);
-      c2 = (T)k.a2;
-    }
-    const T *r = b_rhs(P, l, kc);
-    const T om = C.omega;
-    const int sx = A.nx > 1 ? 1 : 0, sy = A.ny > 1 ? 1 : 0, sz = A.nz > 1 ? 1 : 0;
-    auto e = [&](int i, int j, int k) -> T {
-      const uint32_t Pc = (uint32_t)(i >> sx) * H.nynz + (uint32_t)(j >> sy) * (uint32_t)H.nz + (uint32_t)(k >> sz);
-      return two ? c1 * eH[Pc] + c2 * z2H[Pc] : eH[Pc];
-    };
-    const T *xi = V.xb;
-    BCELL_LOOP(tl, p) {
-      Pos q = A.g.pos(p);
-      const uint32_t SI = A.g.nynz, SJ = (uint32_t)A.nz;
-      T on = 0;
-      if (q.i > 0) on += A.w[p] * (xi[p - SI] + e(q.i - 1, q.j, q.k));
-      if (q.i < A.nx - 1) on += A.w[p + SI] * (xi[p + SI] + e(q.i + 1, q.j, q.k));
-      if (q.j > 0) on += A.s[p] * (xi[p - SJ] + e(q.i, q.j - 1, q.k));
-      if (q.j < A.ny - 1) on += A.s[p + SJ] * (xi[p + SJ] + e(q.i, q.j + 1, q.k));
-      if (q.k > 0) on += A.b[p] * (xi[p - 1] + e(q.i, q.j, q.k - 1));
-      if (q.k < A.nz - 1) on += A.b[p + 1] * (xi[p + 1] + e(q.i, q.j, q.k + 1));
-      const T xp = xi[p] + e(q.i, q.j, q.k);
-      V.xa[p] = xp + om * ((r[p] + on) * A.dinv[p] - xp);
-    }
+    if (!b_tile_level(S, P, l)) continue;
+    const T *eH;
+    bool two;
+    T c1, c2;
+    b_coarse(P, S, l, C.kc_max, eH, two, c1, c2);
+    const T *r = b_rhs(P, l, kc != 0);
+    BCELL_LOOP(tl, p) cell_prolong_jac(P.L[l], P.L[l + 1], r, eH, two, c1, c2, C.omega, p);
   }
 }
 
-// Last sweep of a preconditioner application: z = xa + w D^-1 (rhs - A xa).
-// Level 0 writes z0 and reduces z.r0 and z.q0 (q of the previous FCG
-// iteration) into the slot's FCG scalars; coarse levels write z1 (first
-// application) or z2 (kc).
+// Last sweep; level 0 writes z0 and reduces z.r0 and z.q0 (q of the
+// previous FCG iteration) into the slot's FCG scalars.
 template <typename T>
 __global__ void kb_jac(BCtx<T> C, int l, int kc) {
   BTILE_LOOP(C, l, t) {
     const BTile tl = C.tiles[t];
     BState &S = C.st[tl.slot];
     const BProb<T> &P = C.prob[tl.slot];
-    if (!b_running(S) || P.nlev - 1 <= l) continue;
+    if (!b_tile_level(S, P, l)) continue;
     const BLev<T> &V = P.L[l];
-    const EMat<T> &A = V.A;
-    const T *r = b_rhs(P, l, kc);
+    const T *r = b_rhs(P, l, kc != 0);
     T *z = l == 0 ? P.z0 : (kc ? V.z2 : V.z1);
-    const T om = C.omega;
     double v[2] = {0.0, 0.0};
     BCELL_LOOP(tl, p) {
-      Pos q = A.g.pos(p);
-      const T on = offdiag(A, p, q, [&](uint32_t s) { return V.xa[s]; });
-      const T xp = V.xa[p];
-      const T zz = xp + om * ((r[p] + on) * A.dinv[p] - xp);
-      z[p] = zz;
+      const T zz = cell_jac(V, r, z, C.omega, p);
       if (l == 0) {
         v[0] += (double)zz * (double)r[p];
         v[1] += (double)zz * (double)P.q0[p];
@@ -570,63 +626,146 @@ __global__ void kb_jac(BCtx<T> C, int l, int kc) {
   }
 }
 
-// K-cycle, first FCG step on level l: q1 = A z1, a1 = z1.b / z1.q1
 template <typename T>
 __global__ void kb_kc_q1(BCtx<T> C, int l) {
   BTILE_LOOP(C, l, t) {
     const BTile tl = C.tiles[t];
     BState &S = C.st[tl.slot];
     const BProb<T> &P = C.prob[tl.slot];
-    if (!b_running(S) || P.nlev - 1 <= l) continue;
-    const BLev<T> &V = P.L[l];
+    if (!b_tile_level(S, P, l)) continue;
     double v[2] = {0.0, 0.0};
-    BCELL_LOOP(tl, p) {
-      Pos q = V.A.g.pos(p);
-      const T qq = ax_at(V.A, p, q, V.z1);
-      V.q1[p] = qq;
-      v[0] += (double)V.z1[p] * (double)V.b[p];
-      v[1] += (double)V.z1[p] * (double)qq;
-    }
+    BCELL_LOOP(tl, p) cell_q1(P.L[l], p, v);
     double o[2];
-    if (b_reduce<2>(C, l, t, tl.slot, v, o)) {
-      KScal &k = S.ks[l];
-      k.zb = o[0];
-      k.zq = o[1];
-      k.a1 = (o[1] > 0.0 && o[1] == o[1]) ? o[0] / o[1] : 0.0;
-    }
+    if (b_reduce<2>(C, l, t, tl.slot, v, o)) kc_after_q1(S.ks[l], o);
   }
 }
 
-// K-cycle, second FCG step on level l (k_kc_q2): beta and a2 from
-// z2.q1, z2.r1 and z2.A z2.
 template <typename T>
 __global__ void kb_kc_q2(BCtx<T> C, int l) {
   BTILE_LOOP(C, l, t) {
     const BTile tl = C.tiles[t];
     BState &S = C.st[tl.slot];
     const BProb<T> &P = C.prob[tl.slot];
-    if (!b_running(S) || P.nlev - 1 <= l) continue;
-    const BLev<T> &V = P.L[l];
+    if (!b_tile_level(S, P, l)) continue;
     double v[3] = {0.0, 0.0, 0.0};
-    BCELL_LOOP(tl, p) {
-      Pos q = V.A.g.pos(p);
-      const T av = ax_at(V.A, p, q, V.z2);
-      const double zz = (double)V.z2[p];
-      v[0] += zz * (double)V.q1[p];
-      v[1] += zz * (double)V.r1[p];
-      v[2] += zz * (double)av;
-    }
+    BCELL_LOOP(tl, p) cell_q2(P.L[l], p, v);
     double o[3];
-    if (b_reduce<3>(C, l, t, tl.slot, v, o)) {
-      KScal &k = S.ks[l];
-      const double zq = k.zq;
-      const double beta = zq > 0.0 ? o[0] / zq : 0.0;
-      const double z1r1 = k.zb - k.a1 * zq;
-      const double pr = o[1] - beta * z1r1;
-      const double pq = o[2] - 2.0 * beta * o[0] + beta * beta * zq;
-      k.beta = beta;
-      k.a2 = (pq > 0.0 && pq == pq && pr == pr) ? pr / pq : 0.0;
+    if (b_reduce<3>(C, l, t, tl.slot, v, o)) kc_after_q2(S.ks[l], o);
+  }
+}
+
+// ---------------------------------------------------------------- K-cycle: CTA-local tail
+// Block sum of K values, broadcast to every thread (fixed order).
+template <int K>
+__device__ __forceinline__ void t_allreduce(double (&v)[K], double (*sm)[kBThreadsMax / 32], double (&bc)[4]) {
+  b_block_sum<K>(v, sm);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < K; ++q) bc[q] = v[q];
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < K; ++q) v[q] = bc[q];
+  __syncthreads();
+}
+
+#define TCELL_LOOP(p, N) for (uint32_t p = threadIdx.x; p < (uint32_t)(N); p += blockDim.x)
+
+// The whole K-cycle of level `top` of one slot, by one CTA (every level
+// from `top` down lies in one tile, so a CTA barrier separates the phases).
+// The same program as the tile-kernel sequence, with the recursion as a
+// loop and a program counter per level: 0 / 2 start the first / second
+// preconditioner application, 1 / 3 finish it. Leaves z1 (and z2) on level
+// top and its scalars in S.ks[top] as a1 = c1, a2 = c2, beta = 0.
+template <typename T>
+__device__ void t_kcycle(const BProb<T> &P, BState &S, int top, int kc_max, T om) {
+  __shared__ double sm[3][kBThreadsMax / 32];
+  __shared__ double bc[4];
+  const int last = P.nlev - 1;
+  const int nw = blockDim.x >> 5, wid = threadIdx.x >> 5;
+  int step[kBMaxLev];
+  double c1v[kBMaxLev], c2v[kBMaxLev];
+  KScal ks[kBMaxLev];
+  int l = top;
+  step[l] = 0;
+  for (int guard = 0; guard < (1 << 24); ++guard) {
+    const BLev<T> &V = P.L[l];
+    const uint32_t n = V.A.g.n;
+    const int s = step[l];
+    const bool second = s >= 2;
+    const T *rr = second ? V.r1 : V.b;
+    if (s == 0 || s == 2) {
+      const T a1 = second ? (T)ks[l].a1 : T(0);
+      TCELL_LOOP(p, n) cell_jac2(V, V.b, p, a1, second, om);
+      __syncthreads();
+      const BLev<T> &H = P.L[l + 1];
+      for (uint32_t base = 0; base < H.A.g.n * 8u; base += blockDim.x) {
+        const uint32_t u = base + threadIdx.x;
+        const bool valid = u < H.A.g.n * 8u;
+        T v = valid ? restrict_child(V.A, rr, V.xb, H.A.g, u) : T(0);
+        v = sum8(v);
+        if (valid && (u & 7u) == 0u) H.b[u >> 3] = v;
+      }
+      __syncthreads();
+      step[l] = s + 1;
+      if (l + 1 == last) {
+        for (int row = wid; row < P.ncoarse; row += nw) warp_dense_row(P.Ainv, P.ncoarse, H.b, H.x, row);
+        __syncthreads();
+      } else {
+        l = l + 1;
+        step[l] = 0;
+      }
+      continue;
     }
+    {
+      const BLev<T> &H = P.L[l + 1];
+      const bool hdense = l + 1 == last;
+      const bool two = !hdense && (l + 1) <= kc_max;
+      const T *eH = hdense ? H.x : H.z1;
+      const T c1 = hdense ? T(1) : (T)c1v[l + 1], c2 = hdense ? T(0) : (T)c2v[l + 1];
+      TCELL_LOOP(p, n) cell_prolong_jac(V, H, rr, eH, two, c1, c2, om, p);
+      __syncthreads();
+      TCELL_LOOP(p, n) cell_jac(V, rr, second ? V.z2 : V.z1, om, p);
+      __syncthreads();
+    }
+    if (!second) {
+      if (l > kc_max) {
+        c1v[l] = 1.0;
+        c2v[l] = 0.0;
+      } else {
+        double v[2] = {0.0, 0.0};
+        TCELL_LOOP(p, n) cell_q1(V, p, v);
+        t_allreduce<2>(v, sm, bc);
+        kc_after_q1(ks[l], v);
+        step[l] = 2;
+        continue;
+      }
+    } else {
+      double v[3] = {0.0, 0.0, 0.0};
+      TCELL_LOOP(p, n) cell_q2(V, p, v);
+      t_allreduce<3>(v, sm, bc);
+      kc_after_q2(ks[l], v);
+      c1v[l] = ks[l].a1 - ks[l].a2 * ks[l].beta;
+      c2v[l] = ks[l].a2;
+    }
+    if (l == top) break;
+    l = l - 1;
+  }
+  if (threadIdx.x == 0) {
+    S.ks[top].a1 = c1v[top];
+    S.ks[top].a2 = c2v[top];
+    S.ks[top].beta = 0.0;
+  }
+  __syncthreads();
+}
+
+// K-cycles of level l for every slot whose tail starts there.
+template <typename T>
+__global__ void __launch_bounds__(kBThreadsMax) kb_tail(BCtx<T> C, int l) {
+  for (int slot = blockIdx.x; slot < C.S; slot += gridDim.x) {
+    BState &S = C.st[slot];
+    const BProb<T> &P = C.prob[slot];
+    if (!b_running(S) || P.tail != l) continue;
+    t_kcycle(P, S, l, C.kc_max, C.omega);
   }
 }
 

@@ -59,6 +59,7 @@ BatchShape shape_of(const pbg_batch_config &c) {
   s.tile_cells = c.tile_cells;
   s.grid = c.grid;
   s.kc_max = c.kc_max;
+  s.tail_cells = c.tail_cells;
   return s;
 }
 
@@ -162,10 +163,11 @@ bool tune_read(const std::string &path, const std::string &key, pbg_batch_config
   while (std::getline(f, line)) {
     const size_t at = line.find(want);
     if (at == std::string::npos) continue;
-    int th, tc, g, kc;
+    int th, tc, g, kc, tl;
     const char *q = line.c_str() + at + want.size();
-    if (std::sscanf(q, ": {\"threads\": %d, \"tile_cells\": %d, \"grid\": %d, \"kc_max\": %d", &th, &tc, &g, &kc) == 4) {
-      c.threads = th; c.tile_cells = tc; c.grid = g; c.kc_max = kc;
+    if (std::sscanf(q, ": {\"threads\": %d, \"tile_cells\": %d, \"grid\": %d, \"kc_max\": %d, \"tail_cells\": %d",
+                    &th, &tc, &g, &kc, &tl) == 5) {
+      c.threads = th; c.tile_cells = tc; c.grid = g; c.kc_max = kc; c.tail_cells = tl;
       return true;
     }
   }
@@ -185,8 +187,9 @@ void tune_write(const std::string &path, const std::string &key, const pbg_batch
     }
   }
   char buf[512];
-  std::snprintf(buf, sizeof(buf), "  \"%s\": {\"threads\": %d, \"tile_cells\": %d, \"grid\": %d, \"kc_max\": %d, \"ms\": %.3f}",
-                key.c_str(), c.threads, c.tile_cells, c.grid, c.kc_max, ms);
+  std::snprintf(buf, sizeof(buf),
+                "  \"%s\": {\"threads\": %d, \"tile_cells\": %d, \"grid\": %d, \"kc_max\": %d, \"tail_cells\": %d, \"ms\": %.3f}",
+                key.c_str(), c.threads, c.tile_cells, c.grid, c.kc_max, c.tail_cells, ms);
   entries.push_back(buf);
   std::ofstream o(path);
   o << "{\n";
@@ -207,6 +210,7 @@ void pbg_batch_config_default(pbg_batch_config *c) {
   c->tile_cells = s.tile_cells;
   c->grid = s.grid;
   c->kc_max = s.kc_max;
+  c->tail_cells = s.tail_cells;
 }
 
 int pbg_batch_create(const pbg_batch_config *c, int device, pbg_batch **out) {
@@ -353,6 +357,13 @@ int pbg_batch_autotune(pbg_batch *b, const int *ids, int n, const pbg_params *p,
       pbg_batch_config c = after_grid;
       c.kc_max = kc;
       if (kc == after_grid.kc_max) continue;
+      consider(c);
+    }
+    const pbg_batch_config after_kc = bc;
+    for (int tl : {0, 512, 1024, 4096, 16384}) {
+      pbg_batch_config c = after_kc;
+      c.tail_cells = tl;
+      if (tl == after_kc.tail_cells) continue;
       consider(c);
     }
     b->eng->set_shape(shape_of(bc));

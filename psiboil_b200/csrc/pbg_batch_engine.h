@@ -25,6 +25,7 @@ struct BatchShape {
   int tile_cells = 1024;  // cells per tile
   int grid = 148 * 4;     // CTAs of every tile kernel
   int kc_max = 99;        // levels 1..kc_max run a K-cycle, deeper levels one visit
+  int tail_cells = 1024;  // levels of at most this many cells run in one CTA per problem (0: none)
 };
 
 struct BatchSolveParams {

@@ -105,31 +105,46 @@ __global__ void __launch_bounds__(kThreads, 8)
   }
 }
 
-// coarse rhs = block sums of the fine residual r - A x (restriction by the
-// transpose of piecewise-constant prolongation)
+// Restriction by the transpose of piecewise-constant prolongation: the
+// coarse rhs is the block sum of the fine residual r - A x. Eight lanes per
+// coarse cell, one per child (a, b, c) of its 2x2x2 block; absent children
+// (unit extents, odd edges) add zero; the eight are summed by shuffles in a
+// fixed order. t = 8 * coarse cell + child.
+template <typename T>
+__device__ __forceinline__ T restrict_child(const EMat<T> &A, const T *r, const T *x, const Geo &H, uint32_t t) {
+  const int fx = A.nx > 1 ? 2 : 1, fy = A.ny > 1 ? 2 : 1, fz = A.nz > 1 ? 2 : 1;
+  const uint32_t c = t & 7u;
+  const int a = (int)(c >> 2), bb = (int)((c >> 1) & 1u), cc = (int)(c & 1u);
+  if (a >= fx || bb >= fy || cc >= fz) return T(0);
+  const Pos Q = H.pos(t >> 3);
+  const int i = Q.i * fx + a, j = Q.j * fy + bb, k = Q.k * fz + cc;
+  if (i >= A.nx || j >= A.ny || k >= A.nz) return T(0);
+  const uint32_t p = ((uint32_t)i * A.ny + j) * A.nz + k;
+  return r[p] - ax_at(A, p, Pos{i, j, k}, x);
+}
+
+// Sum over the eight lanes of a coarse cell (every lane of the warp must
+// take part); lane (t & 7) == 0 holds the result.
+template <typename T>
+__device__ __forceinline__ T sum8(T v) {
+  v += __shfl_xor_sync(0xffffffffu, v, 1);
+  v += __shfl_xor_sync(0xffffffffu, v, 2);
+  v += __shfl_xor_sync(0xffffffffu, v, 4);
+  return v;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 8) k_resid_restrict(EMat<T> A, const T *__restrict__ r, const T *__restrict__ x,
                                  Geo H, T *__restrict__ rH, const int *stop) {
   if (stop && *stop) return;
-  const int fx = A.nx > 1 ? 2 : 1, fy = A.ny > 1 ? 2 : 1, fz = A.nz > 1 ? 2 : 1;
-  GRID_LOOP(P, H.n) {
-    Pos Q = H.pos(P);
-    T sum = 0;
-    for (int a = 0; a < fx; ++a) {
-      int i = Q.i * fx + a;
-      if (i >= A.nx) break;
-      for (int bb = 0; bb < fy; ++bb) {
-        int j = Q.j * fy + bb;
-        if (j >= A.ny) break;
-        for (int cc = 0; cc < fz; ++cc) {
-          int k = Q.k * fz + cc;
-          if (k >= A.nz) break;
-          uint32_t p = ((uint32_t)i * A.ny + j) * A.nz + k;
-          sum += r[p] - ax_at(A, p, Pos{i, j, k}, x);
-        }
-      }
-    }
-    rH[P] = sum;
+  const uint32_t total = H.n * 8u;
+  // warp-uniform trip count: every lane reaches the shuffles
+  for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
+    const uint32_t t = base + threadIdx.x;
+    const bool valid = t < total;
+    T v = valid ? restrict_child(A, r, x, H, t) : T(0);
+    v = sum8(v);
+    if (valid && (t & 7u) == 0u) rH[t >> 3] = v;
   }
 }
 

@@ -285,6 +285,7 @@ void pbg_server_config_default(pbg_server_config *c) {
   c->tile_cells = b.tile_cells;
   c->grid = b.grid;
   c->kc_max = b.kc_max;
+  c->tail_cells = b.tail_cells;
   c->tol = 1e-8;
   c->inner_tol = 1e-4;
   c->max_sweeps = 8;
@@ -309,6 +310,7 @@ int pbg_server_create(const pbg_server_config *c, int device, pbg_server **out) 
     sh.tile_cells = k.tile_cells;
     sh.grid = k.grid;
     sh.kc_max = k.kc_max;
+    sh.tail_cells = k.tail_cells;
     s->eng = pbg::make_batch_engine(k.precision == PBG_MIXED ? 1 : 0, k.slots, sh);
     s->part.alloc(pbg::kRhsBlocks);
     return PBG_OK;

@@ -133,7 +133,7 @@ def test_autotune_and_cache(engine, oracle, tmp_path):
         assert all(r.converged for r in res)
     import json
     d = json.load(open(cache))
-    assert len(d) == 1 and set(next(iter(d.values()))) >= {"threads", "tile_cells", "grid", "kc_max"}
+    assert len(d) == 1 and set(next(iter(d.values()))) >= {"threads", "tile_cells", "grid", "kc_max", "tail_cells"}
 
 
 def test_bad_inputs_fail_loudly(engine, oracle):
