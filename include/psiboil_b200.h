@@ -103,6 +103,10 @@ typedef struct {
    * sequential i,j,k order (bit-for-bit reference results, one thread per
    * cell and a serial sum per dot product); 0 = deterministic tree sums */
   int exact_sums;
+  /* engine: cells of the dense coarsest level (0: 512). Larger (4096) saves
+   * launches in repeated solves with one matrix and costs a longer set-up
+   * after every matrix change (a dense inverse, O(cells^3)). */
+  int coarse_max;
 } pbg_params;
 
 typedef struct {

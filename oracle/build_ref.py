@@ -116,7 +116,8 @@ def build(ref, jobs):
     englib = os.path.join(REPO, "psiboil_b200", "libpsiboil_b200.so")
     exe_gpu = os.path.join(OUT, "ref_harness_gpu")
     if os.path.exists(englib):
-        deps_gpu = deps + [englib, os.path.join(REPO, "include", "psiboil_b200_psiboil.hpp")]
+        deps_gpu = deps + [englib, os.path.join(REPO, "include", "psiboil_b200_psiboil.hpp"),
+                           os.path.join(REPO, "include", "psiboil_b200.h")]
         if not os.path.exists(exe_gpu) or max(os.path.getmtime(d) for d in deps_gpu) > os.path.getmtime(exe_gpu):
             cuda = "/usr/local/cuda"
             subprocess.check_call(["g++"] + CXXFLAGS + flags + ["-DPBG_WITH_ENGINE",

@@ -56,7 +56,8 @@ class Params(ctypes.Structure):
                 ("stop_if_div", ctypes.c_int), ("priority_min_cyc", ctypes.c_int),
                 ("mv", ctypes.c_int * 3), ("ms", ctypes.c_int * 3),
                 ("tol", ctypes.c_double), ("inner_tol", ctypes.c_double),
-                ("max_sweeps", ctypes.c_int), ("exact_sums", ctypes.c_int)]
+                ("max_sweeps", ctypes.c_int), ("exact_sums", ctypes.c_int),
+                ("coarse_max", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):
@@ -486,10 +487,10 @@ class Engine:
         self.last = None
 
     def solve(self, x, b, tol=1.0e-8, precision=FP64, inner_tol=1.0e-4, max_iter=500,
-              max_sweeps=8):
+              max_sweeps=8, coarse_max=0):
         p = default_params(SOLVER_ENGINE)
         p.precision, p.tol, p.inner_tol = precision, tol, inner_tol
-        p.max_iter, p.max_sweeps = max_iter, max_sweeps
+        p.max_iter, p.max_sweeps, p.coarse_max = max_iter, max_sweeps, coarse_max
         self.last = self.session.solve(x, b, p)
         return bool(self.last.converged)
 

@@ -384,8 +384,13 @@ void ensure_refac(pbg_session *s) {
   }
 }
 
-void ensure_engine(pbg_session *s, bool mixed) {
+void ensure_engine(pbg_session *s, bool mixed, int coarse_max) {
   if (!s->eng) s->eng = std::make_unique<Engine>();
+  if (coarse_max > 0 && coarse_max != s->eng->opt.coarse_max) {
+    s->eng->opt.coarse_max = coarse_max;  // a different hierarchy: build anew
+    s->eng->L.clear();
+    s->eng_dirty = true;
+  }
   if (s->eng_dirty || (mixed && !s->eng->have32)) {
     const Mat64 &A = s->A;
     EMat<double> m = make_emat<double>(A.nx, A.ny, A.nz, A.c.p, A.w.p, A.s.p, A.b.p, nullptr);
@@ -459,7 +464,8 @@ int solve_device(pbg_session *s, double *xd, const double *bd, const pbg_params 
   } else if (p->solver == PBG_SOLVER_ENGINE) {
     if (!s->A.sym) return fail(PBG_ERR_UNSUPPORTED, "the engine solver needs a symmetric matrix");
     const bool mixed = p->precision == PBG_MIXED;
-    ensure_engine(s, mixed);
+    if (p->coarse_max < 0) return fail(PBG_ERR_ARG, "coarse_max must be >= 0");
+    ensure_engine(s, mixed, p->coarse_max);
     EngineResult er = mixed ? s->eng->solve_mixed(xd, bd, p->tol, p->inner_tol, p->max_sweeps,
                                                   p->max_iter, s->red, s->stream, s->hist.p)
                             : s->eng->solve_fp64(xd, bd, p->tol, p->max_iter, s->red, s->stream,
@@ -610,7 +616,7 @@ int pbg_levels(pbg_session *s, int kind, int *count, int *dims, int cap) {
       ensure_refac(s);
       for (auto &l : s->refac->L) { d.push_back(l.nx); d.push_back(l.ny); d.push_back(l.nz); }
     } else {
-      ensure_engine(s, false);
+      ensure_engine(s, false, 0);
       for (auto &l : s->eng->L) { d.push_back(l.nx); d.push_back(l.ny); d.push_back(l.nz); }
     }
     *count = (int)d.size() / 3;
@@ -679,7 +685,7 @@ int pbg_bench_kernel(pbg_session *s, int which, int precision, int reps, double 
     const long long N = s->ncell();
     if (which == 0) {
       if (!s->A.sym) return fail(PBG_ERR_UNSUPPORTED, "engine needs a symmetric matrix");
-      ensure_engine(s, precision == 1);
+      ensure_engine(s, precision == 1, 0);
       *ms = s->eng->bench_sweep(precision, reps, s->stream);
       if (bytes_per_launch) *bytes_per_launch = (double)N * (precision == 1 ? 28.0 : 56.0);
       return PBG_OK;

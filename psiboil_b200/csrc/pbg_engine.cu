@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "pbg_engine.cuh"
@@ -86,7 +87,7 @@ __global__ void k_dense_dmax(int n, const double *__restrict__ D, double *dmax) 
 }
 
 constexpr int kGjB = 32;     // pivots per block step
-constexpr int kGjRows = 8;   // rows per CTA
+constexpr int kGjRows = 32;  // rows per CTA (each reuses the pivot rows from L2)
 
 // One blocked Gauss-Jordan exchange on the pivots k0 .. k0+kb-1 (out of
 // place, A -> B). With A11 the pivot block, G = A11^-1 (by scalar
@@ -134,22 +135,20 @@ __global__ void __launch_bounds__(256) k_gj_block(int n, int k0, const double *_
   for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
     const int i0 = t * kGjRows;
     // U: the row coefficients on the pivot rows; S: the rows' pivot-column entries
-    {
-      const int ii = threadIdx.x / kGjB, l = threadIdx.x % kGjB, i = i0 + ii;
-      if (ii < kGjRows) S[ii][l] = (i < n && l < kb) ? A[(size_t)i * n + k0 + l] : 0.0;
+    for (int e = threadIdx.x; e < kGjRows * kGjB; e += blockDim.x) {
+      const int ii = e / kGjB, l = e % kGjB, i = i0 + ii;
+      S[ii][l] = (i < n && l < kb) ? A[(size_t)i * n + k0 + l] : 0.0;
     }
     __syncthreads();
-    {
-      const int ii = threadIdx.x / kGjB, l = threadIdx.x % kGjB, i = i0 + ii;
-      if (ii < kGjRows) {
-        double u = 0.0;
-        if (i < n && l < kb) {
-          if (i >= k0 && i < k0 + kb) u = G[i - k0][l];
-          else
-            for (int m = 0; m < kb; ++m) u += S[ii][m] * G[m][l];
-        }
-        U[ii][l] = u;
+    for (int e = threadIdx.x; e < kGjRows * kGjB; e += blockDim.x) {
+      const int ii = e / kGjB, l = e % kGjB, i = i0 + ii;
+      double u = 0.0;
+      if (i < n && l < kb) {
+        if (i >= k0 && i < k0 + kb) u = G[i - k0][l];
+        else
+          for (int m = 0; m < kb; ++m) u += S[ii][m] * G[m][l];
       }
+      U[ii][l] = u;
     }
     __syncthreads();
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
@@ -204,11 +203,13 @@ void EWork<T>::drop_graph() {
   iter_nodes = 0;
 }
 
-// Tuning knob (environment): PBG_COARSE_MAX sets the size of the dense
-// coarsest level.
+// Tuning knobs (environment): PBG_COARSE_MAX sets the size of the dense
+// coarsest level, PBG_KC_MAX the deepest level that runs a K-cycle.
 EngineOpts::EngineOpts() {
   const char *c = getenv("PBG_COARSE_MAX");
   if (c && atoi(c) > 0) coarse_max = atoi(c);
+  const char *k = getenv("PBG_KC_MAX");
+  if (k && atoi(k) > 0) kc_max = atoi(k);
 }
 
 template struct EWork<double>;
@@ -220,6 +221,21 @@ Engine::~Engine() {
 
 template <> EMat<double> Engine::mat<double>(int l) const { return L[l].m64; }
 template <> EMat<float> Engine::mat<float>(int l) const { return L[l].m32; }
+template <> const void *Engine::ainv<double>() const { return Ainv.p; }
+template <> const void *Engine::ainv<float>() const { return Ainv32.p; }
+
+__global__ void k_to_float(long long N, const double *__restrict__ a, float *__restrict__ o) {
+  GRID_LOOP(p, N) o[p] = (float)a[p];
+}
+
+// z = Ainv r on the coarsest level (the FP32 inverse for T = float)
+template <typename T>
+void Engine::dense_solve(const T *r, T *z, const int *stop, cudaStream_t s) {
+  using AT = typename std::conditional<sizeof(T) == 4, float, double>::type;
+  const int blocks = (int)(((long long)ncoarse * 32 + kThreads - 1) / kThreads);
+  k_dense_solve<T, AT><<<blocks, kThreads, 0, s>>>(ncoarse, (const AT *)ainv<T>(), r, z, stop);
+  note_launch();
+}
 
 void Engine::build(const EMat<double> &A0, cudaStream_t s, bool mixed) {
   w64.drop_graph();
@@ -248,6 +264,7 @@ void Engine::build(const EMat<double> &A0, cudaStream_t s, bool mixed) {
   }
   ncoarse = (int)L.back().ncell();
   Ainv.alloc((size_t)ncoarse * ncoarse);
+  if (mixed) Ainv32.alloc((size_t)ncoarse * ncoarse);
   Dtmp.alloc((size_t)ncoarse * ncoarse);
   have32 = false;
   if (mixed) {
@@ -294,11 +311,14 @@ void Engine::compute(cudaStream_t s) {
   double *src = Dtmp.p, *dst = Ainv.p;
   const int tiles = (n + kGjRows - 1) / kGjRows;
   for (int k0 = 0; k0 < n; k0 += kGjB) {
-    k_gj_block<<<tiles, kGjRows * kGjB, 0, s>>>(n, k0, src, dst, dsc.p + 7, 1e-10); note_launch();
+    k_gj_block<<<tiles, 256, 0, s>>>(n, k0, src, dst, dsc.p + 7, 1e-10); note_launch();
     std::swap(src, dst);
   }
   if (src != Ainv.p)
     PBG_CUDA(cudaMemcpyAsync(Ainv.p, src, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  if (have32) {
+    k_to_float<<<grid_for((long long)nn), kThreads, 0, s>>>((long long)nn, Ainv.p, Ainv32.p); note_launch();
+  }
   PBG_CUDA(cudaGetLastError());
 }
 
@@ -321,7 +341,7 @@ void Engine::precond(int l, const T *r, T *z, bool dots, const T *u, double *out
   const T om = (T)opt.omega;
   auto &v = w.L[l];
   if (l == last) {
-    k_dense_solve<T><<<(ncoarse * 32 + kThreads - 1) / kThreads, kThreads, 0, s>>>(ncoarse, Ainv.p, r, z, stop); note_launch();
+    dense_solve<T>(r, z, stop, s);
     if (dots) {  // a level-0 problem small enough to be the coarsest
       EMat<T> A = mat<T>(l);
       PBG_CUDA(cudaMemcpyAsync(v.xa.p, z, sizeof(T) * A.ncell(), cudaMemcpyDeviceToDevice, s));
@@ -350,12 +370,16 @@ void Engine::precond(int l, const T *r, T *z, bool dots, const T *u, double *out
   const T *eH, *z2H = nullptr;
   const KScal *ksH = nullptr;
   if (l + 1 == last) {
-    k_dense_solve<T><<<(ncoarse * 32 + kThreads - 1) / kThreads, kThreads, 0, s>>>(
-        ncoarse, Ainv.p, vh.b.p, vh.x.p, stop); note_launch();
+    dense_solve<T>(vh.b.p, vh.x.p, stop, s);
     eH = vh.x.p;
   } else {
-    kcycle<T>(l + 1, w, red, stop, s);
-    eH = vh.z1.p; z2H = vh.z2.p; ksH = w.ks.p + l + 1;
+    if (l + 1 <= opt.kc_max) {
+      kcycle<T>(l + 1, w, red, stop, s);
+      eH = vh.z1.p; z2H = vh.z2.p; ksH = w.ks.p + l + 1;
+    } else {  // one visit: e = M b on level l+1
+      precond<T>(l + 1, vh.b.p, vh.z1.p, false, nullptr, nullptr, w, red, stop, s, false);
+      eH = vh.z1.p;
+    }
   }
   if (vec) {
     kv_prolong_jac<T><<<gv, kThreads, 0, s>>>(A, rr, v.xb.p, H.ny, H.nz, eH, z2H, ksH, v.xa.p, om,

@@ -72,6 +72,7 @@ struct EWork {
 struct EngineOpts {
   double omega = 0.8;        // damped-Jacobi weight
   int coarse_max = 512;      // coarsest level size (dense direct solve)
+  int kc_max = 99;           // levels 1..kc_max run a K-cycle, deeper levels one visit
   EngineOpts();
 };
 
@@ -84,6 +85,7 @@ class Engine {
  public:
   std::vector<ELevel> L;
   DBuf<double> Ainv;           // dense inverse of the coarsest operator
+  DBuf<float> Ainv32;          // its FP32 copy (mixed path)
   DBuf<double> Dtmp;           // its Gauss-Jordan work copy
   int ncoarse = 0;
   bool have32 = false;
@@ -106,6 +108,8 @@ class Engine {
                            double *hist);
   int nlevels() const { return (int)L.size(); }
   template <typename T> EMat<T> mat(int l) const;
+  template <typename T> const void *ainv() const;
+  template <typename T> void dense_solve(const T *r, T *z, const int *stop, cudaStream_t s);
   // Average duration (ms) of the fine-level smoothing sweep, `reps` launches
   // back to back between CUDA events on stream s; precision 0 FP64, 1 FP32.
   double bench_sweep(int precision, int reps, cudaStream_t s);

@@ -274,16 +274,17 @@ __global__ void __launch_bounds__(kThreads, 8) k_kc_x(long long N, const T *__re
   GRID_LOOP(p, N) x[p] = c1 * z1[p] + c2 * z2[p];
 }
 
-// Coarsest level: z = Ainv r with the dense FP64 inverse (one warp per row).
-template <typename T>
-__global__ void k_dense_solve(int n, const double *__restrict__ Ainv, const T *__restrict__ r,
+// Coarsest level: z = Ainv r with the dense inverse (FP64, or its FP32
+// copy in the mixed path), one warp per row, FP64 sums.
+template <typename T, typename AT>
+__global__ void k_dense_solve(int n, const AT *__restrict__ Ainv, const T *__restrict__ r,
                               T *__restrict__ z, const int *stop) {
   if (stop && *stop) return;
   const int lane = threadIdx.x & 31;
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (row >= n) return;
   double acc = 0.0;
-  for (int c = lane; c < n; c += 32) acc += Ainv[(long long)row * n + c] * (double)r[c];
+  for (int c = lane; c < n; c += 32) acc += (double)Ainv[(long long)row * n + c] * (double)r[c];
   for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
   if (lane == 0) z[row] = (T)acc;
 }

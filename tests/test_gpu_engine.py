@@ -29,7 +29,7 @@ def test_engine_reaches_1e8(engine, oracle, kind, kw, precision):
     assert ok and r.status == 0
     rel = true_relres(oracle, P, x)
     assert rel <= 1e-8 * 1.0001, rel
-    assert abs(rel - r.relres) <= 1e-3 * rel + 1e-15
+    assert abs(rel - r.relres) <= 1e-3 * rel + 1e-13  # roundoff floor of a direct solve
     xt, _ = oracle.cg(P, res_rat=1e-13, maxit=100000)
     err = np.linalg.norm(x - xt) / np.linalg.norm(xt)
     assert err < 1e-4, err
