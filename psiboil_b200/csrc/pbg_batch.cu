@@ -120,8 +120,8 @@ class BatchEngine : public BatchEngineBase {
   static void check_shape(const BatchShape &s) {
     if (s.threads < 64 || s.threads > kBThreadsMax || s.threads % 32)
       throw std::invalid_argument("batch: threads must be a multiple of 32 in [64, 512]");
-    if (s.tile_cells < s.threads || s.tile_cells > (1 << 20))
-      throw std::invalid_argument("batch: tile_cells must be in [threads, 2^20]");
+    if (s.tile_cells < s.threads || s.tile_cells > (1 << 20) || s.tile_cells % 4)
+      throw std::invalid_argument("batch: tile_cells must be a multiple of 4 in [threads, 2^20]");
     if (s.grid < 1 || s.grid > 65535) throw std::invalid_argument("batch: grid must be in [1, 65535]");
     if (s.kc_max < 0) throw std::invalid_argument("batch: kc_max must be >= 0");
     if (s.tail_cells < 0 || s.tail_cells > (1 << 20)) throw std::invalid_argument("batch: tail_cells must be in [0, 2^20]");
@@ -133,9 +133,11 @@ class BatchEngine : public BatchEngineBase {
     const int nlev = level_dims(nx, ny, nz, dims);
     if (nlev < 2) throw std::invalid_argument("batch: a problem needs more than 64 cells and at most 12 levels");
     size_t off = 0;
+    // every array ends with 256 bytes of slack: the vectorised kernels' last
+    // group and their shifted pairs of 16-byte loads may read past the end
     auto take = [&](size_t bytes) {
       const size_t o = off;
-      off += align_up(bytes);
+      off += align_up(bytes + 256);
       return o;
     };
     struct Off { size_t c64, w64, s64, b64, c, w, s, b, d, vb, vx, z1, z2, q1, r1, xa, xb; };

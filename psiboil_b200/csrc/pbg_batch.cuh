@@ -547,8 +547,9 @@ __global__ void kb_jac2(BCtx<T> C, int l, int kc) {
   }
 }
 
-// b on level l+1 = block sums of (rhs - A xb) on level l; eight lanes per
-// coarse cell of the tile (restrict_child, sum8)
+// b on level l+1 = block sums of (rhs - A xb) on level l, one thread per
+// coarse cell (restrict_cell): the problems of the batch already fill the
+// GPU, so the eight-lane form is kept for the single-CTA tail.
 template <typename T>
 __global__ void kb_restrict(BCtx<T> C, int l, int kc) {
   BTILE_LOOP(C, l + 1, t) {
@@ -558,14 +559,7 @@ __global__ void kb_restrict(BCtx<T> C, int l, int kc) {
     if (!b_tile_level(S, P, l)) continue;
     const T *r = b_rhs(P, l, kc != 0);
     const BLev<T> &V = P.L[l], &H = P.L[l + 1];
-    const uint32_t total = tl.n * 8u;
-    for (uint32_t base = 0; base < total; base += blockDim.x) {
-      const uint32_t u = base + threadIdx.x;
-      const bool valid = u < total;
-      T v = valid ? restrict_child(V.A, r, V.xb, H.A.g, tl.p0 * 8u + u) : T(0);
-      v = sum8(v);
-      if (valid && (u & 7u) == 0u) H.b[tl.p0 + (u >> 3)] = v;
-    }
+    BCELL_LOOP(tl, Pc) H.b[Pc] = restrict_cell(V.A, r, V.xb, H.A.g, Pc);
   }
 }
 

@@ -365,8 +365,9 @@ void Engine::precond(int l, const T *r, T *z, bool dots, const T *u, double *out
     k_jac2<T><<<g, kThreads, 0, s>>>(A, r, v.b.p, v.q1.p, kc ? w.ks.p + l : nullptr, v.r1.p, v.xb.p,
                                      om, stop); note_launch();
   }
-  k_resid_restrict<T><<<grid_for(H.ncell() * 8), kThreads, 0, s>>>(A, rr, v.xb.p, Geo(H.nx, H.ny, H.nz),
-                                                                   vh.b.p, stop); note_launch();
+  const long long rthreads = H.ncell() >= kRestrictSerialMin ? H.ncell() : H.ncell() * 8;
+  k_resid_restrict<T><<<grid_for(rthreads), kThreads, 0, s>>>(A, rr, v.xb.p, Geo(H.nx, H.ny, H.nz),
+                                                              vh.b.p, stop); note_launch();
   const T *eH, *z2H = nullptr;
   const KScal *ksH = nullptr;
   if (l + 1 == last) {

@@ -133,10 +133,43 @@ __device__ __forceinline__ T sum8(T v) {
   return v;
 }
 
+// One thread per coarse cell, children summed in (a, b, c) order. On large
+// levels this reads better (consecutive threads take fine cells two apart
+// in k) than eight lanes per coarse cell, which spread one warp's load over
+// eight rows; the eight-lane form is for small levels, where one thread per
+// coarse cell would leave most of the GPU idle.
+constexpr uint32_t kRestrictSerialMin = 32768;  // coarse cells
+
+template <typename T>
+__device__ __forceinline__ T restrict_cell(const EMat<T> &A, const T *r, const T *x, const Geo &H, uint32_t P) {
+  const int fx = A.nx > 1 ? 2 : 1, fy = A.ny > 1 ? 2 : 1, fz = A.nz > 1 ? 2 : 1;
+  const Pos Q = H.pos(P);
+  T sum = 0;
+  for (int a = 0; a < fx; ++a) {
+    const int i = Q.i * fx + a;
+    if (i >= A.nx) break;
+    for (int bb = 0; bb < fy; ++bb) {
+      const int j = Q.j * fy + bb;
+      if (j >= A.ny) break;
+      for (int cc = 0; cc < fz; ++cc) {
+        const int k = Q.k * fz + cc;
+        if (k >= A.nz) break;
+        const uint32_t p = ((uint32_t)i * A.ny + j) * A.nz + k;
+        sum += r[p] - ax_at(A, p, Pos{i, j, k}, x);
+      }
+    }
+  }
+  return sum;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 8) k_resid_restrict(EMat<T> A, const T *__restrict__ r, const T *__restrict__ x,
                                  Geo H, T *__restrict__ rH, const int *stop) {
   if (stop && *stop) return;
+  if (H.n >= kRestrictSerialMin) {
+    GRID_LOOP(P, H.n) rH[P] = restrict_cell(A, r, x, H, P);
+    return;
+  }
   const uint32_t total = H.n * 8u;
   // warp-uniform trip count: every lane reaches the shuffles
   for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
