@@ -329,6 +329,25 @@ int pbg_server_wait(pbg_server *s, long long rid, double timeout_s, pbg_result *
 int pbg_server_get_x(pbg_server *s, int sid, double *x, int where);
 int pbg_server_stats_get(pbg_server *s, pbg_server_stats *st);
 
+/* ---------------------------------------------------------------------------
+ * Checkpoints in the reference's .bck format (Scalar::save / Scalar::load,
+ * Src/Field/Scalar/scalar_save.cpp:20-32, scalar_load.cpp:26-37; a Centered
+ * checkpoint is phi then cold, centered_save.cpp:4-23): per field three ints
+ * (block extents with the BW = 3 halo) and the block's doubles, k fastest.
+ * Reading checks the extents (the reference's load does not).
+ * ------------------------------------------------------------------------- */
+/* name_file(base, ".bck", step, cpu) (Src/Global/global_name_file.cpp:4-33) */
+int pbg_bck_name(const char *base, int step, int cpu, char *out, int cap);
+/* nfields full blocks of ni x nj x nk doubles */
+int pbg_bck_write(const char *path, int nfields, const double *const *fields, int ni, int nj, int nk,
+                  int where);
+int pbg_bck_read(const char *path, int nfields, double *const *fields, int ni, int nj, int nk, int where);
+/* compact interior fields of an nx x ny x nz grid (halo written as zero) */
+int pbg_bck_write_compact(const char *path, int nfields, const double *const *fields, int nx, int ny,
+                          int nz, int where);
+int pbg_bck_read_compact(const char *path, int nfields, double *const *fields, int nx, int ny, int nz,
+                         int where);
+
 /* Dot products without allocating (no counterpart in the reference).
  * For callers that cannot call cudaMalloc where they need a dot product —
  * code recorded into a CUDA graph by stream capture, callers whose device

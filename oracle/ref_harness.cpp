@@ -29,7 +29,7 @@
  *   ref_harness --kind single|cyl|batch --n N [--nb NB --rmin R --rmax R
  *               --rc R --ratio Q] [--index I --n2d M --s2 LO HI --s3 LO HI]
  *               --seed S --solver cg|bicgs|ac --resrat RR --maxit M
- *               [--maxcyc C --guard 0|1 --cycle V|F|W] --out PREFIX
+ *               [--maxcyc C --guard 0|1 --cycle V|F|W] [--save NAME] --out PREFIX
  */
 #include "Include/psi-boil.h"
 #include "problem_gen.h"
@@ -49,7 +49,7 @@
 namespace {
 
 struct Args {
-  std::string kind = "single", solver = "cg", out = "ref", cycle = "V";
+  std::string kind = "single", solver = "cg", out = "ref", cycle = "V", save;
   int n = 16, nb = 0, index = 0, n2d = 0, s2lo = 64, s2hi = 512, s3lo = 32, s3hi = 96;
   double rmin = 4, rmax = 16, rc = 0, ratio = 1000;
   unsigned long long seed = 1;
@@ -88,6 +88,7 @@ Args parse(int argc, char **argv) {
     else if (k == "--gpu") a.gpu = std::atoi(nxt());
     else if (k == "--exact") a.exact = std::atoi(nxt());
     else if (k == "--out") a.out = nxt();
+    else if (k == "--save") a.save = nxt();
     else { std::fprintf(stderr, "unknown argument %s\n", k.c_str()); std::exit(2); }
   }
   return a;
@@ -263,6 +264,8 @@ int main(int argc, char **argv) {
       if (rep == 0) secs = dt;
     }
   }
+  /* the reference's own checkpoint of the result (phi, cold) */
+  if (!a.save.empty()) pr.save(a.save.c_str(), 0);
   std::cout.rdbuf(saved);
 
   /* parse the reference's own log lines */

@@ -174,6 +174,19 @@ _SIGS.update({
     "pbg_server_stats_get": (ctypes.c_int, [_vp, ctypes.POINTER(ServerStats)]),
 })
 
+_PP = ctypes.POINTER(ctypes.c_void_p)
+_SIGS.update({
+    "pbg_bck_name": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
+    "pbg_bck_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _PP, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_int]),
+    "pbg_bck_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _PP, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_int]),
+    "pbg_bck_write_compact": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _PP, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_int]),
+    "pbg_bck_read_compact": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _PP, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_int]),
+})
+
 _lib = None
 
 
@@ -711,4 +724,46 @@ class Server:
         st = ServerStats()
         _check(lib().pbg_server_stats_get(self._h, ctypes.byref(st)))
         return st.as_dict()
+
+
+# ---------------------------------------------------------------- .bck checkpoints
+BW = 3  # the reference's halo width
+
+
+def bck_name(base, step=-1, cpu=-1):
+    """name_file(base, ".bck", step, cpu) of the reference."""
+    buf = ctypes.create_string_buffer(len(base) + 64)
+    _check(lib().pbg_bck_name(base.encode(), step, cpu, buf, len(buf)))
+    return buf.value.decode()
+
+
+def _field_ptrs(fields):
+    ps, where = [], None
+    for f in fields:
+        p, w = _ptr(f)
+        if where is not None and w != where:
+            raise ValueError("fields must all be host or all device arrays")
+        ps.append(p)
+        where = w
+    return (ctypes.c_void_p * len(ps))(*ps), where
+
+
+def bck_write(path, fields, dims, compact=True):
+    """Write fields (phi, cold, ...) to a .bck file. compact: interior
+    arrays of an nx x ny x nz grid (dims); else full halo blocks (dims =
+    block extents)."""
+    arr, where = _field_ptrs(fields)
+    fn = lib().pbg_bck_write_compact if compact else lib().pbg_bck_write
+    _check(fn(path.encode(), len(fields), arr, dims[0], dims[1], dims[2], where))
+
+
+def bck_read(path, nfields, dims, compact=True, out=None):
+    """Read nfields fields from a .bck file (see bck_write); host arrays."""
+    if out is None:
+        n = dims[0] * dims[1] * dims[2] if compact else dims[0] * dims[1] * dims[2]
+        out = [np.zeros(n) for _ in range(nfields)]
+    arr, where = _field_ptrs(out)
+    fn = lib().pbg_bck_read_compact if compact else lib().pbg_bck_read
+    _check(fn(path.encode(), nfields, arr, dims[0], dims[1], dims[2], where))
+    return out
 
