@@ -107,6 +107,11 @@ typedef struct {
    * launches in repeated solves with one matrix and costs a longer set-up
    * after every matrix change (a dense inverse, O(cells^3)). */
   int coarse_max;
+  /* CG preconditioner, the reference's Prec codes (preconditioner.h:15-29):
+   * 0 diagonal (Prec::di, default), 1 IC0, 2 IC2, 3 IC3 (incomplete
+   * Cholesky, preconditioner_form.cpp:16-144 / preconditioner_solve.cpp:14-110;
+   * bit for bit with exact_sums). BiCGS takes the diagonal only. */
+  int prec;
 } pbg_params;
 
 typedef struct {

@@ -65,14 +65,14 @@ inline void strides_of(const Scalar &x, long long &si, long long &sj, long long 
 
 class GpuKrylov : public Krylov {
  public:
-  GpuKrylov(const Domain &d, int solver, bool exact_sums)
-      : Krylov(d, Prec::di()), solver_(solver), exact_(exact_sums) {}
+  GpuKrylov(const Domain &d, int solver, const Prec &pc, bool exact_sums)
+      : Krylov(d, Prec::di()), solver_(solver), prec_(int(pc)), exact_(exact_sums) {}
 
   bool solve(Matrix &A, Scalar &x, Scalar &b, const MinIter &mini, const MaxIter &mi,
              const char *name = NULL, const ResRat &rr = ResRat(), const ResTol &rt = ResTol(),
              const real scale = 1.0, const int stalecount = -1,
              const bool precform = true) override {
-    (void)precform;  // the diagonal preconditioner is formed on every call
+    (void)precform;  // the preconditioner is formed on every call
     pbg_session *s = cache_.get(x);
     long long si, sj, sk, off;
     strides_of(x, si, sj, sk, off);
@@ -89,6 +89,7 @@ class GpuKrylov : public Krylov {
     p.scale = scale;
     p.stalecount = stalecount;
     p.exact_sums = exact_ ? 1 : 0;
+    p.prec = prec_;
     pbg_result r;
     check(pbg_solve_strided(s, &x[0][0][0], &b[0][0][0], si, sj, sk, off, PBG_HOST, &p, &r));
     x.exchange();
@@ -104,22 +105,23 @@ class GpuKrylov : public Krylov {
     if (rc != PBG_OK) throw std::runtime_error(pbg_last_error());
   }
   int solver_;
+  int prec_;
   bool exact_;
   SessionCache cache_;
 };
 
-// CG(d, Prec::di()) on the GPU (Src/Solver/Linear/Krylov/cg.h)
+// CG(d, Prec::di() | ic0() | ic2() | ic3()) on the GPU (Src/Solver/Linear/Krylov/cg.h)
 class GpuCG : public GpuKrylov {
  public:
   explicit GpuCG(const Domain &d, const Prec &pc = Prec::di(), bool exact_sums = false)
-      : GpuKrylov(d, PBG_SOLVER_CG, exact_sums) { (void)pc; }
+      : GpuKrylov(d, PBG_SOLVER_CG, pc, exact_sums) {}
 };
 
 // BiCGS(d, Prec::di()) on the GPU (Src/Solver/Linear/Krylov/bicgs.h)
 class GpuBiCGS : public GpuKrylov {
  public:
   explicit GpuBiCGS(const Domain &d, const Prec &pc = Prec::di(), bool exact_sums = false)
-      : GpuKrylov(d, PBG_SOLVER_BICGS, exact_sums) { (void)pc; }
+      : GpuKrylov(d, PBG_SOLVER_BICGS, pc, exact_sums) {}
 };
 
 }  // namespace pbg_psiboil

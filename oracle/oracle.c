@@ -107,13 +107,115 @@ static int stale_step(stale_win *w, double res) {
 
 /* cg.cpp:10-182 with Diagonal (preconditioner_form.cpp:4-13,
  * preconditioner_solve.cpp:4-11) */
+/* Incomplete Cholesky IC0 / IC2 / IC3: IncompleteCholesky0/2/3::form
+ * (preconditioner_form.cpp:16-144) and ::solve (preconditioner_solve.cpp:
+ * 14-110), in the reference's lexicographic order and operation order, on
+ * compact arrays. Entries outside the domain (the reference's halo) are not
+ * stored: the factor writes them but no interior cell reads them, and the
+ * sweeps multiply them by the zero halo of z, so those terms are skipped. */
+typedef struct {
+  int kind;
+  double *c, *w, *s, *b, *tw, *ts, *nw;
+} orc_ic;
+
+static void ic_form(const orc_mat *A, orc_ic *M) {
+  const int nx = A->nx, ny = A->ny, nz = A->nz;
+  const size_t SI = (size_t)ny * nz, SJ = nz;
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        const size_t p = ((size_t)i * ny + j) * nz + k;
+        const int xp = i + 1 < nx, yp = j + 1 < ny, zp = k + 1 < nz, zm = k > 0, ym = j > 0;
+        double sum = A->c[p];
+        sum = sum - M->w[p] * M->w[p];
+        if (M->kind >= 2) sum = sum - M->tw[p] * M->tw[p];
+        if (M->kind == 3) sum = sum - M->nw[p] * M->nw[p];
+        sum = sum - M->s[p] * M->s[p];
+        if (M->kind >= 2) sum = sum - M->ts[p] * M->ts[p];
+        sum = sum - M->b[p] * M->b[p];
+        sum = sqrt(sum);
+        M->c[p] = sum;
+        if (M->kind == 1) { /* IC0 (:16-38) */
+          if (xp) M->w[p + SI] = -A->w[p + SI] / sum;
+          if (yp) M->s[p + SJ] = -A->s[p + SJ] / sum;
+          if (zp) M->b[p + 1] = -A->b[p + 1] / sum;
+          continue;
+        }
+        /* IC2 (:42-84), IC3 (:88-144) */
+        if (xp) M->w[p + SI] = -A->w[p + SI] / sum;
+        if (xp && zm) M->tw[p + SI - 1] = -M->w[p + SI - 1] * M->b[p] / sum;
+        if (M->kind == 3 && xp && ym)
+          M->nw[p + SI - SJ] = (-M->w[p + SI - SJ] * M->s[p] - M->tw[p + SI - SJ] * M->ts[p]) / sum;
+        if (yp) {
+          if (M->kind == 2) M->s[p + SJ] = -A->s[p + SJ] / sum;
+          else M->s[p + SJ] = (-A->s[p + SJ] - M->w[p + SJ] * M->nw[p] - M->nw[p + SJ] * M->s[p]) / sum;
+        }
+        if (yp && zm) {
+          if (M->kind == 2) M->ts[p + SJ - 1] = -M->s[p + SJ - 1] * M->b[p] / sum;
+          else M->ts[p + SJ - 1] = (-M->s[p + SJ - 1] * M->b[p] - M->tw[p + SJ - 1] * M->nw[p]) / sum;
+        }
+        if (zp) M->b[p + 1] = (-A->b[p + 1] - M->w[p + 1] * M->tw[p] - M->s[p + 1] * M->ts[p]) / sum;
+      }
+}
+
+static void ic_solve(const orc_mat *A, const orc_ic *M, double *z, const double *r) {
+  const int nx = A->nx, ny = A->ny, nz = A->nz;
+  const size_t SI = (size_t)ny * nz, SJ = nz;
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        const size_t p = ((size_t)i * ny + j) * nz + k;
+        double sum = r[p];
+        if (i > 0) sum = sum - M->w[p] * z[p - SI];
+        if (M->kind >= 2 && i > 0 && k + 1 < nz) sum = sum - M->tw[p] * z[p - SI + 1];
+        if (M->kind == 3 && i > 0 && j + 1 < ny) sum = sum - M->nw[p] * z[p - SI + SJ];
+        if (j > 0) sum = sum - M->s[p] * z[p - SJ];
+        if (M->kind >= 2 && j > 0 && k + 1 < nz) sum = sum - M->ts[p] * z[p - SJ + 1];
+        if (k > 0) sum = sum - M->b[p] * z[p - 1];
+        z[p] = sum / M->c[p];
+      }
+  for (int i = nx - 1; i >= 0; --i)
+    for (int j = ny - 1; j >= 0; --j)
+      for (int k = nz - 1; k >= 0; --k) {
+        const size_t p = ((size_t)i * ny + j) * nz + k;
+        const int xp = i + 1 < nx, yp = j + 1 < ny, zp = k + 1 < nz, zm = k > 0, ym = j > 0;
+        double sum = z[p];
+        if (xp) sum = sum - M->w[p + SI] * z[p + SI];
+        if (M->kind >= 2 && xp && zm) sum = sum - M->tw[p + SI - 1] * z[p + SI - 1];
+        if (M->kind == 3 && xp && ym) sum = sum - M->nw[p + SI - SJ] * z[p + SI - SJ];
+        if (yp) sum = sum - M->s[p + SJ] * z[p + SJ];
+        if (M->kind >= 2 && yp && zm) sum = sum - M->ts[p + SJ - 1] * z[p + SJ - 1];
+        if (zp) sum = sum - M->b[p + 1] * z[p + 1];
+        z[p] = sum / M->c[p];
+      }
+}
+
+/* cg.cpp:10-182 with Prec::di (prec 0) or Prec::ic0/ic2/ic3 (1, 2, 3) */
+int orc_cg_prec(const orc_mat *A, double *x, const double *b, int mini, int maxit,
+                double res_rat, double res_tol, double scale, int stalecount,
+                double dV, orc_stats *st, double *hist, int prec);
+
 int orc_cg(const orc_mat *A, double *x, const double *b, int mini, int maxit,
            double res_rat, double res_tol, double scale, int stalecount,
            double dV, orc_stats *st, double *hist) {
+  return orc_cg_prec(A, x, b, mini, maxit, res_rat, res_tol, scale, stalecount, dV, st, hist, 0);
+}
+
+int orc_cg_prec(const orc_mat *A, double *x, const double *b, int mini, int maxit,
+                double res_rat, double res_tol, double scale, int stalecount,
+                double dV, orc_stats *st, double *hist, int prec) {
   const size_t N = (size_t)A->nx * A->ny * A->nz;
   double *p = calloc(N, sizeof(double)), *q = calloc(N, sizeof(double));
   double *r = calloc(N, sizeof(double)), *z = calloc(N, sizeof(double));
   double *Mc = calloc(N, sizeof(double));
+  orc_ic M = {prec, NULL, NULL, NULL, NULL, NULL, NULL, NULL};
+  if (prec > 0) {
+    M.c = calloc(N, sizeof(double)); M.w = calloc(N, sizeof(double));
+    M.s = calloc(N, sizeof(double)); M.b = calloc(N, sizeof(double));
+    if (prec >= 2) { M.tw = calloc(N, sizeof(double)); M.ts = calloc(N, sizeof(double)); }
+    if (prec == 3) M.nw = calloc(N, sizeof(double));
+    ic_form(A, &M);
+  }
   for (size_t c = 0; c < N; ++c) Mc[c] = 1.0 / A->c[c];
   orc_resid(A, x, b, r);
   double res = sqrt(orc_dot_voldiv_avg(N, r, r, dV)) / scale;
@@ -124,6 +226,7 @@ int orc_cg(const orc_mat *A, double *x, const double *b, int mini, int maxit,
   if (res < res_tol) {
     s.converged = 1; s.status = 4;
     free(p); free(q); free(r); free(z); free(Mc); free(win.v);
+    free(M.c); free(M.w); free(M.s); free(M.b); free(M.tw); free(M.ts); free(M.nw);
     if (st) *st = s;
     return 1;
   }
@@ -131,7 +234,9 @@ int orc_cg(const orc_mat *A, double *x, const double *b, int mini, int maxit,
   int converged = 0, i, broke = 0;
   s.status = 1;
   for (i = 0; i < maxit; ++i) {
-    for (size_t c = 0; c < N; ++c) z[c] = r[c] * Mc[c];
+    if (prec > 0) ic_solve(A, &M, z, r);
+    else
+      for (size_t c = 0; c < N; ++c) z[c] = r[c] * Mc[c];
     rho = orc_dot(N, r, z);
     if (i == 0) {
       memcpy(p, z, N * sizeof(double));
@@ -157,6 +262,7 @@ int orc_cg(const orc_mat *A, double *x, const double *b, int mini, int maxit,
   s.res = res;
   if (st) *st = s;
   free(p); free(q); free(r); free(z); free(Mc); free(win.v);
+  free(M.c); free(M.w); free(M.s); free(M.b); free(M.tw); free(M.ts); free(M.nw);
   return converged;
 }
 

@@ -56,6 +56,10 @@ double orc_max_abs_voldiv(size_t n, const double *x, double dV);
 int orc_cg(const orc_mat *A, double *x, const double *b, int mini, int maxit,
            double res_rat, double res_tol, double scale, int stalecount,
            double dV, orc_stats *st, double *hist);
+/* the same with a preconditioner: prec 0 Diagonal, 1/2/3 IncompleteCholesky0/2/3 */
+int orc_cg_prec(const orc_mat *A, double *x, const double *b, int mini, int maxit,
+                double res_rat, double res_tol, double scale, int stalecount,
+                double dV, orc_stats *st, double *hist, int prec);
 
 /* BiCGStab with the diagonal preconditioner, BiCGS::solve (bicgs.cpp:9-229). */
 int orc_bicgs(const orc_mat *A, double *x, const double *b, int mini, int maxit,

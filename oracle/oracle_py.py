@@ -57,11 +57,12 @@ def lib():
         L.orc_dot.argtypes = [ctypes.c_size_t, _dp, _dp]
         L.orc_dot_voldiv_avg.restype = ctypes.c_double
         L.orc_dot_voldiv_avg.argtypes = [ctypes.c_size_t, _dp, _dp, ctypes.c_double]
-        for fn in (L.orc_cg, L.orc_bicgs):
+        for fn in (L.orc_cg, L.orc_bicgs, L.orc_cg_prec):
             fn.restype = ctypes.c_int
             fn.argtypes = [ctypes.POINTER(OrcMat), _dp, _dp, ctypes.c_int, ctypes.c_int,
                            ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                            ctypes.c_double, ctypes.POINTER(OrcStats), _dp]
+        L.orc_cg_prec.argtypes = L.orc_cg_prec.argtypes + [ctypes.c_int]
         L.orc_ac_create.restype = ctypes.c_void_p
         L.orc_ac_create.argtypes = [ctypes.POINTER(OrcMat), ctypes.c_void_p, ctypes.c_double]
         L.orc_ac_destroy.argtypes = [ctypes.c_void_p]
@@ -160,16 +161,24 @@ def dot_voldiv_avg(x, y, dV):
     return lib().orc_dot_voldiv_avg(x.size, _p(x), _p(y), dV)
 
 
+PRECS = {"di": 0, "ic0": 1, "ic2": 2, "ic3": 3}
+
+
 def cg(P, b=None, x0=None, mini=1, maxit=20000, res_rat=1e-8, res_tol=1e-18, scale=1.0,
-       stalecount=-1, hist=False, solver="cg"):
+       stalecount=-1, hist=False, solver="cg", prec="di"):
     b = P.b if b is None else b
     x = np.zeros(P.N) if x0 is None else x0.copy()
     st = OrcStats()
     h = np.zeros(maxit + 1) if hist else None
     m = P.mat()
-    fn = lib().orc_cg if solver == "cg" else lib().orc_bicgs
-    fn(ctypes.byref(m), _p(x), _p(b), mini, maxit, res_rat, res_tol, scale, stalecount, P.dV,
-       ctypes.byref(st), _p(h) if hist else None)
+    args = (ctypes.byref(m), _p(x), _p(b), mini, maxit, res_rat, res_tol, scale, stalecount, P.dV,
+            ctypes.byref(st), _p(h) if hist else None)
+    if solver == "cg":
+        lib().orc_cg_prec(*args, PRECS[prec])
+    else:
+        if prec != "di":
+            raise ValueError("BiCGS takes the diagonal preconditioner")
+        lib().orc_bicgs(*args)
     out = dict(converged=st.converged, iterations=st.iterations, printed=st.printed,
                res0=st.res0, res=st.res, status=st.status)
     if hist:
@@ -233,7 +242,7 @@ def harness_available():
 
 
 def run_reference(P, solver="cg", resrat=1e-8, maxit=20000, maxcyc=20, guard=1, cycle="V",
-                  out_prefix=None, dump=True, timeout=3600):
+                  out_prefix=None, dump=True, timeout=3600, prec="di"):
     """Run the compiled reference on P's fixture; returns (meta, arrays)."""
     import tempfile
     kind = {KIND_SINGLE: "single", KIND_CYL: "cyl", KIND_BATCH: "batch"}[P.kind]
@@ -248,7 +257,7 @@ def run_reference(P, solver="cg", resrat=1e-8, maxit=20000, maxcyc=20, guard=1, 
            "--s2", str(a["s2"][0]), str(a["s2"][1]), "--s3", str(a["s3"][0]), str(a["s3"][1]),
            "--seed", str(P.seed), "--solver", solver, "--resrat", repr(resrat),
            "--maxit", str(maxit), "--maxcyc", str(maxcyc), "--guard", str(guard),
-           "--cycle", cycle, "--dump", "1" if dump else "0", "--out", out_prefix]
+           "--cycle", cycle, "--prec", prec, "--dump", "1" if dump else "0", "--out", out_prefix]
     subprocess.run(cmd, check=True, capture_output=True, timeout=timeout)
     meta = {}
     for line in open(out_prefix + ".txt"):

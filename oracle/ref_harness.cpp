@@ -29,7 +29,8 @@
  *   ref_harness --kind single|cyl|batch --n N [--nb NB --rmin R --rmax R
  *               --rc R --ratio Q] [--index I --n2d M --s2 LO HI --s3 LO HI]
  *               --seed S --solver cg|bicgs|ac --resrat RR --maxit M
- *               [--maxcyc C --guard 0|1 --cycle V|F|W] [--save NAME] --out PREFIX
+ *               [--maxcyc C --guard 0|1 --cycle V|F|W] [--prec di|ic0|ic2|ic3] [--save NAME]
+ *               --out PREFIX
  */
 #include "Include/psi-boil.h"
 #include "problem_gen.h"
@@ -49,7 +50,7 @@
 namespace {
 
 struct Args {
-  std::string kind = "single", solver = "cg", out = "ref", cycle = "V", save;
+  std::string kind = "single", solver = "cg", out = "ref", cycle = "V", save, prec = "di";
   int n = 16, nb = 0, index = 0, n2d = 0, s2lo = 64, s2hi = 512, s3lo = 32, s3hi = 96;
   double rmin = 4, rmax = 16, rc = 0, ratio = 1000;
   unsigned long long seed = 1;
@@ -89,6 +90,7 @@ Args parse(int argc, char **argv) {
     else if (k == "--exact") a.exact = std::atoi(nxt());
     else if (k == "--out") a.out = nxt();
     else if (k == "--save") a.save = nxt();
+    else if (k == "--prec") a.prec = nxt();
     else { std::fprintf(stderr, "unknown argument %s\n", k.c_str()); std::exit(2); }
   }
   return a;
@@ -210,14 +212,16 @@ int main(int argc, char **argv) {
   Times time(1, 1.0);
 
   Linear *solver = nullptr;
+  const Prec pc = a.prec == "ic0" ? Prec::ic0() : a.prec == "ic2" ? Prec::ic2()
+                 : a.prec == "ic3" ? Prec::ic3() : Prec::di();
 #ifdef PBG_WITH_ENGINE
   /* the drop-in: the engine's Krylov classes behind the reference's virtual */
-  if (a.gpu && a.solver == "bicgs") solver = new pbg_psiboil::GpuBiCGS(d, Prec::di(), a.exact != 0);
-  else if (a.gpu) solver = new pbg_psiboil::GpuCG(d, Prec::di(), a.exact != 0);
+  if (a.gpu && a.solver == "bicgs") solver = new pbg_psiboil::GpuBiCGS(d, pc, a.exact != 0);
+  else if (a.gpu) solver = new pbg_psiboil::GpuCG(d, pc, a.exact != 0);
   else
 #endif
-  if (a.solver == "bicgs") solver = new BiCGS(d, Prec::di());
-  else solver = new CG(d, Prec::di());
+  if (a.solver == "bicgs") solver = new BiCGS(d, pc);
+  else solver = new CG(d, pc);
 
   Vector uvw(d);
   Scalar p(d), f(d);

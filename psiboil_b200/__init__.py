@@ -57,7 +57,7 @@ class Params(ctypes.Structure):
                 ("mv", ctypes.c_int * 3), ("ms", ctypes.c_int * 3),
                 ("tol", ctypes.c_double), ("inner_tol", ctypes.c_double),
                 ("max_sweeps", ctypes.c_int), ("exact_sums", ctypes.c_int),
-                ("coarse_max", ctypes.c_int)]
+                ("coarse_max", ctypes.c_int), ("prec", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):
@@ -393,9 +393,12 @@ class Session:
 class _Krylov:
     solver = SOLVER_CG
 
+    PREC = {"di": 0, "diagonal": 0, "ic0": 1, "ic2": 2, "ic3": 3}
+
     def __init__(self, session, prec="di", exact_sums=False):
-        if prec not in ("di", "diagonal"):
-            raise NotImplementedError("only the diagonal preconditioner (Prec::di) is provided")
+        if prec not in self.PREC:
+            raise ValueError("prec must be one of %s (Prec::di/ic0/ic2/ic3)" % sorted(self.PREC))
+        self.prec = self.PREC[prec]
         self.session = session
         self.exact_sums = exact_sums
         self.last = None
@@ -408,6 +411,7 @@ class _Krylov:
         p.min_iter, p.max_iter = int(min_iter), int(max_iter)
         p.res_rat, p.res_tol, p.scale, p.stalecount = res_rat, res_tol, scale, int(stalecount)
         p.exact_sums = int(self.exact_sums)
+        p.prec = self.prec
         self.last = self.session.solve(x, b, p)
         if name is not None:
             r = self.last

@@ -424,6 +424,10 @@ int solve_device(pbg_session *s, double *xd, const double *bd, const pbg_params 
     pr.hist_cap = kHistMax;
     pr.res_rat = p->res_rat; pr.res_tol = p->res_tol; pr.scale = p->scale; pr.dV = dV;
     pr.seq = exact_terms(s, p);
+    if (p->prec < 0 || p->prec > 3) return fail(PBG_ERR_ARG, "prec must be 0 (diagonal), 1 (IC0), 2 (IC2) or 3 (IC3)");
+    if (p->prec > 0 && p->solver != PBG_SOLVER_CG)
+      return fail(PBG_ERR_UNSUPPORTED, "incomplete Cholesky is provided for CG only");
+    pr.prec = p->prec;
     RefKrylovResult rr = ref_krylov_solve(s->A.view(), xd, bd, pr, p->solver == PBG_SOLVER_BICGS ? 1 : 0,
                                           s->rkw, s->red, s->kst.p, s->hkst, s->hist.p, s->stream);
     out.status = rr.status;

@@ -165,15 +165,17 @@ __global__ void k_cg_init(MatView<double> A, const double *__restrict__ x,
 }
 
 __global__ void k_cg_pq(MatView<double> A, const double *__restrict__ r, double *pA, double *pB,
-                        double *__restrict__ qv, KrylovState *st, double *part, unsigned *count) {
+                        double *__restrict__ qv, KrylovState *st, double *part, unsigned *count,
+                        const double *__restrict__ zarr) {
   if (st->done) return;
   const int it = st->iter;
   const double *pold = (it & 1) ? pB : pA;
   double *pnew = (it & 1) ? pA : pB;
   const double beta = it == 0 ? 0.0 : __ddiv_rn(st->rho, st->rho_old);
   const long long N = A.ncell();
+  // z = r * Mc (diagonal) or the preconditioner's output zarr
   auto pv = [&](long long s) {
-    double z = __dmul_rn(r[s], mc_of(A.c, s));
+    double z = zarr ? zarr[s] : __dmul_rn(r[s], mc_of(A.c, s));
     return it == 0 ? z : __dadd_rn(z, __dmul_rn(beta, pold[s]));
   };
   double v[1] = {0.0};
@@ -197,7 +199,7 @@ __global__ void k_cg_pq(MatView<double> A, const double *__restrict__ r, double 
 __global__ void k_cg_xr(long long N, const double *__restrict__ c, double *__restrict__ x,
                         double *__restrict__ r, const double *pA, const double *pB,
                         const double *__restrict__ qv, KrylovState *st, double *hist,
-                        double *part, unsigned *count) {
+                        double *part, unsigned *count, int ic) {
   if (st->done) return;
   const int it = st->iter;
   const double *p_ = (it & 1) ? pA : pB;  // the buffer k_cg_pq wrote
@@ -224,12 +226,139 @@ __global__ void k_cg_xr(long long N, const double *__restrict__ c, double *__res
     } else if (!(res == res)) {
       st->done = 1; st->status = ST_NAN; st->iterations = it + 1;
     } else {
-      st->rho_old = st->rho;
-      st->rho = o[1];
+      if (!ic) {  // with an IC preconditioner k_cg_rho forms rho after the solve
+        st->rho_old = st->rho;
+        st->rho = o[1];
+      }
       st->iter = it + 1;
       st->iterations = it + 1;
       if (it + 1 >= st->maxit) { st->done = 1; st->status = ST_MAXITER; }
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Incomplete Cholesky preconditioners (Prec::ic0/ic2/ic3):
+// IncompleteCholesky0/2/3::form (preconditioner_form.cpp:16-144) and ::solve
+// (preconditioner_solve.cpp:14-110). The reference runs factor and sweeps in
+// lexicographic i, j, k order. Every value a cell reads was written by a cell
+// with a smaller index h = a i + b j + k (a = b = 2 for IC0/IC2; a = 5, b = 2
+// for IC3, whose Mnw term reaches (i-1, j+2, k)), so one launch per
+// hyperplane h processes independent cells, each with the reference's
+// arithmetic in the reference's order (__dmul_rn/__dsub_rn/__ddiv_rn/
+// __dsqrt_rn, no contraction): the results are the reference's bit for bit.
+// The arrays are compact and start at zero; the factor's writes outside the
+// domain (the reference's halo, which no interior cell reads) are skipped,
+// and so are the sweeps' terms with a neighbour outside (the reference
+// multiplies them by its zero halo).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double msub(double s, double a, double b) { return __dsub_rn(s, __dmul_rn(a, b)); }
+
+// cell (i, j, k) of hyperplane h for thread index t over the (i, j) plane
+__device__ __forceinline__ bool ic_cell(const MatView<double> &A, int h, int wa, int wb, long long t, int &i,
+                                        int &j, int &k) {
+  i = (int)(t / A.ny);
+  j = (int)(t - (long long)i * A.ny);
+  k = h - wa * i - wb * j;
+  return k >= 0 && k < A.nz;
+}
+
+__global__ void k_ic_form(MatView<double> A, IcFactor M, int h) {
+  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)A.nx * A.ny;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    if (!ic_cell(A, h, M.wa, M.wb, t, i, j, k)) continue;
+    const long long p = ((long long)i * A.ny + j) * A.nz + k;
+    const bool xp = i + 1 < A.nx, yp = j + 1 < A.ny, zp = k + 1 < A.nz, zm = k > 0, ym = j > 0;
+    double sum = A.c[p];
+    sum = msub(sum, M.w[p], M.w[p]);
+    if (M.kind >= 2) sum = msub(sum, M.tw[p], M.tw[p]);
+    if (M.kind == 3) sum = msub(sum, M.nw[p], M.nw[p]);
+    sum = msub(sum, M.s[p], M.s[p]);
+    if (M.kind >= 2) sum = msub(sum, M.ts[p], M.ts[p]);
+    sum = msub(sum, M.b[p], M.b[p]);
+    sum = __dsqrt_rn(sum);
+    M.c[p] = sum;
+    if (M.kind == 1) {
+      if (xp) M.w[p + SI] = __ddiv_rn(-A.w[p + SI], sum);
+      if (yp) M.s[p + SJ] = __ddiv_rn(-A.s[p + SJ], sum);
+      if (zp) M.b[p + 1] = __ddiv_rn(-A.b[p + 1], sum);
+      continue;
+    }
+    if (xp) M.w[p + SI] = __ddiv_rn(-A.w[p + SI], sum);
+    if (xp && zm) M.tw[p + SI - 1] = __ddiv_rn(__dmul_rn(-M.w[p + SI - 1], M.b[p]), sum);
+    if (M.kind == 3 && xp && ym)
+      M.nw[p + SI - SJ] = __ddiv_rn(__dsub_rn(__dmul_rn(-M.w[p + SI - SJ], M.s[p]),
+                                              __dmul_rn(M.tw[p + SI - SJ], M.ts[p])), sum);
+    if (yp) {
+      if (M.kind == 2) M.s[p + SJ] = __ddiv_rn(-A.s[p + SJ], sum);
+      else M.s[p + SJ] = __ddiv_rn(msub(msub(-A.s[p + SJ], M.w[p + SJ], M.nw[p]), M.nw[p + SJ], M.s[p]), sum);
+    }
+    if (yp && zm) {
+      if (M.kind == 2) M.ts[p + SJ - 1] = __ddiv_rn(__dmul_rn(-M.s[p + SJ - 1], M.b[p]), sum);
+      else
+        M.ts[p + SJ - 1] = __ddiv_rn(__dsub_rn(__dmul_rn(-M.s[p + SJ - 1], M.b[p]),
+                                               __dmul_rn(M.tw[p + SJ - 1], M.nw[p])), sum);
+    }
+    if (zp) M.b[p + 1] = __ddiv_rn(msub(msub(-A.b[p + 1], M.w[p + 1], M.tw[p]), M.s[p + 1], M.ts[p]), sum);
+  }
+}
+
+// forward sweep on hyperplane h: z = (r - lower terms) / Mc
+__global__ void k_ic_fwd(MatView<double> A, IcFactor M, int h, const double *__restrict__ r, double *z,
+                         const KrylovState *st) {
+  if (st->done) return;
+  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)A.nx * A.ny;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    if (!ic_cell(A, h, M.wa, M.wb, t, i, j, k)) continue;
+    const long long p = ((long long)i * A.ny + j) * A.nz + k;
+    double sum = r[p];
+    if (i > 0) sum = msub(sum, M.w[p], z[p - SI]);
+    if (M.kind >= 2 && i > 0 && k + 1 < A.nz) sum = msub(sum, M.tw[p], z[p - SI + 1]);
+    if (M.kind == 3 && i > 0 && j + 1 < A.ny) sum = msub(sum, M.nw[p], z[p - SI + SJ]);
+    if (j > 0) sum = msub(sum, M.s[p], z[p - SJ]);
+    if (M.kind >= 2 && j > 0 && k + 1 < A.nz) sum = msub(sum, M.ts[p], z[p - SJ + 1]);
+    if (k > 0) sum = msub(sum, M.b[p], z[p - 1]);
+    z[p] = __ddiv_rn(sum, M.c[p]);
+  }
+}
+
+// backward sweep on hyperplane h: z = (z - upper terms) / Mc
+__global__ void k_ic_bwd(MatView<double> A, IcFactor M, int h, double *z, const KrylovState *st) {
+  if (st->done) return;
+  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)A.nx * A.ny;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    if (!ic_cell(A, h, M.wa, M.wb, t, i, j, k)) continue;
+    const long long p = ((long long)i * A.ny + j) * A.nz + k;
+    const bool xp = i + 1 < A.nx, yp = j + 1 < A.ny, zp = k + 1 < A.nz, zm = k > 0, ym = j > 0;
+    double sum = z[p];
+    if (xp) sum = msub(sum, M.w[p + SI], z[p + SI]);
+    if (M.kind >= 2 && xp && zm) sum = msub(sum, M.tw[p + SI - 1], z[p + SI - 1]);
+    if (M.kind == 3 && xp && ym) sum = msub(sum, M.nw[p + SI - SJ], z[p + SI - SJ]);
+    if (yp) sum = msub(sum, M.s[p + SJ], z[p + SJ]);
+    if (M.kind >= 2 && yp && zm) sum = msub(sum, M.ts[p + SJ - 1], z[p + SJ - 1]);
+    if (zp) sum = msub(sum, M.b[p + 1], z[p + 1]);
+    z[p] = __ddiv_rn(sum, M.c[p]);
+  }
+}
+
+// rho = r.z (Scalar::dot, scalar.h:296-298) for the next CG step
+__global__ void k_cg_rho(long long N, const double *__restrict__ r, const double *__restrict__ z,
+                         KrylovState *st, double *part, unsigned *count) {
+  if (st->done) return;
+  double v[1] = {0.0};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x)
+    v[0] += __dmul_rn(r[p], z[p]);
+  double o[1];
+  if (grid_reduce<1>(v, part, count, o, st->seq, N)) {
+    st->rho_old = st->rho;
+    st->rho = o[0];
   }
 }
 
@@ -635,6 +764,27 @@ void RefKrylovWork::ensure(size_t n, bool bicgs) {
   if (bicgs) { fit(rt); fit(ph); fit(v); fit(s); fit(sh); fit(t); }
 }
 
+IcFactor RefKrylovWork::ic(int kind, size_t n) {
+  auto fit = [n](DBuf<double> &b) { if (b.n < n) b.alloc(n); };
+  fit(z); fit(mc); fit(mw); fit(ms); fit(mb);
+  if (kind >= 2) { fit(mtw); fit(mts); }
+  if (kind == 3) fit(mnw);
+  IcFactor M;
+  M.c = mc.p; M.w = mw.p; M.s = ms.p; M.b = mb.p;
+  M.tw = kind >= 2 ? mtw.p : nullptr;
+  M.ts = kind >= 2 ? mts.p : nullptr;
+  M.nw = kind == 3 ? mnw.p : nullptr;
+  M.kind = kind;
+  M.wa = kind == 3 ? 5 : 2;
+  M.wb = 2;
+  return M;
+}
+
+// hyperplanes of the IC schedule (h = wa i + wb j + k over the grid)
+static int ic_planes(const MatView<double> &A, const IcFactor &M) {
+  return M.wa * (A.nx - 1) + M.wb * (A.ny - 1) + (A.nz - 1) + 1;
+}
+
 void enqueue_ref_setup(const MatView<double> &A, double *x, const double *b, const KrylovParams &pr,
                        int solver, RefKrylovWork &w, const RedPool &red, KrylovState *st,
                        cudaStream_t s) {
@@ -644,6 +794,14 @@ void enqueue_ref_setup(const MatView<double> &A, double *x, const double *b, con
   k_krylov_setup<<<1, 1, 0, s>>>(st, pr, N); note_launch();
   if (solver == 0) {
     PBG_CUDA(cudaMemsetAsync(w.pA.p, 0, sizeof(double) * N, s));
+    if (pr.prec > 0) {  // IncompleteCholesky*::form on every solve (precform)
+      const IcFactor M = w.ic(pr.prec, (size_t)N);
+      DBuf<double> *arr[8] = {&w.z, &w.mc, &w.mw, &w.ms, &w.mb, &w.mtw, &w.mts, &w.mnw};
+      for (DBuf<double> *a : arr)
+        if (a->p) PBG_CUDA(cudaMemsetAsync(a->p, 0, sizeof(double) * N, s));
+      const int H = ic_planes(A, M), gp = grid_for((long long)A.nx * A.ny);
+      for (int h = 0; h < H; ++h) { k_ic_form<<<gp, kThreads, 0, s>>>(A, M, h); note_launch(); }
+    }
     k_cg_init<<<g, kThreads, 0, s>>>(A, x, b, w.r.p, st, red.slot_part(0), red.slot_count(0)); note_launch();
   } else {
     PBG_CUDA(cudaMemsetAsync(w.pA.p, 0, sizeof(double) * N, s));
@@ -655,15 +813,24 @@ void enqueue_ref_setup(const MatView<double> &A, double *x, const double *b, con
 
 void enqueue_ref_iters(const MatView<double> &A, double *x, int solver, int count,
                        RefKrylovWork &w, const RedPool &red, KrylovState *st, double *hist,
-                       cudaStream_t s, bool exact) {
+                       cudaStream_t s, bool exact, int prec) {
   const long long N = A.ncell();
   const int g = exact ? grid_exact(N) : grid_for(N);
   double *P0 = red.slot_part(0), *P1 = red.slot_part(1);
   unsigned *C0 = red.slot_count(0), *C1 = red.slot_count(1);
   for (int it = 0; it < count; ++it) {
-    if (solver == 0) {
-      k_cg_pq<<<g, kThreads, 0, s>>>(A, w.r.p, w.pA.p, w.pB.p, w.q.p, st, P0, C0); note_launch();
-      k_cg_xr<<<g, kThreads, 0, s>>>(N, A.c, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1); note_launch();
+    if (solver == 0 && prec > 0) {
+      // z = M^-1 r (forward and backward sweeps), rho = r.z, then the CG step
+      const IcFactor M = w.ic(prec, (size_t)N);
+      const int H = ic_planes(A, M), gp = grid_for((long long)A.nx * A.ny);
+      for (int h = 0; h < H; ++h) { k_ic_fwd<<<gp, kThreads, 0, s>>>(A, M, h, w.r.p, w.z.p, st); note_launch(); }
+      for (int h = H - 1; h >= 0; --h) { k_ic_bwd<<<gp, kThreads, 0, s>>>(A, M, h, w.z.p, st); note_launch(); }
+      k_cg_rho<<<g, kThreads, 0, s>>>(N, w.r.p, w.z.p, st, P0, C0); note_launch();
+      k_cg_pq<<<g, kThreads, 0, s>>>(A, w.r.p, w.pA.p, w.pB.p, w.q.p, st, P0, C0, w.z.p); note_launch();
+      k_cg_xr<<<g, kThreads, 0, s>>>(N, A.c, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1, 1); note_launch();
+    } else if (solver == 0) {
+      k_cg_pq<<<g, kThreads, 0, s>>>(A, w.r.p, w.pA.p, w.pB.p, w.q.p, st, P0, C0, nullptr); note_launch();
+      k_cg_xr<<<g, kThreads, 0, s>>>(N, A.c, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1, 0); note_launch();
     } else {
       k_bi_rho<<<g, kThreads, 0, s>>>(N, w.rt.p, w.r.p, st, P0, C0); note_launch();
       k_bi_p<<<g, kThreads, 0, s>>>(N, A.c, w.r.p, w.pA.p, w.v.p, w.ph.p, st); note_launch();
@@ -689,7 +856,7 @@ RefKrylovResult ref_krylov_solve(const MatView<double> &A, double *x, const doub
     if (hst->done || enq >= pr.maxit) break;
     int cnt = chunk;
     if (enq + cnt > pr.maxit) cnt = pr.maxit - enq;
-    enqueue_ref_iters(A, x, solver, cnt, w, red, st, hist, s, pr.seq != nullptr);
+    enqueue_ref_iters(A, x, solver, cnt, w, red, st, hist, s, pr.seq != nullptr, pr.prec);
     enq += cnt;
     if (chunk < 256) chunk *= 2;
   }
@@ -789,7 +956,7 @@ void RefAC::smooth(int l, int mi, double res_rat, double res_tol, int ms, RefKry
   pr.seq = seq;
   MatView<double> A = view(l);
   enqueue_ref_setup(A, L[l].phi.p, L[l].fnew.p, pr, 0, w, red, st, s);
-  enqueue_ref_iters(A, L[l].phi.p, 0, mi, w, red, st, nullptr, s, seq != nullptr);
+  enqueue_ref_iters(A, L[l].phi.p, 0, mi, w, red, st, nullptr, s, seq != nullptr, 0);
 }
 
 void RefAC::restrict_to(int l, RedPool &red, double *dmean, cudaStream_t s) {

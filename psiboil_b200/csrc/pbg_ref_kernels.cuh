@@ -9,7 +9,15 @@
 
 namespace pbg {
 
+// Incomplete Cholesky factor (compact arrays; kind 1 = IC0, 2 = IC2, 3 =
+// IC3) and the hyperplane weights h = wa i + wb j + k of its schedule.
+struct IcFactor {
+  double *c, *w, *s, *b, *tw, *ts, *nw;
+  int kind, wa, wb;
+};
+
 struct KrylovParams {
+  int prec = 0;            // Prec code: 0 diagonal, 1 IC0, 2 IC2, 3 IC3 (CG)
   int mini, maxit, stalecount, hist_cap;
   double res_rat, res_tol, scale, dV;
   double *seq = nullptr;   // exact-order reduction terms (2 x ncell), null: tree
@@ -17,7 +25,9 @@ struct KrylovParams {
 
 struct RefKrylovWork {
   DBuf<double> r, q, pA, pB, rt, ph, v, s, sh, t;
+  DBuf<double> z, mc, mw, ms, mb, mtw, mts, mnw;  // IC preconditioner
   void ensure(size_t n, bool bicgs);
+  IcFactor ic(int kind, size_t n);
 };
 
 struct RefKrylovResult {
@@ -36,7 +46,7 @@ void enqueue_ref_setup(const MatView<double> &A, double *x, const double *b, con
                        cudaStream_t s);
 void enqueue_ref_iters(const MatView<double> &A, double *x, int solver, int count,
                        RefKrylovWork &w, const RedPool &red, KrylovState *st, double *hist,
-                       cudaStream_t s, bool exact);
+                       cudaStream_t s, bool exact, int prec);
 RefKrylovResult ref_krylov_solve(const MatView<double> &A, double *x, const double *b,
                                  const KrylovParams &pr, int solver, RefKrylovWork &w,
                                  const RedPool &red, KrylovState *st, KrylovState *hst,

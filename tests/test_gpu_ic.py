@@ -1,0 +1,57 @@
+"""CG with the incomplete Cholesky preconditioners (Prec::ic0/ic2/ic3) on the
+GPU: factor and sweeps scheduled on hyperplanes, each cell with the
+reference's arithmetic in the reference's order. With exact sums the
+iterations and the solution equal the oracle's (which equals the compiled
+reference's, tests/test_oracle_vs_reference.py) bit for bit; with tree sums
+the solution agrees to 1e-10 and the iterations to +-2."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CASES = [(0, dict(n=10)), (1, dict(n=14, nb=2, rmin=2.0, rmax=3.0, rc=3.0)),
+         (2, dict(index=1, n2d=2, s2=(10, 14), s3=(6, 8))), (2, dict(index=0, n2d=2, s2=(10, 14), s3=(6, 8))),
+         (0, dict(n=24))]
+
+
+@pytest.mark.parametrize("prec", ["ic0", "ic2", "ic3"])
+@pytest.mark.parametrize("kind,kw", CASES)
+def test_ic_cg_bit_exact(engine, oracle, prec, kind, kw):
+    P = oracle.Problem(kind, 5, **kw)
+    if prec == "ic3" and P.dims[2] == 1:
+        pytest.skip("the reference's IC3 breaks down on 2-D grids (checked on the oracle)")
+    xo, st = oracle.cg(P, prec=prec, res_rat=1e-8, res_tol=1e-15)
+    with engine.Session(*P.dims, P.h) as s:
+        s.assemble_pressure(P.rho, P.solid)
+        for exact in (True, False):
+            x = np.zeros(P.N)
+            cg = engine.CG(s, prec=prec, exact_sums=exact)
+            ok = cg.solve(x, P.b.copy(), 1, 20000, None, 1e-8, 1e-15)
+            assert ok == bool(st["converged"])
+            if exact:
+                assert cg.last.iterations == st["iterations"]
+                assert np.array_equal(x, xo)
+            else:
+                assert abs(cg.last.iterations - st["iterations"]) <= 2
+                assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-10
+
+
+def test_ic_reduces_iterations(engine, oracle):
+    P = oracle.Problem(1, 4, n=24, nb=3, rmin=2.0, rmax=4.0, rc=5.0)
+    its = {}
+    with engine.Session(*P.dims, P.h) as s:
+        s.assemble_pressure(P.rho, P.solid)
+        for prec in ("di", "ic0", "ic2", "ic3"):
+            x = np.zeros(P.N)
+            cg = engine.CG(s, prec=prec)
+            assert cg.solve(x, P.b.copy(), 1, 20000, None, 1e-8, 1e-15)
+            its[prec] = cg.last.iterations
+    assert its["ic0"] < its["di"] and its["ic2"] <= its["ic0"] and its["ic3"] <= its["ic2"]
+
+
+def test_ic_rejected_for_bicgs(engine, oracle):
+    P = oracle.Problem(0, 5, n=8)
+    with engine.Session(*P.dims, P.h) as s:
+        s.assemble_pressure(P.rho, P.solid)
+        with pytest.raises(engine.PbgError):
+            engine.BiCGS(s, prec="ic2").solve(np.zeros(P.N), P.b.copy(), 1, 100)

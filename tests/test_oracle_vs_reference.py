@@ -22,3 +22,19 @@ def test_live_cg_and_ac(oracle, kind, kw):
     x, st = oracle.AC(P).cycle()
     assert st["cycles"] == int(meta["cycles"])
     assert np.array_equal(x, arr["x"])
+
+
+@pytest.mark.parametrize("prec", ["ic0", "ic2", "ic3"])
+@pytest.mark.parametrize("kind,kw", [(0, dict(n=10)), (1, dict(n=12, nb=2, rmin=2.0, rmax=3.0, rc=3.0)),
+                                     (2, dict(index=1, n2d=2, s2=(10, 14), s3=(6, 8))),
+                                     (2, dict(index=0, n2d=2, s2=(10, 14), s3=(6, 8)))])
+def test_oracle_ic_cg_equals_reference(oracle, prec, kind, kw):
+    """CG with Prec::ic0/ic2/ic3: the oracle's factor and sweeps give the
+    compiled reference's iterations and solution bit for bit (on 2-D grids
+    the reference's IC3 factor breaks down into NaN; the oracle does the
+    same)."""
+    P = oracle.Problem(kind, 5, **kw)
+    meta, arr = oracle.run_reference(P, solver="cg", resrat=1e-8, prec=prec)
+    x, st = oracle.cg(P, prec=prec, res_rat=1e-8, res_tol=1e-15)
+    assert st["printed"] == int(meta["iterations"])
+    assert np.array_equal(x, arr["x"], equal_nan=True)
