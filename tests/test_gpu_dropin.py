@@ -54,3 +54,20 @@ def test_reference_ac_with_gpu_krylov_tree_sums():
                    "--gpu", "1", "--exact", "0"])
     assert abs(int(meta["cycles"][0]) - int(g["ac_cycles"])) <= 2
     assert np.abs(x - g["ac_x"]).max() <= 1e-8 * np.abs(g["ac_x"]).max()
+
+
+@pytest.mark.skipif(not os.path.exists(EXE), reason="GPU-backed reference harness not built")
+@pytest.mark.parametrize("case,args,prec", [
+    ("single16", ["--kind", "single", "--n", "16"], "ic0"),
+    ("single16", ["--kind", "single", "--n", "16"], "ic2"),
+    ("single16", ["--kind", "single", "--n", "16"], "ic3"),
+    ("cyl24", ["--kind", "cyl", "--n", "24", "--nb", "3", "--rmin", "2.0", "--rmax", "4.0", "--rc", "5.0"], "ic2")])
+def test_reference_with_gpu_ic_cg_is_bit_exact(case, args, prec):
+    """`new GpuCG(d, Prec::ic2())` in place of `new CG(d, Prec::ic2())`: the
+    reference's pressure solve gives the CPU reference's solution and
+    iteration count bit for bit (golden fixtures from the CPU reference)."""
+    g = load(case)
+    x, meta = run(args + ["--seed", "7", "--solver", "cg", "--prec", prec, "--resrat", "1e-8",
+                          "--gpu", "1", "--exact", "1"])
+    assert np.array_equal(x, g["cg_" + prec + "_x"])
+    assert int(meta["iterations"][0]) == int(g["cg_" + prec + "_iterations"])
