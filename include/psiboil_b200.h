@@ -175,6 +175,44 @@ int pbg_active_upload(pbg_session *s, const int *aflag, long long si, long long 
  * active flags to !solid. Compact arrays. */
 int pbg_assemble_pressure(pbg_session *s, const double *rho, const uint8_t *solid, int where);
 
+/* The pressure-correction step around the solve (compact layouts; faces:
+ * u (nx+1) x ny x nz, v nx x (ny+1) x nz, w nx x ny x (nz+1), k fastest,
+ * face f of u between cells f-1 and f; w may be NULL in 2-D). Bit for bit
+ * the reference on a uniform grid whose coordinates are exact multiples of
+ * h (n a power of two).
+ *
+ * pbg_assemble_mix: Pressure::discretize (pressure_discretize.cpp:24-148)
+ * for a two-phase Matter (matter.cpp:78): cell density PropertyMix
+ * rho_a*col + rho_b*(1-col) with col clamped to [0,1]
+ * (property_value.cpp:52-70), face density the arithmetic mean of the two
+ * cells (:73-85; a boundary face takes the boundary cell's), dS/dx with
+ * dx = h/2 from a boundary cell's centre to the wall, then
+ * Centered::create_system_bnd (Neumann c -= a_bnd; Dirichlet a_bnd = 0).
+ * col NULL: one fluid of density rho_a. solid (1 = solid, may be NULL):
+ * faces to solid cells cut, solid cells c *= 1e-12. Replaces the host
+ * assembly of Pressure(...)/discretize(). Sets the active flags. */
+int pbg_assemble_mix(pbg_session *s, const double *col, double rho_a, double rho_b,
+                     const uint8_t *solid, int where);
+/* Pressure::update_rhs without an immersed body (pressure_update_rhs.cpp:
+ * 16-139): rhs = dS/dt * (u_w - u_e + v_s - v_n + w_b - w_t) per cell. */
+int pbg_divergence(pbg_session *s, const double *u, const double *v, const double *w, double dt,
+                   double *rhs, int where);
+/* Momentum::project without an immersed body (momentum_project.cpp:11-80):
+ * every interior face u += (p[i-1] - p[i]) / rho_face * dt / h (rho_face
+ * as in pbg_assemble_mix). The normal faces on the domain boundary keep
+ * the caller's values (the boundary condition; walls are 0), w is not
+ * touched in 2-D. u, v, w updated in place. */
+int pbg_project(pbg_session *s, const double *p, const double *col, double rho_a, double rho_b,
+                double dt, double *u, double *v, double *w, int where);
+/* One pressure-correction step on the device: pbg_assemble_mix,
+ * pbg_divergence, pbg_solve of p (p in: initial guess; solver scale
+ * params->scale / dt as Centered::solve passes, centered_solve.cpp:25-31)
+ * and pbg_project. u, v, w and p updated in place; with PBG_HOST each
+ * input crosses to the device once and each output back once. */
+int pbg_pressure_step(pbg_session *s, const double *col, double rho_a, double rho_b,
+                      const uint8_t *solid, double dt, double *u, double *v, double *w,
+                      double *p, int where, const pbg_params *params, pbg_result *res);
+
 /* Solve A x = b with x as initial guess and result (x updated in place,
  * b read only), compact layout. The reference-parity solvers follow
  * Linear::solve / AC::cycle semantics (x0 as given, residual measure
@@ -210,6 +248,12 @@ int pbg_ac_level_matrix(pbg_session *s, int level, double *out7, int where);
  * stream. With rho == NULL only dims/h are returned. */
 int pbg_generate(int kind, const double *params, uint64_t seed, int dims[3], double *h,
                  double *rho, uint8_t *solid, double *b);
+/* Flow state of one pressure-correction step of the same workload: the
+ * liquid colour col (cells), a predicted velocity u, v, w (face layouts of
+ * pbg_assemble_mix; walls 0) drawn from stream params[12], and the phase
+ * densities rho[0] liquid, rho[1] vapour. */
+int pbg_generate_flow(int kind, const double *params, uint64_t seed, double *col, double *u,
+                      double *v, double *w, double rho[2]);
 
 /* Instrumentation (no reference counterpart): kernels launched by this
  * library so far in the process; the session's CUDA stream (for events);

@@ -11,8 +11,7 @@
 #include <stdlib.h>
 #include "problem_gen.h"
 
-int orc_gen_problem(int kind, const double *params, uint64_t seed, int *dims,
-                    uint8_t *solid, double *hb, double *out) {
+static void make_desc(int kind, const double *params, uint64_t seed, pbg_problem_desc *dd) {
   pbg_problem_desc d;
   int n = (int)params[0];
   if (kind == 0) pbg_desc_single_bubble(&d, n, seed);
@@ -22,6 +21,13 @@ int orc_gen_problem(int kind, const double *params, uint64_t seed, int *dims,
   else
     pbg_desc_batch_member(&d, seed, (int)params[6], (int)params[7], (int)params[8],
                           (int)params[9], (int)params[10], (int)params[11]);
+  *dd = d;
+}
+
+int orc_gen_problem(int kind, const double *params, uint64_t seed, int *dims,
+                    uint8_t *solid, double *hb, double *out) {
+  pbg_problem_desc d;
+  make_desc(kind, params, seed, &d);
   dims[0] = d.nx; dims[1] = d.ny; dims[2] = d.nz;
   hb[0] = d.h;
   hb[1] = d.rho_liquid / d.rho_vapour;
@@ -33,5 +39,20 @@ int orc_gen_problem(int kind, const double *params, uint64_t seed, int *dims,
   double *m = out + 2 * N;
   pbg_gen_assemble(d.nx, d.ny, d.nz, d.h, d.bc, rho, solid, m, m + N, m + 2 * N, m + 3 * N,
                    m + 4 * N, m + 5 * N, m + 6 * N, m + 7 * N);
+  return 0;
+}
+
+/* Flow state of a pressure-correction step (pbg_gen_flow): colour and the
+ * face velocities u, v, w, plus the two phase densities in rho2 (liquid,
+ * vapour) and the pressure boundary types in bc (imin..kmax). `stream` is
+ * params[12]. */
+int orc_gen_flow(int kind, const double *params, uint64_t seed, double *col, double *u,
+                 double *v, double *w, double *rho2, int *bc) {
+  pbg_problem_desc d;
+  make_desc(kind, params, seed, &d);
+  for (int f = 0; f < 6; ++f) bc[f] = d.bc[f];
+  rho2[0] = d.rho_liquid;
+  rho2[1] = d.rho_vapour;
+  pbg_gen_flow(&d, (uint64_t)params[12], col, u, v, w);
   return 0;
 }

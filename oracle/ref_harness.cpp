@@ -30,7 +30,17 @@
  *               --rc R --ratio Q] [--index I --n2d M --s2 LO HI --s3 LO HI]
  *               --seed S --solver cg|bicgs|ac --resrat RR --maxit M
  *               [--maxcyc C --guard 0|1 --cycle V|F|W] [--prec di|ic0|ic2|ic3] [--save NAME]
- *               --out PREFIX
+ *               [--step 1 --dt DT] --out PREFIX
+ *
+ * --step 1 runs one pressure-correction step with the reference's own
+ * classes and no override: a two-phase Matter (liquid and vapour densities
+ * of the workload mixed by the colour function of pbg_gen_flow,
+ * matter.cpp:78 -> PropertyMix), `Pressure pr(...)` whose constructor runs
+ * Pressure::discretize, `pr.solve(...)` (Pressure::update_rhs from the
+ * predicted velocity u*, then the Krylov solver with scale dti), and
+ * `Momentum::project(p)` (momentum_project.cpp:11-80). It writes the
+ * matrix, the right-hand side, the pressure and the projected faces
+ * (PREFIX.u/.v/.w, the layouts of pbg_gen_flow).
  */
 #include "Include/psi-boil.h"
 #include "problem_gen.h"
@@ -56,6 +66,8 @@ struct Args {
   unsigned long long seed = 1;
   double resrat = 1e-8;
   int maxit = 20000, maxcyc = 20, guard = 1, dump = 1, repeat = 1, gpu = 0, exact = 1;
+  int step = 0;
+  double dt = 1.0;
 };
 
 Args parse(int argc, char **argv) {
@@ -91,6 +103,8 @@ Args parse(int argc, char **argv) {
     else if (k == "--out") a.out = nxt();
     else if (k == "--save") a.save = nxt();
     else if (k == "--prec") a.prec = nxt();
+    else if (k == "--step") a.step = std::atoi(nxt());
+    else if (k == "--dt") a.dt = std::atof(nxt());
     else { std::fprintf(stderr, "unknown argument %s\n", k.c_str()); std::exit(2); }
   }
   return a;
@@ -179,6 +193,153 @@ class Fixture : public Pressure {
   bool ready = false;
 };
 
+/* The reference's own Pressure (no override), with read access to the
+ * matrix and the right-hand side it assembled. */
+class Probe : public Pressure {
+ public:
+  Probe(const Scalar &p, const Scalar &f, const Vector &u, Times &t, Linear *sm, Matter *m)
+      : Pressure(p, f, u, t, sm, m) {}
+  void dump_matrix(const pbg_problem_desc &D, std::ofstream &f) const {
+    const Scalar *arr[8] = {&A.c, &A.w, &A.e, &A.s, &A.n, &A.b, &A.t, &A.ci};
+    for (auto *s : arr) dump_cells(*s, D, f);
+  }
+  void dump_rhs(const pbg_problem_desc &D, std::ofstream &f) const { dump_cells(fnew, D, f); }
+
+  static void dump_cells(const Scalar &s, const pbg_problem_desc &D, std::ofstream &f) {
+    const int B = boil::BW;
+    std::vector<double> out(pbg_ncells(&D));
+    for (int i = 0; i < D.nx; ++i)
+      for (int j = 0; j < D.ny; ++j)
+        for (int k = 0; k < D.nz; ++k) out[((size_t)i * D.ny + j) * D.nz + k] = s[i + B][j + B][k + B];
+    f.write((const char *)out.data(), out.size() * sizeof(double));
+  }
+};
+
+/* Face extents of one component in the layouts of pbg_gen_flow. */
+void face_dims(const pbg_problem_desc &D, int m, int &ex, int &ey, int &ez) {
+  ex = D.nx + (m == 0);
+  ey = D.ny + (m == 1);
+  ez = D.nz + (m == 2);
+}
+
+void put_faces(Vector &uvw, int m, const pbg_problem_desc &D, const std::vector<double> &src) {
+  const Comp comps[3] = {Comp::u(), Comp::v(), Comp::w()};
+  const int B = boil::BW;
+  int ex, ey, ez;
+  face_dims(D, m, ex, ey, ez);
+  for (int i = 0; i < ex; ++i)
+    for (int j = 0; j < ey; ++j)
+      for (int k = 0; k < ez; ++k) uvw[comps[m]][i + B][j + B][k + B] = src[((size_t)i * ey + j) * ez + k];
+}
+
+void write_faces(const Vector &uvw, int m, const pbg_problem_desc &D, const std::string &path) {
+  const Comp comps[3] = {Comp::u(), Comp::v(), Comp::w()};
+  const int B = boil::BW;
+  int ex, ey, ez;
+  face_dims(D, m, ex, ey, ez);
+  std::vector<double> out((size_t)ex * ey * ez);
+  for (int i = 0; i < ex; ++i)
+    for (int j = 0; j < ey; ++j)
+      for (int k = 0; k < ez; ++k) out[((size_t)i * ey + j) * ez + k] = uvw[comps[m]][i + B][j + B][k + B];
+  std::ofstream f(path, std::ios::binary);
+  f.write((const char *)out.data(), out.size() * sizeof(double));
+}
+
+/* --step 1: one pressure-correction step through the reference's classes. */
+int run_step(const Args &a, const pbg_problem_desc &D) {
+  const size_t N = pbg_ncells(&D);
+  std::vector<double> col(N), fu(pbg_nfaces(&D, 0)), fv(pbg_nfaces(&D, 1)), fw(pbg_nfaces(&D, 2));
+  pbg_gen_flow(&D, 0, col.data(), fu.data(), fv.data(), fw.data());
+
+  std::ostringstream log;
+  std::streambuf *saved = std::cout.rdbuf(log.rdbuf());
+  std::cout.precision(17);
+
+  const double h = D.h;
+  Grid1D gx(Range<real>(0.0, D.nx * h), Range<real>(h, h), D.nx, Periodic::no());
+  Grid1D gy(Range<real>(0.0, D.ny * h), Range<real>(h, h), D.ny, Periodic::no());
+  Grid1D *gz = (D.nz > 1) ? new Grid1D(Range<real>(0.0, D.nz * h), Range<real>(h, h), D.nz, Periodic::no())
+                          : new Grid1D(h);
+  Domain d(gx, gy, *gz);
+  Times time(1, a.dt);
+  const Prec pc = a.prec == "ic0" ? Prec::ic0() : a.prec == "ic2" ? Prec::ic2()
+                 : a.prec == "ic3" ? Prec::ic3() : Prec::di();
+  Linear *solver = nullptr;
+  if (a.solver == "bicgs") solver = new BiCGS(d, pc);
+  else solver = new CG(d, pc);
+
+  const Dir dirs[6] = {Dir::imin(), Dir::imax(), Dir::jmin(), Dir::jmax(), Dir::kmin(), Dir::kmax()};
+  Scalar p(d), f(d), c(d);
+  for (int q = 0; q < 6; ++q) {
+    const bool pseudo = D.nz == 1 && q >= 4;
+    if (pseudo) p.bc().add(BndCnd(dirs[q], BndType::pseudo()));
+    else if (D.bc[q] == PBG_BC_DIRICHLET) p.bc().add(BndCnd(dirs[q], BndType::dirichlet(), 0.0));
+    else p.bc().add(BndCnd(dirs[q], BndType::neumann()));
+    c.bc().add(BndCnd(dirs[q], pseudo ? BndType::pseudo() : BndType::neumann()));
+  }
+  Vector uvw(d), xyz(d);
+  const Comp comps[3] = {Comp::u(), Comp::v(), Comp::w()};
+  for (int m = 0; m < 3; ++m)
+    for (int q = 0; q < 6; ++q) {
+      const BndType t = (D.nz == 1 && q >= 4) ? BndType::pseudo() : BndType::wall();
+      uvw.bc(comps[m]).add(BndCnd(dirs[q], t));
+      xyz.bc(comps[m]).add(BndCnd(dirs[q], t));
+    }
+  const int B = boil::BW;
+  for (int i = 0; i < D.nx; ++i)
+    for (int j = 0; j < D.ny; ++j)
+      for (int k = 0; k < D.nz; ++k) c[i + B][j + B][k + B] = col[((size_t)i * D.ny + j) * D.nz + k];
+  c.bnd_update();
+  c.exchange_all();
+  put_faces(uvw, 0, D, fu);
+  put_faces(uvw, 1, D, fv);
+  put_faces(uvw, 2, D, fw);
+
+  Matter liquid(d), vapour(d);
+  liquid.rho(D.rho_liquid);
+  vapour.rho(D.rho_vapour);
+  Matter mix(liquid, vapour, &c);
+
+  Probe pr(p, f, uvw, time, solver, &mix);
+  p = 0.0;
+  auto t0 = std::chrono::steady_clock::now();
+  pr.solve(ResTol(boil::atto), ResRat(a.resrat), "refsolve", a.maxit);
+  Momentum ns(uvw, xyz, time, solver, &mix);
+  ns.project(p);
+  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  std::cout.rdbuf(saved);
+
+  int iters = -1;
+  double res_final = -1, ratio_final = -1;
+  std::istringstream in(log.str());
+  std::string line;
+  while (std::getline(in, line)) {
+    size_t q;
+    if ((q = line.find("refsolve, residual = ")) != std::string::npos)
+      std::sscanf(line.c_str() + q, "refsolve, residual = %lf, ratio = %lf, iterations = %d", &res_final,
+                  &ratio_final, &iters);
+  }
+  {
+    std::ofstream fa(a.out + ".A", std::ios::binary);
+    pr.dump_matrix(D, fa);
+    std::ofstream fb(a.out + ".b", std::ios::binary);
+    pr.dump_rhs(D, fb);
+    std::ofstream fx(a.out + ".x", std::ios::binary);
+    Probe::dump_cells(p, D, fx);
+  }
+  write_faces(uvw, 0, D, a.out + ".u");
+  write_faces(uvw, 1, D, a.out + ".v");
+  write_faces(uvw, 2, D, a.out + ".w");
+  std::ofstream fm(a.out + ".txt");
+  fm.precision(17);
+  fm << "nx " << D.nx << "\nny " << D.ny << "\nnz " << D.nz << "\n";
+  fm << "solver " << a.solver << "\niterations " << iters << "\nresidual " << res_final
+     << "\nratio " << ratio_final << "\nseconds " << secs << "\n";
+  std::printf("{\"step\": 1, \"solver\": \"%s\", \"iterations\": %d, \"ratio\": %.17g, "
+              "\"seconds\": %.6f, \"cells\": %zu}\n", a.solver.c_str(), iters, ratio_final, secs, N);
+  return 0;
+}
+
 pbg_problem_desc make_desc(const Args &a) {
   pbg_problem_desc d;
   if (a.kind == "single") pbg_desc_single_bubble(&d, a.n, a.seed);
@@ -193,6 +354,7 @@ pbg_problem_desc make_desc(const Args &a) {
 int main(int argc, char **argv) {
   Args a = parse(argc, argv);
   pbg_problem_desc D = make_desc(a);
+  if (a.step) return run_step(a, D);
   const size_t N = pbg_ncells(&D);
   std::vector<double> rho(N), rhs(N);
   std::vector<uint8_t> solid(N);

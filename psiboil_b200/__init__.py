@@ -90,6 +90,14 @@ _SIGS = {
     "pbg_matrix_download": (ctypes.c_int, [_vp] + [_vp] * 7 + [ctypes.c_int]),
     "pbg_active_upload": (ctypes.c_int, [_vp, _vp, _ll, _ll, _ll, _ll, ctypes.c_int]),
     "pbg_assemble_pressure": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
+    "pbg_assemble_mix": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_double, _vp, ctypes.c_int]),
+    "pbg_divergence": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, _vp, ctypes.c_int]),
+    "pbg_project": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                   _vp, _vp, _vp, ctypes.c_int]),
+    "pbg_pressure_step": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_double, _vp, ctypes.c_double,
+                                         _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.POINTER(Params),
+                                         ctypes.POINTER(Result)]),
+    "pbg_generate_flow": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_uint64, _vp, _vp, _vp, _vp, _dp]),
     "pbg_solve": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.POINTER(Params),
                                  ctypes.POINTER(Result)]),
     "pbg_solve_strided": (ctypes.c_int, [_vp, _vp, _vp, _ll, _ll, _ll, _ll, ctypes.c_int,
@@ -319,6 +327,40 @@ class Session:
             raise ValueError("rho and solid must live in the same memory")
         _check(lib().pbg_assemble_pressure(self._h, pr, ps, where))
 
+    def assemble_mix(self, col, rho_a, rho_b=1.0, solid=None):
+        """Pressure::discretize of a two-phase mixture on the device
+        (arithmetic face density from the colour; col None: one fluid)."""
+        pc, where = _ptr(col)
+        ps, where2 = _ptr(solid)
+        if col is not None and solid is not None and where != where2:
+            raise ValueError("col and solid must live in the same memory")
+        if col is None:
+            where = where2
+        _check(lib().pbg_assemble_mix(self._h, pc, rho_a, rho_b, ps, where))
+
+    def divergence(self, u, v, w, dt, rhs):
+        """Pressure::update_rhs: rhs from the face velocities."""
+        pu, where = _ptr(u)
+        _check(lib().pbg_divergence(self._h, pu, _ptr(v)[0], _ptr(w)[0], dt, _ptr(rhs)[0], where))
+        return rhs
+
+    def project(self, p, col, rho_a, rho_b, dt, u, v, w):
+        """Momentum::project: u, v, w updated in place."""
+        pp, where = _ptr(p)
+        _check(lib().pbg_project(self._h, pp, _ptr(col)[0], rho_a, rho_b, dt, _ptr(u)[0],
+                                 _ptr(v)[0], _ptr(w)[0], where))
+        return u, v, w
+
+    def pressure_step(self, col, rho_a, rho_b, dt, u, v, w, p, params, solid=None):
+        """Assemble, divergence, solve and project in one call; u, v, w and
+        p updated in place. Returns the solver's Result."""
+        pp, where = _ptr(p)
+        res = Result()
+        _check(lib().pbg_pressure_step(self._h, _ptr(col)[0], rho_a, rho_b, _ptr(solid)[0], dt,
+                                       _ptr(u)[0], _ptr(v)[0], _ptr(w)[0], pp, where,
+                                       ctypes.byref(params), ctypes.byref(res)))
+        return res
+
     def symmetric(self):
         sym = ctypes.c_int(0)
         _check(lib().pbg_session_info(self._h, None, ctypes.byref(sym), None))
@@ -528,6 +570,25 @@ def generate(kind, seed, n=16, nb=0, rmin=4.0, rmax=16.0, rc=0.0, ratio=1000.0, 
     _check(lib().pbg_generate(kind, params, seed, dims, ctypes.byref(h), rho.ctypes.data_as(_dp),
                               solid.ctypes.data, b.ctypes.data))
     return tuple(dims), h.value, rho, solid, b
+
+
+def generate_flow(kind, seed, n=16, nb=0, rmin=4.0, rmax=16.0, rc=0.0, ratio=1000.0, index=0, n2d=0,
+                  s2=(64, 512), s3=(32, 96), stream=0):
+    """Flow state of one pressure-correction step (problem_gen.h
+    pbg_gen_flow): (col, u, v, w, rho_liquid, rho_vapour), face arrays
+    shaped (nx+1,ny,nz), (nx,ny+1,nz), (nx,ny,nz+1)."""
+    (nx, ny, nz), _, _, _, _ = generate(kind, seed, n, nb, rmin, rmax, rc, ratio, index, n2d, s2, s3,
+                                        stream)
+    params = (ctypes.c_double * 13)(n, nb, rmin, rmax, rc, ratio, index, n2d, s2[0], s2[1],
+                                    s3[0], s3[1], stream)
+    col = np.zeros((nx, ny, nz))
+    u = np.zeros((nx + 1, ny, nz))
+    v = np.zeros((nx, ny + 1, nz))
+    w = np.zeros((nx, ny, nz + 1))
+    rho = (ctypes.c_double * 2)()
+    _check(lib().pbg_generate_flow(kind, params, seed, col.ctypes.data, u.ctypes.data, v.ctypes.data,
+                                   w.ctypes.data, rho))
+    return col, u, v, w, rho[0], rho[1]
 
 
 KIND_SINGLE, KIND_CYL, KIND_BATCH = 0, 1, 2

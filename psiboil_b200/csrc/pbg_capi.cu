@@ -10,6 +10,7 @@
 #include "../../include/psiboil_b200.h"
 #include "pbg_assemble.cuh"
 #include "pbg_engine.cuh"
+#include "pbg_flow.cuh"
 #include "pbg_ref_kernels.cuh"
 #include "problem_gen.h"
 
@@ -371,6 +372,197 @@ int pbg_assemble_pressure(pbg_session *s, const double *rho, const uint8_t *soli
   });
 }
 
+int pbg_assemble_mix(pbg_session *s, const double *col, double rho_a, double rho_b, const uint8_t *solid,
+                     int where) {
+  if (!s) return fail(PBG_ERR_ARG, "session is NULL");
+  if (!(rho_a > 0.0) || (col && !(rho_b > 0.0))) return fail(PBG_ERR_ARG, "densities must be positive");
+  return guard(s, [&]() -> int {
+    const long long N = s->ncell();
+    DBuf<double> dcol;
+    DBuf<uint8_t> dsol;
+    const double *cp = col;
+    const uint8_t *sp = solid;
+    if (where == PBG_HOST) {
+      if (col) {
+        dcol.alloc(N);
+        PBG_CUDA(cudaMemcpyAsync(dcol.p, col, N * 8, cudaMemcpyHostToDevice, s->stream));
+        cp = dcol.p;
+      }
+      if (solid) {
+        dsol.alloc(N);
+        PBG_CUDA(cudaMemcpyAsync(dsol.p, solid, N, cudaMemcpyHostToDevice, s->stream));
+        sp = dsol.p;
+      }
+    }
+    Mat64 &A = s->A;
+    A.nx = s->nx; A.ny = s->ny; A.nz = s->nz; A.sym = true;
+    if (A.c.n != (size_t)N) { A.c.alloc(N); A.w.alloc(N); A.s.alloc(N); A.b.alloc(N); }
+    A.e.release(); A.n.release(); A.t.release();
+    k_assemble_mix<<<grid_for(N), kThreads, 0, s->stream>>>(
+        s->nx, s->ny, s->nz, s->h, make_int4(s->bc[0], s->bc[1], s->bc[2], s->bc[3]),
+        make_int2(s->bc[4], s->bc[5]), cp, rho_a, rho_b, sp, A.c.p, A.w.p, A.s.p, A.b.p, s->aflag.p);
+    note_launch();
+    PBG_CUDA(cudaGetLastError());
+    PBG_CUDA(cudaStreamSynchronize(s->stream));
+    s->have_matrix = true;
+    invalidate(s);
+    return PBG_OK;
+  });
+}
+
+}  // extern "C"
+
+namespace {
+
+// Face counts of the three velocity components.
+long long nfaces(const pbg_session *s, int m) {
+  return (long long)(s->nx + (m == 0)) * (s->ny + (m == 1)) * (s->nz + (m == 2));
+}
+
+// Device copies of host face arrays (where == PBG_HOST) or the caller's
+// device pointers. w may be NULL in 2-D.
+struct FaceArgs {
+  DBuf<double> buf[3];
+  double *d[3] = {nullptr, nullptr, nullptr};
+  void in(pbg_session *s, double *const f[3], int where, bool copy) {
+    for (int m = 0; m < 3; ++m) {
+      if (!f[m]) continue;
+      if (where == PBG_HOST) {
+        buf[m].alloc(nfaces(s, m));
+        if (copy)
+          PBG_CUDA(cudaMemcpyAsync(buf[m].p, f[m], nfaces(s, m) * 8, cudaMemcpyHostToDevice, s->stream));
+        d[m] = buf[m].p;
+      } else {
+        d[m] = f[m];
+      }
+    }
+  }
+  void out(pbg_session *s, double *const f[3], int where) {
+    if (where != PBG_HOST) return;
+    for (int m = 0; m < 3; ++m)
+      if (f[m]) PBG_CUDA(cudaMemcpyAsync(f[m], d[m], nfaces(s, m) * 8, cudaMemcpyDeviceToHost, s->stream));
+  }
+};
+
+int check_faces(const pbg_session *s, const double *u, const double *v, const double *w) {
+  if (!u || !v) return fail(PBG_ERR_ARG, "u and v are required");
+  if (!w && s->nz > 1) return fail(PBG_ERR_ARG, "w is required in 3-D");
+  return PBG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pbg_divergence(pbg_session *s, const double *u, const double *v, const double *w, double dt, double *rhs,
+                   int where) {
+  if (!s || !rhs) return fail(PBG_ERR_ARG, "NULL argument");
+  if (int rc = check_faces(s, u, v, w)) return rc;
+  if (!(dt > 0.0)) return fail(PBG_ERR_ARG, "dt must be positive");
+  return guard(s, [&]() -> int {
+    const long long N = s->ncell();
+    FaceArgs fa;
+    double *f[3] = {const_cast<double *>(u), const_cast<double *>(v), const_cast<double *>(w)};
+    fa.in(s, f, where, true);
+    DBuf<double> drhs;
+    double *r = rhs;
+    if (where == PBG_HOST) { drhs.alloc(N); r = drhs.p; }
+    const double dti = 1.0 / dt;
+    const double a = (s->h * s->h) * dti;
+    k_divergence<<<grid_for(N), kThreads, 0, s->stream>>>(s->nx, s->ny, s->nz, a, fa.d[0], fa.d[1], fa.d[2], r);
+    note_launch();
+    PBG_CUDA(cudaGetLastError());
+    if (where == PBG_HOST) PBG_CUDA(cudaMemcpyAsync(rhs, r, N * 8, cudaMemcpyDeviceToHost, s->stream));
+    PBG_CUDA(cudaStreamSynchronize(s->stream));
+    return PBG_OK;
+  });
+}
+
+int pbg_project(pbg_session *s, const double *p, const double *col, double rho_a, double rho_b, double dt,
+                double *u, double *v, double *w, int where) {
+  if (!s || !p) return fail(PBG_ERR_ARG, "NULL argument");
+  if (int rc = check_faces(s, u, v, w)) return rc;
+  if (!(dt > 0.0)) return fail(PBG_ERR_ARG, "dt must be positive");
+  if (!(rho_a > 0.0) || (col && !(rho_b > 0.0))) return fail(PBG_ERR_ARG, "densities must be positive");
+  return guard(s, [&]() -> int {
+    const long long N = s->ncell();
+    FaceArgs fa;
+    double *f[3] = {u, v, w};
+    fa.in(s, f, where, true);
+    DBuf<double> dp, dcol;
+    const double *pp = p, *cp = col;
+    if (where == PBG_HOST) {
+      dp.alloc(N);
+      PBG_CUDA(cudaMemcpyAsync(dp.p, p, N * 8, cudaMemcpyHostToDevice, s->stream));
+      pp = dp.p;
+      if (col) {
+        dcol.alloc(N);
+        PBG_CUDA(cudaMemcpyAsync(dcol.p, col, N * 8, cudaMemcpyHostToDevice, s->stream));
+        cp = dcol.p;
+      }
+    }
+    k_project<<<grid_for(N), kThreads, 0, s->stream>>>(s->nx, s->ny, s->nz, s->h, dt, pp, cp, rho_a, rho_b,
+                                                       fa.d[0], fa.d[1], fa.d[2]);
+    note_launch();
+    PBG_CUDA(cudaGetLastError());
+    fa.out(s, f, where);
+    PBG_CUDA(cudaStreamSynchronize(s->stream));
+    return PBG_OK;
+  });
+}
+
+int pbg_pressure_step(pbg_session *s, const double *col, double rho_a, double rho_b, const uint8_t *solid,
+                      double dt, double *u, double *v, double *w, double *p, int where, const pbg_params *prm,
+                      pbg_result *res) {
+  if (!s || !p || !prm) return fail(PBG_ERR_ARG, "NULL argument");
+  if (int rc = check_faces(s, u, v, w)) return rc;
+  if (!(dt > 0.0)) return fail(PBG_ERR_ARG, "dt must be positive");
+  return guard(s, [&]() -> int {
+    const long long N = s->ncell();
+    // inputs on the device once; every stage then runs on device pointers
+    FaceArgs fa;
+    double *f[3] = {u, v, w};
+    fa.in(s, f, where, true);
+    DBuf<double> dcol, dp, drhs;
+    DBuf<uint8_t> dsol;
+    const double *cp = col;
+    const uint8_t *sp = solid;
+    double *pp = p;
+    drhs.alloc(N);
+    if (where == PBG_HOST) {
+      if (col) {
+        dcol.alloc(N);
+        PBG_CUDA(cudaMemcpyAsync(dcol.p, col, N * 8, cudaMemcpyHostToDevice, s->stream));
+        cp = dcol.p;
+      }
+      if (solid) {
+        dsol.alloc(N);
+        PBG_CUDA(cudaMemcpyAsync(dsol.p, solid, N, cudaMemcpyHostToDevice, s->stream));
+        sp = dsol.p;
+      }
+      dp.alloc(N);
+      PBG_CUDA(cudaMemcpyAsync(dp.p, p, N * 8, cudaMemcpyHostToDevice, s->stream));
+      pp = dp.p;
+    }
+    int rc = pbg_assemble_mix(s, cp, rho_a, rho_b, sp, PBG_DEVICE);
+    if (rc != PBG_OK) return rc;
+    rc = pbg_divergence(s, fa.d[0], fa.d[1], fa.d[2], dt, drhs.p, PBG_DEVICE);
+    if (rc != PBG_OK) return rc;
+    // Centered::solve hands the solver scale * dti (centered_solve.cpp:31)
+    pbg_params q = *prm;
+    q.scale = prm->scale * (1.0 / dt);
+    pbg_result local;
+    rc = pbg_solve(s, pp, drhs.p, PBG_DEVICE, &q, res ? res : &local);
+    if (rc != PBG_OK) return rc;
+    rc = pbg_project(s, pp, cp, rho_a, rho_b, dt, fa.d[0], fa.d[1], fa.d[2], PBG_DEVICE);
+    if (rc != PBG_OK) return rc;
+    fa.out(s, f, where);
+    if (where == PBG_HOST) PBG_CUDA(cudaMemcpyAsync(p, pp, N * 8, cudaMemcpyDeviceToHost, s->stream));
+    PBG_CUDA(cudaStreamSynchronize(s->stream));
+    return PBG_OK;
+  });
+}
+
 }  // extern "C"
 
 namespace {
@@ -666,6 +858,24 @@ int pbg_generate(int kind, const double *params, uint64_t seed, int dims[3], dou
   if (!solid || !b) return fail(PBG_ERR_ARG, "rho, solid and b go together");
   pbg_gen_fields(&d, rho, solid);
   pbg_gen_rhs(&d, (uint64_t)params[12], solid, b);
+  return PBG_OK;
+}
+
+int pbg_generate_flow(int kind, const double *params, uint64_t seed, double *col, double *u, double *v,
+                      double *w, double rho[2]) {
+  if (!params || !col || !u || !v || !w || !rho) return fail(PBG_ERR_ARG, "NULL argument");
+  pbg_problem_desc d;
+  int n = (int)params[0];
+  if (kind == 0) pbg_desc_single_bubble(&d, n, seed);
+  else if (kind == 1)
+    pbg_desc_bubbles_cylinder(&d, n, (int)params[1], params[2], params[3], params[4], params[5], seed);
+  else if (kind == 2)
+    pbg_desc_batch_member(&d, seed, (int)params[6], (int)params[7], (int)params[8], (int)params[9],
+                          (int)params[10], (int)params[11]);
+  else return fail(PBG_ERR_ARG, "unknown kind");
+  rho[0] = d.rho_liquid;
+  rho[1] = d.rho_vapour;
+  pbg_gen_flow(&d, (uint64_t)params[12], col, u, v, w);
   return PBG_OK;
 }
 

@@ -242,6 +242,65 @@ static inline void pbg_gen_rhs(const pbg_problem_desc *d, uint64_t stream,
     b[c] = solid[c] ? 0.0 : (b[c] - mean) * s;
 }
 
+/* ------------------------------------------------------------------ */
+/* Flow state of a pressure-correction step                           */
+/* ------------------------------------------------------------------ */
+/* Face layouts (interior faces of the staggered Vector, boundary faces
+ * included): u (nx+1) x ny x nz, v nx x (ny+1) x nz, w nx x ny x (nz+1),
+ * each k fastest. Face f of u lies between cells f-1 and f. */
+static inline size_t pbg_nfaces(const pbg_problem_desc *d, int comp) {
+  return (size_t)(d->nx + (comp == 0)) * (size_t)(d->ny + (comp == 1)) *
+         (size_t)(d->nz + (comp == 2));
+}
+
+/* Liquid colour of a cell (1 liquid, 0 vapour): a linear ramp over three
+ * cells across each bubble's surface, the minimum over the bubbles. */
+static inline double pbg_color_at(const pbg_problem_desc *d, int i, int j, int k) {
+  double x = i + 0.5, y = j + 0.5, z = (d->nz > 1) ? k + 0.5 : 0.5;
+  double c = 1.0;
+  for (int q = 0; q < d->nbub; ++q) {
+    double ddx = x - d->bub[q][0], ddy = y - d->bub[q][1], ddz = z - d->bub[q][2];
+    if (d->nz == 1) ddz = 0.0;
+    double s = (sqrt(ddx * ddx + ddy * ddy + ddz * ddz) - d->bub[q][3]) / 3.0 + 0.5;
+    if (s < 0.0) s = 0.0;
+    if (s > 1.0) s = 1.0;
+    if (s < c) c = s;
+  }
+  return c;
+}
+
+/* Colour field and a predicted velocity u* for one step: face velocities
+ * U[-0.5, 0.5) drawn over u, then v, then w faces in index order; the
+ * normal faces on the domain boundary are walls (0), and w is 0 in 2-D.
+ * `stream` selects an independent draw. */
+static inline void pbg_gen_flow(const pbg_problem_desc *d, uint64_t stream, double *col,
+                                double *u, double *v, double *w) {
+  const int nx = d->nx, ny = d->ny, nz = d->nz;
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) col[((size_t)i * ny + j) * nz + k] = pbg_color_at(d, i, j, k);
+  pbg_mt64 g;
+  pbg_mt64_seed(&g, d->seed ^ (0xD1B54A32D192ED03ULL * (stream + 1ULL)));
+  for (int i = 0; i <= nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        double r = pbg_u01(&g) - 0.5;
+        u[((size_t)i * ny + j) * nz + k] = (i == 0 || i == nx) ? 0.0 : r;
+      }
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j <= ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        double r = pbg_u01(&g) - 0.5;
+        v[((size_t)i * (ny + 1) + j) * nz + k] = (j == 0 || j == ny) ? 0.0 : r;
+      }
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k <= nz; ++k) {
+        double r = nz > 1 ? pbg_u01(&g) - 0.5 : 0.0;
+        w[((size_t)i * ny + j) * (nz + 1) + k] = (k == 0 || k == nz) ? 0.0 : r;
+      }
+}
+
 /* Harmonic mean of two face-adjacent densities; symmetric bit-for-bit. */
 static inline double pbg_harm(double a, double b) {
   return (a * b) * 2.0 / (a + b);

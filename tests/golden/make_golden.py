@@ -6,7 +6,8 @@ seeded problems and stores its matrix, right-hand side, solutions,
 iteration/cycle counts and residual histories under tests/golden/*.npz.
 Only needed where the reference sources exist; the fixtures are committed.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            (everything)
+    python tests/golden/make_golden.py --steps    (the step fixtures only)
 """
 import os
 import sys
@@ -26,6 +27,36 @@ CASES = [
     ("odd15", O.KIND_BATCH, dict(index=40, n2d=0, s3=(15, 16)), ["cg", "ac"]),
     ("flat2d", O.KIND_BATCH, dict(index=1, n2d=8, s2=(24, 40)), ["cg", "bicgs", "ac"]),
 ]
+
+
+# pressure-correction steps (ref_harness --step 1): the reference's own
+# Pressure::discretize of a two-phase Matter, update_rhs, CG and
+# Momentum::project on the flow state of pbg_gen_flow
+STEP_CASES = [
+    # name, kind, problem kwargs, dt
+    ("step8", O.KIND_SINGLE, dict(n=8), 0.003),
+    ("step2d", O.KIND_BATCH, dict(index=0, n2d=1, s2=(32, 32)), 0.01),
+    ("step12", O.KIND_SINGLE, dict(n=12), 1.0),
+]
+
+
+def make_steps():
+    import flow
+    for name, kind, kw, dt in STEP_CASES:
+        P = O.Problem(kind, 7, **kw)
+        r = flow.run_reference_step(P, dt, res_rat=1e-10)
+        out = dict(dims=np.array(P.dims), h=np.array(P.h), kind=np.array(kind), seed=np.array(7),
+                   dt=np.array(dt), res_rat=np.array(1e-10),
+                   iterations=np.array(r["meta"]["iterations"]))
+        for k, v in kw.items():
+            out["arg_" + k] = np.array(v)
+        for k in "cwsb":
+            out["A_" + k] = r["A"][k]
+        out["rhs"] = r["b"]
+        for k in "xuvw":
+            out[k] = r[k]
+        print(name, P.dims, dt, r["meta"]["iterations"])
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 
 def main():
@@ -64,7 +95,12 @@ def main():
             out["A"] = True
         del out["A"]
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    make_steps()
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["--steps"]:
+        O.build()
+        make_steps()
+    else:
+        main()

@@ -1,0 +1,96 @@
+"""The pressure-correction step oracle (oracle/flow.py) against the
+reference: the committed fixtures made by the compiled reference's own
+Pressure::discretize / update_rhs / CG / Momentum::project
+(tests/golden/make_golden.py --steps), and live runs where the reference
+harness is built. CPU only."""
+import numpy as np
+import pytest
+
+import flow
+import oracle_py
+from golden_util import GOLDEN, problem_of
+
+import os
+
+STEP_NAMES = ["step8", "step2d", "step12"]
+
+
+def _load(name):
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+
+def _exact_grid(P):
+    """True where the reference's grid coordinates are exact multiples of h
+    (n a power of two in every real direction)."""
+    return all(n & (n - 1) == 0 for n in P.dims if n > 1)
+
+
+@pytest.mark.parametrize("name", STEP_NAMES)
+def test_step_oracle_matches_golden(oracle, name):
+    g = _load(name)
+    P = problem_of(g, oracle)
+    r = flow.step(P, float(g["dt"]), res_rat=float(g["res_rat"]))
+    assert r["stats"]["printed"] == int(g["iterations"])
+    pairs = [(r["A"][k], g["A_" + k]) for k in "cwsb"] + [(r["b"], g["rhs"])] + \
+        [(r[k].reshape(-1), g[k].reshape(-1)) for k in "xuvw"]
+    for got, ref in pairs:
+        if _exact_grid(P):
+            assert np.array_equal(got, ref)
+        else:
+            # the reference's grid spacings of a non-power-of-two n carry
+            # rounding from its node fit; the restatement uses h exactly
+            assert np.abs(got - ref).max() <= 1e-11 * max(np.abs(ref).max(), 1e-300)
+
+
+@pytest.mark.skipif(not oracle_py.harness_available(), reason="reference harness not built here")
+@pytest.mark.parametrize("kind,kw,dt", [(0, dict(n=16), 1.0), (0, dict(n=32), 0.002),
+                                        (2, dict(index=3, n2d=1, s2=(64, 64)), 0.05),
+                                        (2, dict(index=0, n2d=1, s2=(32, 32)), 1.0)])
+def test_step_oracle_matches_reference_live(oracle, kind, kw, dt):
+    P = oracle.Problem(kind, 13, **kw)
+    if not _exact_grid(P):
+        pytest.skip("grid %s is not a power of two" % (P.dims,))
+    ref = flow.run_reference_step(P, dt)
+    r = flow.step(P, dt)
+    assert r["stats"]["printed"] == int(ref["meta"]["iterations"])
+    for k in "cwesnbt":
+        assert np.array_equal(r["A"][k], ref["A"][k]), k
+    assert np.array_equal(r["A"]["ci"], ref["ci"])
+    for k in "bxuvw":
+        assert np.array_equal(np.reshape(r[k], -1), np.reshape(ref[k], -1)), k
+
+
+def test_projection_removes_divergence(oracle):
+    """Size-independent property: with Neumann sides everywhere the
+    projected field's divergence is the solver's residual, far below the
+    predicted field's."""
+    P = oracle.Problem(0, 5, n=16)
+    dt = 0.01
+    r = flow.step(P, dt, res_rat=1e-12, bc=[0] * 6)
+    d0 = flow.divergence(P.dims, P.h, dt, r["u0"], r["v0"], r["w0"])
+    d1 = flow.divergence(P.dims, P.h, dt, r["u"], r["v"], r["w"])
+    assert np.abs(d1).max() < 1e-9 * np.abs(d0).max()
+    # the projection only touches interior faces
+    assert np.all(r["u"][0] == 0.0) and np.all(r["u"][-1] == 0.0)
+    assert np.all(r["v"][:, 0] == 0.0) and np.all(r["w"][:, :, -1] == 0.0)
+
+
+def test_planted_density_error_is_caught(oracle):
+    """A harmonic face density in place of PropertyMix's arithmetic mean
+    (planted in the oracle) changes the matrix: the golden comparison
+    would fail."""
+    g = _load("step8")
+    P = problem_of(g, oracle)
+    col, u, v, w, ra, rb, bc = flow.flow_state(P)
+    good = flow.assemble_mix(P.dims, P.h, bc, col, ra, rb)
+    saved = flow.face_density
+    try:
+        def harmonic(cell, axis):
+            inv = saved(1.0 / cell, axis)
+            return 1.0 / inv
+        flow.face_density = harmonic
+        bad = flow.assemble_mix(P.dims, P.h, bc, col, ra, rb)
+    finally:
+        flow.face_density = saved
+    assert np.array_equal(good["c"], g["A_c"])
+    assert not np.array_equal(bad["c"], g["A_c"])
