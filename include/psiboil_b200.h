@@ -193,17 +193,21 @@ int pbg_assemble_pressure(pbg_session *s, const double *rho, const uint8_t *soli
  * assembly of Pressure(...)/discretize(). Sets the active flags. */
 int pbg_assemble_mix(pbg_session *s, const double *col, double rho_a, double rho_b,
                      const uint8_t *solid, int where);
-/* Pressure::update_rhs without an immersed body (pressure_update_rhs.cpp:
- * 16-139): rhs = dS/dt * (u_w - u_e + v_s - v_n + w_b - w_t) per cell. */
-int pbg_divergence(pbg_session *s, const double *u, const double *v, const double *w, double dt,
-                   double *rhs, int where);
-/* Momentum::project without an immersed body (momentum_project.cpp:11-80):
- * every interior face u += (p[i-1] - p[i]) / rho_face * dt / h (rho_face
- * as in pbg_assemble_mix). The normal faces on the domain boundary keep
- * the caller's values (the boundary condition; walls are 0), w is not
- * touched in 2-D. u, v, w updated in place. */
+/* Pressure::update_rhs (pressure_update_rhs.cpp:16-139): rhs = dS/dt *
+ * (u_w - u_e + v_s - v_n + w_b - w_t) per cell. solid (may be NULL): a
+ * voxel body, the immersed-body branch (:65-101): faces to solid
+ * neighbours are left out and solid cells get 0. */
+int pbg_divergence(pbg_session *s, const double *u, const double *v, const double *w,
+                   const uint8_t *solid, double dt, double *rhs, int where);
+/* Momentum::project (momentum_project.cpp:11-80): every interior face
+ * u += (p[i-1] - p[i]) / rho_face * dt / h (rho_face as in
+ * pbg_assemble_mix); with a solid mask the immersed-body branch (:47-73):
+ * only faces between two fluid cells, u += (p[i-1] - p[i]) * dt /
+ * rho_face / h. The normal faces on the domain boundary keep the caller's
+ * values (the boundary condition; walls are 0), w is not touched in 2-D.
+ * u, v, w updated in place. */
 int pbg_project(pbg_session *s, const double *p, const double *col, double rho_a, double rho_b,
-                double dt, double *u, double *v, double *w, int where);
+                const uint8_t *solid, double dt, double *u, double *v, double *w, int where);
 /* One pressure-correction step on the device: pbg_assemble_mix,
  * pbg_divergence, pbg_solve of p (p in: initial guess; solver scale
  * params->scale / dt as Centered::solve passes, centered_solve.cpp:25-31)

@@ -22,15 +22,17 @@ What it restates (reference file:line):
                      k sides of a 2-D grid: c -= a_bnd, a_bnd = 0, in the
                      order imin, imax, jmin, jmax, kmin, kmax) and :142-184
                      (Dirichlet: a_bnd = 0).
-  * divergence       Pressure::update_rhs without an immersed body,
-                     pressure_update_rhs.cpp:25-53,134-136 (fnew = 0,
-                     += a_w u_w, -= a_e u_e, += a_s v_s, -= a_n v_n,
-                     += a_b w_b, -= a_t w_t with a = dS * dti; then
-                     += fext + fbnd, both zero here).
-  * project          Momentum::project without an immersed body,
-                     Src/Equation/Staggered/Momentum/momentum_project.cpp:
-                     26-45: u += (p[i-1] - p[i]) / rho_face * dt / dxc on
-                     every interior face; the normal faces on the domain
+  * divergence       Pressure::update_rhs, pressure_update_rhs.cpp:25-53,
+                     134-136 (fnew = 0, += a_w u_w, -= a_e u_e, += a_s v_s,
+                     -= a_n v_n, += a_b w_b, -= a_t w_t with a = dS * dti;
+                     then += fext + fbnd, both zero here); a solid mask
+                     takes the immersed-body branch (:65-101) of a voxel
+                     body.
+  * project          Momentum::project, Src/Equation/Staggered/Momentum/
+                     momentum_project.cpp:26-45: u += (p[i-1] - p[i]) /
+                     rho_face * dt / dxc on every interior face (with a
+                     solid mask :47-73: faces between fluid cells only,
+                     (dp * dt) / rho / dxc); the normal faces on the domain
                      boundary keep their boundary value (the walls of
                      bnd_update_nooutlet, vector_bnd_update.cpp:54-85),
                      and w is not touched in 2-D (kfull false,
@@ -171,33 +173,52 @@ def assemble_mix(dims, h, bc, col, rho_a, rho_b, solid=None):
     return out
 
 
-def divergence(dims, h, dt, u, v, w):
+def divergence(dims, h, dt, u, v, w, solid=None):
     """Right-hand side of the pressure equation from face velocities
-    (flat, compact layout)."""
+    (flat, compact layout). solid: a voxel body, the immersed-body branch
+    of update_rhs (pressure_update_rhs.cpp:65-101; every fluid cell uncut,
+    so the face fractions are 1): a face counts only if the cell across it
+    is fluid (cells beyond the domain count as fluid), solid cells get 0."""
     nx, ny, nz = dims
     dti = 1.0 / dt
     a = (h * h) * dti
     u = np.asarray(u).reshape(nx + 1, ny, nz)
     v = np.asarray(v).reshape(nx, ny + 1, nz)
     w = np.asarray(w).reshape(nx, ny, nz + 1)
-    f = 0.0 + a * u[:-1]
-    f = f - a * u[1:]
-    f = f + a * v[:, :-1]
-    f = f - a * v[:, 1:]
-    f = f + a * w[:, :, :-1]
-    f = f - a * w[:, :, 1:]
+    terms = [(1, a * u[:-1]), (-1, a * u[1:]), (1, a * v[:, :-1]), (-1, a * v[:, 1:]),
+             (1, a * w[:, :, :-1]), (-1, a * w[:, :, 1:])]
+    if solid is None or not np.any(solid):
+        f = 0.0 + terms[0][1]
+        for sign, t in terms[1:]:
+            f = f + t if sign > 0 else f - t
+        f = f + (0.0 + 0.0)
+        return f.reshape(-1)
+    sol = np.asarray(solid).reshape(dims).astype(bool)
+    fluid = ~sol
+    pad = np.pad(fluid, 1, constant_values=True)
+    nb_open = [pad[:-2, 1:-1, 1:-1], pad[2:, 1:-1, 1:-1], pad[1:-1, :-2, 1:-1],
+               pad[1:-1, 2:, 1:-1], pad[1:-1, 1:-1, :-2], pad[1:-1, 1:-1, 2:]]
+    f = np.zeros(dims)
+    for (sign, t), op_ in zip(terms, nb_open):
+        g = f + t if sign > 0 else f - t
+        f = np.where(op_, g, f)
+    f = np.where(sol, 0.0, f)
     f = f + (0.0 + 0.0)
     return f.reshape(-1)
 
 
-def project(dims, h, dt, p, col, rho_a, rho_b, u, v, w):
-    """Projected face velocities (new arrays, the layouts of pbg_gen_flow)."""
+def project(dims, h, dt, p, col, rho_a, rho_b, u, v, w, solid=None):
+    """Projected face velocities (new arrays, the layouts of pbg_gen_flow).
+    solid: the immersed-body branch (momentum_project.cpp:47-73): only
+    faces between two fluid cells, in the order (dp * dt) / rho / dxc."""
     nx, ny, nz = dims
     p = np.asarray(p).reshape(dims)
     rc = _cell_density(col, rho_a, rho_b, dims)
     u = np.array(u, dtype=np.float64).reshape(nx + 1, ny, nz)
     v = np.array(v, dtype=np.float64).reshape(nx, ny + 1, nz)
     w = np.array(w, dtype=np.float64).reshape(nx, ny, nz + 1)
+    body = solid is not None and np.any(solid)
+    fluid = ~np.asarray(solid).reshape(dims).astype(bool) if body else None
 
     def rface(axis, shape):
         if rc is None:
@@ -205,13 +226,24 @@ def project(dims, h, dt, p, col, rho_a, rho_b, u, v, w):
         f = face_density(rc, axis)
         return np.take(f, np.arange(1, f.shape[axis] - 1), axis=axis)
 
+    def incr(dp, rho):
+        if body:
+            return dp * dt / rho / h
+        return dp / rho * dt / h
+
     ru = rface(0, (nx - 1, ny, nz))
-    u[1:-1] = u[1:-1] + (p[:-1] - p[1:]) / ru * dt / h
+    du = incr(p[:-1] - p[1:], ru)
+    v_u = u[1:-1] + du
+    u[1:-1] = np.where(fluid[:-1] & fluid[1:], v_u, u[1:-1]) if body else v_u
     rv = rface(1, (nx, ny - 1, nz))
-    v[:, 1:-1] = v[:, 1:-1] + (p[:, :-1] - p[:, 1:]) / rv * dt / h
+    dv = incr(p[:, :-1] - p[:, 1:], rv)
+    v_v = v[:, 1:-1] + dv
+    v[:, 1:-1] = np.where(fluid[:, :-1] & fluid[:, 1:], v_v, v[:, 1:-1]) if body else v_v
     if nz > 1:
         rw = rface(2, (nx, ny, nz - 1))
-        w[:, :, 1:-1] = w[:, :, 1:-1] + (p[:, :, :-1] - p[:, :, 1:]) / rw * dt / h
+        dw = incr(p[:, :, :-1] - p[:, :, 1:], rw)
+        v_w = w[:, :, 1:-1] + dw
+        w[:, :, 1:-1] = np.where(fluid[:, :, :-1] & fluid[:, :, 1:], v_w, w[:, :, 1:-1]) if body else v_w
     return u, v, w
 
 
@@ -245,12 +277,13 @@ def step(P, dt, res_rat=1e-10, maxit=20000, solver="cg", stream=0, bc=None):
     of A, b, x, u, v, w and the solver's statistics."""
     col, u, v, w, ra, rb, bc0 = flow_state(P, stream)
     bc = list(bc0 if bc is None else bc)
-    A = assemble_mix(P.dims, P.h, bc, col, ra, rb)
-    b = divergence(P.dims, P.h, dt, u, v, w)
+    sol = P.solid if np.any(P.solid) else None
+    A = assemble_mix(P.dims, P.h, bc, col, ra, rb, solid=sol)
+    b = divergence(P.dims, P.h, dt, u, v, w, solid=sol)
     sp = StepProblem(P.dims, P.h, A, b)
     x, st = op.cg(sp, b=b, res_rat=res_rat, res_tol=1e-18, maxit=maxit, scale=1.0 / dt,
                   solver=solver)
-    un, vn, wn = project(P.dims, P.h, dt, x, col, ra, rb, u, v, w)
+    un, vn, wn = project(P.dims, P.h, dt, x, col, ra, rb, u, v, w, solid=sol)
     return dict(A=A, b=b, x=x, u=un, v=vn, w=wn, stats=st, col=col, u0=u, v0=v, w0=w,
                 rho=(ra, rb), bc=bc)
 

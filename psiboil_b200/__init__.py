@@ -91,8 +91,8 @@ _SIGS = {
     "pbg_active_upload": (ctypes.c_int, [_vp, _vp, _ll, _ll, _ll, _ll, ctypes.c_int]),
     "pbg_assemble_pressure": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
     "pbg_assemble_mix": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_double, _vp, ctypes.c_int]),
-    "pbg_divergence": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, _vp, ctypes.c_int]),
-    "pbg_project": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+    "pbg_divergence": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_double, _vp, ctypes.c_int]),
+    "pbg_project": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp, ctypes.c_double,
                                    _vp, _vp, _vp, ctypes.c_int]),
     "pbg_pressure_step": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_double, _vp, ctypes.c_double,
                                          _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.POINTER(Params),
@@ -338,17 +338,19 @@ class Session:
             where = where2
         _check(lib().pbg_assemble_mix(self._h, pc, rho_a, rho_b, ps, where))
 
-    def divergence(self, u, v, w, dt, rhs):
-        """Pressure::update_rhs: rhs from the face velocities."""
+    def divergence(self, u, v, w, dt, rhs, solid=None):
+        """Pressure::update_rhs: rhs from the face velocities (solid: a
+        voxel body, the immersed-body branch)."""
         pu, where = _ptr(u)
-        _check(lib().pbg_divergence(self._h, pu, _ptr(v)[0], _ptr(w)[0], dt, _ptr(rhs)[0], where))
+        _check(lib().pbg_divergence(self._h, pu, _ptr(v)[0], _ptr(w)[0], _ptr(solid)[0], dt,
+                                    _ptr(rhs)[0], where))
         return rhs
 
-    def project(self, p, col, rho_a, rho_b, dt, u, v, w):
+    def project(self, p, col, rho_a, rho_b, dt, u, v, w, solid=None):
         """Momentum::project: u, v, w updated in place."""
         pp, where = _ptr(p)
-        _check(lib().pbg_project(self._h, pp, _ptr(col)[0], rho_a, rho_b, dt, _ptr(u)[0],
-                                 _ptr(v)[0], _ptr(w)[0], where))
+        _check(lib().pbg_project(self._h, pp, _ptr(col)[0], rho_a, rho_b, _ptr(solid)[0], dt,
+                                 _ptr(u)[0], _ptr(v)[0], _ptr(w)[0], where))
         return u, v, w
 
     def pressure_step(self, col, rho_a, rho_b, dt, u, v, w, p, params, solid=None):

@@ -40,6 +40,7 @@ struct pbg_session {
   std::unique_ptr<Engine> eng;
   bool eng_dirty = true, eng_mixed = false;
   DBuf<double> dx, db, dscal, hist, seq;
+  DBuf<double> frhs;               // pressure-step right-hand side (ncell)
   DBuf<unsigned long long> dlinf;
   double *hbuf = nullptr;          // pinned: 64 doubles
   double *px = nullptr, *pb = nullptr;  // pinned staging (ncell each)
@@ -454,8 +455,8 @@ int check_faces(const pbg_session *s, const double *u, const double *v, const do
 
 extern "C" {
 
-int pbg_divergence(pbg_session *s, const double *u, const double *v, const double *w, double dt, double *rhs,
-                   int where) {
+int pbg_divergence(pbg_session *s, const double *u, const double *v, const double *w, const uint8_t *solid,
+                   double dt, double *rhs, int where) {
   if (!s || !rhs) return fail(PBG_ERR_ARG, "NULL argument");
   if (int rc = check_faces(s, u, v, w)) return rc;
   if (!(dt > 0.0)) return fail(PBG_ERR_ARG, "dt must be positive");
@@ -465,11 +466,22 @@ int pbg_divergence(pbg_session *s, const double *u, const double *v, const doubl
     double *f[3] = {const_cast<double *>(u), const_cast<double *>(v), const_cast<double *>(w)};
     fa.in(s, f, where, true);
     DBuf<double> drhs;
+    DBuf<uint8_t> dsol;
     double *r = rhs;
-    if (where == PBG_HOST) { drhs.alloc(N); r = drhs.p; }
+    const uint8_t *sp = solid;
+    if (where == PBG_HOST) {
+      drhs.alloc(N);
+      r = drhs.p;
+      if (solid) {
+        dsol.alloc(N);
+        PBG_CUDA(cudaMemcpyAsync(dsol.p, solid, N, cudaMemcpyHostToDevice, s->stream));
+        sp = dsol.p;
+      }
+    }
     const double dti = 1.0 / dt;
     const double a = (s->h * s->h) * dti;
-    k_divergence<<<grid_for(N), kThreads, 0, s->stream>>>(s->nx, s->ny, s->nz, a, fa.d[0], fa.d[1], fa.d[2], r);
+    k_divergence<<<grid_for(N), kThreads, 0, s->stream>>>(s->nx, s->ny, s->nz, a, fa.d[0], fa.d[1], fa.d[2], sp,
+                                                          r);
     note_launch();
     PBG_CUDA(cudaGetLastError());
     if (where == PBG_HOST) PBG_CUDA(cudaMemcpyAsync(rhs, r, N * 8, cudaMemcpyDeviceToHost, s->stream));
@@ -478,8 +490,8 @@ int pbg_divergence(pbg_session *s, const double *u, const double *v, const doubl
   });
 }
 
-int pbg_project(pbg_session *s, const double *p, const double *col, double rho_a, double rho_b, double dt,
-                double *u, double *v, double *w, int where) {
+int pbg_project(pbg_session *s, const double *p, const double *col, double rho_a, double rho_b,
+                const uint8_t *solid, double dt, double *u, double *v, double *w, int where) {
   if (!s || !p) return fail(PBG_ERR_ARG, "NULL argument");
   if (int rc = check_faces(s, u, v, w)) return rc;
   if (!(dt > 0.0)) return fail(PBG_ERR_ARG, "dt must be positive");
@@ -490,7 +502,9 @@ int pbg_project(pbg_session *s, const double *p, const double *col, double rho_a
     double *f[3] = {u, v, w};
     fa.in(s, f, where, true);
     DBuf<double> dp, dcol;
+    DBuf<uint8_t> dsol;
     const double *pp = p, *cp = col;
+    const uint8_t *sp = solid;
     if (where == PBG_HOST) {
       dp.alloc(N);
       PBG_CUDA(cudaMemcpyAsync(dp.p, p, N * 8, cudaMemcpyHostToDevice, s->stream));
@@ -500,8 +514,13 @@ int pbg_project(pbg_session *s, const double *p, const double *col, double rho_a
         PBG_CUDA(cudaMemcpyAsync(dcol.p, col, N * 8, cudaMemcpyHostToDevice, s->stream));
         cp = dcol.p;
       }
+      if (solid) {
+        dsol.alloc(N);
+        PBG_CUDA(cudaMemcpyAsync(dsol.p, solid, N, cudaMemcpyHostToDevice, s->stream));
+        sp = dsol.p;
+      }
     }
-    k_project<<<grid_for(N), kThreads, 0, s->stream>>>(s->nx, s->ny, s->nz, s->h, dt, pp, cp, rho_a, rho_b,
+    k_project<<<grid_for(N), kThreads, 0, s->stream>>>(s->nx, s->ny, s->nz, s->h, dt, pp, cp, rho_a, rho_b, sp,
                                                        fa.d[0], fa.d[1], fa.d[2]);
     note_launch();
     PBG_CUDA(cudaGetLastError());
@@ -523,12 +542,12 @@ int pbg_pressure_step(pbg_session *s, const double *col, double rho_a, double rh
     FaceArgs fa;
     double *f[3] = {u, v, w};
     fa.in(s, f, where, true);
-    DBuf<double> dcol, dp, drhs;
+    DBuf<double> dcol, dp;
     DBuf<uint8_t> dsol;
     const double *cp = col;
     const uint8_t *sp = solid;
     double *pp = p;
-    drhs.alloc(N);
+    if (s->frhs.n != (size_t)N) s->frhs.alloc(N);
     if (where == PBG_HOST) {
       if (col) {
         dcol.alloc(N);
@@ -546,15 +565,15 @@ int pbg_pressure_step(pbg_session *s, const double *col, double rho_a, double rh
     }
     int rc = pbg_assemble_mix(s, cp, rho_a, rho_b, sp, PBG_DEVICE);
     if (rc != PBG_OK) return rc;
-    rc = pbg_divergence(s, fa.d[0], fa.d[1], fa.d[2], dt, drhs.p, PBG_DEVICE);
+    rc = pbg_divergence(s, fa.d[0], fa.d[1], fa.d[2], sp, dt, s->frhs.p, PBG_DEVICE);
     if (rc != PBG_OK) return rc;
     // Centered::solve hands the solver scale * dti (centered_solve.cpp:31)
     pbg_params q = *prm;
     q.scale = prm->scale * (1.0 / dt);
     pbg_result local;
-    rc = pbg_solve(s, pp, drhs.p, PBG_DEVICE, &q, res ? res : &local);
+    rc = pbg_solve(s, pp, s->frhs.p, PBG_DEVICE, &q, res ? res : &local);
     if (rc != PBG_OK) return rc;
-    rc = pbg_project(s, pp, cp, rho_a, rho_b, dt, fa.d[0], fa.d[1], fa.d[2], PBG_DEVICE);
+    rc = pbg_project(s, pp, cp, rho_a, rho_b, sp, dt, fa.d[0], fa.d[1], fa.d[2], PBG_DEVICE);
     if (rc != PBG_OK) return rc;
     fa.out(s, f, where);
     if (where == PBG_HOST) PBG_CUDA(cudaMemcpyAsync(p, pp, N * 8, cudaMemcpyDeviceToHost, s->stream));

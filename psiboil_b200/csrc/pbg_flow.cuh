@@ -127,63 +127,82 @@ __global__ void k_assemble_mix(int nx, int ny, int nz, double h, int4 bc03, int2
   }
 }
 
-// Pressure::update_rhs without an immersed body (pressure_update_rhs.cpp:
-// 25-53,134-136): fnew = 0; += a u_w; -= a u_e; += a v_s; -= a v_n;
-// += a w_b; -= a w_t with a = dS * dti (the caller passes a); then
-// += fext + fbnd, which are zero for homogeneous boundary values. w may be
-// nullptr in 2-D (its faces then count as zero).
+// Pressure::update_rhs (pressure_update_rhs.cpp:16-139): fnew = 0;
+// += a u_w; -= a u_e; += a v_s; -= a v_n; += a w_b; -= a w_t with
+// a = dS * dti (the caller passes a); then += fext + fbnd, which are zero
+// for homogeneous boundary values. With a solid mask (a voxel body: every
+// fluid cell uncut, face fractions 1) the immersed-body branch (:65-101): a
+// face counts only if the neighbour across it is fluid (cells beyond the
+// domain count as fluid), and solid cells get 0. w may be nullptr in 2-D
+// (its faces then count as zero).
 __global__ void k_divergence(int nx, int ny, int nz, double a, const double *__restrict__ u,
                              const double *__restrict__ v, const double *__restrict__ w,
-                             double *__restrict__ rhs) {
+                             const uint8_t *__restrict__ solid, double *__restrict__ rhs) {
   const long long N = (long long)nx * ny * nz;
-  const long long SIu = (long long)ny * nz;
+  const long long SI = (long long)ny * nz, SJ = nz;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
        p += (long long)gridDim.x * blockDim.x) {
     Pos q = pos_of(p, ny, nz);
     const long long iu = p;  // west face of the cell
     const long long iv = ((long long)q.i * (ny + 1) + q.j) * nz + q.k;
     const long long iw = ((long long)q.i * ny + q.j) * (nz + 1) + q.k;
-    double f = __dadd_rn(0.0, __dmul_rn(a, u[iu]));
-    f = __dsub_rn(f, __dmul_rn(a, u[iu + SIu]));
-    f = __dadd_rn(f, __dmul_rn(a, v[iv]));
-    f = __dsub_rn(f, __dmul_rn(a, v[iv + nz]));
-    f = __dadd_rn(f, __dmul_rn(a, w ? w[iw] : 0.0));
-    f = __dsub_rn(f, __dmul_rn(a, w ? w[iw + 1] : 0.0));
+    bool open[6] = {true, true, true, true, true, true};
+    if (solid) {
+      open[0] = q.i == 0 || !solid[p - SI];
+      open[1] = q.i == nx - 1 || !solid[p + SI];
+      open[2] = q.j == 0 || !solid[p - SJ];
+      open[3] = q.j == ny - 1 || !solid[p + SJ];
+      open[4] = q.k == 0 || !solid[p - 1];
+      open[5] = q.k == nz - 1 || !solid[p + 1];
+    }
+    double f = 0.0;
+    if (open[0]) f = __dadd_rn(f, __dmul_rn(a, u[iu]));
+    if (open[1]) f = __dsub_rn(f, __dmul_rn(a, u[iu + SI]));
+    if (open[2]) f = __dadd_rn(f, __dmul_rn(a, v[iv]));
+    if (open[3]) f = __dsub_rn(f, __dmul_rn(a, v[iv + nz]));
+    if (open[4]) f = __dadd_rn(f, __dmul_rn(a, w ? w[iw] : 0.0));
+    if (open[5]) f = __dsub_rn(f, __dmul_rn(a, w ? w[iw + 1] : 0.0));
+    if (solid && solid[p]) f = 0.0;
     rhs[p] = __dadd_rn(f, 0.0);
   }
 }
 
-// Momentum::project without an immersed body (Src/Equation/Staggered/
-// Momentum/momentum_project.cpp:26-45): on every interior face,
-// u += (p[i-1] - p[i]) / rho_face * dt / dxc with dxc = h. Thread p owns
-// the west, south and bottom faces of its cell; the faces on the domain
+// Momentum::project (Src/Equation/Staggered/Momentum/momentum_project.cpp:
+// 11-80) on every interior face: without a body (:26-45)
+// u += (p[i-1] - p[i]) / rho_face * dt / dxc; with a solid mask, the
+// immersed-body branch (:47-73): only faces between two fluid cells, as
+// u += (p[i-1] - p[i]) * dt / rho_face / dxc. dxc = h. Thread p owns the
+// west, south and bottom faces of its cell; the faces on the domain
 // boundary are not touched (they hold the walls' values, which
 // bnd_update_nooutlet restores in the reference), nor is w in 2-D.
+__device__ __forceinline__ double project_increment(double pm, double pp, double rho, double dt, double h,
+                                                    bool body) {
+  const double dp = __dsub_rn(pm, pp);
+  if (body) return __ddiv_rn(__ddiv_rn(__dmul_rn(dp, dt), rho), h);
+  return __ddiv_rn(__dmul_rn(__ddiv_rn(dp, rho), dt), h);
+}
+
 __global__ void k_project(int nx, int ny, int nz, double h, double dt, const double *__restrict__ pr,
-                          const double *__restrict__ col, double ra, double rb, double *__restrict__ u,
-                          double *__restrict__ v, double *__restrict__ w) {
+                          const double *__restrict__ col, double ra, double rb,
+                          const uint8_t *__restrict__ solid, double *__restrict__ u, double *__restrict__ v,
+                          double *__restrict__ w) {
   const long long N = (long long)nx * ny * nz;
   const long long SI = (long long)ny * nz, SJ = nz;
+  const bool body = solid != nullptr;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
        p += (long long)gridDim.x * blockDim.x) {
     Pos q = pos_of(p, ny, nz);
+    const bool sp = body && solid[p];
     const double pp = pr[p];
-    if (q.i > 0) {
-      double t = __ddiv_rn(__dsub_rn(pr[p - SI], pp), mix_face(col, ra, rb, p, p - SI));
-      t = __ddiv_rn(__dmul_rn(t, dt), h);
-      u[p] = __dadd_rn(u[p], t);
-    }
-    if (q.j > 0) {
+    if (q.i > 0 && !(body && (sp || solid[p - SI])))
+      u[p] = __dadd_rn(u[p], project_increment(pr[p - SI], pp, mix_face(col, ra, rb, p, p - SI), dt, h, body));
+    if (q.j > 0 && !(body && (sp || solid[p - SJ]))) {
       const long long iv = ((long long)q.i * (ny + 1) + q.j) * nz + q.k;
-      double t = __ddiv_rn(__dsub_rn(pr[p - SJ], pp), mix_face(col, ra, rb, p, p - SJ));
-      t = __ddiv_rn(__dmul_rn(t, dt), h);
-      v[iv] = __dadd_rn(v[iv], t);
+      v[iv] = __dadd_rn(v[iv], project_increment(pr[p - SJ], pp, mix_face(col, ra, rb, p, p - SJ), dt, h, body));
     }
-    if (nz > 1 && q.k > 0) {
+    if (nz > 1 && q.k > 0 && !(body && (sp || solid[p - 1]))) {
       const long long iw = ((long long)q.i * ny + q.j) * (nz + 1) + q.k;
-      double t = __ddiv_rn(__dsub_rn(pr[p - 1], pp), mix_face(col, ra, rb, p, p - 1));
-      t = __ddiv_rn(__dmul_rn(t, dt), h);
-      w[iw] = __dadd_rn(w[iw], t);
+      w[iw] = __dadd_rn(w[iw], project_increment(pr[p - 1], pp, mix_face(col, ra, rb, p, p - 1), dt, h, body));
     }
   }
 }

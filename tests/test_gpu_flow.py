@@ -60,17 +60,19 @@ def test_divergence_and_project_bit_exact(engine, oracle, kind, kw, dt):
     P, col, u, v, w, ra, rb, bc = _state(oracle, kind, kw)
     rng = np.random.default_rng(3)
     p = rng.standard_normal(P.N)
+    sols = [None] + ([P.solid] if np.any(P.solid) else [])
     with engine.Session(*P.dims, P.h, bc=bc) as s:
-        rhs = s.divergence(u, v, w, dt, np.zeros(P.N))
-        assert np.array_equal(rhs, flow.divergence(P.dims, P.h, dt, u, v, w))
-        if P.nz == 1:
-            rhs2 = s.divergence(u, v, None, dt, np.zeros(P.N))
-            assert np.array_equal(rhs2, rhs)
-        for c in (col, None):
-            uu, vv, ww = u.copy(), v.copy(), w.copy()
-            s.project(p, c, ra, rb, dt, uu, vv, ww)
-            ru, rv, rw = flow.project(P.dims, P.h, dt, p, c, ra, rb, u, v, w)
-            assert np.array_equal(uu, ru) and np.array_equal(vv, rv) and np.array_equal(ww, rw)
+        for sol in sols:
+            rhs = s.divergence(u, v, w, dt, np.zeros(P.N), solid=sol)
+            assert np.array_equal(rhs, flow.divergence(P.dims, P.h, dt, u, v, w, solid=sol))
+            if P.nz == 1:
+                rhs2 = s.divergence(u, v, None, dt, np.zeros(P.N), solid=sol)
+                assert np.array_equal(rhs2, rhs)
+            for c in (col, None):
+                uu, vv, ww = u.copy(), v.copy(), w.copy()
+                s.project(p, c, ra, rb, dt, uu, vv, ww, solid=sol)
+                ru, rv, rw = flow.project(P.dims, P.h, dt, p, c, ra, rb, u, v, w, solid=sol)
+                assert np.array_equal(uu, ru) and np.array_equal(vv, rv) and np.array_equal(ww, rw)
 
 
 def _cg_params(engine, res_rat):
@@ -126,12 +128,15 @@ def test_pressure_step_device_tensors(engine, oracle):
         assert np.array_equal(t.cpu().numpy(), a)
 
 
-@pytest.mark.parametrize("n,mixed", [(64, 0), (128, 1)])
-def test_engine_step_leaves_divergence_free_field(engine, oracle, n, mixed):
+@pytest.mark.parametrize("kind,kw,mixed", [(0, dict(n=64), 0), (0, dict(n=128), 1),
+                                           (1, dict(n=128, nb=8, rmin=4.0, rmax=10.0, rc=15.0), 1)])
+def test_engine_step_leaves_divergence_free_field(engine, oracle, kind, kw, mixed):
     """Size-independent property at sizes the oracle cannot run quickly:
     with Neumann sides everywhere the projected field's divergence is the
-    engine's residual: |div u| / |div u*| <= 10 * tol."""
-    P, col, u, v, w, ra, rb, _ = _state(oracle, 0, dict(n=n))
+    engine's residual, |div u| / |div u*| <= 10 * tol (a voxel solid
+    included: its faces are closed on both sides)."""
+    P, col, u, v, w, ra, rb, _ = _state(oracle, kind, kw)
+    sol = _solid(P)
     bc = [0] * 6
     dt = 0.01
     prm = engine.default_params(engine.SOLVER_ENGINE)
@@ -139,9 +144,9 @@ def test_engine_step_leaves_divergence_free_field(engine, oracle, n, mixed):
     prm.tol = 1e-9
     p = np.zeros(P.N)
     with engine.Session(*P.dims, P.h, bc=bc) as s:
-        d0 = s.divergence(u, v, w, dt, np.zeros(P.N))
-        res = s.pressure_step(col, ra, rb, dt, u, v, w, p, prm)
-        d1 = s.divergence(u, v, w, dt, np.zeros(P.N))
+        d0 = s.divergence(u, v, w, dt, np.zeros(P.N), solid=sol)
+        res = s.pressure_step(col, ra, rb, dt, u, v, w, p, prm, solid=sol)
+        d1 = s.divergence(u, v, w, dt, np.zeros(P.N), solid=sol)
     assert res.converged
     assert np.linalg.norm(d1) <= 10 * prm.tol * np.linalg.norm(d0)
     assert np.all(u[0] == 0.0) and np.all(u[-1] == 0.0) and np.all(w[:, :, 0] == 0.0)
