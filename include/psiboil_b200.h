@@ -72,7 +72,8 @@ enum {
   PBG_SOLVER_CG = 0,      /* CG with diagonal preconditioner (reference parity)   */
   PBG_SOLVER_BICGS = 1,   /* BiCGStab with diagonal preconditioner (parity)       */
   PBG_SOLVER_AC = 2,      /* additive-correction multigrid, CG smoother (parity)  */
-  PBG_SOLVER_ENGINE = 3   /* flexible CG + AC K-cycle (the engine's fast solver)  */
+  PBG_SOLVER_ENGINE = 3,  /* flexible CG + AC K-cycle (the engine's fast solver)  */
+  PBG_SOLVER_CGS = 4      /* conjugate gradient squared, CGS::solve (parity)       */
 };
 enum { PBG_FP64 = 0, PBG_MIXED = 1 };
 enum { PBG_CYCLE_NONE = -1, PBG_CYCLE_V = 1, PBG_CYCLE_F = 2, PBG_CYCLE_W = 4 };
@@ -107,10 +108,12 @@ typedef struct {
    * launches in repeated solves with one matrix and costs a longer set-up
    * after every matrix change (a dense inverse, O(cells^3)). */
   int coarse_max;
-  /* CG preconditioner, the reference's Prec codes (preconditioner.h:15-29):
-   * 0 diagonal (Prec::di, default), 1 IC0, 2 IC2, 3 IC3 (incomplete
-   * Cholesky, preconditioner_form.cpp:16-144 / preconditioner_solve.cpp:14-110;
-   * bit for bit with exact_sums). BiCGS takes the diagonal only. */
+  /* Krylov preconditioner (CG, BiCGS, CGS), the reference's Prec codes
+   * (preconditioner.h:15-29): 0 diagonal (Prec::di, default), 1 IC0, 2 IC2,
+   * 3 IC3 (incomplete Cholesky, preconditioner_form.cpp:16-144 /
+   * preconditioner_solve.cpp:14-110; bit for bit with exact_sums). The IC
+   * factor reads the lower couplings w, s, b, as the reference's does, also
+   * for a non-symmetric matrix. */
   int prec;
 } pbg_params;
 

@@ -117,11 +117,18 @@ class GpuCG : public GpuKrylov {
       : GpuKrylov(d, PBG_SOLVER_CG, pc, exact_sums) {}
 };
 
-// BiCGS(d, Prec::di()) on the GPU (Src/Solver/Linear/Krylov/bicgs.h)
+// BiCGS(d, pc) on the GPU (Src/Solver/Linear/Krylov/bicgs.h)
 class GpuBiCGS : public GpuKrylov {
  public:
   explicit GpuBiCGS(const Domain &d, const Prec &pc = Prec::di(), bool exact_sums = false)
       : GpuKrylov(d, PBG_SOLVER_BICGS, pc, exact_sums) {}
+};
+
+// CGS(d, pc) on the GPU (Src/Solver/Linear/Krylov/cgs.h)
+class GpuCGS : public GpuKrylov {
+ public:
+  explicit GpuCGS(const Domain &d, const Prec &pc = Prec::di(), bool exact_sums = false)
+      : GpuKrylov(d, PBG_SOLVER_CGS, pc, exact_sums) {}
 };
 
 }  // namespace pbg_psiboil

@@ -266,17 +266,55 @@ int orc_cg_prec(const orc_mat *A, double *x, const double *b, int mini, int maxi
   return converged;
 }
 
-/* bicgs.cpp:9-229 with Diagonal */
-int orc_bicgs(const orc_mat *A, double *x, const double *b, int mini, int maxit,
-              double res_rat, double res_tol, double scale, int stalecount,
-              double dV, orc_stats *st, double *hist) {
+/* The preconditioner of a Krylov solve: Prec::di (prec 0, Mc = 1/c, z = r
+ * Mc) or Prec::ic0/ic2/ic3 (1, 2, 3), formed once per solve as
+ * Krylov::solve does with precform (bicgs.cpp:37-39, cgs.cpp:38-39). */
+typedef struct {
+  int prec;
+  double *Mc;
+  orc_ic M;
+} orc_prec;
+
+static void prec_form(const orc_mat *A, int prec, orc_prec *P) {
+  const size_t N = (size_t)A->nx * A->ny * A->nz;
+  P->prec = prec;
+  P->Mc = calloc(N, sizeof(double));
+  for (size_t c = 0; c < N; ++c) P->Mc[c] = 1.0 / A->c[c];
+  orc_ic M = {prec, NULL, NULL, NULL, NULL, NULL, NULL, NULL};
+  if (prec > 0) {
+    M.c = calloc(N, sizeof(double)); M.w = calloc(N, sizeof(double));
+    M.s = calloc(N, sizeof(double)); M.b = calloc(N, sizeof(double));
+    if (prec >= 2) { M.tw = calloc(N, sizeof(double)); M.ts = calloc(N, sizeof(double)); }
+    if (prec == 3) M.nw = calloc(N, sizeof(double));
+    ic_form(A, &M);
+  }
+  P->M = M;
+}
+
+/* M z = r (Diagonal::solve, preconditioner_solve.cpp:4-11, or the IC sweeps) */
+static void prec_solve(const orc_mat *A, const orc_prec *P, double *z, const double *r) {
+  const size_t N = (size_t)A->nx * A->ny * A->nz;
+  if (P->prec > 0) ic_solve(A, &P->M, z, r);
+  else
+    for (size_t c = 0; c < N; ++c) z[c] = r[c] * P->Mc[c];
+}
+
+static void prec_free(orc_prec *P) {
+  free(P->Mc);
+  free(P->M.c); free(P->M.w); free(P->M.s); free(P->M.b); free(P->M.tw); free(P->M.ts); free(P->M.nw);
+}
+
+/* bicgs.cpp:9-229 with Prec::di (prec 0) or Prec::ic0/ic2/ic3 */
+int orc_bicgs_prec(const orc_mat *A, double *x, const double *b, int mini, int maxit,
+                   double res_rat, double res_tol, double scale, int stalecount,
+                   double dV, orc_stats *st, double *hist, int prec) {
   const size_t N = (size_t)A->nx * A->ny * A->nz;
   double *p = calloc(N, sizeof(double)), *r = calloc(N, sizeof(double));
   double *s = calloc(N, sizeof(double)), *t = calloc(N, sizeof(double));
   double *v = calloc(N, sizeof(double)), *p_ = calloc(N, sizeof(double));
   double *r_ = calloc(N, sizeof(double)), *s_ = calloc(N, sizeof(double));
-  double *Mc = calloc(N, sizeof(double));
-  for (size_t c = 0; c < N; ++c) Mc[c] = 1.0 / A->c[c];
+  orc_prec P;
+  prec_form(A, prec, &P);
   orc_resid(A, x, b, r);
   double res = sqrt(orc_dot_voldiv_avg(N, r, r, dV)) / scale;
   double res0 = res;
@@ -302,7 +340,7 @@ int orc_bicgs(const orc_mat *A, double *x, const double *b, int mini, int maxit,
       double bo = beta * omega;
       for (size_t c = 0; c < N; ++c) p[c] -= bo * v[c];
     }
-    for (size_t c = 0; c < N; ++c) p_[c] = p[c] * Mc[c];
+    prec_solve(A, &P, p_, p);
     orc_spmv(A, p_, v);
     r_v = orc_dot(N, r_, v);
     alfa = rho / r_v;
@@ -313,7 +351,7 @@ int orc_bicgs(const orc_mat *A, double *x, const double *b, int mini, int maxit,
       broke = 1; so.status = 3;
       break;
     }
-    for (size_t c = 0; c < N; ++c) s_[c] = s[c] * Mc[c];
+    prec_solve(A, &P, s_, s);
     orc_spmv(A, s_, t);
     ts = orc_dot(N, t, s);
     tt = orc_dot(N, t, t);
@@ -335,7 +373,82 @@ int orc_bicgs(const orc_mat *A, double *x, const double *b, int mini, int maxit,
   so.res = res;
 done_early:
   if (st) *st = so;
-  free(p); free(r); free(s); free(t); free(v); free(p_); free(r_); free(s_); free(Mc);
+  free(p); free(r); free(s); free(t); free(v); free(p_); free(r_); free(s_);
+  prec_free(&P);
+  free(win.v);
+  return converged || so.status == 4;
+}
+
+int orc_bicgs(const orc_mat *A, double *x, const double *b, int mini, int maxit,
+              double res_rat, double res_tol, double scale, int stalecount,
+              double dV, orc_stats *st, double *hist) {
+  return orc_bicgs_prec(A, x, b, mini, maxit, res_rat, res_tol, scale, stalecount, dV, st, hist, 0);
+}
+
+/* cgs.cpp:8-210 (conjugate gradient squared) with Prec::di or Prec::ic* */
+int orc_cgs_prec(const orc_mat *A, double *x, const double *b, int mini, int maxit,
+                 double res_rat, double res_tol, double scale, int stalecount,
+                 double dV, orc_stats *st, double *hist, int prec) {
+  const size_t N = (size_t)A->nx * A->ny * A->nz;
+  double *p = calloc(N, sizeof(double)), *q = calloc(N, sizeof(double));
+  double *r = calloc(N, sizeof(double)), *s = calloc(N, sizeof(double));
+  double *u = calloc(N, sizeof(double)), *p_ = calloc(N, sizeof(double));
+  double *q_ = calloc(N, sizeof(double)), *r_ = calloc(N, sizeof(double));
+  double *u_ = calloc(N, sizeof(double)), *v_ = calloc(N, sizeof(double));
+  orc_prec P;
+  prec_form(A, prec, &P);
+  orc_resid(A, x, b, r);
+  double res = sqrt(orc_dot_voldiv_avg(N, r, r, dV)) / scale;
+  double res0 = res;
+  stale_win win;
+  stale_init(&win, stalecount, res);
+  orc_stats so = {0, 0, 0, res0, res, 0};
+  int converged = 0, i, broke = 0;
+  if (res < res_tol) { /* cgs.cpp:69: returns true */
+    so.converged = 1; so.status = 4;
+    goto done_early;
+  }
+  memcpy(r_, r, N * sizeof(double));
+  double alfa, beta, rho = 0, rho_old = 0, r_v_;
+  so.status = 1;
+  for (i = 0; i < maxit; ++i) {
+    rho = orc_dot(N, r_, r);
+    if (sqrt(fabs(rho)) < res_tol) { broke = 1; so.status = 3; break; }
+    if (i == 0) {
+      memcpy(u, r, N * sizeof(double));
+      memcpy(p, u, N * sizeof(double));
+    } else {
+      beta = rho / rho_old;
+      const double bb = beta * beta;
+      for (size_t c = 0; c < N; ++c) u[c] = r[c] + beta * q[c];
+      for (size_t c = 0; c < N; ++c) p[c] = u[c] + bb * p[c];
+      for (size_t c = 0; c < N; ++c) p[c] += beta * q[c];
+    }
+    prec_solve(A, &P, p_, p);
+    orc_spmv(A, p_, v_);
+    r_v_ = orc_dot(N, r_, v_);
+    alfa = rho / r_v_;
+    for (size_t c = 0; c < N; ++c) q[c] = u[c] - alfa * v_[c];
+    for (size_t c = 0; c < N; ++c) s[c] = u[c] + q[c];
+    prec_solve(A, &P, u_, s);
+    for (size_t c = 0; c < N; ++c) x[c] += alfa * u_[c];
+    orc_spmv(A, u_, q_);
+    for (size_t c = 0; c < N; ++c) r[c] -= alfa * q_[c];
+    res = sqrt(orc_dot_voldiv_avg(N, r, r, dV)) / scale;
+    if (hist) hist[i] = res;
+    if (res < res_tol && i >= mini - 1) { converged = 1; broke = 1; so.status = 0; break; }
+    if (res < res0 * res_rat && i >= mini - 1) { converged = 1; broke = 1; so.status = 0; break; }
+    if (stale_step(&win, res)) { broke = 1; so.status = 2; break; }
+    rho_old = rho;
+  }
+  so.converged = converged;
+  so.iterations = broke ? i + 1 : maxit;
+  so.printed = i + 1;
+  so.res = res;
+done_early:
+  if (st) *st = so;
+  free(p); free(q); free(r); free(s); free(u); free(p_); free(q_); free(r_); free(u_); free(v_);
+  prec_free(&P);
   free(win.v);
   return converged || so.status == 4;
 }

@@ -65,6 +65,14 @@ int orc_cg_prec(const orc_mat *A, double *x, const double *b, int mini, int maxi
 int orc_bicgs(const orc_mat *A, double *x, const double *b, int mini, int maxit,
               double res_rat, double res_tol, double scale, int stalecount,
               double dV, orc_stats *st, double *hist);
+/* the same with a preconditioner (prec as for orc_cg_prec) */
+int orc_bicgs_prec(const orc_mat *A, double *x, const double *b, int mini, int maxit,
+                   double res_rat, double res_tol, double scale, int stalecount,
+                   double dV, orc_stats *st, double *hist, int prec);
+/* Conjugate gradient squared, CGS::solve (cgs.cpp:8-210). */
+int orc_cgs_prec(const orc_mat *A, double *x, const double *b, int mini, int maxit,
+                 double res_rat, double res_tol, double scale, int stalecount,
+                 double dV, orc_stats *st, double *hist, int prec);
 
 /* Additive-correction multigrid (Src/Solver/Additive) around CG smoothers. */
 typedef struct orc_ac orc_ac;

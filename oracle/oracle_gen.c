@@ -56,3 +56,10 @@ int orc_gen_flow(int kind, const double *params, uint64_t seed, double *col, dou
   pbg_gen_flow(&d, (uint64_t)params[12], col, u, v, w);
   return 0;
 }
+
+/* Non-symmetric variant of a fixture matrix (pbg_gen_convect), in place. */
+int orc_convect(int nx, int ny, int nz, double F, const uint8_t *solid, double *c, double *w,
+                double *ci) {
+  pbg_gen_convect(nx, ny, nz, F, solid, c, w, ci);
+  return 0;
+}

@@ -57,12 +57,13 @@ def lib():
         L.orc_dot.argtypes = [ctypes.c_size_t, _dp, _dp]
         L.orc_dot_voldiv_avg.restype = ctypes.c_double
         L.orc_dot_voldiv_avg.argtypes = [ctypes.c_size_t, _dp, _dp, ctypes.c_double]
-        for fn in (L.orc_cg, L.orc_bicgs, L.orc_cg_prec):
+        for fn in (L.orc_cg, L.orc_bicgs, L.orc_cg_prec, L.orc_bicgs_prec, L.orc_cgs_prec):
             fn.restype = ctypes.c_int
             fn.argtypes = [ctypes.POINTER(OrcMat), _dp, _dp, ctypes.c_int, ctypes.c_int,
                            ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                            ctypes.c_double, ctypes.POINTER(OrcStats), _dp]
-        L.orc_cg_prec.argtypes = L.orc_cg_prec.argtypes + [ctypes.c_int]
+        for fn in (L.orc_cg_prec, L.orc_bicgs_prec, L.orc_cgs_prec):
+            fn.argtypes = fn.argtypes + [ctypes.c_int]
         L.orc_ac_create.restype = ctypes.c_void_p
         L.orc_ac_create.argtypes = [ctypes.POINTER(OrcMat), ctypes.c_void_p, ctypes.c_double]
         L.orc_ac_destroy.argtypes = [ctypes.c_void_p]
@@ -97,7 +98,7 @@ class Problem:
     """A seeded fixture problem: dims, density, solid mask, rhs, matrix."""
 
     def __init__(self, kind, seed, n=16, nb=0, rmin=4.0, rmax=16.0, rc=0.0, ratio=1000.0,
-                 index=0, n2d=0, s2=(64, 512), s3=(32, 96), stream=0):
+                 index=0, n2d=0, s2=(64, 512), s3=(32, 96), stream=0, convect=0.0):
         self.kind, self.seed = kind, seed
         params = np.array([n, nb, rmin, rmax, rc, ratio, index, n2d, s2[0], s2[1], s3[0], s3[1],
                            stream], dtype=np.float64)
@@ -122,6 +123,12 @@ class Problem:
         self.ci = out[9 * N:10 * N].copy()
         self.solid = solid
         self.bc = None
+        self.convect = float(convect)
+        if self.convect != 0.0:
+            # upwind convection along +x: a non-symmetric matrix (pbg_gen_convect)
+            L.orc_convect.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double, ctypes.c_void_p, _dp, _dp, _dp]
+            L.orc_convect(self.nx, self.ny, self.nz, self.convect, solid.ctypes.data, _p(self.A["c"]),
+                          _p(self.A["w"]), _p(self.ci))
 
     @property
     def dims(self):
@@ -173,12 +180,8 @@ def cg(P, b=None, x0=None, mini=1, maxit=20000, res_rat=1e-8, res_tol=1e-18, sca
     m = P.mat()
     args = (ctypes.byref(m), _p(x), _p(b), mini, maxit, res_rat, res_tol, scale, stalecount, P.dV,
             ctypes.byref(st), _p(h) if hist else None)
-    if solver == "cg":
-        lib().orc_cg_prec(*args, PRECS[prec])
-    else:
-        if prec != "di":
-            raise ValueError("BiCGS takes the diagonal preconditioner")
-        lib().orc_bicgs(*args)
+    fn = {"cg": lib().orc_cg_prec, "bicgs": lib().orc_bicgs_prec, "cgs": lib().orc_cgs_prec}[solver]
+    fn(*args, PRECS[prec])
     out = dict(converged=st.converged, iterations=st.iterations, printed=st.printed,
                res0=st.res0, res=st.res, status=st.status)
     if hist:
@@ -257,7 +260,8 @@ def run_reference(P, solver="cg", resrat=1e-8, maxit=20000, maxcyc=20, guard=1, 
            "--s2", str(a["s2"][0]), str(a["s2"][1]), "--s3", str(a["s3"][0]), str(a["s3"][1]),
            "--seed", str(P.seed), "--solver", solver, "--resrat", repr(resrat),
            "--maxit", str(maxit), "--maxcyc", str(maxcyc), "--guard", str(guard),
-           "--cycle", cycle, "--prec", prec, "--dump", "1" if dump else "0", "--out", out_prefix]
+           "--cycle", cycle, "--prec", prec, "--dump", "1" if dump else "0", "--out", out_prefix,
+           "--convect", repr(getattr(P, "convect", 0.0))]
     subprocess.run(cmd, check=True, capture_output=True, timeout=timeout)
     meta = {}
     for line in open(out_prefix + ".txt"):

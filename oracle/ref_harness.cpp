@@ -30,7 +30,11 @@
  *               --rc R --ratio Q] [--index I --n2d M --s2 LO HI --s3 LO HI]
  *               --seed S --solver cg|bicgs|ac --resrat RR --maxit M
  *               [--maxcyc C --guard 0|1 --cycle V|F|W] [--prec di|ic0|ic2|ic3] [--save NAME]
- *               [--step 1 --dt DT] --out PREFIX
+ *               [--step 1 --dt DT] [--convect F] --out PREFIX
+ *
+ * --solver cgs runs `CGS::solve` (cgs.cpp); --convect F adds the upwind
+ * convection of pbg_gen_convect to the fixture after the boundary
+ * correction (a non-symmetric matrix, for BiCGS and CGS).
  *
  * --step 1 runs one pressure-correction step with the reference's own
  * classes and no override: a two-phase Matter (liquid and vapour densities
@@ -67,7 +71,7 @@ struct Args {
   double resrat = 1e-8;
   int maxit = 20000, maxcyc = 20, guard = 1, dump = 1, repeat = 1, gpu = 0, exact = 1;
   int step = 0;
-  double dt = 1.0;
+  double dt = 1.0, convect = 0.0;
 };
 
 Args parse(int argc, char **argv) {
@@ -105,6 +109,7 @@ Args parse(int argc, char **argv) {
     else if (k == "--prec") a.prec = nxt();
     else if (k == "--step") a.step = std::atoi(nxt());
     else if (k == "--dt") a.dt = std::atof(nxt());
+    else if (k == "--convect") a.convect = std::atof(nxt());
     else { std::fprintf(stderr, "unknown argument %s\n", k.c_str()); std::exit(2); }
   }
   return a;
@@ -116,8 +121,8 @@ class Fixture : public Pressure {
   Fixture(const Scalar &p, const Scalar &f, const Vector &u, Times &t,
           Linear *sm, Matter *m, const pbg_problem_desc &d,
           const std::vector<double> &rho, const std::vector<uint8_t> &solid,
-          const std::vector<double> &rhs)
-      : Pressure(p, f, u, t, sm, m), D(d), RHO(rho), SOLID(solid), RHS(rhs) {
+          const std::vector<double> &rhs, double convect)
+      : Pressure(p, f, u, t, sm, m), D(d), RHO(rho), SOLID(solid), RHS(rhs), CONV(convect) {
     ready = true;
     discretize();
     for (int i = 0; i < D.nx; ++i)
@@ -146,6 +151,15 @@ class Fixture : public Pressure {
         }
     /* the reference's own boundary correction */
     Centered::create_system_bnd();
+    /* non-symmetric variant: upwind convection along +x (pbg_gen_convect) */
+    if (CONV != 0.0)
+      for (int i = 1; i < D.nx; ++i)
+        for (int j = 0; j < D.ny; ++j)
+          for (int k = 0; k < D.nz; ++k) {
+            if (SOLID[at(i, j, k)] || SOLID[at(i - 1, j, k)]) continue;
+            A.w[i + B][j + B][k + B] += CONV;
+            A.c[i + B][j + B][k + B] += CONV;
+          }
     for (int i = 0; i < D.nx; ++i)
       for (int j = 0; j < D.ny; ++j)
         for (int k = 0; k < D.nz; ++k) {
@@ -190,6 +204,7 @@ class Fixture : public Pressure {
   std::vector<double> RHO;
   std::vector<uint8_t> SOLID;
   std::vector<double> RHS;
+  double CONV = 0.0;
   bool ready = false;
 };
 
@@ -379,10 +394,12 @@ int main(int argc, char **argv) {
 #ifdef PBG_WITH_ENGINE
   /* the drop-in: the engine's Krylov classes behind the reference's virtual */
   if (a.gpu && a.solver == "bicgs") solver = new pbg_psiboil::GpuBiCGS(d, pc, a.exact != 0);
+  else if (a.gpu && a.solver == "cgs") solver = new pbg_psiboil::GpuCGS(d, pc, a.exact != 0);
   else if (a.gpu) solver = new pbg_psiboil::GpuCG(d, pc, a.exact != 0);
   else
 #endif
   if (a.solver == "bicgs") solver = new BiCGS(d, pc);
+  else if (a.solver == "cgs") solver = new CGS(d, pc);
   else solver = new CG(d, pc);
 
   Vector uvw(d);
@@ -402,7 +419,7 @@ int main(int argc, char **argv) {
   Matter fluid(d);
   fluid.rho(1.0);
 
-  Fixture pr(p, f, uvw, time, solver, &fluid, D, rho, solid, rhs);
+  Fixture pr(p, f, uvw, time, solver, &fluid, D, rho, solid, rhs, a.convect);
 
   p = 0.0;
   bool conv = false;

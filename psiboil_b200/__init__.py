@@ -26,7 +26,7 @@ LIB_PATH = os.path.join(_HERE, "libpsiboil_b200.so")
 PBG_OK = 0
 HOST, DEVICE = 0, 1
 NEUMANN, DIRICHLET = 0, 1
-SOLVER_CG, SOLVER_BICGS, SOLVER_AC, SOLVER_ENGINE = 0, 1, 2, 3
+SOLVER_CG, SOLVER_BICGS, SOLVER_AC, SOLVER_ENGINE, SOLVER_CGS = 0, 1, 2, 3, 4
 FP64, MIXED = 0, 1
 CYCLE_NONE, CYCLE_V, CYCLE_F, CYCLE_W = -1, 1, 2, 4
 STATUS = {0: "converged", 1: "maxiter", 2: "stale", 3: "breakdown", 4: "initial", 5: "nan",
@@ -470,8 +470,13 @@ class CG(_Krylov):
 
 
 class BiCGS(_Krylov):
-    """BiCGStab with the diagonal preconditioner (Krylov/bicgs.cpp)."""
+    """BiCGStab (Krylov/bicgs.cpp), diagonal or IC preconditioner."""
     solver = SOLVER_BICGS
+
+
+class CGS(_Krylov):
+    """Conjugate gradient squared (Krylov/cgs.cpp), diagonal or IC preconditioner."""
+    solver = SOLVER_CGS
 
 
 class AC:

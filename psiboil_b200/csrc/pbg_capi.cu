@@ -628,7 +628,7 @@ int solve_device(pbg_session *s, double *xd, const double *bd, const pbg_params 
   std::memset(&out, 0, sizeof(out));
   const double dV = s->dV;
   s->nhist = 0;
-  if (p->solver == PBG_SOLVER_CG || p->solver == PBG_SOLVER_BICGS) {
+  if (p->solver == PBG_SOLVER_CG || p->solver == PBG_SOLVER_BICGS || p->solver == PBG_SOLVER_CGS) {
     KrylovParams pr;
     pr.mini = p->min_iter; pr.maxit = p->max_iter;
     pr.stalecount = p->stalecount > kStaleMax ? kStaleMax : p->stalecount;
@@ -636,10 +636,9 @@ int solve_device(pbg_session *s, double *xd, const double *bd, const pbg_params 
     pr.res_rat = p->res_rat; pr.res_tol = p->res_tol; pr.scale = p->scale; pr.dV = dV;
     pr.seq = exact_terms(s, p);
     if (p->prec < 0 || p->prec > 3) return fail(PBG_ERR_ARG, "prec must be 0 (diagonal), 1 (IC0), 2 (IC2) or 3 (IC3)");
-    if (p->prec > 0 && p->solver != PBG_SOLVER_CG)
-      return fail(PBG_ERR_UNSUPPORTED, "incomplete Cholesky is provided for CG only");
     pr.prec = p->prec;
-    RefKrylovResult rr = ref_krylov_solve(s->A.view(), xd, bd, pr, p->solver == PBG_SOLVER_BICGS ? 1 : 0,
+    const int kind = p->solver == PBG_SOLVER_CG ? 0 : p->solver == PBG_SOLVER_BICGS ? 1 : 2;
+    RefKrylovResult rr = ref_krylov_solve(s->A.view(), xd, bd, pr, kind,
                                           s->rkw, s->red, s->kst.p, s->hkst, s->hist.p, s->stream);
     out.status = rr.status;
     out.converged = rr.converged;

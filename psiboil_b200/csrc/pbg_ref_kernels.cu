@@ -364,8 +364,7 @@ __global__ void k_cg_rho(long long N, const double *__restrict__ r, const double
 
 
 // ---------------------------------------------------------------------------
-// BiCGStab with the diagonal preconditioner, BiCGS::solve (bicgs.cpp:9-229).
-// One iteration:
+// BiCGStab, BiCGS::solve (bicgs.cpp:9-229). One iteration:
 //   k_bi_rho   rho = r~.r; breakdown test; beta                     (:91-99)
 //   k_bi_p     p = r (i=0) | p = r + beta p; p -= (beta omega) v; p^ = p Mc
 //   k_bi_v     v = A p^; r~.v; alfa                                 (:124-133)
@@ -373,7 +372,8 @@ __global__ void k_cg_rho(long long N, const double *__restrict__ r, const double
 //   k_bi_t     t = A s^; t.s, t.t; omega                           (:163-175)
 //   k_bi_xr    x += alfa p^; x += omega s^; r = s - omega t; res; tests
 // The early exit of :146-150 (x += alfa p^, break) is carried by
-// pending_x, which k_bi_xr applies and clears.
+// pending_x, which k_bi_xr applies and clears. With an incomplete Cholesky
+// preconditioner (diag == 0) the IC sweeps form p^ and s^ instead.
 // ---------------------------------------------------------------------------
 __global__ void k_bi_init(MatView<double> A, const double *__restrict__ x, const double *__restrict__ b,
                           double *__restrict__ r, double *__restrict__ rt, KrylovState *st,
@@ -430,7 +430,7 @@ __global__ void k_bi_rho(long long N, const double *__restrict__ rt, const doubl
 
 __global__ void k_bi_p(long long N, const double *__restrict__ c, const double *__restrict__ r,
                        double *__restrict__ pv, const double *__restrict__ v, double *__restrict__ ph,
-                       const KrylovState *st) {
+                       const KrylovState *st, int diag) {
   if (st->done) return;
   const int it = st->iter;
   const double beta = st->beta, bo = __dmul_rn(st->beta, st->omega);
@@ -443,7 +443,7 @@ __global__ void k_bi_p(long long N, const double *__restrict__ c, const double *
       pp = __dsub_rn(pp, __dmul_rn(bo, v[p]));
     }
     pv[p] = pp;
-    ph[p] = __dmul_rn(pp, mc_of(c, p));
+    if (diag) ph[p] = __dmul_rn(pp, mc_of(c, p));
   }
 }
 
@@ -471,7 +471,7 @@ __global__ void k_bi_spmv(MatView<double> A, const double *__restrict__ x, doubl
 
 __global__ void k_bi_s(long long N, const double *__restrict__ c, const double *__restrict__ r,
                        const double *__restrict__ v, double *__restrict__ s, double *__restrict__ sh,
-                       KrylovState *st, double *part, unsigned *count) {
+                       KrylovState *st, double *part, unsigned *count, int diag) {
   if (st->done) return;
   const double alfa = st->alfa;
   double a[1] = {0.0};
@@ -479,7 +479,7 @@ __global__ void k_bi_s(long long N, const double *__restrict__ c, const double *
        p += (long long)gridDim.x * blockDim.x) {
     double sv = __dsub_rn(r[p], __dmul_rn(alfa, v[p]));
     s[p] = sv;
-    sh[p] = __dmul_rn(sv, mc_of(c, p));
+    if (diag) sh[p] = __dmul_rn(sv, mc_of(c, p));
     a[0] += __dmul_rn(sv, sv);
   }
   double o[1];
@@ -520,6 +520,114 @@ __global__ void k_bi_xr(long long N, double *__restrict__ x, double *__restrict_
       st->done = 1; st->converged = 1; st->status = ST_CONVERGED; st->iterations = it + 1;
     } else if (omega >= -st->res_tol && omega <= st->res_tol) {  // bicgs.cpp:189
       st->done = 1; st->status = ST_BREAKDOWN; st->iterations = it + 1;
+    } else if (stale_step_dev(st, res)) {
+      st->done = 1; st->status = ST_STALE; st->iterations = it + 1;
+    } else if (!(res == res)) {
+      st->done = 1; st->status = ST_NAN; st->iterations = it + 1;
+    } else {
+      st->rho_old = st->rho;
+      st->iter = it + 1;
+      st->iterations = it + 1;
+      if (it + 1 >= st->maxit) { st->done = 1; st->status = ST_MAXITER; }
+    }
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Conjugate gradient squared, CGS::solve (cgs.cpp:8-210). One iteration:
+//   k_cgs_rho  rho = r~.r; breakdown test; beta = rho / rho_old      (:83-104)
+//   k_cgs_up   u = r + beta q; p = u + beta^2 p; p += beta q (u = p = r at
+//              i = 0); p^ = p Mc                                      (:90-115)
+//   k_bi_spmv  v^ = A p^; r~.v^; alfa                                (:120-126)
+//   k_cgs_qs   q = u - alfa v^; s = u + q; u^ = s Mc                  (:131-139)
+//   k_cgs_xr   x += alfa u^; r -= alfa A u^; res; tests               (:144-196)
+// The initialisation (r = b - A x, r~ = r, res0) is k_bi_init's. With an
+// incomplete Cholesky preconditioner (diag == 0) the IC sweeps form p^
+// and u^ instead.
+// ---------------------------------------------------------------------------
+__global__ void k_cgs_rho(long long N, const double *__restrict__ rt, const double *__restrict__ r,
+                          KrylovState *st, double *part, unsigned *count) {
+  if (st->done) return;
+  double v[1] = {0.0};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x)
+    v[0] += __dmul_rn(rt[p], r[p]);
+  double o[1];
+  if (grid_reduce<1>(v, part, count, o, st->seq, N)) {
+    const int it = st->iter;
+    st->rho = o[0];
+    if (__dsqrt_rn(fabs(o[0])) < st->res_tol) {
+      st->done = 1; st->status = ST_BREAKDOWN; st->iterations = it + 1;
+    } else if (it > 0) {
+      st->beta = __ddiv_rn(o[0], st->rho_old);
+    }
+  }
+}
+
+__global__ void k_cgs_up(long long N, const double *__restrict__ c, const double *__restrict__ r,
+                         const double *__restrict__ q, double *__restrict__ u, double *__restrict__ pv,
+                         double *__restrict__ ph, const KrylovState *st, int diag) {
+  if (st->done) return;
+  const int it = st->iter;
+  const double beta = st->beta, bb = __dmul_rn(st->beta, st->beta);
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    double uu, pp;
+    if (it == 0) {
+      uu = r[p];
+      pp = uu;
+    } else {
+      uu = __dadd_rn(r[p], __dmul_rn(beta, q[p]));
+      pp = __dadd_rn(uu, __dmul_rn(bb, pv[p]));
+      pp = __dadd_rn(pp, __dmul_rn(beta, q[p]));
+    }
+    u[p] = uu;
+    pv[p] = pp;
+    if (diag) ph[p] = __dmul_rn(pp, mc_of(c, p));
+  }
+}
+
+__global__ void k_cgs_qs(long long N, const double *__restrict__ c, const double *__restrict__ u,
+                         const double *__restrict__ v, double *__restrict__ q, double *__restrict__ s,
+                         double *__restrict__ sh, const KrylovState *st, int diag) {
+  if (st->done) return;
+  const double alfa = st->alfa;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    const double qq = __dsub_rn(u[p], __dmul_rn(alfa, v[p]));
+    const double ss = __dadd_rn(u[p], qq);
+    q[p] = qq;
+    s[p] = ss;
+    if (diag) sh[p] = __dmul_rn(ss, mc_of(c, p));
+  }
+}
+
+__global__ void k_cgs_xr(MatView<double> A, double *__restrict__ x, double *__restrict__ r,
+                         const double *__restrict__ sh, KrylovState *st, double *hist, double *part,
+                         unsigned *count) {
+  if (st->done) return;
+  const long long N = A.ncell();
+  const double alfa = st->alfa, dV = st->dV;
+  double v[1] = {0.0};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    x[p] = __dadd_rn(x[p], __dmul_rn(alfa, sh[p]));
+    const double qq = ref_ax(A, p, q, [&](long long t) { return sh[t]; });
+    const double rv = __dsub_rn(r[p], __dmul_rn(alfa, qq));
+    r[p] = rv;
+    v[0] += voldiv(rv, rv, dV);
+  }
+  double o[1];
+  if (grid_reduce<1>(v, part, count, o, st->seq, N)) {
+    const int it = st->iter;
+    double res = res_of(o[0], st);
+    st->res = res;
+    if (hist && it < st->hist_cap) hist[it] = res;
+    const bool minok = it >= st->mini - 1;
+    if ((res < st->res_tol && minok) || (res < st->res0 * st->res_rat && minok)) {
+      st->done = 1; st->converged = 1; st->status = ST_CONVERGED; st->iterations = it + 1;
     } else if (stale_step_dev(st, res)) {
       st->done = 1; st->status = ST_STALE; st->iterations = it + 1;
     } else if (!(res == res)) {
@@ -758,10 +866,11 @@ __global__ void k_krylov_setup(KrylovState *st, KrylovParams pr, long long ncell
   st->rho = st->rho_old = st->alfa = st->beta = st->omega = st->pq = 0.0;
 }
 
-void RefKrylovWork::ensure(size_t n, bool bicgs) {
+void RefKrylovWork::ensure(size_t n, int solver) {
   auto fit = [n](DBuf<double> &b) { if (b.n < n) b.alloc(n); };
   fit(r); fit(q); fit(pA); fit(pB);
-  if (bicgs) { fit(rt); fit(ph); fit(v); fit(s); fit(sh); fit(t); }
+  if (solver >= 1) { fit(rt); fit(ph); fit(v); fit(s); fit(sh); fit(t); }
+  if (solver == 2) fit(u);
 }
 
 IcFactor RefKrylovWork::ic(int kind, size_t n) {
@@ -790,25 +899,35 @@ void enqueue_ref_setup(const MatView<double> &A, double *x, const double *b, con
                        cudaStream_t s) {
   const long long N = A.ncell();
   const int g = pr.seq ? grid_exact(N) : grid_for(N);
-  w.ensure((size_t)N, solver == 1);
+  w.ensure((size_t)N, solver);
   k_krylov_setup<<<1, 1, 0, s>>>(st, pr, N); note_launch();
-  if (solver == 0) {
-    PBG_CUDA(cudaMemsetAsync(w.pA.p, 0, sizeof(double) * N, s));
-    if (pr.prec > 0) {  // IncompleteCholesky*::form on every solve (precform)
-      const IcFactor M = w.ic(pr.prec, (size_t)N);
-      DBuf<double> *arr[8] = {&w.z, &w.mc, &w.mw, &w.ms, &w.mb, &w.mtw, &w.mts, &w.mnw};
-      for (DBuf<double> *a : arr)
-        if (a->p) PBG_CUDA(cudaMemsetAsync(a->p, 0, sizeof(double) * N, s));
-      const int H = ic_planes(A, M), gp = grid_for((long long)A.nx * A.ny);
-      for (int h = 0; h < H; ++h) { k_ic_form<<<gp, kThreads, 0, s>>>(A, M, h); note_launch(); }
-    }
-    k_cg_init<<<g, kThreads, 0, s>>>(A, x, b, w.r.p, st, red.slot_part(0), red.slot_count(0)); note_launch();
-  } else {
-    PBG_CUDA(cudaMemsetAsync(w.pA.p, 0, sizeof(double) * N, s));
+  PBG_CUDA(cudaMemsetAsync(w.pA.p, 0, sizeof(double) * N, s));
+  if (solver >= 1) {
     PBG_CUDA(cudaMemsetAsync(w.v.p, 0, sizeof(double) * N, s));
-    k_bi_init<<<g, kThreads, 0, s>>>(A, x, b, w.r.p, w.rt.p, st, red.slot_part(0), red.slot_count(0)); note_launch();
+    PBG_CUDA(cudaMemsetAsync(w.q.p, 0, sizeof(double) * N, s));
   }
+  if (pr.prec > 0) {  // IncompleteCholesky*::form on every solve (precform)
+    const IcFactor M = w.ic(pr.prec, (size_t)N);
+    DBuf<double> *arr[8] = {&w.z, &w.mc, &w.mw, &w.ms, &w.mb, &w.mtw, &w.mts, &w.mnw};
+    for (DBuf<double> *a : arr)
+      if (a->p) PBG_CUDA(cudaMemsetAsync(a->p, 0, sizeof(double) * N, s));
+    const int H = ic_planes(A, M), gp = grid_for((long long)A.nx * A.ny);
+    for (int h = 0; h < H; ++h) { k_ic_form<<<gp, kThreads, 0, s>>>(A, M, h); note_launch(); }
+  }
+  if (solver == 0)
+    k_cg_init<<<g, kThreads, 0, s>>>(A, x, b, w.r.p, st, red.slot_part(0), red.slot_count(0));
+  else
+    k_bi_init<<<g, kThreads, 0, s>>>(A, x, b, w.r.p, w.rt.p, st, red.slot_part(0), red.slot_count(0));
+  note_launch();
   PBG_CUDA(cudaGetLastError());
+}
+
+// z = M^-1 r with the IC factor: forward then backward hyperplane sweeps
+static void ic_apply(const MatView<double> &A, const IcFactor &M, const double *r, double *z,
+                     const KrylovState *st, cudaStream_t s) {
+  const int H = ic_planes(A, M), gp = grid_for((long long)A.nx * A.ny);
+  for (int h = 0; h < H; ++h) { k_ic_fwd<<<gp, kThreads, 0, s>>>(A, M, h, r, z, st); note_launch(); }
+  for (int h = H - 1; h >= 0; --h) { k_ic_bwd<<<gp, kThreads, 0, s>>>(A, M, h, z, st); note_launch(); }
 }
 
 void enqueue_ref_iters(const MatView<double> &A, double *x, int solver, int count,
@@ -818,26 +937,36 @@ void enqueue_ref_iters(const MatView<double> &A, double *x, int solver, int coun
   const int g = exact ? grid_exact(N) : grid_for(N);
   double *P0 = red.slot_part(0), *P1 = red.slot_part(1);
   unsigned *C0 = red.slot_count(0), *C1 = red.slot_count(1);
+  const int diag = prec > 0 ? 0 : 1;
+  IcFactor M{};
+  if (prec > 0) M = w.ic(prec, (size_t)N);
   for (int it = 0; it < count; ++it) {
     if (solver == 0 && prec > 0) {
       // z = M^-1 r (forward and backward sweeps), rho = r.z, then the CG step
-      const IcFactor M = w.ic(prec, (size_t)N);
-      const int H = ic_planes(A, M), gp = grid_for((long long)A.nx * A.ny);
-      for (int h = 0; h < H; ++h) { k_ic_fwd<<<gp, kThreads, 0, s>>>(A, M, h, w.r.p, w.z.p, st); note_launch(); }
-      for (int h = H - 1; h >= 0; --h) { k_ic_bwd<<<gp, kThreads, 0, s>>>(A, M, h, w.z.p, st); note_launch(); }
+      ic_apply(A, M, w.r.p, w.z.p, st, s);
       k_cg_rho<<<g, kThreads, 0, s>>>(N, w.r.p, w.z.p, st, P0, C0); note_launch();
       k_cg_pq<<<g, kThreads, 0, s>>>(A, w.r.p, w.pA.p, w.pB.p, w.q.p, st, P0, C0, w.z.p); note_launch();
       k_cg_xr<<<g, kThreads, 0, s>>>(N, A.c, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1, 1); note_launch();
     } else if (solver == 0) {
       k_cg_pq<<<g, kThreads, 0, s>>>(A, w.r.p, w.pA.p, w.pB.p, w.q.p, st, P0, C0, nullptr); note_launch();
       k_cg_xr<<<g, kThreads, 0, s>>>(N, A.c, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1, 0); note_launch();
-    } else {
+    } else if (solver == 1) {
       k_bi_rho<<<g, kThreads, 0, s>>>(N, w.rt.p, w.r.p, st, P0, C0); note_launch();
-      k_bi_p<<<g, kThreads, 0, s>>>(N, A.c, w.r.p, w.pA.p, w.v.p, w.ph.p, st); note_launch();
+      k_bi_p<<<g, kThreads, 0, s>>>(N, A.c, w.r.p, w.pA.p, w.v.p, w.ph.p, st, diag); note_launch();
+      if (!diag) ic_apply(A, M, w.pA.p, w.ph.p, st, s);
       k_bi_spmv<<<g, kThreads, 0, s>>>(A, w.ph.p, w.v.p, w.rt.p, 0, st, P1, C1); note_launch();
-      k_bi_s<<<g, kThreads, 0, s>>>(N, A.c, w.r.p, w.v.p, w.s.p, w.sh.p, st, P0, C0); note_launch();
+      k_bi_s<<<g, kThreads, 0, s>>>(N, A.c, w.r.p, w.v.p, w.s.p, w.sh.p, st, P0, C0, diag); note_launch();
+      if (!diag) ic_apply(A, M, w.s.p, w.sh.p, st, s);
       k_bi_spmv<<<g, kThreads, 0, s>>>(A, w.sh.p, w.t.p, w.s.p, 1, st, P1, C1); note_launch();
       k_bi_xr<<<g, kThreads, 0, s>>>(N, x, w.r.p, w.ph.p, w.sh.p, w.s.p, w.t.p, st, hist, P0, C0); note_launch();
+    } else {
+      k_cgs_rho<<<g, kThreads, 0, s>>>(N, w.rt.p, w.r.p, st, P0, C0); note_launch();
+      k_cgs_up<<<g, kThreads, 0, s>>>(N, A.c, w.r.p, w.q.p, w.u.p, w.pA.p, w.ph.p, st, diag); note_launch();
+      if (!diag) ic_apply(A, M, w.pA.p, w.ph.p, st, s);
+      k_bi_spmv<<<g, kThreads, 0, s>>>(A, w.ph.p, w.v.p, w.rt.p, 0, st, P1, C1); note_launch();
+      k_cgs_qs<<<g, kThreads, 0, s>>>(N, A.c, w.u.p, w.v.p, w.q.p, w.s.p, w.sh.p, st, diag); note_launch();
+      if (!diag) ic_apply(A, M, w.s.p, w.sh.p, st, s);
+      k_cgs_xr<<<g, kThreads, 0, s>>>(A, x, w.r.p, w.sh.p, st, hist, P0, C0); note_launch();
     }
   }
   PBG_CUDA(cudaGetLastError());

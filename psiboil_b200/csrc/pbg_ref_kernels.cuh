@@ -17,16 +17,17 @@ struct IcFactor {
 };
 
 struct KrylovParams {
-  int prec = 0;            // Prec code: 0 diagonal, 1 IC0, 2 IC2, 3 IC3 (CG)
+  int prec = 0;            // Prec code: 0 diagonal, 1 IC0, 2 IC2, 3 IC3
   int mini, maxit, stalecount, hist_cap;
   double res_rat, res_tol, scale, dV;
   double *seq = nullptr;   // exact-order reduction terms (2 x ncell), null: tree
 };
 
+// solver codes of the drivers below: 0 CG, 1 BiCGS, 2 CGS
 struct RefKrylovWork {
-  DBuf<double> r, q, pA, pB, rt, ph, v, s, sh, t;
+  DBuf<double> r, q, pA, pB, rt, ph, v, s, sh, t, u;
   DBuf<double> z, mc, mw, ms, mb, mtw, mts, mnw;  // IC preconditioner
-  void ensure(size_t n, bool bicgs);
+  void ensure(size_t n, int solver);
   IcFactor ic(int kind, size_t n);
 };
 

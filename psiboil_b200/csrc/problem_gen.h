@@ -392,6 +392,25 @@ static inline void pbg_gen_bc_finalize(int nx, int ny, int nz, const int bc[6],
   }
 }
 
+/* Non-symmetric variant of the fixture, the shape of the reference's other
+ * Centered equations (convection-diffusion): first-order upwind convection
+ * with a mass flux F > 0 along +x between fluid cells adds F to the west
+ * coupling and to the diagonal of the downstream cell. Applied after the
+ * boundary correction; ci = 1/c is recomputed for the cells it changes. */
+static inline void pbg_gen_convect(int nx, int ny, int nz, double F, const uint8_t *solid,
+                                   double *c, double *w, double *ci) {
+  const size_t SI = (size_t)ny * nz;
+  for (int i = 1; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        size_t p = (size_t)i * SI + (size_t)j * nz + k;
+        if (solid[p] || solid[p - SI]) continue;
+        w[p] += F;
+        c[p] += F;
+        if (ci) ci[p] = 1.0 / c[p];
+      }
+}
+
 /* Full fixture assembly (stage 1 + stage 2). Outputs the seven coefficient
  * arrays with the reference sign convention  A x = c x_P - sum a_nb x_nb,
  * and ci = 1/c taken before the solid-cell scaling. */

@@ -21,11 +21,15 @@ import oracle_py as O  # noqa: E402
 
 CASES = [
     # name, kind, problem kwargs, runs
-    ("single16", O.KIND_SINGLE, dict(n=16), ["cg", "bicgs", "ac", "cg_ic0", "cg_ic2", "cg_ic3"]),
+    ("single16", O.KIND_SINGLE, dict(n=16), ["cg", "bicgs", "ac", "cg_ic0", "cg_ic2", "cg_ic3", "cgs",
+                                             "bicgs_ic2", "cgs_ic0"]),
     ("single12", O.KIND_SINGLE, dict(n=12), ["cg", "ac_w", "ac_f", "ac_noguard"]),
     ("cyl24", O.KIND_CYL, dict(n=24, nb=3, rmin=2.0, rmax=4.0, rc=5.0), ["cg", "ac", "cg_ic2"]),
     ("odd15", O.KIND_BATCH, dict(index=40, n2d=0, s3=(15, 16)), ["cg", "ac"]),
     ("flat2d", O.KIND_BATCH, dict(index=1, n2d=8, s2=(24, 40)), ["cg", "bicgs", "ac"]),
+    # non-symmetric: upwind convection along +x added to the fixture
+    ("conv12", O.KIND_SINGLE, dict(n=12, convect=2e-5), ["bicgs", "cgs", "bicgs_ic0", "bicgs_ic2",
+                                                        "cgs_ic2", "cgs_ic3"]),
 ]
 
 
@@ -71,7 +75,7 @@ def main():
         for run in runs:
             solver = "ac" if run.startswith("ac") else run.split("_")[0]
             extra = {}
-            if run.startswith("cg_ic"):
+            if "_ic" in run:
                 extra = dict(prec=run.split("_")[1])
             if run == "ac_w":
                 extra = dict(cycle="W")

@@ -4,7 +4,7 @@ import os
 import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-NAMES = ["single16", "single12", "cyl24", "odd15", "flat2d"]
+NAMES = ["single16", "single12", "cyl24", "odd15", "flat2d", "conv12"]
 
 
 def load(name):

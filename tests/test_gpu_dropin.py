@@ -71,3 +71,24 @@ def test_reference_with_gpu_ic_cg_is_bit_exact(case, args, prec):
                           "--gpu", "1", "--exact", "1"])
     assert np.array_equal(x, g["cg_" + prec + "_x"])
     assert int(meta["iterations"][0]) == int(g["cg_" + prec + "_iterations"])
+
+
+@pytest.mark.skipif(not os.path.exists(EXE), reason="GPU-backed reference harness not built")
+@pytest.mark.parametrize("case,args,key", [
+    ("single16", ["--kind", "single", "--n", "16"], "cgs"),
+    ("single16", ["--kind", "single", "--n", "16"], "bicgs_ic2"),
+    ("single16", ["--kind", "single", "--n", "16"], "cgs_ic0"),
+    ("conv12", ["--kind", "single", "--n", "12", "--convect", "2e-05"], "bicgs_ic0"),
+    ("conv12", ["--kind", "single", "--n", "12", "--convect", "2e-05"], "cgs"),
+    ("conv12", ["--kind", "single", "--n", "12", "--convect", "2e-05"], "cgs_ic3")])
+def test_reference_with_gpu_bicgs_cgs_is_bit_exact(case, args, key):
+    """`new GpuCGS(d, pc)` / `new GpuBiCGS(d, pc)` in place of the reference's
+    CGS / BiCGS, on the pressure fixture and on its convected (non-symmetric)
+    variant: the CPU reference's solution and iteration count bit for bit."""
+    g = load(case)
+    parts = key.split("_")
+    prec = parts[1] if len(parts) > 1 else "di"
+    x, meta = run(args + ["--seed", "7", "--solver", parts[0], "--prec", prec, "--resrat", "1e-8",
+                          "--gpu", "1", "--exact", "1"])
+    assert np.array_equal(x, g[key + "_x"])
+    assert int(meta["iterations"][0]) == int(g[key + "_iterations"])

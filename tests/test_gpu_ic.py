@@ -47,11 +47,3 @@ def test_ic_reduces_iterations(engine, oracle):
             assert cg.solve(x, P.b.copy(), 1, 20000, None, 1e-8, 1e-15)
             its[prec] = cg.last.iterations
     assert its["ic0"] < its["di"] and its["ic2"] <= its["ic0"] and its["ic3"] <= its["ic2"]
-
-
-def test_ic_rejected_for_bicgs(engine, oracle):
-    P = oracle.Problem(0, 5, n=8)
-    with engine.Session(*P.dims, P.h) as s:
-        s.assemble_pressure(P.rho, P.solid)
-        with pytest.raises(engine.PbgError):
-            engine.BiCGS(s, prec="ic2").solve(np.zeros(P.N), P.b.copy(), 1, 100)

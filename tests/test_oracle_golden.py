@@ -17,23 +17,27 @@ def test_fixture_matrix_and_rhs_bit_exact(oracle, name):
     assert np.array_equal(P.b, g["b"])
 
 
-@pytest.mark.parametrize("name", NAMES)
-def test_cg_bit_exact(oracle, name):
-    g = load(name)
-    P = problem_of(g, oracle)
-    x, st = oracle.cg(P, res_rat=1e-8, maxit=20000)
-    assert st["printed"] == int(g["cg_iterations"])
-    assert st["converged"] == int(g["cg_converged"])
-    assert np.array_equal(x, g["cg_x"])
+def _krylov_runs():
+    out = []
+    for n in NAMES:
+        for key in load(n):
+            if key.endswith("_x") and key.split("_")[0] in ("cg", "bicgs", "cgs"):
+                out.append((n, key[:-2]))
+    return out
 
 
-@pytest.mark.parametrize("name", [n for n in NAMES if "bicgs_x" in load(n)])
-def test_bicgs_bit_exact(oracle, name):
+@pytest.mark.parametrize("name,run", _krylov_runs())
+def test_krylov_bit_exact(oracle, name, run):
+    """CG, BiCGS and CGS, with the diagonal or an IC preconditioner, on
+    symmetric and convected (non-symmetric) fixtures."""
     g = load(name)
     P = problem_of(g, oracle)
-    x, st = oracle.cg(P, res_rat=1e-8, maxit=20000, solver="bicgs")
-    assert st["printed"] == int(g["bicgs_iterations"])
-    assert np.array_equal(x, g["bicgs_x"])
+    parts = run.split("_")
+    solver, prec = parts[0], (parts[1] if len(parts) > 1 else "di")
+    x, st = oracle.cg(P, res_rat=1e-8, maxit=20000, solver=solver, prec=prec)
+    assert st["printed"] == int(g[run + "_iterations"])
+    assert st["converged"] == int(g[run + "_converged"])
+    assert np.array_equal(x, g[run + "_x"], equal_nan=True)
 
 
 AC_RUNS = {"ac": dict(loop=1), "ac_w": dict(loop=4), "ac_f": dict(loop=2),
