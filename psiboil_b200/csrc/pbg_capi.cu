@@ -1,10 +1,12 @@
 // C ABI of the engine: sessions, uploads, on-device pressure assembly and
 // the solver entry points. No torch types; plain pointers and sizes.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/psiboil_b200.h"
@@ -117,6 +119,78 @@ __global__ void k_assemble(int nx, int ny, int nz, double h, int4 bc03, int2 bc4
     B[p] = b;
     aflag[p] = solid[p] ? 0 : 1;
   }
+}
+
+// Host buffers: pinned ones (cudaMallocHost, cudaHostRegister, torch's
+// pin_memory) are copied by DMA directly; pageable ones go through the
+// session's pinned staging in chunks, the host copy of chunk k+1 (split over
+// a few threads) overlapping the DMA of chunk k.
+bool is_pinned(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+constexpr size_t kStageChunk = 16u << 20;
+
+void par_memcpy(void *dst, const void *src, size_t n) {
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t parts = std::min<size_t>({8, hw, n / (2u << 20)});
+  if (parts <= 1) {
+    std::memcpy(dst, src, n);
+    return;
+  }
+  const size_t step = (n / parts + 63) & ~size_t(63);
+  std::vector<std::thread> th;
+  for (size_t q = 1; q < parts; ++q) {
+    const size_t off = q * step;
+    if (off >= n) break;
+    th.emplace_back([=] { std::memcpy((char *)dst + off, (const char *)src + off, std::min(step, n - off)); });
+  }
+  std::memcpy(dst, src, std::min(step, n));
+  for (auto &t : th) t.join();
+}
+
+// host -> device of n bytes; stage: pinned scratch of at least n bytes
+void h2d(pbg_session *s, void *dev, const void *host, size_t n, void *stage) {
+  if (is_pinned(host)) {
+    PBG_CUDA(cudaMemcpyAsync(dev, host, n, cudaMemcpyHostToDevice, s->stream));
+    return;
+  }
+  for (size_t off = 0; off < n; off += kStageChunk) {
+    const size_t len = std::min(kStageChunk, n - off);
+    par_memcpy((char *)stage + off, (const char *)host + off, len);
+    PBG_CUDA(cudaMemcpyAsync((char *)dev + off, (char *)stage + off, len, cudaMemcpyHostToDevice, s->stream));
+  }
+}
+
+// device -> host of n bytes (returns with the data on the host)
+void d2h(pbg_session *s, void *host, const void *dev, size_t n, void *stage) {
+  if (is_pinned(host)) {
+    PBG_CUDA(cudaMemcpyAsync(host, dev, n, cudaMemcpyDeviceToHost, s->stream));
+    PBG_CUDA(cudaStreamSynchronize(s->stream));
+    return;
+  }
+  std::vector<cudaEvent_t> ev;
+  for (size_t off = 0; off < n; off += kStageChunk) {
+    const size_t len = std::min(kStageChunk, n - off);
+    PBG_CUDA(cudaMemcpyAsync((char *)stage + off, (const char *)dev + off, len, cudaMemcpyDeviceToHost, s->stream));
+    cudaEvent_t e;
+    PBG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    PBG_CUDA(cudaEventRecord(e, s->stream));
+    ev.push_back(e);
+  }
+  size_t k = 0;
+  cudaError_t err = cudaSuccess;
+  for (size_t off = 0; off < n; off += kStageChunk, ++k) {
+    if (err == cudaSuccess) err = cudaEventSynchronize(ev[k]);
+    if (err == cudaSuccess) par_memcpy((char *)host + off, (char *)stage + off, std::min(kStageChunk, n - off));
+  }
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  PBG_CUDA(err);
 }
 
 void ensure_staging(pbg_session *s) {
@@ -724,29 +798,29 @@ int pbg_solve_strided(pbg_session *s, double *x, const double *b, long long si, 
       ensure_staging(s);
       if (where == PBG_HOST) {
         if (compact) {
-          std::memcpy(s->px, x, N * 8);
-          std::memcpy(s->pb, b, N * 8);
+          h2d(s, s->dx.p, x, N * 8, s->px);
+          h2d(s, s->db.p, b, N * 8, s->pb);
         } else {
           gather(x, s->px, s->nx, s->ny, s->nz, si, sj, sk, offset);
           gather(b, s->pb, s->nx, s->ny, s->nz, si, sj, sk, offset);
+          PBG_CUDA(cudaMemcpyAsync(s->dx.p, s->px, N * 8, cudaMemcpyHostToDevice, s->stream));
+          PBG_CUDA(cudaMemcpyAsync(s->db.p, s->pb, N * 8, cudaMemcpyHostToDevice, s->stream));
         }
-        PBG_CUDA(cudaMemcpyAsync(s->dx.p, s->px, N * 8, cudaMemcpyHostToDevice, s->stream));
-        PBG_CUDA(cudaMemcpyAsync(s->db.p, s->pb, N * 8, cudaMemcpyHostToDevice, s->stream));
       } else {
         k_gather<<<grid_for(N), kThreads, 0, s->stream>>>(x, s->dx.p, s->nx, s->ny, s->nz, si, sj, sk, offset); note_launch();
         k_gather<<<grid_for(N), kThreads, 0, s->stream>>>(b, s->db.p, s->nx, s->ny, s->nz, si, sj, sk, offset); note_launch();
       }
       rc = solve_device(s, s->dx.p, s->db.p, p, r);
       if (rc == PBG_OK) {
-        if (where == PBG_HOST) {
+        if (where == PBG_HOST && compact) {
+          d2h(s, x, s->dx.p, N * 8, s->px);
+        } else if (where == PBG_HOST) {
           PBG_CUDA(cudaMemcpyAsync(s->px, s->dx.p, N * 8, cudaMemcpyDeviceToHost, s->stream));
           PBG_CUDA(cudaStreamSynchronize(s->stream));
-          if (compact) std::memcpy(x, s->px, N * 8);
-          else
-            for (int i = 0; i < s->nx; ++i)
-              for (int j = 0; j < s->ny; ++j)
-                for (int k = 0; k < s->nz; ++k)
-                  x[offset + i * si + j * sj + k * sk] = s->px[((size_t)i * s->ny + j) * s->nz + k];
+          for (int i = 0; i < s->nx; ++i)
+            for (int j = 0; j < s->ny; ++j)
+              for (int k = 0; k < s->nz; ++k)
+                x[offset + i * si + j * sj + k * sk] = s->px[((size_t)i * s->ny + j) * s->nz + k];
         } else {
           k_scatter<<<grid_for(N), kThreads, 0, s->stream>>>(s->dx.p, x, s->nx, s->ny, s->nz, si, sj, sk, offset); note_launch();
         }

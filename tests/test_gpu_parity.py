@@ -29,8 +29,11 @@ def relerr(x, ref):
 
 
 def session_for(engine, P, assemble=True):
+    """A session holding P's matrix: assembled on the device, or uploaded
+    (always uploaded for the convected fixtures, which the on-device
+    pressure assembly does not make)."""
     s = engine.Session(*P.dims, P.h)
-    if assemble:
+    if assemble and not P.convect:
         s.assemble_pressure(P.rho, P.solid)
     else:
         s.upload_matrix(P.A)
@@ -41,6 +44,8 @@ def session_for(engine, P, assemble=True):
 @pytest.mark.parametrize("name", NAMES)
 def test_assembly_bit_exact(engine, oracle, name):
     P = problem_of(load(name), oracle)
+    if P.convect:
+        pytest.skip("the convected fixture is uploaded, not assembled")
     with session_for(engine, P) as s:
         assert s.symmetric()
         M = s.download_matrix()
