@@ -14,6 +14,7 @@
 
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 namespace pbg {
 
@@ -49,6 +50,43 @@ inline int grid_for(long long n, int threads = kThreads, int cap = kMaxBlocks) {
   if (b < 1) b = 1;
   if (b > cap) b = cap;
   return (int)b;
+}
+
+// ---------------------------------------------------------------------------
+// Programmatic dependent launch. A kernel launched with launch_pdl may be
+// scheduled while its predecessor in the stream (or the graph captured from
+// it) drains, so that the launch latency of the many small coarse-level
+// kernels overlaps the tail of the previous one. Every such kernel starts
+// with PBG_PDL_ENTRY: it waits for the predecessor grid to complete and its
+// memory to be visible (griddepcontrol.wait, a hardware dependency, not a
+// spin) before touching anything, then lets its own successor be scheduled.
+// Without the launch attribute both instructions return at once.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+#define PBG_PDL_ENTRY() \
+  do {                   \
+    ::pbg::pdl_wait();   \
+    ::pbg::pdl_trigger(); \
+  } while (0)
+
+// PBG_PDL=0 in the environment launches these kernels the ordinary way.
+bool pdl_enabled();
+
+template <typename... K, typename... A>
+inline void launch_pdl(void (*kern)(K...), int grid, int block, cudaStream_t s, A &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  PBG_CUDA(cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...));
+  note_launch();
 }
 
 // ---------------------------------------------------------------------------

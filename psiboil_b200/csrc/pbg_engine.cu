@@ -199,8 +199,40 @@ void EWork<T>::ensure(const std::vector<ELevel> &lv) {
 template <typename T>
 void EWork<T>::drop_graph() {
   if (iter_graph) cudaGraphExecDestroy(iter_graph);
+  if (loop_graph) cudaGraphExecDestroy(loop_graph);
   iter_graph = nullptr;
+  loop_graph = nullptr;
   iter_nodes = 0;
+}
+
+// Programmatic dependent launch measured no gain inside the captured
+// iteration (20.0 against 20.2 ms at 256^3), so it is off unless PBG_PDL=1.
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char *e = getenv("PBG_PDL");
+    return e && atoi(e) == 1;
+  }();
+  return on;
+}
+
+// End of one FCG iteration in the device-side loop (a conditional WHILE
+// node of a CUDA graph): continue while the solve is running, and never
+// more than maxit times, whatever the flags say.
+__global__ void k_fcg_continue(cudaGraphConditionalHandle h, FcgScal *fs) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int n = ++fs->loops;
+  cudaGraphSetConditional(h, (!fs->done && n < fs->maxit) ? 1u : 0u);
+}
+
+// The FCG iterations of a refinement sweep run as a device-side loop (a
+// conditional WHILE graph node) unless PBG_GRAPH_LOOP=0, which replays the
+// one-iteration graph in host-polled chunks instead.
+static bool graph_loop_enabled() {
+  static const bool on = [] {
+    const char *e = getenv("PBG_GRAPH_LOOP");
+    return !(e && atoi(e) == 0);
+  }();
+  return on;
 }
 
 // Tuning knobs (environment): PBG_COARSE_MAX sets the size of the dense
@@ -233,8 +265,7 @@ template <typename T>
 void Engine::dense_solve(const T *r, T *z, const int *stop, cudaStream_t s) {
   using AT = typename std::conditional<sizeof(T) == 4, float, double>::type;
   const int blocks = (int)(((long long)ncoarse * 32 + kThreads - 1) / kThreads);
-  k_dense_solve<T, AT><<<blocks, kThreads, 0, s>>>(ncoarse, (const AT *)ainv<T>(), r, z, stop);
-  note_launch();
+  launch_pdl(k_dense_solve<T, AT>, blocks, kThreads, s, ncoarse, (const AT *)ainv<T>(), r, z, stop);
 }
 
 void Engine::build(const EMat<double> &A0, cudaStream_t s, bool mixed) {
@@ -346,8 +377,8 @@ void Engine::precond(int l, const T *r, T *z, bool dots, const T *u, double *out
       EMat<T> A = mat<T>(l);
       PBG_CUDA(cudaMemcpyAsync(v.xa.p, z, sizeof(T) * A.ncell(), cudaMemcpyDeviceToDevice, s));
       // omega = 0 keeps z and computes the dot products
-      k_jac_dots<T><<<grid_for(A.ncell()), kThreads, 0, s>>>(A, r, v.xa.p, z, T(0), u, out2,
-                                                            red.slot_part(0), red.slot_count(0), stop); note_launch();
+      launch_pdl(k_jac_dots<T>, grid_for(A.ncell()), kThreads, s, A, r, (const T *)v.xa.p, z, T(0), u, out2,
+                 red.slot_part(0), red.slot_count(0), stop);
     }
     return;
   }
@@ -358,16 +389,12 @@ void Engine::precond(int l, const T *r, T *z, bool dots, const T *u, double *out
   const T *rr = kc ? v.r1.p : r;
   const bool vec = A.nz % VecTraits<T>::V == 0;
   const int gv = grid_for(A.ncell() / VecTraits<T>::V, kThreads, kVecBlocks);
-  if (vec) {
-    kv_jac2<T><<<gv, kThreads, 0, s>>>(A, r, v.b.p, v.q1.p, kc ? w.ks.p + l : nullptr, v.r1.p,
-                                       v.xb.p, om, stop); note_launch();
-  } else {
-    k_jac2<T><<<g, kThreads, 0, s>>>(A, r, v.b.p, v.q1.p, kc ? w.ks.p + l : nullptr, v.r1.p, v.xb.p,
-                                     om, stop); note_launch();
-  }
+  const KScal *ksl = kc ? w.ks.p + l : nullptr;
+  launch_pdl(vec ? kv_jac2<T> : k_jac2<T>, vec ? gv : g, kThreads, s, A, r, (const T *)v.b.p,
+             (const T *)v.q1.p, ksl, v.r1.p, v.xb.p, om, stop);
   const long long rthreads = H.ncell() >= kRestrictSerialMin ? H.ncell() : H.ncell() * 8;
-  k_resid_restrict<T><<<grid_for(rthreads), kThreads, 0, s>>>(A, rr, v.xb.p, Geo(H.nx, H.ny, H.nz),
-                                                              vh.b.p, stop); note_launch();
+  launch_pdl(k_resid_restrict<T>, grid_for(rthreads), kThreads, s, A, rr, (const T *)v.xb.p,
+             Geo(H.nx, H.ny, H.nz), vh.b.p, stop);
   const T *eH, *z2H = nullptr;
   const KScal *ksH = nullptr;
   if (l + 1 == last) {
@@ -382,25 +409,21 @@ void Engine::precond(int l, const T *r, T *z, bool dots, const T *u, double *out
       eH = vh.z1.p;
     }
   }
-  if (vec) {
-    kv_prolong_jac<T><<<gv, kThreads, 0, s>>>(A, rr, v.xb.p, H.ny, H.nz, eH, z2H, ksH, v.xa.p, om,
-                                              stop); note_launch();
-  } else {
-    k_prolong_jac<T><<<g, kThreads, 0, s>>>(A, rr, v.xb.p, H.ny, H.nz, eH, z2H, ksH, v.xa.p, om,
-                                            stop); note_launch();
-  }
+  launch_pdl(vec ? kv_prolong_jac<T> : k_prolong_jac<T>, vec ? gv : g, kThreads, s, A, rr,
+             (const T *)v.xb.p, H.ny, H.nz, eH, z2H, ksH, v.xa.p, om, stop);
   if (dots && vec && l == 0) {
     // u is the q of the previous FCG iteration, picked by parity on the device
-    kv_jac<T, true><<<gv, kThreads, 0, s>>>(A, rr, v.xa.p, z, om, w.q0.p, w.q0b.p, w.fs.p, out2,
-                                            red.slot_part(0), red.slot_count(0), stop); note_launch();
+    launch_pdl(kv_jac<T, true>, gv, kThreads, s, A, rr, (const T *)v.xa.p, z, om, (const T *)w.q0.p,
+               (const T *)w.q0b.p, (const FcgScal *)w.fs.p, out2, red.slot_part(0), red.slot_count(0), stop);
   } else if (dots) {
-    k_jac_dots<T><<<g, kThreads, 0, s>>>(A, rr, v.xa.p, z, om, u, out2, red.slot_part(0),
-                                         red.slot_count(0), stop); note_launch();
+    launch_pdl(k_jac_dots<T>, g, kThreads, s, A, rr, (const T *)v.xa.p, z, om, u, out2, red.slot_part(0),
+               red.slot_count(0), stop);
   } else if (vec) {
-    kv_jac<T, false><<<gv, kThreads, 0, s>>>(A, rr, v.xa.p, z, om, nullptr, nullptr, nullptr,
-                                             nullptr, nullptr, nullptr, stop); note_launch();
+    launch_pdl(kv_jac<T, false>, gv, kThreads, s, A, rr, (const T *)v.xa.p, z, om, (const T *)nullptr,
+               (const T *)nullptr, (const FcgScal *)nullptr, (double *)nullptr, (double *)nullptr,
+               (unsigned *)nullptr, stop);
   } else {
-    k_jac<T><<<g, kThreads, 0, s>>>(A, rr, v.xa.p, z, om, stop); note_launch();
+    launch_pdl(k_jac<T>, g, kThreads, s, A, rr, (const T *)v.xa.p, z, om, stop);
   }
 }
 
@@ -411,10 +434,11 @@ void Engine::kcycle(int l, EWork<T> &w, RedPool &red, const int *stop, cudaStrea
   auto &v = w.L[l];
   KScal *ks = w.ks.p + l;
   precond<T>(l, v.b.p, v.z1.p, false, nullptr, nullptr, w, red, stop, s, false);
-  k_kc_q1<T><<<g, kThreads, 0, s>>>(A, v.z1.p, v.b.p, v.q1.p, ks, red.slot_part(0), red.slot_count(0), stop); note_launch();
+  launch_pdl(k_kc_q1<T>, g, kThreads, s, A, (const T *)v.z1.p, (const T *)v.b.p, v.q1.p, ks,
+             red.slot_part(0), red.slot_count(0), stop);
   precond<T>(l, nullptr, v.z2.p, false, nullptr, nullptr, w, red, stop, s, true);
-  k_kc_q2<T><<<g, kThreads, 0, s>>>(A, v.z2.p, v.q1.p, v.r1.p, v.v.p, ks, red.slot_part(0),
-                                    red.slot_count(0), stop); note_launch();
+  launch_pdl(k_kc_q2<T>, g, kThreads, s, A, (const T *)v.z2.p, (const T *)v.q1.p, (const T *)v.r1.p, v.v.p,
+             ks, red.slot_part(0), red.slot_count(0), stop);
 }
 
 // Flexible CG on level 0 for A e = b (e starts at zero); returns iterations.
@@ -429,24 +453,29 @@ int Engine::fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red, cu
   const int g = grid_for(N);
   FcgScal *fs = w.fs.p;
   const int *stop = &fs->done;
+  // one FCG iteration: the preconditioner's K-cycle over all levels plus
+  // the two FCG kernels
+  auto iteration = [&]() {
+    precond<T>(0, w.r0.p, w.z0.p, true, w.q0.p, &fs->zr, w, red, stop, s, false);
+    if (A.nz % VecTraits<T>::V == 0 && (int)L.size() > 1) {
+      const int gv = grid_for(N / VecTraits<T>::V, kThreads, kVecBlocks);
+      launch_pdl(kv_fcg_pq<T>, gv, kThreads, s, A, (const T *)w.z0.p, w.pA.p, w.pB.p, w.q0.p, w.q0b.p, fs,
+                 red.slot_part(0), red.slot_count(0));
+      launch_pdl(kv_fcg_xr<T>, gv, kThreads, s, N, w.x0.p, w.r0.p, (const T *)w.pA.p, (const T *)w.pB.p,
+                 (const T *)w.q0.p, (const T *)w.q0b.p, fs, red.slot_part(0), red.slot_count(0));
+    } else {
+      launch_pdl(k_fcg_pq<T>, g, kThreads, s, A, (const T *)w.z0.p, w.pA.p, w.pB.p, w.q0.p, fs,
+                 red.slot_part(0), red.slot_count(0));
+      launch_pdl(k_fcg_xr<T>, g, kThreads, s, N, w.x0.p, w.r0.p, (const T *)w.pA.p, (const T *)w.pB.p,
+                 (const T *)w.q0.p, fs, red.slot_part(0), red.slot_count(0));
+    }
+  };
   if (!w.iter_graph) {
     cudaGraph_t graph = nullptr;
     const unsigned long long before = g_launch_count;
     PBG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     try {
-      precond<T>(0, w.r0.p, w.z0.p, true, w.q0.p, &fs->zr, w, red, stop, s, false);
-      if (A.nz % VecTraits<T>::V == 0 && (int)L.size() > 1) {
-        const int gv = grid_for(N / VecTraits<T>::V, kThreads, kVecBlocks);
-        kv_fcg_pq<T><<<gv, kThreads, 0, s>>>(A, w.z0.p, w.pA.p, w.pB.p, w.q0.p, w.q0b.p, fs,
-                                             red.slot_part(0), red.slot_count(0)); note_launch();
-        kv_fcg_xr<T><<<gv, kThreads, 0, s>>>(N, w.x0.p, w.r0.p, w.pA.p, w.pB.p, w.q0.p, w.q0b.p, fs,
-                                             red.slot_part(0), red.slot_count(0)); note_launch();
-      } else {
-        k_fcg_pq<T><<<g, kThreads, 0, s>>>(A, w.z0.p, w.pA.p, w.pB.p, w.q0.p, fs, red.slot_part(0),
-                                           red.slot_count(0)); note_launch();
-        k_fcg_xr<T><<<g, kThreads, 0, s>>>(N, w.x0.p, w.r0.p, w.pA.p, w.pB.p, w.q0.p, fs,
-                                           red.slot_part(0), red.slot_count(0)); note_launch();
-      }
+      iteration();
     } catch (...) {
       cudaStreamEndCapture(s, &graph);  // leave the stream usable
       if (graph) cudaGraphDestroy(graph);
@@ -457,12 +486,52 @@ int Engine::fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red, cu
     __atomic_sub_fetch(&g_launch_count, (unsigned long long)w.iter_nodes, __ATOMIC_RELAXED);
     PBG_CUDA(cudaGraphInstantiate(&w.iter_graph, graph, 0));
     cudaGraphDestroy(graph);
+    if (graph_loop_enabled()) {
+      // the same iteration as the body of a WHILE node whose condition the
+      // last kernel of the body sets on the device
+      cudaGraph_t lg = nullptr;
+      PBG_CUDA(cudaGraphCreate(&lg, 0));
+      try {
+        cudaGraphConditionalHandle h;
+        PBG_CUDA(cudaGraphConditionalHandleCreate(&h, lg, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        PBG_CUDA(cudaGraphAddNode(&node, lg, nullptr, 0, &np));
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        PBG_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        try {
+          iteration();
+          k_fcg_continue<<<1, 32, 0, s>>>(h, fs);
+        } catch (...) {
+          cudaStreamEndCapture(s, &body);
+          throw;
+        }
+        PBG_CUDA(cudaStreamEndCapture(s, &body));
+        __atomic_sub_fetch(&g_launch_count, (unsigned long long)w.iter_nodes, __ATOMIC_RELAXED);
+        PBG_CUDA(cudaGraphInstantiate(&w.loop_graph, lg, 0));
+      } catch (...) {
+        cudaGraphDestroy(lg);
+        throw;
+      }
+      cudaGraphDestroy(lg);
+    }
   }
   PBG_CUDA(cudaMemsetAsync(w.q0.p, 0, sizeof(T) * N, s));
   PBG_CUDA(cudaMemsetAsync(w.q0b.p, 0, sizeof(T) * N, s));
   k_fcg_init<T><<<g, kThreads, 0, s>>>(N, b, w.x0.p, w.r0.p, fs, tol, maxit, hist,
                                        red.slot_part(0), red.slot_count(0)); note_launch();
   PBG_CUDA(cudaGetLastError());
+  if (w.loop_graph) {
+    PBG_CUDA(cudaGraphLaunch(w.loop_graph, s));
+    PBG_CUDA(cudaMemcpyAsync(hfs, fs, sizeof(FcgScal), cudaMemcpyDeviceToHost, s));
+    PBG_CUDA(cudaStreamSynchronize(s));
+    __atomic_add_fetch(&g_launch_count, (unsigned long long)hfs->loops * (w.iter_nodes + 1), __ATOMIC_RELAXED);
+    return hfs->iter;
+  }
   int enq = 0, chunk = 4;
   for (;;) {
     PBG_CUDA(cudaMemcpyAsync(hfs, fs, sizeof(FcgScal), cudaMemcpyDeviceToHost, s));

@@ -37,7 +37,8 @@ struct KScal {
 struct FcgScal {
   double zr, zq;          // written together by k_jac_dots (z.r, z.q_old)
   double pr, pq, beta, alpha, rr, rr0, tol;
-  int iter, maxit, done, converged, status, pad;
+  int iter, maxit, done, converged, status;
+  int loops;              // iterations run by the device-side loop (bounds it)
   double *hist;           // per-iteration |r|/|r0| (kHistMax entries) or null
 };
 
@@ -63,6 +64,7 @@ struct EWork {
   DBuf<KScal> ks;                      // one per level
   DBuf<FcgScal> fs;
   cudaGraphExec_t iter_graph = nullptr;  // one captured FCG iteration
+  cudaGraphExec_t loop_graph = nullptr;  // the same iteration in a device-side while loop
   size_t iter_nodes = 0;
   void ensure(const std::vector<ELevel> &lv);
   void drop_graph();

@@ -65,6 +65,7 @@ __device__ __forceinline__ T ax_at(const EMat<T> &A, uint32_t p, Pos q, const T 
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 8) k_jac0(EMat<T> A, const T *__restrict__ r, T *__restrict__ x, T omega,
                        const int *stop) {
+  PBG_PDL_ENTRY();
   if (stop && *stop) return;
   GRID_LOOP(p, A.g.n) x[p] = omega * r[p] * A.dinv[p];
 }
@@ -72,6 +73,7 @@ __global__ void __launch_bounds__(kThreads, 8) k_jac0(EMat<T> A, const T *__rest
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 8) k_jac(EMat<T> A, const T *__restrict__ r, const T *__restrict__ xi,
                       T *__restrict__ xo, T omega, const int *stop) {
+  PBG_PDL_ENTRY();
   if (stop && *stop) return;
   GRID_LOOP(p, A.g.n) {
     Pos q = A.g.pos(p);
@@ -90,6 +92,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads, 8)
     k_jac2(EMat<T> A, const T *__restrict__ r, const T *__restrict__ b2, const T *__restrict__ q2,
            const KScal *ks, T *__restrict__ r_out, T *__restrict__ xo, T omega, const int *stop) {
+  PBG_PDL_ENTRY();
   if (stop && *stop) return;
   const T a1 = ks ? (T)ks->a1 : T(0);
   auto rv = [&](uint32_t s) -> T { return ks ? b2[s] - a1 * q2[s] : r[s]; };
@@ -165,6 +168,7 @@ __device__ __forceinline__ T restrict_cell(const EMat<T> &A, const T *r, const T
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 8) k_resid_restrict(EMat<T> A, const T *__restrict__ r, const T *__restrict__ x,
                                  Geo H, T *__restrict__ rH, const int *stop) {
+  PBG_PDL_ENTRY();
   if (stop && *stop) return;
   if (H.n >= kRestrictSerialMin) {
     GRID_LOOP(P, H.n) rH[P] = restrict_cell(A, r, x, H, P);
@@ -189,6 +193,7 @@ __global__ void __launch_bounds__(kThreads, 8)
     k_prolong_jac(EMat<T> A, const T *__restrict__ r, const T *__restrict__ xi, int Hny, int Hnz,
                   const T *__restrict__ eH, const T *__restrict__ z2H, const KScal *ksH,
                   T *__restrict__ xo, T omega, const int *stop) {
+  PBG_PDL_ENTRY();
   if (stop && *stop) return;
   const int sx = A.nx > 1 ? 1 : 0, sy = A.ny > 1 ? 1 : 0, sz = A.nz > 1 ? 1 : 0;
   const uint32_t HnYZ = (uint32_t)Hny * Hnz;
@@ -219,6 +224,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads, 8) k_jac_dots(EMat<T> A, const T *__restrict__ r, const T *__restrict__ xi,
                            T *__restrict__ z, T omega, const T *__restrict__ u, double *out2,
                            double *part, unsigned *count, const int *stop) {
+  PBG_PDL_ENTRY();
   if (stop && *stop) return;
   double v[2] = {0.0, 0.0};
   GRID_LOOP(p, A.g.n) {
@@ -246,6 +252,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads, 8) k_kc_q1(EMat<T> A, const T *__restrict__ z1, const T *__restrict__ b,
                         T *__restrict__ q1, KScal *ks, double *part, unsigned *count,
                         const int *stop) {
+  PBG_PDL_ENTRY();
   if (stop && *stop) return;
   double v[2] = {0.0, 0.0};
   GRID_LOOP(p, A.g.n) {
@@ -266,6 +273,7 @@ __global__ void __launch_bounds__(kThreads, 8) k_kc_q1(EMat<T> A, const T *__res
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 8) k_kc_r1(long long N, const T *__restrict__ b, const T *__restrict__ q1,
                         T *__restrict__ r1, const KScal *ks, const int *stop) {
+  PBG_PDL_ENTRY();
   if (stop && *stop) return;
   const T a1 = (T)ks->a1;
   GRID_LOOP(p, N) r1[p] = b[p] - a1 * q1[p];
@@ -275,6 +283,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads, 8) k_kc_q2(EMat<T> A, const T *__restrict__ z2, const T *__restrict__ q1,
                         const T *__restrict__ r1, T *__restrict__ vv, KScal *ks, double *part,
                         unsigned *count, const int *stop) {
+  PBG_PDL_ENTRY();
   if (stop && *stop) return;
   double v[3] = {0.0, 0.0, 0.0};
   GRID_LOOP(p, A.g.n) {
@@ -302,6 +311,7 @@ __global__ void __launch_bounds__(kThreads, 8) k_kc_q2(EMat<T> A, const T *__res
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 8) k_kc_x(long long N, const T *__restrict__ z1, const T *__restrict__ z2,
                        T *__restrict__ x, const KScal *ks, const int *stop) {
+  PBG_PDL_ENTRY();
   if (stop && *stop) return;
   const T c1 = (T)(ks->a1 - ks->a2 * ks->beta), c2 = (T)ks->a2;
   GRID_LOOP(p, N) x[p] = c1 * z1[p] + c2 * z2[p];
@@ -312,6 +322,7 @@ __global__ void __launch_bounds__(kThreads, 8) k_kc_x(long long N, const T *__re
 template <typename T, typename AT>
 __global__ void k_dense_solve(int n, const AT *__restrict__ Ainv, const T *__restrict__ r,
                               T *__restrict__ z, const int *stop) {
+  PBG_PDL_ENTRY();
   if (stop && *stop) return;
   const int lane = threadIdx.x & 31;
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -333,6 +344,7 @@ __global__ void k_dense_solve(int n, const AT *__restrict__ Ainv, const T *__res
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 8) k_fcg_pq(EMat<T> A, const T *__restrict__ z, T *pA, T *pB, T *__restrict__ qv,
                          FcgScal *fs, double *part, unsigned *count) {
+  PBG_PDL_ENTRY();
   if (fs->done) return;
   const int it = fs->iter;
   const T *pold = (it & 1) ? pB : pA;
@@ -363,6 +375,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads, 8) k_fcg_xr(long long N, T *__restrict__ x, T *__restrict__ r, const T *pA,
                          const T *pB, const T *__restrict__ qv, FcgScal *fs,
                          double *part, unsigned *count) {
+  PBG_PDL_ENTRY();
   if (fs->done) return;
   const int it = fs->iter;
   const T *pp = (it & 1) ? pA : pB;
@@ -394,6 +407,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads, 8) k_fcg_init(long long N, const T *__restrict__ b, T *__restrict__ x,
                            T *__restrict__ r, FcgScal *fs, double tol, int maxit, double *hist,
                            double *part, unsigned *count) {
+  PBG_PDL_ENTRY();
   double v[1] = {0.0};
   GRID_LOOP(p, N) {
     T bv = b[p];
@@ -409,6 +423,7 @@ __global__ void __launch_bounds__(kThreads, 8) k_fcg_init(long long N, const T *
     fs->tol = tol;
     fs->maxit = maxit;
     fs->iter = 0;
+    fs->loops = 0;
     fs->pq = 0.0;
     fs->pr = 0.0;
     fs->zq = 0.0;
@@ -424,6 +439,7 @@ __global__ void __launch_bounds__(kThreads, 8) k_fcg_init(long long N, const T *
 // x64 += e (T), elementwise
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 8) k_add_corr(long long N, double *__restrict__ x, const T *__restrict__ e) {
+  PBG_PDL_ENTRY();
   GRID_LOOP(p, N) x[p] += (double)e[p];
 }
 
@@ -432,6 +448,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads, 8) k_true_resid(EMat<double> A, const double *__restrict__ x, const double *__restrict__ b,
                              double *__restrict__ r, T *__restrict__ rT, double *out, double *part,
                              unsigned *count) {
+  PBG_PDL_ENTRY();
   double v[2] = {0.0, 0.0};
   GRID_LOOP(p, A.g.n) {
     Pos q = A.g.pos(p);

@@ -169,6 +169,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads, 4)
     kv_jac2(EMat<T> A, const T *__restrict__ r, const T *__restrict__ b2, const T *__restrict__ q2,
             const KScal *ks, T *__restrict__ r_out, T *__restrict__ xo, T omega, const int *stop) {
+  PBG_PDL_ENTRY();
   if (stop && *stop) return;
   constexpr int V = VecTraits<T>::V;
   const T a1 = ks ? (T)ks->a1 : T(0);
@@ -206,6 +207,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     kv_jac(EMat<T> A, const T *__restrict__ r, const T *__restrict__ xi, T *__restrict__ xo, T omega,
            const T *uA, const T *uB, const FcgScal *usel, double *out2, double *part,
            unsigned *count, const int *stop) {
+  PBG_PDL_ENTRY();
   if (stop && *stop) return;
   constexpr int V = VecTraits<T>::V;
   const T *u = (usel && (usel->iter & 1)) ? uB : uA;
@@ -246,6 +248,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     kv_prolong_jac(EMat<T> A, const T *__restrict__ r, const T *__restrict__ xi, int Hny, int Hnz,
                    const T *__restrict__ eH, const T *__restrict__ z2H, const KScal *ksH,
                    T *__restrict__ xo, T omega, const int *stop) {
+  PBG_PDL_ENTRY();
   if (stop && *stop) return;
   constexpr int V = VecTraits<T>::V;
   const int sx = A.nx > 1 ? 1 : 0, sy = A.ny > 1 ? 1 : 0;
@@ -315,6 +318,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads, 4)
     kv_fcg_pq(EMat<T> A, const T *__restrict__ z, T *pA, T *pB, T *qA, T *qB, FcgScal *fs,
               double *part, unsigned *count) {
+  PBG_PDL_ENTRY();
   if (fs->done) return;
   constexpr int V = VecTraits<T>::V;
   const int it = fs->iter;
@@ -363,6 +367,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads, 4)
     kv_fcg_xr(long long N, T *__restrict__ x, T *__restrict__ r, const T *pA, const T *pB,
               const T *qA, const T *qB, FcgScal *fs, double *part, unsigned *count) {
+  PBG_PDL_ENTRY();
   if (fs->done) return;
   constexpr int V = VecTraits<T>::V;
   const int it = fs->iter;
