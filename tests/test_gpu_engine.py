@@ -103,3 +103,32 @@ def test_refresh_equals_fresh_build(engine, oracle, precision):
     assert ita == itb
     assert np.array_equal(xa, xb)
     assert true_relres(oracle, P2, xa) <= 1e-8 * 1.0001
+
+
+def test_host_polled_loop_matches_device_loop(oracle):
+    """PBG_GRAPH_LOOP=0 replays the one-iteration graph in host-polled
+    chunks instead of the device-side WHILE loop: the same iterations and
+    the same solution bits."""
+    import json
+    import os
+    import subprocess
+    import sys
+    code = (
+        "import sys, json, hashlib, numpy as np; sys.path[:0] = %r\n"
+        "import psiboil_b200 as pb, oracle_py as O\n"
+        "P = O.Problem(1, 3, n=48, nb=4, rmin=3.0, rmax=6.0, rc=8.0)\n"
+        "s = pb.Session(*P.dims, P.h); s.assemble_pressure(P.rho, P.solid)\n"
+        "out = {}\n"
+        "for prec in (pb.FP64, pb.MIXED):\n"
+        "    x = np.zeros(P.N); E = pb.Engine(s); E.solve(x, P.b.copy(), tol=1e-9, precision=prec)\n"
+        "    out[str(prec)] = [E.last.iterations, hashlib.sha256(x.tobytes()).hexdigest()]\n"
+        "print(json.dumps(out))\n"
+    ) % ([os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+          os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle")],)
+    res = {}
+    for mode in ("0", "1"):
+        env = dict(os.environ, PBG_GRAPH_LOOP=mode)
+        r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        res[mode] = json.loads(r.stdout.strip().splitlines()[-1])
+    assert res["0"] == res["1"]
