@@ -128,9 +128,27 @@ class BatchEngine : public BatchEngineBase {
   }
 
   // ------------------------------------------------------------ problems
+  // Padded level-0 geometry of the inner solve (kBPad): (nx, ny0, nzp) with
+  // true fast extent F; otherwise the compact one.
+  static void level0_pad(int nx, int ny, int nz, int &ny0, int &F, int &nzp) {
+    (void)nx;
+    if (!kBPad<T>) { ny0 = ny; F = nz; nzp = nz; return; }
+    if (nz == 1) { ny0 = 1; F = ny; }
+    else { ny0 = ny; F = nz; }
+    nzp = (F + 3) / 4 * 4;
+  }
+
+  static size_t level_cells(const Prob &P, int l) {
+    if (l == 0 && kBPad<T>) return (size_t)P.nx * P.d.L[0].A.ny * P.d.L[0].A.nz;
+    return (size_t)P.dims[l][0] * P.dims[l][1] * P.dims[l][2];
+  }
+
   size_t layout(int nx, int ny, int nz, Prob *P) const {
     int dims[kBMaxLev][3];
     const int nlev = level_dims(nx, ny, nz, dims);
+    int ny0, F, nzp;
+    level0_pad(nx, ny, nz, ny0, F, nzp);
+    const size_t n0p = (size_t)nx * ny0 * nzp;
     if (nlev < 2) throw std::invalid_argument("batch: a problem needs more than 64 cells and at most 12 levels");
     size_t off = 0;
     // every array ends with 256 bytes of slack: the vectorised kernels' last
@@ -144,19 +162,20 @@ class BatchEngine : public BatchEngineBase {
     Off lo[kBMaxLev];
     for (int l = 0; l < nlev; ++l) {
       const size_t n = (size_t)dims[l][0] * dims[l][1] * dims[l][2];
+      const size_t nt = l == 0 ? n0p : n;  // cells of the level's T arrays
       Off &o = lo[l];
       o.c64 = take(8 * n); o.w64 = take(8 * n); o.s64 = take(8 * n); o.b64 = take(8 * n);
-      if (kMixed) { o.c = take(4 * n); o.w = take(4 * n); o.s = take(4 * n); o.b = take(4 * n); }
-      o.d = take(sizeof(T) * n);
+      if (kMixed) { o.c = take(4 * nt); o.w = take(4 * nt); o.s = take(4 * nt); o.b = take(4 * nt); }
+      o.d = take(sizeof(T) * nt);
       if (l > 0) {
         o.vb = take(sizeof(T) * n); o.vx = take(sizeof(T) * n); o.z1 = take(sizeof(T) * n);
         o.z2 = take(sizeof(T) * n); o.q1 = take(sizeof(T) * n); o.r1 = take(sizeof(T) * n);
       }
-      o.xa = take(sizeof(T) * n); o.xb = take(sizeof(T) * n);
+      o.xa = take(sizeof(T) * nt); o.xb = take(sizeof(T) * nt);
     }
     const size_t n0 = (size_t)nx * ny * nz;
-    const size_t ox0 = take(sizeof(T) * n0), or0 = take(sizeof(T) * n0), oz0 = take(sizeof(T) * n0),
-                 opA = take(sizeof(T) * n0), opB = take(sizeof(T) * n0), oq0 = take(sizeof(T) * n0);
+    const size_t ox0 = take(sizeof(T) * n0p), or0 = take(sizeof(T) * n0p), oz0 = take(sizeof(T) * n0p),
+                 opA = take(sizeof(T) * n0p), opB = take(sizeof(T) * n0p), oq0 = take(sizeof(T) * n0p);
     const size_t ox = take(8 * n0), ob = take(8 * n0), orho = take(8 * n0), osol = take(n0);
     const int nc = dims[nlev - 1][0] * dims[nlev - 1][1] * dims[nlev - 1][2];
     const size_t oai = take(8 * (size_t)nc * nc);
@@ -173,6 +192,8 @@ class BatchEngine : public BatchEngineBase {
     d.nlev = nlev;
     d.ncoarse = nc;
     d.nx = nx; d.ny = ny; d.nz = nz;
+    d.F = F; d.nzp = nzp; d.rel2d = (kBPad<T> && nz == 1) ? 1 : 0;
+    d.g0 = Geo(nx, ny, nz);
     for (int l = 0; l < nlev; ++l) {
       const Off &o = lo[l];
       BLev<T> &V = d.L[l];
@@ -180,7 +201,8 @@ class BatchEngine : public BatchEngineBase {
       const T *c, *w, *s, *b;
       if (kMixed) { c = (T *)at(o.c); w = (T *)at(o.w); s = (T *)at(o.s); b = (T *)at(o.b); }
       else { c = (T *)V.c64; w = (T *)V.w64; s = (T *)V.s64; b = (T *)V.b64; }
-      V.A = make_emat<T>(dims[l][0], dims[l][1], dims[l][2], c, w, s, b, (T *)at(o.d));
+      if (l == 0 && kBPad<T>) V.A = make_emat<T>(nx, ny0, nzp, c, w, s, b, (T *)at(o.d));
+      else V.A = make_emat<T>(dims[l][0], dims[l][1], dims[l][2], c, w, s, b, (T *)at(o.d));
       if (l > 0) {
         V.b = (T *)at(o.vb); V.x = (T *)at(o.vx); V.z1 = (T *)at(o.z1); V.z2 = (T *)at(o.z2);
         V.q1 = (T *)at(o.q1); V.r1 = (T *)at(o.r1);
@@ -208,6 +230,8 @@ class BatchEngine : public BatchEngineBase {
     const int top = nz > 1 ? 5 : 3;
     for (int f = 0; f < 6; ++f) P->bc[f] = bc ? bc[f] : (f == top ? PBG_BC_DIRICHLET : PBG_BC_NEUMANN);
     layout(nx, ny, nz, P.get());
+    // pad cells (and everything else) start at zero; kernels keep pads zero
+    PBG_CUDA(cudaMemsetAsync(P->arena.p, 0, P->bytes, stream));
     P->d.h = h;
     for (int f = 0; f < 6; ++f) P->d.bc[f] = P->bc[f];
     PBG_CUDA(cudaMemsetAsync(P->d.x, 0, 8 * (size_t)nx * ny * nz, stream));
@@ -373,7 +397,7 @@ class BatchEngine : public BatchEngineBase {
         if (slot_pid_[s] < 0) continue;
         const Prob &P = get(slot_pid_[s]);
         if (P.nlev <= l) continue;
-        const uint32_t n = (uint32_t)((size_t)P.dims[l][0] * P.dims[l][1] * P.dims[l][2]);
+        const uint32_t n = (uint32_t)level_cells(P, l);
         tbeg[(size_t)l * S_ + s] = (int)tiles.size();
         int k = 0;
         for (uint32_t p0 = 0; p0 < n; p0 += tc, ++k) tiles.push_back({s, p0, std::min(tc, n - p0)});

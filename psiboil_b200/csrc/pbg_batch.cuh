@@ -36,6 +36,7 @@
 #include "pbg_assemble.cuh"
 #include "pbg_engine.cuh"
 #include "pbg_engine_kernels.cuh"
+#include "pbg_vec.cuh"
 
 namespace pbg {
 
@@ -53,12 +54,24 @@ struct BLev {
   T *b, *x, *z1, *z2, *q1, *r1, *xa, *xb;
 };
 
+// Level 0 of a mixed-precision (FP32) batch keeps its inner-solve arrays in
+// padded rows: the fast axis (k in 3-D; j in 2-D, whose rows are relabelled
+// (nx, 1, ny)) is rounded up to a multiple of 4 cells, so that every group
+// of four cells is one 16-byte vector and the row neighbours are aligned
+// vectors too. Pad cells hold zero coefficients, zero inverse diagonal and
+// zero vectors, and every kernel leaves them zero; the FP64 arrays of level
+// 0 (matrix, solution, right-hand side, fields) stay compact.
+template <typename T>
+constexpr bool kBPad = sizeof(T) == 4;
+
 // Device descriptor of the problem in a slot (written by the host).
 template <typename T>
 struct BProb {
   int nlev, ncoarse;
   int tail;                 // first level run by the CTA-local tail (kBMaxLev: none)
   int nx, ny, nz;
+  int F, nzp, rel2d;        // padded level 0: fast-axis extent, padded extent, 2-D relabelled
+  Geo g0;                   // compact level-0 geometry (the FP64 arrays)
   int bc[6];
   double h;
   const double *rho;        // assembly inputs (device) or null: level-0 FP64 matrix given
@@ -105,6 +118,31 @@ struct BCtx {
 
 // Is slot s running its inner solve (this launch's work applies)?
 __device__ __forceinline__ bool b_running(const BState &S) { return S.phase == BP_RUN && !S.f.done; }
+
+// Padded level-0 index -> compact index of the FP64 arrays; false for a pad
+// cell. Without padding the index is the same.
+template <typename T>
+__device__ __forceinline__ bool b_compact(const BProb<T> &P, uint32_t pp, uint32_t &p) {
+  if constexpr (!kBPad<T>) {
+    p = pp;
+    return true;
+  } else {
+    const uint32_t row = P.L[0].A.g.dnz.div(pp), k = pp - row * (uint32_t)P.nzp;
+    if (k >= (uint32_t)P.F) return false;
+    p = row * (uint32_t)P.F + k;
+    return true;
+  }
+}
+
+// Kernels with a padded level-0 path: at most 64 registers, so that 512-thread
+// CTAs keep two per SM (the vector path would otherwise take up to 90).
+#define BPAD_BOUNDS __launch_bounds__(kBThreadsMax, 2)
+
+// Groups of four cells of a padded level-0 tile (tiles start at multiples of
+// four and hold a multiple of four cells).
+#define BGROUP_LOOP(T_, p)                                                          \
+  for (uint32_t g_ = threadIdx.x, p = (T_).p0 + 4u * threadIdx.x; g_ < (T_).n / 4u; \
+       g_ += blockDim.x, p = (T_).p0 + 4u * g_)
 
 // Block sum of v[0..K-1] in a fixed order (warp shuffles, then warps in
 // index order); the result is valid on thread 0. Ends with the CTA
@@ -178,9 +216,11 @@ __global__ void kb_assemble(BCtx<T> C) {
     const BProb<T> &P = C.prob[tl.slot];
     if (!P.rho) continue;
     const BLev<T> &V = P.L[0];
-    BCELL_LOOP(tl, p) {
+    BCELL_LOOP(tl, pp) {
+      uint32_t p;
+      if (!b_compact(P, pp, p)) continue;
       double c, w, s, b;
-      const Pos q = V.A.g.pos(p);
+      const Pos q = P.g0.pos(p);
       assemble_cell(P.nx, P.ny, P.nz, P.h, P.bc, P.rho, P.solid, (long long)p, q, c, w, s, b);
       V.c64[p] = c; V.w64[p] = w; V.s64[p] = s; V.b64[p] = b;
     }
@@ -196,15 +236,17 @@ __global__ void kb_galerkin(BCtx<T> C, int l) {
     if (!C.st[tl.slot].setup) continue;
     const BProb<T> &P = C.prob[tl.slot];
     const BLev<T> &F = P.L[l - 1], &V = P.L[l];
-    const int fx = F.A.nx > 1 ? 2 : 1, fy = F.A.ny > 1 ? 2 : 1, fz = F.A.nz > 1 ? 2 : 1;
+    // the fine FP64 arrays: level 0's are compact even when its T arrays are padded
+    const Geo Fg = l == 1 ? P.g0 : F.A.g;
+    const int fx = Fg.nx > 1 ? 2 : 1, fy = Fg.ny > 1 ? 2 : 1, fz = Fg.nz > 1 ? 2 : 1;
     BCELL_LOOP(tl, P_) {
       Pos Q = V.A.g.pos(P_);
       double c = 0.0, w = 0.0, s = 0.0, b = 0.0;
       const int i0 = Q.i * fx, j0 = Q.j * fy, k0 = Q.k * fz;
-      for (int a = 0; a < fx && i0 + a < F.A.nx; ++a)
-        for (int bb = 0; bb < fy && j0 + bb < F.A.ny; ++bb)
-          for (int cc = 0; cc < fz && k0 + cc < F.A.nz; ++cc) {
-            const uint32_t p = ((uint32_t)(i0 + a) * F.A.ny + (j0 + bb)) * F.A.nz + (k0 + cc);
+      for (int a = 0; a < fx && i0 + a < Fg.nx; ++a)
+        for (int bb = 0; bb < fy && j0 + bb < Fg.ny; ++bb)
+          for (int cc = 0; cc < fz && k0 + cc < Fg.nz; ++cc) {
+            const uint32_t p = ((uint32_t)(i0 + a) * Fg.ny + (j0 + bb)) * Fg.nz + (k0 + cc);
             c += F.c64[p];
             if (a == 0) w += F.w64[p]; else c -= 2.0 * F.w64[p];
             if (bb == 0) s += F.s64[p]; else c -= 2.0 * F.s64[p];
@@ -220,6 +262,39 @@ __global__ void kb_galerkin(BCtx<T> C, int l) {
 // arrays).
 template <typename T>
 __global__ void kb_finish(BCtx<T> C, int l) {
+  if constexpr (kBPad<T>) {
+    if (l == 0) {
+      // padded level 0: compact FP64 in, padded T out (2-D: the j coupling
+      // goes to the fast axis, b); pad cells keep their zeros
+      BTILE_LOOP(C, 0, t) {
+        const BTile tl = C.tiles[t];
+        if (!C.st[tl.slot].setup) continue;
+        const BProb<T> &P = C.prob[tl.slot];
+        const BLev<T> &V = P.L[0];
+        const Geo &G = P.g0;
+        const uint32_t SI = G.nynz, SJ = (uint32_t)G.nz;
+        BCELL_LOOP(tl, pp) {
+          uint32_t p;
+          if (!b_compact(P, pp, p)) continue;
+          const double c = V.c64[p];
+          const Pos q = G.pos(p);
+          double sum = 0.0;
+          if (q.i > 0) sum += V.w64[p];
+          if (q.i < G.nx - 1) sum += V.w64[p + SI];
+          if (q.j > 0) sum += V.s64[p];
+          if (q.j < G.ny - 1) sum += V.s64[p + SJ];
+          if (q.k > 0) sum += V.b64[p];
+          if (q.k < G.nz - 1) sum += V.b64[p + 1];
+          const_cast<T *>(V.A.dinv)[pp] = (T)(1.0 / c);
+          const_cast<T *>(V.A.c)[pp] = (T)(c - sum);
+          const_cast<T *>(V.A.w)[pp] = (T)V.w64[p];
+          const_cast<T *>(V.A.s)[pp] = P.rel2d ? T(0) : (T)V.s64[p];
+          const_cast<T *>(V.A.b)[pp] = P.rel2d ? (T)V.s64[p] : (T)V.b64[p];
+        }
+      }
+      return;
+    }
+  }
   BTILE_LOOP(C, l, t) {
     const BTile tl = C.tiles[t];
     if (!C.st[tl.slot].setup) continue;
@@ -313,7 +388,10 @@ __global__ void kb_outer_corr(BCtx<T> C) {
     const BState &S = C.st[tl.slot];
     if (!(S.phase == BP_RUN && S.f.done)) continue;
     const BProb<T> &P = C.prob[tl.slot];
-    BCELL_LOOP(tl, p) P.x[p] += (double)P.x0[p];
+    BCELL_LOOP(tl, pp) {
+      uint32_t p;
+      if (b_compact(P, pp, p)) P.x[p] += (double)P.x0[pp];
+    }
   }
 }
 
@@ -328,26 +406,28 @@ __global__ void kb_outer_resid(BCtx<T> C) {
     BState &S = C.st[tl.slot];
     if (!(S.phase == BP_INIT || (S.phase == BP_RUN && S.f.done))) continue;
     const BProb<T> &P = C.prob[tl.slot];
-    const EMat<T> &A = P.L[0].A;
+    const Geo &G = P.g0;
     const BLev<T> &V = P.L[0];
     double v[3] = {0.0, 0.0, 0.0};
-    BCELL_LOOP(tl, p) {
-      Pos q = A.g.pos(p);
-      const uint32_t SI = A.g.nynz, SJ = (uint32_t)A.nz;
+    BCELL_LOOP(tl, pp) {
+      uint32_t p;
+      if (!b_compact(P, pp, p)) continue;
+      Pos q = G.pos(p);
+      const uint32_t SI = G.nynz, SJ = (uint32_t)G.nz;
       const double *x = P.x;
       double on = 0.0;
       if (q.i > 0) on += V.w64[p] * x[p - SI];
-      if (q.i < A.nx - 1) on += V.w64[p + SI] * x[p + SI];
+      if (q.i < G.nx - 1) on += V.w64[p + SI] * x[p + SI];
       if (q.j > 0) on += V.s64[p] * x[p - SJ];
-      if (q.j < A.ny - 1) on += V.s64[p + SJ] * x[p + SJ];
+      if (q.j < G.ny - 1) on += V.s64[p + SJ] * x[p + SJ];
       if (q.k > 0) on += V.b64[p] * x[p - 1];
-      if (q.k < A.nz - 1) on += V.b64[p + 1] * x[p + 1];
+      if (q.k < G.nz - 1) on += V.b64[p + 1] * x[p + 1];
       const double bp = P.b[p];
       const double r = bp - (V.c64[p] * x[p] - on);
       const T rt = (T)r;
-      P.r0[p] = rt;
-      P.x0[p] = T(0);
-      P.q0[p] = T(0);
+      P.r0[pp] = rt;
+      P.x0[pp] = T(0);
+      P.q0[pp] = T(0);
       v[0] += r * r;
       v[1] += bp * bp;
       v[2] += (double)rt * (double)rt;
@@ -533,9 +613,124 @@ __device__ __forceinline__ void b_coarse(const BProb<T> &P, const BState &S, int
   }
 }
 
+// ---------------------------------------------------------------- padded level 0: groups of four
+// The level-0 phases on a padded tile, four cells per thread with 16-byte
+// loads (the helpers of the single-problem vector kernels; the same
+// formulas as the cell functions above).
+
+// two damped-Jacobi sweeps from zero into xb (level 0 has no K-cycle rhs)
+template <typename T>
+__device__ __forceinline__ void vgroup_jac2(const BLev<T> &V, const T *r, T om, uint32_t p) {
+  constexpr int W = VecTraits<T>::V;
+  const EMat<T> &A = V.A;
+  const Pos q = A.g.pos(p);
+  const CoefV<T> Cf = load_coef(A, p, q);
+  const Vec<T> d = ldv(A.dinv, p), rp = ldv(r, p);
+  const HoodV<T> X = load_hood(A, p, q, FJac0<T>{r, A.dinv, om});
+  Vec<T> o;
+#pragma unroll
+  for (int m = 0; m < W; ++m) {
+    const T xp = X.c.v[m];
+    o.v[m] = xp + om * ((rp.v[m] + offd(Cf, X, m)) * d.v[m] - xp);
+  }
+  stv(V.xb, p, o);
+}
+
+// coarse cell Pc of level 1 = sum over its fine children of (r - A xb),
+// the children read from the padded level 0 (2-D: the coarse j is the fine
+// fast axis); the same (a, b, c) order as restrict_cell
+template <typename T>
+__device__ __forceinline__ T restrict_cell_pad(const BProb<T> &P, const EMat<T> &A, const T *r, const T *x,
+                                               const Geo &H, uint32_t Pc) {
+  const Pos Q = H.pos(Pc);
+  const int fx = A.nx > 1 ? 2 : 1, fy = A.ny > 1 ? 2 : 1, fz = P.F > 1 ? 2 : 1;
+  const int qj = P.rel2d ? 0 : Q.j, qk = P.rel2d ? Q.j : Q.k;
+  T sum = 0;
+  for (int a = 0; a < fx; ++a) {
+    const int i = Q.i * fx + a;
+    if (i >= A.nx) break;
+    for (int bb = 0; bb < fy; ++bb) {
+      const int j = qj * fy + bb;
+      if (j >= A.ny) break;
+      for (int cc = 0; cc < fz; ++cc) {
+        const int k = qk * fz + cc;
+        if (k >= P.F) break;
+        const uint32_t p = ((uint32_t)i * A.ny + j) * A.nz + k;
+        sum += r[p] - ax_at(A, p, Pos{i, j, k}, x);
+      }
+    }
+  }
+  return sum;
+}
+
+// xa = xb + P e, then one sweep; pad lanes (k >= F) take no correction
+template <typename T>
+__device__ __forceinline__ void vgroup_prolong_jac(const BProb<T> &P, const BLev<T> &V, const BLev<T> &Hl,
+                                                   const T *r, const T *eH, bool two, T c1, T c2, T om,
+                                                   uint32_t p) {
+  constexpr int W = VecTraits<T>::V;
+  const EMat<T> &A = V.A;
+  const Geo &H = Hl.A.g;
+  const T *z2H = Hl.z2;
+  const int sx = A.nx > 1 ? 1 : 0, sy = A.ny > 1 ? 1 : 0, sz = P.F > 1 ? 1 : 0;
+  const int F = P.F;
+  auto e = [&](int i, int j, int k) -> T {
+    if (k >= F) return T(0);
+    const uint32_t Pc = (uint32_t)(i >> sx) * H.nynz + (uint32_t)(j >> sy) * (uint32_t)H.nz + (uint32_t)(k >> sz);
+    return two ? c1 * eH[Pc] + c2 * z2H[Pc] : eH[Pc];
+  };
+  const T *xi = V.xb;
+  const Pos q = A.g.pos(p);
+  auto rowv = [&](uint32_t pr, int i, int j) -> Vec<T> {
+    Vec<T> x = ldv(xi, pr);
+#pragma unroll
+    for (int m = 0; m < W; ++m) x.v[m] += e(i, j, q.k + m);
+    return x;
+  };
+  const uint32_t SI = A.g.nynz, SJ = (uint32_t)A.nz;
+  HoodV<T> X;
+  X.c = rowv(p, q.i, q.j);
+  X.w = q.i > 0 ? rowv(p - SI, q.i - 1, q.j) : zerov<T>();
+  X.e = q.i < A.nx - 1 ? rowv(p + SI, q.i + 1, q.j) : zerov<T>();
+  X.s = q.j > 0 ? rowv(p - SJ, q.i, q.j - 1) : zerov<T>();
+  X.n = q.j < A.ny - 1 ? rowv(p + SJ, q.i, q.j + 1) : zerov<T>();
+  X.km = q.k > 0 ? xi[p - 1] + e(q.i, q.j, q.k - 1) : T(0);
+  X.kp = q.k + W < A.nz ? xi[p + W] + e(q.i, q.j, q.k + W) : T(0);
+  const CoefV<T> Cf = load_coef(A, p, q);
+  const Vec<T> d = ldv(A.dinv, p), rp = ldv(r, p);
+  Vec<T> o;
+#pragma unroll
+  for (int m = 0; m < W; ++m) {
+    const T xp = X.c.v[m];
+    o.v[m] = xp + om * ((rp.v[m] + offd(Cf, X, m)) * d.v[m] - xp);
+  }
+  stv(V.xa, p, o);
+}
+
+// z = xa + w D^-1 (r - A xa); v += (z.r, z.q0)
+template <typename T>
+__device__ __forceinline__ void vgroup_jac(const BProb<T> &P, const BLev<T> &V, const T *r, T om, uint32_t p,
+                                           double (&v)[2]) {
+  constexpr int W = VecTraits<T>::V;
+  const EMat<T> &A = V.A;
+  const Pos q = A.g.pos(p);
+  const CoefV<T> Cf = load_coef(A, p, q);
+  const Vec<T> d = ldv(A.dinv, p), rp = ldv(r, p), qo = ldv(P.q0, p);
+  const HoodV<T> X = load_hood(A, p, q, FArr<T>{V.xa});
+  Vec<T> o;
+#pragma unroll
+  for (int m = 0; m < W; ++m) {
+    const T xp = X.c.v[m];
+    o.v[m] = xp + om * ((rp.v[m] + offd(Cf, X, m)) * d.v[m] - xp);
+    v[0] += (double)o.v[m] * (double)rp.v[m];
+    v[1] += (double)o.v[m] * (double)qo.v[m];
+  }
+  stv(P.z0, p, o);
+}
+
 // ---------------------------------------------------------------- K-cycle: tile kernels
 template <typename T>
-__global__ void kb_jac2(BCtx<T> C, int l, int kc) {
+__global__ void BPAD_BOUNDS kb_jac2(BCtx<T> C, int l, int kc) {
   BTILE_LOOP(C, l, t) {
     const BTile tl = C.tiles[t];
     const BState &S = C.st[tl.slot];
@@ -543,6 +738,10 @@ __global__ void kb_jac2(BCtx<T> C, int l, int kc) {
     if (!b_tile_level(S, P, l)) continue;
     const T a1 = kc ? (T)S.ks[l].a1 : T(0);
     const T *r = l == 0 ? P.r0 : P.L[l].b;
+    if (kBPad<T> && l == 0) {
+      BGROUP_LOOP(tl, p) vgroup_jac2(P.L[0], r, C.omega, p);
+      continue;
+    }
     BCELL_LOOP(tl, p) cell_jac2(P.L[l], r, p, a1, kc != 0, C.omega);
   }
 }
@@ -559,6 +758,10 @@ __global__ void kb_restrict(BCtx<T> C, int l, int kc) {
     if (!b_tile_level(S, P, l)) continue;
     const T *r = b_rhs(P, l, kc != 0);
     const BLev<T> &V = P.L[l], &H = P.L[l + 1];
+    if (kBPad<T> && l == 0) {
+      BCELL_LOOP(tl, Pc) H.b[Pc] = restrict_cell_pad(P, V.A, r, V.xb, H.A.g, Pc);
+      continue;
+    }
     BCELL_LOOP(tl, Pc) H.b[Pc] = restrict_cell(V.A, r, V.xb, H.A.g, Pc);
   }
 }
@@ -578,7 +781,7 @@ __global__ void kb_dense(BCtx<T> C, int L) {
 }
 
 template <typename T>
-__global__ void kb_prolong_jac(BCtx<T> C, int l, int kc) {
+__global__ void BPAD_BOUNDS kb_prolong_jac(BCtx<T> C, int l, int kc) {
   BTILE_LOOP(C, l, t) {
     const BTile tl = C.tiles[t];
     const BState &S = C.st[tl.slot];
@@ -589,6 +792,10 @@ __global__ void kb_prolong_jac(BCtx<T> C, int l, int kc) {
     T c1, c2;
     b_coarse(P, S, l, C.kc_max, eH, two, c1, c2);
     const T *r = b_rhs(P, l, kc != 0);
+    if (kBPad<T> && l == 0) {
+      BGROUP_LOOP(tl, p) vgroup_prolong_jac(P, P.L[0], P.L[1], r, eH, two, c1, c2, C.omega, p);
+      continue;
+    }
     BCELL_LOOP(tl, p) cell_prolong_jac(P.L[l], P.L[l + 1], r, eH, two, c1, c2, C.omega, p);
   }
 }
@@ -596,7 +803,7 @@ __global__ void kb_prolong_jac(BCtx<T> C, int l, int kc) {
 // Last sweep; level 0 writes z0 and reduces z.r0 and z.q0 (q of the
 // previous FCG iteration) into the slot's FCG scalars.
 template <typename T>
-__global__ void kb_jac(BCtx<T> C, int l, int kc) {
+__global__ void BPAD_BOUNDS kb_jac(BCtx<T> C, int l, int kc) {
   BTILE_LOOP(C, l, t) {
     const BTile tl = C.tiles[t];
     BState &S = C.st[tl.slot];
@@ -606,6 +813,12 @@ __global__ void kb_jac(BCtx<T> C, int l, int kc) {
     const T *r = b_rhs(P, l, kc != 0);
     T *z = l == 0 ? P.z0 : (kc ? V.z2 : V.z1);
     double v[2] = {0.0, 0.0};
+    if (kBPad<T> && l == 0) {
+      BGROUP_LOOP(tl, p) vgroup_jac(P, V, r, C.omega, p, v);
+      double o[2];
+      if (b_reduce<2>(C, 0, t, tl.slot, v, o)) { S.f.zr = o[0]; S.f.zq = o[1]; }
+      continue;
+    }
     BCELL_LOOP(tl, p) {
       const T zz = cell_jac(V, r, z, C.omega, p);
       if (l == 0) {
@@ -766,7 +979,7 @@ __global__ void __launch_bounds__(kBThreadsMax) kb_tail(BCtx<T> C, int l) {
 // ---------------------------------------------------------------- outer FCG (level 0)
 // p = z - beta p_old, q = A p, alpha = p.r / p.q (k_fcg_pq)
 template <typename T>
-__global__ void kb_fcg_pq(BCtx<T> C) {
+__global__ void BPAD_BOUNDS kb_fcg_pq(BCtx<T> C) {
   BTILE_LOOP(C, 0, t) {
     const BTile tl = C.tiles[t];
     BState &S = C.st[tl.slot];
@@ -782,13 +995,41 @@ __global__ void kb_fcg_pq(BCtx<T> C) {
     const T *z = P.z0;
     auto pv = [&](uint32_t s) -> T { return it == 0 ? z[s] : z[s] - beta * pold[s]; };
     double v[1] = {0.0};
-    BCELL_LOOP(tl, p) {
-      Pos q = A.g.pos(p);
-      const T pp = pv(p);
-      const T qq = ax_f(A, p, q, pv);
-      pnew[p] = pp;
-      P.q0[p] = qq;
-      v[0] += (double)pp * (double)qq;
+    if constexpr (kBPad<T>) {
+      // q = A z - beta q_old (= A p, with q_old = A p_old kept in q0), so
+      // only z is read around the group (as kv_fcg_pq)
+      constexpr int W = VecTraits<T>::V;
+      BGROUP_LOOP(tl, p) {
+        const Pos q = A.g.pos(p);
+        const CoefV<T> Cf = load_coef(A, p, q);
+        const Vec<T> c = ldv(A.c, p);
+        const HoodV<T> Z = load_hood(A, p, q, FArr<T>{z});
+        Vec<T> pv, qv;
+        if (it == 0) {
+#pragma unroll
+          for (int m = 0; m < W; ++m) { pv.v[m] = Z.c.v[m]; qv.v[m] = axv(c.v[m], Cf, Z, m); }
+        } else {
+          const Vec<T> po = ldv(pold, p), qo = ldv(P.q0, p);
+#pragma unroll
+          for (int m = 0; m < W; ++m) {
+            pv.v[m] = Z.c.v[m] - beta * po.v[m];
+            qv.v[m] = axv(c.v[m], Cf, Z, m) - beta * qo.v[m];
+          }
+        }
+#pragma unroll
+        for (int m = 0; m < W; ++m) v[0] += (double)pv.v[m] * (double)qv.v[m];
+        stv(pnew, p, pv);
+        stv(P.q0, p, qv);
+      }
+    } else {
+      BCELL_LOOP(tl, p) {
+        Pos q = A.g.pos(p);
+        const T pp = pv(p);
+        const T qq = ax_f(A, p, q, pv);
+        pnew[p] = pp;
+        P.q0[p] = qq;
+        v[0] += (double)pp * (double)qq;
+      }
     }
     double o[1];
     if (b_reduce<1>(C, 0, t, tl.slot, v, o)) {
@@ -803,7 +1044,7 @@ __global__ void kb_fcg_pq(BCtx<T> C) {
 
 // x += alpha p, r -= alpha q; inner convergence (k_fcg_xr)
 template <typename T>
-__global__ void kb_fcg_xr(BCtx<T> C) {
+__global__ void BPAD_BOUNDS kb_fcg_xr(BCtx<T> C) {
   BTILE_LOOP(C, 0, t) {
     const BTile tl = C.tiles[t];
     BState &S = C.st[tl.slot];
@@ -814,13 +1055,30 @@ __global__ void kb_fcg_xr(BCtx<T> C) {
     const T *pp = (it & 1) ? P.pA : P.pB;
     const T alpha = (T)f.alpha;
     double v[2] = {0.0, 0.0};
-    BCELL_LOOP(tl, p) {
-      const T pv = pp[p];
-      P.x0[p] += alpha * pv;
-      const T rv = P.r0[p] - alpha * P.q0[p];
-      P.r0[p] = rv;
-      v[0] += (double)rv * (double)rv;
-      v[1] += (double)pv * (double)rv;
+    if constexpr (kBPad<T>) {
+      constexpr int W = VecTraits<T>::V;
+      BGROUP_LOOP(tl, p) {
+        const Vec<T> pv = ldv(pp, p), qv = ldv(P.q0, p);
+        Vec<T> xv = ldv(P.x0, p), rv = ldv(P.r0, p);
+#pragma unroll
+        for (int m = 0; m < W; ++m) {
+          xv.v[m] += alpha * pv.v[m];
+          rv.v[m] = rv.v[m] - alpha * qv.v[m];
+          v[0] += (double)rv.v[m] * (double)rv.v[m];
+          v[1] += (double)pv.v[m] * (double)rv.v[m];
+        }
+        stv(P.x0, p, xv);
+        stv(P.r0, p, rv);
+      }
+    } else {
+      BCELL_LOOP(tl, p) {
+        const T pv = pp[p];
+        P.x0[p] += alpha * pv;
+        const T rv = P.r0[p] - alpha * P.q0[p];
+        P.r0[p] = rv;
+        v[0] += (double)rv * (double)rv;
+        v[1] += (double)pv * (double)rv;
+      }
     }
     double o[2];
     if (b_reduce<2>(C, 0, t, tl.slot, v, o)) {
