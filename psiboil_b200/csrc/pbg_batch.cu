@@ -82,7 +82,10 @@ class BatchEngine : public BatchEngineBase {
     cudaGraphExec_t exec = nullptr;
     size_t nodes = 0;
   };
-  std::map<unsigned long long, Graph> graphs_;
+  // graphs by (launch-sequence signature, per-level grid code)
+  std::map<std::pair<unsigned long long, unsigned long long>, Graph> graphs_;
+  int lgrid_[kBMaxLev] = {};     // tile-kernel grid per level: min(grid, tiles rounded up to 2^k)
+  unsigned long long gcode_ = 0; // the lgrid_ values, 5 bits of log2 each
   unsigned long long launches_ = 0;
 
  public:
@@ -405,6 +408,17 @@ class BatchEngine : public BatchEngineBase {
       }
     }
     lbeg[kBMaxLev] = (int)tiles.size();
+    // small levels launch only as many CTAs as they have tiles (rounded up
+    // to a power of two so that the graphs stay few); the grid-stride tile
+    // loops are correct for any grid
+    gcode_ = 0;
+    for (int l = 0; l < kBMaxLev; ++l) {
+      const int nt = std::max(1, lbeg[l + 1] - lbeg[l]);
+      int g = 1, lg = 0;
+      while (g < nt && g < shape_.grid) { g <<= 1; ++lg; }
+      lgrid_[l] = std::min(g, shape_.grid);
+      gcode_ |= (unsigned long long)lg << (5 * l);
+    }
     const size_t nt = std::max<size_t>(tiles.size(), 1);
     if (nt > tile_cap_) {
       PBG_CUDA(cudaStreamSynchronize(stream));
@@ -471,11 +485,11 @@ class BatchEngine : public BatchEngineBase {
   // the tile K-cycle of level l+1 where some slot needs them; counts the
   // launches.
   void seq_precond(const BCtx<T> &C, int l, int kc, size_t &n) {
-    const int G = shape_.grid, NT = shape_.threads;
+    const int G = lgrid_[l], GH = lgrid_[l + 1 < kBMaxLev ? l + 1 : l], NT = shape_.threads;
     const int dtile = (int)(sig_ & 0xff);
     const unsigned dense_mask = (unsigned)((sig_ >> 8) & 0xffff), tail_mask = (unsigned)((sig_ >> 24) & 0xffff);
     kb_jac2<T><<<G, NT, 0, stream>>>(C, l, kc); ++n;
-    kb_restrict<T><<<G, NT, 0, stream>>>(C, l, kc); ++n;
+    kb_restrict<T><<<GH, NT, 0, stream>>>(C, l, kc); ++n;
     if (dense_mask & (1u << (l + 1))) { kb_dense<T><<<slot_grid(), NT, 0, stream>>>(C, l + 1); ++n; }
     if (tail_mask & (1u << (l + 1))) { kb_tail<T><<<slot_grid(), NT, 0, stream>>>(C, l + 1); ++n; }
     if (l + 1 < dtile) seq_kcycle(C, l + 1, n);
@@ -484,7 +498,7 @@ class BatchEngine : public BatchEngineBase {
   }
 
   void seq_kcycle(const BCtx<T> &C, int l, size_t &n) {
-    const int G = shape_.grid, NT = shape_.threads;
+    const int G = lgrid_[l], NT = shape_.threads;
     seq_precond(C, l, 0, n);
     if (l <= shape_.kc_max) {
       kb_kc_q1<T><<<G, NT, 0, stream>>>(C, l); ++n;
@@ -493,11 +507,12 @@ class BatchEngine : public BatchEngineBase {
     }
   }
 
-  Graph &graph(unsigned long long key) {
+  Graph &graph(unsigned long long sig) {
+    const std::pair<unsigned long long, unsigned long long> key(sig, gcode_);
     auto it = graphs_.find(key);
     if (it != graphs_.end()) return it->second;
     const BCtx<T> C = ctx();
-    const int G = shape_.grid, NT = shape_.threads;
+    const int G = lgrid_[0], NT = shape_.threads;
     cudaGraph_t g = nullptr;
     size_t n = 0;
     PBG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
