@@ -338,7 +338,7 @@ int pbg_batch_autotune(pbg_batch *b, const int *ids, int n, const pbg_params *p,
       if (s < best_s) { best_s = s; bc = c; }
     };
     for (int th : {128, 256, 512})
-      for (int mult : {2, 4, 8}) {
+      for (int mult : {2, 4, 8, 16, 32}) {
         pbg_batch_config c = bc;
         c.threads = th;
         c.tile_cells = th * mult;
