@@ -115,6 +115,10 @@ typedef struct {
    * factor reads the lower couplings w, s, b, as the reference's does, also
    * for a non-symmetric matrix. */
   int prec;
+  /* 1: start from x = 0 whatever x holds (x is then output only, and with
+   * PBG_HOST it is not copied to the device); 0: x is the initial guess,
+   * as in the reference's Linear::solve. */
+  int x0_zero;
 } pbg_params;
 
 typedef struct {

@@ -57,7 +57,7 @@ class Params(ctypes.Structure):
                 ("mv", ctypes.c_int * 3), ("ms", ctypes.c_int * 3),
                 ("tol", ctypes.c_double), ("inner_tol", ctypes.c_double),
                 ("max_sweeps", ctypes.c_int), ("exact_sums", ctypes.c_int),
-                ("coarse_max", ctypes.c_int), ("prec", ctypes.c_int)]
+                ("coarse_max", ctypes.c_int), ("prec", ctypes.c_int), ("x0_zero", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):
@@ -553,10 +553,12 @@ class Engine:
         self.last = None
 
     def solve(self, x, b, tol=1.0e-8, precision=FP64, inner_tol=1.0e-4, max_iter=500,
-              max_sweeps=8, coarse_max=0):
+              max_sweeps=8, coarse_max=0, x0_zero=False):
+        """x0_zero: start from zero (x is output only and is not uploaded)."""
         p = default_params(SOLVER_ENGINE)
         p.precision, p.tol, p.inner_tol = precision, tol, inner_tol
         p.max_iter, p.max_sweeps, p.coarse_max = max_iter, max_sweeps, coarse_max
+        p.x0_zero = 1 if x0_zero else 0
         self.last = self.session.solve(x, b, p)
         return bool(self.last.converged)
 

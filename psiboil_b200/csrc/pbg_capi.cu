@@ -792,22 +792,28 @@ int pbg_solve_strided(pbg_session *s, double *x, const double *b, long long si, 
     const long long N = s->ncell();
     const bool compact = (si == (long long)s->ny * s->nz && sj == s->nz && sk == 1 && offset == 0);
     int rc;
+    const bool zero = p->x0_zero != 0;
     if (where == PBG_DEVICE && compact) {
+      if (zero) PBG_CUDA(cudaMemsetAsync(x, 0, N * 8, s->stream));
       rc = solve_device(s, x, b, p, r);
     } else {
       ensure_staging(s);
+      if (zero) PBG_CUDA(cudaMemsetAsync(s->dx.p, 0, N * 8, s->stream));
       if (where == PBG_HOST) {
         if (compact) {
-          h2d(s, s->dx.p, x, N * 8, s->px);
+          if (!zero) h2d(s, s->dx.p, x, N * 8, s->px);
           h2d(s, s->db.p, b, N * 8, s->pb);
         } else {
-          gather(x, s->px, s->nx, s->ny, s->nz, si, sj, sk, offset);
+          if (!zero) gather(x, s->px, s->nx, s->ny, s->nz, si, sj, sk, offset);
           gather(b, s->pb, s->nx, s->ny, s->nz, si, sj, sk, offset);
-          PBG_CUDA(cudaMemcpyAsync(s->dx.p, s->px, N * 8, cudaMemcpyHostToDevice, s->stream));
+          if (!zero) PBG_CUDA(cudaMemcpyAsync(s->dx.p, s->px, N * 8, cudaMemcpyHostToDevice, s->stream));
           PBG_CUDA(cudaMemcpyAsync(s->db.p, s->pb, N * 8, cudaMemcpyHostToDevice, s->stream));
         }
       } else {
-        k_gather<<<grid_for(N), kThreads, 0, s->stream>>>(x, s->dx.p, s->nx, s->ny, s->nz, si, sj, sk, offset); note_launch();
+        if (!zero) {
+          k_gather<<<grid_for(N), kThreads, 0, s->stream>>>(x, s->dx.p, s->nx, s->ny, s->nz, si, sj, sk, offset);
+          note_launch();
+        }
         k_gather<<<grid_for(N), kThreads, 0, s->stream>>>(b, s->db.p, s->nx, s->ny, s->nz, si, sj, sk, offset); note_launch();
       }
       rc = solve_device(s, s->dx.p, s->db.p, p, r);

@@ -132,3 +132,22 @@ def test_host_polled_loop_matches_device_loop(oracle):
         assert r.returncode == 0, r.stderr[-2000:]
         res[mode] = json.loads(r.stdout.strip().splitlines()[-1])
     assert res["0"] == res["1"]
+
+
+def test_x0_zero_option(engine, oracle):
+    """x0_zero ignores what x holds (it is not uploaded) and gives the bits of
+    a solve from an explicit zero guess, for host and device buffers."""
+    import torch
+    P = oracle.Problem(1, 3, n=32, nb=3, rmin=2.0, rmax=4.0, rc=5.0)
+    with engine.Session(*P.dims, P.h) as s:
+        s.assemble_pressure(P.rho, P.solid)
+        E = engine.Engine(s)
+        ref = np.zeros(P.N)
+        E.solve(ref, P.b.copy(), tol=1e-9, precision=engine.MIXED)
+        x = np.full(P.N, 7.0)
+        E.solve(x, P.b.copy(), tol=1e-9, precision=engine.MIXED, x0_zero=True)
+        assert np.array_equal(x, ref)
+        xd = torch.full((P.N,), -3.0, dtype=torch.float64, device="cuda")
+        E.solve(xd, torch.from_numpy(P.b).cuda(), tol=1e-9, precision=engine.MIXED, x0_zero=True)
+        torch.cuda.synchronize()
+        assert np.array_equal(xd.cpu().numpy(), ref)
