@@ -256,6 +256,58 @@ template <> EMat<float> Engine::mat<float>(int l) const { return L[l].m32; }
 template <> const void *Engine::ainv<double>() const { return Ainv.p; }
 template <> const void *Engine::ainv<float>() const { return Ainv32.p; }
 
+// Row-scaled FP16 copy of the dense inverse: row i is stored as a / s_i with
+// s_i = max_j |a_ij|, so every entry lies in [-1, 1] (one warp per row).
+__global__ void k_to_half_rows(int n, const double *__restrict__ a, __half *__restrict__ o,
+                               float *__restrict__ sc) {
+  const int lane = threadIdx.x & 31;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= n) return;
+  const double *ar = a + (long long)row * n;
+  double m = 0.0;
+  for (int c = lane; c < n; c += 32) m = fmax(m, fabs(ar[c]));
+  for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+  const double inv = m > 0.0 ? 1.0 / m : 0.0;
+  for (int c = lane; c < n; c += 32) o[(long long)row * n + c] = __double2half(ar[c] * inv);
+  if (lane == 0) sc[row] = (float)m;
+}
+
+// z = Ainv r from the row-scaled FP16 copy: 16-byte loads of eight entries,
+// FP32 sums, one warp per row (n a multiple of 8)
+__global__ void k_dense_solve_h(int n, const __half *__restrict__ Ah, const float *__restrict__ sc,
+                                const float *__restrict__ r, float *__restrict__ z, const int *stop) {
+  PBG_PDL_ENTRY();
+  if (stop && *stop) return;
+  const int lane = threadIdx.x & 31;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= n) return;
+  const uint4 *ar = reinterpret_cast<const uint4 *>(Ah + (long long)row * n);
+  float acc = 0.0f;
+  for (int c8 = lane; c8 < n / 8; c8 += 32) {
+    const uint4 u = ar[c8];
+    const __half2 *h = reinterpret_cast<const __half2 *>(&u);
+    const float4 r0 = *reinterpret_cast<const float4 *>(r + c8 * 8);
+    const float4 r1 = *reinterpret_cast<const float4 *>(r + c8 * 8 + 4);
+    const float2 a0 = __half22float2(h[0]), a1 = __half22float2(h[1]);
+    const float2 a2 = __half22float2(h[2]), a3 = __half22float2(h[3]);
+    acc += a0.x * r0.x + a0.y * r0.y + a1.x * r0.z + a1.y * r0.w;
+    acc += a2.x * r1.x + a2.y * r1.y + a3.x * r1.z + a3.y * r1.w;
+  }
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+  if (lane == 0) z[row] = acc * sc[row];
+}
+
+// Large coarsest levels in the mixed path apply the FP16 copy (half the
+// bytes of the FP32 one) unless PBG_DENSE_HALF=0.
+static bool dense_half_enabled() {
+  static const bool on = [] {
+    const char *e = getenv("PBG_DENSE_HALF");
+    return !(e && atoi(e) == 0);
+  }();
+  return on;
+}
+constexpr int kDenseHalfMin = 2048;  // coarsest cells from which the FP16 copy is used
+
 __global__ void k_to_float(long long N, const double *__restrict__ a, float *__restrict__ o) {
   GRID_LOOP(p, N) o[p] = (float)a[p];
 }
@@ -265,6 +317,13 @@ template <typename T>
 void Engine::dense_solve(const T *r, T *z, const int *stop, cudaStream_t s) {
   using AT = typename std::conditional<sizeof(T) == 4, float, double>::type;
   const int blocks = (int)(((long long)ncoarse * 32 + kThreads - 1) / kThreads);
+  if constexpr (sizeof(T) == 4) {
+    if (Ainv16.n) {
+      launch_pdl(k_dense_solve_h, blocks, kThreads, s, ncoarse, (const __half *)Ainv16.p,
+                 (const float *)Ainv16s.p, (const float *)r, (float *)z, stop);
+      return;
+    }
+  }
   launch_pdl(k_dense_solve<T, AT>, blocks, kThreads, s, ncoarse, (const AT *)ainv<T>(), r, z, stop);
 }
 
@@ -296,6 +355,12 @@ void Engine::build(const EMat<double> &A0, cudaStream_t s, bool mixed) {
   ncoarse = (int)L.back().ncell();
   Ainv.alloc((size_t)ncoarse * ncoarse);
   if (mixed) Ainv32.alloc((size_t)ncoarse * ncoarse);
+  Ainv16.release();
+  Ainv16s.release();
+  if (mixed && dense_half_enabled() && ncoarse >= kDenseHalfMin && ncoarse % 8 == 0) {
+    Ainv16.alloc((size_t)ncoarse * ncoarse);
+    Ainv16s.alloc((size_t)ncoarse);
+  }
   Dtmp.alloc((size_t)ncoarse * ncoarse);
   have32 = false;
   if (mixed) {
@@ -349,6 +414,10 @@ void Engine::compute(cudaStream_t s) {
     PBG_CUDA(cudaMemcpyAsync(Ainv.p, src, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
   if (have32) {
     k_to_float<<<grid_for((long long)nn), kThreads, 0, s>>>((long long)nn, Ainv.p, Ainv32.p); note_launch();
+    if (Ainv16.n) {
+      const int blocks = (int)(((long long)ncoarse * 32 + kThreads - 1) / kThreads);
+      k_to_half_rows<<<blocks, kThreads, 0, s>>>(ncoarse, Ainv.p, Ainv16.p, Ainv16s.p); note_launch();
+    }
   }
   PBG_CUDA(cudaGetLastError());
 }

@@ -1,5 +1,6 @@
 // Engine solver: flexible CG + additive-correction K-cycle, FP64 and mixed.
 #pragma once
+#include <cuda_fp16.h>
 
 #include <vector>
 
@@ -88,6 +89,8 @@ class Engine {
   std::vector<ELevel> L;
   DBuf<double> Ainv;           // dense inverse of the coarsest operator
   DBuf<float> Ainv32;          // its FP32 copy (mixed path)
+  DBuf<__half> Ainv16;         // row-scaled FP16 copy (mixed path, large coarsest levels)
+  DBuf<float> Ainv16s;         // the row scales
   DBuf<double> Dtmp;           // its Gauss-Jordan work copy
   int ncoarse = 0;
   bool have32 = false;
