@@ -151,3 +151,22 @@ def test_x0_zero_option(engine, oracle):
         E.solve(xd, torch.from_numpy(P.b).cuda(), tol=1e-9, precision=engine.MIXED, x0_zero=True)
         torch.cuda.synchronize()
         assert np.array_equal(xd.cpu().numpy(), ref)
+
+
+def test_large_coarse_level_fp16_inverse(engine, oracle):
+    """A 4096-cell coarsest level in the mixed path is applied from the
+    row-scaled FP16 copy of its inverse: the solve still reaches the FP64
+    target, in no more iterations than with the default 512-cell level."""
+    P = oracle.Problem(1, 6, n=128, nb=6, rmin=3.0, rmax=8.0, rc=12.0)
+    its = {}
+    with engine.Session(*P.dims, P.h) as s:
+        s.assemble_pressure(P.rho, P.solid)
+        E = engine.Engine(s)
+        for cm in (512, 4096):
+            x = np.zeros(P.N)
+            assert E.solve(x, P.b.copy(), tol=1e-8, precision=engine.MIXED, coarse_max=cm)
+            its[cm] = E.last.iterations
+            r = np.zeros(P.N)
+            s.residual(x, P.b, r)
+            assert np.linalg.norm(r) <= 1.0001e-8 * np.linalg.norm(P.b)
+    assert its[4096] <= its[512] + 2
