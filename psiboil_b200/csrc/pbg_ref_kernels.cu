@@ -106,6 +106,14 @@ __global__ void k_dot2(long long N, const double *__restrict__ x, const double *
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double mc_of(const double *c, long long p) { return __ddiv_rn(1.0, c[p]); }
 
+// Mc = 1 / c once per solve (Diagonal::form, preconditioner_form.cpp:4-13);
+// the kernels below read it instead of dividing at every use
+__global__ void k_recip(long long N, const double *__restrict__ c, double *__restrict__ mc) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x)
+    mc[p] = mc_of(c, p);
+}
+
 __device__ void stale_init_dev(KrylovState *st, double res0) {
   int n = st->stalecount > kStaleMax ? kStaleMax : st->stalecount;
   for (int q = 0; q < n; ++q) st->stale[q] = 1.0e24;  // boil::unreal
@@ -127,7 +135,7 @@ __device__ bool stale_step_dev(KrylovState *st, double res) {
 
 __global__ void k_cg_init(MatView<double> A, const double *__restrict__ x,
                           const double *__restrict__ b, double *__restrict__ r,
-                          KrylovState *st, double *part, unsigned *count) {
+                          KrylovState *st, double *part, unsigned *count, const double *__restrict__ mc) {
   const long long N = A.ncell();
   const double dV = st->dV;
   double v[2] = {0.0, 0.0};
@@ -137,7 +145,7 @@ __global__ void k_cg_init(MatView<double> A, const double *__restrict__ x,
     double rv = ref_bmax(A, p, q, x, b[p]);
     r[p] = rv;
     v[0] += voldiv(rv, rv, dV);
-    v[1] += __dmul_rn(rv, __dmul_rn(rv, mc_of(A.c, p)));
+    v[1] += __dmul_rn(rv, __dmul_rn(rv, mc[p]));
   }
   double o[2];
   if (grid_reduce<2>(v, part, count, o, st->seq, N)) {
@@ -166,7 +174,7 @@ __global__ void k_cg_init(MatView<double> A, const double *__restrict__ x,
 
 __global__ void k_cg_pq(MatView<double> A, const double *__restrict__ r, double *pA, double *pB,
                         double *__restrict__ qv, KrylovState *st, double *part, unsigned *count,
-                        const double *__restrict__ zarr) {
+                        const double *__restrict__ zarr, const double *__restrict__ mc) {
   if (st->done) return;
   const int it = st->iter;
   const double *pold = (it & 1) ? pB : pA;
@@ -175,7 +183,7 @@ __global__ void k_cg_pq(MatView<double> A, const double *__restrict__ r, double 
   const long long N = A.ncell();
   // z = r * Mc (diagonal) or the preconditioner's output zarr
   auto pv = [&](long long s) {
-    double z = zarr ? zarr[s] : __dmul_rn(r[s], mc_of(A.c, s));
+    double z = zarr ? zarr[s] : __dmul_rn(r[s], mc[s]);
     return it == 0 ? z : __dadd_rn(z, __dmul_rn(beta, pold[s]));
   };
   double v[1] = {0.0};
@@ -196,7 +204,7 @@ __global__ void k_cg_pq(MatView<double> A, const double *__restrict__ r, double 
   }
 }
 
-__global__ void k_cg_xr(long long N, const double *__restrict__ c, double *__restrict__ x,
+__global__ void k_cg_xr(long long N, const double *__restrict__ mc, double *__restrict__ x,
                         double *__restrict__ r, const double *pA, const double *pB,
                         const double *__restrict__ qv, KrylovState *st, double *hist,
                         double *part, unsigned *count, int ic) {
@@ -211,7 +219,7 @@ __global__ void k_cg_xr(long long N, const double *__restrict__ c, double *__res
     double rv = __dsub_rn(r[p], __dmul_rn(alfa, qv[p]));
     r[p] = rv;
     v[0] += voldiv(rv, rv, dV);
-    v[1] += __dmul_rn(rv, __dmul_rn(rv, mc_of(c, p)));
+    v[1] += __dmul_rn(rv, __dmul_rn(rv, mc[p]));
   }
   double o[2];
   if (grid_reduce<2>(v, part, count, o, st->seq, N)) {
@@ -443,7 +451,7 @@ __global__ void k_bi_p(long long N, const double *__restrict__ c, const double *
       pp = __dsub_rn(pp, __dmul_rn(bo, v[p]));
     }
     pv[p] = pp;
-    if (diag) ph[p] = __dmul_rn(pp, mc_of(c, p));
+    if (diag) ph[p] = __dmul_rn(pp, c[p]);
   }
 }
 
@@ -479,7 +487,7 @@ __global__ void k_bi_s(long long N, const double *__restrict__ c, const double *
        p += (long long)gridDim.x * blockDim.x) {
     double sv = __dsub_rn(r[p], __dmul_rn(alfa, v[p]));
     s[p] = sv;
-    if (diag) sh[p] = __dmul_rn(sv, mc_of(c, p));
+    if (diag) sh[p] = __dmul_rn(sv, c[p]);
     a[0] += __dmul_rn(sv, sv);
   }
   double o[1];
@@ -584,7 +592,7 @@ __global__ void k_cgs_up(long long N, const double *__restrict__ c, const double
     }
     u[p] = uu;
     pv[p] = pp;
-    if (diag) ph[p] = __dmul_rn(pp, mc_of(c, p));
+    if (diag) ph[p] = __dmul_rn(pp, c[p]);
   }
 }
 
@@ -599,7 +607,7 @@ __global__ void k_cgs_qs(long long N, const double *__restrict__ c, const double
     const double ss = __dadd_rn(u[p], qq);
     q[p] = qq;
     s[p] = ss;
-    if (diag) sh[p] = __dmul_rn(ss, mc_of(c, p));
+    if (diag) sh[p] = __dmul_rn(ss, c[p]);
   }
 }
 
@@ -868,7 +876,7 @@ __global__ void k_krylov_setup(KrylovState *st, KrylovParams pr, long long ncell
 
 void RefKrylovWork::ensure(size_t n, int solver) {
   auto fit = [n](DBuf<double> &b) { if (b.n < n) b.alloc(n); };
-  fit(r); fit(q); fit(pA); fit(pB);
+  fit(r); fit(q); fit(pA); fit(pB); fit(mcd);
   if (solver >= 1) { fit(rt); fit(ph); fit(v); fit(s); fit(sh); fit(t); }
   if (solver == 2) fit(u);
 }
@@ -914,8 +922,9 @@ void enqueue_ref_setup(const MatView<double> &A, double *x, const double *b, con
     const int H = ic_planes(A, M), gp = grid_for((long long)A.nx * A.ny);
     for (int h = 0; h < H; ++h) { k_ic_form<<<gp, kThreads, 0, s>>>(A, M, h); note_launch(); }
   }
+  k_recip<<<grid_for(N), kThreads, 0, s>>>(N, A.c, w.mcd.p); note_launch();
   if (solver == 0)
-    k_cg_init<<<g, kThreads, 0, s>>>(A, x, b, w.r.p, st, red.slot_part(0), red.slot_count(0));
+    k_cg_init<<<g, kThreads, 0, s>>>(A, x, b, w.r.p, st, red.slot_part(0), red.slot_count(0), w.mcd.p);
   else
     k_bi_init<<<g, kThreads, 0, s>>>(A, x, b, w.r.p, w.rt.p, st, red.slot_part(0), red.slot_count(0));
   note_launch();
@@ -945,26 +954,26 @@ void enqueue_ref_iters(const MatView<double> &A, double *x, int solver, int coun
       // z = M^-1 r (forward and backward sweeps), rho = r.z, then the CG step
       ic_apply(A, M, w.r.p, w.z.p, st, s);
       k_cg_rho<<<g, kThreads, 0, s>>>(N, w.r.p, w.z.p, st, P0, C0); note_launch();
-      k_cg_pq<<<g, kThreads, 0, s>>>(A, w.r.p, w.pA.p, w.pB.p, w.q.p, st, P0, C0, w.z.p); note_launch();
-      k_cg_xr<<<g, kThreads, 0, s>>>(N, A.c, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1, 1); note_launch();
+      k_cg_pq<<<g, kThreads, 0, s>>>(A, w.r.p, w.pA.p, w.pB.p, w.q.p, st, P0, C0, w.z.p, w.mcd.p); note_launch();
+      k_cg_xr<<<g, kThreads, 0, s>>>(N, w.mcd.p, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1, 1); note_launch();
     } else if (solver == 0) {
-      k_cg_pq<<<g, kThreads, 0, s>>>(A, w.r.p, w.pA.p, w.pB.p, w.q.p, st, P0, C0, nullptr); note_launch();
-      k_cg_xr<<<g, kThreads, 0, s>>>(N, A.c, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1, 0); note_launch();
+      k_cg_pq<<<g, kThreads, 0, s>>>(A, w.r.p, w.pA.p, w.pB.p, w.q.p, st, P0, C0, nullptr, w.mcd.p); note_launch();
+      k_cg_xr<<<g, kThreads, 0, s>>>(N, w.mcd.p, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1, 0); note_launch();
     } else if (solver == 1) {
       k_bi_rho<<<g, kThreads, 0, s>>>(N, w.rt.p, w.r.p, st, P0, C0); note_launch();
-      k_bi_p<<<g, kThreads, 0, s>>>(N, A.c, w.r.p, w.pA.p, w.v.p, w.ph.p, st, diag); note_launch();
+      k_bi_p<<<g, kThreads, 0, s>>>(N, w.mcd.p, w.r.p, w.pA.p, w.v.p, w.ph.p, st, diag); note_launch();
       if (!diag) ic_apply(A, M, w.pA.p, w.ph.p, st, s);
       k_bi_spmv<<<g, kThreads, 0, s>>>(A, w.ph.p, w.v.p, w.rt.p, 0, st, P1, C1); note_launch();
-      k_bi_s<<<g, kThreads, 0, s>>>(N, A.c, w.r.p, w.v.p, w.s.p, w.sh.p, st, P0, C0, diag); note_launch();
+      k_bi_s<<<g, kThreads, 0, s>>>(N, w.mcd.p, w.r.p, w.v.p, w.s.p, w.sh.p, st, P0, C0, diag); note_launch();
       if (!diag) ic_apply(A, M, w.s.p, w.sh.p, st, s);
       k_bi_spmv<<<g, kThreads, 0, s>>>(A, w.sh.p, w.t.p, w.s.p, 1, st, P1, C1); note_launch();
       k_bi_xr<<<g, kThreads, 0, s>>>(N, x, w.r.p, w.ph.p, w.sh.p, w.s.p, w.t.p, st, hist, P0, C0); note_launch();
     } else {
       k_cgs_rho<<<g, kThreads, 0, s>>>(N, w.rt.p, w.r.p, st, P0, C0); note_launch();
-      k_cgs_up<<<g, kThreads, 0, s>>>(N, A.c, w.r.p, w.q.p, w.u.p, w.pA.p, w.ph.p, st, diag); note_launch();
+      k_cgs_up<<<g, kThreads, 0, s>>>(N, w.mcd.p, w.r.p, w.q.p, w.u.p, w.pA.p, w.ph.p, st, diag); note_launch();
       if (!diag) ic_apply(A, M, w.pA.p, w.ph.p, st, s);
       k_bi_spmv<<<g, kThreads, 0, s>>>(A, w.ph.p, w.v.p, w.rt.p, 0, st, P1, C1); note_launch();
-      k_cgs_qs<<<g, kThreads, 0, s>>>(N, A.c, w.u.p, w.v.p, w.q.p, w.s.p, w.sh.p, st, diag); note_launch();
+      k_cgs_qs<<<g, kThreads, 0, s>>>(N, w.mcd.p, w.u.p, w.v.p, w.q.p, w.s.p, w.sh.p, st, diag); note_launch();
       if (!diag) ic_apply(A, M, w.s.p, w.sh.p, st, s);
       k_cgs_xr<<<g, kThreads, 0, s>>>(A, x, w.r.p, w.sh.p, st, hist, P0, C0); note_launch();
     }

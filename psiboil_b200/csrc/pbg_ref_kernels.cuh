@@ -26,6 +26,7 @@ struct KrylovParams {
 // solver codes of the drivers below: 0 CG, 1 BiCGS, 2 CGS
 struct RefKrylovWork {
   DBuf<double> r, q, pA, pB, rt, ph, v, s, sh, t, u;
+  DBuf<double> mcd;                               // 1 / c (the diagonal preconditioner)
   DBuf<double> z, mc, mw, ms, mb, mtw, mts, mnw;  // IC preconditioner
   void ensure(size_t n, int solver);
   IcFactor ic(int kind, size_t n);
