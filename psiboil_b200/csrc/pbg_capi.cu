@@ -53,6 +53,17 @@ struct pbg_session {
 
 namespace {
 
+// Geometry with 32-bit division for the flow kernels (n = 0 above 2^31
+// cells selects their 64-bit path).
+Geo flow_geo(const pbg_session *s) {
+  if (s->ncell() >= (1ll << 31)) {
+    Geo g;
+    g.n = 0;
+    return g;
+  }
+  return Geo(s->nx, s->ny, s->nz);
+}
+
 int fail(int code, const std::string &m) {
   g_err = m;
   return code;
@@ -474,7 +485,7 @@ int pbg_assemble_mix(pbg_session *s, const double *col, double rho_a, double rho
     if (A.c.n != (size_t)N) { A.c.alloc(N); A.w.alloc(N); A.s.alloc(N); A.b.alloc(N); }
     A.e.release(); A.n.release(); A.t.release();
     k_assemble_mix<<<grid_for(N), kThreads, 0, s->stream>>>(
-        s->nx, s->ny, s->nz, s->h, make_int4(s->bc[0], s->bc[1], s->bc[2], s->bc[3]),
+        flow_geo(s), s->nx, s->ny, s->nz, s->h, make_int4(s->bc[0], s->bc[1], s->bc[2], s->bc[3]),
         make_int2(s->bc[4], s->bc[5]), cp, rho_a, rho_b, sp, A.c.p, A.w.p, A.s.p, A.b.p, s->aflag.p);
     note_launch();
     PBG_CUDA(cudaGetLastError());
@@ -554,7 +565,7 @@ int pbg_divergence(pbg_session *s, const double *u, const double *v, const doubl
     }
     const double dti = 1.0 / dt;
     const double a = (s->h * s->h) * dti;
-    k_divergence<<<grid_for(N), kThreads, 0, s->stream>>>(s->nx, s->ny, s->nz, a, fa.d[0], fa.d[1], fa.d[2], sp,
+    k_divergence<<<grid_for(N), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, a, fa.d[0], fa.d[1], fa.d[2], sp,
                                                           r);
     note_launch();
     PBG_CUDA(cudaGetLastError());
@@ -594,7 +605,7 @@ int pbg_project(pbg_session *s, const double *p, const double *col, double rho_a
         sp = dsol.p;
       }
     }
-    k_project<<<grid_for(N), kThreads, 0, s->stream>>>(s->nx, s->ny, s->nz, s->h, dt, pp, cp, rho_a, rho_b, sp,
+    k_project<<<grid_for(N), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, s->h, dt, pp, cp, rho_a, rho_b, sp,
                                                        fa.d[0], fa.d[1], fa.d[2]);
     note_launch();
     PBG_CUDA(cudaGetLastError());

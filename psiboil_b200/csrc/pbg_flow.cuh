@@ -18,6 +18,13 @@
 
 namespace pbg {
 
+// Cell position: 32-bit multiply-shift division (Geo) below 2^31 cells,
+// 64-bit division above.
+__device__ __forceinline__ Pos flow_pos(const Geo &g, long long p, int ny, int nz) {
+  if (g.n != 0u) return g.pos((uint32_t)p);
+  return pos_of(p, ny, nz);
+}
+
 // Cell density of the mixture, PropertyMix::value(i,j,k)
 // (Src/Matter/property_value.cpp:52-70): col clamped to [0, 1], then
 // rho_a * col + rho_b * (1 - col).
@@ -107,7 +114,7 @@ __device__ __forceinline__ void assemble_mix_cell(int nx, int ny, int nz, double
   B = a[4];
 }
 
-__global__ void k_assemble_mix(int nx, int ny, int nz, double h, int4 bc03, int2 bc45,
+__global__ void k_assemble_mix(Geo G, int nx, int ny, int nz, double h, int4 bc03, int2 bc45,
                                const double *__restrict__ col, double ra, double rb,
                                const uint8_t *__restrict__ solid, double *__restrict__ C,
                                double *__restrict__ W, double *__restrict__ S, double *__restrict__ B,
@@ -116,7 +123,7 @@ __global__ void k_assemble_mix(int nx, int ny, int nz, double h, int4 bc03, int2
   const int bc[6] = {bc03.x, bc03.y, bc03.z, bc03.w, bc45.x, bc45.y};
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
        p += (long long)gridDim.x * blockDim.x) {
-    Pos q = pos_of(p, ny, nz);
+    Pos q = flow_pos(G, p, ny, nz);
     double c, w, sv, b;
     assemble_mix_cell(nx, ny, nz, h, bc, col, ra, rb, solid, p, q, c, w, sv, b);
     C[p] = c;
@@ -135,14 +142,14 @@ __global__ void k_assemble_mix(int nx, int ny, int nz, double h, int4 bc03, int2
 // face counts only if the neighbour across it is fluid (cells beyond the
 // domain count as fluid), and solid cells get 0. w may be nullptr in 2-D
 // (its faces then count as zero).
-__global__ void k_divergence(int nx, int ny, int nz, double a, const double *__restrict__ u,
+__global__ void k_divergence(Geo G, int nx, int ny, int nz, double a, const double *__restrict__ u,
                              const double *__restrict__ v, const double *__restrict__ w,
                              const uint8_t *__restrict__ solid, double *__restrict__ rhs) {
   const long long N = (long long)nx * ny * nz;
   const long long SI = (long long)ny * nz, SJ = nz;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
        p += (long long)gridDim.x * blockDim.x) {
-    Pos q = pos_of(p, ny, nz);
+    Pos q = flow_pos(G, p, ny, nz);
     const long long iu = p;  // west face of the cell
     const long long iv = ((long long)q.i * (ny + 1) + q.j) * nz + q.k;
     const long long iw = ((long long)q.i * ny + q.j) * (nz + 1) + q.k;
@@ -182,7 +189,7 @@ __device__ __forceinline__ double project_increment(double pm, double pp, double
   return __ddiv_rn(__dmul_rn(__ddiv_rn(dp, rho), dt), h);
 }
 
-__global__ void k_project(int nx, int ny, int nz, double h, double dt, const double *__restrict__ pr,
+__global__ void k_project(Geo G, int nx, int ny, int nz, double h, double dt, const double *__restrict__ pr,
                           const double *__restrict__ col, double ra, double rb,
                           const uint8_t *__restrict__ solid, double *__restrict__ u, double *__restrict__ v,
                           double *__restrict__ w) {
@@ -191,7 +198,7 @@ __global__ void k_project(int nx, int ny, int nz, double h, double dt, const dou
   const bool body = solid != nullptr;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
        p += (long long)gridDim.x * blockDim.x) {
-    Pos q = pos_of(p, ny, nz);
+    Pos q = flow_pos(G, p, ny, nz);
     const bool sp = body && solid[p];
     const double pp = pr[p];
     if (q.i > 0 && !(body && (sp || solid[p - SI])))
