@@ -246,6 +246,86 @@ __global__ void k_cg_xr(long long N, const double *__restrict__ mc, double *__re
 }
 
 // ---------------------------------------------------------------------------
+// CG with the diagonal preconditioner and tree-order sums, split for
+// 16-byte access (nz even): k_cg_p forms p = z + beta p_old in place
+// (z = r Mc), k_cg_q forms q = A p with the dot p.q, and k_cg_xr follows as
+// in the fused path (given the one p buffer twice). Every element gets the
+// arithmetic of k_cg_pq / ref_ax in the same order, so the iterates equal
+// the fused path's up to the order of the global sums.
+// ---------------------------------------------------------------------------
+__global__ void k_cg_p(long long N, const double *__restrict__ r, const double *__restrict__ mc,
+                       double *__restrict__ p, KrylovState *st) {
+  if (st->done) return;
+  const int it = st->iter;
+  const double beta = it == 0 ? 0.0 : __ddiv_rn(st->rho, st->rho_old);
+  const long long NP = N / 2;
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < NP;
+       g += (long long)gridDim.x * blockDim.x) {
+    const double2 rv = reinterpret_cast<const double2 *>(r)[g];
+    const double2 mv = reinterpret_cast<const double2 *>(mc)[g];
+    double2 z = make_double2(__dmul_rn(rv.x, mv.x), __dmul_rn(rv.y, mv.y));
+    if (it > 0) {
+      const double2 po = reinterpret_cast<const double2 *>(p)[g];
+      z.x = __dadd_rn(z.x, __dmul_rn(beta, po.x));
+      z.y = __dadd_rn(z.y, __dmul_rn(beta, po.y));
+    }
+    reinterpret_cast<double2 *>(p)[g] = z;
+  }
+  if ((N & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+    const long long e = N - 1;
+    double z = __dmul_rn(r[e], mc[e]);
+    if (it > 0) z = __dadd_rn(z, __dmul_rn(beta, p[e]));
+    p[e] = z;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->beta = beta;
+}
+
+// q = A p for two cells of one k-row (nz even), in ref_ax's order
+__global__ void k_cg_q(MatView<double> A, Geo G, const double *__restrict__ p, double *__restrict__ qv,
+                       KrylovState *st, double *part, unsigned *count) {
+  if (st->done) return;
+  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
+  const long long NP = A.ncell() / 2;
+  double v[1] = {0.0};
+  auto ld2 = [&](const double *a, long long e) { return reinterpret_cast<const double2 *>(a + e)[0]; };
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < NP;
+       g += (long long)gridDim.x * blockDim.x) {
+    const long long e = 2 * g;
+    const Pos q = G.pos((uint32_t)e);
+    const double2 x = ld2(p, e), c = ld2(A.c, e), w = ld2(A.w, e), s = ld2(A.s, e), b = ld2(A.b, e);
+    const double2 z2 = make_double2(0.0, 0.0);
+    const double2 xw = q.i > 0 ? ld2(p, e - SI) : z2, xe = q.i < A.nx - 1 ? ld2(p, e + SI) : z2;
+    const double2 xs = q.j > 0 ? ld2(p, e - SJ) : z2, xn = q.j < A.ny - 1 ? ld2(p, e + SJ) : z2;
+    const double xb0 = q.k > 0 ? p[e - 1] : 0.0, xt1 = q.k + 2 < A.nz ? p[e + 2] : 0.0;
+    double2 ec, nc, tc;
+    if (A.e) {
+      ec = ld2(A.e, e); nc = ld2(A.n, e); tc = ld2(A.t, e);
+    } else {
+      ec = q.i < A.nx - 1 ? ld2(A.w, e + SI) : z2;
+      nc = q.j < A.ny - 1 ? ld2(A.s, e + SJ) : z2;
+      tc = make_double2(b.y, q.k + 2 < A.nz ? A.b[e + 2] : 0.0);
+    }
+    // lane 0: k, lane 1: k + 1 (its b neighbour is lane 0, lane 0's t neighbour is lane 1)
+    double y0 = __dmul_rn(c.x, x.x);
+    y0 = __dsub_rn(y0, __dadd_rn(__dmul_rn(w.x, xw.x), __dmul_rn(ec.x, xe.x)));
+    y0 = __dsub_rn(y0, __dadd_rn(__dmul_rn(s.x, xs.x), __dmul_rn(nc.x, xn.x)));
+    y0 = __dsub_rn(y0, __dadd_rn(__dmul_rn(b.x, xb0), __dmul_rn(tc.x, x.y)));
+    double y1 = __dmul_rn(c.y, x.y);
+    y1 = __dsub_rn(y1, __dadd_rn(__dmul_rn(w.y, xw.y), __dmul_rn(ec.y, xe.y)));
+    y1 = __dsub_rn(y1, __dadd_rn(__dmul_rn(s.y, xs.y), __dmul_rn(nc.y, xn.y)));
+    y1 = __dsub_rn(y1, __dadd_rn(__dmul_rn(b.y, x.x), __dmul_rn(tc.y, xt1)));
+    reinterpret_cast<double2 *>(qv + e)[0] = make_double2(y0, y1);
+    v[0] += __dmul_rn(x.x, y0);
+    v[0] += __dmul_rn(x.y, y1);
+  }
+  double o[1];
+  if (grid_reduce<1>(v, part, count, o)) {
+    st->pq = o[0];
+    st->alfa = __ddiv_rn(st->rho, o[0]);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Incomplete Cholesky preconditioners (Prec::ic0/ic2/ic3):
 // IncompleteCholesky0/2/3::form (preconditioner_form.cpp:16-144) and ::solve
 // (preconditioner_solve.cpp:14-110). The reference runs factor and sweeps in
@@ -956,6 +1036,11 @@ void enqueue_ref_iters(const MatView<double> &A, double *x, int solver, int coun
       k_cg_rho<<<g, kThreads, 0, s>>>(N, w.r.p, w.z.p, st, P0, C0); note_launch();
       k_cg_pq<<<g, kThreads, 0, s>>>(A, w.r.p, w.pA.p, w.pB.p, w.q.p, st, P0, C0, w.z.p, w.mcd.p); note_launch();
       k_cg_xr<<<g, kThreads, 0, s>>>(N, w.mcd.p, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1, 1); note_launch();
+    } else if (solver == 0 && !exact && A.nz % 2 == 0) {
+      const int gq = grid_for(N / 2);
+      k_cg_p<<<gq, kThreads, 0, s>>>(N, w.r.p, w.mcd.p, w.pA.p, st); note_launch();
+      k_cg_q<<<gq, kThreads, 0, s>>>(A, Geo(A.nx, A.ny, A.nz), w.pA.p, w.q.p, st, P0, C0); note_launch();
+      k_cg_xr<<<g, kThreads, 0, s>>>(N, w.mcd.p, x, w.r.p, w.pA.p, w.pA.p, w.q.p, st, hist, P1, C1, 0); note_launch();
     } else if (solver == 0) {
       k_cg_pq<<<g, kThreads, 0, s>>>(A, w.r.p, w.pA.p, w.pB.p, w.q.p, st, P0, C0, nullptr, w.mcd.p); note_launch();
       k_cg_xr<<<g, kThreads, 0, s>>>(N, w.mcd.p, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1, 0); note_launch();
