@@ -141,7 +141,7 @@ int pbg_device_count(int *count);
  * ResTol(1e-15), scale 1, stalecount -1 (linear.h:46-56, resrat.h,
  * restol.h, maxiter.h); AC defaults of additive.cpp:11-19 (max_cyc 20,
  * min_cyc 0, stop_if_div true, priority_min_cyc true, mv {20,20,20},
- * ms {-1,-1,-1}); engine tol 1e-8, inner_tol 1e-4, max_sweeps 8. */
+ * ms {-1,-1,-1}); engine tol 1e-8, inner_tol 1e-3, max_sweeps 8. */
 void pbg_params_default(pbg_params *p, int solver);
 
 /* A session owns one grid (nx, ny, nz interior cells, nz == 1 for 2-D, uniform

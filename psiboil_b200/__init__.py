@@ -552,7 +552,7 @@ class Engine:
         self.session = session
         self.last = None
 
-    def solve(self, x, b, tol=1.0e-8, precision=FP64, inner_tol=1.0e-4, max_iter=500,
+    def solve(self, x, b, tol=1.0e-8, precision=FP64, inner_tol=1.0e-3, max_iter=500,
               max_sweeps=8, coarse_max=0, x0_zero=False):
         """x0_zero: start from zero (x is output only and is not uploaded)."""
         p = default_params(SOLVER_ENGINE)
@@ -697,7 +697,7 @@ class Batch:
         p.tol, p.inner_tol, p.max_iter, p.max_sweeps = tol, inner_tol, max_iter, max_sweeps
         return p
 
-    def solve(self, ids, tol=1.0e-8, inner_tol=1.0e-4, max_iter=500, max_sweeps=8):
+    def solve(self, ids, tol=1.0e-8, inner_tol=1.0e-3, max_iter=500, max_sweeps=8):
         """Solve the problems `ids`; returns a list of Result (seconds = time
         from the start of the call until that problem finished)."""
         ids = list(ids)
@@ -707,7 +707,7 @@ class Batch:
         _check(lib().pbg_batch_solve(self._h, arr, len(ids), ctypes.byref(p), res))
         return list(res)
 
-    def autotune(self, ids, cache=None, tol=1.0e-8, inner_tol=1.0e-4, max_iter=500, max_sweeps=8):
+    def autotune(self, ids, cache=None, tol=1.0e-8, inner_tol=1.0e-3, max_iter=500, max_sweeps=8):
         ids = list(ids)
         arr = (ctypes.c_int * len(ids))(*ids)
         p = self._params(tol, inner_tol, max_iter, max_sweeps)

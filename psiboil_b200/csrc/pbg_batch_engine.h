@@ -30,7 +30,7 @@ struct BatchShape {
 
 struct BatchSolveParams {
   double tol = 1e-8;        // FP64 |b - A x| / |b|
-  double inner_tol = 1e-4;  // mixed: inner reduction per refinement sweep
+  double inner_tol = 1e-3;  // mixed: inner reduction per refinement sweep
   int max_sweeps = 8;       // refinement sweeps at most (plain FP64: 4)
   int max_iter = 500;       // inner iterations at most, all sweeps together
   int inner_max_iter = 500; // inner iterations per sweep

@@ -252,7 +252,7 @@ void pbg_params_default(pbg_params *p, int solver) {
   p->priority_min_cyc = 1;
   for (int q = 0; q < 3; ++q) { p->mv[q] = 20; p->ms[q] = -1; }
   p->tol = 1.0e-8;
-  p->inner_tol = 1.0e-4;
+  p->inner_tol = 1.0e-3;
   p->max_sweeps = 8;
   if (solver == PBG_SOLVER_ENGINE) p->max_iter = 500;
 }

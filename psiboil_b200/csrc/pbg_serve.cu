@@ -287,7 +287,7 @@ void pbg_server_config_default(pbg_server_config *c) {
   c->kc_max = b.kc_max;
   c->tail_cells = b.tail_cells;
   c->tol = 1e-8;
-  c->inner_tol = 1e-4;
+  c->inner_tol = 1e-3;
   c->max_sweeps = 8;
   c->max_iter = 500;
 }
