@@ -489,6 +489,7 @@ class BatchEngine : public BatchEngineBase {
     const int dtile = (int)(sig_ & 0xff);
     const unsigned dense_mask = (unsigned)((sig_ >> 8) & 0xffff), tail_mask = (unsigned)((sig_ >> 24) & 0xffff);
     kb_jac2<T><<<G, NT, 0, stream>>>(C, l, kc); ++n;
+    if (kBPad<T> && l == 0) { kb_resid0<T><<<G, NT, 0, stream>>>(C); ++n; }
     kb_restrict<T><<<GH, NT, 0, stream>>>(C, l, kc); ++n;
     if (dense_mask & (1u << (l + 1))) { kb_dense<T><<<slot_grid(), NT, 0, stream>>>(C, l + 1); ++n; }
     if (tail_mask & (1u << (l + 1))) { kb_tail<T><<<slot_grid(), NT, 0, stream>>>(C, l + 1); ++n; }

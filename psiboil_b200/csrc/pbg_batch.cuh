@@ -636,12 +636,27 @@ __device__ __forceinline__ void vgroup_jac2(const BLev<T> &V, const T *r, T om, 
   stv(V.xb, p, o);
 }
 
-// coarse cell Pc of level 1 = sum over its fine children of (r - A xb),
-// the children read from the padded level 0 (2-D: the coarse j is the fine
-// fast axis); the same (a, b, c) order as restrict_cell
+// residual rhs - A xb of a group, into xa (free until the prolongation):
+// the restriction onto level 1 then only sums children
 template <typename T>
-__device__ __forceinline__ T restrict_cell_pad(const BProb<T> &P, const EMat<T> &A, const T *r, const T *x,
-                                               const Geo &H, uint32_t Pc) {
+__device__ __forceinline__ void vgroup_resid(const BLev<T> &V, const T *r, uint32_t p) {
+  constexpr int W = VecTraits<T>::V;
+  const EMat<T> &A = V.A;
+  const Pos q = A.g.pos(p);
+  const CoefV<T> Cf = load_coef(A, p, q);
+  const Vec<T> c = ldv(A.c, p), rp = ldv(r, p);
+  const HoodV<T> X = load_hood(A, p, q, FArr<T>{V.xb});
+  Vec<T> o;
+#pragma unroll
+  for (int m = 0; m < W; ++m) o.v[m] = rp.v[m] - axv(c.v[m], Cf, X, m);
+  stv(V.xa, p, o);
+}
+
+// coarse cell Pc of level 1 = the sum of its children's residuals (in xa),
+// in restrict_cell's (a, b, c) order
+template <typename T>
+__device__ __forceinline__ T restrict_sum_pad(const BProb<T> &P, const EMat<T> &A, const T *res, const Geo &H,
+                                              uint32_t Pc) {
   const Pos Q = H.pos(Pc);
   const int fx = A.nx > 1 ? 2 : 1, fy = A.ny > 1 ? 2 : 1, fz = P.F > 1 ? 2 : 1;
   const int qj = P.rel2d ? 0 : Q.j, qk = P.rel2d ? Q.j : Q.k;
@@ -655,8 +670,7 @@ __device__ __forceinline__ T restrict_cell_pad(const BProb<T> &P, const EMat<T> 
       for (int cc = 0; cc < fz; ++cc) {
         const int k = qk * fz + cc;
         if (k >= P.F) break;
-        const uint32_t p = ((uint32_t)i * A.ny + j) * A.nz + k;
-        sum += r[p] - ax_at(A, p, Pos{i, j, k}, x);
+        sum += res[((uint32_t)i * A.ny + j) * A.nz + k];
       }
     }
   }
@@ -758,11 +772,25 @@ __global__ void kb_restrict(BCtx<T> C, int l, int kc) {
     if (!b_tile_level(S, P, l)) continue;
     const T *r = b_rhs(P, l, kc != 0);
     const BLev<T> &V = P.L[l], &H = P.L[l + 1];
-    if (kBPad<T> && l == 0) {
-      BCELL_LOOP(tl, Pc) H.b[Pc] = restrict_cell_pad(P, V.A, r, V.xb, H.A.g, Pc);
+    if (kBPad<T> && l == 0) {  // the residuals are in xa (kb_resid0)
+      BCELL_LOOP(tl, Pc) H.b[Pc] = restrict_sum_pad(P, V.A, V.xa, H.A.g, Pc);
       continue;
     }
     BCELL_LOOP(tl, Pc) H.b[Pc] = restrict_cell(V.A, r, V.xb, H.A.g, Pc);
+  }
+}
+
+// padded level 0: residuals of the two sweeps into xa, for kb_restrict
+template <typename T>
+__global__ void BPAD_BOUNDS kb_resid0(BCtx<T> C) {
+  if constexpr (kBPad<T>) {
+    BTILE_LOOP(C, 0, t) {
+      const BTile tl = C.tiles[t];
+      const BState &S = C.st[tl.slot];
+      const BProb<T> &P = C.prob[tl.slot];
+      if (!b_tile_level(S, P, 0)) continue;
+      BGROUP_LOOP(tl, p) vgroup_resid(P.L[0], P.r0, p);
+    }
   }
 }
 
