@@ -73,7 +73,9 @@ enum {
   PBG_SOLVER_BICGS = 1,   /* BiCGStab with diagonal preconditioner (parity)       */
   PBG_SOLVER_AC = 2,      /* additive-correction multigrid, CG smoother (parity)  */
   PBG_SOLVER_ENGINE = 3,  /* flexible CG + AC K-cycle (the engine's fast solver)  */
-  PBG_SOLVER_CGS = 4      /* conjugate gradient squared, CGS::solve (parity)       */
+  PBG_SOLVER_CGS = 4,     /* conjugate gradient squared, CGS::solve (parity)       */
+  PBG_SOLVER_JACOBI = 5,  /* Jacobi::solve (Src/Solver/Linear/Iterative, parity)   */
+  PBG_SOLVER_GAUSS_SEIDEL = 6  /* GaussSeidel::solve, lexicographic (parity)       */
 };
 enum { PBG_FP64 = 0, PBG_MIXED = 1 };
 enum { PBG_CYCLE_NONE = -1, PBG_CYCLE_V = 1, PBG_CYCLE_F = 2, PBG_CYCLE_W = 4 };
@@ -173,6 +175,15 @@ int pbg_matrix_download(pbg_session *s, double *c, double *w, double *e, double 
  * active), strided like the matrix. Default: all active. */
 int pbg_active_upload(pbg_session *s, const int *aflag, long long si, long long sj, long long sk,
                       long long offset, int where);
+/* The matrix's stored inverse central coefficient A.ci (matrix.h:23-54),
+ * strided like the matrix, for PBG_SOLVER_JACOBI and PBG_SOLVER_GAUSS_SEIDEL,
+ * which divide by it (jacobi.cpp:43, gaussseidel.cpp:51). The reference
+ * forms ci before it scales the central coefficient of cells inside a body
+ * by 1e-12 (pressure_discretize.cpp:127-138), so there ci is not 1/c. Until
+ * it is uploaded, and after every change of the matrix, those solvers use
+ * 1/c. */
+int pbg_ci_upload(pbg_session *s, const double *ci, long long si, long long sj, long long sk,
+                  long long offset, int where);
 
 /* On-device assembly of the pressure matrix from cell densities and a solid
  * mask (1 = solid), Pressure::discretize with a harmonic face density:

@@ -454,6 +454,103 @@ done_early:
 }
 
 /* ------------------------------------------------------------------ */
+/* Stationary iterations (Src/Solver/Linear/Iterative)                 */
+/* ------------------------------------------------------------------ */
+
+/* Jacobi::solve (jacobi.cpp:10-75): x = ci (r + c x) with the residual of
+ * the previous sweep, then r = b - A x; the measure is sqrt(r.r) (res and
+ * res0 in st are square roots). */
+int orc_jacobi(const orc_mat *A, const double *ci, double *x, const double *b, int mini,
+               int maxit, double res_rat, double res_tol, orc_stats *st, double *hist) {
+  const size_t N = (size_t)A->nx * A->ny * A->nz;
+  double *r = calloc(N, sizeof(double));
+  orc_resid(A, x, b, r);
+  double res = orc_dot(N, r, r);
+  const double res0 = res;
+  orc_stats so = {0, 0, 0, sqrt(res0), sqrt(res), 0};
+  if (sqrt(res) < res_tol) {
+    so.converged = 1; so.status = 4;
+    if (st) *st = so;
+    free(r);
+    return 1;
+  }
+  int converged = 0, i, broke = 0;
+  so.status = 1;
+  for (i = 0; i < maxit; ++i) {
+    for (size_t c = 0; c < N; ++c) x[c] = ci[c] * (r[c] + A->c[c] * x[c]);
+    orc_resid(A, x, b, r);
+    res = orc_dot(N, r, r);
+    if (hist) hist[i] = sqrt(res);
+    if (sqrt(res) < res_tol && i >= mini - 1) { converged = 1; broke = 1; so.status = 0; break; }
+    if (sqrt(res) < sqrt(res0) * res_rat && i >= mini - 1) {
+      converged = 1; broke = 1; so.status = 0; break;
+    }
+  }
+  so.converged = converged;
+  so.iterations = broke ? i + 1 : maxit;
+  so.printed = i + 1;
+  so.res = sqrt(res);
+  if (st) *st = so;
+  free(r);
+  return converged;
+}
+
+/* GaussSeidel::solve (gaussseidel.cpp:10-117): in-place sweeps in i, j, k
+ * order, x = ci (b + w xw + e xe + s xs + n xn + b xb + t xt) summed left to
+ * right, then r = b - A x; the measure is sqrt(dot_voldiv_avg(r, r)) / scale
+ * and the stale window starts with every entry unreal (:28-33). */
+int orc_gauss_seidel(const orc_mat *A, const double *ci, double *x, const double *b, int mini,
+                     int maxit, double res_rat, double res_tol, double scale, int stalecount,
+                     double dV, orc_stats *st, double *hist) {
+  const int nx = A->nx, ny = A->ny, nz = A->nz;
+  const size_t N = (size_t)nx * ny * nz, SI = (size_t)ny * nz, SJ = (size_t)nz;
+  double *r = calloc(N, sizeof(double));
+  orc_resid(A, x, b, r);
+  double res = sqrt(orc_dot_voldiv_avg(N, r, r, dV)) / scale;
+  const double res0 = res;
+  stale_win win;
+  stale_init(&win, stalecount, res);
+  for (int q = 0; q < win.n; ++q) win.v[q] = 1.0e24; /* boil::unreal, no res0 */
+  orc_stats so = {0, 0, 0, res0, res, 0};
+  if (res < res_tol) {
+    so.converged = 1; so.status = 4;
+    if (st) *st = so;
+    free(r); free(win.v);
+    return 1;
+  }
+  int converged = 0, it, broke = 0;
+  so.status = 1;
+  for (it = 0; it < maxit; ++it) {
+    for (int i = 0; i < nx; ++i)
+      for (int j = 0; j < ny; ++j)
+        for (int k = 0; k < nz; ++k) {
+          const size_t p = ((size_t)i * ny + j) * nz + k;
+          double v = b[p];
+          v += A->w[p] * (i > 0 ? x[p - SI] : 0.0);
+          v += A->e[p] * (i < nx - 1 ? x[p + SI] : 0.0);
+          v += A->s[p] * (j > 0 ? x[p - SJ] : 0.0);
+          v += A->n[p] * (j < ny - 1 ? x[p + SJ] : 0.0);
+          v += A->b[p] * (k > 0 ? x[p - 1] : 0.0);
+          v += A->t[p] * (k < nz - 1 ? x[p + 1] : 0.0);
+          x[p] = ci[p] * v;
+        }
+    orc_resid(A, x, b, r);
+    res = sqrt(orc_dot_voldiv_avg(N, r, r, dV)) / scale;
+    if (hist) hist[it] = res;
+    if (res < res_tol && it >= mini - 1) { converged = 1; broke = 1; so.status = 0; break; }
+    if (res < res0 * res_rat && it >= mini - 1) { converged = 1; broke = 1; so.status = 0; break; }
+    if (stale_step(&win, res)) { broke = 1; so.status = 2; break; }
+  }
+  so.converged = converged;
+  so.iterations = broke ? it + 1 : maxit;
+  so.printed = it + 1;
+  so.res = res;
+  if (st) *st = so;
+  free(r); free(win.v);
+  return converged;
+}
+
+/* ------------------------------------------------------------------ */
 /* Additive-correction multigrid                                       */
 /* ------------------------------------------------------------------ */
 

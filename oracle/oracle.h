@@ -74,6 +74,15 @@ int orc_cgs_prec(const orc_mat *A, double *x, const double *b, int mini, int max
                  double res_rat, double res_tol, double scale, int stalecount,
                  double dV, orc_stats *st, double *hist, int prec);
 
+/* Jacobi::solve (Src/Solver/Linear/Iterative/jacobi.cpp:10-75) with the
+ * matrix's stored inverse central coefficient ci; st->res0/res are sqrt(r.r). */
+int orc_jacobi(const orc_mat *A, const double *ci, double *x, const double *b, int mini,
+               int maxit, double res_rat, double res_tol, orc_stats *st, double *hist);
+/* GaussSeidel::solve (gaussseidel.cpp:10-117), lexicographic in-place sweeps. */
+int orc_gauss_seidel(const orc_mat *A, const double *ci, double *x, const double *b, int mini,
+                     int maxit, double res_rat, double res_tol, double scale, int stalecount,
+                     double dV, orc_stats *st, double *hist);
+
 /* Additive-correction multigrid (Src/Solver/Additive) around CG smoothers. */
 typedef struct orc_ac orc_ac;
 

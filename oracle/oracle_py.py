@@ -64,6 +64,14 @@ def lib():
                            ctypes.c_double, ctypes.POINTER(OrcStats), _dp]
         for fn in (L.orc_cg_prec, L.orc_bicgs_prec, L.orc_cgs_prec):
             fn.argtypes = fn.argtypes + [ctypes.c_int]
+        L.orc_jacobi.restype = ctypes.c_int
+        L.orc_jacobi.argtypes = [ctypes.POINTER(OrcMat), _dp, _dp, _dp, ctypes.c_int, ctypes.c_int,
+                                 ctypes.c_double, ctypes.c_double, ctypes.POINTER(OrcStats), _dp]
+        L.orc_gauss_seidel.restype = ctypes.c_int
+        L.orc_gauss_seidel.argtypes = [ctypes.POINTER(OrcMat), _dp, _dp, _dp, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                       ctypes.POINTER(OrcStats), _dp]
         L.orc_ac_create.restype = ctypes.c_void_p
         L.orc_ac_create.argtypes = [ctypes.POINTER(OrcMat), ctypes.c_void_p, ctypes.c_double]
         L.orc_ac_destroy.argtypes = [ctypes.c_void_p]
@@ -180,8 +188,19 @@ def cg(P, b=None, x0=None, mini=1, maxit=20000, res_rat=1e-8, res_tol=1e-18, sca
     m = P.mat()
     args = (ctypes.byref(m), _p(x), _p(b), mini, maxit, res_rat, res_tol, scale, stalecount, P.dV,
             ctypes.byref(st), _p(h) if hist else None)
-    fn = {"cg": lib().orc_cg_prec, "bicgs": lib().orc_bicgs_prec, "cgs": lib().orc_cgs_prec}[solver]
-    fn(*args, PRECS[prec])
+    if solver == "jacobi":  # Jacobi::solve: no scale, no stale window, |r| = sqrt(r.r)
+        ci = np.ascontiguousarray(P.ci, dtype=np.float64)
+        lib().orc_jacobi(ctypes.byref(m), _p(ci), _p(x), _p(b), mini, maxit, res_rat, res_tol,
+                         ctypes.byref(st), _p(h) if hist else None)
+    elif solver == "gs":
+        ci = np.ascontiguousarray(P.ci, dtype=np.float64)
+        lib().orc_gauss_seidel(ctypes.byref(m), _p(ci), _p(x), _p(b), mini, maxit, res_rat,
+                               res_tol, scale, stalecount, P.dV, ctypes.byref(st),
+                               _p(h) if hist else None)
+    else:
+        fn = {"cg": lib().orc_cg_prec, "bicgs": lib().orc_bicgs_prec,
+              "cgs": lib().orc_cgs_prec}[solver]
+        fn(*args, PRECS[prec])
     out = dict(converged=st.converged, iterations=st.iterations, printed=st.printed,
                res0=st.res0, res=st.res, status=st.status)
     if hist:

@@ -32,7 +32,9 @@
  *               [--maxcyc C --guard 0|1 --cycle V|F|W] [--prec di|ic0|ic2|ic3] [--save NAME]
  *               [--step 1 --dt DT] [--convect F] --out PREFIX
  *
- * --solver cgs runs `CGS::solve` (cgs.cpp); --convect F adds the upwind
+ * --solver cgs runs `CGS::solve` (cgs.cpp), --solver jacobi `Jacobi::solve`
+ * and --solver gs `GaussSeidel::solve` (Src/Solver/Linear/Iterative);
+ * --convect F adds the upwind
  * convection of pbg_gen_convect to the fixture after the boundary
  * correction (a non-symmetric matrix, for BiCGS and CGS).
  *
@@ -395,11 +397,15 @@ int main(int argc, char **argv) {
   /* the drop-in: the engine's Krylov classes behind the reference's virtual */
   if (a.gpu && a.solver == "bicgs") solver = new pbg_psiboil::GpuBiCGS(d, pc, a.exact != 0);
   else if (a.gpu && a.solver == "cgs") solver = new pbg_psiboil::GpuCGS(d, pc, a.exact != 0);
+  else if (a.gpu && a.solver == "jacobi") solver = new pbg_psiboil::GpuJacobi(d, a.exact != 0);
+  else if (a.gpu && a.solver == "gs") solver = new pbg_psiboil::GpuGaussSeidel(d, a.exact != 0);
   else if (a.gpu) solver = new pbg_psiboil::GpuCG(d, pc, a.exact != 0);
   else
 #endif
   if (a.solver == "bicgs") solver = new BiCGS(d, pc);
   else if (a.solver == "cgs") solver = new CGS(d, pc);
+  else if (a.solver == "jacobi") solver = new Jacobi(d);
+  else if (a.solver == "gs") solver = new GaussSeidel(d);
   else solver = new CG(d, pc);
 
   Vector uvw(d);

@@ -27,6 +27,9 @@ PBG_OK = 0
 HOST, DEVICE = 0, 1
 NEUMANN, DIRICHLET = 0, 1
 SOLVER_CG, SOLVER_BICGS, SOLVER_AC, SOLVER_ENGINE, SOLVER_CGS = 0, 1, 2, 3, 4
+SOLVER_JACOBI, SOLVER_GAUSS_SEIDEL = 5, 6
+# pbg_result.status
+CONVERGED, MAXITER, STALE, BREAKDOWN, INITIAL, NAN, DIVERGED = 0, 1, 2, 3, 4, 5, 6
 FP64, MIXED = 0, 1
 CYCLE_NONE, CYCLE_V, CYCLE_F, CYCLE_W = -1, 1, 2, 4
 STATUS = {0: "converged", 1: "maxiter", 2: "stale", 3: "breakdown", 4: "initial", 5: "nan",
@@ -89,6 +92,7 @@ _SIGS = {
     "pbg_matrix_upload": (ctypes.c_int, [_vp] + [_vp] * 7 + [_ll, _ll, _ll, _ll, ctypes.c_int]),
     "pbg_matrix_download": (ctypes.c_int, [_vp] + [_vp] * 7 + [ctypes.c_int]),
     "pbg_active_upload": (ctypes.c_int, [_vp, _vp, _ll, _ll, _ll, _ll, ctypes.c_int]),
+    "pbg_ci_upload": (ctypes.c_int, [_vp, _vp, _ll, _ll, _ll, _ll, ctypes.c_int]),
     "pbg_assemble_pressure": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
     "pbg_assemble_mix": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_double, _vp, ctypes.c_int]),
     "pbg_divergence": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_double, _vp, ctypes.c_int]),
@@ -319,6 +323,14 @@ class Session:
         si, sj, sk = strides if strides else (ny * nz, nz, 1)
         _check(lib().pbg_active_upload(self._h, a.ctypes.data, si, sj, sk, offset, HOST))
 
+    def upload_ci(self, ci, strides=None, offset=0):
+        """The matrix's stored inverse central coefficient A.ci, read by Jacobi
+        and Gauss-Seidel (1/c until it is uploaded, and after every matrix change)."""
+        p, where = _ptr(ci)
+        nx, ny, nz = self.dims
+        si, sj, sk = strides if strides else (ny * nz, nz, 1)
+        _check(lib().pbg_ci_upload(self._h, p, si, sj, sk, offset, where))
+
     def assemble_pressure(self, rho, solid):
         """Pressure::discretize on the device (harmonic face density)."""
         pr, where = _ptr(rho)
@@ -477,6 +489,24 @@ class BiCGS(_Krylov):
 class CGS(_Krylov):
     """Conjugate gradient squared (Krylov/cgs.cpp), diagonal or IC preconditioner."""
     solver = SOLVER_CGS
+
+
+class Jacobi(_Krylov):
+    """Jacobi (Src/Solver/Linear/Iterative/jacobi.cpp): x = ci (r + c x) per sweep;
+    res and res0 are sqrt(r.r). Reads the session's A.ci (Session.upload_ci)."""
+    solver = SOLVER_JACOBI
+
+    def __init__(self, session, exact_sums=False):
+        super().__init__(session, "di", exact_sums)
+
+
+class GaussSeidel(_Krylov):
+    """Gauss-Seidel (Iterative/gaussseidel.cpp), lexicographic sweeps run as one
+    launch per hyperplane i + j + k (the sequential sweep's values)."""
+    solver = SOLVER_GAUSS_SEIDEL
+
+    def __init__(self, session, exact_sums=False):
+        super().__init__(session, "di", exact_sums)
 
 
 class AC:

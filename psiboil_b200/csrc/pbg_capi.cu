@@ -43,6 +43,8 @@ struct pbg_session {
   bool eng_dirty = true, eng_mixed = false;
   DBuf<double> dx, db, dscal, hist, seq;
   DBuf<double> frhs;               // pressure-step right-hand side (ncell)
+  DBuf<double> ci;                 // uploaded A.ci (Jacobi, Gauss-Seidel)
+  unsigned long long mat_gen = 0, ci_gen = ~0ull;  // ci is valid while ci_gen == mat_gen
   DBuf<unsigned long long> dlinf;
   double *hbuf = nullptr;          // pinned: 64 doubles
   double *px = nullptr, *pb = nullptr;  // pinned staging (ncell each)
@@ -374,6 +376,7 @@ int pbg_matrix_upload(pbg_session *s, const double *c, const double *w, const do
       if (dst[q]->p) PBG_CUDA(cudaMemcpyAsync(dst[q]->p, h[q].data(), N * 8, cudaMemcpyHostToDevice, s->stream));
     PBG_CUDA(cudaStreamSynchronize(s->stream));
     s->have_matrix = true;
+    ++s->mat_gen;
     invalidate(s);
     return PBG_OK;
   });
@@ -429,6 +432,28 @@ int pbg_active_upload(pbg_session *s, const int *aflag, long long si, long long 
   });
 }
 
+int pbg_ci_upload(pbg_session *s, const double *ci, long long si, long long sj, long long sk,
+                  long long offset, int where) {
+  if (!s || !ci) return fail(PBG_ERR_ARG, "NULL argument");
+  if (!s->have_matrix) return fail(PBG_ERR_STATE, "no matrix uploaded or assembled");
+  return guard(s, [&]() -> int {
+    const long long N = s->ncell();
+    if (s->ci.n != (size_t)N) s->ci.alloc(N);
+    if (where == PBG_HOST) {
+      std::vector<double> h(N);
+      gather(ci, h.data(), s->nx, s->ny, s->nz, si, sj, sk, offset);
+      PBG_CUDA(cudaMemcpyAsync(s->ci.p, h.data(), N * 8, cudaMemcpyHostToDevice, s->stream));
+      PBG_CUDA(cudaStreamSynchronize(s->stream));
+    } else {
+      k_gather<<<grid_for(N), kThreads, 0, s->stream>>>(ci, s->ci.p, s->nx, s->ny, s->nz, si, sj, sk,
+                                                         offset); note_launch();
+      PBG_CUDA(cudaGetLastError());
+    }
+    s->ci_gen = s->mat_gen;
+    return PBG_OK;
+  });
+}
+
 int pbg_assemble_pressure(pbg_session *s, const double *rho, const uint8_t *solid, int where) {
   if (!s || !rho || !solid) return fail(PBG_ERR_ARG, "NULL argument");
   return guard(s, [&]() -> int {
@@ -453,6 +478,7 @@ int pbg_assemble_pressure(pbg_session *s, const double *rho, const uint8_t *soli
     PBG_CUDA(cudaGetLastError());
     PBG_CUDA(cudaStreamSynchronize(s->stream));
     s->have_matrix = true;
+    ++s->mat_gen;
     invalidate(s);
     return PBG_OK;
   });
@@ -491,6 +517,7 @@ int pbg_assemble_mix(pbg_session *s, const double *col, double rho_a, double rho
     PBG_CUDA(cudaGetLastError());
     PBG_CUDA(cudaStreamSynchronize(s->stream));
     s->have_matrix = true;
+    ++s->mat_gen;
     invalidate(s);
     return PBG_OK;
   });
@@ -713,7 +740,8 @@ int solve_device(pbg_session *s, double *xd, const double *bd, const pbg_params 
   std::memset(&out, 0, sizeof(out));
   const double dV = s->dV;
   s->nhist = 0;
-  if (p->solver == PBG_SOLVER_CG || p->solver == PBG_SOLVER_BICGS || p->solver == PBG_SOLVER_CGS) {
+  if (p->solver == PBG_SOLVER_CG || p->solver == PBG_SOLVER_BICGS || p->solver == PBG_SOLVER_CGS ||
+      p->solver == PBG_SOLVER_JACOBI || p->solver == PBG_SOLVER_GAUSS_SEIDEL) {
     KrylovParams pr;
     pr.mini = p->min_iter; pr.maxit = p->max_iter;
     pr.stalecount = p->stalecount > kStaleMax ? kStaleMax : p->stalecount;
@@ -722,7 +750,12 @@ int solve_device(pbg_session *s, double *xd, const double *bd, const pbg_params 
     pr.seq = exact_terms(s, p);
     if (p->prec < 0 || p->prec > 3) return fail(PBG_ERR_ARG, "prec must be 0 (diagonal), 1 (IC0), 2 (IC2) or 3 (IC3)");
     pr.prec = p->prec;
-    const int kind = p->solver == PBG_SOLVER_CG ? 0 : p->solver == PBG_SOLVER_BICGS ? 1 : 2;
+    const int kind = p->solver == PBG_SOLVER_CG ? 0 : p->solver == PBG_SOLVER_BICGS ? 1
+                     : p->solver == PBG_SOLVER_CGS ? 2 : p->solver == PBG_SOLVER_JACOBI ? 3 : 4;
+    if (kind >= 3) {  // no preconditioner (iterative.h:15-31); A.ci if uploaded
+      pr.prec = 0;
+      pr.ci = s->ci_gen == s->mat_gen ? s->ci.p : nullptr;
+    }
     RefKrylovResult rr = ref_krylov_solve(s->A.view(), xd, bd, pr, kind,
                                           s->rkw, s->red, s->kst.p, s->hkst, s->hist.p, s->stream);
     out.status = rr.status;

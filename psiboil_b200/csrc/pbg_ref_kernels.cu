@@ -930,6 +930,142 @@ __global__ void k_ac_resnorm(MatView<double> A, const double *__restrict__ phi,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Jacobi::solve (Src/Solver/Linear/Iterative/jacobi.cpp:10-75) and
+// GaussSeidel::solve (gaussseidel.cpp:10-117). Both update x in place with
+// the matrix's stored inverse central coefficient ci and form r = b - A x
+// after every sweep. Jacobi measures sqrt(r.r) (jacobi.cpp:24,52,59-61);
+// Gauss-Seidel measures sqrt(dot_voldiv_avg(r, r)) / scale and keeps a stale
+// window (gaussseidel.cpp:24,68,85-105).
+//
+// Gauss-Seidel's sweep runs i, then j, then k (for_vijk) and reads the new
+// values of the cells before the current one and the old values of the
+// cells after it. Every neighbour of (i, j, k) lies on the hyperplane
+// i + j + k - 1 (those before it) or i + j + k + 1 (those after it), so one
+// launch per hyperplane h = i + j + k, in increasing h, computes every cell
+// from exactly the values the sequential sweep uses.
+// ---------------------------------------------------------------------------
+// all entries unreal (gaussseidel.cpp:28-33; CG also seeds the last with res0)
+__device__ void stale_fill_dev(KrylovState *st) {
+  int n = st->stalecount > kStaleMax ? kStaleMax : st->stalecount;
+  for (int q = 0; q < n; ++q) st->stale[q] = 1.0e24;  // boil::unreal
+}
+
+// the residual measure of the two solvers from the sum over cells
+__device__ __forceinline__ double it_res(double d, const KrylovState *st, int gs) {
+  return gs ? res_of(d, st) : __dsqrt_rn(d);
+}
+
+__global__ void k_it_init(MatView<double> A, const double *__restrict__ x,
+                          const double *__restrict__ b, double *__restrict__ r, KrylovState *st,
+                          double *part, unsigned *count, int gs) {
+  const long long N = A.ncell();
+  const double dV = st->dV;
+  double v[1] = {0.0};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    double rv = ref_bmax(A, p, q, x, b[p]);
+    r[p] = rv;
+    v[0] += gs ? voldiv(rv, rv, dV) : __dmul_rn(rv, rv);
+  }
+  double o[1];
+  if (grid_reduce<1>(v, part, count, o, st->seq, N)) {
+    const double res = it_res(o[0], st, gs);
+    st->res0 = res;
+    st->res = res;
+    st->iter = 0;
+    st->iterations = 0;
+    st->converged = 0;
+    st->pending_x = 0;
+    if (gs) stale_fill_dev(st);
+    if (res < st->res_tol) {  // jacobi.cpp:35, gaussseidel.cpp:43
+      st->done = 1;
+      st->converged = 1;
+      st->status = ST_INITIAL;
+    } else if (st->maxit <= 0) {
+      st->done = 1;
+      st->status = ST_MAXITER;
+    } else {
+      st->done = 0;
+      st->status = ST_RUNNING;
+    }
+  }
+}
+
+// x = ci (r + c x) with the r of the previous sweep (jacobi.cpp:42-44)
+__global__ void k_jacobi_x(long long N, const double *__restrict__ c, const double *__restrict__ ci,
+                           const double *__restrict__ r, double *__restrict__ x,
+                           const KrylovState *st) {
+  if (st->done) return;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x)
+    x[p] = __dmul_rn(ci[p], __dadd_rn(r[p], __dmul_rn(c[p], x[p])));
+}
+
+// the cells of hyperplane h: x = ci (b + w xw + e xe + s xs + n xn + b xb
+// + t xt), summed left to right (gaussseidel.cpp:50-60). One thread per
+// (i, j) column; k = h - i - j.
+__global__ void k_gs_plane(MatView<double> A, const double *__restrict__ ci,
+                           const double *__restrict__ b, double *x, int h, const KrylovState *st) {
+  if (st->done) return;
+  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
+  const long long nij = (long long)A.nx * A.ny;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nij;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / A.ny), j = (int)(t - (long long)i * A.ny);
+    const int k = h - i - j;
+    if (k < 0 || k >= A.nz) continue;
+    const long long p = ((long long)i * A.ny + j) * A.nz + k;
+    const Pos q{i, j, k};
+    Nb<double> a = coeffs(A, p, q);
+    double v = b[p];
+    v = __dadd_rn(v, __dmul_rn(a.w, ld0(x, p - SI, i > 0)));
+    v = __dadd_rn(v, __dmul_rn(a.e, ld0(x, p + SI, i < A.nx - 1)));
+    v = __dadd_rn(v, __dmul_rn(a.s, ld0(x, p - SJ, j > 0)));
+    v = __dadd_rn(v, __dmul_rn(a.n, ld0(x, p + SJ, j < A.ny - 1)));
+    v = __dadd_rn(v, __dmul_rn(a.b, ld0(x, p - 1, k > 0)));
+    v = __dadd_rn(v, __dmul_rn(a.t, ld0(x, p + 1, k < A.nz - 1)));
+    x[p] = __dmul_rn(ci[p], v);
+  }
+}
+
+// r = b - A x after a sweep, the residual measure and the exits
+// (jacobi.cpp:47-61, gaussseidel.cpp:63-105)
+__global__ void k_it_resid(MatView<double> A, const double *__restrict__ x,
+                           const double *__restrict__ b, double *__restrict__ r, KrylovState *st,
+                           double *hist, double *part, unsigned *count, int gs) {
+  if (st->done) return;
+  const int it = st->iter;
+  const long long N = A.ncell();
+  const double dV = st->dV;
+  double v[1] = {0.0};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    Pos q = pos_of(p, A.ny, A.nz);
+    double rv = ref_bmax(A, p, q, x, b[p]);
+    r[p] = rv;
+    v[0] += gs ? voldiv(rv, rv, dV) : __dmul_rn(rv, rv);
+  }
+  double o[1];
+  if (grid_reduce<1>(v, part, count, o, st->seq, N)) {
+    const double res = it_res(o[0], st, gs);
+    st->res = res;
+    if (hist && it < st->hist_cap) hist[it] = res;
+    const bool minok = it >= st->mini - 1;
+    if ((res < st->res_tol && minok) || (res < st->res0 * st->res_rat && minok)) {
+      st->done = 1; st->converged = 1; st->status = ST_CONVERGED; st->iterations = it + 1;
+    } else if (gs && stale_step_dev(st, res)) {
+      st->done = 1; st->status = ST_STALE; st->iterations = it + 1;
+    } else if (!(res == res)) {
+      st->done = 1; st->status = ST_NAN; st->iterations = it + 1;
+    } else {
+      st->iter = it + 1;
+      st->iterations = it + 1;
+      if (it + 1 >= st->maxit) { st->done = 1; st->status = ST_MAXITER; }
+    }
+  }
+}
 
 // ---------------------------------------------------------------------------
 // Host drivers
@@ -956,7 +1092,9 @@ __global__ void k_krylov_setup(KrylovState *st, KrylovParams pr, long long ncell
 
 void RefKrylovWork::ensure(size_t n, int solver) {
   auto fit = [n](DBuf<double> &b) { if (b.n < n) b.alloc(n); };
-  fit(r); fit(q); fit(pA); fit(pB); fit(mcd);
+  fit(r); fit(mcd);
+  if (solver >= 3) return;  // Jacobi, Gauss-Seidel: r and 1/c only
+  fit(q); fit(pA); fit(pB);
   if (solver >= 1) { fit(rt); fit(ph); fit(v); fit(s); fit(sh); fit(t); }
   if (solver == 2) fit(u);
 }
@@ -989,6 +1127,18 @@ void enqueue_ref_setup(const MatView<double> &A, double *x, const double *b, con
   const int g = pr.seq ? grid_exact(N) : grid_for(N);
   w.ensure((size_t)N, solver);
   k_krylov_setup<<<1, 1, 0, s>>>(st, pr, N); note_launch();
+  if (solver >= 3) {  // Jacobi, Gauss-Seidel: ci as stored with the matrix, else 1/c
+    w.rhs = b;
+    w.ci = pr.ci;
+    if (!w.ci) {
+      k_recip<<<grid_for(N), kThreads, 0, s>>>(N, A.c, w.mcd.p); note_launch();
+      w.ci = w.mcd.p;
+    }
+    k_it_init<<<g, kThreads, 0, s>>>(A, x, b, w.r.p, st, red.slot_part(0), red.slot_count(0),
+                                     solver == 4 ? 1 : 0); note_launch();
+    PBG_CUDA(cudaGetLastError());
+    return;
+  }
   PBG_CUDA(cudaMemsetAsync(w.pA.p, 0, sizeof(double) * N, s));
   if (solver >= 1) {
     PBG_CUDA(cudaMemsetAsync(w.v.p, 0, sizeof(double) * N, s));
@@ -1027,6 +1177,22 @@ void enqueue_ref_iters(const MatView<double> &A, double *x, int solver, int coun
   double *P0 = red.slot_part(0), *P1 = red.slot_part(1);
   unsigned *C0 = red.slot_count(0), *C1 = red.slot_count(1);
   const int diag = prec > 0 ? 0 : 1;
+  if (solver >= 3) {  // Jacobi, Gauss-Seidel
+    const int gs = solver == 4 ? 1 : 0;
+    const int H = A.nx + A.ny + A.nz - 2, gp = grid_for((long long)A.nx * A.ny);
+    for (int it = 0; it < count; ++it) {
+      if (gs) {
+        for (int h = 0; h < H; ++h) {
+          k_gs_plane<<<gp, kThreads, 0, s>>>(A, w.ci, w.rhs, x, h, st); note_launch();
+        }
+      } else {
+        k_jacobi_x<<<grid_for(N), kThreads, 0, s>>>(N, A.c, w.ci, w.r.p, x, st); note_launch();
+      }
+      k_it_resid<<<g, kThreads, 0, s>>>(A, x, w.rhs, w.r.p, st, hist, P0, C0, gs); note_launch();
+    }
+    PBG_CUDA(cudaGetLastError());
+    return;
+  }
   IcFactor M{};
   if (prec > 0) M = w.ic(prec, (size_t)N);
   for (int it = 0; it < count; ++it) {

@@ -21,12 +21,15 @@ struct KrylovParams {
   int mini, maxit, stalecount, hist_cap;
   double res_rat, res_tol, scale, dV;
   double *seq = nullptr;   // exact-order reduction terms (2 x ncell), null: tree
+  const double *ci = nullptr;  // Jacobi / Gauss-Seidel: the matrix's stored 1/c (null: 1/c here)
 };
 
-// solver codes of the drivers below: 0 CG, 1 BiCGS, 2 CGS
+// solver codes of the drivers below: 0 CG, 1 BiCGS, 2 CGS, 3 Jacobi,
+// 4 Gauss-Seidel
 struct RefKrylovWork {
   DBuf<double> r, q, pA, pB, rt, ph, v, s, sh, t, u;
   DBuf<double> mcd;                               // 1 / c (the diagonal preconditioner)
+  const double *rhs = nullptr, *ci = nullptr;     // Jacobi / Gauss-Seidel operands of a solve
   DBuf<double> z, mc, mw, ms, mb, mtw, mts, mnw;  // IC preconditioner
   void ensure(size_t n, int solver);
   IcFactor ic(int kind, size_t n);

@@ -92,3 +92,18 @@ def test_reference_with_gpu_bicgs_cgs_is_bit_exact(case, args, key):
                           "--gpu", "1", "--exact", "1"])
     assert np.array_equal(x, g[key + "_x"])
     assert int(meta["iterations"][0]) == int(g[key + "_iterations"])
+
+
+@pytest.mark.skipif(not os.path.exists(EXE), reason="GPU-backed reference harness not built")
+@pytest.mark.parametrize("case,args", [
+    ("cyl24", ["--kind", "cyl", "--n", "24", "--nb", "3", "--rmin", "2.0", "--rmax", "4.0", "--rc", "5.0"]),
+    ("odd15", ["--kind", "batch", "--index", "40", "--n2d", "0", "--s3", "15", "16"])])
+@pytest.mark.parametrize("solver", ["jacobi", "gs"])
+def test_reference_with_gpu_stationary_is_bit_exact(case, args, solver):
+    """`new GpuGaussSeidel(d)` / `new GpuJacobi(d)` in place of the reference's
+    GaussSeidel / Jacobi behind Centered::solve; A.ci goes up with the matrix."""
+    g = load(case)
+    x, meta = run(args + ["--seed", "7", "--solver", solver, "--resrat", "0.01", "--maxit", "2000",
+                          "--gpu", "1", "--exact", "1"])
+    assert np.array_equal(x, g[solver + "_x"])
+    assert int(meta["iterations"][0]) == int(g[solver + "_iterations"])

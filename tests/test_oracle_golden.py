@@ -21,20 +21,25 @@ def _krylov_runs():
     out = []
     for n in NAMES:
         for key in load(n):
-            if key.endswith("_x") and key.split("_")[0] in ("cg", "bicgs", "cgs"):
+            if key.endswith("_x") and key.split("_")[0] in ("cg", "bicgs", "cgs", "jacobi", "gs"):
                 out.append((n, key[:-2]))
     return out
 
 
 @pytest.mark.parametrize("name,run", _krylov_runs())
 def test_krylov_bit_exact(oracle, name, run):
-    """CG, BiCGS and CGS, with the diagonal or an IC preconditioner, on
-    symmetric and convected (non-symmetric) fixtures."""
+    """CG, BiCGS and CGS, with the diagonal or an IC preconditioner, and
+    Jacobi and Gauss-Seidel (with the reference's stored ci), on symmetric
+    and convected (non-symmetric) fixtures."""
     g = load(name)
     P = problem_of(g, oracle)
     parts = run.split("_")
     solver, prec = parts[0], (parts[1] if len(parts) > 1 else "di")
-    x, st = oracle.cg(P, res_rat=1e-8, maxit=20000, solver=solver, prec=prec)
+    rr, mi = 1e-8, 20000
+    if run + "_maxit" in g:
+        rr, mi = float(g[run + "_resrat"]), int(g[run + "_maxit"])
+        assert np.array_equal(P.ci, g["ci"])
+    x, st = oracle.cg(P, res_rat=rr, maxit=mi, solver=solver, prec=prec)
     assert st["printed"] == int(g[run + "_iterations"])
     assert st["converged"] == int(g[run + "_converged"])
     assert np.array_equal(x, g[run + "_x"], equal_nan=True)
