@@ -234,6 +234,20 @@ int pbg_project(pbg_session *s, const double *p, const double *col, double rho_a
 int pbg_pressure_step(pbg_session *s, const double *col, double rho_a, double rho_b,
                       const uint8_t *solid, double dt, double *u, double *v, double *w,
                       double *p, int where, const pbg_params *params, pbg_result *res);
+/* An immersed body with cut cells for the four functions above (the
+ * reference's Body after Domain(gx, gy, gz, &body) has cut it): fV the
+ * fluid volume fraction of every cell (Body::fV(i,j,k); 0 inside the body,
+ * between 0 and 1 in a cut cell), fS the face fractions of every cell as
+ * Body::fSw..fSt(i,j,k) return them, six planes of ncell in the order
+ * w e s n b t (only the cut cells' are read). The body's cut-cell list is
+ * its cut cells (0 < fV < 1). With a body those functions take solid =
+ * NULL and follow the reference's body branches: discretize's cut-cell
+ * fractions and off-cell decoupling (pressure_discretize.cpp:72-119; the
+ * matrix is then stored in the seven-array form, as the two cells of a
+ * face carry their own fractions), update_rhs's face fractions (:34-43)
+ * and project's fluid-only faces. Cells on the domain boundary must not be
+ * cut (PBG_ERR_UNSUPPORTED). fV = NULL removes the body. */
+int pbg_body_upload(pbg_session *s, const double *fV, const double *fS, int where);
 
 /* Solve A x = b with x as initial guess and result (x updated in place,
  * b read only), compact layout. The reference-parity solvers follow

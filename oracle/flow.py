@@ -100,11 +100,39 @@ def _cell_density(col, rho_a, rho_b, dims):
     return mix_density(np.asarray(col, dtype=np.float64).reshape(dims), rho_a, rho_b)
 
 
-def assemble_mix(dims, h, bc, col, rho_a, rho_b, solid=None):
+# the six neighbour directions: matrix key, axis, shift, plane of fS
+_DIRS = [("w", 0, -1, 0), ("e", 0, 1, 1), ("s", 1, -1, 2), ("n", 1, 1, 3), ("b", 2, -1, 4),
+         ("t", 2, 1, 5)]
+
+
+def _pair(axis, shift):
+    """Index of the cells that have the neighbour (axis, shift) inside the
+    domain, and of those neighbours."""
+    me = [slice(None)] * 3
+    nb = [slice(None)] * 3
+    me[axis] = slice(1, None) if shift < 0 else slice(None, -1)
+    nb[axis] = slice(None, -1) if shift < 0 else slice(1, None)
+    return tuple(me), tuple(nb)
+
+
+def body_masks(body, dims):
+    """off (fV == 0, Body::off_p) and cut (0 < fV < 1, Body::cut_p) cells and
+    the face fractions (6, nx, ny, nz) of a body given as fV and fS."""
+    fV = np.asarray(body["fV"], dtype=np.float64).reshape(dims)
+    fS = np.asarray(body["fS"], dtype=np.float64).reshape((6,) + tuple(dims))
+    return fV == 0.0, (fV > 0.0) & (fV < 1.0), fS
+
+
+def assemble_mix(dims, h, bc, col, rho_a, rho_b, solid=None, body=None):
     """Pressure matrix of a two-phase mixture: dict c, w, e, s, n, b, t, ci
     (flat, compact layout). col None: a single fluid of density rho_a
     (Property::value(Comp) of a constant property is the constant,
-    property_value.cpp:18-21). bc: imin..kmax, 0 Neumann / 1 Dirichlet."""
+    property_value.cpp:18-21). bc: imin..kmax, 0 Neumann / 1 Dirichlet.
+    body: dict fV, fS of a cut body (the reference's Body after cutting):
+    pressure_discretize.cpp:72-119 over the body's cut-cell list (its cut
+    cells): a cut cell's coupling to a cut neighbour times its own face
+    fraction, couplings between a listed cell and an off cell zeroed both
+    ways, c of every cell not off recomputed."""
     nx, ny, nz = dims
     hx = (h * h) / h
     rc = _cell_density(col, rho_a, rho_b, dims)
@@ -139,7 +167,18 @@ def assemble_mix(dims, h, bc, col, rho_a, rho_b, solid=None):
              n=gy[:, 1:] / fy[:, 1:], b=gz[:, :, :-1] / fz[:, :, :-1], t=gz[:, :, 1:] / fz[:, :, 1:])
     c = A["w"] + A["e"] + A["s"] + A["n"] + A["b"] + A["t"]
     sol = None
-    if solid is not None and np.any(solid):
+    if body is not None and np.any(body_masks(body, dims)[1]):
+        off, cut, fS = body_masks(body, dims)
+        for key, axis, shift, d in _DIRS:
+            me, nb = _pair(axis, shift)
+            a = A[key][me]
+            a = np.where(cut[me] & cut[nb], a * fS[d][me], a)
+            a = np.where((cut[me] | cut[nb]) & (off[me] | off[nb]), 0.0, a)
+            A[key][me] = a
+        c2 = A["w"] + A["e"] + A["s"] + A["n"] + A["b"] + A["t"]
+        c = np.where(off, c, c2)
+        sol = off
+    elif solid is not None and np.any(solid):
         # faces between fluid and solid cells zeroed on both sides; c of
         # fluid cells recomputed (pressure_discretize.cpp:91-117)
         sol = np.asarray(solid).reshape(dims).astype(bool)
@@ -173,7 +212,7 @@ def assemble_mix(dims, h, bc, col, rho_a, rho_b, solid=None):
     return out
 
 
-def divergence(dims, h, dt, u, v, w, solid=None):
+def divergence(dims, h, dt, u, v, w, solid=None, body=None):
     """Right-hand side of the pressure equation from face velocities
     (flat, compact layout). solid: a voxel body, the immersed-body branch
     of update_rhs (pressure_update_rhs.cpp:65-101; every fluid cell uncut,
@@ -185,8 +224,15 @@ def divergence(dims, h, dt, u, v, w, solid=None):
     u = np.asarray(u).reshape(nx + 1, ny, nz)
     v = np.asarray(v).reshape(nx, ny + 1, nz)
     w = np.asarray(w).reshape(nx, ny, nz + 1)
-    terms = [(1, a * u[:-1]), (-1, a * u[1:]), (1, a * v[:, :-1]), (-1, a * v[:, 1:]),
-             (1, a * w[:, :, :-1]), (-1, a * w[:, :, 1:])]
+    ad = [a] * 6
+    if body is not None and np.any(body_masks(body, dims)[1]):
+        # face areas times the cell's face fractions (pressure_update_rhs.cpp:
+        # 34-43; an uncut fluid cell's are 1), then the branch below
+        off, cut, fS = body_masks(body, dims)
+        ad = [np.where(cut, a * fS[d], a) for d in range(6)]
+        solid = off
+    terms = [(1, ad[0] * u[:-1]), (-1, ad[1] * u[1:]), (1, ad[2] * v[:, :-1]), (-1, ad[3] * v[:, 1:]),
+             (1, ad[4] * w[:, :, :-1]), (-1, ad[5] * w[:, :, 1:])]
     if solid is None or not np.any(solid):
         f = 0.0 + terms[0][1]
         for sign, t in terms[1:]:
@@ -271,15 +317,19 @@ class StepProblem:
         return m
 
 
-def step(P, dt, res_rat=1e-10, maxit=20000, solver="cg", stream=0, bc=None):
+def step(P, dt, res_rat=1e-10, maxit=20000, solver="cg", stream=0, bc=None, body=None):
     """One pressure-correction step: assemble, divergence, Krylov solve from
     p = 0 with scale dti (centered_solve.cpp:25-31), project. Returns a dict
-    of A, b, x, u, v, w and the solver's statistics."""
+    of A, b, x, u, v, w and the solver's statistics. body: dict fV, fS of a
+    cut body (then P's voxel solid is not used)."""
     col, u, v, w, ra, rb, bc0 = flow_state(P, stream)
     bc = list(bc0 if bc is None else bc)
     sol = P.solid if np.any(P.solid) else None
-    A = assemble_mix(P.dims, P.h, bc, col, ra, rb, solid=sol)
-    b = divergence(P.dims, P.h, dt, u, v, w, solid=sol)
+    if body is not None:
+        off, cut, _ = body_masks(body, P.dims)
+        sol = off.reshape(-1) if np.any(cut) else None
+    A = assemble_mix(P.dims, P.h, bc, col, ra, rb, solid=sol, body=body)
+    b = divergence(P.dims, P.h, dt, u, v, w, solid=sol, body=body)
     sp = StepProblem(P.dims, P.h, A, b)
     x, st = op.cg(sp, b=b, res_rat=res_rat, res_tol=1e-18, maxit=maxit, scale=1.0 / dt,
                   solver=solver)
@@ -288,9 +338,11 @@ def step(P, dt, res_rat=1e-10, maxit=20000, solver="cg", stream=0, bc=None):
                 rho=(ra, rb), bc=bc)
 
 
-def run_reference_step(P, dt, res_rat=1e-10, maxit=20000, solver="cg", timeout=600):
+def run_reference_step(P, dt, res_rat=1e-10, maxit=20000, solver="cg", timeout=600, body=0.0):
     """The compiled reference's own step (ref_harness --step 1) on P's
-    workload: dict of A, b, x, u, v, w and the harness summary."""
+    workload: dict of A, b, x, u, v, w and the harness summary. body > 0: a
+    sphere of that radius in cells, cut by the reference's Body; its fV and
+    fS come back as well."""
     import os
     import shutil
     import subprocess
@@ -306,7 +358,7 @@ def run_reference_step(P, dt, res_rat=1e-10, maxit=20000, solver="cg", timeout=6
                "--s2", str(a["s2"][0]), str(a["s2"][1]), "--s3", str(a["s3"][0]),
                str(a["s3"][1]), "--seed", str(P.seed), "--solver", solver,
                "--resrat", repr(res_rat), "--maxit", str(maxit), "--step", "1",
-               "--dt", repr(dt), "--out", out]
+               "--dt", repr(dt), "--out", out, "--body", repr(float(body))]
         subprocess.run(cmd, check=True, capture_output=True, timeout=timeout)
         meta = {}
         for line in open(out + ".txt"):
@@ -322,6 +374,9 @@ def run_reference_step(P, dt, res_rat=1e-10, maxit=20000, solver="cg", timeout=6
                    u=np.fromfile(out + ".u", dtype=np.float64).reshape(nx + 1, ny, nz),
                    v=np.fromfile(out + ".v", dtype=np.float64).reshape(nx, ny + 1, nz),
                    w=np.fromfile(out + ".w", dtype=np.float64).reshape(nx, ny, nz + 1))
+        if body > 0.0:
+            bd = np.fromfile(out + ".body", dtype=np.float64).reshape(8, N)
+            res["body"] = dict(fV=bd[0].copy(), fS=bd[1:7].copy(), listed=bd[7].copy())
         return res
     finally:
         shutil.rmtree(tmp, ignore_errors=True)

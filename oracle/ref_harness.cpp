@@ -55,6 +55,7 @@
 #endif
 
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -73,7 +74,7 @@ struct Args {
   double resrat = 1e-8;
   int maxit = 20000, maxcyc = 20, guard = 1, dump = 1, repeat = 1, gpu = 0, exact = 1;
   int step = 0;
-  double dt = 1.0, convect = 0.0;
+  double dt = 1.0, convect = 0.0, body = 0.0;
 };
 
 Args parse(int argc, char **argv) {
@@ -97,6 +98,7 @@ Args parse(int argc, char **argv) {
     else if (k == "--s3") { a.s3lo = std::atoi(nxt()); a.s3hi = std::atoi(nxt()); }
     else if (k == "--seed") a.seed = std::strtoull(nxt(), nullptr, 10);
     else if (k == "--solver") a.solver = nxt();
+    else if (k == "--body") a.body = std::atof(nxt());
     else if (k == "--resrat") a.resrat = std::atof(nxt());
     else if (k == "--maxit") a.maxit = std::atoi(nxt());
     else if (k == "--maxcyc") a.maxcyc = std::atoi(nxt());
@@ -221,6 +223,34 @@ class Probe : public Pressure {
     for (auto *s : arr) dump_cells(*s, D, f);
   }
   void dump_rhs(const pbg_problem_desc &D, std::ofstream &f) const { dump_cells(fnew, D, f); }
+  /* the immersed body as the pressure equation sees it: fV of every cell,
+   * the six face fractions fSw..fSt(i,j,k) of every cell (the accessors'
+   * values, planes w e s n b t), and 1.0 for the cells of the cut-cell list
+   * (Body::ijk(cc), cc < nccells()) */
+  void dump_body(const pbg_problem_desc &D, std::ofstream &f) const {
+    const int B = boil::BW;
+    const size_t N = pbg_ncells(&D);
+    std::vector<double> out(8 * N, 0.0);
+    const Body &bd = dom->ibody();
+    auto at = [&](int i, int j, int k) { return ((size_t)i * D.ny + j) * D.nz + k; };
+    for (int i = 0; i < D.nx; ++i)
+      for (int j = 0; j < D.ny; ++j)
+        for (int k = 0; k < D.nz; ++k) {
+          const int I = i + B, J = j + B, K = k + B;
+          const size_t p = at(i, j, k);
+          out[p] = bd.fV(I, J, K);
+          out[1 * N + p] = bd.fSw(I, J, K); out[2 * N + p] = bd.fSe(I, J, K);
+          out[3 * N + p] = bd.fSs(I, J, K); out[4 * N + p] = bd.fSn(I, J, K);
+          out[5 * N + p] = bd.fSb(I, J, K); out[6 * N + p] = bd.fSt(I, J, K);
+        }
+    for (int cc = 0; cc < bd.nccells(); ++cc) {
+      int i, j, k;
+      bd.ijk(cc, &i, &j, &k);
+      if (i >= B && i < D.nx + B && j >= B && j < D.ny + B && k >= B && k < D.nz + B)
+        out[7 * N + at(i - B, j - B, k - B)] = 1.0;
+    }
+    f.write((const char *)out.data(), out.size() * sizeof(double));
+  }
 
   static void dump_cells(const Scalar &s, const pbg_problem_desc &D, std::ofstream &f) {
     const int B = boil::BW;
@@ -231,6 +261,44 @@ class Probe : public Pressure {
     f.write((const char *)out.data(), out.size() * sizeof(double));
   }
 };
+
+/* A closed sphere as an ASCII STL: latitude/longitude quads split in two
+ * triangles, vertices counter-clockwise seen from outside (the pole rows
+ * give one triangle each). */
+void write_sphere_stl(const std::string &path, double cx, double cy, double cz, double r) {
+  const int nt = 24, np = 48;
+  const double pi = 3.14159265358979323846;
+  auto pt = [&](int it, int ip, double *v) {
+    const double th = pi * it / nt, ph = 2.0 * pi * ip / np;
+    v[0] = cx + r * std::sin(th) * std::cos(ph);
+    v[1] = cy + r * std::sin(th) * std::sin(ph);
+    v[2] = cz + r * std::cos(th);
+  };
+  std::ofstream f(path);
+  f.precision(17);
+  f << "solid sphere\n";
+  auto tri = [&](const double *a, const double *b, const double *c) {
+    double u[3], w[3], n[3];
+    for (int q = 0; q < 3; ++q) { u[q] = b[q] - a[q]; w[q] = c[q] - a[q]; }
+    n[0] = u[1] * w[2] - u[2] * w[1];
+    n[1] = u[2] * w[0] - u[0] * w[2];
+    n[2] = u[0] * w[1] - u[1] * w[0];
+    const double l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    f << " facet normal " << n[0] / l << " " << n[1] / l << " " << n[2] / l << "\n  outer loop\n";
+    f << "   vertex " << a[0] << " " << a[1] << " " << a[2] << "\n";
+    f << "   vertex " << b[0] << " " << b[1] << " " << b[2] << "\n";
+    f << "   vertex " << c[0] << " " << c[1] << " " << c[2] << "\n";
+    f << "  endloop\n endfacet\n";
+  };
+  for (int it = 0; it < nt; ++it)
+    for (int ip = 0; ip < np; ++ip) {
+      double a[3], b[3], c[3], d[3];
+      pt(it, ip, a); pt(it + 1, ip, b); pt(it + 1, ip + 1, c); pt(it, ip + 1, d);
+      if (it > 0) tri(a, b, d);        /* (t0,p0) (t1,p0) (t0,p1) */
+      if (it < nt - 1) tri(d, b, c);   /* (t0,p1) (t1,p0) (t1,p1) */
+    }
+  f << "endsolid sphere\n";
+}
 
 /* Face extents of one component in the layouts of pbg_gen_flow. */
 void face_dims(const pbg_problem_desc &D, int m, int &ex, int &ey, int &ez) {
@@ -277,7 +345,18 @@ int run_step(const Args &a, const pbg_problem_desc &D) {
   Grid1D gy(Range<real>(0.0, D.ny * h), Range<real>(h, h), D.ny, Periodic::no());
   Grid1D *gz = (D.nz > 1) ? new Grid1D(Range<real>(0.0, D.nz * h), Range<real>(h, h), D.nz, Periodic::no())
                           : new Grid1D(h);
-  Domain d(gx, gy, *gz);
+  /* --body R: a sphere of radius R cells inside the domain, written as an
+   * ASCII STL and cut by the reference's own Body (Body::Body(name),
+   * Domain(gx, gy, gz, &body)) */
+  Body *body = nullptr;
+  if (a.body > 0.0) {
+    const std::string stl = a.out + ".stl";
+    write_sphere_stl(stl, 0.5 * D.nx * h + 0.37 * h, 0.5 * D.ny * h + 0.21 * h,
+                     0.5 * D.nz * h + 0.13 * h, a.body * h);
+    body = new Body(stl);
+  }
+  Domain *dp = body ? new Domain(gx, gy, *gz, body) : new Domain(gx, gy, *gz);
+  Domain &d = *dp;
   Times time(1, a.dt);
   const Prec pc = a.prec == "ic0" ? Prec::ic0() : a.prec == "ic2" ? Prec::ic2()
                  : a.prec == "ic3" ? Prec::ic3() : Prec::di();
@@ -339,6 +418,10 @@ int run_step(const Args &a, const pbg_problem_desc &D) {
   {
     std::ofstream fa(a.out + ".A", std::ios::binary);
     pr.dump_matrix(D, fa);
+    if (body) {
+      std::ofstream fbd(a.out + ".body", std::ios::binary);
+      pr.dump_body(D, fbd);
+    }
     std::ofstream fb(a.out + ".b", std::ios::binary);
     pr.dump_rhs(D, fb);
     std::ofstream fx(a.out + ".x", std::ios::binary);

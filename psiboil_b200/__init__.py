@@ -93,6 +93,7 @@ _SIGS = {
     "pbg_matrix_download": (ctypes.c_int, [_vp] + [_vp] * 7 + [ctypes.c_int]),
     "pbg_active_upload": (ctypes.c_int, [_vp, _vp, _ll, _ll, _ll, _ll, ctypes.c_int]),
     "pbg_ci_upload": (ctypes.c_int, [_vp, _vp, _ll, _ll, _ll, _ll, ctypes.c_int]),
+    "pbg_body_upload": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
     "pbg_assemble_pressure": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
     "pbg_assemble_mix": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_double, _vp, ctypes.c_int]),
     "pbg_divergence": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_double, _vp, ctypes.c_int]),
@@ -364,6 +365,20 @@ class Session:
         _check(lib().pbg_project(self._h, pp, _ptr(col)[0], rho_a, rho_b, _ptr(solid)[0], dt,
                                  _ptr(u)[0], _ptr(v)[0], _ptr(w)[0], where))
         return u, v, w
+
+    def upload_body(self, fV, fS):
+        """A cut immersed body for the flow functions (the reference's Body:
+        fV per cell, fS the six face fractions per cell, planes w e s n b t);
+        fV None removes it. With a body the flow functions take solid=None."""
+        if fV is None:
+            _check(lib().pbg_body_upload(self._h, None, None, HOST))
+            return
+        pv, where = _ptr(fV)
+        if where == HOST:
+            fV = np.ascontiguousarray(fV, dtype=np.float64)
+            fS = np.ascontiguousarray(fS, dtype=np.float64)
+            pv = fV.ctypes.data
+        _check(lib().pbg_body_upload(self._h, pv, _ptr(fS)[0], where))
 
     def pressure_step(self, col, rho_a, rho_b, dt, u, v, w, p, params, solid=None):
         """Assemble, divergence, solve and project in one call; u, v, w and

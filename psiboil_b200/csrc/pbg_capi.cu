@@ -44,6 +44,12 @@ struct pbg_session {
   DBuf<double> dx, db, dscal, hist, seq;
   DBuf<double> frhs;               // pressure-step right-hand side (ncell)
   DBuf<double> ci;                 // uploaded A.ci (Jacobi, Gauss-Seidel)
+  // immersed body with cut cells (pbg_body_upload): off cells, the index of
+  // each cut cell in bfs (-1: not cut) and six face fractions per cut cell
+  DBuf<uint8_t> boff;
+  DBuf<int> bidx;
+  DBuf<double> bfs;
+  long long ncut = 0;
   unsigned long long mat_gen = 0, ci_gen = ~0ull;  // ci is valid while ci_gen == mat_gen
   DBuf<unsigned long long> dlinf;
   double *hbuf = nullptr;          // pinned: 64 doubles
@@ -70,6 +76,26 @@ int fail(int code, const std::string &m) {
   g_err = m;
   return code;
 }
+
+// The solid mask and cut-cell data a flow kernel gets: the caller's voxel
+// mask, or the session's body when it has cut cells (a body without cut
+// cells changes nothing in the reference: every body branch is guarded by
+// nccells() > 0).
+struct BodyArgs {
+  const uint8_t *off = nullptr;
+  const int *idx = nullptr;
+  const double *fs = nullptr;
+};
+int body_args(const pbg_session *s, const uint8_t *solid_dev, BodyArgs &b) {
+  b.off = solid_dev;
+  if (s->ncut == 0) return PBG_OK;
+  if (solid_dev) return fail(PBG_ERR_ARG, "the session holds a body: pass solid = NULL");
+  b.off = s->boff.p;
+  b.idx = s->bidx.p;
+  b.fs = s->bfs.p;
+  return PBG_OK;
+}
+
 
 template <typename F>
 int guard(pbg_session *s, F &&f) {
@@ -454,6 +480,48 @@ int pbg_ci_upload(pbg_session *s, const double *ci, long long si, long long sj, 
   });
 }
 
+int pbg_body_upload(pbg_session *s, const double *fV, const double *fS, int where) {
+  if (!s) return fail(PBG_ERR_ARG, "session is NULL");
+  if (!fV) {  // no body
+    s->boff.release(); s->bidx.release(); s->bfs.release();
+    s->ncut = 0;
+    return PBG_OK;
+  }
+  if (!fS) return fail(PBG_ERR_ARG, "fS is NULL");
+  return guard(s, [&]() -> int {
+    const long long N = s->ncell();
+    std::vector<double> v(N), f(6 * N);
+    if (where == PBG_HOST) {
+      std::memcpy(v.data(), fV, N * 8);
+      std::memcpy(f.data(), fS, 6 * N * 8);
+    } else {
+      PBG_CUDA(cudaMemcpy(v.data(), fV, N * 8, cudaMemcpyDeviceToHost));
+      PBG_CUDA(cudaMemcpy(f.data(), fS, 6 * N * 8, cudaMemcpyDeviceToHost));
+    }
+    std::vector<uint8_t> off(N);
+    std::vector<int> idx(N, -1);
+    std::vector<double> fs;
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    for (long long p = 0; p < N; ++p) {
+      off[p] = v[p] == 0.0 ? 1 : 0;          // Body::off_p (body_interface.cpp:131-137)
+      if (!(v[p] > 0.0 && v[p] < 1.0)) continue;  // Body::cut_p (:56-61)
+      const int i = (int)(p / ((long long)ny * nz)), j = (int)(p / nz % ny), k = (int)(p % nz);
+      if (i == 0 || i == nx - 1 || j == 0 || j == ny - 1 || (nz > 1 && (k == 0 || k == nz - 1)))
+        return fail(PBG_ERR_UNSUPPORTED, "a cut cell on the domain boundary");
+      idx[p] = (int)(fs.size() / 6);
+      for (int d = 0; d < 6; ++d) fs.push_back(f[(size_t)d * N + p]);
+    }
+    s->ncut = (long long)(fs.size() / 6);
+    s->boff.alloc(N);
+    s->bidx.alloc(N);
+    s->bfs.alloc(fs.empty() ? 6 : fs.size());
+    PBG_CUDA(cudaMemcpy(s->boff.p, off.data(), N, cudaMemcpyHostToDevice));
+    PBG_CUDA(cudaMemcpy(s->bidx.p, idx.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+    if (!fs.empty()) PBG_CUDA(cudaMemcpy(s->bfs.p, fs.data(), fs.size() * 8, cudaMemcpyHostToDevice));
+    return PBG_OK;
+  });
+}
+
 int pbg_assemble_pressure(pbg_session *s, const double *rho, const uint8_t *solid, int where) {
   if (!s || !rho || !solid) return fail(PBG_ERR_ARG, "NULL argument");
   return guard(s, [&]() -> int {
@@ -506,13 +574,20 @@ int pbg_assemble_mix(pbg_session *s, const double *col, double rho_a, double rho
         sp = dsol.p;
       }
     }
+    BodyArgs bd;
+    if (int rc = body_args(s, sp, bd)) return rc;
     Mat64 &A = s->A;
-    A.nx = s->nx; A.ny = s->ny; A.nz = s->nz; A.sym = true;
+    // a cut body's face fractions differ between the two cells of a face:
+    // the seven-array form
+    const bool sym = bd.idx == nullptr;
+    A.nx = s->nx; A.ny = s->ny; A.nz = s->nz; A.sym = sym;
     if (A.c.n != (size_t)N) { A.c.alloc(N); A.w.alloc(N); A.s.alloc(N); A.b.alloc(N); }
-    A.e.release(); A.n.release(); A.t.release();
+    if (sym) { A.e.release(); A.n.release(); A.t.release(); }
+    else if (A.e.n != (size_t)N) { A.e.alloc(N); A.n.alloc(N); A.t.alloc(N); }
     k_assemble_mix<<<grid_for(N), kThreads, 0, s->stream>>>(
         flow_geo(s), s->nx, s->ny, s->nz, s->h, make_int4(s->bc[0], s->bc[1], s->bc[2], s->bc[3]),
-        make_int2(s->bc[4], s->bc[5]), cp, rho_a, rho_b, sp, A.c.p, A.w.p, A.s.p, A.b.p, s->aflag.p);
+        make_int2(s->bc[4], s->bc[5]), cp, rho_a, rho_b, bd.off, bd.idx, bd.fs, A.c.p, A.w.p, A.s.p, A.b.p,
+        A.e.p, A.n.p, A.t.p, s->aflag.p);
     note_launch();
     PBG_CUDA(cudaGetLastError());
     PBG_CUDA(cudaStreamSynchronize(s->stream));
@@ -590,10 +665,12 @@ int pbg_divergence(pbg_session *s, const double *u, const double *v, const doubl
         sp = dsol.p;
       }
     }
+    BodyArgs bd;
+    if (int rc = body_args(s, sp, bd)) return rc;
     const double dti = 1.0 / dt;
     const double a = (s->h * s->h) * dti;
-    k_divergence<<<grid_for(N), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, a, fa.d[0], fa.d[1], fa.d[2], sp,
-                                                          r);
+    k_divergence<<<grid_for(N), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, a, fa.d[0], fa.d[1],
+                                                          fa.d[2], bd.off, bd.idx, bd.fs, r);
     note_launch();
     PBG_CUDA(cudaGetLastError());
     if (where == PBG_HOST) PBG_CUDA(cudaMemcpyAsync(rhs, r, N * 8, cudaMemcpyDeviceToHost, s->stream));
@@ -632,8 +709,10 @@ int pbg_project(pbg_session *s, const double *p, const double *col, double rho_a
         sp = dsol.p;
       }
     }
-    k_project<<<grid_for(N), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, s->h, dt, pp, cp, rho_a, rho_b, sp,
-                                                       fa.d[0], fa.d[1], fa.d[2]);
+    BodyArgs bd;
+    if (int rc = body_args(s, sp, bd)) return rc;
+    k_project<<<grid_for(N), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, s->h, dt, pp, cp, rho_a,
+                                                       rho_b, bd.off, fa.d[0], fa.d[1], fa.d[2]);
     note_launch();
     PBG_CUDA(cudaGetLastError());
     fa.out(s, f, where);

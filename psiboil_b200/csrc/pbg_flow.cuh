@@ -60,15 +60,26 @@ __device__ __forceinline__ double mix_face(const double *__restrict__ col, doubl
 //  * Neumann sides, and the pseudo k sides of a 2-D grid, in the order
 //    imin..kmax: c -= a_bnd, a_bnd = 0; Dirichlet sides: a_bnd = 0
 //  * solid cells: c *= 1e-12, no couplings.
+// With a cut body (bidx != nullptr; solid then holds its off cells, fV = 0,
+// and bidx the index of each cut cell, 0 < fV < 1, in bfs, six face
+// fractions w e s n b t per cut cell) the body branch of :72-119 instead:
+// the reference visits the cells of the body's cut-cell list, which are its
+// cut cells. A coupling of a cut cell to a cut neighbour is multiplied by
+// the cell's own face fraction; a coupling between a listed cell and an
+// off cell, in either direction, is zeroed; c of every cell that is not
+// off is recomputed. The two cells of a face carry their own fractions,
+// so the matrix is not symmetric. Cells on the domain boundary must not
+// be cut (their neighbours beyond it count as fluid).
 __device__ __forceinline__ void assemble_mix_cell(int nx, int ny, int nz, double h, const int (&bc)[6],
                                                   const double *__restrict__ col, double ra, double rb,
-                                                  const uint8_t *__restrict__ solid, long long p, Pos q,
-                                                  double &C, double &W, double &S, double &B) {
+                                                  const uint8_t *__restrict__ solid,
+                                                  const int *__restrict__ bidx,
+                                                  const double *__restrict__ bfs, long long p, Pos q,
+                                                  double (&a)[6], double &C) {
   const long long SI = (long long)ny * nz, SJ = nz;
   const double hh = __dmul_rn(h, h);
   const double hx = __ddiv_rn(hh, h);
   const double hxb = __ddiv_rn(hh, __dmul_rn(0.5, h));
-  double a[6];
   a[0] = __ddiv_rn(q.i == 0 ? hxb : hx, mix_face(col, ra, rb, p, q.i > 0 ? p - SI : p));
   a[1] = __ddiv_rn(q.i == nx - 1 ? hxb : hx, mix_face(col, ra, rb, q.i < nx - 1 ? p + SI : p, p));
   a[2] = __ddiv_rn(q.j == 0 ? hxb : hx, mix_face(col, ra, rb, p, q.j > 0 ? p - SJ : p));
@@ -83,7 +94,21 @@ __device__ __forceinline__ void assemble_mix_cell(int nx, int ny, int nz, double
   double c = a[0];
   for (int f = 1; f < 6; ++f) c = __dadd_rn(c, a[f]);
   const uint8_t sp = solid ? solid[p] : 0;
-  if (solid) {
+  if (bidx) {
+    const long long nbp[6] = {p - SI, p + SI, p - SJ, p + SJ, p - 1, p + 1};
+    const bool inb[6] = {q.i > 0, q.i < nx - 1, q.j > 0, q.j < ny - 1, q.k > 0, q.k < nz - 1};
+    const int me = bidx[p];
+    for (int f = 0; f < 6; ++f) {
+      if (!inb[f]) continue;
+      const int nb = bidx[nbp[f]];
+      if (me >= 0 && nb >= 0) a[f] = __dmul_rn(a[f], bfs[6ll * me + f]);
+      if ((me >= 0 || nb >= 0) && (sp || solid[nbp[f]])) a[f] = 0.0;
+    }
+    if (!sp) {
+      c = a[0];
+      for (int f = 1; f < 6; ++f) c = __dadd_rn(c, a[f]);
+    }
+  } else if (solid) {
     if (q.i > 0 && solid[p - SI] != sp) a[0] = 0.0;
     if (q.i < nx - 1 && solid[p + SI] != sp) a[1] = 0.0;
     if (q.j > 0 && solid[p - SJ] != sp) a[2] = 0.0;
@@ -109,27 +134,33 @@ __device__ __forceinline__ void assemble_mix_cell(int nx, int ny, int nz, double
     for (int f = 0; f < 6; ++f) a[f] = 0.0;
   }
   C = c;
-  W = a[0];
-  S = a[2];
-  B = a[4];
 }
 
+// Writes c, w, s, b (and e, n, t when E is not null: the seven-array form
+// of a cut body's matrix).
 __global__ void k_assemble_mix(Geo G, int nx, int ny, int nz, double h, int4 bc03, int2 bc45,
                                const double *__restrict__ col, double ra, double rb,
-                               const uint8_t *__restrict__ solid, double *__restrict__ C,
+                               const uint8_t *__restrict__ solid, const int *__restrict__ bidx,
+                               const double *__restrict__ bfs, double *__restrict__ C,
                                double *__restrict__ W, double *__restrict__ S, double *__restrict__ B,
+                               double *__restrict__ E, double *__restrict__ Nn, double *__restrict__ T,
                                uint8_t *__restrict__ aflag) {
   const long long N = (long long)nx * ny * nz;
   const int bc[6] = {bc03.x, bc03.y, bc03.z, bc03.w, bc45.x, bc45.y};
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
        p += (long long)gridDim.x * blockDim.x) {
     Pos q = flow_pos(G, p, ny, nz);
-    double c, w, sv, b;
-    assemble_mix_cell(nx, ny, nz, h, bc, col, ra, rb, solid, p, q, c, w, sv, b);
+    double a[6], c;
+    assemble_mix_cell(nx, ny, nz, h, bc, col, ra, rb, solid, bidx, bfs, p, q, a, c);
     C[p] = c;
-    W[p] = w;
-    S[p] = sv;
-    B[p] = b;
+    W[p] = a[0];
+    S[p] = a[2];
+    B[p] = a[4];
+    if (E) {
+      E[p] = a[1];
+      Nn[p] = a[3];
+      T[p] = a[5];
+    }
     aflag[p] = (solid && solid[p]) ? 0 : 1;
   }
 }
@@ -140,11 +171,14 @@ __global__ void k_assemble_mix(Geo G, int nx, int ny, int nz, double h, int4 bc0
 // for homogeneous boundary values. With a solid mask (a voxel body: every
 // fluid cell uncut, face fractions 1) the immersed-body branch (:65-101): a
 // face counts only if the neighbour across it is fluid (cells beyond the
-// domain count as fluid), and solid cells get 0. w may be nullptr in 2-D
-// (its faces then count as zero).
+// domain count as fluid), and solid cells get 0. With a cut body (bidx, bfs
+// as for the assembly) the face areas of a cut cell are first multiplied by
+// its face fractions (:34-43; an uncut fluid cell's fractions are 1). w may
+// be nullptr in 2-D (its faces then count as zero).
 __global__ void k_divergence(Geo G, int nx, int ny, int nz, double a, const double *__restrict__ u,
                              const double *__restrict__ v, const double *__restrict__ w,
-                             const uint8_t *__restrict__ solid, double *__restrict__ rhs) {
+                             const uint8_t *__restrict__ solid, const int *__restrict__ bidx,
+                             const double *__restrict__ bfs, double *__restrict__ rhs) {
   const long long N = (long long)nx * ny * nz;
   const long long SI = (long long)ny * nz, SJ = nz;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
@@ -162,13 +196,16 @@ __global__ void k_divergence(Geo G, int nx, int ny, int nz, double a, const doub
       open[4] = q.k == 0 || !solid[p - 1];
       open[5] = q.k == nz - 1 || !solid[p + 1];
     }
+    double ad[6] = {a, a, a, a, a, a};
+    if (bidx && bidx[p] >= 0)
+      for (int d = 0; d < 6; ++d) ad[d] = __dmul_rn(a, bfs[6ll * bidx[p] + d]);
     double f = 0.0;
-    if (open[0]) f = __dadd_rn(f, __dmul_rn(a, u[iu]));
-    if (open[1]) f = __dsub_rn(f, __dmul_rn(a, u[iu + SI]));
-    if (open[2]) f = __dadd_rn(f, __dmul_rn(a, v[iv]));
-    if (open[3]) f = __dsub_rn(f, __dmul_rn(a, v[iv + nz]));
-    if (open[4]) f = __dadd_rn(f, __dmul_rn(a, w ? w[iw] : 0.0));
-    if (open[5]) f = __dsub_rn(f, __dmul_rn(a, w ? w[iw + 1] : 0.0));
+    if (open[0]) f = __dadd_rn(f, __dmul_rn(ad[0], u[iu]));
+    if (open[1]) f = __dsub_rn(f, __dmul_rn(ad[1], u[iu + SI]));
+    if (open[2]) f = __dadd_rn(f, __dmul_rn(ad[2], v[iv]));
+    if (open[3]) f = __dsub_rn(f, __dmul_rn(ad[3], v[iv + nz]));
+    if (open[4]) f = __dadd_rn(f, __dmul_rn(ad[4], w ? w[iw] : 0.0));
+    if (open[5]) f = __dsub_rn(f, __dmul_rn(ad[5], w ? w[iw + 1] : 0.0));
     if (solid && solid[p]) f = 0.0;
     rhs[p] = __dadd_rn(f, 0.0);
   }

@@ -48,6 +48,12 @@ STEP_CASES = [
     ("step2d", O.KIND_BATCH, dict(index=0, n2d=1, s2=(32, 32)), 0.01),
     ("step12", O.KIND_SINGLE, dict(n=12), 1.0),
 ]
+# the same with an immersed body: a sphere of 4.3 cells written as an STL
+# and cut by the reference's own Body (fV, fS stored with the fixture)
+BODY_STEP_CASES = [
+    # name, kind, problem kwargs, dt, sphere radius in cells
+    ("stepbody16", O.KIND_SINGLE, dict(n=16), 0.01, 4.3),
+]
 
 
 def make_steps():
@@ -66,6 +72,23 @@ def make_steps():
         for k in "xuvw":
             out[k] = r[k]
         print(name, P.dims, dt, r["meta"]["iterations"])
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    for name, kind, kw, dt, radius in BODY_STEP_CASES:
+        P = O.Problem(kind, 7, **kw)
+        r = flow.run_reference_step(P, dt, res_rat=1e-10, body=radius)
+        out = dict(dims=np.array(P.dims), h=np.array(P.h), kind=np.array(kind), seed=np.array(7),
+                   dt=np.array(dt), res_rat=np.array(1e-10), body_radius=np.array(radius),
+                   iterations=np.array(r["meta"]["iterations"]),
+                   fV=r["body"]["fV"], fS=r["body"]["fS"])
+        for k, v in kw.items():
+            out["arg_" + k] = np.array(v)
+        for k in "cwesnbt":
+            out["A_" + k] = r["A"][k]
+        out["ci"] = r["ci"]
+        out["rhs"] = r["b"]
+        for k in "xuvw":
+            out[k] = r[k]
+        print(name, P.dims, dt, radius, r["meta"]["iterations"])
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 

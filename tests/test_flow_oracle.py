@@ -101,3 +101,40 @@ def test_planted_density_error_is_caught(oracle):
         flow.face_density = saved
     assert np.array_equal(good["c"], g["A_c"])
     assert not np.array_equal(bad["c"], g["A_c"])
+
+
+def _body(g):
+    return dict(fV=g["fV"], fS=g["fS"])
+
+
+def test_body_step_oracle_matches_golden(oracle):
+    """A sphere cut by the reference's own Body (STL): the body branches of
+    discretize (cut-cell fractions, off-cell decoupling; a non-symmetric
+    matrix), update_rhs (face fractions) and project, bit for bit."""
+    g = _load("stepbody16")
+    P = problem_of(g, oracle)
+    r = flow.step(P, float(g["dt"]), res_rat=float(g["res_rat"]), body=_body(g))
+    assert r["stats"]["printed"] == int(g["iterations"])
+    for k in "cwesnbt":
+        assert np.array_equal(r["A"][k], g["A_" + k]), k
+    assert not np.array_equal(r["A"]["e"].reshape(P.dims)[:-1], r["A"]["w"].reshape(P.dims)[1:])
+    assert np.array_equal(r["A"]["ci"], g["ci"])
+    assert np.array_equal(r["b"], g["rhs"])
+    for k in "xuvw":
+        assert np.array_equal(r[k].reshape(-1), g[k].reshape(-1)), k
+
+
+@pytest.mark.skipif(not oracle_py.harness_available(), reason="reference harness not built here")
+@pytest.mark.parametrize("n,radius,dt", [(32, 9.7, 0.003), (16, 5.55, 1.0)])
+def test_body_step_oracle_matches_reference_live(oracle, n, radius, dt):
+    P = oracle.Problem(0, 13, n=n)
+    ref = flow.run_reference_step(P, dt, body=radius)
+    bd = ref["body"]
+    cut = (bd["fV"] > 0) & (bd["fV"] < 1)
+    assert np.array_equal(bd["listed"] > 0, cut)  # the cut-cell list is the cut cells
+    r = flow.step(P, dt, body=bd)
+    assert r["stats"]["printed"] == int(ref["meta"]["iterations"])
+    for k in "cwesnbt":
+        assert np.array_equal(r["A"][k], ref["A"][k]), k
+    for k in "bxuvw":
+        assert np.array_equal(np.reshape(r[k], -1), np.reshape(ref[k], -1)), k

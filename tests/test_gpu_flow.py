@@ -150,3 +150,71 @@ def test_engine_step_leaves_divergence_free_field(engine, oracle, kind, kw, mixe
     assert res.converged
     assert np.linalg.norm(d1) <= 10 * prm.tol * np.linalg.norm(d0)
     assert np.all(u[0] == 0.0) and np.all(u[-1] == 0.0) and np.all(w[:, :, 0] == 0.0)
+
+
+def _body(g):
+    return np.ascontiguousarray(g["fV"]), np.ascontiguousarray(g["fS"])
+
+
+def test_body_step_matches_reference(engine, oracle):
+    """A sphere cut by the reference's Body: assemble (seven arrays), divergence,
+    CG with exact sums and projection equal the reference's step bit for bit."""
+    g = dict(np.load(os.path.join(GOLDEN, "stepbody16.npz")))
+    P = problem_of(g, oracle)
+    col, u, v, w, ra, rb, bc = flow.flow_state(P)
+    dt = float(g["dt"])
+    p = np.zeros(P.N)
+    with engine.Session(*P.dims, P.h, bc=bc) as s:
+        s.upload_body(*_body(g))
+        res = s.pressure_step(col, ra, rb, dt, u, v, w, p, _cg_params(engine, float(g["res_rat"])))
+        assert res.iterations == int(g["iterations"])
+        assert not s.symmetric()
+        M = s.download_matrix()
+    for k in "cwesnbt":
+        assert np.array_equal(M[k], g["A_" + k]), k
+    assert np.array_equal(p, g["x"])
+    for a, k in ((u, "u"), (v, "v"), (w, "w")):
+        assert np.array_equal(a.reshape(-1), g[k].reshape(-1)), k
+
+
+def test_body_stages_match_oracle(engine, oracle):
+    """Each stage with the body against the oracle, and the rules around it."""
+    g = dict(np.load(os.path.join(GOLDEN, "stepbody16.npz")))
+    P = problem_of(g, oracle)
+    col, u, v, w, ra, rb, bc = flow.flow_state(P)
+    body = dict(fV=g["fV"], fS=g["fS"])
+    off = (g["fV"] == 0).astype(np.uint8)
+    dt = float(g["dt"])
+    ref_A = flow.assemble_mix(P.dims, P.h, bc, col, ra, rb, solid=off, body=body)
+    ref_b = flow.divergence(P.dims, P.h, dt, u, v, w, solid=off, body=body)
+    x = np.asarray(g["x"], dtype=np.float64)
+    ref_uvw = flow.project(P.dims, P.h, dt, x, col, ra, rb, u, v, w, solid=off)
+    with engine.Session(*P.dims, P.h, bc=bc) as s:
+        s.upload_body(*_body(g))
+        s.assemble_mix(col, ra, rb)
+        M = s.download_matrix()
+        for k in "cwesnbt":
+            assert np.array_equal(M[k], ref_A[k]), k
+        rhs = np.zeros(P.N)
+        s.divergence(u, v, w, dt, rhs)
+        assert np.array_equal(rhs, ref_b)
+        uu, vv, ww = u.copy(), v.copy(), w.copy()
+        s.project(x, col, ra, rb, dt, uu, vv, ww)
+        for a, b in zip((uu, vv, ww), ref_uvw):
+            assert np.array_equal(a.reshape(-1), np.reshape(b, -1))
+        # a body and a voxel mask together are refused
+        with pytest.raises(engine.PbgError):
+            s.assemble_mix(col, ra, rb, solid=off)
+        # the engine's solver needs the symmetric form
+        prm = engine.default_params(engine.SOLVER_ENGINE)
+        with pytest.raises(engine.PbgError):
+            s.solve(np.zeros(P.N), rhs, prm)
+        # without the body the symmetric form comes back
+        s.upload_body(None, None)
+        s.assemble_mix(col, ra, rb)
+        assert s.symmetric()
+        # a cut cell on the domain boundary is refused
+        fV = np.ones(P.N)
+        fV[0] = 0.5
+        with pytest.raises(engine.PbgError):
+            s.upload_body(fV, np.ones((6, P.N)))
