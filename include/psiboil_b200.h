@@ -246,7 +246,10 @@ int pbg_pressure_step(pbg_session *s, const double *col, double rho_a, double rh
  * matrix is then stored in the seven-array form, as the two cells of a
  * face carry their own fractions), update_rhs's face fractions (:34-43)
  * and project's fluid-only faces. Cells on the domain boundary must not be
- * cut (PBG_ERR_UNSUPPORTED). fV = NULL removes the body. */
+ * cut (PBG_ERR_UNSUPPORTED). fV = NULL removes the body. PBG_SOLVER_ENGINE
+ * solves such a matrix by FP64 refinement around its symmetric part; a
+ * sweep that does not reduce the residual is undone and ends the solve with
+ * PBG_DIVERGED (strongly non-symmetric matrices: use BiCGS or CGS). */
 int pbg_body_upload(pbg_session *s, const double *fV, const double *fS, int where);
 
 /* Solve A x = b with x as initial guess and result (x updated in place,

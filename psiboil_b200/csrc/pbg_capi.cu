@@ -50,6 +50,8 @@ struct pbg_session {
   DBuf<int> bidx;
   DBuf<double> bfs;
   long long ncut = 0;
+  // symmetric part of a non-symmetric matrix, the engine's hierarchy input
+  DBuf<double> symc, symw, syms, symb;
   unsigned long long mat_gen = 0, ci_gen = ~0ull;  // ci is valid while ci_gen == mat_gen
   DBuf<unsigned long long> dlinf;
   double *hbuf = nullptr;          // pinned: 64 doubles
@@ -796,6 +798,16 @@ void ensure_engine(pbg_session *s, bool mixed, int coarse_max) {
   if (s->eng_dirty || (mixed && !s->eng->have32)) {
     const Mat64 &A = s->A;
     EMat<double> m = make_emat<double>(A.nx, A.ny, A.nz, A.c.p, A.w.p, A.s.p, A.b.p, nullptr);
+    s->eng->nonsym = !A.sym;
+    if (!A.sym) {
+      // a cut body's matrix: the hierarchy from its symmetric part, the
+      // refinement against the matrix itself
+      const long long N = s->ncell();
+      if (s->symc.n != (size_t)N) { s->symc.alloc(N); s->symw.alloc(N); s->syms.alloc(N); s->symb.alloc(N); }
+      symmetrize(A.view(), s->symc.p, s->symw.p, s->syms.p, s->symb.p, s->stream);
+      m = make_emat<double>(A.nx, A.ny, A.nz, s->symc.p, s->symw.p, s->syms.p, s->symb.p, nullptr);
+      s->eng->top = A.view();
+    }
     // same shape and buffers (a re-assembled matrix): numeric refresh only
     if (s->eng->refresh(m, mixed, s->stream)) {
       s->eng_dirty = false;
@@ -873,7 +885,6 @@ int solve_device(pbg_session *s, double *xd, const double *bd, const pbg_params 
     out.res = ar.res;
     out.levels = s->refac->nlevels();
   } else if (p->solver == PBG_SOLVER_ENGINE) {
-    if (!s->A.sym) return fail(PBG_ERR_UNSUPPORTED, "the engine solver needs a symmetric matrix");
     const bool mixed = p->precision == PBG_MIXED;
     if (p->coarse_max < 0) return fail(PBG_ERR_ARG, "coarse_max must be >= 0");
     ensure_engine(s, mixed, p->coarse_max);

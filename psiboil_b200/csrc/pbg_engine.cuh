@@ -99,6 +99,10 @@ class Engine {
   EWork<float> w32;
   DBuf<double> r64, xtmp, dsc; // FP64 refinement residual, scratch, scalars
   double *hsc = nullptr;       // pinned host scalars
+  // a non-symmetric operator (seven arrays): the hierarchy is built from its
+  // symmetric part, and the refinement's true residual uses this one
+  MatView<double> top{};
+  bool nonsym = false;
 
   ~Engine();
   void build(const EMat<double> &A0, cudaStream_t s, bool mixed);
@@ -126,6 +130,14 @@ class Engine {
   template <typename T> void kcycle(int l, EWork<T> &w, RedPool &red, const int *stop, cudaStream_t s);
   template <typename T> int fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red,
                                 cudaStream_t s, double *hist, FcgScal *hfs);
+  template <typename T> void true_resid(const double *x, const double *b, T *rT, RedPool &red,
+                                        cudaStream_t s);
+  void keep_iterate(const double *x, long long N, cudaStream_t s);
+  void restore_iterate(double *x, long long N, cudaStream_t s);
 };
+
+// The symmetric part of a seven-array operator in the engine's storage
+// c, w, s, b (k_symmetrize), enqueued on st.
+void symmetrize(const MatView<double> &A, double *c, double *w, double *s, double *b, cudaStream_t st);
 
 }  // namespace pbg

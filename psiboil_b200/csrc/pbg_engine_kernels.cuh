@@ -462,6 +462,36 @@ __global__ void __launch_bounds__(kThreads, 8) k_true_resid(EMat<double> A, cons
   if (grid_reduce<2>(v, part, count, o)) { out[0] = o[0]; out[1] = o[1]; }
 }
 
+// The same for a non-symmetric operator in the seven-array form (a cut
+// body's pressure matrix), which the engine solves by refinement around
+// its symmetric part: r = b - (c x - sum a_nb x_nb).
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 8) k_true_resid_ns(MatView<double> A, Geo G, const double *__restrict__ x,
+                                const double *__restrict__ b, double *__restrict__ r,
+                                T *__restrict__ rT, double *out, double *part, unsigned *count) {
+  PBG_PDL_ENTRY();
+  const uint32_t SI = G.nynz, SJ = (uint32_t)A.nz;
+  double v[2] = {0.0, 0.0};
+  GRID_LOOP(p, G.n) {
+    const Pos q = G.pos(p);
+    const Nb<double> a = coeffs(A, p, q);
+    double nb = 0.0;
+    if (q.i > 0) nb += a.w * x[p - SI];
+    if (q.i < A.nx - 1) nb += a.e * x[p + SI];
+    if (q.j > 0) nb += a.s * x[p - SJ];
+    if (q.j < A.ny - 1) nb += a.n * x[p + SJ];
+    if (q.k > 0) nb += a.b * x[p - 1];
+    if (q.k < A.nz - 1) nb += a.t * x[p + 1];
+    const double rv = b[p] - (A.c[p] * x[p] - nb);
+    if (r) r[p] = rv;
+    if (rT) rT[p] = (T)rv;
+    v[0] += rv * rv;
+    v[1] += b[p] * b[p];
+  }
+  double o[2];
+  if (grid_reduce<2>(v, part, count, o)) { out[0] = o[0]; out[1] = o[1]; }
+}
+
 // ---------------------------------------------------------------- hierarchy
 // Galerkin coarse operator P^T A P for piecewise-constant aggregation by 2
 // in every direction with more than one cell (last block partial on odd
