@@ -61,7 +61,8 @@ enum {
   PBG_BREAKDOWN = 3,
   PBG_INITIAL = 4,   /* converged before the first iteration */
   PBG_NAN = 5,
-  PBG_DIVERGED = 6   /* AC divergence guard restored the last good iterate */
+  PBG_DIVERGED = 6   /* AC divergence guard, or an engine refinement sweep that did not
+                        reduce the residual: the last good iterate restored */
 };
 
 enum { PBG_HOST = 0, PBG_DEVICE = 1 };
