@@ -236,12 +236,15 @@ static bool graph_loop_enabled() {
 }
 
 // Tuning knobs (environment): PBG_COARSE_MAX sets the size of the dense
-// coarsest level, PBG_KC_MAX the deepest level that runs a K-cycle.
+// coarsest level, PBG_KC_MAX the deepest level that runs a K-cycle,
+// PBG_OMEGA the damped-Jacobi weight (0 < omega < 1).
 EngineOpts::EngineOpts() {
   const char *c = getenv("PBG_COARSE_MAX");
   if (c && atoi(c) > 0) coarse_max = atoi(c);
   const char *k = getenv("PBG_KC_MAX");
   if (k && atoi(k) > 0) kc_max = atoi(k);
+  const char *o = getenv("PBG_OMEGA");
+  if (o && atof(o) > 0.0 && atof(o) < 1.0) omega = atof(o);
 }
 
 template struct EWork<double>;
