@@ -619,12 +619,22 @@ int Engine::fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red, cu
   return hfs->iter;
 }
 
-// Symmetric part (A + A^T) / 2 of a seven-array operator in the engine's
+// Symmetric approximation of a seven-array operator in the engine's
 // storage: each coupling the mean of the two cells' own values (w of a cell
-// with e of its west neighbour, and so on), c unchanged. On a cut body's
-// matrix the refinement around it reduces the residual by about 1e-2 per
-// sweep; keeping the row sums instead (moving c with the couplings) gave
-// only 0.3.
+// and e of its west neighbour, and so on), c unchanged; a coupling that only
+// one side keeps drops out. That one-sided case is a cell inside a body
+// (c = 1e-12 c0, its couplings zeroed) next to a fluid cell off the cut
+// list: half the coupling against that tiny diagonal would make the
+// approximation indefinite, while in the matrix itself the inside cell's
+// value is decoupled. On the reference's cut sphere the refinement around
+// it reduces the residual by 1e-2 to 3e-2 per sweep past the first; the
+// smaller of the two sides instead (always diagonally dominant) gave 2e-2
+// to 4e-2 there but lost the upwind part of a convected matrix, where the
+// mean keeps it as a skew term.
+__device__ __forceinline__ double sym_coupling(double x, double y) {
+  return (x != 0.0 && y != 0.0) ? 0.5 * (x + y) : 0.0;
+}
+
 __global__ void k_symmetrize(MatView<double> A, Geo G, double *__restrict__ C, double *__restrict__ W,
                              double *__restrict__ S, double *__restrict__ B) {
   const uint32_t SI = G.nynz, SJ = (uint32_t)A.nz;
@@ -632,9 +642,9 @@ __global__ void k_symmetrize(MatView<double> A, Geo G, double *__restrict__ C, d
     const Pos q = G.pos(p);
     const Nb<double> a = coeffs(A, p, q);
     C[p] = A.c[p];
-    W[p] = q.i > 0 ? 0.5 * (a.w + A.e[p - SI]) : 0.0;
-    S[p] = q.j > 0 ? 0.5 * (a.s + A.n[p - SJ]) : 0.0;
-    B[p] = q.k > 0 ? 0.5 * (a.b + A.t[p - 1]) : 0.0;
+    W[p] = q.i > 0 ? sym_coupling(a.w, A.e[p - SI]) : 0.0;
+    S[p] = q.j > 0 ? sym_coupling(a.s, A.n[p - SJ]) : 0.0;
+    B[p] = q.k > 0 ? sym_coupling(a.b, A.t[p - 1]) : 0.0;
   }
 }
 

@@ -59,8 +59,8 @@ def test_engine_nonsymmetric(engine, oracle, precision):
     """A mildly non-symmetric matrix (seven-array form, weak upwind
     convection) converges by the refinement around its symmetric part to the
     FP64 target; a strongly non-symmetric one (stronger convection, where that
-    refinement stalls and the symmetric part may be indefinite) ends with
-    DIVERGED or BREAKDOWN and keeps an iterate better than the start."""
+    refinement stalls) ends unconverged (DIVERGED, BREAKDOWN or MAXITER) with
+    an iterate better than the start."""
     P = oracle.Problem(0, 5, n=16, convect=2e-7)
     with engine.Session(*P.dims, P.h) as s:
         s.upload_matrix(P.A)
@@ -76,7 +76,7 @@ def test_engine_nonsymmetric(engine, oracle, precision):
         E = engine.Engine(s)
         ok = E.solve(x, P.b.copy(), tol=1e-8, precision=precision)
         r = E.last
-    assert not ok and r.status in (engine.DIVERGED, engine.BREAKDOWN)
+    assert not ok and r.status in (engine.DIVERGED, engine.BREAKDOWN, engine.MAXITER)
     assert true_relres(oracle, P, x) == pytest.approx(r.relres, rel=1e-6)
     assert r.relres < 1.0
 
