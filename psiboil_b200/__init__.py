@@ -378,7 +378,10 @@ class Session:
             fV = np.ascontiguousarray(fV, dtype=np.float64)
             fS = np.ascontiguousarray(fS, dtype=np.float64)
             pv = fV.ctypes.data
-        _check(lib().pbg_body_upload(self._h, pv, _ptr(fS)[0], where))
+        ps, where2 = _ptr(fS)
+        if where2 != where:
+            raise ValueError("fV and fS must live in the same memory")
+        _check(lib().pbg_body_upload(self._h, pv, ps, where))
 
     def pressure_step(self, col, rho_a, rho_b, dt, u, v, w, p, params, solid=None):
         """Assemble, divergence, solve and project in one call; u, v, w and
