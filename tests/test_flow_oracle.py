@@ -138,3 +138,26 @@ def test_body_step_oracle_matches_reference_live(oracle, n, radius, dt):
         assert np.array_equal(r["A"][k], ref["A"][k]), k
     for k in "bxuvw":
         assert np.array_equal(np.reshape(r[k], -1), np.reshape(ref[k], -1)), k
+
+
+def test_sampled_sphere_body_is_consistent():
+    """The bench's sampled sphere (bench.sphere_body) has the structure of a
+    cut body: every cell the surface crosses is cut and keeps an open face,
+    no fluid cell meets a cell inside the body, and the oracle's assembly
+    with it has a positive diagonal everywhere."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(GOLDEN)))  # the repository root
+    import bench
+    n = 32
+    fV, fS = bench.sphere_body(n, n / 6.0)
+    V = fV.reshape(n, n, n)
+    F = fS.reshape(6, n, n, n)
+    off, full, cut = V == 0.0, V == 1.0, (V > 0.0) & (V < 1.0)
+    assert cut.sum() > 0 and off.sum() > 0
+    assert (F.max(axis=0)[cut] > 0.0).all()
+    for ax in range(3):
+        a, b = np.swapaxes(off, 0, ax), np.swapaxes(full, 0, ax)
+        assert not ((a[1:] & b[:-1]) | (a[:-1] & b[1:])).any()
+    A = flow.assemble_mix((n, n, n), 1.0 / n, [0, 0, 0, 0, 0, 1], None, 1.0, 1.0,
+                          solid=off.reshape(-1).astype(np.uint8), body=dict(fV=fV, fS=fS))
+    assert (A["c"] > 0.0).all()
