@@ -161,3 +161,47 @@ def test_sampled_sphere_body_is_consistent():
     A = flow.assemble_mix((n, n, n), 1.0 / n, [0, 0, 0, 0, 0, 1], None, 1.0, 1.0,
                           solid=off.reshape(-1).astype(np.uint8), body=dict(fV=fV, fS=fS))
     assert (A["c"] > 0.0).all()
+
+
+def _sparse(dims, A):
+    """The seven-array matrix (c x - sum a_nb x_nb) as scipy CSR."""
+    import scipy.sparse as sp
+    nx, ny, nz = dims
+    N = nx * ny * nz
+    idx = np.arange(N).reshape(dims)
+    I, J, K = np.meshgrid(range(nx), range(ny), range(nz), indexing="ij")
+    rows, cols, vals = [idx.ravel()], [idx.ravel()], [A["c"]]
+    for key, ax, sh, mask in (("w", 0, -1, I > 0), ("e", 0, 1, I < nx - 1), ("s", 1, -1, J > 0),
+                              ("n", 1, 1, J < ny - 1), ("b", 2, -1, K > 0), ("t", 2, 1, K < nz - 1)):
+        nb = np.roll(idx, -sh, ax)
+        rows.append(idx[mask])
+        cols.append(nb[mask])
+        vals.append(-A[key].reshape(dims)[mask])
+    return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(N, N))
+
+
+def test_symmetric_part_refinement_on_reference_body():
+    """The engine's symmetric approximation of a cut body's matrix (mean of
+    the two sides, one-sided couplings dropped, c kept; k_symmetrize),
+    restated with scipy on the reference's own sphere matrix: the refinement
+    around it with exact inner solves reduces the residual by at most 5e-2
+    per sweep past the first."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as sla
+    g = _load("stepbody16")
+    dims = tuple(int(v) for v in g["dims"])
+    M = _sparse(dims, {k: g["A_" + k] for k in "cwesnbt"})
+    off = M - sp.diags(M.diagonal())
+    offT = off.T.tocsr()
+    both = off.multiply(offT) != 0          # couplings both sides keep
+    S = (off + offT).multiply(both) * 0.5 + sp.diags(M.diagonal())
+    lu = sla.splu(S.tocsc())
+    b = g["rhs"]
+    x = np.zeros_like(b)
+    rel = []
+    for _ in range(5):
+        r = b - M @ x
+        rel.append(np.linalg.norm(r) / np.linalg.norm(b))
+        x = x + lu.solve(r)
+    for k in range(2, len(rel)):
+        assert rel[k] <= 5e-2 * rel[k - 1], rel
