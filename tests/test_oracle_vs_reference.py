@@ -38,3 +38,20 @@ def test_oracle_ic_cg_equals_reference(oracle, prec, kind, kw):
     x, st = oracle.cg(P, prec=prec, res_rat=1e-8, res_tol=1e-15)
     assert st["printed"] == int(meta["iterations"])
     assert np.array_equal(x, arr["x"], equal_nan=True)
+
+
+@pytest.mark.parametrize("solver", ["jacobi", "gs"])
+@pytest.mark.parametrize("resrat,maxit", [(0.5, 300), (1e-3, 7), (1e-2, 1), (0.9, 50)])
+@pytest.mark.parametrize("kind,kw", [(1, dict(n=12, nb=2, rmin=2.0, rmax=3.0, rc=3.0)),
+                                     (2, dict(index=3, n2d=2, s2=(10, 14), s3=(6, 8)))])
+def test_oracle_stationary_equals_reference(oracle, solver, resrat, maxit, kind, kw):
+    """Jacobi::solve and GaussSeidel::solve: early stops, caps of one and a few
+    sweeps, 2-D and bodies; the oracle (with the reference's stored ci) gives
+    the compiled reference's sweep count, convergence flag and iterate."""
+    P = oracle.Problem(kind, 9, **kw)
+    meta, arr = oracle.run_reference(P, solver=solver, resrat=resrat, maxit=maxit)
+    P.ci = arr["ci"].copy()
+    x, st = oracle.cg(P, solver=solver, res_rat=resrat, maxit=maxit, res_tol=1e-18)  # ResTol(atto)
+    assert st["printed"] == int(meta["iterations"])
+    assert bool(st["converged"]) == bool(meta["converged"])
+    assert np.array_equal(x, arr["x"])
