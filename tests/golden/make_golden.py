@@ -53,6 +53,7 @@ STEP_CASES = [
 BODY_STEP_CASES = [
     # name, kind, problem kwargs, dt, sphere radius in cells
     ("stepbody16", O.KIND_SINGLE, dict(n=16), 0.01, 4.3),
+    ("stepbody32", O.KIND_SINGLE, dict(n=32), 0.003, 9.7),
 ]
 
 

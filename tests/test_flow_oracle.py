@@ -107,11 +107,12 @@ def _body(g):
     return dict(fV=g["fV"], fS=g["fS"])
 
 
-def test_body_step_oracle_matches_golden(oracle):
+@pytest.mark.parametrize("name", ["stepbody16", "stepbody32"])
+def test_body_step_oracle_matches_golden(oracle, name):
     """A sphere cut by the reference's own Body (STL): the body branches of
     discretize (cut-cell fractions, off-cell decoupling; a non-symmetric
     matrix), update_rhs (face fractions) and project, bit for bit."""
-    g = _load("stepbody16")
+    g = _load(name)
     P = problem_of(g, oracle)
     r = flow.step(P, float(g["dt"]), res_rat=float(g["res_rat"]), body=_body(g))
     assert r["stats"]["printed"] == int(g["iterations"])

@@ -156,10 +156,11 @@ def _body(g):
     return np.ascontiguousarray(g["fV"]), np.ascontiguousarray(g["fS"])
 
 
-def test_body_step_matches_reference(engine, oracle):
+@pytest.mark.parametrize("name", ["stepbody16", "stepbody32"])
+def test_body_step_matches_reference(engine, oracle, name):
     """A sphere cut by the reference's Body: assemble (seven arrays), divergence,
     CG with exact sums and projection equal the reference's step bit for bit."""
-    g = dict(np.load(os.path.join(GOLDEN, "stepbody16.npz")))
+    g = dict(np.load(os.path.join(GOLDEN, name + ".npz")))
     P = problem_of(g, oracle)
     col, u, v, w, ra, rb, bc = flow.flow_state(P)
     dt = float(g["dt"])
