@@ -594,7 +594,10 @@ class AC:
 
 
 class Engine:
-    """Flexible CG + AC K-cycle; FP64 or mixed (FP32 inner, FP64 refinement)."""
+    """Flexible CG + AC K-cycle; FP64 or mixed (FP32 inner, FP64 refinement).
+    A non-symmetric matrix (a cut body's) is solved by FP64 refinement around
+    its symmetric part; a sweep that does not reduce the residual is undone
+    and the result says DIVERGED."""
 
     def __init__(self, session):
         self.session = session
