@@ -347,7 +347,9 @@ int pbg_session_info(const pbg_session *s, long long *ncell, int *symmetric, lon
   if (symmetric) *symmetric = s->A.sym ? 1 : 0;
   if (device_bytes) {
     size_t b = s->A.c.bytes() + s->A.w.bytes() + s->A.e.bytes() + s->A.s.bytes() + s->A.n.bytes() +
-               s->A.b.bytes() + s->A.t.bytes() + s->aflag.bytes() + s->dx.bytes() + s->db.bytes();
+               s->A.b.bytes() + s->A.t.bytes() + s->aflag.bytes() + s->dx.bytes() + s->db.bytes() +
+               s->ci.bytes() + s->boff.bytes() + s->bidx.bytes() + s->bfs.bytes() + s->symc.bytes() +
+               s->symw.bytes() + s->syms.bytes() + s->symb.bytes();
     *device_bytes = (long long)b;
   }
   return PBG_OK;
