@@ -122,6 +122,13 @@ typedef struct {
    * PBG_HOST it is not copied to the device); 0: x is the initial guess,
    * as in the reference's Linear::solve. */
   int x0_zero;
+  /* PBG_SOLVER_AC: the solver that smooths every level and solves the
+   * coarsest one, the Linear the reference's Centered object holds
+   * (additive_cycle_functions.cpp:90-107): PBG_SOLVER_CG (default),
+   * PBG_SOLVER_BICGS, PBG_SOLVER_CGS (each with `prec`), PBG_SOLVER_JACOBI
+   * or PBG_SOLVER_GAUSS_SEIDEL (level 0 with the uploaded A.ci, coarse levels
+   * with ci = 1/c, as additive_coarsen_system.cpp forms it). */
+  int ac_smoother;
 } pbg_params;
 
 typedef struct {

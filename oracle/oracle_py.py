@@ -264,7 +264,7 @@ def harness_available():
 
 
 def run_reference(P, solver="cg", resrat=1e-8, maxit=20000, maxcyc=20, guard=1, cycle="V",
-                  out_prefix=None, dump=True, timeout=3600, prec="di"):
+                  out_prefix=None, dump=True, timeout=3600, prec="di", acsm="cg"):
     """Run the compiled reference on P's fixture; returns (meta, arrays)."""
     import tempfile
     kind = {KIND_SINGLE: "single", KIND_CYL: "cyl", KIND_BATCH: "batch"}[P.kind]
@@ -280,7 +280,7 @@ def run_reference(P, solver="cg", resrat=1e-8, maxit=20000, maxcyc=20, guard=1, 
            "--seed", str(P.seed), "--solver", solver, "--resrat", repr(resrat),
            "--maxit", str(maxit), "--maxcyc", str(maxcyc), "--guard", str(guard),
            "--cycle", cycle, "--prec", prec, "--dump", "1" if dump else "0", "--out", out_prefix,
-           "--convect", repr(getattr(P, "convect", 0.0))]
+           "--convect", repr(getattr(P, "convect", 0.0)), "--acsm", acsm]
     subprocess.run(cmd, check=True, capture_output=True, timeout=timeout)
     meta = {}
     for line in open(out_prefix + ".txt"):

@@ -28,7 +28,7 @@
  * Usage:
  *   ref_harness --kind single|cyl|batch --n N [--nb NB --rmin R --rmax R
  *               --rc R --ratio Q] [--index I --n2d M --s2 LO HI --s3 LO HI]
- *               --seed S --solver cg|bicgs|ac --resrat RR --maxit M
+ *               --seed S --solver cg|bicgs|cgs|jacobi|gs|ac [--acsm SOLVER] --resrat RR --maxit M
  *               [--maxcyc C --guard 0|1 --cycle V|F|W] [--prec di|ic0|ic2|ic3] [--save NAME]
  *               [--step 1 --dt DT] [--convect F] --out PREFIX
  *
@@ -67,7 +67,7 @@
 namespace {
 
 struct Args {
-  std::string kind = "single", solver = "cg", out = "ref", cycle = "V", save, prec = "di";
+  std::string kind = "single", solver = "cg", out = "ref", cycle = "V", save, prec = "di", acsm = "cg";
   int n = 16, nb = 0, index = 0, n2d = 0, s2lo = 64, s2hi = 512, s3lo = 32, s3hi = 96;
   double rmin = 4, rmax = 16, rc = 0, ratio = 1000;
   unsigned long long seed = 1;
@@ -99,6 +99,7 @@ Args parse(int argc, char **argv) {
     else if (k == "--seed") a.seed = std::strtoull(nxt(), nullptr, 10);
     else if (k == "--solver") a.solver = nxt();
     else if (k == "--body") a.body = std::atof(nxt());
+    else if (k == "--acsm") a.acsm = nxt();
     else if (k == "--resrat") a.resrat = std::atof(nxt());
     else if (k == "--maxit") a.maxit = std::atoi(nxt());
     else if (k == "--maxcyc") a.maxcyc = std::atoi(nxt());
@@ -476,19 +477,22 @@ int main(int argc, char **argv) {
   Linear *solver = nullptr;
   const Prec pc = a.prec == "ic0" ? Prec::ic0() : a.prec == "ic2" ? Prec::ic2()
                  : a.prec == "ic3" ? Prec::ic3() : Prec::di();
+  /* with --solver ac, --acsm names the Pressure's own solver, which AC uses
+     on every level (additive_cycle_functions.cpp:90-107) */
+  const std::string lin = a.solver == "ac" ? a.acsm : a.solver;
 #ifdef PBG_WITH_ENGINE
   /* the drop-in: the engine's Krylov classes behind the reference's virtual */
-  if (a.gpu && a.solver == "bicgs") solver = new pbg_psiboil::GpuBiCGS(d, pc, a.exact != 0);
-  else if (a.gpu && a.solver == "cgs") solver = new pbg_psiboil::GpuCGS(d, pc, a.exact != 0);
-  else if (a.gpu && a.solver == "jacobi") solver = new pbg_psiboil::GpuJacobi(d, a.exact != 0);
-  else if (a.gpu && a.solver == "gs") solver = new pbg_psiboil::GpuGaussSeidel(d, a.exact != 0);
+  if (a.gpu && lin == "bicgs") solver = new pbg_psiboil::GpuBiCGS(d, pc, a.exact != 0);
+  else if (a.gpu && lin == "cgs") solver = new pbg_psiboil::GpuCGS(d, pc, a.exact != 0);
+  else if (a.gpu && lin == "jacobi") solver = new pbg_psiboil::GpuJacobi(d, a.exact != 0);
+  else if (a.gpu && lin == "gs") solver = new pbg_psiboil::GpuGaussSeidel(d, a.exact != 0);
   else if (a.gpu) solver = new pbg_psiboil::GpuCG(d, pc, a.exact != 0);
   else
 #endif
-  if (a.solver == "bicgs") solver = new BiCGS(d, pc);
-  else if (a.solver == "cgs") solver = new CGS(d, pc);
-  else if (a.solver == "jacobi") solver = new Jacobi(d);
-  else if (a.solver == "gs") solver = new GaussSeidel(d);
+  if (lin == "bicgs") solver = new BiCGS(d, pc);
+  else if (lin == "cgs") solver = new CGS(d, pc);
+  else if (lin == "jacobi") solver = new Jacobi(d);
+  else if (lin == "gs") solver = new GaussSeidel(d);
   else solver = new CG(d, pc);
 
   Vector uvw(d);

@@ -60,7 +60,8 @@ class Params(ctypes.Structure):
                 ("mv", ctypes.c_int * 3), ("ms", ctypes.c_int * 3),
                 ("tol", ctypes.c_double), ("inner_tol", ctypes.c_double),
                 ("max_sweeps", ctypes.c_int), ("exact_sums", ctypes.c_int),
-                ("coarse_max", ctypes.c_int), ("prec", ctypes.c_int), ("x0_zero", ctypes.c_int)]
+                ("coarse_max", ctypes.c_int), ("prec", ctypes.c_int), ("x0_zero", ctypes.c_int),
+                ("ac_smoother", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):
@@ -528,11 +529,20 @@ class GaussSeidel(_Krylov):
 
 
 class AC:
-    """Additive-correction multigrid with CG smoothers (Src/Solver/Additive)."""
+    """Additive-correction multigrid (Src/Solver/Additive). smoother: the
+    Linear solver every level uses ("cg", "bicgs", "cgs" with prec, or
+    "jacobi", "gs"), as the Centered object's solver is in the reference."""
 
-    def __init__(self, session, exact_sums=False):
+    SMOOTHERS = {"cg": SOLVER_CG, "bicgs": SOLVER_BICGS, "cgs": SOLVER_CGS, "jacobi": SOLVER_JACOBI,
+                 "gs": SOLVER_GAUSS_SEIDEL}
+
+    def __init__(self, session, exact_sums=False, smoother="cg", prec="di"):
+        if smoother not in self.SMOOTHERS:
+            raise ValueError("smoother must be one of %s" % sorted(self.SMOOTHERS))
         self.session = session
         self.exact_sums = exact_sums
+        self.smoother = self.SMOOTHERS[smoother]
+        self.prec = _Krylov.PREC[prec]
         self._max_cyc, self._min_cyc = 20, 0
         self._stop_if_div, self._prio = True, True
         self.mv = [20, 20, 20]
@@ -577,6 +587,7 @@ class AC:
             p.mv[q] = (mv or self.mv)[q]
             p.ms[q] = (ms or self.ms)[q]
         p.exact_sums = int(self.exact_sums)
+        p.ac_smoother, p.prec = self.smoother, self.prec
         self.last = self.session.solve(x, b, p)
         return bool(self.last.converged), self.last.cycles
 

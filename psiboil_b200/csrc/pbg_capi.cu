@@ -284,6 +284,7 @@ void pbg_params_default(pbg_params *p, int solver) {
   p->tol = 1.0e-8;
   p->inner_tol = 1.0e-3;
   p->max_sweeps = 8;
+  p->ac_smoother = PBG_SOLVER_CG;
   if (solver == PBG_SOLVER_ENGINE) p->max_iter = 500;
 }
 
@@ -877,6 +878,15 @@ int solve_device(pbg_session *s, double *xd, const double *bd, const pbg_params 
     for (int q = 0; q < 3; ++q) { cx.mv[q] = pa.mv[q]; cx.ms[q] = pa.ms[q]; }
     cx.resrat_val = pa.resrat_val; cx.restol_val = pa.restol_val;
     s->refac->seq = exact_terms(s, p);
+    const int sm = p->ac_smoother;
+    if (sm != PBG_SOLVER_CG && sm != PBG_SOLVER_BICGS && sm != PBG_SOLVER_CGS && sm != PBG_SOLVER_JACOBI &&
+        sm != PBG_SOLVER_GAUSS_SEIDEL)
+      return fail(PBG_ERR_ARG, "ac_smoother must be CG, BiCGS, CGS, Jacobi or Gauss-Seidel");
+    if (p->prec < 0 || p->prec > 3) return fail(PBG_ERR_ARG, "prec must be 0 (diagonal), 1 (IC0), 2 (IC2) or 3 (IC3)");
+    s->refac->sm_kind = sm == PBG_SOLVER_CG ? 0 : sm == PBG_SOLVER_BICGS ? 1 : sm == PBG_SOLVER_CGS ? 2
+                        : sm == PBG_SOLVER_JACOBI ? 3 : 4;
+    s->refac->sm_prec = s->refac->sm_kind <= 2 ? p->prec : 0;
+    s->refac->sm_ci0 = s->ci_gen == s->mat_gen ? s->ci.p : nullptr;
     s->hhist.assign(p->max_cycles + 2, 0.0);
     RefACResult ar = s->refac->cycle(xd, bd, pa, cx, s->hhist.data(), (int)s->hhist.size());
     s->nhist = ar.nhist < (int)s->hhist.size() ? ar.nhist : (int)s->hhist.size();

@@ -1343,9 +1343,11 @@ void RefAC::smooth(int l, int mi, double res_rat, double res_tol, int ms, RefKry
   pr.mini = 1; pr.maxit = mi; pr.stalecount = ms;
   pr.res_rat = res_rat; pr.res_tol = res_tol; pr.scale = 1.0; pr.dV = L[l].dV; pr.hist_cap = 0;
   pr.seq = seq;
+  pr.prec = sm_prec;
+  pr.ci = l == 0 ? sm_ci0 : nullptr;  // coarse levels: ci = 1/c (additive_coarsen_system.cpp)
   MatView<double> A = view(l);
-  enqueue_ref_setup(A, L[l].phi.p, L[l].fnew.p, pr, 0, w, red, st, s);
-  enqueue_ref_iters(A, L[l].phi.p, 0, mi, w, red, st, nullptr, s, seq != nullptr, 0);
+  enqueue_ref_setup(A, L[l].phi.p, L[l].fnew.p, pr, sm_kind, w, red, st, s);
+  enqueue_ref_iters(A, L[l].phi.p, sm_kind, mi, w, red, st, nullptr, s, seq != nullptr, sm_prec);
 }
 
 void RefAC::restrict_to(int l, RedPool &red, double *dmean, cudaStream_t s) {

@@ -95,6 +95,10 @@ class RefAC {
   DBuf<double> fold;
   double *seq = nullptr;   // exact-order reduction terms, or null
   MatView<double> A0v{};
+  // the smoother of every level (the Centered object's Linear): solver code
+  // of the drivers above, its Prec code, and level 0's stored ci (or null)
+  int sm_kind = 0, sm_prec = 0;
+  const double *sm_ci0 = nullptr;
 
   void build(const MatView<double> &A0, const uint8_t *aflag0, double h, cudaStream_t s);
   MatView<double> view(int l) const;

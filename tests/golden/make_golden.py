@@ -23,10 +23,12 @@ CASES = [
     # name, kind, problem kwargs, runs
     ("single16", O.KIND_SINGLE, dict(n=16), ["cg", "bicgs", "ac", "cg_ic0", "cg_ic2", "cg_ic3", "cgs",
                                              "bicgs_ic2", "cgs_ic0"]),
-    ("single12", O.KIND_SINGLE, dict(n=12), ["cg", "ac_w", "ac_f", "ac_noguard", "jacobi", "gs"]),
+    ("single12", O.KIND_SINGLE, dict(n=12), ["cg", "ac_w", "ac_f", "ac_noguard", "jacobi", "gs",
+                                             "acsm_gs", "acsm_bicgs"]),
     ("cyl24", O.KIND_CYL, dict(n=24, nb=3, rmin=2.0, rmax=4.0, rc=5.0), ["cg", "ac", "cg_ic2", "jacobi",
-                                                                          "gs"]),
-    ("odd15", O.KIND_BATCH, dict(index=40, n2d=0, s3=(15, 16)), ["cg", "ac", "jacobi", "gs"]),
+                                                                          "gs", "acsm_gs", "acsm_jacobi"]),
+    ("odd15", O.KIND_BATCH, dict(index=40, n2d=0, s3=(15, 16)), ["cg", "ac", "jacobi", "gs",
+                                                                 "acsm_bicgs"]),
     ("flat2d", O.KIND_BATCH, dict(index=1, n2d=8, s2=(24, 40)), ["cg", "bicgs", "ac", "jacobi", "gs"]),
     # non-symmetric: upwind convection along +x added to the fixture
     ("conv12", O.KIND_SINGLE, dict(n=12, convect=2e-5), ["bicgs", "cgs", "bicgs_ic0", "bicgs_ic2",
@@ -113,6 +115,8 @@ def main():
                 extra = dict(cycle="F")
             elif run == "ac_noguard":
                 extra = dict(guard=0, maxcyc=6)
+            elif run.startswith("acsm_"):  # AC with the Pressure's solver of that kind
+                extra = dict(acsm=run.split("_")[1])
             kw_run = dict(resrat=1e-8)
             if solver in ("jacobi", "gs"):
                 kw_run = dict(STATIONARY)

@@ -169,6 +169,30 @@ def test_ac_parity(engine, oracle, name, run, exact):
         assert relerr(x, g[run + "_x"]) <= 1e-8, relerr(x, g[run + "_x"])
 
 
+ACSM_RUNS = [(n, k) for n in NAMES for k in load(n) if k.startswith("acsm_") and k.endswith("_x")]
+
+
+@pytest.mark.parametrize("name,key", ACSM_RUNS)
+def test_ac_with_other_smoothers(engine, oracle, name, key):
+    """AC whose levels are smoothed by the Centered object's own solver:
+    Gauss-Seidel, Jacobi or BiCGS instead of CG (ref_harness --acsm). With
+    exact sums the cycles, the residual history and the iterate are the
+    compiled reference's."""
+    run = key[:-2]
+    g = load(name)
+    P = problem_of(g, oracle)
+    x = np.zeros(P.N)
+    with session_for(engine, P) as s:
+        s.upload_ci(g["ci"])
+        ac = engine.AC(s, exact_sums=True, smoother=run.split("_")[1])
+        ok, ncyc = ac.cycle(x, P.b.copy(), loop=engine.CYCLE_V, factor=1e-8)
+        hist = s.history()
+    assert ok == bool(g[run + "_converged"])
+    assert ncyc == int(g[run + "_cycles"])
+    np.testing.assert_allclose(hist, g[run + "_hist"], rtol=1e-13)
+    assert np.array_equal(x, g[run + "_x"])
+
+
 @pytest.mark.parametrize("name", ["single16", "cyl24", "odd15", "flat2d"])
 def test_ac_hierarchy_and_coarse_operators(engine, oracle, name):
     P = problem_of(load(name), oracle)
