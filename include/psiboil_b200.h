@@ -10,12 +10,17 @@
  * interface it stands in for:
  *   - Linear::solve / Krylov::solve        Src/Solver/Linear/linear.h:46-56,
  *                                          Src/Solver/Linear/Krylov/krylov.h:20-30
- *   - CG::solve, BiCGS::solve              Src/Solver/Linear/Krylov/cg.cpp:10-182,
- *                                          bicgs.cpp:9-229
+ *   - CG::solve, BiCGS::solve, CGS::solve  Src/Solver/Linear/Krylov/cg.cpp:10-182,
+ *                                          bicgs.cpp:9-229, cgs.cpp:8-210
+ *   - Jacobi::solve, GaussSeidel::solve    Src/Solver/Linear/Iterative/jacobi.cpp:10-75,
+ *                                          gaussseidel.cpp:10-117
  *   - AC::AC, AC::cycle and the vcycle/fcycle/wcycle/fullcycle overloads and
  *     setters                             Src/Solver/Additive/additive.h:26-142
  *   - Matrix (c, w, e, s, n, b, t, ci)     Src/Matrix/matrix.h:23-54
  *   - Pressure::discretize                 Src/Equation/Centered/Pressure/pressure_discretize.cpp:11-151
+ *     (with a cut Body: Src/Body/body_interface.cpp fV, fSw..fSt)
+ *   - Pressure::update_rhs                 pressure_update_rhs.cpp:16-139
+ *   - Momentum::project                    Src/Equation/Staggered/Momentum/momentum_project.cpp:11-80
  *   - Scalar::operator=(A_x), (y_m_A_x)    Src/Field/Scalar/scalar_operators.cpp:22-72
  *   - Scalar::dot, dot_voldiv_avg          Src/Field/Scalar/scalar.h:296-326
  *
