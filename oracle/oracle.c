@@ -570,6 +570,11 @@ struct orc_ac {
   double *res;        /* fine residual scratch                        */
   /* cycle parameters (additive.cpp:11-19) */
   double resrat_val, restol_val;
+  /* the smoother of every level (the Centered object's Linear): 0 CG,
+   * 1 BiCGS, 2 CGS (with prec), 3 Jacobi, 4 Gauss-Seidel; ci0 level 0's
+   * stored ci (coarse levels: 1/c) */
+  int sm_kind, sm_prec;
+  const double *ci0;
 };
 
 /* Domain::factor (domain_factor.cpp:4-21): first factor = smallest prime */
@@ -817,11 +822,39 @@ static double residual(orc_ac *ac, double *linf) {
   return r2;
 }
 
-/* call_smoother / call_solver (additive_cycle_functions.cpp:90-107):
- * CG on level l with scale dti*scale = 1 */
+/* call_smoother / call_solver (additive_cycle_functions.cpp:90-107): the
+ * level's Linear solver (CG unless set) with scale dti*scale = 1 */
 static void smooth(orc_ac *ac, int l, int mi, double res_rat, double res_tol, int ms) {
   orc_level *lv = &ac->L[l];
-  orc_cg(&lv->A, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, 1.0, ms, lv->dV, NULL, NULL);
+  const int k = ac->sm_kind;
+  if (k == 1) {
+    orc_bicgs_prec(&lv->A, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, 1.0, ms, lv->dV, NULL, NULL,
+                   ac->sm_prec);
+  } else if (k == 2) {
+    orc_cgs_prec(&lv->A, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, 1.0, ms, lv->dV, NULL, NULL,
+                 ac->sm_prec);
+  } else if (k == 3 || k == 4) {
+    /* coarse levels: ci = 1/c (additive_coarsen_system.cpp) */
+    const size_t N = (size_t)lv->A.nx * lv->A.ny * lv->A.nz;
+    double *ci = NULL;
+    if (l > 0 || !ac->ci0) {
+      ci = malloc(N * sizeof(double));
+      for (size_t c = 0; c < N; ++c) ci[c] = 1.0 / lv->A.c[c];
+    }
+    const double *cv = ci ? ci : ac->ci0;
+    if (k == 3) orc_jacobi(&lv->A, cv, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, NULL, NULL);
+    else orc_gauss_seidel(&lv->A, cv, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, 1.0, ms, lv->dV, NULL, NULL);
+    free(ci);
+  } else {
+    orc_cg_prec(&lv->A, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, 1.0, ms, lv->dV, NULL, NULL,
+                ac->sm_prec);
+  }
+}
+
+void orc_ac_set_smoother(orc_ac *ac, int kind, int prec, const double *ci0) {
+  ac->sm_kind = kind;
+  ac->sm_prec = prec;
+  ac->ci0 = ci0;
 }
 
 static void v_cycle(orc_ac *ac, int l, const int mv[3], const int ms[3]);

@@ -83,7 +83,8 @@ int orc_gauss_seidel(const orc_mat *A, const double *ci, double *x, const double
                      int maxit, double res_rat, double res_tol, double scale, int stalecount,
                      double dV, orc_stats *st, double *hist);
 
-/* Additive-correction multigrid (Src/Solver/Additive) around CG smoothers. */
+/* Additive-correction multigrid (Src/Solver/Additive) around the levels'
+ * solver (CG unless orc_ac_set_smoother names another). */
 typedef struct orc_ac orc_ac;
 
 /* Builds the level hierarchy with Domain::coarsen's rule
@@ -92,6 +93,10 @@ typedef struct orc_ac orc_ac;
  * active. h: fine spacing (uniform). is2d: z is a dummy direction. */
 orc_ac *orc_ac_create(const orc_mat *A, const uint8_t *aflag, double h);
 void orc_ac_destroy(orc_ac *ac);
+/* The solver of every level (default CG): 0 CG, 1 BiCGS, 2 CGS (with the
+ * Prec code prec), 3 Jacobi, 4 Gauss-Seidel (level 0 with ci0, the stored
+ * A.ci, kept by the caller; coarse levels with 1/c). */
+void orc_ac_set_smoother(orc_ac *ac, int kind, int prec, const double *ci0);
 int orc_ac_nlevels(const orc_ac *ac);
 void orc_ac_level_dims(const orc_ac *ac, int l, int *dims /* 3 */);
 /* Coarse operators of all levels (AC::coarsen_system,

@@ -75,6 +75,7 @@ def lib():
         L.orc_ac_create.restype = ctypes.c_void_p
         L.orc_ac_create.argtypes = [ctypes.POINTER(OrcMat), ctypes.c_void_p, ctypes.c_double]
         L.orc_ac_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_ac_set_smoother.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp]
         L.orc_ac_nlevels.restype = ctypes.c_int
         L.orc_ac_nlevels.argtypes = [ctypes.c_void_p]
         L.orc_ac_level_dims.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
@@ -211,13 +212,18 @@ def cg(P, b=None, x0=None, mini=1, maxit=20000, res_rat=1e-8, res_tol=1e-18, sca
 class AC:
     """Oracle AC hierarchy for one problem (reference coarsening rule)."""
 
-    def __init__(self, P):
+    SMOOTHERS = {"cg": 0, "bicgs": 1, "cgs": 2, "jacobi": 3, "gs": 4}
+
+    def __init__(self, P, smoother="cg", prec="di"):
         self.P = P
         aflag = (1 - P.solid).astype(np.uint8)
         self._aflag = aflag
         m = P.mat()
         self._m = m
         self.h = lib().orc_ac_create(ctypes.byref(m), aflag.ctypes.data, P.h)
+        if smoother != "cg" or prec != "di":
+            self._ci = np.ascontiguousarray(P.ci, dtype=np.float64)  # level 0's stored ci
+            lib().orc_ac_set_smoother(self.h, self.SMOOTHERS[smoother], PRECS[prec], _p(self._ci))
 
     def __del__(self):
         if getattr(self, "h", None):

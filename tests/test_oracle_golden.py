@@ -64,6 +64,22 @@ def test_ac_bit_exact(oracle, name, run):
     assert np.array_equal(x, g[run + "_x"])
 
 
+@pytest.mark.parametrize("name,run", [(n, k[:-2]) for n in NAMES for k in load(n)
+                                      if k.startswith("acsm_") and k.endswith("_x")])
+def test_ac_other_smoothers_bit_exact(oracle, name, run):
+    """AC whose levels are smoothed by Gauss-Seidel, Jacobi or BiCGS (the
+    reference's Pressure solver of that kind): cycles, history and iterate."""
+    g = load(name)
+    P = problem_of(g, oracle)
+    assert np.array_equal(P.ci, g["ci"])
+    ac = oracle.AC(P, smoother=run.split("_")[1])
+    x, st = ac.cycle(factor=1e-8, loop=1)
+    assert st["cycles"] == int(g[run + "_cycles"])
+    assert st["converged"] == int(g[run + "_converged"])
+    np.testing.assert_allclose(st["hist"], g[run + "_hist"], rtol=1e-13, atol=0)
+    assert np.array_equal(x, g[run + "_x"])
+
+
 def test_mt64_matches_standard_engine(oracle):
     # the 10000th draw of a default-seeded mt19937_64 is fixed by the C++ standard
     import ctypes
