@@ -77,7 +77,8 @@ enum { PBG_BC_NEUMANN_ = 0, PBG_BC_DIRICHLET_ = 1 };
 enum {
   PBG_SOLVER_CG = 0,      /* CG with diagonal preconditioner (reference parity)   */
   PBG_SOLVER_BICGS = 1,   /* BiCGStab with diagonal preconditioner (parity)       */
-  PBG_SOLVER_AC = 2,      /* additive-correction multigrid, CG smoother (parity)  */
+  PBG_SOLVER_AC = 2,      /* additive-correction multigrid, level solver from
+                             ac_smoother (parity)                               */
   PBG_SOLVER_ENGINE = 3,  /* flexible CG + AC K-cycle (the engine's fast solver)  */
   PBG_SOLVER_CGS = 4,     /* conjugate gradient squared, CGS::solve (parity)       */
   PBG_SOLVER_JACOBI = 5,  /* Jacobi::solve (Src/Solver/Linear/Iterative, parity)   */
@@ -285,6 +286,14 @@ int pbg_history(const pbg_session *s, double *out, int cap, int *count);
 int pbg_spmv(pbg_session *s, const double *x, double *y, int where);
 int pbg_residual(pbg_session *s, const double *x, const double *b, double *r, int where);
 int pbg_dot(pbg_session *s, const double *x, const double *y, int where, double out[2]);
+/* Sequential sum in index order, rounded after every addition: out[0] for
+ * a, out[1] for b (0 when b is NULL), n terms. It reproduces the
+ * reference's `real sum = 0; for_ijk sum += ...` loops (scalar.h:296-326,
+ * the reductions behind CG::solve and AC::residual) bit for bit, computed
+ * in parallel; the reference-parity solvers use the same reduction when
+ * pbg_params.exact_sums is set. */
+int pbg_seq_sum(pbg_session *s, const double *a, const double *b, long long n, int where,
+                double out[2]);
 
 /* Multigrid hierarchy sizes: count and per-level dims (3 ints per level).
  * kind 0: the reference AC hierarchy (Domain::coarsen rule), kind 1: the
@@ -450,20 +459,22 @@ int pbg_bck_read_compact(const char *path, int nfields, double *const *fields, i
                          int where);
 
 /* Dot products without allocating (no counterpart in the reference).
- * For callers that cannot call cudaMalloc where they need a dot product —
- * code recorded into a CUDA graph by stream capture, callers whose device
- * memory belongs to another allocator or pool, time-step loops that must not
- * take an allocation's latency or failure path. Same results as pbg_dot:
+ * For callers that cannot call cudaMalloc where they need a dot product: a
+ * host code that hands the whole device memory to its own pool at start-up
+ * (a further cudaMalloc fails or takes memory the pool counted on), or a
+ * time-step loop that must not take an allocation's latency, device-wide
+ * synchronisation or failure path in mid-step. Same results as pbg_dot:
  * out[0] = x.y, out[1] = sum x*y/dV/dV / n / n, written to `out` (two
  * doubles in device memory); x and y are device arrays of n doubles, on
  * `stream` (a cudaStream_t, NULL for the default stream) of the current
  * device. No session is needed and nothing is allocated: the scratch is a
  * fixed array of about 19 KB in the library's device memory, held on every
  * GPU that loads the library until the process exits; n must not exceed
- * 2^31 - 1. Every call on a device shares that array and it keeps the last
- * call's contents; calls that overlap on the GPU race and must be
- * serialised. The first call on a device looks the array up for that device
- * (make it before any stream capture). */
+ * 2^31 - 1 (larger n is rejected with PBG_ERR_ARG). Every call on a device
+ * shares that array and it keeps the last call's contents; calls that
+ * overlap on the GPU race and must be serialised. The first call on a
+ * device looks the array up for that device (make that call before any
+ * stream capture); a failed look-up is retried by the next call. */
 int pbg_dot_noalloc(const double *x, const double *y, long long n, double dV, double *out,
                     void *stream);
 

@@ -21,7 +21,7 @@ All outputs stay under `oracle/_ref/` (git-ignored). The built harness
 travels to the GPU host with the working tree; the reference sources do not
 need to exist there.
 
-Usage: python oracle/build_ref.py [--ref /path/to/reference] [-j N]
+Usage: python oracle/build_ref.py [--ref DIR] [-j N]   (DIR defaults to $PBG_REFERENCE)
 """
 import argparse
 import os
@@ -132,7 +132,10 @@ def build(ref, jobs):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("PBG_REFERENCE"),
+                    help="PSI-BOIL source tree (default: $PBG_REFERENCE)")
     ap.add_argument("-j", type=int, default=os.cpu_count() or 4)
     a = ap.parse_args()
+    if not a.ref:
+        raise SystemExit("name the reference source tree: --ref DIR or PBG_REFERENCE=DIR")
     build(a.ref, a.j)

@@ -112,6 +112,7 @@ _SIGS = {
     "pbg_spmv": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
     "pbg_residual": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int]),
     "pbg_dot": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _dp]),
+    "pbg_seq_sum": (ctypes.c_int, [_vp, _vp, _vp, _ll, ctypes.c_int, _dp]),
     "pbg_levels": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                   ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
     "pbg_ac_level_matrix": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
@@ -224,17 +225,36 @@ def _check(code):
         raise PbgError(code, lib().pbg_last_error().decode())
 
 
-def _ptr(a):
-    """(pointer, where) of a numpy array or a CUDA tensor."""
+def _ptr(a, dtype="float64"):
+    """(pointer, where) of a numpy array or a CUDA tensor of the given dtype,
+    C-contiguous; anything else raises before it reaches the library."""
     if a is None:
         return None, HOST
-    if hasattr(a, "data_ptr") and getattr(a, "is_cuda", False):
+    if hasattr(a, "data_ptr") and hasattr(a, "is_cuda"):
+        if not a.is_cuda:
+            raise TypeError("tensors must be CUDA tensors (use numpy arrays for host memory)")
+        if str(a.dtype) != "torch." + dtype:
+            raise TypeError("expected a torch.%s tensor, got %s" % (dtype, a.dtype))
+        if not a.is_contiguous():
+            raise ValueError("tensors must be contiguous")
         return a.data_ptr(), DEVICE
     if isinstance(a, np.ndarray):
         if not a.flags["C_CONTIGUOUS"]:
             raise ValueError("arrays must be C-contiguous")
+        if a.dtype != np.dtype(dtype):
+            raise TypeError("expected a %s array, got %s" % (dtype, a.dtype))
         return a.ctypes.data, HOST
     raise TypeError("expected a numpy array or a CUDA tensor, got %r" % type(a))
+
+
+def _ptrn(a, n, dtype="float64"):
+    """_ptr that also requires at least n elements (the compact layout)."""
+    p = _ptr(a, dtype)
+    if a is not None:
+        size = a.numel() if hasattr(a, "numel") else a.size
+        if size < n:
+            raise ValueError("array holds %d elements, %d needed" % (size, n))
+    return p
 
 
 def default_params(solver):
@@ -245,7 +265,16 @@ def default_params(solver):
 
 def dot_noalloc(x, y, dV, out, stream=None):
     """pbg_dot_noalloc on CUDA tensors: out (2 doubles, device) = (x.y,
-    sum x*y/dV/dV / n / n); allocates nothing."""
+    sum x*y/dV/dV / n / n); allocates nothing.
+
+    x, y and out must be contiguous float64 CUDA tensors on the current
+    device; anything else raises here instead of reaching the kernel."""
+    import torch
+    dev = torch.cuda.current_device()
+    for name, t in (("x", x), ("y", y), ("out", out)):
+        _ptr(t)
+        if t.device.index != dev:
+            raise ValueError("%s is on cuda:%s, the current device is cuda:%d" % (name, t.device.index, dev))
     n = x.numel()
     if y.numel() != n or out.numel() < 2:
         raise ValueError("x and y must have the same length, out at least 2")
@@ -336,7 +365,7 @@ class Session:
     def assemble_pressure(self, rho, solid):
         """Pressure::discretize on the device (harmonic face density)."""
         pr, where = _ptr(rho)
-        ps, where2 = _ptr(solid)
+        ps, where2 = _ptr(solid, "uint8")
         if where != where2:
             raise ValueError("rho and solid must live in the same memory")
         _check(lib().pbg_assemble_pressure(self._h, pr, ps, where))
@@ -345,7 +374,7 @@ class Session:
         """Pressure::discretize of a two-phase mixture on the device
         (arithmetic face density from the colour; col None: one fluid)."""
         pc, where = _ptr(col)
-        ps, where2 = _ptr(solid)
+        ps, where2 = _ptr(solid, "uint8")
         if col is not None and solid is not None and where != where2:
             raise ValueError("col and solid must live in the same memory")
         if col is None:
@@ -356,14 +385,14 @@ class Session:
         """Pressure::update_rhs: rhs from the face velocities (solid: a
         voxel body, the immersed-body branch)."""
         pu, where = _ptr(u)
-        _check(lib().pbg_divergence(self._h, pu, _ptr(v)[0], _ptr(w)[0], _ptr(solid)[0], dt,
+        _check(lib().pbg_divergence(self._h, pu, _ptr(v)[0], _ptr(w)[0], _ptr(solid, "uint8")[0], dt,
                                     _ptr(rhs)[0], where))
         return rhs
 
     def project(self, p, col, rho_a, rho_b, dt, u, v, w, solid=None):
         """Momentum::project: u, v, w updated in place."""
         pp, where = _ptr(p)
-        _check(lib().pbg_project(self._h, pp, _ptr(col)[0], rho_a, rho_b, _ptr(solid)[0], dt,
+        _check(lib().pbg_project(self._h, pp, _ptr(col)[0], rho_a, rho_b, _ptr(solid, "uint8")[0], dt,
                                  _ptr(u)[0], _ptr(v)[0], _ptr(w)[0], where))
         return u, v, w
 
@@ -389,7 +418,7 @@ class Session:
         p updated in place. Returns the solver's Result."""
         pp, where = _ptr(p)
         res = Result()
-        _check(lib().pbg_pressure_step(self._h, _ptr(col)[0], rho_a, rho_b, _ptr(solid)[0], dt,
+        _check(lib().pbg_pressure_step(self._h, _ptr(col)[0], rho_a, rho_b, _ptr(solid, "uint8")[0], dt,
                                        _ptr(u)[0], _ptr(v)[0], _ptr(w)[0], pp, where,
                                        ctypes.byref(params), ctypes.byref(res)))
         return res
@@ -401,20 +430,33 @@ class Session:
 
     # -- operators ---------------------------------------------------------
     def spmv(self, x, y):
-        px, w = _ptr(x)
-        py, _ = _ptr(y)
+        px, w = _ptrn(x, self.ncell)
+        py, _ = _ptrn(y, self.ncell)
         _check(lib().pbg_spmv(self._h, px, py, w))
         return y
 
     def residual(self, x, b, r):
-        px, w = _ptr(x)
-        _check(lib().pbg_residual(self._h, px, _ptr(b)[0], _ptr(r)[0], w))
+        px, w = _ptrn(x, self.ncell)
+        _check(lib().pbg_residual(self._h, px, _ptrn(b, self.ncell)[0], _ptrn(r, self.ncell)[0], w))
         return r
 
     def dot(self, x, y):
         out = (ctypes.c_double * 2)()
-        px, w = _ptr(x)
-        _check(lib().pbg_dot(self._h, px, _ptr(y)[0], w, out))
+        px, w = _ptrn(x, self.ncell)
+        _check(lib().pbg_dot(self._h, px, _ptrn(y, self.ncell)[0], w, out))
+        return out[0], out[1]
+
+    def seq_sum(self, a, b=None):
+        """Sequential sums in index order (pbg_seq_sum): the rounded
+        left-to-right sum of a (and of b)."""
+        out = (ctypes.c_double * 2)()
+        pa, w = _ptr(a)
+        pb = None
+        if b is not None:
+            pb, w2 = _ptr(b)
+            if w2 != w or len(b) != len(a):
+                raise ValueError("a and b must have the same length and memory")
+        _check(lib().pbg_seq_sum(self._h, pa, pb, len(a), w, out))
         return out[0], out[1]
 
     def levels(self, kind=0):
@@ -432,8 +474,9 @@ class Session:
 
     # -- solve -------------------------------------------------------------
     def solve(self, x, b, params, strides=None, offset=0):
-        px, where = _ptr(x)
-        pb, where2 = _ptr(b)
+        need = self.ncell if strides is None else 0
+        px, where = _ptrn(x, need)
+        pb, where2 = _ptrn(b, need)
         if where != where2:
             raise ValueError("x and b must live in the same memory")
         res = Result()
@@ -732,7 +775,7 @@ class Batch:
 
     def set_fields(self, i, rho, solid):
         pr, wr = _ptr(rho)
-        ps, ws = _ptr(solid)
+        ps, ws = _ptr(solid, "uint8")
         if wr != ws:
             raise ValueError("rho and solid must live on the same side")
         _check(lib().pbg_batch_set_fields(self._h, i, pr, ps, wr))
@@ -830,7 +873,7 @@ class Server:
     def submit(self, sid, rhs, rho=None, solid=None):
         pb_, w = _ptr(rhs)
         pr, _ = _ptr(rho)
-        ps, _ = _ptr(solid)
+        ps, _ = _ptr(solid, "uint8")
         rid = _ll(-1)
         _check(lib().pbg_server_submit(self._h, sid, pr, ps, pb_, w, ctypes.byref(rid)))
         return rid.value

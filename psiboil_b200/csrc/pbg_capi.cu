@@ -822,11 +822,16 @@ void ensure_engine(pbg_session *s, bool mixed, int coarse_max) {
   }
 }
 
-// Scratch of the exact-order reductions (2 terms per cell), when requested.
+// Scratch of the exact-order reductions (2 terms per cell, the chunk and
+// group records and the look-back flags), when requested.
 double *exact_terms(pbg_session *s, const pbg_params *p) {
   if (!p->exact_sums) return nullptr;
-  if (s->seq.n < (size_t)(2 * s->ncell())) s->seq.alloc(2 * s->ncell());
-  return s->seq.p;
+  const size_t need = exact_scratch_doubles(s->ncell());
+  if (s->seq.n < need) {
+    s->seq.alloc(need);
+    exact_scratch_init(s->seq.p, s->ncell(), s->stream);
+  }
+  return exact_seq(s->seq.p);
 }
 
 int solve_device(pbg_session *s, double *xd, const double *bd, const pbg_params *p, pbg_result *r) {
@@ -1030,6 +1035,34 @@ static int op_run(pbg_session *s, int op, const double *x, const double *b, doub
       out2[0] = s->hbuf[0];
       out2[1] = s->hbuf[1] / n / n;
     }
+    return PBG_OK;
+  });
+}
+
+int pbg_seq_sum(pbg_session *s, const double *a, const double *b, long long n, int where, double out[2]) {
+  if (!s || !a || !out) return fail(PBG_ERR_ARG, "NULL argument");
+  if (n < 1 || n > (1LL << 31) - 1) return fail(PBG_ERR_ARG, "n must be in 1 .. 2^31-1");
+  return guard(s, [&]() -> int {
+    const double *da = a, *db = b;
+    DBuf<double> t1, t2, scratch(exact_scratch_doubles(n)), res(2);
+    if (where == PBG_HOST) {
+      t1.alloc(n);
+      PBG_CUDA(cudaMemcpyAsync(t1.p, a, n * 8, cudaMemcpyHostToDevice, s->stream));
+      da = t1.p;
+      if (b) {
+        t2.alloc(n);
+        PBG_CUDA(cudaMemcpyAsync(t2.p, b, n * 8, cudaMemcpyHostToDevice, s->stream));
+        db = t2.p;
+      }
+    }
+    exact_scratch_init(scratch.p, n, s->stream);
+    k_seq_sum<<<grid_exact(n), kThreads, 0, s->stream>>>(n, da, db, exact_seq(scratch.p),
+                                                          s->red.slot_count(0), res.p); note_launch();
+    PBG_CUDA(cudaGetLastError());
+    PBG_CUDA(cudaMemcpyAsync(s->hbuf, res.p, 16, cudaMemcpyDeviceToHost, s->stream));
+    PBG_CUDA(cudaStreamSynchronize(s->stream));
+    out[0] = s->hbuf[0];
+    out[1] = s->hbuf[1];
     return PBG_OK;
   });
 }

@@ -16,6 +16,8 @@
 #include <string>
 #include <utility>
 
+#include "pbg_exact_sum.cuh"
+
 namespace pbg {
 
 constexpr int kThreads = 256;          // threads per block of the streaming kernels
@@ -199,17 +201,21 @@ __device__ __forceinline__ void warp_sum(double (&v)[NV]) {
 
 // Returns true in thread 0 of the last block; out[] then holds the totals.
 //
-// Exact-order mode (seq != nullptr): the launch has one thread per element
-// (thread p holds element p's term in v), every term is stored in
-// seq[q*n + p], and the last block's thread 0 adds them in index order —
-// the reference's sequential i,j,k summation (Src/Field/Scalar/scalar.h:296-326)
-// reproduced to the bit. Used by the reference-parity solvers on request.
+// Exact-order mode (seq != nullptr, a scratch laid out by
+// exact_scratch_doubles): the launch has one thread per element (thread p
+// holds element p's term in v) and the result is the reference's sequential
+// i,j,k summation (Src/Field/Scalar/scalar.h:296-326) reproduced to the bit,
+// computed in parallel by exact_reduce (pbg_exact_sum.cuh). Used by the
+// reference-parity solvers on request.
 template <int NV>
 __device__ bool grid_reduce(double (&v)[NV], double *part, unsigned *count, double (&out)[NV],
                             double *seq = nullptr, long long n = 0) {
   __shared__ double sm[NV][kThreads / 32];
   __shared__ bool last;
-  if (seq) {
+  if constexpr (NV <= kExactVals) {
+    if (seq && blockDim.x == kExactChunkThreads) return exact_reduce<NV>(v, seq, n, count, out);
+  }
+  if (seq) {  // other launch shapes: the last block adds every term in order
     const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (p < n)
 #pragma unroll

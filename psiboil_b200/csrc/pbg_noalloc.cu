@@ -4,13 +4,13 @@
 // pbg_dot (pbg_capi.cu) reduces through per-block partial sums and an
 // arrival counter that live in the session's scratch, which the session
 // allocates with cudaMalloc. Some callers cannot allocate at the point where
-// they need a dot product: code running while a stream is being captured
-// into a CUDA graph (cudaMalloc is not permitted then), a caller whose device
-// memory is owned by another allocator or pool, or a time-step loop of a
-// host code that must not take an allocation's latency or failure path.
-// This variant takes device inputs and a device output and keeps its
-// scratch in a fixed file-scope __device__ array instead, so it calls no
-// cudaMalloc, cudaFree or allocating library routine.
+// they need a dot product: a host code that hands the whole device memory to
+// its own pool when it starts (a further cudaMalloc fails, or takes memory
+// the pool counted on), or a time-step loop that must not take an
+// allocation's latency, its device-wide synchronisation or its failure path
+// in the middle of a step. This variant takes device inputs and a device
+// output and keeps its scratch in a fixed file-scope __device__ array
+// instead, so it calls no cudaMalloc, cudaFree or allocating library routine.
 //
 // Limits and sharing: the scratch holds one partial sum per block for two
 // values (kMaxBlocks blocks), so any n up to 2^31 - 1 elements fits; larger
@@ -24,7 +24,8 @@
 // Set-up: the first call on a device, with that device current, looks up
 // the array's device address with cudaGetSymbolAddress (a host-side name of
 // a __device__ variable is not a device address) and keeps it for later
-// calls. Make the first call on each device before any stream capture.
+// calls; a look-up that fails is retried by the next call. Make the first
+// call on each device before any stream capture.
 #include <mutex>
 
 #include "../../include/psiboil_b200.h"
@@ -64,8 +65,8 @@ namespace {
 constexpr int kMaxDevices = 64;
 double *g_part_addr[kMaxDevices];
 unsigned *g_count_addr[kMaxDevices];
-std::once_flag g_once[kMaxDevices];
-cudaError_t g_setup_err[kMaxDevices];
+bool g_ready[kMaxDevices];
+std::mutex g_setup_mutex;
 
 int err(int code, const char *m) {
   set_last_error(m);
@@ -87,12 +88,23 @@ extern "C" int pbg_dot_noalloc(const double *x, const double *y, long long n, do
   if (e != cudaSuccess) return err(PBG_ERR_CUDA, cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return err(PBG_ERR_UNSUPPORTED, "pbg_dot_noalloc: device index too large");
   // once per device, with that device current: the array's device address
-  std::call_once(g_once[dev], [dev]() {
-    cudaError_t a = cudaGetSymbolAddress((void **)&g_part_addr[dev], g_noalloc_part);
-    cudaError_t b = cudaGetSymbolAddress((void **)&g_count_addr[dev], g_noalloc_count);
-    g_setup_err[dev] = a != cudaSuccess ? a : b;
-  });
-  if (g_setup_err[dev] != cudaSuccess) return err(PBG_ERR_CUDA, cudaGetErrorString(g_setup_err[dev]));
+  // (marked ready only after both look-ups succeed, so a failure is retried)
+  {
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!g_ready[dev]) {
+      double *pa = nullptr;
+      unsigned *ca = nullptr;
+      e = cudaGetSymbolAddress((void **)&pa, g_noalloc_part);
+      if (e == cudaSuccess) e = cudaGetSymbolAddress((void **)&ca, g_noalloc_count);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return err(PBG_ERR_CUDA, cudaGetErrorString(e));
+      }
+      g_part_addr[dev] = pa;
+      g_count_addr[dev] = ca;
+      g_ready[dev] = true;
+    }
+  }
   cudaStream_t s = (cudaStream_t)stream;
   // the arrival counter must start at zero
   e = cudaMemsetAsync(g_count_addr[dev], 0, sizeof(unsigned), s);

@@ -3,6 +3,8 @@
 // that the compiler cannot contract a multiply and an add into one FMA.
 // Only the order of the global sums differs from the reference (a tree
 // instead of a sequential i,j,k sum).
+#include <cstring>
+
 #include "pbg_ref_kernels.cuh"
 
 namespace pbg {
@@ -91,6 +93,39 @@ __global__ void k_dot2(long long N, const double *__restrict__ x, const double *
   }
   double o[2];
   if (grid_reduce<2>(v, part, count, o)) { out[0] = o[0]; out[1] = o[1]; }
+}
+
+// Sequential sum of n terms: out[0] = (..((0 + a0) + a1) + ..) + a_{n-1}, the
+// reference's `for_ijk sum += ...` order, and out[1] the same for b (when
+// given). One thread per term, exact-order reduction.
+__global__ void k_seq_sum(long long N, const double *__restrict__ a, const double *__restrict__ b,
+                          double *seq, unsigned *count, double *out) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double v[2] = {p < N ? a[p] : 0.0, (p < N && b) ? b[p] : 0.0};
+  double o[2];
+  if (grid_reduce<2>(v, nullptr, count, o, seq, N)) { out[0] = o[0]; out[1] = o[1]; }
+}
+
+void exact_scratch_init(double *base, long long ncell, cudaStream_t s) {
+  const long long ch = (ncell + kExactChunkThreads - 1) / kExactChunkThreads + 1;
+  const long long gr = (ch + kExactGroup - 1) / kExactGroup + 1;
+  char *q = reinterpret_cast<char *>(base) + kExactHdrBytes + sizeof(double) * (size_t)kExactVals * ncell;
+  ExactHdr h;
+  std::memset(&h, 0, sizeof(h));
+  h.crec = reinterpret_cast<ExactRec *>(q); q += sizeof(ExactRec) * kExactVals * (size_t)ch;
+  h.grec = reinterpret_cast<ExactRec *>(q); q += sizeof(ExactRec) * kExactVals * (size_t)gr;
+  h.agg = reinterpret_cast<double *>(q); q += sizeof(double) * kExactVals * (size_t)ch;
+  h.incl = reinterpret_cast<double *>(q); q += sizeof(double) * kExactVals * (size_t)ch;
+  h.flag = reinterpret_cast<unsigned *>(q); q += sizeof(unsigned) * (size_t)ch;
+  h.gcount = reinterpret_cast<unsigned *>(q); q += sizeof(unsigned) * (size_t)gr;
+  h.cap_chunks = ch;
+  h.cap_groups = gr;
+  h.gen = 1;
+  if ((size_t)(q - reinterpret_cast<char *>(base)) > exact_scratch_doubles(ncell) * sizeof(double))
+    throw CudaError("exact-sum scratch layout exceeds its allocation");
+  PBG_CUDA(cudaMemsetAsync(h.flag, 0, sizeof(unsigned) * (size_t)(ch + gr), s));
+  PBG_CUDA(cudaMemcpyAsync(base, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+  PBG_CUDA(cudaStreamSynchronize(s));
 }
 
 // ---------------------------------------------------------------------------

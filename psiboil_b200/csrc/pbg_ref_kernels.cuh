@@ -43,6 +43,11 @@ struct RefKrylovResult {
 __global__ void k_spmv_ref(MatView<double> A, const double *__restrict__ x, double *__restrict__ y);
 __global__ void k_resid_ref(MatView<double> A, const double *__restrict__ x,
                             const double *__restrict__ b, double *__restrict__ r);
+__global__ void k_seq_sum(long long N, const double *__restrict__ a, const double *__restrict__ b,
+                          double *seq, unsigned *count, double *out);
+// Lays out an exact-order reduction scratch of exact_scratch_doubles(ncell)
+// doubles at base (header, records, zeroed flags and counters).
+void exact_scratch_init(double *base, long long ncell, cudaStream_t s);
 __global__ void k_dot2(long long N, const double *__restrict__ x, const double *__restrict__ y,
                        double dV, double *part, unsigned *count, double *out);
 
