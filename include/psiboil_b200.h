@@ -71,7 +71,7 @@ enum {
 };
 
 enum { PBG_HOST = 0, PBG_DEVICE = 1 };
-enum { PBG_BC_NEUMANN_ = 0, PBG_BC_DIRICHLET_ = 1 };
+enum { PBG_BC_NEUMANN_ = 0, PBG_BC_DIRICHLET_ = 1, PBG_BC_PERIODIC_ = 2 };
 
 /* solvers */
 enum {
@@ -163,8 +163,16 @@ void pbg_params_default(pbg_params *p, int solver);
 /* A session owns one grid (nx, ny, nz interior cells, nz == 1 for 2-D, uniform
  * spacing h), its matrix, the multigrid hierarchies and all scratch on one
  * device. bc: imin, imax, jmin, jmax, kmin, kmax (PBG_BC_NEUMANN_ |
- * PBG_BC_DIRICHLET_), used by pbg_assemble_pressure. Stands in for the
- * Centered/Pressure object plus its Linear solver (centered.h:62-200). */
+ * PBG_BC_DIRICHLET_ | PBG_BC_PERIODIC_), used by pbg_assemble_pressure.
+ * PBG_BC_PERIODIC_ goes on both faces of an axis: the matrix's couplings
+ * on that axis's outer faces then join the cells at the two ends, as the
+ * reference's periodic halo does (Scalar::exchange,
+ * scalar_exchange.cpp:47-58, with a zero jump value). The reference-parity
+ * solvers (CG, BiCGS, CGS, Jacobi, Gauss-Seidel, IC preconditioners, AC)
+ * take periodic matrices; the on-device assembly, the pressure step and the
+ * engine solver return PBG_ERR_UNSUPPORTED on a periodic session. Stands in
+ * for the Centered/Pressure object plus its Linear solver
+ * (centered.h:62-200). */
 int pbg_session_create(int nx, int ny, int nz, double h, const int bc[6], int device,
                        pbg_session **out);
 int pbg_session_destroy(pbg_session *s);

@@ -58,8 +58,8 @@ def flow_state(P, stream=0):
     nx, ny, nz = P.dims
     a = P.args
     params = np.array([a["n"], a["nb"], a["rmin"], a["rmax"], a["rc"], a["ratio"], a["index"],
-                       a["n2d"], a["s2"][0], a["s2"][1], a["s3"][0], a["s3"][1], stream],
-                      dtype=np.float64)
+                       a["n2d"], a["s2"][0], a["s2"][1], a["s3"][0], a["s3"][1], stream,
+                       a.get("periodic", 0)], dtype=np.float64)
     col = np.zeros((nx, ny, nz))
     u = np.zeros((nx + 1, ny, nz))
     v = np.zeros((nx, ny + 1, nz))

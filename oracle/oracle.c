@@ -18,17 +18,28 @@
 /* Scalar operators                                                    */
 /* ------------------------------------------------------------------ */
 
+/* The value of field x at (i, j, k), which may lie one cell outside the
+ * grid: the reference's halo, zero on a non-periodic face and the cell at
+ * the other end on a periodic one (scalar_exchange.cpp:47-58). */
+static double halo(const orc_mat *A, const double *x, int i, int j, int k) {
+  const int nx = A->nx, ny = A->ny, nz = A->nz;
+  if (i < 0 || i >= nx) { if (!(A->per & 1)) return 0.0; i = i < 0 ? i + nx : i - nx; }
+  if (j < 0 || j >= ny) { if (!(A->per & 2)) return 0.0; j = j < 0 ? j + ny : j - ny; }
+  if (k < 0 || k >= nz) { if (!(A->per & 4)) return 0.0; k = k < 0 ? k + nz : k - nz; }
+  return x[IDX(i, j, k)];
+}
+
 /* scalar_operators.cpp:49-72: four passes; each pair sum is formed first
- * and then subtracted. Out-of-domain neighbours are the (zero) halo. */
+ * and then subtracted. Out-of-domain neighbours are the halo. */
 void orc_spmv(const orc_mat *A, const double *x, double *y) {
   const int nx = A->nx, ny = A->ny, nz = A->nz;
   for (int i = 0; i < nx; ++i)
     for (int j = 0; j < ny; ++j)
       for (int k = 0; k < nz; ++k) {
         size_t p = IDX(i, j, k);
-        double xw = i > 0 ? x[IDX(i - 1, j, k)] : 0.0, xe = i < nx - 1 ? x[IDX(i + 1, j, k)] : 0.0;
-        double xs = j > 0 ? x[IDX(i, j - 1, k)] : 0.0, xn = j < ny - 1 ? x[IDX(i, j + 1, k)] : 0.0;
-        double xb = k > 0 ? x[IDX(i, j, k - 1)] : 0.0, xt = k < nz - 1 ? x[IDX(i, j, k + 1)] : 0.0;
+        double xw = halo(A, x, i - 1, j, k), xe = halo(A, x, i + 1, j, k);
+        double xs = halo(A, x, i, j - 1, k), xn = halo(A, x, i, j + 1, k);
+        double xb = halo(A, x, i, j, k - 1), xt = halo(A, x, i, j, k + 1);
         double v = A->c[p] * x[p];
         v -= (A->w[p] * xw + A->e[p] * xe);
         v -= (A->s[p] * xs + A->n[p] * xn);
@@ -44,9 +55,9 @@ void orc_resid(const orc_mat *A, const double *x, const double *b, double *r) {
     for (int j = 0; j < ny; ++j)
       for (int k = 0; k < nz; ++k) {
         size_t p = IDX(i, j, k);
-        double xw = i > 0 ? x[IDX(i - 1, j, k)] : 0.0, xe = i < nx - 1 ? x[IDX(i + 1, j, k)] : 0.0;
-        double xs = j > 0 ? x[IDX(i, j - 1, k)] : 0.0, xn = j < ny - 1 ? x[IDX(i, j + 1, k)] : 0.0;
-        double xb = k > 0 ? x[IDX(i, j, k - 1)] : 0.0, xt = k < nz - 1 ? x[IDX(i, j, k + 1)] : 0.0;
+        double xw = halo(A, x, i - 1, j, k), xe = halo(A, x, i + 1, j, k);
+        double xs = halo(A, x, i, j - 1, k), xn = halo(A, x, i, j + 1, k);
+        double xb = halo(A, x, i, j, k - 1), xt = halo(A, x, i, j, k + 1);
         double v = b[p] - A->c[p] * x[p];
         v += A->w[p] * xw + A->e[p] * xe;
         v += A->s[p] * xs + A->n[p] * xn;
@@ -520,18 +531,22 @@ int orc_gauss_seidel(const orc_mat *A, const double *ci, double *x, const double
   }
   int converged = 0, it, broke = 0;
   so.status = 1;
+  /* the halo is filled by the exchange before each sweep (:12, :53): on a
+   * periodic face it holds the other end's value from before the sweep */
+  double *xh = calloc(N, sizeof(double));
   for (it = 0; it < maxit; ++it) {
+    memcpy(xh, x, N * sizeof(double));
     for (int i = 0; i < nx; ++i)
       for (int j = 0; j < ny; ++j)
         for (int k = 0; k < nz; ++k) {
           const size_t p = ((size_t)i * ny + j) * nz + k;
           double v = b[p];
-          v += A->w[p] * (i > 0 ? x[p - SI] : 0.0);
-          v += A->e[p] * (i < nx - 1 ? x[p + SI] : 0.0);
-          v += A->s[p] * (j > 0 ? x[p - SJ] : 0.0);
-          v += A->n[p] * (j < ny - 1 ? x[p + SJ] : 0.0);
-          v += A->b[p] * (k > 0 ? x[p - 1] : 0.0);
-          v += A->t[p] * (k < nz - 1 ? x[p + 1] : 0.0);
+          v += A->w[p] * (i > 0 ? x[p - SI] : halo(A, xh, i - 1, j, k));
+          v += A->e[p] * (i < nx - 1 ? x[p + SI] : halo(A, xh, i + 1, j, k));
+          v += A->s[p] * (j > 0 ? x[p - SJ] : halo(A, xh, i, j - 1, k));
+          v += A->n[p] * (j < ny - 1 ? x[p + SJ] : halo(A, xh, i, j + 1, k));
+          v += A->b[p] * (k > 0 ? x[p - 1] : halo(A, xh, i, j, k - 1));
+          v += A->t[p] * (k < nz - 1 ? x[p + 1] : halo(A, xh, i, j, k + 1));
           x[p] = ci[p] * v;
         }
     orc_resid(A, x, b, r);
@@ -546,7 +561,7 @@ int orc_gauss_seidel(const orc_mat *A, const double *ci, double *x, const double
   so.printed = it + 1;
   so.res = res;
   if (st) *st = so;
-  free(r); free(win.v);
+  free(r); free(win.v); free(xh);
   return converged;
 }
 
@@ -575,6 +590,11 @@ struct orc_ac {
    * stored ci (coarse levels: 1/c) */
   int sm_kind, sm_prec;
   const double *ci0;
+  /* AC's own solver (AC(cen, sol), additive.cpp:41-45) for call_solver:
+   * sol_kind -1 = the levels' solver */
+  int sol_kind, sol_prec;
+  int use_linf;       /* AC::use_linf_error (additive.h:141) */
+  int flex_capped;    /* the last flex cycle hit its visit bound */
 };
 
 /* Domain::factor (domain_factor.cpp:4-21): first factor = smallest prime */
@@ -597,6 +617,7 @@ static void alloc_level(orc_level *lv) {
   lv->fnew = calloc(N, sizeof(double));
   lv->aflag = calloc(N, 1);
   lv->A.nx = lv->nx; lv->A.ny = lv->ny; lv->A.nz = lv->nz;
+  lv->A.per = 0;
 }
 
 /* additive.cpp:8-48 + domain_coarsen.cpp:6-112 + additive_coarsen_flag.cpp */
@@ -604,10 +625,12 @@ orc_ac *orc_ac_create(const orc_mat *A, const uint8_t *aflag, double h) {
   orc_ac *ac = calloc(1, sizeof(orc_ac));
   ac->resrat_val = 1.0e-18; /* boil::atto */
   ac->restol_val = 1.0e-18;
+  ac->sol_kind = -1;
   orc_level *L0 = &ac->L[0];
   L0->nx = A->nx; L0->ny = A->ny; L0->nz = A->nz;
   L0->CI = L0->CJ = L0->CK = 1;
   alloc_level(L0);
+  L0->A.per = A->per;
   size_t N0 = (size_t)A->nx * A->ny * A->nz;
   memcpy(L0->A.c, A->c, N0 * 8); memcpy(L0->A.w, A->w, N0 * 8);
   memcpy(L0->A.e, A->e, N0 * 8); memcpy(L0->A.s, A->s, N0 * 8);
@@ -635,6 +658,7 @@ orc_ac *orc_ac_create(const orc_mat *A, const uint8_t *aflag, double h) {
     hx *= c->CI; hy *= c->CJ; hz *= c->CK;
     c->dV = hx * hy * hz;
     alloc_level(c);
+    c->A.per = A->per; /* coarse Scalars keep the boundary conditions */
     /* OR of the fine active flags (additive_coarsen_flag.cpp:20-38) */
     const int nyf = f->ny, nzf = f->nz;
     for (int I = 0; I < c->nx; ++I)
@@ -740,7 +764,7 @@ static void restriction(const orc_level *h, orc_level *H) {
   const int nxf = h->nx, nyf = h->ny, nzf = h->nz;
   double *D = malloc(sizeof(double) * CI * CJ * CK);
 #define FI(i, j, k) (((size_t)(i) * nyf + (size_t)(j)) * nzf + (size_t)(k))
-#define PHI(i, j, k) (((i) < 0 || (i) >= nxf || (j) < 0 || (j) >= nyf || (k) < 0 || (k) >= nzf) ? 0.0 : h->phi[FI(i, j, k)])
+#define PHI(i, j, k) halo(&h->A, h->phi, (i), (j), (k))
 #define DD(i, j, k) D[((i) * CJ + (j)) * CK + (k)]
   for (int I = 0; I < H->nx; ++I)
     for (int J = 0; J < H->ny; ++J)
@@ -824,15 +848,20 @@ static double residual(orc_ac *ac, double *linf) {
 
 /* call_smoother / call_solver (additive_cycle_functions.cpp:90-107): the
  * level's Linear solver (CG unless set) with scale dti*scale = 1 */
-static void smooth(orc_ac *ac, int l, int mi, double res_rat, double res_tol, int ms) {
+/* call_smoother (as_solver 0, the level's Linear) and call_solver
+ * (as_solver 1, AC's own solver); returns the solver's converged flag */
+static int smooth_as(orc_ac *ac, int l, int mi, double res_rat, double res_tol, int ms, int as_solver) {
   orc_level *lv = &ac->L[l];
-  const int k = ac->sm_kind;
+  const int use_sol = as_solver && ac->sol_kind >= 0;
+  const int k = use_sol ? ac->sol_kind : ac->sm_kind;
+  const int prec = use_sol ? ac->sol_prec : ac->sm_prec;
+  int ok;
   if (k == 1) {
-    orc_bicgs_prec(&lv->A, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, 1.0, ms, lv->dV, NULL, NULL,
-                   ac->sm_prec);
+    ok = orc_bicgs_prec(&lv->A, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, 1.0, ms, lv->dV, NULL, NULL,
+                        prec);
   } else if (k == 2) {
-    orc_cgs_prec(&lv->A, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, 1.0, ms, lv->dV, NULL, NULL,
-                 ac->sm_prec);
+    ok = orc_cgs_prec(&lv->A, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, 1.0, ms, lv->dV, NULL, NULL,
+                      prec);
   } else if (k == 3 || k == 4) {
     /* coarse levels: ci = 1/c (additive_coarsen_system.cpp) */
     const size_t N = (size_t)lv->A.nx * lv->A.ny * lv->A.nz;
@@ -842,19 +871,41 @@ static void smooth(orc_ac *ac, int l, int mi, double res_rat, double res_tol, in
       for (size_t c = 0; c < N; ++c) ci[c] = 1.0 / lv->A.c[c];
     }
     const double *cv = ci ? ci : ac->ci0;
-    if (k == 3) orc_jacobi(&lv->A, cv, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, NULL, NULL);
-    else orc_gauss_seidel(&lv->A, cv, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, 1.0, ms, lv->dV, NULL, NULL);
+    if (k == 3) ok = orc_jacobi(&lv->A, cv, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, NULL, NULL);
+    else ok = orc_gauss_seidel(&lv->A, cv, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, 1.0, ms, lv->dV,
+                               NULL, NULL);
     free(ci);
   } else {
-    orc_cg_prec(&lv->A, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, 1.0, ms, lv->dV, NULL, NULL,
-                ac->sm_prec);
+    ok = orc_cg_prec(&lv->A, lv->phi, lv->fnew, 1, mi, res_rat, res_tol, 1.0, ms, lv->dV, NULL, NULL,
+                     prec);
   }
+  return ok;
+}
+
+static void smooth(orc_ac *ac, int l, int mi, double res_rat, double res_tol, int ms) {
+  smooth_as(ac, l, mi, res_rat, res_tol, ms, 0);
+}
+
+/* call_solver */
+static void solve_l(orc_ac *ac, int l, int mi, double res_rat, double res_tol, int ms) {
+  smooth_as(ac, l, mi, res_rat, res_tol, ms, 1);
 }
 
 void orc_ac_set_smoother(orc_ac *ac, int kind, int prec, const double *ci0) {
   ac->sm_kind = kind;
   ac->sm_prec = prec;
   ac->ci0 = ci0;
+}
+
+int orc_ac_flex_capped(const orc_ac *ac) { return ac->flex_capped; }
+
+void orc_ac_set_params(orc_ac *ac, double resrat_val, double restol_val, int use_linf,
+                       int sol_kind, int sol_prec) {
+  ac->resrat_val = resrat_val;
+  ac->restol_val = restol_val;
+  ac->use_linf = use_linf;
+  ac->sol_kind = sol_kind;
+  ac->sol_prec = sol_prec;
 }
 
 static void v_cycle(orc_ac *ac, int l, const int mv[3], const int ms[3]);
@@ -865,11 +916,11 @@ static void v_cycle(orc_ac *ac, int l, const int mv[3], const int ms[3]) {
     smooth(ac, l, mv[0], ac->resrat_val, ac->restol_val, ms[0]);
     restriction(&ac->L[l], &ac->L[l + 1]);
     v_cycle(ac, l + 1, mv, ms);
-    smooth(ac, l, mv[2], ac->resrat_val, ac->restol_val, ms[2]);
+    solve_l(ac, l, mv[2], ac->resrat_val, ac->restol_val, ms[2]);
     if (l > 0) interpolation(&ac->L[l], &ac->L[l - 1]);
   } else {
-    smooth(ac, l, 100, -1.0, ac->restol_val, -1);
-    interpolation(&ac->L[l], &ac->L[l - 1]);
+    solve_l(ac, l, 100, -1.0, ac->restol_val, -1);
+    if (l > 0) interpolation(&ac->L[l], &ac->L[l - 1]);
   }
 }
 
@@ -883,11 +934,50 @@ static void fw_cycle(orc_ac *ac, int l, const int mv[3], const int ms[3], int w)
     restriction(&ac->L[l], &ac->L[l + 1]);
     if (w) fw_cycle(ac, l + 1, mv, ms, w);
     else v_cycle(ac, l + 1, mv, ms);
-    smooth(ac, l, mv[2], ac->resrat_val, ac->restol_val, ms[2]);
+    solve_l(ac, l, mv[2], ac->resrat_val, ac->restol_val, ms[2]);
     if (l > 0) interpolation(&ac->L[l], &ac->L[l - 1]);
   } else {
-    smooth(ac, l, 100, -1.0, ac->restol_val, -1);
-    interpolation(&ac->L[l], &ac->L[l - 1]);
+    solve_l(ac, l, 100, -1.0, ac->restol_val, -1);
+    if (l > 0) interpolation(&ac->L[l], &ac->L[l - 1]);
+  }
+}
+
+/* additive_recursive.cpp:161-197, the recursion unrolled into a loop over
+ * (level, sign): a level whose smoother converges hands its correction up
+ * (Sign::pos on the finer level: mv[2], ms[2]); one that does not restricts
+ * down (Sign::neg: mv[0], ms[0]); the coarsest level is solved and
+ * interpolated up with Sign::neg. It starts at level l and ends when level
+ * 0's smoother converges.
+ * The reference recurses without a bound and never returns when level 0
+ * never converges (AC::resrat at its default atto, for instance); here at
+ * most 1000 smoother calls per level are made, after which the cycle ends
+ * and flex_capped is set. */
+static void flex_cycle(orc_ac *ac, int l, const int mv[3], const int ms[3]) {
+  const int last = ac->nlevels - 1;
+  long long visits = 0, cap = 1000LL * ac->nlevels;
+  int pos = 0;
+  ac->flex_capped = 0;
+  for (;;) {
+    if (l != last) {
+      const int idx = pos ? 2 : 0;
+      if (++visits > cap) { ac->flex_capped = 1; return; }
+      if (smooth_as(ac, l, mv[idx], ac->resrat_val, ac->restol_val, ms[idx], 0)) {
+        if (l == 0) return;
+        interpolation(&ac->L[l], &ac->L[l - 1]);
+        l -= 1;
+        pos = 1;
+      } else {
+        restriction(&ac->L[l], &ac->L[l + 1]);
+        l += 1;
+        pos = 0;
+      }
+    } else {
+      solve_l(ac, l, 100, -1.0, ac->restol_val, -1);
+      if (l == 0) return;
+      interpolation(&ac->L[l], &ac->L[l - 1]);
+      l -= 1;
+      pos = 0;
+    }
   }
 }
 
@@ -895,6 +985,8 @@ static void run_cycle(orc_ac *ac, int kind, int l, const int mv[3], const int ms
   if (kind == 1) v_cycle(ac, l, mv, ms);
   else if (kind == 2) fw_cycle(ac, l, mv, ms, 0);
   else if (kind == 4) fw_cycle(ac, l, mv, ms, 1);
+  else if (kind == 5) flex_cycle(ac, l, mv, ms);
+  else solve_l(ac, l, 100, -1.0, ac->restol_val, -1); /* full_cycle's "shouldn't happen" branch */
 }
 
 /* additive_recursive.cpp:121-158 */
@@ -904,13 +996,20 @@ static void full_cycle(orc_ac *ac, int l, int kind, const int mv[3], const int m
     full_cycle(ac, l + 1, kind, mv, ms);
     run_cycle(ac, kind, l, mv, ms);
   } else {
-    smooth(ac, l, 100, -1.0, ac->restol_val, -1);
-    interpolation(&ac->L[l], &ac->L[l - 1]);
+    solve_l(ac, l, 100, -1.0, ac->restol_val, -1);
+    if (l > 0) interpolation(&ac->L[l], &ac->L[l - 1]);
   }
 }
 
 /* AC::cycle (additive_cycle.cpp:4-99), init_cycles and converged
- * (additive_cycle_functions.cpp:12-87) */
+ * (additive_cycle_functions.cpp:12-87). loop 1 V, 2 F, 4 W, 5 flex; any
+ * other loop value is the "just solve" branch (:66-71): one call of AC's
+ * solver on level 0 (MaxIter 40, ResRat 0.001, ResTol femto), then the
+ * loop ends and the cycle reports max_cyc cycles, not converged. With
+ * use_linf the tests read the max-norm residual instead: against the
+ * initial one for the ratio, and for the divergence check against the
+ * value before the loop, which the reference never refreshes (its
+ * `reslinf_m1 = reslinf_m1`, additive_cycle.cpp:78). */
 int orc_ac_cycle(orc_ac *ac, double *x, const double *b, int init, int loop,
                  double toler, double factor, const int mv[3], const int ms[3],
                  int max_cyc, int min_cyc, int stop_if_div, int priority_min_cyc,
@@ -921,13 +1020,14 @@ int orc_ac_cycle(orc_ac *ac, double *x, const double *b, int init, int loop,
   memcpy(L0->phi, x, N0 * 8);
   memcpy(L0->fnew, b, N0 * 8);
   orc_ac_coarsen_all(ac);
-  double linf;
-  double res_0 = residual(ac, &linf);
+  double linf_0;
+  double res_0 = residual(ac, &linf_0);
   if (res_hist) res_hist[nh] = res_0;
   nh++;
   memcpy(ac->fold, L0->phi, N0 * 8);
   int ret = 0, nc = 0;
-  if ((res_0 < toler && min_cyc == 0) || res_0 == 0.0) {
+  const double res_0_control = ac->use_linf ? linf_0 : res_0;
+  if ((res_0_control < toler && min_cyc == 0) || res_0 == 0.0) {
     ret = 1; nc = 0;
     goto out;
   }
@@ -936,34 +1036,54 @@ int orc_ac_cycle(orc_ac *ac, double *x, const double *b, int init, int loop,
     memset(ac->L[l].phi, 0, N * 8);
     memset(ac->L[l].fnew, 0, N * 8);
   }
-  double res_m1;
+  double res_m1, linf_m1;
   if (init != -1) {
     full_cycle(ac, 0, init, mv, ms);
-    res_m1 = residual(ac, NULL);
-    /* converged(...) at cycle 0: its result is not used by the reference */
+    res_m1 = residual(ac, &linf_m1);
+    /* converged(..., cycle 0, ...) (:39-43): its return value is dropped,
+     * but its divergence branch runs. It compares the residual with itself
+     * (res0 is res_m1, the same state), so unless cycle 0 already meets the
+     * tolerance, stop_if_div restores phi = fold, the initial guess
+     * (additive_cycle_functions.cpp:67-83). */
+    const double rc = ac->use_linf ? linf_m1 : res_m1;
+    const double rbc = ac->use_linf ? linf_0 : res_0;
+    if (!(0 >= min_cyc && (rc / rbc < factor || rc < toler))) {
+      int check = stop_if_div;
+      if (priority_min_cyc && 0 < min_cyc) check = 0;
+      if (check) memcpy(L0->phi, ac->fold, N0 * 8);
+    }
   } else {
-    res_m1 = residual(ac, NULL);
+    res_m1 = residual(ac, &linf_m1);
   }
   nc = max_cyc;
   for (int c = 1; c <= max_cyc; ++c) {
+    if (loop != 1 && loop != 2 && loop != 4 && loop != 5) {
+      /* just solve */
+      solve_l(ac, 0, 40, 0.001, 1.0e-15, -1);
+      break;
+    }
     run_cycle(ac, loop, 0, mv, ms);
-    double res1 = residual(ac, NULL);
+    double linf1;
+    double res1 = residual(ac, &linf1);
     if (res_hist) res_hist[nh] = res1;
     nh++;
+    const double rc = ac->use_linf ? linf1 : res1;
+    const double r0c = ac->use_linf ? linf_m1 : res_m1;
+    const double rbc = ac->use_linf ? linf_0 : res_0;
     int con;
-    if (c >= min_cyc && (res1 / res_0 < factor || res1 < toler)) {
+    if (c >= min_cyc && (rc / rbc < factor || rc < toler)) {
       con = 0;
     } else {
       int check = stop_if_div;
       if (priority_min_cyc && c < min_cyc) check = 0;
-      if (check && res1 >= res_m1) {
+      if (check && rc >= r0c) {
         memcpy(L0->phi, ac->fold, N0 * 8);
         con = 1;
       } else {
         con = 2;
       }
     }
-    res_m1 = res1;
+    res_m1 = res1;  /* linf_m1 stays (the reference's self-assignment) */
     if (con == 0) { ret = 1; nc = c; goto out; }
     if (con == 1) { ret = 0; nc = c; goto out; }
     memcpy(ac->fold, L0->phi, N0 * 8);

@@ -12,7 +12,9 @@
  * the reference are zero on the non-periodic faces of these problems and
  * the boundary coefficients are zero after the boundary correction, so every
  * out-of-domain neighbour term is taken as the product with a zero value,
- * in the reference's operation order.
+ * in the reference's operation order. On a periodic axis the halo holds the
+ * cell at the other end (Scalar::exchange, scalar_exchange.cpp:47-58), so
+ * the neighbour across that face is that cell.
  */
 #ifndef PSIBOIL_ORACLE_H
 #define PSIBOIL_ORACLE_H
@@ -27,6 +29,8 @@ extern "C" {
 typedef struct {
   int nx, ny, nz;
   double *c, *w, *e, *s, *n, *b, *t;
+  int per;   /* periodic axes: bit 0 i, 1 j, 2 k (the reference's periodic
+                halo, scalar_exchange.cpp:47-58, zero jump value) */
 } orc_mat;
 
 typedef struct {
@@ -97,6 +101,16 @@ void orc_ac_destroy(orc_ac *ac);
  * Prec code prec), 3 Jacobi, 4 Gauss-Seidel (level 0 with ci0, the stored
  * A.ci, kept by the caller; coarse levels with 1/c). */
 void orc_ac_set_smoother(orc_ac *ac, int kind, int prec, const double *ci0);
+/* AC::resrat / AC::restol (the level solvers' ResRat and ResTol, atto by
+ * default, additive.h:105-110), AC::use_linf_error (additive.h:141) and AC's
+ * own solver (AC(cen, sol): sol_kind -1 = the levels' solver, else 0 CG,
+ * 1 BiCGS, 2 CGS, 3 Jacobi, 4 Gauss-Seidel, with sol_prec), which
+ * call_solver uses for post-smoothing and the coarsest level
+ * (additive_cycle_functions.cpp:100-107). */
+void orc_ac_set_params(orc_ac *ac, double resrat_val, double restol_val, int use_linf,
+                       int sol_kind, int sol_prec);
+/* 1 when the last flex cycle stopped at its visit bound (see oracle.c) */
+int orc_ac_flex_capped(const orc_ac *ac);
 int orc_ac_nlevels(const orc_ac *ac);
 void orc_ac_level_dims(const orc_ac *ac, int l, int *dims /* 3 */);
 /* Coarse operators of all levels (AC::coarsen_system,
@@ -106,7 +120,8 @@ void orc_ac_coarsen_all(orc_ac *ac);
 void orc_ac_level_matrix(const orc_ac *ac, int l, double *out7);
 
 /* AC::cycle (additive_cycle.cpp:4-99, additive_cycle_functions.cpp,
- * additive_recursive.cpp). init/loop: -1 none, 1 V, 2 F, 4 W.
+ * additive_recursive.cpp). init/loop: -1 none, 1 V, 2 F, 4 W, 5 flex; a
+ * loop of none is the reference's "just solve" branch.
  * toler: ResTol, factor: ResRat (negative disables), mv/ms as in the
  * reference, max_cyc/min_cyc/stop_if_div/priority_min_cyc as the setters.
  * res_hist receives [initial res, res after cycle 1, ...] (max_cyc+2). */

@@ -4,13 +4,15 @@
  *
  * kind 0: single bubble n^3; 1: bubbles + solid cylinder; 2: batch member.
  * params: n, nb, rmin, rmax, rc, ratio, index, n2d, s2lo, s2hi, s3lo, s3hi,
- *         rhs stream.
+ *         rhs stream, periodic axes.
  * With solid == NULL only dims and hb (h, density ratio) are written;
  * otherwise out receives rho, rhs, c, w, e, s, n, b, t, ci (N each).
  */
 #include <stdlib.h>
 #include "problem_gen.h"
 
+/* params[13]: periodic axes (bit 0 i, 1 j, 2 k): both faces of each set
+ * axis become PBG_BC_PERIODIC */
 static void make_desc(int kind, const double *params, uint64_t seed, pbg_problem_desc *dd) {
   pbg_problem_desc d;
   int n = (int)params[0];
@@ -21,6 +23,9 @@ static void make_desc(int kind, const double *params, uint64_t seed, pbg_problem
   else
     pbg_desc_batch_member(&d, seed, (int)params[6], (int)params[7], (int)params[8],
                           (int)params[9], (int)params[10], (int)params[11]);
+  const int per = (int)params[13];
+  for (int ax = 0; ax < 3; ++ax)
+    if (per & (1 << ax)) d.bc[2 * ax] = d.bc[2 * ax + 1] = PBG_BC_PERIODIC;
   *dd = d;
 }
 

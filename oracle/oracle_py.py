@@ -33,7 +33,7 @@ def build():
 
 class OrcMat(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int)] + \
-               [(k, _dp) for k in "cwesnbt"]
+               [(k, _dp) for k in "cwesnbt"] + [("per", ctypes.c_int)]
 
 
 class OrcStats(ctypes.Structure):
@@ -76,6 +76,10 @@ def lib():
         L.orc_ac_create.argtypes = [ctypes.POINTER(OrcMat), ctypes.c_void_p, ctypes.c_double]
         L.orc_ac_destroy.argtypes = [ctypes.c_void_p]
         L.orc_ac_set_smoother.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp]
+        L.orc_ac_set_params.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int]
+        L.orc_ac_flex_capped.restype = ctypes.c_int
+        L.orc_ac_flex_capped.argtypes = [ctypes.c_void_p]
         L.orc_ac_nlevels.restype = ctypes.c_int
         L.orc_ac_nlevels.argtypes = [ctypes.c_void_p]
         L.orc_ac_level_dims.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
@@ -107,10 +111,12 @@ class Problem:
     """A seeded fixture problem: dims, density, solid mask, rhs, matrix."""
 
     def __init__(self, kind, seed, n=16, nb=0, rmin=4.0, rmax=16.0, rc=0.0, ratio=1000.0,
-                 index=0, n2d=0, s2=(64, 512), s3=(32, 96), stream=0, convect=0.0):
+                 index=0, n2d=0, s2=(64, 512), s3=(32, 96), stream=0, convect=0.0, periodic=0):
+        """periodic: axes with periodic boundaries (bit 0 i, 1 j, 2 k)."""
         self.kind, self.seed = kind, seed
+        self.periodic = int(periodic)
         params = np.array([n, nb, rmin, rmax, rc, ratio, index, n2d, s2[0], s2[1], s3[0], s3[1],
-                           stream], dtype=np.float64)
+                           stream, self.periodic], dtype=np.float64)
         dims = np.zeros(3, dtype=np.int32)
         hb = np.zeros(2, dtype=np.float64)  # h, rho ratio
         L = lib()
@@ -121,7 +127,7 @@ class Problem:
         N = self.nx * self.ny * self.nz
         self.N = N
         self.args = dict(n=n, nb=nb, rmin=rmin, rmax=rmax, rc=rc, ratio=ratio, index=index,
-                         n2d=n2d, s2=s2, s3=s3)
+                         n2d=n2d, s2=s2, s3=s3, periodic=self.periodic)
         out = np.zeros(10 * N, dtype=np.float64)  # rho, rhs, c,w,e,s,n,b,t,ci
         solid = np.zeros(N, dtype=np.uint8)
         L.orc_gen_problem(kind, params.ctypes.data, seed, dims.ctypes.data, solid.ctypes.data,
@@ -148,7 +154,7 @@ class Problem:
         return self.h * self.h * self.h
 
     def mat(self):
-        m = OrcMat(self.nx, self.ny, self.nz, *[_p(self.A[k]) for k in "cwesnbt"])
+        m = OrcMat(self.nx, self.ny, self.nz, *[_p(self.A[k]) for k in "cwesnbt"], self.periodic)
         m._keep = self
         return m
 
@@ -214,16 +220,28 @@ class AC:
 
     SMOOTHERS = {"cg": 0, "bicgs": 1, "cgs": 2, "jacobi": 3, "gs": 4}
 
-    def __init__(self, P, smoother="cg", prec="di"):
+    def __init__(self, P, smoother="cg", prec="di", solver=None, solver_prec="di", resrat=1e-18,
+                 restol=1e-18, use_linf=False):
+        """smoother: the levels' solver (the Pressure's Linear); solver: AC's
+        own solver for call_solver (AC(cen, sol)), None for the same;
+        resrat/restol: AC::resrat/restol; use_linf: AC::use_linf_error."""
         self.P = P
         aflag = (1 - P.solid).astype(np.uint8)
         self._aflag = aflag
         m = P.mat()
         self._m = m
         self.h = lib().orc_ac_create(ctypes.byref(m), aflag.ctypes.data, P.h)
+        self._ci = np.ascontiguousarray(P.ci, dtype=np.float64)  # level 0's stored ci
         if smoother != "cg" or prec != "di":
-            self._ci = np.ascontiguousarray(P.ci, dtype=np.float64)  # level 0's stored ci
             lib().orc_ac_set_smoother(self.h, self.SMOOTHERS[smoother], PRECS[prec], _p(self._ci))
+        elif solver in ("jacobi", "gs"):
+            lib().orc_ac_set_smoother(self.h, 0, 0, _p(self._ci))
+        lib().orc_ac_set_params(self.h, resrat, restol, int(use_linf),
+                                -1 if solver is None else self.SMOOTHERS[solver], PRECS[solver_prec])
+
+    @property
+    def flex_capped(self):
+        return bool(lib().orc_ac_flex_capped(self.h))
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -270,7 +288,8 @@ def harness_available():
 
 
 def run_reference(P, solver="cg", resrat=1e-8, maxit=20000, maxcyc=20, guard=1, cycle="V",
-                  out_prefix=None, dump=True, timeout=3600, prec="di", acsm="cg"):
+                  out_prefix=None, dump=True, timeout=3600, prec="di", acsm="cg", init="none",
+                  acsolver=None, linf=0, acresrat=None, mincyc=0):
     """Run the compiled reference on P's fixture; returns (meta, arrays)."""
     import tempfile
     kind = {KIND_SINGLE: "single", KIND_CYL: "cyl", KIND_BATCH: "batch"}[P.kind]
@@ -286,7 +305,13 @@ def run_reference(P, solver="cg", resrat=1e-8, maxit=20000, maxcyc=20, guard=1, 
            "--seed", str(P.seed), "--solver", solver, "--resrat", repr(resrat),
            "--maxit", str(maxit), "--maxcyc", str(maxcyc), "--guard", str(guard),
            "--cycle", cycle, "--prec", prec, "--dump", "1" if dump else "0", "--out", out_prefix,
-           "--convect", repr(getattr(P, "convect", 0.0)), "--acsm", acsm]
+           "--convect", repr(getattr(P, "convect", 0.0)), "--acsm", acsm,
+           "--periodic", str(getattr(P, "periodic", 0)), "--init", init, "--linf", str(int(linf)),
+           "--mincyc", str(mincyc)]
+    if acsolver:
+        cmd += ["--acsolver", acsolver]
+    if acresrat is not None:
+        cmd += ["--acresrat", repr(acresrat)]
     subprocess.run(cmd, check=True, capture_output=True, timeout=timeout)
     meta = {}
     for line in open(out_prefix + ".txt"):

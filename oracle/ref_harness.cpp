@@ -29,14 +29,27 @@
  *   ref_harness --kind single|cyl|batch --n N [--nb NB --rmin R --rmax R
  *               --rc R --ratio Q] [--index I --n2d M --s2 LO HI --s3 LO HI]
  *               --seed S --solver cg|bicgs|cgs|jacobi|gs|ac [--acsm SOLVER] --resrat RR --maxit M
- *               [--maxcyc C --guard 0|1 --cycle V|F|W] [--prec di|ic0|ic2|ic3] [--save NAME]
- *               [--step 1 --dt DT] [--convect F] --out PREFIX
+ *               [--maxcyc C --guard 0|1 --cycle V|F|W|flex|none --init none|V|F|W
+ *                --mincyc C --linf 0|1 --acsolver SOLVER --acresrat RR] [--prec di|ic0|ic2|ic3] [--save NAME]
+ *               [--step 1 --dt DT] [--convect F] [--periodic MASK] --out PREFIX
  *
  * --solver cgs runs `CGS::solve` (cgs.cpp), --solver jacobi `Jacobi::solve`
  * and --solver gs `GaussSeidel::solve` (Src/Solver/Linear/Iterative);
  * --convect F adds the upwind
  * convection of pbg_gen_convect to the fixture after the boundary
  * correction (a non-symmetric matrix, for BiCGS and CGS).
+ *
+ * With --solver ac: --cycle flex runs AC's flex cycle and --cycle none its
+ * "just solve" branch (AC::cycle with Cycle::none() as the loop, through
+ * AC::cycle(init, loop, ResTol(-1), ResRat, mv, ms)); --init V|F|W starts
+ * with a full cycle of that kind; --linf 1 sets use_linf_error(true);
+ * --acsolver names a distinct solver for AC(cen, sol); --acresrat sets
+ * AC::resrat, the ResRat of the level solvers (atto by default).
+ *
+ * --periodic MASK makes the axes of MASK (bit 0 i, 1 j, 2 k) periodic: the
+ * grids are built with Periodic::yes(), the pressure (and velocity) get
+ * BndType::periodic() on both faces, and the fixture's boundary faces on
+ * those axes couple to the cell at the other end.
  *
  * --step 1 runs one pressure-correction step with the reference's own
  * classes and no override: a two-phase Matter (liquid and vapour densities
@@ -75,6 +88,10 @@ struct Args {
   int maxit = 20000, maxcyc = 20, guard = 1, dump = 1, repeat = 1, gpu = 0, exact = 1;
   int step = 0;
   double dt = 1.0, convect = 0.0, body = 0.0;
+  int periodic = 0;   // periodic axes: bit 0 i, 1 j, 2 k
+  std::string init = "none", acsolver;  // AC: full-cycle init, distinct solver
+  int linf = 0, mincyc = 0;
+  double acresrat = -1.0;   // AC::resrat (the level solvers' ResRat), default atto
 };
 
 Args parse(int argc, char **argv) {
@@ -115,6 +132,12 @@ Args parse(int argc, char **argv) {
     else if (k == "--step") a.step = std::atoi(nxt());
     else if (k == "--dt") a.dt = std::atof(nxt());
     else if (k == "--convect") a.convect = std::atof(nxt());
+    else if (k == "--periodic") a.periodic = std::atoi(nxt());
+    else if (k == "--init") a.init = nxt();
+    else if (k == "--acsolver") a.acsolver = nxt();
+    else if (k == "--linf") a.linf = std::atoi(nxt());
+    else if (k == "--mincyc") a.mincyc = std::atoi(nxt());
+    else if (k == "--acresrat") a.acresrat = std::atof(nxt());
     else { std::fprintf(stderr, "unknown argument %s\n", k.c_str()); std::exit(2); }
   }
   return a;
@@ -142,8 +165,8 @@ class Fixture : public Pressure {
     if (!ready) { Pressure::discretize(diff_eddy); return; }
     const size_t N = pbg_ncells(&D);
     std::vector<double> c(N), w(N), e(N), s(N), n(N), b(N), t(N);
-    pbg_gen_faces(D.nx, D.ny, D.nz, D.h, RHO.data(), SOLID.data(),
-                  c.data(), w.data(), e.data(), s.data(), n.data(), b.data(), t.data());
+    pbg_gen_faces_per(D.nx, D.ny, D.nz, D.h, pbg_periodic_mask(D.bc), RHO.data(), SOLID.data(),
+                      c.data(), w.data(), e.data(), s.data(), n.data(), b.data(), t.data());
     const int B = boil::BW;
     for (int i = 0; i < D.nx; ++i)
       for (int j = 0; j < D.ny; ++j)
@@ -342,9 +365,10 @@ int run_step(const Args &a, const pbg_problem_desc &D) {
   std::cout.precision(17);
 
   const double h = D.h;
-  Grid1D gx(Range<real>(0.0, D.nx * h), Range<real>(h, h), D.nx, Periodic::no());
-  Grid1D gy(Range<real>(0.0, D.ny * h), Range<real>(h, h), D.ny, Periodic::no());
-  Grid1D *gz = (D.nz > 1) ? new Grid1D(Range<real>(0.0, D.nz * h), Range<real>(h, h), D.nz, Periodic::no())
+  auto pd = [&](int ax) { return (a.periodic & (1 << ax)) ? Periodic::yes() : Periodic::no(); };
+  Grid1D gx(Range<real>(0.0, D.nx * h), Range<real>(h, h), D.nx, pd(0));
+  Grid1D gy(Range<real>(0.0, D.ny * h), Range<real>(h, h), D.ny, pd(1));
+  Grid1D *gz = (D.nz > 1) ? new Grid1D(Range<real>(0.0, D.nz * h), Range<real>(h, h), D.nz, pd(2))
                           : new Grid1D(h);
   /* --body R: a sphere of radius R cells inside the domain, written as an
    * ASCII STL and cut by the reference's own Body (Body::Body(name),
@@ -455,6 +479,9 @@ pbg_problem_desc make_desc(const Args &a) {
 int main(int argc, char **argv) {
   Args a = parse(argc, argv);
   pbg_problem_desc D = make_desc(a);
+  for (int ax = 0; ax < 3; ++ax)
+    if (a.periodic & (1 << ax)) D.bc[2 * ax] = D.bc[2 * ax + 1] = PBG_BC_PERIODIC;
+  if (a.step && a.periodic) { std::fprintf(stderr, "--step takes walls only\n"); return 2; }
   if (a.step) return run_step(a, D);
   const size_t N = pbg_ncells(&D);
   std::vector<double> rho(N), rhs(N);
@@ -467,9 +494,10 @@ int main(int argc, char **argv) {
   std::cout.precision(17);
 
   const double h = D.h;
-  Grid1D gx(Range<real>(0.0, D.nx * h), Range<real>(h, h), D.nx, Periodic::no());
-  Grid1D gy(Range<real>(0.0, D.ny * h), Range<real>(h, h), D.ny, Periodic::no());
-  Grid1D *gz = (D.nz > 1) ? new Grid1D(Range<real>(0.0, D.nz * h), Range<real>(h, h), D.nz, Periodic::no())
+  auto pd = [&](int ax) { return (a.periodic & (1 << ax)) ? Periodic::yes() : Periodic::no(); };
+  Grid1D gx(Range<real>(0.0, D.nx * h), Range<real>(h, h), D.nx, pd(0));
+  Grid1D gy(Range<real>(0.0, D.ny * h), Range<real>(h, h), D.ny, pd(1));
+  Grid1D *gz = (D.nz > 1) ? new Grid1D(Range<real>(0.0, D.nz * h), Range<real>(h, h), D.nz, pd(2))
                           : new Grid1D(h);
   Domain d(gx, gy, *gz);
   Times time(1, 1.0);
@@ -500,6 +528,7 @@ int main(int argc, char **argv) {
   const Dir dirs[6] = {Dir::imin(), Dir::imax(), Dir::jmin(), Dir::jmax(), Dir::kmin(), Dir::kmax()};
   for (int q = 0; q < 6; ++q) {
     if (D.nz == 1 && q >= 4) p.bc().add(BndCnd(dirs[q], BndType::pseudo()));
+    else if (D.bc[q] == PBG_BC_PERIODIC) p.bc().add(BndCnd(dirs[q], BndType::periodic()));
     else if (D.bc[q] == PBG_BC_DIRICHLET) p.bc().add(BndCnd(dirs[q], BndType::dirichlet(), 0.0));
     else p.bc().add(BndCnd(dirs[q], BndType::neumann()));
   }
@@ -507,6 +536,7 @@ int main(int argc, char **argv) {
   for (int m = 0; m < 3; ++m)
     for (int q = 0; q < 6; ++q) {
       if (D.nz == 1 && q >= 4) uvw.bc(comps[m]).add(BndCnd(dirs[q], BndType::pseudo()));
+      else if (D.bc[q] == PBG_BC_PERIODIC) uvw.bc(comps[m]).add(BndCnd(dirs[q], BndType::periodic()));
       else uvw.bc(comps[m]).add(BndCnd(dirs[q], BndType::wall()));
     }
   Matter fluid(d);
@@ -520,12 +550,32 @@ int main(int argc, char **argv) {
   double secs = 0.0;
   std::vector<double> rep_secs;
   if (a.solver == "ac") {
-    AC mg(&pr);
+    /* --acsolver: AC's own solver (AC(cen, sol), additive.cpp:8-48), used by
+       call_solver (post-smoothing, coarsest level); the levels keep the
+       Pressure's solver for call_smoother */
+    Linear *acsol = nullptr;
+    if (a.acsolver == "cg") acsol = new CG(d, pc);
+    else if (a.acsolver == "bicgs") acsol = new BiCGS(d, pc);
+    else if (a.acsolver == "cgs") acsol = new CGS(d, pc);
+    else if (a.acsolver == "jacobi") acsol = new Jacobi(d);
+    else if (a.acsolver == "gs") acsol = new GaussSeidel(d);
+    AC mg(&pr, acsol);
     mg.max_cycles(a.maxcyc);
+    mg.min_cycles(a.mincyc);
     mg.stop_if_diverging(a.guard != 0);
+    mg.use_linf_error(a.linf != 0);
+    if (a.acresrat > 0.0) mg.resrat(ResRat(a.acresrat));
     p = 0.0;
+    auto cyc = [](const std::string &c) {
+      return c == "V" ? Cycle::V() : c == "F" ? Cycle::F() : c == "W" ? Cycle::W()
+             : c == "flex" ? Cycle::flex() : Cycle::none();
+    };
+    const std::array<MaxIter, 3> mv = {MaxIter(20), MaxIter(20), MaxIter(20)};
+    const std::array<MaxIter, 3> ms = {MaxIter(-1), MaxIter(-1), MaxIter(-1)};
     auto t0 = std::chrono::steady_clock::now();
-    if (a.cycle == "F") conv = mg.fcycle(ResRat(a.resrat), &ncyc);
+    if (a.init != "none" || a.cycle == "flex" || a.cycle == "none")
+      conv = mg.cycle(cyc(a.init), cyc(a.cycle), ResTol(-1.0), ResRat(a.resrat), mv, ms, &ncyc);
+    else if (a.cycle == "F") conv = mg.fcycle(ResRat(a.resrat), &ncyc);
     else if (a.cycle == "W") conv = mg.wcycle(ResRat(a.resrat), &ncyc);
     else conv = mg.vcycle(ResRat(a.resrat), &ncyc);
     secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -24,8 +24,9 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libpsiboil_b200.so")
 
 PBG_OK = 0
+ERR_ARG, ERR_CUDA, ERR_STATE, ERR_NOMEM, ERR_UNSUPPORTED, ERR_ADMISSION = -1, -2, -3, -4, -5, -6
 HOST, DEVICE = 0, 1
-NEUMANN, DIRICHLET = 0, 1
+NEUMANN, DIRICHLET, PERIODIC = 0, 1, 2   # boundary types; PERIODIC goes on both faces of an axis
 SOLVER_CG, SOLVER_BICGS, SOLVER_AC, SOLVER_ENGINE, SOLVER_CGS = 0, 1, 2, 3, 4
 SOLVER_JACOBI, SOLVER_GAUSS_SEIDEL = 5, 6
 # pbg_result.status

@@ -30,6 +30,7 @@ struct pbg_session {
   int nx = 0, ny = 0, nz = 0;
   double h = 0.0, dV = 0.0;
   int bc[6] = {0, 0, 0, 0, 0, 0};
+  int per = 0;                     // periodic axes (bit 0 i, 1 j, 2 k)
   Mat64 A;
   bool have_matrix = false;
   DBuf<uint8_t> aflag;
@@ -301,6 +302,14 @@ int pbg_session_create(int nx, int ny, int nz, double h, const int bc[6], int de
   s->nx = nx; s->ny = ny; s->nz = nz; s->h = h;
   s->dV = (h * h) * h;
   if (bc) for (int f = 0; f < 6; ++f) s->bc[f] = bc[f];
+  for (int f = 0; f < 6; ++f)
+    if (s->bc[f] != PBG_BC_NEUMANN_ && s->bc[f] != PBG_BC_DIRICHLET_ && s->bc[f] != PBG_BC_PERIODIC_)
+      return fail(PBG_ERR_ARG, "boundary types are PBG_BC_NEUMANN_, PBG_BC_DIRICHLET_ or PBG_BC_PERIODIC_");
+  for (int d = 0; d < 3; ++d) {
+    const bool a = s->bc[2 * d] == PBG_BC_PERIODIC_, b2 = s->bc[2 * d + 1] == PBG_BC_PERIODIC_;
+    if (a != b2) return fail(PBG_ERR_ARG, "a periodic axis needs PBG_BC_PERIODIC_ on both of its faces");
+    if (a) s->per |= 1 << d;
+  }
   int rc = guard(s.get(), [&]() -> int {
     PBG_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     s->red.init();
@@ -362,50 +371,87 @@ int pbg_session_set_cell_volume(pbg_session *s, double dV) {
   return PBG_OK;
 }
 
+// Checks of an uploaded seven-array matrix, one thread per cell: bit 0 of
+// *flags when the symmetric form does not hold (e(i) == w(i+1), n(j) ==
+// s(j+1), t(k) == b(k+1) bit for bit, across a periodic face with the cell
+// at the other end, and zero on a non-periodic outer face), bit 1 when a
+// coupling across a non-periodic outer face is non-zero.
+__global__ void k_mat_check(MatView<double> A, unsigned *flags) {
+  const long long N = A.ncell();
+  unsigned f = 0;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    const Pos q = pos_of(p, A.ny, A.nz);
+    const NbIdx m = nb_index(A, p, q);
+    const double ee = m.e >= 0 ? A.w[m.e] : 0.0;
+    const double nn = m.n >= 0 ? A.s[m.n] : 0.0;
+    const double tt = m.t >= 0 ? A.b[m.t] : 0.0;
+    if (__double_as_longlong(ee) != __double_as_longlong(A.e[p]) ||
+        __double_as_longlong(nn) != __double_as_longlong(A.n[p]) ||
+        __double_as_longlong(tt) != __double_as_longlong(A.t[p]))
+      f |= 1u;
+    if ((m.w < 0 && A.w[p] != 0.0) || (m.e < 0 && A.e[p] != 0.0) || (m.s < 0 && A.s[p] != 0.0) ||
+        (m.n < 0 && A.n[p] != 0.0) || (m.b < 0 && A.b[p] != 0.0) || (m.t < 0 && A.t[p] != 0.0))
+      f |= 2u;
+  }
+  for (int off = 16; off > 0; off >>= 1) f |= __shfl_down_sync(0xffffffffu, f, off);
+  if ((threadIdx.x & 31) == 0 && f) atomicOr(flags, f);
+}
+
+// One compact device array from a caller array: a straight copy for the
+// compact layout, else a gather (host arrays through a staging vector).
+static void upload_compact(pbg_session *s, const double *src, double *dst, long long si, long long sj,
+                           long long sk, long long offset, int where) {
+  const int nx = s->nx, ny = s->ny, nz = s->nz;
+  const long long N = s->ncell();
+  const bool compact = si == (long long)ny * nz && sj == nz && sk == 1;
+  if (where == PBG_HOST) {
+    if (compact) {
+      PBG_CUDA(cudaMemcpyAsync(dst, src + offset, N * 8, cudaMemcpyHostToDevice, s->stream));
+    } else {
+      std::vector<double> h(N);
+      gather(src, h.data(), nx, ny, nz, si, sj, sk, offset);
+      PBG_CUDA(cudaMemcpyAsync(dst, h.data(), N * 8, cudaMemcpyHostToDevice, s->stream));
+      PBG_CUDA(cudaStreamSynchronize(s->stream));
+    }
+  } else if (compact) {
+    PBG_CUDA(cudaMemcpyAsync(dst, src + offset, N * 8, cudaMemcpyDeviceToDevice, s->stream));
+  } else {
+    k_gather<<<grid_for(N), kThreads, 0, s->stream>>>(src, dst, nx, ny, nz, si, sj, sk, offset); note_launch();
+  }
+}
+
 int pbg_matrix_upload(pbg_session *s, const double *c, const double *w, const double *e,
                       const double *sv, const double *n, const double *b, const double *t,
                       long long si, long long sj, long long sk, long long offset, int where) {
   if (!s || !c || !w || !e || !sv || !n || !b || !t) return fail(PBG_ERR_ARG, "NULL argument");
   return guard(s, [&]() -> int {
     const long long N = s->ncell();
-    const int nx = s->nx, ny = s->ny, nz = s->nz;
-    const double *src[7] = {c, w, e, sv, n, b, t};
-    std::vector<std::vector<double>> h(7, std::vector<double>(N));
-    if (where == PBG_HOST) {
-      for (int q = 0; q < 7; ++q) gather(src[q], h[q].data(), nx, ny, nz, si, sj, sk, offset);
-    } else {
-      DBuf<double> tmp(N);
-      for (int q = 0; q < 7; ++q) {
-        k_gather<<<grid_for(N), kThreads, 0, s->stream>>>(src[q], tmp.p, nx, ny, nz, si, sj, sk, offset); note_launch();
-        PBG_CUDA(cudaMemcpyAsync(h[q].data(), tmp.p, N * 8, cudaMemcpyDeviceToHost, s->stream));
-      }
-      PBG_CUDA(cudaStreamSynchronize(s->stream));
-    }
-    // symmetry: e(i) == w(i+1), n(j) == s(j+1), t(k) == b(k+1) bit for bit,
-    // and the outermost e / n / t are zero
-    const long long SI = (long long)ny * nz, SJ = nz;
-    bool sym = true;
-    for (int i = 0; i < nx && sym; ++i)
-      for (int j = 0; j < ny && sym; ++j)
-        for (int k = 0; k < nz && sym; ++k) {
-          long long p = ((long long)i * ny + j) * nz + k;
-          double ee = i < nx - 1 ? h[1][p + SI] : 0.0;
-          double nn = j < ny - 1 ? h[3][p + SJ] : 0.0;
-          double tt = k < nz - 1 ? h[5][p + 1] : 0.0;
-          if (std::memcmp(&ee, &h[2][p], 8) || std::memcmp(&nn, &h[4][p], 8) ||
-              std::memcmp(&tt, &h[6][p], 8))
-            sym = false;
-        }
     Mat64 &A = s->A;
-    A.nx = nx; A.ny = ny; A.nz = nz; A.sym = sym;
+    A.nx = s->nx; A.ny = s->ny; A.nz = s->nz;
+    A.per = s->per;
     // same-size uploads keep the buffers (the engine then refreshes in place)
     if (A.c.n != (size_t)N) { A.c.alloc(N); A.w.alloc(N); A.s.alloc(N); A.b.alloc(N); }
-    if (sym) { A.e.release(); A.n.release(); A.t.release(); }
-    else { A.e.alloc(N); A.n.alloc(N); A.t.alloc(N); }
+    if (A.e.n != (size_t)N) { A.e.alloc(N); A.n.alloc(N); A.t.alloc(N); }
+    const double *src[7] = {c, w, e, sv, n, b, t};
     DBuf<double> *dst[7] = {&A.c, &A.w, &A.e, &A.s, &A.n, &A.b, &A.t};
-    for (int q = 0; q < 7; ++q)
-      if (dst[q]->p) PBG_CUDA(cudaMemcpyAsync(dst[q]->p, h[q].data(), N * 8, cudaMemcpyHostToDevice, s->stream));
+    for (int q = 0; q < 7; ++q) upload_compact(s, src[q], dst[q]->p, si, sj, sk, offset, where);
+    // symmetry and outer faces, checked on the device
+    PBG_CUDA(cudaMemsetAsync(s->dlinf.p, 0, sizeof(unsigned long long), s->stream));
+    A.sym = false;
+    k_mat_check<<<grid_for(N), kThreads, 0, s->stream>>>(A.view(), (unsigned *)s->dlinf.p); note_launch();
+    PBG_CUDA(cudaMemcpyAsync(s->hbuf, s->dlinf.p, 8, cudaMemcpyDeviceToHost, s->stream));
     PBG_CUDA(cudaStreamSynchronize(s->stream));
+    unsigned flags = 0;
+    std::memcpy(&flags, s->hbuf, sizeof(flags));
+    if (flags & 2u) {
+      s->have_matrix = false;
+      return fail(PBG_ERR_UNSUPPORTED,
+                  "the matrix couples a cell across a non-periodic outer face (apply the boundary "
+                  "correction first, or create the session with periodic boundaries on that axis)");
+    }
+    A.sym = !(flags & 1u);
+    if (A.sym) { A.e.release(); A.n.release(); A.t.release(); }
     s->have_matrix = true;
     ++s->mat_gen;
     invalidate(s);
@@ -427,14 +473,15 @@ int pbg_matrix_download(pbg_session *s, double *c, double *w, double *e, double 
     for (int q = 0; q < 7; ++q)
       if (src[q]) PBG_CUDA(cudaMemcpyAsync(&h[q * N], src[q], N * 8, cudaMemcpyDeviceToHost, s->stream));
     PBG_CUDA(cudaStreamSynchronize(s->stream));
+    const int per = A.per;
     if (A.sym)
       for (int i = 0; i < nx; ++i)
         for (int j = 0; j < ny; ++j)
           for (int k = 0; k < nz; ++k) {
             long long p = ((long long)i * ny + j) * nz + k;
-            h[2 * N + p] = i < nx - 1 ? h[1 * N + p + SI] : 0.0;
-            h[4 * N + p] = j < ny - 1 ? h[3 * N + p + SJ] : 0.0;
-            h[6 * N + p] = k < nz - 1 ? h[5 * N + p + 1] : 0.0;
+            h[2 * N + p] = i < nx - 1 ? h[1 * N + p + SI] : ((per & 1) ? h[1 * N + p - (nx - 1) * SI] : 0.0);
+            h[4 * N + p] = j < ny - 1 ? h[3 * N + p + SJ] : ((per & 2) ? h[3 * N + p - (ny - 1) * SJ] : 0.0);
+            h[6 * N + p] = k < nz - 1 ? h[5 * N + p + 1] : ((per & 4) ? h[5 * N + p - (nz - 1)] : 0.0);
           }
     double *dst[7] = {c, w, e, sv, n, b, t};
     for (int q = 0; q < 7; ++q) {
@@ -529,6 +576,7 @@ int pbg_body_upload(pbg_session *s, const double *fV, const double *fS, int wher
 
 int pbg_assemble_pressure(pbg_session *s, const double *rho, const uint8_t *solid, int where) {
   if (!s || !rho || !solid) return fail(PBG_ERR_ARG, "NULL argument");
+  if (s->per) return fail(PBG_ERR_UNSUPPORTED, "periodic boundaries: the on-device assembly and the flow functions take walls only (upload the matrix)");
   return guard(s, [&]() -> int {
     const long long N = s->ncell();
     DBuf<double> drho;
@@ -560,6 +608,7 @@ int pbg_assemble_pressure(pbg_session *s, const double *rho, const uint8_t *soli
 int pbg_assemble_mix(pbg_session *s, const double *col, double rho_a, double rho_b, const uint8_t *solid,
                      int where) {
   if (!s) return fail(PBG_ERR_ARG, "session is NULL");
+  if (s->per) return fail(PBG_ERR_UNSUPPORTED, "periodic boundaries: the on-device assembly and the flow functions take walls only (upload the matrix)");
   if (!(rho_a > 0.0) || (col && !(rho_b > 0.0))) return fail(PBG_ERR_ARG, "densities must be positive");
   return guard(s, [&]() -> int {
     const long long N = s->ncell();
@@ -650,6 +699,7 @@ extern "C" {
 int pbg_divergence(pbg_session *s, const double *u, const double *v, const double *w, const uint8_t *solid,
                    double dt, double *rhs, int where) {
   if (!s || !rhs) return fail(PBG_ERR_ARG, "NULL argument");
+  if (s->per) return fail(PBG_ERR_UNSUPPORTED, "periodic boundaries: the on-device assembly and the flow functions take walls only (upload the matrix)");
   if (int rc = check_faces(s, u, v, w)) return rc;
   if (!(dt > 0.0)) return fail(PBG_ERR_ARG, "dt must be positive");
   return guard(s, [&]() -> int {
@@ -687,6 +737,7 @@ int pbg_divergence(pbg_session *s, const double *u, const double *v, const doubl
 int pbg_project(pbg_session *s, const double *p, const double *col, double rho_a, double rho_b,
                 const uint8_t *solid, double dt, double *u, double *v, double *w, int where) {
   if (!s || !p) return fail(PBG_ERR_ARG, "NULL argument");
+  if (s->per) return fail(PBG_ERR_UNSUPPORTED, "periodic boundaries: the on-device assembly and the flow functions take walls only (upload the matrix)");
   if (int rc = check_faces(s, u, v, w)) return rc;
   if (!(dt > 0.0)) return fail(PBG_ERR_ARG, "dt must be positive");
   if (!(rho_a > 0.0) || (col && !(rho_b > 0.0))) return fail(PBG_ERR_ARG, "densities must be positive");
@@ -730,6 +781,7 @@ int pbg_pressure_step(pbg_session *s, const double *col, double rho_a, double rh
                       double dt, double *u, double *v, double *w, double *p, int where, const pbg_params *prm,
                       pbg_result *res) {
   if (!s || !p || !prm) return fail(PBG_ERR_ARG, "NULL argument");
+  if (s->per) return fail(PBG_ERR_UNSUPPORTED, "periodic boundaries: the on-device assembly and the flow functions take walls only (upload the matrix)");
   if (int rc = check_faces(s, u, v, w)) return rc;
   if (!(dt > 0.0)) return fail(PBG_ERR_ARG, "dt must be positive");
   return guard(s, [&]() -> int {
@@ -902,6 +954,9 @@ int solve_device(pbg_session *s, double *xd, const double *bd, const pbg_params 
     out.res = ar.res;
     out.levels = s->refac->nlevels();
   } else if (p->solver == PBG_SOLVER_ENGINE) {
+    if (s->A.per)
+      return fail(PBG_ERR_UNSUPPORTED, "periodic boundaries: the engine solver takes walls only "
+                                       "(use CG, BiCGS, CGS or AC)");
     const bool mixed = p->precision == PBG_MIXED;
     if (p->coarse_max < 0) return fail(PBG_ERR_ARG, "coarse_max must be >= 0");
     ensure_engine(s, mixed, p->coarse_max);

@@ -102,6 +102,7 @@ template <typename T>
 struct MatView {
   int nx, ny, nz;
   const T *c, *w, *e, *s, *n, *b, *t;   // e, n, t == nullptr: symmetric storage
+  int per;   // periodic axes: bit 0 i, bit 1 j, bit 2 k (0 in aggregate initialisers)
   __host__ __device__ long long ncell() const { return (long long)nx * ny * nz; }
 };
 
@@ -160,9 +161,27 @@ struct Geo {
 template <typename T>
 struct Nb { T w, e, s, n, b, t; };
 
+// Indices of the six neighbours of cell p: -1 across a non-periodic
+// boundary face; across a periodic one the cell at the other end, which is
+// where the reference's periodic halo copy takes its value from
+// (Src/Field/Scalar/scalar_exchange.cpp:47-58).
+struct NbIdx { long long w, e, s, n, b, t; };
+
+template <typename T>
+__device__ __forceinline__ NbIdx nb_index(const MatView<T> &A, long long p, Pos q) {
+  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
+  NbIdx o;
+  o.w = q.i > 0 ? p - SI : ((A.per & 1) ? p + (long long)(A.nx - 1) * SI : -1);
+  o.e = q.i < A.nx - 1 ? p + SI : ((A.per & 1) ? p - (long long)(A.nx - 1) * SI : -1);
+  o.s = q.j > 0 ? p - SJ : ((A.per & 2) ? p + (long long)(A.ny - 1) * SJ : -1);
+  o.n = q.j < A.ny - 1 ? p + SJ : ((A.per & 2) ? p - (long long)(A.ny - 1) * SJ : -1);
+  o.b = q.k > 0 ? p - 1 : ((A.per & 4) ? p + (long long)(A.nz - 1) : -1);
+  o.t = q.k < A.nz - 1 ? p + 1 : ((A.per & 4) ? p - (long long)(A.nz - 1) : -1);
+  return o;
+}
+
 template <typename T>
 __device__ __forceinline__ Nb<T> coeffs(const MatView<T> &A, long long p, Pos q) {
-  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
   Nb<T> o;
   o.w = A.w[p];
   o.s = A.s[p];
@@ -172,9 +191,10 @@ __device__ __forceinline__ Nb<T> coeffs(const MatView<T> &A, long long p, Pos q)
     o.n = A.n[p];
     o.t = A.t[p];
   } else {
-    o.e = (q.i < A.nx - 1) ? A.w[p + SI] : T(0);
-    o.n = (q.j < A.ny - 1) ? A.s[p + SJ] : T(0);
-    o.t = (q.k < A.nz - 1) ? A.b[p + 1] : T(0);
+    const NbIdx m = nb_index(A, p, q);
+    o.e = m.e >= 0 ? A.w[m.e] : T(0);
+    o.n = m.n >= 0 ? A.s[m.n] : T(0);
+    o.t = m.t >= 0 ? A.b[m.t] : T(0);
   }
   return o;
 }

@@ -21,11 +21,11 @@ __device__ __forceinline__ double ld0(const double *x, long long p, bool ok) {
 //   y = c x;  y -= (w xw + e xe);  y -= (s xs + n xn);  y -= (b xb + t xt)
 template <typename XF>
 __device__ __forceinline__ double ref_ax(const MatView<double> &A, long long p, Pos q, XF xv) {
-  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
   Nb<double> a = coeffs(A, p, q);
-  double xw = q.i > 0 ? xv(p - SI) : 0.0, xe = q.i < A.nx - 1 ? xv(p + SI) : 0.0;
-  double xs = q.j > 0 ? xv(p - SJ) : 0.0, xn = q.j < A.ny - 1 ? xv(p + SJ) : 0.0;
-  double xb = q.k > 0 ? xv(p - 1) : 0.0, xt = q.k < A.nz - 1 ? xv(p + 1) : 0.0;
+  const NbIdx m = nb_index(A, p, q);
+  double xw = m.w >= 0 ? xv(m.w) : 0.0, xe = m.e >= 0 ? xv(m.e) : 0.0;
+  double xs = m.s >= 0 ? xv(m.s) : 0.0, xn = m.n >= 0 ? xv(m.n) : 0.0;
+  double xb = m.b >= 0 ? xv(m.b) : 0.0, xt = m.t >= 0 ? xv(m.t) : 0.0;
   double v = __dmul_rn(A.c[p], xv(p));
   v = __dsub_rn(v, __dadd_rn(__dmul_rn(a.w, xw), __dmul_rn(a.e, xe)));
   v = __dsub_rn(v, __dadd_rn(__dmul_rn(a.s, xs), __dmul_rn(a.n, xn)));
@@ -38,11 +38,11 @@ __device__ __forceinline__ double ref_ax(const MatView<double> &A, long long p, 
 //   r = b - c x;  r += w xw + e xe;  r += s xs + n xn;  r += b xb + t xt
 __device__ __forceinline__ double ref_bmax(const MatView<double> &A, long long p, Pos q,
                                            const double *x, double bp) {
-  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
   Nb<double> a = coeffs(A, p, q);
-  double xw = ld0(x, p - SI, q.i > 0), xe = ld0(x, p + SI, q.i < A.nx - 1);
-  double xs = ld0(x, p - SJ, q.j > 0), xn = ld0(x, p + SJ, q.j < A.ny - 1);
-  double xb = ld0(x, p - 1, q.k > 0), xt = ld0(x, p + 1, q.k < A.nz - 1);
+  const NbIdx m = nb_index(A, p, q);
+  double xw = ld0(x, m.w, m.w >= 0), xe = ld0(x, m.e, m.e >= 0);
+  double xs = ld0(x, m.s, m.s >= 0), xn = ld0(x, m.n, m.n >= 0);
+  double xb = ld0(x, m.b, m.b >= 0), xt = ld0(x, m.t, m.t >= 0);
   double v = __dsub_rn(bp, __dmul_rn(A.c[p], x[p]));
   v = __dadd_rn(v, __dadd_rn(__dmul_rn(a.w, xw), __dmul_rn(a.e, xe)));
   v = __dadd_rn(v, __dadd_rn(__dmul_rn(a.s, xs), __dmul_rn(a.n, xn)));
@@ -781,13 +781,24 @@ struct FineCell {
   __device__ double s(int i, int j, int k) const { return A.s[at(i, j, k)]; }
   __device__ double b(int i, int j, int k) const { return A.b[at(i, j, k)]; }
   __device__ double e(int i, int j, int k) const {
-    return A.e ? A.e[at(i, j, k)] : (i < A.nx - 1 ? A.w[at(i + 1, j, k)] : 0.0);
+    return A.e ? A.e[at(i, j, k)]
+               : (i < A.nx - 1 ? A.w[at(i + 1, j, k)] : ((A.per & 1) ? A.w[at(0, j, k)] : 0.0));
   }
   __device__ double n(int i, int j, int k) const {
-    return A.n ? A.n[at(i, j, k)] : (j < A.ny - 1 ? A.s[at(i, j + 1, k)] : 0.0);
+    return A.n ? A.n[at(i, j, k)]
+               : (j < A.ny - 1 ? A.s[at(i, j + 1, k)] : ((A.per & 2) ? A.s[at(i, 0, k)] : 0.0));
   }
   __device__ double t(int i, int j, int k) const {
-    return A.t ? A.t[at(i, j, k)] : (k < A.nz - 1 ? A.b[at(i, j, k + 1)] : 0.0);
+    return A.t ? A.t[at(i, j, k)]
+               : (k < A.nz - 1 ? A.b[at(i, j, k + 1)] : ((A.per & 4) ? A.b[at(i, j, 0)] : 0.0));
+  }
+  // a neighbour's value of a level field: the zero halo outside a
+  // non-periodic face, the other end's cell across a periodic one
+  __device__ double nbv(const double *x, int i, int j, int k) const {
+    if (i < 0 || i >= A.nx) { if (!(A.per & 1)) return 0.0; i = i < 0 ? i + A.nx : i - A.nx; }
+    if (j < 0 || j >= A.ny) { if (!(A.per & 2)) return 0.0; j = j < 0 ? j + A.ny : j - A.ny; }
+    if (k < 0 || k >= A.nz) { if (!(A.per & 4)) return 0.0; k = k < 0 ? k + A.nz : k - A.nz; }
+    return x[at(i, j, k)];
   }
 };
 
@@ -870,9 +881,7 @@ __global__ void k_ac_restrict(MatView<double> A, const double *__restrict__ phi,
                               int CI, int CJ, int CK, double *mean_out, double *part,
                               unsigned *count, double *seq) {
   FineCell f(A);
-  auto ph = [&](int i, int j, int k) -> double {
-    return (i < 0 || i >= A.nx || j < 0 || j >= A.ny || k < 0 || k >= A.nz) ? 0.0 : phi[f.at(i, j, k)];
-  };
+  auto ph = [&](int i, int j, int k) -> double { return f.nbv(phi, i, j, k); };
   const long long NH = (long long)Hnx * Hny * Hnz;
   double v[2] = {0.0, 0.0};
   for (long long P = blockIdx.x * (long long)blockDim.x + threadIdx.x; P < NH;
@@ -1040,9 +1049,12 @@ __global__ void k_jacobi_x(long long N, const double *__restrict__ c, const doub
 
 // the cells of hyperplane h: x = ci (b + w xw + e xe + s xs + n xn + b xb
 // + t xt), summed left to right (gaussseidel.cpp:50-60). One thread per
-// (i, j) column; k = h - i - j.
+// (i, j) column; k = h - i - j. Across a periodic face the reference reads
+// its halo, filled by the exchange before the sweep: xold, a copy of x
+// taken before the sweep (only read when the matrix has periodic axes).
 __global__ void k_gs_plane(MatView<double> A, const double *__restrict__ ci,
-                           const double *__restrict__ b, double *x, int h, const KrylovState *st) {
+                           const double *__restrict__ b, double *x, int h, const KrylovState *st,
+                           const double *__restrict__ xold) {
   if (st->done) return;
   const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
   const long long nij = (long long)A.nx * A.ny;
@@ -1054,13 +1066,19 @@ __global__ void k_gs_plane(MatView<double> A, const double *__restrict__ ci,
     const long long p = ((long long)i * A.ny + j) * A.nz + k;
     const Pos q{i, j, k};
     Nb<double> a = coeffs(A, p, q);
+    const NbIdx m = nb_index(A, p, q);
+    // interior neighbours from x (this sweep's values where they come
+    // first), wrapped ones from the pre-sweep copy
+    auto nv = [&](long long idx, bool inside) {
+      return idx < 0 ? 0.0 : (inside ? x[idx] : xold[idx]);
+    };
     double v = b[p];
-    v = __dadd_rn(v, __dmul_rn(a.w, ld0(x, p - SI, i > 0)));
-    v = __dadd_rn(v, __dmul_rn(a.e, ld0(x, p + SI, i < A.nx - 1)));
-    v = __dadd_rn(v, __dmul_rn(a.s, ld0(x, p - SJ, j > 0)));
-    v = __dadd_rn(v, __dmul_rn(a.n, ld0(x, p + SJ, j < A.ny - 1)));
-    v = __dadd_rn(v, __dmul_rn(a.b, ld0(x, p - 1, k > 0)));
-    v = __dadd_rn(v, __dmul_rn(a.t, ld0(x, p + 1, k < A.nz - 1)));
+    v = __dadd_rn(v, __dmul_rn(a.w, nv(m.w, i > 0)));
+    v = __dadd_rn(v, __dmul_rn(a.e, nv(m.e, i < A.nx - 1)));
+    v = __dadd_rn(v, __dmul_rn(a.s, nv(m.s, j > 0)));
+    v = __dadd_rn(v, __dmul_rn(a.n, nv(m.n, j < A.ny - 1)));
+    v = __dadd_rn(v, __dmul_rn(a.b, nv(m.b, k > 0)));
+    v = __dadd_rn(v, __dmul_rn(a.t, nv(m.t, k < A.nz - 1)));
     x[p] = __dmul_rn(ci[p], v);
   }
 }
@@ -1217,8 +1235,12 @@ void enqueue_ref_iters(const MatView<double> &A, double *x, int solver, int coun
     const int H = A.nx + A.ny + A.nz - 2, gp = grid_for((long long)A.nx * A.ny);
     for (int it = 0; it < count; ++it) {
       if (gs) {
+        if (A.per) {  // the halo the exchange fills before each sweep
+          if (w.xold.n < (size_t)N) w.xold.alloc(N);
+          PBG_CUDA(cudaMemcpyAsync(w.xold.p, x, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+        }
         for (int h = 0; h < H; ++h) {
-          k_gs_plane<<<gp, kThreads, 0, s>>>(A, w.ci, w.rhs, x, h, st); note_launch();
+          k_gs_plane<<<gp, kThreads, 0, s>>>(A, w.ci, w.rhs, x, h, st, w.xold.p); note_launch();
         }
       } else {
         k_jacobi_x<<<grid_for(N), kThreads, 0, s>>>(N, A.c, w.ci, w.r.p, x, st); note_launch();
@@ -1237,7 +1259,7 @@ void enqueue_ref_iters(const MatView<double> &A, double *x, int solver, int coun
       k_cg_rho<<<g, kThreads, 0, s>>>(N, w.r.p, w.z.p, st, P0, C0); note_launch();
       k_cg_pq<<<g, kThreads, 0, s>>>(A, w.r.p, w.pA.p, w.pB.p, w.q.p, st, P0, C0, w.z.p, w.mcd.p); note_launch();
       k_cg_xr<<<g, kThreads, 0, s>>>(N, w.mcd.p, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1, 1); note_launch();
-    } else if (solver == 0 && !exact && A.nz % 2 == 0) {
+    } else if (solver == 0 && !exact && A.nz % 2 == 0 && !A.per) {
       const int gq = grid_for(N / 2);
       k_cg_p<<<gq, kThreads, 0, s>>>(N, w.r.p, w.mcd.p, w.pA.p, st); note_launch();
       k_cg_q<<<gq, kThreads, 0, s>>>(A, Geo(A.nx, A.ny, A.nz), w.pA.p, w.q.p, st, P0, C0); note_launch();
@@ -1335,6 +1357,7 @@ void RefAC::build(const MatView<double> &A0, const uint8_t *aflag0, double h, cu
     c.dV = hx * hy * hz;
     const long long NH = (long long)c.nx * c.ny * c.nz;
     c.A.nx = c.nx; c.A.ny = c.ny; c.A.nz = c.nz; c.A.sym = false;
+    c.A.per = A0.per;  // coarse levels keep the fine level's periodic axes
     DBuf<double> *arr[7] = {&c.A.c, &c.A.w, &c.A.e, &c.A.s, &c.A.n, &c.A.b, &c.A.t};
     for (auto *a : arr) a->alloc(NH);
     c.phi.alloc(NH); c.fnew.alloc(NH); c.aflag.alloc(NH);

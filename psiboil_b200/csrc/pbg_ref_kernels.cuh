@@ -29,6 +29,7 @@ struct KrylovParams {
 struct RefKrylovWork {
   DBuf<double> r, q, pA, pB, rt, ph, v, s, sh, t, u;
   DBuf<double> mcd;                               // 1 / c (the diagonal preconditioner)
+  DBuf<double> xold;                              // Gauss-Seidel: x before the sweep (periodic)
   const double *rhs = nullptr, *ci = nullptr;     // Jacobi / Gauss-Seidel operands of a solve
   DBuf<double> z, mc, mw, ms, mb, mtw, mts, mnw;  // IC preconditioner
   void ensure(size_t n, int solver);

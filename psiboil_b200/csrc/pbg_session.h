@@ -70,10 +70,11 @@ struct RedPool {
 struct Mat64 {
   int nx = 0, ny = 0, nz = 0;
   bool sym = false;
+  int per = 0;   // periodic axes (bit 0 i, 1 j, 2 k)
   DBuf<double> c, w, e, s, n, b, t;
   MatView<double> view() const {
     return {nx, ny, nz, c.p, w.p, sym ? nullptr : e.p, s.p, sym ? nullptr : n.p, b.p,
-            sym ? nullptr : t.p};
+            sym ? nullptr : t.p, per};
   }
   long long ncell() const { return (long long)nx * ny * nz; }
 };

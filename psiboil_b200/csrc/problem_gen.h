@@ -74,7 +74,7 @@ static inline double pbg_u01(pbg_mt64 *g) {
 /* ------------------------------------------------------------------ */
 /* Problem description                                                 */
 /* ------------------------------------------------------------------ */
-enum { PBG_BC_NEUMANN = 0, PBG_BC_DIRICHLET = 1 };
+enum { PBG_BC_NEUMANN = 0, PBG_BC_DIRICHLET = 1, PBG_BC_PERIODIC = 2 };
 enum { PBG_MAX_BUBBLES = 64 };
 
 typedef struct {
@@ -306,28 +306,50 @@ static inline double pbg_harm(double a, double b) {
   return (a * b) * 2.0 / (a + b);
 }
 
+/* Periodic axes of a boundary-type list: bit d set when both faces of axis
+ * d (0 i, 1 j, 2 k) are periodic. */
+static inline int pbg_periodic_mask(const int bc[6]) {
+  int m = 0;
+  for (int d = 0; d < 3; ++d)
+    if (bc[2 * d] == PBG_BC_PERIODIC && bc[2 * d + 1] == PBG_BC_PERIODIC) m |= 1 << d;
+  return m;
+}
+
 /* Fixture assembly, stage 1: face coefficients dS/dx/rho_face from the
  * cell densities (pressure_discretize.cpp:24-57), c = sum of the six
  * (:65-67), faces between fluid and solid cells zeroed on both sides and c
  * of fluid cells recomputed (:72-119 for a voxel body: every fluid/solid
- * face pair is a "touch"). Boundary faces use the boundary cell's density. */
-static inline void pbg_gen_faces(int nx, int ny, int nz, double h,
-                                 const double *rho, const uint8_t *solid,
-                                 double *c, double *w, double *e, double *s,
-                                 double *n, double *b, double *t) {
+ * face pair is a "touch"). Boundary faces use the boundary cell's density;
+ * on a periodic axis (bit d of per) the boundary face couples to the cell
+ * at the other end, as the reference's periodic halo does
+ * (scalar_exchange.cpp:47-58), with the same harmonic density both ways. */
+static inline void pbg_gen_faces_per(int nx, int ny, int nz, double h, int per,
+                                     const double *rho, const uint8_t *solid,
+                                     double *c, double *w, double *e, double *s,
+                                     double *n, double *b, double *t) {
   const size_t SI = (size_t)ny * nz, SJ = (size_t)nz;
   const double hx = (h * h) / h; /* dS / dx for a uniform cube */
+  const int pi = per & 1, pj = (per >> 1) & 1, pk = (per >> 2) & 1;
+  /* neighbour index across each face, or -1 outside a non-periodic face */
+#define PBG_WEST(i) ((i) > 0 ? (long long)(p - SI) : (pi ? (long long)(p + (size_t)(nx - 1) * SI) : -1LL))
+#define PBG_EAST(i) ((i) < nx - 1 ? (long long)(p + SI) : (pi ? (long long)(p - (size_t)(nx - 1) * SI) : -1LL))
+#define PBG_SOUTH(j) ((j) > 0 ? (long long)(p - SJ) : (pj ? (long long)(p + (size_t)(ny - 1) * SJ) : -1LL))
+#define PBG_NORTH(j) ((j) < ny - 1 ? (long long)(p + SJ) : (pj ? (long long)(p - (size_t)(ny - 1) * SJ) : -1LL))
+#define PBG_BOT(k) ((k) > 0 ? (long long)(p - 1) : (pk ? (long long)(p + (size_t)(nz - 1)) : -1LL))
+#define PBG_TOP(k) ((k) < nz - 1 ? (long long)(p + 1) : (pk ? (long long)(p - (size_t)(nz - 1)) : -1LL))
   for (int i = 0; i < nx; ++i)
     for (int j = 0; j < ny; ++j)
       for (int k = 0; k < nz; ++k) {
         size_t p = (size_t)i * SI + (size_t)j * SJ + k;
         double rp = rho[p];
-        double rw = i > 0 ? pbg_harm(rho[p - SI], rp) : rp;
-        double re = i < nx - 1 ? pbg_harm(rp, rho[p + SI]) : rp;
-        double rs = j > 0 ? pbg_harm(rho[p - SJ], rp) : rp;
-        double rn = j < ny - 1 ? pbg_harm(rp, rho[p + SJ]) : rp;
-        double rb = k > 0 ? pbg_harm(rho[p - 1], rp) : rp;
-        double rt = k < nz - 1 ? pbg_harm(rp, rho[p + 1]) : rp;
+        long long qw = PBG_WEST(i), qe = PBG_EAST(i), qs = PBG_SOUTH(j), qn = PBG_NORTH(j);
+        long long qb = PBG_BOT(k), qt = PBG_TOP(k);
+        double rw = qw >= 0 ? pbg_harm(rho[qw], rp) : rp;
+        double re = qe >= 0 ? pbg_harm(rp, rho[qe]) : rp;
+        double rs = qs >= 0 ? pbg_harm(rho[qs], rp) : rp;
+        double rn = qn >= 0 ? pbg_harm(rp, rho[qn]) : rp;
+        double rb = qb >= 0 ? pbg_harm(rho[qb], rp) : rp;
+        double rt = qt >= 0 ? pbg_harm(rp, rho[qt]) : rp;
         w[p] = hx / rw; e[p] = hx / re;
         s[p] = hx / rs; n[p] = hx / rn;
         if (nz > 1) { b[p] = hx / rb; t[p] = hx / rt; }
@@ -339,21 +361,37 @@ static inline void pbg_gen_faces(int nx, int ny, int nz, double h,
       for (int k = 0; k < nz; ++k) {
         size_t p = (size_t)i * SI + (size_t)j * SJ + k;
         int sp = solid[p];
-        if (i > 0 && solid[p - SI] != sp) w[p] = 0.0;
-        if (i < nx - 1 && solid[p + SI] != sp) e[p] = 0.0;
-        if (j > 0 && solid[p - SJ] != sp) s[p] = 0.0;
-        if (j < ny - 1 && solid[p + SJ] != sp) n[p] = 0.0;
-        if (k > 0 && solid[p - 1] != sp) b[p] = 0.0;
-        if (k < nz - 1 && solid[p + 1] != sp) t[p] = 0.0;
+        long long qw = PBG_WEST(i), qe = PBG_EAST(i), qs = PBG_SOUTH(j), qn = PBG_NORTH(j);
+        long long qb = PBG_BOT(k), qt = PBG_TOP(k);
+        if (qw >= 0 && solid[qw] != sp) w[p] = 0.0;
+        if (qe >= 0 && solid[qe] != sp) e[p] = 0.0;
+        if (qs >= 0 && solid[qs] != sp) s[p] = 0.0;
+        if (qn >= 0 && solid[qn] != sp) n[p] = 0.0;
+        if (nz > 1 && qb >= 0 && solid[qb] != sp) b[p] = 0.0;
+        if (nz > 1 && qt >= 0 && solid[qt] != sp) t[p] = 0.0;
       }
+#undef PBG_WEST
+#undef PBG_EAST
+#undef PBG_SOUTH
+#undef PBG_NORTH
+#undef PBG_BOT
+#undef PBG_TOP
   for (size_t p = 0; p < (size_t)nx * SI; ++p)
     if (!solid[p]) c[p] = w[p] + e[p] + s[p] + n[p] + b[p] + t[p];
+}
+
+static inline void pbg_gen_faces(int nx, int ny, int nz, double h,
+                                 const double *rho, const uint8_t *solid,
+                                 double *c, double *w, double *e, double *s,
+                                 double *n, double *b, double *t) {
+  pbg_gen_faces_per(nx, ny, nz, h, 0, rho, solid, c, w, e, s, n, b, t);
 }
 
 /* Fixture assembly, stage 2: boundary correction restated from
  * centered_system_bnd.cpp:17-62 (Neumann sides in the order imin, imax,
  * jmin, jmax, kmin, kmax: c -= a_bnd, a_bnd = 0) and :143-185 (Dirichlet
- * p = 0: a_bnd = 0, c keeps it); then ci = 1/c (pressure_discretize.cpp:127)
+ * p = 0: a_bnd = 0, c keeps it); periodic faces keep their couplings; then
+ * ci = 1/c (pressure_discretize.cpp:127)
  * and solid cells c *= pico with all faces zeroed (:132-148). 2-D problems
  * (nz == 1) have no k faces. */
 static inline void pbg_gen_bc_finalize(int nx, int ny, int nz, const int bc[6],
@@ -418,7 +456,7 @@ static inline void pbg_gen_assemble(int nx, int ny, int nz, double h, const int 
                                     const double *rho, const uint8_t *solid,
                                     double *c, double *w, double *e, double *s,
                                     double *n, double *b, double *t, double *ci) {
-  pbg_gen_faces(nx, ny, nz, h, rho, solid, c, w, e, s, n, b, t);
+  pbg_gen_faces_per(nx, ny, nz, h, pbg_periodic_mask(bc), rho, solid, c, w, e, s, n, b, t);
   pbg_gen_bc_finalize(nx, ny, nz, bc, solid, c, w, e, s, n, b, t, ci);
 }
 

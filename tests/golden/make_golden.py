@@ -8,6 +8,7 @@ Only needed where the reference sources exist; the fixtures are committed.
 
     python tests/golden/make_golden.py            (everything)
     python tests/golden/make_golden.py --steps    (the step fixtures only)
+    python tests/golden/make_golden.py NAME ...   (those solver fixtures only)
 """
 import os
 import sys
@@ -33,6 +34,11 @@ CASES = [
     # non-symmetric: upwind convection along +x added to the fixture
     ("conv12", O.KIND_SINGLE, dict(n=12, convect=2e-5), ["bicgs", "cgs", "bicgs_ic0", "bicgs_ic2",
                                                         "cgs_ic2", "cgs_ic3", "jacobi", "gs"]),
+    # periodic boundaries (Periodic::yes grids, BndType::periodic): x and y
+    # periodic around the cylinder case; x periodic on the single bubble
+    ("per12", O.KIND_CYL, dict(n=12, nb=2, rmin=1.5, rmax=2.5, rc=3.0, periodic=3),
+     ["cg", "bicgs", "ac", "jacobi", "gs", "cg_ic2", "acsm_gs", "ac_w"]),
+    ("per16", O.KIND_SINGLE, dict(n=16, periodic=1), ["cg", "cgs", "ac", "gs", "acsm_jacobi"]),
 ]
 
 # Jacobi and Gauss-Seidel converge slowly on these density jumps: a looser
@@ -99,7 +105,10 @@ def main():
     O.build()
     if not O.harness_available():
         raise SystemExit("oracle/_ref/ref_harness missing: run python oracle/build_ref.py")
+    only = [a for a in sys.argv[1:] if not a.startswith("--")]
     for name, kind, kw, runs in CASES:
+        if only and name not in only:
+            continue
         P = O.Problem(kind, 7, **kw)
         out = dict(dims=np.array(P.dims), h=np.array(P.h), kind=np.array(kind), seed=np.array(7))
         for k, v in kw.items():
@@ -138,7 +147,8 @@ def main():
             out["A"] = True
         del out["A"]
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
-    make_steps()
+    if not only:
+        make_steps()
 
 
 if __name__ == "__main__":

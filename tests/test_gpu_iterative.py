@@ -10,7 +10,7 @@ reference's as well."""
 import numpy as np
 import pytest
 
-from golden_util import NAMES, load, problem_of
+from golden_util import NAMES, bc_of, load, problem_of
 
 pytestmark = pytest.mark.gpu
 
@@ -18,7 +18,7 @@ RUNS = [(n, s) for n in NAMES for s in ("jacobi", "gs") if s + "_x" in load(n)]
 
 
 def _session(engine, g, P, ci=True):
-    s = engine.Session(*P.dims, P.h)
+    s = engine.Session(*P.dims, P.h, bc=bc_of(P))
     s.upload_matrix({k: g["A_" + k] for k in "cwesnbt"})
     if ci:
         s.upload_ci(g["ci"])

@@ -18,7 +18,7 @@ reduction modes:
 import numpy as np
 import pytest
 
-from golden_util import NAMES, load, problem_of
+from golden_util import NAMES, bc_of, load, problem_of
 
 pytestmark = pytest.mark.gpu
 RTOL_X = 1e-10
@@ -32,8 +32,8 @@ def session_for(engine, P, assemble=True):
     """A session holding P's matrix: assembled on the device, or uploaded
     (always uploaded for the convected fixtures, which the on-device
     pressure assembly does not make)."""
-    s = engine.Session(*P.dims, P.h)
-    if assemble and not P.convect:
+    s = engine.Session(*P.dims, P.h, bc=bc_of(P))
+    if assemble and not P.convect and not P.periodic:
         s.assemble_pressure(P.rho, P.solid)
     else:
         s.upload_matrix(P.A)
@@ -46,6 +46,12 @@ def test_assembly_bit_exact(engine, oracle, name):
     P = problem_of(load(name), oracle)
     if P.convect:
         pytest.skip("the convected fixture is uploaded, not assembled")
+    if P.periodic:
+        with engine.Session(*P.dims, P.h, bc=bc_of(P)) as s:
+            with pytest.raises(engine.PbgError) as e:
+                s.assemble_pressure(P.rho, P.solid)
+            assert e.value.code == engine.ERR_UNSUPPORTED
+        return
     with session_for(engine, P) as s:
         assert s.symmetric()
         M = s.download_matrix()
@@ -224,3 +230,27 @@ def test_config0_64_cg_and_ac(engine, oracle):
             ok, ncyc = engine.AC(s, exact_sums=exact).vcycle(xa, P.b.copy(), factor=1e-8)
             assert ncyc == sr["cycles"] and ok == bool(sr["converged"])
             assert relerr(xa, xr) <= (0.0 if exact else RTOL_X)
+
+
+def test_periodic_couplings_need_a_periodic_session(engine, oracle):
+    """A matrix that couples cells across an outer face is refused, with
+    PBG_ERR_UNSUPPORTED, by a session whose boundaries there are walls: the
+    solvers would otherwise solve a different operator. With periodic
+    boundaries on those axes the same matrix is taken, and the engine solver
+    (walls only) refuses it."""
+    g = load("per12")
+    P = problem_of(g, oracle)
+    A = {k: g["A_" + k] for k in "cwesnbt"}
+    with engine.Session(*P.dims, P.h) as s:
+        with pytest.raises(engine.PbgError) as e:
+            s.upload_matrix(A)
+        assert e.value.code == engine.ERR_UNSUPPORTED
+    with engine.Session(*P.dims, P.h, bc=bc_of(P)) as s:
+        s.upload_matrix(A)
+        assert s.symmetric()
+        M = s.download_matrix()
+        for k in "cwesnbt":
+            assert np.array_equal(M[k], A[k]), k
+        with pytest.raises(engine.PbgError) as e:
+            engine.Engine(s).solve(np.zeros(P.N), P.b.copy(), tol=1e-8)
+        assert e.value.code == engine.ERR_UNSUPPORTED
