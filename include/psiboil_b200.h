@@ -85,7 +85,7 @@ enum {
   PBG_SOLVER_GAUSS_SEIDEL = 6  /* GaussSeidel::solve, lexicographic (parity)       */
 };
 enum { PBG_FP64 = 0, PBG_MIXED = 1 };
-enum { PBG_CYCLE_NONE = -1, PBG_CYCLE_V = 1, PBG_CYCLE_F = 2, PBG_CYCLE_W = 4 };
+enum { PBG_CYCLE_NONE = -1, PBG_CYCLE_V = 1, PBG_CYCLE_F = 2, PBG_CYCLE_W = 4, PBG_CYCLE_FLEX = 5 };
 
 typedef struct {
   int solver;
@@ -99,8 +99,12 @@ typedef struct {
   double scale;
   int stalecount;         /* <= 0: off; at most 64                              */
   /* AC::cycle(init, loop, ResTol, ResRat, mv, ms, &ncyc) and setters */
-  int init_cycle;         /* PBG_CYCLE_NONE | V | F | W                         */
-  int loop_cycle;         /* PBG_CYCLE_V | F | W                                */
+  int init_cycle;         /* PBG_CYCLE_NONE | V | F | W | FLEX (a full cycle first) */
+  int loop_cycle;         /* PBG_CYCLE_V | F | W | FLEX, or PBG_CYCLE_NONE: the
+                             reference's "just solve" branch (additive_cycle.cpp:
+                             66-71): one call of AC's solver on level 0 (MaxIter 40,
+                             ResRat 0.001, ResTol 1e-15), then not converged with
+                             cycles = max_cycles                                */
   double toler;           /* ResTol of the cycle loop (< 0 disables)            */
   double factor;          /* ResRat of the cycle loop (< 0 disables)            */
   int max_cycles, min_cycles, stop_if_div, priority_min_cyc;
@@ -135,6 +139,27 @@ typedef struct {
    * or PBG_SOLVER_GAUSS_SEIDEL (level 0 with the uploaded A.ci, coarse levels
    * with ci = 1/c, as additive_coarsen_system.cpp forms it). */
   int ac_smoother;
+  /* PBG_SOLVER_AC: AC's own solver, AC(cen, sol) (additive.cpp:41-45), which
+   * call_solver uses for post-smoothing and the coarsest level
+   * (additive_cycle_functions.cpp:100-107): -1 (default) the same as
+   * ac_smoother, else a solver code as for ac_smoother with ac_solver_prec. */
+  int ac_solver, ac_solver_prec;
+  /* PBG_SOLVER_AC: AC::resrat / AC::restol, the ResRat and ResTol of the
+   * level solvers (additive.h:105-110; default 1e-18, boil::atto). */
+  double ac_resrat, ac_restol;
+  /* PBG_SOLVER_AC: AC::use_linf_error (additive.h:141): 1 drives the cycle's
+   * tests with max |r/dV| instead of the volume-averaged 2-norm. */
+  int use_linf;
+  /* PBG_SOLVER_AC with PBG_CYCLE_FLEX: smoother calls per flex cycle at most
+   * (0: 10^6). The reference's flex cycle returns only when level 0's
+   * smoother reaches AC::resrat, and runs forever when it never does; at this
+   * bound the cycle ends and the solve reports PBG_MAXITER. */
+  int flex_visits;
+  /* PBG_SOLVER_AC: the time step dt that scales AC's residual measure
+   * (additive_residual.cpp:19-27, L[0]->time->dt(); default 1). The level
+   * solvers get `scale` as their scale (the reference passes dti * scale,
+   * additive_cycle_functions.cpp:90-107). */
+  double ac_dt;
 } pbg_params;
 
 typedef struct {

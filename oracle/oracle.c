@@ -595,6 +595,7 @@ struct orc_ac {
   int sol_kind, sol_prec;
   int use_linf;       /* AC::use_linf_error (additive.h:141) */
   int flex_capped;    /* the last flex cycle hit its visit bound */
+  long long flex_cap; /* smoother calls per flex cycle at most */
 };
 
 /* Domain::factor (domain_factor.cpp:4-21): first factor = smallest prime */
@@ -626,6 +627,7 @@ orc_ac *orc_ac_create(const orc_mat *A, const uint8_t *aflag, double h) {
   ac->resrat_val = 1.0e-18; /* boil::atto */
   ac->restol_val = 1.0e-18;
   ac->sol_kind = -1;
+  ac->flex_cap = 1000000;
   orc_level *L0 = &ac->L[0];
   L0->nx = A->nx; L0->ny = A->ny; L0->nz = A->nz;
   L0->CI = L0->CJ = L0->CK = 1;
@@ -898,6 +900,7 @@ void orc_ac_set_smoother(orc_ac *ac, int kind, int prec, const double *ci0) {
 }
 
 int orc_ac_flex_capped(const orc_ac *ac) { return ac->flex_capped; }
+void orc_ac_set_flex_cap(orc_ac *ac, long long cap) { ac->flex_cap = cap; }
 
 void orc_ac_set_params(orc_ac *ac, double resrat_val, double restol_val, int use_linf,
                        int sol_kind, int sol_prec) {
@@ -950,11 +953,11 @@ static void fw_cycle(orc_ac *ac, int l, const int mv[3], const int ms[3], int w)
  * 0's smoother converges.
  * The reference recurses without a bound and never returns when level 0
  * never converges (AC::resrat at its default atto, for instance); here at
- * most 1000 smoother calls per level are made, after which the cycle ends
- * and flex_capped is set. */
+ * most flex_cap smoother calls (10^6 unless set) are made, after which the
+ * cycle ends and flex_capped is set. */
 static void flex_cycle(orc_ac *ac, int l, const int mv[3], const int ms[3]) {
   const int last = ac->nlevels - 1;
-  long long visits = 0, cap = 1000LL * ac->nlevels;
+  long long visits = 0, cap = ac->flex_cap;
   int pos = 0;
   ac->flex_capped = 0;
   for (;;) {
@@ -1040,6 +1043,8 @@ int orc_ac_cycle(orc_ac *ac, double *x, const double *b, int init, int loop,
   if (init != -1) {
     full_cycle(ac, 0, init, mv, ms);
     res_m1 = residual(ac, &linf_m1);
+    if (res_hist) res_hist[nh] = res_m1;  /* the reference logs "Cycle 0" */
+    nh++;
     /* converged(..., cycle 0, ...) (:39-43): its return value is dropped,
      * but its divergence branch runs. It compares the residual with itself
      * (res0 is res_m1, the same state), so unless cycle 0 already meets the

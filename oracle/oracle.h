@@ -109,8 +109,10 @@ void orc_ac_set_smoother(orc_ac *ac, int kind, int prec, const double *ci0);
  * (additive_cycle_functions.cpp:100-107). */
 void orc_ac_set_params(orc_ac *ac, double resrat_val, double restol_val, int use_linf,
                        int sol_kind, int sol_prec);
-/* 1 when the last flex cycle stopped at its visit bound (see oracle.c) */
+/* 1 when the last flex cycle stopped at its visit bound (see oracle.c),
+ * and the bound itself (smoother calls per flex cycle, 10^6 by default) */
 int orc_ac_flex_capped(const orc_ac *ac);
+void orc_ac_set_flex_cap(orc_ac *ac, long long cap);
 int orc_ac_nlevels(const orc_ac *ac);
 void orc_ac_level_dims(const orc_ac *ac, int l, int *dims /* 3 */);
 /* Coarse operators of all levels (AC::coarsen_system,

@@ -80,6 +80,7 @@ def lib():
                                         ctypes.c_int, ctypes.c_int]
         L.orc_ac_flex_capped.restype = ctypes.c_int
         L.orc_ac_flex_capped.argtypes = [ctypes.c_void_p]
+        L.orc_ac_set_flex_cap.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
         L.orc_ac_nlevels.restype = ctypes.c_int
         L.orc_ac_nlevels.argtypes = [ctypes.c_void_p]
         L.orc_ac_level_dims.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
@@ -221,7 +222,7 @@ class AC:
     SMOOTHERS = {"cg": 0, "bicgs": 1, "cgs": 2, "jacobi": 3, "gs": 4}
 
     def __init__(self, P, smoother="cg", prec="di", solver=None, solver_prec="di", resrat=1e-18,
-                 restol=1e-18, use_linf=False):
+                 restol=1e-18, use_linf=False, flex_cap=1000000):
         """smoother: the levels' solver (the Pressure's Linear); solver: AC's
         own solver for call_solver (AC(cen, sol)), None for the same;
         resrat/restol: AC::resrat/restol; use_linf: AC::use_linf_error."""
@@ -238,6 +239,7 @@ class AC:
             lib().orc_ac_set_smoother(self.h, 0, 0, _p(self._ci))
         lib().orc_ac_set_params(self.h, resrat, restol, int(use_linf),
                                 -1 if solver is None else self.SMOOTHERS[solver], PRECS[solver_prec])
+        lib().orc_ac_set_flex_cap(self.h, int(flex_cap))
 
     @property
     def flex_capped(self):

@@ -44,7 +44,9 @@
  * AC::cycle(init, loop, ResTol(-1), ResRat, mv, ms)); --init V|F|W starts
  * with a full cycle of that kind; --linf 1 sets use_linf_error(true);
  * --acsolver names a distinct solver for AC(cen, sol); --acresrat sets
- * AC::resrat, the ResRat of the level solvers (atto by default).
+ * AC::resrat, the ResRat of the level solvers (atto by default). In the
+ * engine-linked build (ref_harness_gpu), --gpu 1 swaps the Pressure's solver
+ * for the drop-in Gpu* class and --gpu 2 also swaps AC for GpuAC.
  *
  * --periodic MASK makes the axes of MASK (bit 0 i, 1 j, 2 k) periodic: the
  * grids are built with Periodic::yes(), the pressure (and velocity) get
@@ -465,6 +467,30 @@ int run_step(const Args &a, const pbg_problem_desc &D) {
   return 0;
 }
 
+/* The AC run of --solver ac with the harness's settings, for the
+ * reference's AC and for the drop-in GpuAC alike. */
+template <typename ACT>
+bool run_ac(ACT &mg, const Args &a, int *ncyc) {
+  mg.max_cycles(a.maxcyc);
+  mg.min_cycles(a.mincyc);
+  mg.stop_if_diverging(a.guard != 0);
+  mg.use_linf_error(a.linf != 0);
+  if (a.acresrat > 0.0) mg.resrat(ResRat(a.acresrat));
+  struct C {
+    static Cycle of(const std::string &c) {
+      return c == "V" ? Cycle::V() : c == "F" ? Cycle::F() : c == "W" ? Cycle::W()
+             : c == "flex" ? Cycle::flex() : Cycle::none();
+    }
+  };
+  const std::array<MaxIter, 3> mv = {{MaxIter(20), MaxIter(20), MaxIter(20)}};
+  const std::array<MaxIter, 3> ms = {{MaxIter(-1), MaxIter(-1), MaxIter(-1)}};
+  if (a.init != "none" || a.cycle == "flex" || a.cycle == "none")
+    return mg.cycle(C::of(a.init), C::of(a.cycle), ResTol(-1.0), ResRat(a.resrat), mv, ms, ncyc);
+  if (a.cycle == "F") return mg.fcycle(ResRat(a.resrat), ncyc);
+  if (a.cycle == "W") return mg.wcycle(ResRat(a.resrat), ncyc);
+  return mg.vcycle(ResRat(a.resrat), ncyc);
+}
+
 pbg_problem_desc make_desc(const Args &a) {
   pbg_problem_desc d;
   if (a.kind == "single") pbg_desc_single_bubble(&d, a.n, a.seed);
@@ -559,25 +585,19 @@ int main(int argc, char **argv) {
     else if (a.acsolver == "cgs") acsol = new CGS(d, pc);
     else if (a.acsolver == "jacobi") acsol = new Jacobi(d);
     else if (a.acsolver == "gs") acsol = new GaussSeidel(d);
-    AC mg(&pr, acsol);
-    mg.max_cycles(a.maxcyc);
-    mg.min_cycles(a.mincyc);
-    mg.stop_if_diverging(a.guard != 0);
-    mg.use_linf_error(a.linf != 0);
-    if (a.acresrat > 0.0) mg.resrat(ResRat(a.acresrat));
     p = 0.0;
-    auto cyc = [](const std::string &c) {
-      return c == "V" ? Cycle::V() : c == "F" ? Cycle::F() : c == "W" ? Cycle::W()
-             : c == "flex" ? Cycle::flex() : Cycle::none();
-    };
-    const std::array<MaxIter, 3> mv = {MaxIter(20), MaxIter(20), MaxIter(20)};
-    const std::array<MaxIter, 3> ms = {MaxIter(-1), MaxIter(-1), MaxIter(-1)};
     auto t0 = std::chrono::steady_clock::now();
-    if (a.init != "none" || a.cycle == "flex" || a.cycle == "none")
-      conv = mg.cycle(cyc(a.init), cyc(a.cycle), ResTol(-1.0), ResRat(a.resrat), mv, ms, &ncyc);
-    else if (a.cycle == "F") conv = mg.fcycle(ResRat(a.resrat), &ncyc);
-    else if (a.cycle == "W") conv = mg.wcycle(ResRat(a.resrat), &ncyc);
-    else conv = mg.vcycle(ResRat(a.resrat), &ncyc);
+#ifdef PBG_WITH_ENGINE
+    /* --gpu 2: the reference's AC replaced by the engine's GpuAC */
+    if (a.gpu == 2) {
+      pbg_psiboil::GpuAC mg(&pr, acsol, a.exact != 0);
+      conv = run_ac(mg, a, &ncyc);
+    } else
+#endif
+    {
+      AC mg(&pr, acsol);
+      conv = run_ac(mg, a, &ncyc);
+    }
     secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   } else {
     /* `repeat` timed solves from x0 = 0 (the first one's log is parsed) */

@@ -32,7 +32,7 @@ SOLVER_JACOBI, SOLVER_GAUSS_SEIDEL = 5, 6
 # pbg_result.status
 CONVERGED, MAXITER, STALE, BREAKDOWN, INITIAL, NAN, DIVERGED = 0, 1, 2, 3, 4, 5, 6
 FP64, MIXED = 0, 1
-CYCLE_NONE, CYCLE_V, CYCLE_F, CYCLE_W = -1, 1, 2, 4
+CYCLE_NONE, CYCLE_V, CYCLE_F, CYCLE_W, CYCLE_FLEX = -1, 1, 2, 4, 5
 STATUS = {0: "converged", 1: "maxiter", 2: "stale", 3: "breakdown", 4: "initial", 5: "nan",
           6: "diverged"}
 
@@ -62,7 +62,9 @@ class Params(ctypes.Structure):
                 ("tol", ctypes.c_double), ("inner_tol", ctypes.c_double),
                 ("max_sweeps", ctypes.c_int), ("exact_sums", ctypes.c_int),
                 ("coarse_max", ctypes.c_int), ("prec", ctypes.c_int), ("x0_zero", ctypes.c_int),
-                ("ac_smoother", ctypes.c_int)]
+                ("ac_smoother", ctypes.c_int), ("ac_solver", ctypes.c_int), ("ac_solver_prec", ctypes.c_int),
+                ("ac_resrat", ctypes.c_double), ("ac_restol", ctypes.c_double), ("use_linf", ctypes.c_int),
+                ("flex_visits", ctypes.c_int), ("ac_dt", ctypes.c_double)]
 
 
 class Result(ctypes.Structure):
@@ -580,13 +582,19 @@ class AC:
     SMOOTHERS = {"cg": SOLVER_CG, "bicgs": SOLVER_BICGS, "cgs": SOLVER_CGS, "jacobi": SOLVER_JACOBI,
                  "gs": SOLVER_GAUSS_SEIDEL}
 
-    def __init__(self, session, exact_sums=False, smoother="cg", prec="di"):
-        if smoother not in self.SMOOTHERS:
-            raise ValueError("smoother must be one of %s" % sorted(self.SMOOTHERS))
+    def __init__(self, session, exact_sums=False, smoother="cg", prec="di", solver=None, solver_prec="di"):
+        """solver: AC's own solver for post-smoothing and the coarsest level,
+        AC(cen, sol) (additive.cpp:8-48); None: the smoother."""
+        if smoother not in self.SMOOTHERS or (solver is not None and solver not in self.SMOOTHERS):
+            raise ValueError("smoother and solver must be one of %s" % sorted(self.SMOOTHERS))
         self.session = session
         self.exact_sums = exact_sums
         self.smoother = self.SMOOTHERS[smoother]
         self.prec = _Krylov.PREC[prec]
+        self.solver = -1 if solver is None else self.SMOOTHERS[solver]
+        self.solver_prec = _Krylov.PREC[solver_prec]
+        self._resrat, self._restol, self._linf = 1.0e-18, 1.0e-18, False
+        self.flex_visits = 1000000
         self._max_cyc, self._min_cyc = 20, 0
         self._stop_if_div, self._prio = True, True
         self.mv = [20, 20, 20]
@@ -620,6 +628,24 @@ class AC:
     def stale_iter_array(self, ms):
         self.ms = list(ms)
 
+    def resrat(self, rr=None):
+        """AC::resrat: the ResRat of the level solvers (default 1e-18)."""
+        if rr is None:
+            return self._resrat
+        self._resrat = float(rr)
+
+    def restol(self, rt=None):
+        """AC::restol: the ResTol of the level solvers (default 1e-18)."""
+        if rt is None:
+            return self._restol
+        self._restol = float(rt)
+
+    def use_linf_error(self, s=None):
+        """AC::use_linf_error: the cycle's tests on max |r/dV|."""
+        if s is None:
+            return self._linf
+        self._linf = bool(s)
+
     def cycle(self, x, b, init=CYCLE_NONE, loop=CYCLE_V, toler=-1.0, factor=-1.0, mv=None, ms=None):
         """AC::cycle(init, loop, ResTol, ResRat, mv, ms, &ncyc) -> (bool, ncyc)."""
         p = default_params(SOLVER_AC)
@@ -632,6 +658,9 @@ class AC:
             p.ms[q] = (ms or self.ms)[q]
         p.exact_sums = int(self.exact_sums)
         p.ac_smoother, p.prec = self.smoother, self.prec
+        p.ac_solver, p.ac_solver_prec = self.solver, self.solver_prec
+        p.ac_resrat, p.ac_restol, p.use_linf = self._resrat, self._restol, int(self._linf)
+        p.flex_visits = int(self.flex_visits)
         self.last = self.session.solve(x, b, p)
         return bool(self.last.converged), self.last.cycles
 
@@ -646,6 +675,10 @@ class AC:
 
     def fullcycle(self, x, b, loop=CYCLE_V, factor=-1.0, toler=-1.0):
         return self.cycle(x, b, CYCLE_V, loop, toler, factor)
+
+    def flexcycle(self, x, b, factor=-1.0, toler=-1.0):
+        """AC::flexcycle: ends when level 0's smoother reaches resrat()."""
+        return self.cycle(x, b, CYCLE_NONE, CYCLE_FLEX, toler, factor)
 
 
 class Engine:

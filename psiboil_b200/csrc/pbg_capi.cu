@@ -286,6 +286,11 @@ void pbg_params_default(pbg_params *p, int solver) {
   p->inner_tol = 1.0e-3;
   p->max_sweeps = 8;
   p->ac_smoother = PBG_SOLVER_CG;
+  p->ac_solver = -1;
+  p->ac_resrat = 1.0e-18;
+  p->ac_restol = 1.0e-18;
+  p->flex_visits = 1000000;
+  p->ac_dt = 1.0;
   if (solver == PBG_SOLVER_ENGINE) p->max_iter = 500;
 }
 
@@ -927,29 +932,48 @@ int solve_device(pbg_session *s, double *xd, const double *bd, const pbg_params 
     pa.max_cyc = p->max_cycles; pa.min_cyc = p->min_cycles;
     pa.stop_if_div = p->stop_if_div; pa.priority_min_cyc = p->priority_min_cyc;
     for (int q = 0; q < 3; ++q) { pa.mv[q] = p->mv[q]; pa.ms[q] = p->ms[q] > kStaleMax ? kStaleMax : p->ms[q]; }
-    pa.resrat_val = 1.0e-18;  // AC defaults (additive.cpp:17-18): atto
-    pa.restol_val = 1.0e-18;
+    pa.resrat_val = p->ac_resrat;  // AC::resrat / restol (additive.cpp:17-18 default atto)
+    pa.restol_val = p->ac_restol;
+    pa.use_linf = p->use_linf != 0;
+    s->refac->sm_scale = p->scale;
+    s->refac->res_dt = p->ac_dt;
+    pa.flex_visits = p->flex_visits > 0 ? p->flex_visits : 1000000;
+    auto cyc_ok = [](int c, bool none_ok) {
+      return c == PBG_CYCLE_V || c == PBG_CYCLE_F || c == PBG_CYCLE_W || c == PBG_CYCLE_FLEX ||
+             (none_ok && c == PBG_CYCLE_NONE);
+    };
+    if (!cyc_ok(p->loop_cycle, true) || !cyc_ok(p->init_cycle, true))
+      return fail(PBG_ERR_ARG, "cycles are PBG_CYCLE_NONE, V, F, W or FLEX");
     RefACCtx cx;
     cx.s = s->stream; cx.w = &s->rkw; cx.red = &s->red; cx.st = s->kst.p;
     cx.dscal = s->dscal.p; cx.dmean = s->dscal.p + 4; cx.hbuf = s->hbuf; cx.dlinf = s->dlinf.p;
     for (int q = 0; q < 3; ++q) { cx.mv[q] = pa.mv[q]; cx.ms[q] = pa.ms[q]; }
     cx.resrat_val = pa.resrat_val; cx.restol_val = pa.restol_val;
+    cx.hst = s->hkst;
     s->refac->seq = exact_terms(s, p);
+    auto kind_of = [](int sv) {
+      return sv == PBG_SOLVER_CG ? 0 : sv == PBG_SOLVER_BICGS ? 1 : sv == PBG_SOLVER_CGS ? 2
+             : sv == PBG_SOLVER_JACOBI ? 3 : sv == PBG_SOLVER_GAUSS_SEIDEL ? 4 : -1;
+    };
     const int sm = p->ac_smoother;
-    if (sm != PBG_SOLVER_CG && sm != PBG_SOLVER_BICGS && sm != PBG_SOLVER_CGS && sm != PBG_SOLVER_JACOBI &&
-        sm != PBG_SOLVER_GAUSS_SEIDEL)
+    if (kind_of(sm) < 0)
       return fail(PBG_ERR_ARG, "ac_smoother must be CG, BiCGS, CGS, Jacobi or Gauss-Seidel");
-    if (p->prec < 0 || p->prec > 3) return fail(PBG_ERR_ARG, "prec must be 0 (diagonal), 1 (IC0), 2 (IC2) or 3 (IC3)");
-    s->refac->sm_kind = sm == PBG_SOLVER_CG ? 0 : sm == PBG_SOLVER_BICGS ? 1 : sm == PBG_SOLVER_CGS ? 2
-                        : sm == PBG_SOLVER_JACOBI ? 3 : 4;
+    if (p->ac_solver != -1 && kind_of(p->ac_solver) < 0)
+      return fail(PBG_ERR_ARG, "ac_solver must be -1 (the smoother), CG, BiCGS, CGS, Jacobi or Gauss-Seidel");
+    if (p->prec < 0 || p->prec > 3 || p->ac_solver_prec < 0 || p->ac_solver_prec > 3)
+      return fail(PBG_ERR_ARG, "prec must be 0 (diagonal), 1 (IC0), 2 (IC2) or 3 (IC3)");
+    s->refac->sm_kind = kind_of(sm);
     s->refac->sm_prec = s->refac->sm_kind <= 2 ? p->prec : 0;
+    s->refac->sol_kind = p->ac_solver == -1 ? -1 : kind_of(p->ac_solver);
+    s->refac->sol_prec = s->refac->sol_kind >= 0 && s->refac->sol_kind <= 2 ? p->ac_solver_prec : 0;
     s->refac->sm_ci0 = s->ci_gen == s->mat_gen ? s->ci.p : nullptr;
-    s->hhist.assign(p->max_cycles + 2, 0.0);
+    s->hhist.assign(p->max_cycles + 3, 0.0);  // initial, cycle 0 (a full-cycle start), cycles
     RefACResult ar = s->refac->cycle(xd, bd, pa, cx, s->hhist.data(), (int)s->hhist.size());
     s->nhist = ar.nhist < (int)s->hhist.size() ? ar.nhist : (int)s->hhist.size();
     out.converged = ar.converged;
     out.cycles = ar.cycles;
     out.status = ar.converged ? PBG_CONVERGED : (ar.diverged ? PBG_DIVERGED : PBG_MAXITER);
+    out.iterations = ar.visits;  // flex cycles: smoother calls of the last one
     out.res0 = ar.res0;
     out.res = ar.res;
     out.levels = s->refac->nlevels();

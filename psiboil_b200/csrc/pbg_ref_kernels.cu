@@ -1391,21 +1391,38 @@ double RefAC::residual(RedPool &red, double *dscal, unsigned long long *dlinf, d
   PBG_CUDA(cudaMemcpyAsync(hbuf, dscal, sizeof(double), cudaMemcpyDeviceToHost, s));
   PBG_CUDA(cudaMemcpyAsync(hbuf + 1, dlinf, sizeof(double), cudaMemcpyDeviceToHost, s));
   PBG_CUDA(cudaStreamSynchronize(s));
-  if (linf) *linf = hbuf[1];
-  return hbuf[0];
+  // sqrt(dot_voldiv_avg) * dt and max_abs_voldiv * dt (additive_residual.cpp:19-27)
+  if (linf) *linf = hbuf[1] * res_dt;
+  return hbuf[0] * res_dt;
 }
 
+// call_smoother (the level's Linear) or, with as_solver, call_solver (AC's
+// own solver when one is set), additive_cycle_functions.cpp:90-107
 void RefAC::smooth(int l, int mi, double res_rat, double res_tol, int ms, RefKrylovWork &w,
-                   RedPool &red, KrylovState *st, cudaStream_t s) {
+                   RedPool &red, KrylovState *st, cudaStream_t s, bool as_solver) {
+  const bool own = as_solver && sol_kind >= 0;
+  const int kind = own ? sol_kind : sm_kind;
   KrylovParams pr;
   pr.mini = 1; pr.maxit = mi; pr.stalecount = ms;
-  pr.res_rat = res_rat; pr.res_tol = res_tol; pr.scale = 1.0; pr.dV = L[l].dV; pr.hist_cap = 0;
+  pr.res_rat = res_rat; pr.res_tol = res_tol; pr.scale = sm_scale; pr.dV = L[l].dV; pr.hist_cap = 0;
   pr.seq = seq;
-  pr.prec = sm_prec;
+  pr.prec = own ? sol_prec : sm_prec;
   pr.ci = l == 0 ? sm_ci0 : nullptr;  // coarse levels: ci = 1/c (additive_coarsen_system.cpp)
   MatView<double> A = view(l);
-  enqueue_ref_setup(A, L[l].phi.p, L[l].fnew.p, pr, sm_kind, w, red, st, s);
-  enqueue_ref_iters(A, L[l].phi.p, sm_kind, mi, w, red, st, nullptr, s, seq != nullptr, sm_prec);
+  enqueue_ref_setup(A, L[l].phi.p, L[l].fnew.p, pr, kind, w, red, st, s);
+  enqueue_ref_iters(A, L[l].phi.p, kind, mi, w, red, st, nullptr, s, seq != nullptr, pr.prec);
+}
+
+void RefAC::solve_l(int l, int mi, double res_rat, double res_tol, int ms, RefACCtx &cx) {
+  smooth(l, mi, res_rat, res_tol, ms, *cx.w, *cx.red, cx.st, cx.s, true);
+}
+
+// call_smoother's return value, the solver's converged flag (a host round trip)
+bool RefAC::smooth_converged(int l, int mi, double res_rat, double res_tol, int ms, RefACCtx &cx) {
+  smooth(l, mi, res_rat, res_tol, ms, *cx.w, *cx.red, cx.st, cx.s, false);
+  PBG_CUDA(cudaMemcpyAsync(cx.hst, cx.st, sizeof(KrylovState), cudaMemcpyDeviceToHost, cx.s));
+  PBG_CUDA(cudaStreamSynchronize(cx.s));
+  return cx.hst->converged != 0;
 }
 
 void RefAC::restrict_to(int l, RedPool &red, double *dmean, cudaStream_t s) {
@@ -1429,10 +1446,12 @@ void RefAC::interp_from(int l, cudaStream_t s) {
 
 
 // AC::cycle and its recursions (additive_cycle.cpp:4-99,
-// additive_cycle_functions.cpp:12-107, additive_recursive.cpp:4-158).
+// additive_cycle_functions.cpp:12-107, additive_recursive.cpp:4-197).
 void RefAC::run(int kind, int l, RefACCtx &cx) {
   if (kind == 1) v_cycle(l, cx);
   else if (kind == 2 || kind == 4) fw_cycle(l, cx, kind == 4);
+  else if (kind == 5) flex_cycle(l, cx);
+  else throw CudaError("AC: unknown cycle kind");
 }
 
 void RefAC::v_cycle(int l, RefACCtx &cx) {
@@ -1441,10 +1460,10 @@ void RefAC::v_cycle(int l, RefACCtx &cx) {
     smooth(l, cx.mv[0], cx.resrat_val, cx.restol_val, cx.ms[0], *cx.w, *cx.red, cx.st, cx.s);
     restrict_to(l, *cx.red, cx.dmean, cx.s);
     v_cycle(l + 1, cx);
-    smooth(l, cx.mv[2], cx.resrat_val, cx.restol_val, cx.ms[2], *cx.w, *cx.red, cx.st, cx.s);
+    solve_l(l, cx.mv[2], cx.resrat_val, cx.restol_val, cx.ms[2], cx);
     if (l > 0) interp_from(l, cx.s);
   } else {
-    smooth(l, 100, -1.0, cx.restol_val, -1, *cx.w, *cx.red, cx.st, cx.s);
+    solve_l(l, 100, -1.0, cx.restol_val, -1, cx);
     if (l > 0) interp_from(l, cx.s);
   }
 }
@@ -1459,11 +1478,49 @@ void RefAC::fw_cycle(int l, RefACCtx &cx, bool w) {
     restrict_to(l, *cx.red, cx.dmean, cx.s);
     if (w) fw_cycle(l + 1, cx, w);
     else v_cycle(l + 1, cx);
-    smooth(l, cx.mv[2], cx.resrat_val, cx.restol_val, cx.ms[2], *cx.w, *cx.red, cx.st, cx.s);
+    solve_l(l, cx.mv[2], cx.resrat_val, cx.restol_val, cx.ms[2], cx);
     if (l > 0) interp_from(l, cx.s);
   } else {
-    smooth(l, 100, -1.0, cx.restol_val, -1, *cx.w, *cx.red, cx.st, cx.s);
+    solve_l(l, 100, -1.0, cx.restol_val, -1, cx);
     if (l > 0) interp_from(l, cx.s);
+  }
+}
+
+// AC::flex_cycle (additive_recursive.cpp:161-197). The reference recurses
+// on (level, sign) in tail position; here the same walk is a loop. A level
+// whose smoother converges (to AC::resrat) hands its correction up and the
+// finer level smooths with mv[2], ms[2] (Sign::pos); one that does not
+// restricts down, where the next level smooths with mv[0], ms[0]
+// (Sign::neg); the coarsest level is solved and interpolated up with
+// Sign::neg. It starts at level l and ends when level 0's smoother
+// converges. That needs the smoother's converged flag on the host: one
+// round trip per smoother call. The reference never returns when level 0
+// never converges; here the walk stops after cx.flex_visits smoother calls.
+void RefAC::flex_cycle(int l, RefACCtx &cx) {
+  const int last = (int)L.size() - 1;
+  bool pos = false;
+  flex_calls_ = 0;
+  for (;;) {
+    if (l != last) {
+      const int idx = pos ? 2 : 0;
+      if (++flex_calls_ > cx.flex_visits) { flex_capped_ = true; return; }
+      if (smooth_converged(l, cx.mv[idx], cx.resrat_val, cx.restol_val, cx.ms[idx], cx)) {
+        if (l == 0) return;
+        interp_from(l, cx.s);
+        l -= 1;
+        pos = true;
+      } else {
+        restrict_to(l, *cx.red, cx.dmean, cx.s);
+        l += 1;
+        pos = false;
+      }
+    } else {
+      solve_l(l, 100, -1.0, cx.restol_val, -1, cx);
+      if (l == 0) return;
+      interp_from(l, cx.s);
+      l -= 1;
+      pos = false;
+    }
   }
 }
 
@@ -1472,9 +1529,10 @@ void RefAC::full_cycle(int l, int kind, RefACCtx &cx) {
   if (l != last) {
     restrict_to(l, *cx.red, cx.dmean, cx.s);
     full_cycle(l + 1, kind, cx);
-    run(kind, l, cx);
+    if (kind == 1 || kind == 2 || kind == 4 || kind == 5) run(kind, l, cx);
+    else solve_l(l, 100, -1.0, cx.restol_val, -1, cx);  // the reference's "shouldn't happen" branch
   } else {
-    smooth(l, 100, -1.0, cx.restol_val, -1, *cx.w, *cx.red, cx.st, cx.s);
+    solve_l(l, 100, -1.0, cx.restol_val, -1, cx);
     if (l > 0) interp_from(l, cx.s);
   }
 }
@@ -1484,18 +1542,30 @@ RefACResult RefAC::cycle(double *x, const double *b, const RefACParams &pa, RefA
   RefACLevel &l0 = L[0];
   const long long N0 = A0v.ncell();
   cudaStream_t s = cx.s;
+  cx.flex_visits = pa.flex_visits;
+  flex_capped_ = false;
+  flex_calls_ = 0;
   PBG_CUDA(cudaMemcpyAsync(l0.phi.p, x, sizeof(double) * N0, cudaMemcpyDeviceToDevice, s));
   PBG_CUDA(cudaMemcpyAsync(l0.fnew.p, b, sizeof(double) * N0, cudaMemcpyDeviceToDevice, s));
   coarsen_all(s);  // rebuilt on every call (additive_cycle_functions.cpp:25-26)
   RefACResult out{};
   int nh = 0;
-  double linf0;
-  double res_0 = residual(*cx.red, cx.dscal, cx.dlinf, cx.hbuf, s, &linf0);
-  if (res_hist && nh < hist_cap) res_hist[nh] = res_0;
-  nh++;
+  auto record = [&](double r) {
+    if (res_hist && nh < hist_cap) res_hist[nh] = r;
+    nh++;
+  };
+  auto restore = [&]() {
+    PBG_CUDA(cudaMemcpyAsync(l0.phi.p, fold.p, sizeof(double) * N0, cudaMemcpyDeviceToDevice, s));
+  };
+  // init_cycles (additive_cycle_functions.cpp:12-44); with use_linf the
+  // tests read max |r/dV| (additive_cycle_functions.cpp:58-60)
+  double linf_0;
+  const double res_0 = residual(*cx.red, cx.dscal, cx.dlinf, cx.hbuf, s, &linf_0);
+  record(res_0);
   PBG_CUDA(cudaMemcpyAsync(fold.p, l0.phi.p, sizeof(double) * N0, cudaMemcpyDeviceToDevice, s));
   out.res0 = res_0;
-  if ((res_0 < pa.toler && pa.min_cyc == 0) || res_0 == 0.0) {
+  const double res_0_control = pa.use_linf ? linf_0 : res_0;
+  if ((res_0_control < pa.toler && pa.min_cyc == 0) || res_0 == 0.0) {
     out.converged = 1; out.cycles = 0; out.res = res_0;
   } else {
     for (size_t l = 1; l < L.size(); ++l) {
@@ -1503,25 +1573,58 @@ RefACResult RefAC::cycle(double *x, const double *b, const RefACParams &pa, RefA
       PBG_CUDA(cudaMemsetAsync(L[l].phi.p, 0, sizeof(double) * n, s));
       PBG_CUDA(cudaMemsetAsync(L[l].fnew.p, 0, sizeof(double) * n, s));
     }
-    if (pa.init != -1) full_cycle(0, pa.init, cx);
-    double res_m1 = residual(*cx.red, cx.dscal, cx.dlinf, cx.hbuf, s, nullptr);
+    double linf_m1 = 0.0;
+    double res_m1;
+    if (pa.init != -1) {
+      full_cycle(0, pa.init, cx);
+      res_m1 = residual(*cx.red, cx.dscal, cx.dlinf, cx.hbuf, s, &linf_m1);
+      record(res_m1);  // the reference logs it as cycle 0
+      // converged(..., cycle 0, ...) (additive_cycle.cpp:39-43): its return
+      // value is dropped, but its divergence branch compares the residual
+      // with itself, so unless cycle 0 meets the tolerance stop_if_div
+      // restores phi = fold, the initial guess
+      const double rc = pa.use_linf ? linf_m1 : res_m1;
+      const double rb = pa.use_linf ? linf_0 : res_0;
+      if (!(0 >= pa.min_cyc && (rc / rb < pa.factor || rc < pa.toler))) {
+        bool check = pa.stop_if_div != 0;
+        if (pa.priority_min_cyc && 0 < pa.min_cyc) check = false;
+        if (check) restore();
+      }
+    } else {
+      res_m1 = residual(*cx.red, cx.dscal, cx.dlinf, cx.hbuf, s, &linf_m1);
+    }
     out.cycles = pa.max_cyc;
     out.converged = 0;
     out.res = res_m1;
     for (int c = 1; c <= pa.max_cyc; ++c) {
+      if (pa.loop != 1 && pa.loop != 2 && pa.loop != 4 && pa.loop != 5) {
+        // just solve (additive_cycle.cpp:66-71): AC's solver on level 0
+        solve_l(0, 40, 0.001, 1.0e-15, -1, cx);
+        out.res = residual(*cx.red, cx.dscal, cx.dlinf, cx.hbuf, s, nullptr);
+        break;
+      }
       run(pa.loop, 0, cx);
-      double res1 = residual(*cx.red, cx.dscal, cx.dlinf, cx.hbuf, s, nullptr);
-      if (res_hist && nh < hist_cap) res_hist[nh] = res1;
-      nh++;
+      if (flex_capped_) {  // the flex walk hit its bound: stop, not converged
+        out.res = residual(*cx.red, cx.dscal, cx.dlinf, cx.hbuf, s, nullptr);
+        out.cycles = c;
+        out.flex_capped = 1;
+        break;
+      }
+      double linf1;
+      const double res1 = residual(*cx.red, cx.dscal, cx.dlinf, cx.hbuf, s, &linf1);
+      record(res1);
       out.res = res1;
+      const double rc = pa.use_linf ? linf1 : res1;
+      const double r0 = pa.use_linf ? linf_m1 : res_m1;   // linf_m1 is never refreshed (:78)
+      const double rb = pa.use_linf ? linf_0 : res_0;
       int con;
-      if (c >= pa.min_cyc && (res1 / res_0 < pa.factor || res1 < pa.toler)) {
+      if (c >= pa.min_cyc && (rc / rb < pa.factor || rc < pa.toler)) {
         con = 0;
       } else {
         bool check = pa.stop_if_div != 0;
         if (pa.priority_min_cyc && c < pa.min_cyc) check = false;
-        if (check && res1 >= res_m1) {
-          PBG_CUDA(cudaMemcpyAsync(l0.phi.p, fold.p, sizeof(double) * N0, cudaMemcpyDeviceToDevice, s));
+        if (check && rc >= r0) {
+          restore();
           con = 1;
         } else {
           con = 2;
@@ -1536,6 +1639,7 @@ RefACResult RefAC::cycle(double *x, const double *b, const RefACParams &pa, RefA
   PBG_CUDA(cudaMemcpyAsync(x, l0.phi.p, sizeof(double) * N0, cudaMemcpyDeviceToDevice, s));
   PBG_CUDA(cudaStreamSynchronize(s));
   out.nhist = nh;
+  out.visits = (int)flex_calls_;
   return out;
 }
 

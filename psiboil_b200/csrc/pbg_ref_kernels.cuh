@@ -72,16 +72,20 @@ struct RefACLevel {
 };
 
 struct RefACParams {
-  int init, loop;          // -1 none, 1 V, 2 F, 4 W
+  int init, loop;          // -1 none, 1 V, 2 F, 4 W, 5 flex (loop -1: "just solve")
   double toler, factor;
   int max_cyc, min_cyc, stop_if_div, priority_min_cyc;
   int mv[3], ms[3];
   double resrat_val, restol_val;
+  bool use_linf = false;
+  long long flex_visits = 1000000;
 };
 
 struct RefACResult {
   int converged, cycles, diverged, nhist;
   double res0, res;
+  int visits;              // smoother calls of the last flex cycle
+  int flex_capped;         // a flex cycle stopped at its visit bound
 };
 
 struct RefACCtx {
@@ -89,6 +93,8 @@ struct RefACCtx {
   RefKrylovWork *w;
   RedPool *red;
   KrylovState *st;
+  KrylovState *hst = nullptr;   // pinned host copy of st (flex: the smoother's converged flag)
+  long long flex_visits = 1000000;
   double *dscal, *dmean, *hbuf;
   unsigned long long *dlinf;
   int mv[3], ms[3];
@@ -105,6 +111,11 @@ class RefAC {
   // of the drivers above, its Prec code, and level 0's stored ci (or null)
   int sm_kind = 0, sm_prec = 0;
   const double *sm_ci0 = nullptr;
+  // AC's own solver for call_solver (post-smoothing, coarsest level):
+  // sol_kind -1 = the levels' smoother
+  int sol_kind = -1, sol_prec = 0;
+  // the level solvers' scale (dti * scale) and the dt of AC's residual measure
+  double sm_scale = 1.0, res_dt = 1.0;
 
   void build(const MatView<double> &A0, const uint8_t *aflag0, double h, cudaStream_t s);
   MatView<double> view(int l) const;
@@ -117,13 +128,18 @@ class RefAC {
   double residual(RedPool &red, double *dscal, unsigned long long *dlinf, double *hbuf,
                   cudaStream_t s, double *linf);
   void smooth(int l, int mi, double res_rat, double res_tol, int ms, RefKrylovWork &w,
-              RedPool &red, KrylovState *st, cudaStream_t s);
+              RedPool &red, KrylovState *st, cudaStream_t s, bool as_solver = false);
+  void solve_l(int l, int mi, double res_rat, double res_tol, int ms, RefACCtx &cx);
+  bool smooth_converged(int l, int mi, double res_rat, double res_tol, int ms, RefACCtx &cx);
   void restrict_to(int l, RedPool &red, double *dmean, cudaStream_t s);
   void interp_from(int l, cudaStream_t s);
   void run(int kind, int l, RefACCtx &cx);
   void v_cycle(int l, RefACCtx &cx);
   void fw_cycle(int l, RefACCtx &cx, bool w);
+  void flex_cycle(int l, RefACCtx &cx);
   void full_cycle(int l, int kind, RefACCtx &cx);
+  long long flex_calls_ = 0;
+  bool flex_capped_ = false;
 };
 
 }  // namespace pbg

@@ -20,6 +20,9 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import oracle_py as O  # noqa: E402
 
+sys.path.insert(0, os.path.dirname(HERE))
+from golden_util import ACX_RUNS  # noqa: E402
+
 CASES = [
     # name, kind, problem kwargs, runs
     ("single16", O.KIND_SINGLE, dict(n=16), ["cg", "bicgs", "ac", "cg_ic0", "cg_ic2", "cg_ic3", "cgs",
@@ -39,6 +42,9 @@ CASES = [
     ("per12", O.KIND_CYL, dict(n=12, nb=2, rmin=1.5, rmax=2.5, rc=3.0, periodic=3),
      ["cg", "bicgs", "ac", "jacobi", "gs", "cg_ic2", "acsm_gs", "ac_w"]),
     ("per16", O.KIND_SINGLE, dict(n=16, periodic=1), ["cg", "cgs", "ac", "gs", "acsm_jacobi"]),
+    # the rest of AC's surface: flex cycle, "just solve", use_linf_error, a
+    # full-cycle start, AC's own solver, min_cycles (golden_util.ACX_RUNS)
+    ("acx12", O.KIND_SINGLE, dict(n=12), ["cg"] + sorted(ACX_RUNS)),
 ]
 
 # Jacobi and Gauss-Seidel converge slowly on these density jumps: a looser
@@ -116,6 +122,8 @@ def main():
         for run in runs:
             solver = "ac" if run.startswith("ac") else run.split("_")[0]
             extra = {}
+            if run in ACX_RUNS:
+                extra = dict(ACX_RUNS[run][0])
             if "_ic" in run:
                 extra = dict(prec=run.split("_")[1])
             if run == "ac_w":

@@ -107,3 +107,41 @@ def test_reference_with_gpu_stationary_is_bit_exact(case, args, solver):
                           "--gpu", "1", "--exact", "1"])
     assert np.array_equal(x, g[solver + "_x"])
     assert int(meta["iterations"][0]) == int(g[solver + "_iterations"])
+
+
+def _hist(meta):
+    return np.array([float(meta["res0"][0])] + [float(v) for v in meta.get("cycle_res", [])])
+
+
+GPUAC_CASES = [
+    # golden fixture, harness problem args, harness AC args, golden run key
+    ("single16", ["--kind", "single", "--n", "16"], [], "ac"),
+    ("single12", ["--kind", "single", "--n", "12"], ["--cycle", "W"], "ac_w"),
+    ("single12", ["--kind", "single", "--n", "12"], ["--guard", "0", "--maxcyc", "6"], "ac_noguard"),
+    ("single12", ["--kind", "single", "--n", "12"], ["--acsm", "gs"], "acsm_gs"),
+    ("cyl24", ["--kind", "cyl", "--n", "24", "--nb", "3", "--rmin", "2.0", "--rmax", "4.0", "--rc", "5.0"],
+     [], "ac"),
+    ("per12", ["--kind", "cyl", "--n", "12", "--nb", "2", "--rmin", "1.5", "--rmax", "2.5", "--rc", "3.0",
+               "--periodic", "3"], [], "ac"),
+    ("acx12", ["--kind", "single", "--n", "12"], ["--cycle", "flex", "--acresrat", "0.1"], "acx_flex"),
+    ("acx12", ["--kind", "single", "--n", "12"], ["--cycle", "none"], "acx_solve"),
+    ("acx12", ["--kind", "single", "--n", "12"], ["--linf", "1"], "acx_linf"),
+    ("acx12", ["--kind", "single", "--n", "12"], ["--init", "V"], "acx_fullv"),
+    ("acx12", ["--kind", "single", "--n", "12"], ["--acsolver", "bicgs"], "acx_solbicgs"),
+]
+
+
+@pytest.mark.skipif(not os.path.exists(EXE), reason="GPU-backed reference harness not built")
+@pytest.mark.parametrize("case,args,acargs,key", GPUAC_CASES, ids=[c[0] + "-" + c[3] for c in GPUAC_CASES])
+def test_reference_with_gpu_ac_is_bit_exact(case, args, acargs, key):
+    """`pbg_psiboil::GpuAC multigrid(&pr)` in place of `AC multigrid(&pr)`
+    (--gpu 2): the whole cycle on the GPU behind AC's own interface. With
+    exact sums the cycle count, the residual history the harness parses from
+    the log lines and the iterate are the CPU reference's, bit for bit."""
+    g = load(case)
+    x, meta = run(args + ["--seed", "7", "--solver", "ac", "--resrat", "1e-8", "--gpu", "2",
+                          "--exact", "1"] + acargs)
+    assert int(meta["cycles"][0]) == int(g[key + "_cycles"])
+    assert int(meta["converged"][0]) == int(g[key + "_converged"])
+    np.testing.assert_allclose(_hist(meta), g[key + "_hist"], rtol=1e-13)
+    assert np.array_equal(x, g[key + "_x"])

@@ -18,7 +18,7 @@ reduction modes:
 import numpy as np
 import pytest
 
-from golden_util import NAMES, bc_of, load, problem_of
+from golden_util import ACX_RUNS, NAMES, bc_of, load, problem_of
 
 pytestmark = pytest.mark.gpu
 RTOL_X = 1e-10
@@ -254,3 +254,39 @@ def test_periodic_couplings_need_a_periodic_session(engine, oracle):
         with pytest.raises(engine.PbgError) as e:
             engine.Engine(s).solve(np.zeros(P.N), P.b.copy(), tol=1e-8)
         assert e.value.code == engine.ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("run", sorted(ACX_RUNS))
+def test_ac_extended_parity(engine, oracle, run):
+    """The rest of AC's surface against the reference run that way (fixture
+    acx12): flex cycle (AC::resrat 0.1), the "just solve" branch,
+    use_linf_error, a full-cycle start (whose divergence check restores the
+    initial guess, as the reference's does), AC's own solver, min_cycles.
+    Exact sums: cycles, history and iterate bit for bit."""
+    g = load("acx12")
+    P = problem_of(g, oracle)
+    _, ac_kw, cyc_kw = ACX_RUNS[run]
+    x = np.zeros(P.N)
+    with session_for(engine, P) as s:
+        s.upload_ci(g["ci"])
+        ac = engine.AC(s, exact_sums=True, solver=ac_kw.get("solver"))
+        if "resrat" in ac_kw:
+            ac.resrat(ac_kw["resrat"])
+        ac.use_linf_error(ac_kw.get("use_linf", False))
+        ac.min_cycles(cyc_kw.get("min_cyc", 0))
+        ok, ncyc = ac.cycle(x, P.b.copy(), init=cyc_kw.get("init", engine.CYCLE_NONE),
+                            loop=cyc_kw["loop"], factor=1e-8)
+        hist = s.history()
+    assert ok == bool(g[run + "_converged"])
+    assert ncyc == int(g[run + "_cycles"])
+    np.testing.assert_allclose(hist, g[run + "_hist"], rtol=1e-13)
+    assert np.array_equal(x, g[run + "_x"])
+
+
+def test_ac_rejects_unknown_cycles(engine, oracle):
+    P = problem_of(load("acx12"), oracle)
+    with session_for(engine, P) as s:
+        for loop in (0, 3, 6):
+            with pytest.raises(engine.PbgError) as e:
+                engine.AC(s).cycle(np.zeros(P.N), P.b.copy(), loop=loop, factor=1e-8)
+            assert e.value.code == engine.ERR_ARG

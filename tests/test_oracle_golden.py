@@ -3,7 +3,7 @@ by tests/golden/make_golden.py from the compiled reference)."""
 import numpy as np
 import pytest
 
-from golden_util import NAMES, load, problem_of
+from golden_util import ACX_RUNS, NAMES, load, problem_of
 
 
 @pytest.mark.parametrize("name", NAMES)
@@ -96,3 +96,19 @@ def test_mt64_matches_standard_engine(oracle):
     exe = os.path.join(d, "t")
     subprocess.check_call(["gcc", "-std=c99", "-I", oracle.PROBLEM_GEN_DIR, c, "-o", exe, "-lm"])
     assert subprocess.check_output([exe]).strip() == b"9981545732273789042"
+
+
+@pytest.mark.parametrize("run", sorted(ACX_RUNS))
+def test_ac_extended_bit_exact(oracle, run):
+    """Flex cycle, "just solve", use_linf_error, a full-cycle start, AC's own
+    solver and min_cycles, each against the reference run that way."""
+    g = load("acx12")
+    P = problem_of(g, oracle)
+    _, ac_kw, cyc_kw = ACX_RUNS[run]
+    ac = oracle.AC(P, **ac_kw)
+    x, st = ac.cycle(factor=1e-8, **cyc_kw)
+    assert not ac.flex_capped
+    assert st["cycles"] == int(g[run + "_cycles"])
+    assert st["converged"] == int(g[run + "_converged"])
+    np.testing.assert_allclose(st["hist"], g[run + "_hist"], rtol=1e-13)
+    assert np.array_equal(x, g[run + "_x"])
