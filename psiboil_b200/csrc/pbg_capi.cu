@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -73,6 +74,17 @@ Geo flow_geo(const pbg_session *s) {
     return g;
   }
   return Geo(s->nx, s->ny, s->nz);
+}
+
+// The row-vector flow kernels (4 cells of a k-row per thread) take grids
+// with nz % 4 == 0 below 2^31 cells and no cut body; PBG_FLOW_SCALAR=1
+// selects the one-cell kernels (the same bits).
+bool flow_vec(const pbg_session *s, bool cut) {
+  static const bool scalar = [] {
+    const char *e = std::getenv("PBG_FLOW_SCALAR");
+    return e && e[0] == '1';
+  }();
+  return !scalar && !cut && s->nz % kFlowV == 0 && s->ncell() < (1ll << 31);
 }
 
 int fail(int code, const std::string &m) {
@@ -643,10 +655,16 @@ int pbg_assemble_mix(pbg_session *s, const double *col, double rho_a, double rho
     if (A.c.n != (size_t)N) { A.c.alloc(N); A.w.alloc(N); A.s.alloc(N); A.b.alloc(N); }
     if (sym) { A.e.release(); A.n.release(); A.t.release(); }
     else if (A.e.n != (size_t)N) { A.e.alloc(N); A.n.alloc(N); A.t.alloc(N); }
-    k_assemble_mix<<<grid_for(N), kThreads, 0, s->stream>>>(
-        flow_geo(s), s->nx, s->ny, s->nz, s->h, make_int4(s->bc[0], s->bc[1], s->bc[2], s->bc[3]),
-        make_int2(s->bc[4], s->bc[5]), cp, rho_a, rho_b, bd.off, bd.idx, bd.fs, A.c.p, A.w.p, A.s.p, A.b.p,
-        A.e.p, A.n.p, A.t.p, s->aflag.p);
+    if (flow_vec(s, bd.idx != nullptr)) {
+      kv_assemble_mix<<<grid_for(N / kFlowV), kThreads, 0, s->stream>>>(
+          flow_geo(s), s->nx, s->ny, s->nz, s->h, make_int4(s->bc[0], s->bc[1], s->bc[2], s->bc[3]),
+          make_int2(s->bc[4], s->bc[5]), cp, rho_a, rho_b, bd.off, A.c.p, A.w.p, A.s.p, A.b.p, s->aflag.p);
+    } else {
+      k_assemble_mix<<<grid_for(N), kThreads, 0, s->stream>>>(
+          flow_geo(s), s->nx, s->ny, s->nz, s->h, make_int4(s->bc[0], s->bc[1], s->bc[2], s->bc[3]),
+          make_int2(s->bc[4], s->bc[5]), cp, rho_a, rho_b, bd.off, bd.idx, bd.fs, A.c.p, A.w.p, A.s.p, A.b.p,
+          A.e.p, A.n.p, A.t.p, s->aflag.p);
+    }
     note_launch();
     PBG_CUDA(cudaGetLastError());
     PBG_CUDA(cudaStreamSynchronize(s->stream));
@@ -729,8 +747,12 @@ int pbg_divergence(pbg_session *s, const double *u, const double *v, const doubl
     if (int rc = body_args(s, sp, bd)) return rc;
     const double dti = 1.0 / dt;
     const double a = (s->h * s->h) * dti;
-    k_divergence<<<grid_for(N), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, a, fa.d[0], fa.d[1],
-                                                          fa.d[2], bd.off, bd.idx, bd.fs, r);
+    if (flow_vec(s, bd.idx != nullptr))
+      kv_divergence<<<grid_for(N / kFlowV), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, a,
+                                                                      fa.d[0], fa.d[1], fa.d[2], bd.off, r);
+    else
+      k_divergence<<<grid_for(N), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, a, fa.d[0], fa.d[1],
+                                                            fa.d[2], bd.off, bd.idx, bd.fs, r);
     note_launch();
     PBG_CUDA(cudaGetLastError());
     if (where == PBG_HOST) PBG_CUDA(cudaMemcpyAsync(rhs, r, N * 8, cudaMemcpyDeviceToHost, s->stream));
@@ -772,8 +794,13 @@ int pbg_project(pbg_session *s, const double *p, const double *col, double rho_a
     }
     BodyArgs bd;
     if (int rc = body_args(s, sp, bd)) return rc;
-    k_project<<<grid_for(N), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, s->h, dt, pp, cp, rho_a,
-                                                       rho_b, bd.off, fa.d[0], fa.d[1], fa.d[2]);
+    if (flow_vec(s, false))
+      kv_project<<<grid_for(N / kFlowV), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, s->h, dt, pp,
+                                                                   cp, rho_a, rho_b, bd.off, fa.d[0], fa.d[1],
+                                                                   fa.d[2]);
+    else
+      k_project<<<grid_for(N), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, s->h, dt, pp, cp, rho_a,
+                                                         rho_b, bd.off, fa.d[0], fa.d[1], fa.d[2]);
     note_launch();
     PBG_CUDA(cudaGetLastError());
     fa.out(s, f, where);

@@ -1,7 +1,8 @@
 """The engine's fast solver (flexible CG + AC K-cycle) in FP64 and mixed
 precision. Checked with the oracle: the FP64 true residual |b - A x| / |b|
 <= 1e-8 (recomputed on the CPU), and the error against the tight oracle
-solution (CG to 1e-13) stays within what the residual bound allows."""
+solution (CG to 1e-13) within 10x the error the reference's own CG leaves
+when it stops at the same 1e-8 (the oracle's CG to ResRat 1e-8)."""
 import numpy as np
 import pytest
 
@@ -30,9 +31,16 @@ def test_engine_reaches_1e8(engine, oracle, kind, kw, precision):
     rel = true_relres(oracle, P, x)
     assert rel <= 1e-8 * 1.0001, rel
     assert abs(rel - r.relres) <= 1e-3 * rel + 1e-13  # roundoff floor of a direct solve
+    # the error against the tight solution is bounded by what the reference's
+    # own CG leaves at the same tolerance (its answer at ResRat 1e-8): both
+    # stop at a residual of 1e-8 |b|, so their errors are A^-1 of residuals of
+    # that size; the engine's may differ in direction, not in scale
     xt, _ = oracle.cg(P, res_rat=1e-13, maxit=100000)
-    err = np.linalg.norm(x - xt) / np.linalg.norm(xt)
-    assert err < 1e-4, err
+    xr, _ = oracle.cg(P, res_rat=1e-8, maxit=100000)
+    nt = np.linalg.norm(xt)
+    err = np.linalg.norm(x - xt) / nt
+    err_ref = np.linalg.norm(xr - xt) / nt
+    assert err <= 10.0 * err_ref, (err, err_ref)
     if precision == 1:
         assert r.sweeps >= 2
 

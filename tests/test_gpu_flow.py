@@ -4,8 +4,8 @@ pbg_divergence, pbg_project, pbg_pressure_step) against the oracle
 (tests/golden/step*.npz).
 
 Tolerances: assembly, divergence and projection are bit-exact against the
-oracle on every grid (one thread per cell, the reference's operation
-order). The whole step with the reference-parity CG (exact_sums) is
+oracle on every grid (the reference's operation order, whether a thread
+owns one cell or four cells of a k-row). The whole step with the reference-parity CG (exact_sums) is
 bit-exact against the reference on grids whose n is a power of two; for
 other n the reference's own grid spacings carry rounding, and the step
 agrees to 1e-11 relative. The engine's step is held to the divergence it
@@ -22,7 +22,9 @@ from golden_util import GOLDEN, problem_of
 pytestmark = pytest.mark.gpu
 
 CASES = [(0, dict(n=16)), (0, dict(n=12)), (1, dict(n=20, nb=3, rmin=2.0, rmax=3.0, rc=4.0)),
-         (2, dict(index=0, n2d=1, s2=(32, 32))), (2, dict(index=3, n2d=1, s2=(20, 40)))]
+         (2, dict(index=0, n2d=1, s2=(32, 32))), (2, dict(index=3, n2d=1, s2=(20, 40))),
+         # nz % 4 == 0 grids run the row-vector kernels, others the one-cell ones
+         (1, dict(n=28, nb=4, rmin=2.0, rmax=4.0, rc=6.0)), (0, dict(n=13))]
 
 
 def _state(oracle, kind, kw, seed=5):
