@@ -113,9 +113,10 @@ typedef struct {
   double tol;             /* target |b - A x| / |b| (FP64 true residual)        */
   double inner_tol;       /* mixed: FP32 inner solve reduction per sweep         */
   int max_sweeps;         /* mixed: refinement sweeps at most                    */
-  /* reference-parity solvers: 1 = add every global sum in the reference's
-   * sequential i,j,k order (bit-for-bit reference results, one thread per
-   * cell and a serial sum per dot product); 0 = deterministic tree sums */
+  /* reference-parity solvers: 1 = every global sum rounded as the
+   * reference's sequential i,j,k loop rounds it (bit-for-bit reference
+   * results; computed in parallel, see pbg_seq_sum, about 15x the time of
+   * a tree sum); 0 = deterministic tree sums */
   int exact_sums;
   /* engine: cells of the dense coarsest level (0: 512). Larger (4096) saves
    * launches in repeated solves with one matrix and costs a longer set-up
