@@ -20,15 +20,17 @@
 //   2. an approximate prefix of all earlier terms comes from a decoupled
 //      look-back over the chunks' published sums (bounded polling: a block
 //      that gives up only loses its hint);
-//   3. for the three exponents around the hint, e0..e0+2, the block computes
-//      K = sum of rint(a/u) and the minimum and maximum of its running
-//      integer prefix, and whether every term was tie-free and finite;
+//   3. for the three exponents around the hint, e0..e0+2, each warp computes
+//      K = sum of rint(a/u) over its 32 terms, the minimum and maximum of its
+//      running integer prefix, and whether every term was tie-free and
+//      finite; the chunk's record composes its warps' records;
 //   4. the last chunk of each group of kExactGroup chunks to arrive composes
 //      the group's records for the exponents of the group's last chunk;
 //   5. the last block of the launch walks the groups in order with the exact
-//      running sum: a group (or chunk) whose record holds the current
-//      exponent and keeps s/u + prefix inside [2^52 + 1, 2^53 - 1] is
-//      applied as s += u K; anything else is added term by term.
+//      running sum (one warp per sum): a group, chunk or warp record that
+//      holds the current exponent and keeps s/u + prefix inside
+//      [2^52 + 1, 2^53 - 1] is applied as s += u K; a warp segment whose
+//      record does not is added term by term.
 // Every step of the walk is either the sequential rounding itself or an
 // integer sum proven equal to it, so the result is the sequential sum bit
 // for bit whatever the hints were; bad hints only cost time.
@@ -40,6 +42,7 @@
 namespace pbg {
 
 constexpr int kExactChunkThreads = 256;  // terms per chunk (the reducing block)
+constexpr int kExactWarps = kExactChunkThreads / 32;  // warp records per chunk
 constexpr int kExactGroup = 64;          // chunks per group record
 constexpr int kExactVals = 2;            // sums per reducing kernel at most
 constexpr int kExactPoll = 4096;         // look-back polls before a block gives up its hint
@@ -53,6 +56,7 @@ struct ExactRec {
 
 // Header stored kExactHdrBytes before the terms (the `seq` pointer).
 struct ExactHdr {
+  ExactRec *wrec;      // [kExactVals][cap_chunks][kExactWarps] (32 terms each)
   ExactRec *crec;      // [kExactVals][cap_chunks]
   ExactRec *grec;      // [kExactVals][cap_groups]
   double *agg;         // [kExactVals][cap_chunks] chunk sums (hints)
@@ -72,7 +76,7 @@ inline size_t exact_scratch_doubles(long long ncell) {
   const long long ch = (ncell + kExactChunkThreads - 1) / kExactChunkThreads + 1;
   const long long gr = (ch + kExactGroup - 1) / kExactGroup + 1;
   size_t bytes = kExactHdrBytes + sizeof(double) * (size_t)kExactVals * ncell;
-  bytes += sizeof(ExactRec) * kExactVals * (size_t)(ch + gr);
+  bytes += sizeof(ExactRec) * kExactVals * (size_t)(ch * (kExactWarps + 1) + gr);
   bytes += sizeof(double) * 2 * kExactVals * (size_t)ch;
   bytes += sizeof(unsigned) * (size_t)(ch + gr) + 1024;
   return (bytes + 7) / 8;
@@ -121,65 +125,111 @@ __device__ __forceinline__ bool exact_apply(double &s, const ExactRec &R) {
   return true;
 }
 
-// Block-wide inclusive scan of three 64-bit integers (kExactChunkThreads
-// threads); returns the block totals in tot.
-__device__ __forceinline__ void exact_scan3(long long (&x)[3], long long (&tot)[3],
-                                            long long (*sm)[kExactChunkThreads / 32]) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  constexpr int NW = kExactChunkThreads / 32;
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      long long y = __shfl_up_sync(0xffffffffu, x[c], off);
-      if (lane >= off) x[c] += y;
-    }
-  if (lane == 31)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) sm[c][wid] = x[c];
-  __syncthreads();
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    long long base = 0;
-    for (int w = 0; w < wid; ++w) base += sm[c][w];
-    long long t = 0;
-    for (int w = 0; w < NW; ++w) t += sm[c][w];
-    x[c] += base;
-    tot[c] = t;
+// Running sum of the walk. While `in` holds, s = S * 2^(e-52) with |S| in
+// [2^52, 2^53): the record applications keep it there, so s is formed only
+// when a chunk is added term by term, or at the end.
+struct ExactWalk {
+  double s;
+  long long S;
+  int e;
+  bool in;
+};
+
+__device__ __forceinline__ bool exact_walk_apply(ExactWalk &w, const ExactRec &R) {
+  if (!w.in) {
+    if (!(w.s != 0.0) || !isfinite(w.s)) return false;
+    const int e = ilogb(w.s);
+    if (e < -960 || e > 1000) return false;
+    long long S = (long long)ldexp(fabs(w.s), 52 - e);  // exact
+    w.S = w.s < 0.0 ? -S : S;
+    w.e = e;
+    w.in = true;
   }
-  __syncthreads();
+  const int c = w.e - R.e0;
+  if (c < 0 || c > 2 || !((R.ok >> c) & 1)) return false;
+  const long long LO = (1LL << 52) + 1, HI = (1LL << 53) - 1;
+  const long long lo = w.S + R.mn[c], hi = w.S + R.mx[c];
+  if (w.S > 0) {
+    if (lo < LO || hi > HI) return false;
+  } else {
+    if (hi > -LO || lo < -HI) return false;
+  }
+  w.S += R.K[c];
+  return true;
 }
 
-// Block-wide min and max of three 64-bit integers.
-__device__ __forceinline__ void exact_minmax3(long long (&mn)[3], long long (&mx)[3],
-                                              long long (*smn)[kExactChunkThreads / 32],
-                                              long long (*smx)[kExactChunkThreads / 32]) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  constexpr int NW = kExactChunkThreads / 32;
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      long long a = __shfl_down_sync(0xffffffffu, mn[c], off);
-      long long b = __shfl_down_sync(0xffffffffu, mx[c], off);
-      mn[c] = a < mn[c] ? a : mn[c];
-      mx[c] = b > mx[c] ? b : mx[c];
-    }
-  if (lane == 0)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) { smn[c][wid] = mn[c]; smx[c][wid] = mx[c]; }
-  __syncthreads();
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    long long a = smn[c][0], b = smx[c][0];
-    for (int w = 1; w < NW; ++w) {
-      a = smn[c][w] < a ? smn[c][w] : a;
-      b = smx[c][w] > b ? smx[c][w] : b;
-    }
-    mn[c] = a;
-    mx[c] = b;
+__device__ __forceinline__ void exact_walk_flush(ExactWalk &w) {
+  if (w.in) {
+    w.s = ldexp((double)w.S, w.e - 52);
+    w.in = false;
   }
-  __syncthreads();
+}
+
+// The walk of sum q by one warp: lane 0 carries the running sum through the
+// group records, descending into a group's chunk records, a chunk's warp
+// records and a warp segment's 32 terms only where a record does not apply.
+// The lanes load the records and terms (rec: 32 records, wrec: a chunk's
+// warp records, term: one chunk's terms). Returns the sum on lane 0.
+static __device__ __noinline__ double exact_walk(const ExactHdr *H, const double *seq, long long n, long long nch,
+                                          int q, long long cap, long long capg, ExactRec *rec, ExactRec *wrec,
+                                          double *term) {
+  const int lane = threadIdx.x & 31;
+  const long long ng = (nch + kExactGroup - 1) / kExactGroup;
+  ExactWalk w{0.0, 0, 0, false};
+  long long gi = 0;
+  while (gi < ng) {
+    const int nb = (int)((ng - gi) < 32 ? (ng - gi) : 32);
+    if (lane < nb) exact_load(rec[lane], &H->grec[q * capg + gi + lane]);
+    __syncwarp();
+    int k = 0;
+    if (lane == 0)
+      while (k < nb && exact_walk_apply(w, rec[k])) ++k;
+    k = __shfl_sync(0xffffffffu, k, 0);
+    __syncwarp();
+    gi += k;
+    if (k == nb) continue;
+    // group gi: its chunk records, 32 at a time
+    const long long c0 = gi * kExactGroup;
+    const int cs = (int)((nch - c0) < kExactGroup ? (nch - c0) : kExactGroup);
+    for (int h0 = 0; h0 < cs; h0 += 32) {
+      const int hb = (cs - h0) < 32 ? (cs - h0) : 32;
+      if (lane < hb) exact_load(rec[lane], &H->crec[q * cap + c0 + h0 + lane]);
+      __syncwarp();
+      int ci = 0;
+      while (ci < hb) {
+        int m = ci;
+        if (lane == 0)
+          while (m < hb && exact_walk_apply(w, rec[m])) ++m;
+        m = __shfl_sync(0xffffffffu, m, 0);
+        if (m >= hb) break;
+        // chunk c0 + h0 + m: its warp records, then the terms of a warp
+        // segment where one does not apply
+        const long long ch = c0 + h0 + m;
+        const long long e0 = ch * kExactChunkThreads;
+        const int len = (int)((n - e0) < kExactChunkThreads ? (n - e0) : kExactChunkThreads);
+        if (lane < kExactWarps) exact_load(wrec[lane], &H->wrec[(q * cap + ch) * kExactWarps + lane]);
+        for (int e = lane; e < len; e += 32) term[e] = __ldcg(&seq[q * n + e0 + e]);
+        __syncwarp();
+        if (lane == 0) {
+          for (int ww = 0; ww < kExactWarps && 32 * ww < len; ++ww) {
+            if (exact_walk_apply(w, wrec[ww])) continue;
+            exact_walk_flush(w);
+            double sv = w.s;
+            const int e1 = (32 * ww + 32) < len ? (32 * ww + 32) : len;
+#pragma unroll 8
+            for (int e = 32 * ww; e < e1; ++e) sv = __dadd_rn(sv, term[e]);
+            w.s = sv;
+          }
+        }
+        __syncwarp();
+        ci = m + 1;
+      }
+      __syncwarp();
+    }
+    ++gi;
+  }
+  exact_walk_flush(w);
+  return w.s;
 }
 
 // The exact-order reduction. Launch shape: one thread per term, blocks of
@@ -201,13 +251,12 @@ __device__ bool exact_reduce(const double (&v)[NV], double *seq, long long n, un
 
   __shared__ double s_agg[NV][NW];
   __shared__ double s_hint[NV];
-  __shared__ long long s_a[3][NW], s_b[3][NW];
+  __shared__ ExactRec s_wr[NV][kExactWarps];
   __shared__ ExactRec s_rec;
   __shared__ bool s_last;
-  __shared__ int s_cmd;
-  __shared__ long long s_arg;
-  __shared__ ExactRec s_buf[kExactGroup];
-  __shared__ double s_terms[kExactChunkThreads];
+  __shared__ ExactRec s_wrec[kExactVals][32];
+  __shared__ double s_wterm[kExactVals][kExactChunkThreads];
+  __shared__ double s_res[kExactVals];
 
   // 1. the terms
   double a[NV];
@@ -287,7 +336,9 @@ __device__ bool exact_reduce(const double (&v)[NV], double *seq, long long n, un
   }
   __syncthreads();
 
-  // 3. chunk records for the exponents around the hint
+  // 3. records for the exponents around the hint: one per warp (32 terms,
+  // warp scans only), composed by thread 0 into the chunk's record
+  constexpr long long L53 = 1LL << 53;
 #pragma unroll
   for (int q = 0; q < NV; ++q) {
     const double hint = s_hint[q];
@@ -297,43 +348,66 @@ __device__ bool exact_reduce(const double (&v)[NV], double *seq, long long n, un
       e0 = ilogb(hint) - 1;
       have = e0 >= -960 && e0 + 2 <= 1000;
     }
-    if (!have) {
-      if (t == 0) {
-        ExactRec R;
-        for (int c = 0; c < 3; ++c) R.K[c] = R.mn[c] = R.mx[c] = 0;
-        R.e0 = 0;
-        R.ok = 0;
-        H->crec[q * cap + b] = R;
-      }
-      continue;  // uniform across the block
-    }
-    long long k[3];
-    int okb = 0;
+    ExactRec W;
+    W.e0 = e0;
+    W.ok = 0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const double y = a[q] * ldexp(1.0, 52 - (e0 + c));
-      // finite, |y| <= 2^53 and not half-way between two integers
-      const bool good = isfinite(y) && fabs(y) <= 9007199254740992.0 && fabs(y - trunc(y)) != 0.5;
-      k[c] = good ? __double2ll_rn(y) : 0;
-      if (__syncthreads_and(good)) okb |= 1 << c;
-    }
-    long long tot[3];
-    exact_scan3(k, tot, s_a);
-    long long mn[3] = {k[0], k[1], k[2]}, mx[3] = {k[0], k[1], k[2]};
-    exact_minmax3(mn, mx, s_a, s_b);
-    if (t == 0) {
-      ExactRec R;
-      R.e0 = e0;
-      R.ok = okb;
-      for (int c = 0; c < 3; ++c) {
-        R.K[c] = tot[c];
-        R.mn[c] = mn[c];
-        R.mx[c] = mx[c];
-        const long long L = 1LL << 53;
-        if (mn[c] <= -L || mx[c] >= L || tot[c] <= -L || tot[c] >= L) R.ok &= ~(1 << c);
+      long long k = 0;
+      bool good = false;
+      if (have) {
+        const double y = a[q] * ldexp(1.0, 52 - (e0 + c));
+        // finite, |y| <= 2^53 and not half-way between two integers
+        good = isfinite(y) && fabs(y) <= 9007199254740992.0 && fabs(y - trunc(y)) != 0.5;
+        k = good ? __double2ll_rn(y) : 0;
       }
-      H->crec[q * cap + b] = R;
+      // inclusive prefix over the warp, its total and range
+      for (int off = 1; off < 32; off <<= 1) {
+        const long long v = __shfl_up_sync(0xffffffffu, k, off);
+        if (lane >= off) k += v;
+      }
+      long long mn = k, mx = k;
+      for (int off = 16; off > 0; off >>= 1) {
+        const long long a2 = __shfl_xor_sync(0xffffffffu, mn, off), b2 = __shfl_xor_sync(0xffffffffu, mx, off);
+        mn = a2 < mn ? a2 : mn;
+        mx = b2 > mx ? b2 : mx;
+      }
+      W.K[c] = __shfl_sync(0xffffffffu, k, 31);
+      W.mn[c] = mn;
+      W.mx[c] = mx;
+      if (__all_sync(0xffffffffu, good) && mn > -L53 && mx < L53) W.ok |= 1 << c;
     }
+    if (lane == 0) {
+      s_wr[q][wid] = W;
+      H->wrec[(q * cap + b) * kExactWarps + wid] = W;
+    }
+  }
+  __syncthreads();
+  if (t < NV) {  // thread q composes sum q's chunk record from its warp records
+    const int q = t;
+    ExactRec R;
+    R.e0 = s_wr[q][0].e0;
+    R.ok = 7;
+    for (int c = 0; c < 3; ++c) {
+      long long K = 0, mn = 0x7fffffffffffffffLL, mx = -0x7fffffffffffffffLL;
+      for (int w = 0; w < kExactWarps; ++w) {
+        const ExactRec &Wr = s_wr[q][w];
+        if (!((Wr.ok >> c) & 1)) { R.ok &= ~(1 << c); break; }
+        const long long lo = K + Wr.mn[c], hi = K + Wr.mx[c];
+        mn = lo < mn ? lo : mn;
+        mx = hi > mx ? hi : mx;
+        K += Wr.K[c];
+      }
+      if (!((R.ok >> c) & 1) || mn <= -L53 || mx >= L53 || K <= -L53 || K >= L53) {
+        R.ok &= ~(1 << c);
+        K = mn = mx = 0;
+      }
+      R.K[c] = K;
+      R.mn[c] = mn;
+      R.mx[c] = mx;
+    }
+    if (!(isfinite(s_hint[q]) && s_hint[q] != 0.0)) R.ok = 0;
+    H->crec[q * cap + b] = R;
   }
 
   // 4. group records
@@ -413,7 +487,7 @@ __device__ bool exact_reduce(const double (&v)[NV], double *seq, long long n, un
     if (lane == 0) H->gcount[g] = 0u;
   }
 
-  // 5. the last block walks the groups
+  // 5. the last block walks the groups; warp q walks sum q
   if (t == 0) {
     __threadfence();
     unsigned prev = atomicAdd(count, 1u);
@@ -422,61 +496,14 @@ __device__ bool exact_reduce(const double (&v)[NV], double *seq, long long n, un
   __syncthreads();
   if (!s_last) return false;
   __threadfence();
-  const long long ng = (nch + kExactGroup - 1) / kExactGroup;
-  double res[NV];
-#pragma unroll
-  for (int q = 0; q < NV; ++q) {
-    double s = 0.0;   // meaningful in thread 0
-    long long gi = 0;
-    while (gi < ng) {
-      // a batch of group records
-      const int nb = (int)((ng - gi) < kExactGroup ? (ng - gi) : kExactGroup);
-      if (t < nb) exact_load(s_buf[t], &H->grec[q * capg + gi + t]);
-      __syncthreads();
-      if (t == 0) {
-        int k = 0;
-        while (k < nb && exact_apply(s, s_buf[k])) ++k;
-        s_cmd = k;
-      }
-      __syncthreads();
-      const int k = s_cmd;
-      __syncthreads();
-      gi += k;
-      if (k == nb) continue;
-      // group gi needs its chunk records
-      const long long c0 = gi * kExactGroup;
-      const int cs = (int)((nch - c0) < kExactGroup ? (nch - c0) : kExactGroup);
-      if (t < cs) exact_load(s_buf[t], &H->crec[q * cap + c0 + t]);
-      __syncthreads();
-      int ci = 0;
-      while (ci < cs) {
-        if (t == 0) {
-          int m = ci;
-          while (m < cs && exact_apply(s, s_buf[m])) ++m;
-          s_cmd = m;
-        }
-        __syncthreads();
-        const int m = s_cmd;
-        __syncthreads();
-        ci = m;
-        if (ci >= cs) break;
-        // chunk c0 + ci term by term
-        const long long e0 = (c0 + ci) * kExactChunkThreads;
-        const int len = (int)((n - e0) < kExactChunkThreads ? (n - e0) : kExactChunkThreads);
-        if (t < len) s_terms[t] = __ldcg(&seq[q * n + e0 + t]);
-        __syncthreads();
-        if (t == 0)
-          for (int e = 0; e < len; ++e) s = __dadd_rn(s, s_terms[e]);
-        __syncthreads();
-        ++ci;
-      }
-      ++gi;
-    }
-    res[q] = s;
+  if (wid < NV) {
+    const double r = exact_walk(H, seq, n, nch, wid, cap, capg, s_wrec[wid], s_wr[wid], s_wterm[wid]);
+    if (lane == 0) s_res[wid] = r;
   }
+  __syncthreads();
   if (t != 0) return false;
 #pragma unroll
-  for (int q = 0; q < NV; ++q) out[q] = res[q];
+  for (int q = 0; q < NV; ++q) out[q] = s_res[q];
   ExactHdr *Hw = const_cast<ExactHdr *>(H);
   const unsigned nxt = (gen + 1u) & 0x3fffffffu;
   Hw->gen = nxt ? nxt : 1u;  // generation 0 is the zeroed flags' value

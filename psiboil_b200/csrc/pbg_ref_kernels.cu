@@ -112,6 +112,7 @@ void exact_scratch_init(double *base, long long ncell, cudaStream_t s) {
   char *q = reinterpret_cast<char *>(base) + kExactHdrBytes + sizeof(double) * (size_t)kExactVals * ncell;
   ExactHdr h;
   std::memset(&h, 0, sizeof(h));
+  h.wrec = reinterpret_cast<ExactRec *>(q); q += sizeof(ExactRec) * kExactVals * (size_t)ch * kExactWarps;
   h.crec = reinterpret_cast<ExactRec *>(q); q += sizeof(ExactRec) * kExactVals * (size_t)ch;
   h.grec = reinterpret_cast<ExactRec *>(q); q += sizeof(ExactRec) * kExactVals * (size_t)gr;
   h.agg = reinterpret_cast<double *>(q); q += sizeof(double) * kExactVals * (size_t)ch;
