@@ -224,6 +224,16 @@ __global__ void k_fcg_continue(cudaGraphConditionalHandle h, FcgScal *fs) {
   cudaGraphSetConditional(h, (!fs->done && n < fs->maxit) ? 1u : 0u);
 }
 
+// Start of the device-side loop: enter it only if the solve has not
+// converged at the start (k_fcg_init sets done when |r0| is already below
+// the tolerance). With this gate in front of the WHILE node, no kernel of
+// the loop body runs once the solve is done, so the body's kernels are
+// captured without the done flag and do not load it before their work.
+__global__ void k_fcg_gate(cudaGraphConditionalHandle h, const FcgScal *fs) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  cudaGraphSetConditional(h, (!fs->done && fs->loops < fs->maxit) ? 1u : 0u);
+}
+
 // The FCG iterations of a refinement sweep run as a device-side loop (a
 // conditional WHILE graph node) unless PBG_GRAPH_LOOP=0, which replays the
 // one-iteration graph in host-polled chunks instead.
@@ -524,10 +534,10 @@ int Engine::fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red, cu
   const long long N = A.ncell();
   const int g = grid_for(N);
   FcgScal *fs = w.fs.p;
-  const int *stop = &fs->done;
   // one FCG iteration: the preconditioner's K-cycle over all levels plus
-  // the two FCG kernels
-  auto iteration = [&]() {
+  // the two FCG kernels; every kernel returns at once when *stop is set
+  // (stop == nullptr: no check)
+  auto iteration = [&](const int *stop) {
     precond<T>(0, w.r0.p, w.z0.p, true, w.q0.p, &fs->zr, w, red, stop, s, false);
     if (A.nz % VecTraits<T>::V == 0 && (int)L.size() > 1) {
       const int gv = grid_for(N / VecTraits<T>::V, kThreads, kVecBlocks);
@@ -547,7 +557,7 @@ int Engine::fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red, cu
     const unsigned long long before = g_launch_count;
     PBG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     try {
-      iteration();
+      iteration(&fs->done);
     } catch (...) {
       cudaStreamEndCapture(s, &graph);  // leave the stream usable
       if (graph) cudaGraphDestroy(graph);
@@ -559,24 +569,36 @@ int Engine::fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red, cu
     PBG_CUDA(cudaGraphInstantiate(&w.iter_graph, graph, 0));
     cudaGraphDestroy(graph);
     if (graph_loop_enabled()) {
-      // the same iteration as the body of a WHILE node whose condition the
-      // last kernel of the body sets on the device
+      // the same iteration as the body of a WHILE node: a gate kernel sets
+      // its condition before the first pass, the last kernel of the body
+      // after each pass
       cudaGraph_t lg = nullptr;
       PBG_CUDA(cudaGraphCreate(&lg, 0));
       try {
         cudaGraphConditionalHandle h;
-        PBG_CUDA(cudaGraphConditionalHandleCreate(&h, lg, 1, cudaGraphCondAssignDefault));
+        PBG_CUDA(cudaGraphConditionalHandleCreate(&h, lg, 0, cudaGraphCondAssignDefault));
+        cudaKernelNodeParams kp = {};
+        const FcgScal *cfs = fs;
+        void *kargs[] = {(void *)&h, (void *)&cfs};
+        kp.func = (void *)k_fcg_gate;
+        kp.gridDim = dim3(1);
+        kp.blockDim = dim3(32);
+        kp.sharedMemBytes = 0;
+        kp.kernelParams = kargs;
+        kp.extra = nullptr;
+        cudaGraphNode_t gate;
+        PBG_CUDA(cudaGraphAddKernelNode(&gate, lg, nullptr, 0, &kp));
         cudaGraphNodeParams np = {};
         np.type = cudaGraphNodeTypeConditional;
         np.conditional.handle = h;
         np.conditional.type = cudaGraphCondTypeWhile;
         np.conditional.size = 1;
         cudaGraphNode_t node;
-        PBG_CUDA(cudaGraphAddNode(&node, lg, nullptr, 0, &np));
+        PBG_CUDA(cudaGraphAddNode(&node, lg, &gate, 1, &np));
         cudaGraph_t body = np.conditional.phGraph_out[0];
         PBG_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
         try {
-          iteration();
+          iteration(nullptr);
           k_fcg_continue<<<1, 32, 0, s>>>(h, fs);
         } catch (...) {
           cudaStreamEndCapture(s, &body);
@@ -601,7 +623,7 @@ int Engine::fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red, cu
     PBG_CUDA(cudaGraphLaunch(w.loop_graph, s));
     PBG_CUDA(cudaMemcpyAsync(hfs, fs, sizeof(FcgScal), cudaMemcpyDeviceToHost, s));
     PBG_CUDA(cudaStreamSynchronize(s));
-    __atomic_add_fetch(&g_launch_count, (unsigned long long)hfs->loops * (w.iter_nodes + 1), __ATOMIC_RELAXED);
+    __atomic_add_fetch(&g_launch_count, (unsigned long long)hfs->loops * (w.iter_nodes + 1) + 1, __ATOMIC_RELAXED);
     return hfs->iter;
   }
   int enq = 0, chunk = 4;
