@@ -76,15 +76,18 @@ Geo flow_geo(const pbg_session *s) {
   return Geo(s->nx, s->ny, s->nz);
 }
 
-// The row-vector flow kernels (4 cells of a k-row per thread) take grids
-// with nz % 4 == 0 below 2^31 cells and no cut body; PBG_FLOW_SCALAR=1
-// selects the one-cell kernels (the same bits).
+// The flow kernels that own 4 cells of a k-row per thread (the divergence's
+// row form and the marching assembly and projection) take grids with
+// nz % 4 == 0 below 2^31 cells, no cut body and a marching grid within the
+// launch limits; PBG_FLOW_SCALAR=1 selects the one-cell kernels (the same
+// bits).
 bool flow_vec(const pbg_session *s, bool cut) {
   static const bool scalar = [] {
     const char *e = std::getenv("PBG_FLOW_SCALAR");
     return e && e[0] == '1';
   }();
-  return !scalar && !cut && s->nz % kFlowV == 0 && s->ncell() < (1ll << 31);
+  return !scalar && !cut && s->nz % kFlowV == 0 && s->ncell() < (1ll << 31) &&
+         march_fits(s->nx, s->ny, s->nz);
 }
 
 int fail(int code, const std::string &m) {
@@ -656,9 +659,10 @@ int pbg_assemble_mix(pbg_session *s, const double *col, double rho_a, double rho
     if (sym) { A.e.release(); A.n.release(); A.t.release(); }
     else if (A.e.n != (size_t)N) { A.e.alloc(N); A.n.alloc(N); A.t.alloc(N); }
     if (flow_vec(s, bd.idx != nullptr)) {
-      kv_assemble_mix<<<grid_for(N / kFlowV), kThreads, 0, s->stream>>>(
-          flow_geo(s), s->nx, s->ny, s->nz, s->h, make_int4(s->bc[0], s->bc[1], s->bc[2], s->bc[3]),
-          make_int2(s->bc[4], s->bc[5]), cp, rho_a, rho_b, bd.off, A.c.p, A.w.p, A.s.p, A.b.p, s->aflag.p);
+      km_assemble_mix<<<march_grid(s->nx, s->ny, s->nz), kThreads, 0, s->stream>>>(
+          s->nx, s->ny, s->nz, march_kq(s->nz), march_len(s->nx, s->ny, s->nz), s->h,
+          make_int4(s->bc[0], s->bc[1], s->bc[2], s->bc[3]), make_int2(s->bc[4], s->bc[5]), cp, rho_a, rho_b,
+          bd.off, A.c.p, A.w.p, A.s.p, A.b.p, s->aflag.p);
     } else {
       k_assemble_mix<<<grid_for(N), kThreads, 0, s->stream>>>(
           flow_geo(s), s->nx, s->ny, s->nz, s->h, make_int4(s->bc[0], s->bc[1], s->bc[2], s->bc[3]),
@@ -795,9 +799,9 @@ int pbg_project(pbg_session *s, const double *p, const double *col, double rho_a
     BodyArgs bd;
     if (int rc = body_args(s, sp, bd)) return rc;
     if (flow_vec(s, false))
-      kv_project<<<grid_for(N / kFlowV), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, s->h, dt, pp,
-                                                                   cp, rho_a, rho_b, bd.off, fa.d[0], fa.d[1],
-                                                                   fa.d[2]);
+      km_project<<<march_grid(s->nx, s->ny, s->nz), kThreads, 0, s->stream>>>(
+          s->nx, s->ny, s->nz, march_kq(s->nz), march_len(s->nx, s->ny, s->nz), s->h, dt, pp, cp, rho_a, rho_b,
+          bd.off, fa.d[0], fa.d[1], fa.d[2]);
     else
       k_project<<<grid_for(N), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, s->h, dt, pp, cp, rho_a,
                                                          rho_b, bd.off, fa.d[0], fa.d[1], fa.d[2]);

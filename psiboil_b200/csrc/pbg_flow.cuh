@@ -219,6 +219,93 @@ __global__ void k_divergence(Geo G, int nx, int ny, int nz, double a, const doub
 // west, south and bottom faces of its cell; the faces on the domain
 // boundary are not touched (they hold the walls' values, which
 // bnd_update_nooutlet restores in the reference), nor is w in 2-D.
+// Division by a divisor b known in advance (the spacing h, the density of a
+// pure phase), rounded to nearest like a / b itself: with y = RN(1/b) formed
+// once, q0 = RN(a y) lies within one ulp of a/b, the remainder r = a - b q0
+// is exact in one FMA, and RN(q0 + r y) = RN(a/b) (Markstein's theorem:
+// P. Markstein, IBM J. Res. Develop. 34(1), 1990; its use for a divisor
+// known in advance: N. Brisebarre, J.-M. Muller and S. K. Raina, IEEE Trans.
+// Comput. 53(8), 2004). The theorem needs every intermediate normal, so b
+// is restricted to [2^-60, 2^60] and |a| to (2^-900, 2^900); zero, infinite
+// and NaN dividends, and everything outside those ranges, take the division
+// itself.
+struct KnownDiv {
+  double b, y;
+  bool ok;
+  __device__ __forceinline__ explicit KnownDiv(double b_) : b(b_) {
+    y = __ddiv_rn(1.0, b_);
+    const double m = fabs(b_);
+    ok = m >= 0x1p-60 && m <= 0x1p60;
+  }
+  // a / b
+  __device__ __forceinline__ double operator()(double a) const {
+    const double m = fabs(a);
+    if (ok && m > 0x1p-900 && m < 0x1p900) {
+      const double q0 = __dmul_rn(a, y);
+      return __fma_rn(__fma_rn(-q0, b, a), y, q0);
+    }
+    return __ddiv_rn(a, b);
+  }
+  // a / d for any d: the corrected product when d is b (b nonzero, so d == b
+  // means the same bits), else the division
+  __device__ __forceinline__ double by(double a, double d) const {
+    if (d == b && ok) return (*this)(a);
+    return __ddiv_rn(a, d);
+  }
+};
+
+// Face densities of the two pure phases (colour 1 and 0) and the spacing:
+// the divisors the projection meets on every face away from an interface.
+struct PhaseDiv {
+  KnownDiv a, b, h;
+  __device__ __forceinline__ PhaseDiv(double ra, double rb, double h_) : a(ra), b(rb), h(h_) {}
+  __device__ __forceinline__ double by_rho(double x, double rho) const {
+    if (rho == a.b && a.ok) return a(x);
+    return b.by(x, rho);
+  }
+};
+
+// project_increment with the divisions by a pure-phase density and by h
+// done by KnownDiv: the same bits
+__device__ __forceinline__ double project_increment_k(double pm, double pp, double rho, double dt,
+                                                      const PhaseDiv &D, bool body) {
+  const double dp = __dsub_rn(pm, pp);
+  if (body) return D.h(D.by_rho(__dmul_rn(dp, dt), rho));
+  return D.h(__dmul_rn(D.by_rho(dp, rho), dt));
+}
+
+// project_increment for the fast quads of the marching projection: both
+// divisions by Markstein's correction with no fallback; a face density that
+// is not a pure phase's, a dividend outside the range where the correction
+// is exact (+0 included, -0 not), or a divisor outside [2^-60, 2^60] sets
+// miss, and the quad is redone by the general code.
+struct ProjFast {
+  double ka, kb, ra, rb, ya, yb, h, yh;
+  bool hok;
+  __device__ __forceinline__ explicit ProjFast(const PhaseDiv &D) {
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    ka = D.a.ok ? D.a.b : nan;
+    kb = D.b.ok ? D.b.b : nan;
+    ra = D.a.b; rb = D.b.b; ya = D.a.y; yb = D.b.y;
+    h = D.h.b; yh = D.h.y; hok = D.h.ok;
+  }
+  __device__ __forceinline__ static double corr(double a, double b, double y, bool &miss) {
+    const double m = fabs(a);
+    miss |= !((m > 0x1p-900 && m < 0x1p900) || __double_as_longlong(a) == 0);
+    const double q0 = __dmul_rn(a, y);
+    return __fma_rn(__fma_rn(-q0, b, a), y, q0);
+  }
+  __device__ __forceinline__ double inc(double pm, double pp, double rho, double dt, bool body,
+                                        bool &miss) const {
+    const double dp = __dsub_rn(pm, pp);
+    const bool isa = rho == ka;
+    miss |= !(isa || rho == kb) || !hok;
+    const double bb = isa ? ra : rb, yy = isa ? ya : yb;
+    if (body) return corr(corr(__dmul_rn(dp, dt), bb, yy, miss), h, yh, miss);
+    return corr(__dmul_rn(corr(dp, bb, yy, miss), dt), h, yh, miss);
+  }
+};
+
 __device__ __forceinline__ double project_increment(double pm, double pp, double rho, double dt, double h,
                                                     bool body) {
   const double dp = __dsub_rn(pm, pp);
@@ -252,14 +339,14 @@ __global__ void k_project(Geo G, int nx, int ny, int nz, double h, double dt, co
 }
 
 // ---------------------------------------------------------------------------
-// Row-vector forms of the three flow kernels: a thread owns 4 consecutive
-// cells of a k-row (nz % 4 == 0, no cut body, fewer than 2^31 cells), reads
-// every row with 16-byte loads and shares what neighbouring cells of the row
-// have in common: the mixture density of each cell is formed once, the face
-// density and coefficient between two cells of the row once (the top face
-// of a cell is the bottom face of the next). Every value is computed by the
-// same operations in the same order as the one-cell kernels above, so the
-// outputs are bit for bit theirs.
+// Four cells of a k-row per thread (nz % 4 == 0, no cut body, fewer than
+// 2^31 cells): rows are read with 16-byte loads, and what neighbouring cells
+// of the row have in common is formed once (the mixture density of a cell,
+// the face between two cells of the row: the top face of a cell is the
+// bottom face of the next). The row helpers, the divergence in this form,
+// and the marching assembly and projection below. Every value is computed
+// by the same operations in the same order as the one-cell kernels above,
+// so the outputs are bit for bit theirs.
 // ---------------------------------------------------------------------------
 constexpr int kFlowV = 4;
 
@@ -299,105 +386,6 @@ __device__ __forceinline__ double mix1(const double *__restrict__ col, double ra
 // density without colour
 __device__ __forceinline__ double face_of(bool col, double ra, double m1, double m2) {
   return col ? __dmul_rn(0.5, __dadd_rn(m1, m2)) : ra;
-}
-
-__global__ void __launch_bounds__(kThreads)
-    kv_assemble_mix(Geo G, int nx, int ny, int nz, double h, int4 bc03, int2 bc45,
-                    const double *__restrict__ col, double ra, double rb, const uint8_t *__restrict__ solid,
-                    double *__restrict__ C, double *__restrict__ W, double *__restrict__ S,
-                    double *__restrict__ B, uint8_t *__restrict__ aflag) {
-  const int bc[6] = {bc03.x, bc03.y, bc03.z, bc03.w, bc45.x, bc45.y};
-  const uint32_t SI = G.nynz, SJ = (uint32_t)nz;
-  const double hh = __dmul_rn(h, h);
-  const double hx = __ddiv_rn(hh, h);
-  const double hxb = __ddiv_rn(hh, __dmul_rn(0.5, h));
-  const bool hc = col != nullptr;
-  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < G.n / kFlowV; g += gridDim.x * blockDim.x) {
-    const uint32_t p = g * kFlowV;
-    const Pos q = G.pos(p);
-    double mc[4], mw[4], me[4], ms[4], mn[4];
-    mix4(col, ra, rb, p, mc);
-    if (q.i > 0) mix4(col, ra, rb, p - SI, mw);
-    if (q.i < nx - 1) mix4(col, ra, rb, p + SI, me);
-    if (q.j > 0) mix4(col, ra, rb, p - SJ, ms);
-    if (q.j < ny - 1) mix4(col, ra, rb, p + SJ, mn);
-    const double mkm = q.k > 0 ? mix1(col, ra, rb, (long long)p - 1) : 0.0;
-    const double mkp = q.k + kFlowV < nz ? mix1(col, ra, rb, (long long)p + kFlowV) : 0.0;
-    // bottom faces of the row's cells and the top face of its last cell
-    double bf[5];
-    bf[0] = q.k == 0 ? __ddiv_rn(hxb, face_of(hc, ra, mc[0], mc[0])) : __ddiv_rn(hx, face_of(hc, ra, mc[0], mkm));
-#pragma unroll
-    for (int m = 1; m < 4; ++m) bf[m] = __ddiv_rn(hx, face_of(hc, ra, mc[m], mc[m - 1]));
-    bf[4] = q.k + kFlowV == nz ? __ddiv_rn(hxb, face_of(hc, ra, mc[3], mc[3]))
-                               : __ddiv_rn(hx, face_of(hc, ra, mkp, mc[3]));
-    uchar4 sc = make_uchar4(0, 0, 0, 0), sw = sc, se = sc, ss = sc, sn = sc;
-    uint8_t skm = 0, skp = 0;
-    if (solid) {
-      sc = ld4b(solid, p);
-      if (q.i > 0) sw = ld4b(solid, p - SI);
-      if (q.i < nx - 1) se = ld4b(solid, p + SI);
-      if (q.j > 0) ss = ld4b(solid, p - SJ);
-      if (q.j < ny - 1) sn = ld4b(solid, p + SJ);
-      if (q.k > 0) skm = solid[p - 1];
-      if (q.k + kFlowV < nz) skp = solid[p + kFlowV];
-    }
-    double oc[4], ow[4], os[4], ob[4];
-    uchar4 af;
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-      double a[6];
-      a[0] = __ddiv_rn(q.i == 0 ? hxb : hx, q.i > 0 ? face_of(hc, ra, mc[m], mw[m]) : face_of(hc, ra, mc[m], mc[m]));
-      a[1] = __ddiv_rn(q.i == nx - 1 ? hxb : hx,
-                       q.i < nx - 1 ? face_of(hc, ra, me[m], mc[m]) : face_of(hc, ra, mc[m], mc[m]));
-      a[2] = __ddiv_rn(q.j == 0 ? hxb : hx, q.j > 0 ? face_of(hc, ra, mc[m], ms[m]) : face_of(hc, ra, mc[m], mc[m]));
-      a[3] = __ddiv_rn(q.j == ny - 1 ? hxb : hx,
-                       q.j < ny - 1 ? face_of(hc, ra, mn[m], mc[m]) : face_of(hc, ra, mc[m], mc[m]));
-      a[4] = bf[m];
-      a[5] = bf[m + 1];
-      const int kk = q.k + m;
-      double c = a[0];
-#pragma unroll
-      for (int f = 1; f < 6; ++f) c = __dadd_rn(c, a[f]);
-      const uint8_t sp = byte_of(sc, m);
-      if (solid) {
-        const uint8_t sbm = m > 0 ? byte_of(sc, m - 1) : skm, stp = m < 3 ? byte_of(sc, m + 1) : skp;
-        if (q.i > 0 && byte_of(sw, m) != sp) a[0] = 0.0;
-        if (q.i < nx - 1 && byte_of(se, m) != sp) a[1] = 0.0;
-        if (q.j > 0 && byte_of(ss, m) != sp) a[2] = 0.0;
-        if (q.j < ny - 1 && byte_of(sn, m) != sp) a[3] = 0.0;
-        if (kk > 0 && sbm != sp) a[4] = 0.0;
-        if (kk < nz - 1 && stp != sp) a[5] = 0.0;
-        if (!sp) {
-          c = a[0];
-#pragma unroll
-          for (int f = 1; f < 6; ++f) c = __dadd_rn(c, a[f]);
-        }
-      }
-      const bool onb[6] = {q.i == 0, q.i == nx - 1, q.j == 0, q.j == ny - 1, kk == 0, kk == nz - 1};
-#pragma unroll
-      for (int f = 0; f < 6; ++f) {
-        if (!onb[f] || bc[f] != PBG_BC_NEUMANN_) continue;
-        c = __dsub_rn(c, a[f]);
-        a[f] = 0.0;
-      }
-#pragma unroll
-      for (int f = 0; f < 6; ++f)
-        if (onb[f] && bc[f] == PBG_BC_DIRICHLET_) a[f] = 0.0;
-      if (sp) {
-        c = __dmul_rn(c, 1.0e-12);
-#pragma unroll
-        for (int f = 0; f < 6; ++f) a[f] = 0.0;
-      }
-      oc[m] = c; ow[m] = a[0]; os[m] = a[2]; ob[m] = a[4];
-      const uint8_t fl = sp ? 0 : 1;
-      if (m == 0) af.x = fl; else if (m == 1) af.y = fl; else if (m == 2) af.z = fl; else af.w = fl;
-    }
-    st4d(C, p, oc);
-    st4d(W, p, ow);
-    st4d(S, p, os);
-    st4d(B, p, ob);
-    *reinterpret_cast<uchar4 *>(aflag + p) = af;
-  }
 }
 
 // update_rhs for 4 cells of a row, the voxel-body branch of k_divergence.
@@ -457,66 +445,459 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// Momentum::project for 4 cells of a row (the faces k_project's threads own).
-__global__ void __launch_bounds__(kThreads)
-    kv_project(Geo G, int nx, int ny, int nz, double h, double dt, const double *__restrict__ pr,
-               const double *__restrict__ col, double ra, double rb, const uint8_t *__restrict__ solid,
-               double *__restrict__ u, double *__restrict__ v, double *__restrict__ w) {
-  const uint32_t SI = G.nynz, SJ = (uint32_t)nz;
-  const bool body = solid != nullptr;
+// ---------------------------------------------------------------------------
+// Marching forms of the assembly and the projection (nz % 4 == 0, no cut
+// body, fewer than 2^31 cells). A block of 256 threads owns a tile of the
+// (j, k) plane, TJ rows of 4 KQ cells (KQ threads a row, 4 cells a thread,
+// TJ = 256 / KQ), and walks it through LEN consecutive i planes. The
+// colour, mixture density, pressure and solid flag of a cell are read and
+// formed once per walk (plus the plane before the walk and the tile's
+// one-cell halo); the row and k neighbours in a plane come from shared
+// memory, the previous plane from registers, and the coefficient of the
+// face between planes i and i+1 is formed once, as the east face of i and
+// the west face of i+1. Every value is the same operations in the same
+// order as the one-cell kernels, so the outputs are bit for bit theirs.
+// ---------------------------------------------------------------------------
+constexpr int kMarchI = 8;       // planes a walk, at most
+constexpr int kMarchSmA = 1548;  // assembly: (TJ + 2) (4 KQ + 2) cells at most, TJ KQ = 256
+constexpr int kMarchSmP = 1285;  // projection: (TJ + 1) (4 KQ + 1) cells at most
+
+// threads a row: the smallest power of two with 4 KQ >= nz, at most 64
+inline int march_kq(int nz) {
+  int q = 1;
+  while (q < 64 && 4 * q < nz) q *= 2;
+  return q;
+}
+// planes a walk: kMarchI, halved (down to 2) while the grid would hold
+// fewer than four blocks an SM of a 148-SM GPU
+inline int march_len(int nx, int ny, int nz) {
+  const int kq = march_kq(nz), tj = kThreads / kq;
+  const long long tiles = (long long)((nz + 4 * kq - 1) / (4 * kq)) * ((ny + tj - 1) / tj);
+  int len = kMarchI;
+  while (len > 2 && tiles * ((nx + len - 1) / len) < 4 * 148) len /= 2;
+  return len;
+}
+inline dim3 march_grid(int nx, int ny, int nz) {
+  const int kq = march_kq(nz), tj = kThreads / kq, len = march_len(nx, ny, nz);
+  return dim3((unsigned)((nz + 4 * kq - 1) / (4 * kq)), (unsigned)((ny + tj - 1) / tj),
+              (unsigned)((nx + len - 1) / len));
+}
+inline bool march_fits(int nx, int ny, int nz) {
+  const dim3 g = march_grid(nx, ny, nz);
+  return g.y <= 65535u && g.z <= 65535u;
+}
+
+// hx / f for a face density f, with hx / ra and hx / rb formed once: away
+// from an interface every interior face coefficient is one of the two (a
+// division is deterministic, so the cached quotient is the same bits). A
+// zero density never takes the cached quotient (-0 == +0 would pick the
+// wrong sign of infinity).
+struct QuotCache {
+  double hx, ra, rb, qa, qb;
+  __device__ __forceinline__ QuotCache(double hx_, double ra_, double rb_) : hx(hx_), ra(ra_), rb(rb_) {
+    qa = __ddiv_rn(hx_, ra_);
+    qb = __ddiv_rn(hx_, rb_);
+  }
+  __device__ __forceinline__ double operator()(double f) const {
+    if (f != 0.0) {
+      if (f == ra) return qa;
+      if (f == rb) return qb;
+    }
+    return __ddiv_rn(hx, f);
+  }
+};
+
+// Cache-only quotients for the fast quads of the marching assembly: hx and
+// hxb (the wall faces' numerator) over either pure-phase density. A face
+// density that is neither (an interface face), or a zero density, sets
+// miss and returns a placeholder.
+struct QuotOnly {
+  double ka, kb, qa, qb, qba, qbb;
+  __device__ __forceinline__ QuotOnly(double hx, double hxb, double ra, double rb) {
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    ka = ra != 0.0 ? ra : nan;
+    kb = rb != 0.0 ? rb : nan;
+    qa = __ddiv_rn(hx, ra);
+    qb = __ddiv_rn(hx, rb);
+    qba = __ddiv_rn(hxb, ra);
+    qbb = __ddiv_rn(hxb, rb);
+  }
+  __device__ __forceinline__ double in(double f, bool &miss) const {
+    const bool isa = f == ka;
+    miss |= !(isa || f == kb);
+    return isa ? qa : qb;
+  }
+  __device__ __forceinline__ double bnd(double f, bool &miss) const {
+    const bool isa = f == ka;
+    miss |= !(isa || f == kb);
+    return isa ? qba : qbb;
+  }
+};
+
+__global__ void __launch_bounds__(kThreads, 2)
+    km_assemble_mix(int nx, int ny, int nz, int KQ, int LEN, double h, int4 bc03, int2 bc45,
+                    const double *__restrict__ col, double ra, double rb, const uint8_t *__restrict__ solid,
+                    double *__restrict__ C, double *__restrict__ W, double *__restrict__ S,
+                    double *__restrict__ B, uint8_t *__restrict__ aflag) {
+  __shared__ double sm[2][kMarchSmA];
+  __shared__ uint8_t ss[2][kMarchSmA];
+  const int bc[6] = {bc03.x, bc03.y, bc03.z, bc03.w, bc45.x, bc45.y};
+  const int TJ = kThreads / KQ, WD = 4 * KQ + 2;
+  const int tx = (int)threadIdx.x % KQ, ty = (int)threadIdx.x / KQ;
+  const int k = (int)blockIdx.x * 4 * KQ + 4 * tx, j = (int)blockIdx.y * TJ + ty;
+  const int i0 = (int)blockIdx.z * LEN, i1 = min(nx, i0 + LEN);
+  const bool own = j < ny && k < nz;
+  const uint32_t SI = (uint32_t)ny * nz, SJ = (uint32_t)nz;
+  const double hh = __dmul_rn(h, h);
+  const double hx = __ddiv_rn(hh, h);
+  const double hxb = __ddiv_rn(hh, __dmul_rn(0.5, h));
   const bool hc = col != nullptr;
-  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < G.n / kFlowV; g += gridDim.x * blockDim.x) {
-    const uint32_t p = g * kFlowV;
-    const Pos q = G.pos(p);
-    double pc[4], mc[4];
-    ld4d(pr, p, pc);
-    mix4(col, ra, rb, p, mc);
-    uchar4 sc = make_uchar4(0, 0, 0, 0), sw = sc, ss = sc;
-    uint8_t skm = 0;
-    if (body) {
-      sc = ld4b(solid, p);
-      if (q.i > 0) sw = ld4b(solid, p - SI);
-      if (q.j > 0) ss = ld4b(solid, p - SJ);
-      if (q.k > 0) skm = solid[p - 1];
-    }
-    if (q.i > 0) {
-      double pw[4], mw[4], uo[4];
-      ld4d(pr, p - SI, pw);
-      mix4(col, ra, rb, p - SI, mw);
-      ld4d(u, p, uo);
-#pragma unroll
-      for (int m = 0; m < 4; ++m)
-        if (!(body && (byte_of(sc, m) || byte_of(sw, m))))
-          uo[m] = __dadd_rn(uo[m], project_increment(pw[m], pc[m], face_of(hc, ra, mc[m], mw[m]), dt, h, body));
-      st4d(u, p, uo);
-    }
-    if (q.j > 0) {
-      const uint32_t iv = ((uint32_t)q.i * (ny + 1) + q.j) * nz + q.k;
-      double ps[4], mS[4], vo[4];
-      ld4d(pr, p - SJ, ps);
-      mix4(col, ra, rb, p - SJ, mS);
-      ld4d(v, iv, vo);
-#pragma unroll
-      for (int m = 0; m < 4; ++m)
-        if (!(body && (byte_of(sc, m) || byte_of(ss, m))))
-          vo[m] = __dadd_rn(vo[m], project_increment(ps[m], pc[m], face_of(hc, ra, mc[m], mS[m]), dt, h, body));
-      st4d(v, iv, vo);
-    }
-    if (nz > 1) {
-      const long long iw = ((long long)q.i * ny + q.j) * (nz + 1) + q.k;
-      const double pkm = q.k > 0 ? pr[p - 1] : 0.0;
-      const double mkm = q.k > 0 ? mix1(col, ra, rb, (long long)p - 1) : 0.0;
+  const QuotCache Q(hx, ra, rb);
+  const QuotOnly QC(hx, hxb, ra, rb);
+  const uchar4 z4 = make_uchar4(0, 0, 0, 0);
+  // shared-memory index of the thread's first cell; the halo rows (j0 - 1
+  // and j0 + TJ) are loaded by the threads of the first and last row, the
+  // halo columns (k0 - 1, k0 + 4 KQ) by the first and last thread of a row
+  const int c0 = (ty + 1) * WD + 4 * tx + 1;
+  const int hj = ty == 0 ? j - 1 : (ty == TJ - 1 ? j + 1 : -1);
+  const int hc0 = ty == 0 ? 4 * tx + 1 : (TJ + 1) * WD + 4 * tx + 1;
+  auto stage = [&](int ip, int b, bool halo, double (&mq)[4], uchar4 &sq) {
+    const uint32_t base = (uint32_t)ip * SI;
+    if (own) {
+      const uint32_t p = base + (uint32_t)j * SJ + (uint32_t)k;
+      mix4(col, ra, rb, p, mq);
+      sq = solid ? ld4b(solid, p) : z4;
+      if (!halo) return;
 #pragma unroll
       for (int m = 0; m < 4; ++m) {
-        const int kk = q.k + m;
-        if (kk == 0) continue;
-        const uint8_t sbm = m > 0 ? byte_of(sc, m - 1) : skm;
-        if (body && (byte_of(sc, m) || sbm)) continue;
-        const double pb = m > 0 ? pc[m - 1] : pkm;
-        const double mb = m > 0 ? mc[m - 1] : mkm;
-        w[iw + m] = __dadd_rn(w[iw + m], project_increment(pb, pc[m], face_of(hc, ra, mc[m], mb), dt, h, body));
+        sm[b][c0 + m] = mq[m];
+        ss[b][c0 + m] = byte_of(sq, m);
+      }
+      if (tx == 0 && k > 0) {
+        sm[b][c0 - 1] = mix1(col, ra, rb, (long long)p - 1);
+        ss[b][c0 - 1] = solid ? solid[p - 1] : 0;
+      }
+      if (tx == KQ - 1 && k + 4 < nz) {
+        sm[b][c0 + 4] = mix1(col, ra, rb, (long long)p + 4);
+        ss[b][c0 + 4] = solid ? solid[p + 4] : 0;
       }
     }
+    if (halo && hj >= 0 && hj < ny && k < nz) {
+      const uint32_t ph = base + (uint32_t)hj * SJ + (uint32_t)k;
+      double hq[4];
+      mix4(col, ra, rb, ph, hq);
+      const uchar4 hs = solid ? ld4b(solid, ph) : z4;
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        sm[b][hc0 + m] = hq[m];
+        ss[b][hc0 + m] = byte_of(hs, m);
+      }
+    }
+  };
+  double mC[4], mN[4], aW[4] = {0.0, 0.0, 0.0, 0.0};
+  uchar4 sP = z4, sC = z4, sN = z4;
+  stage(i0, 0, true, mC, sC);
+  if (own && i0 > 0) {
+    double mP[4];
+    const uint32_t p = (uint32_t)(i0 - 1) * SI + (uint32_t)j * SJ + (uint32_t)k;
+    mix4(col, ra, rb, p, mP);
+    sP = solid ? ld4b(solid, p) : z4;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) aW[m] = Q(face_of(hc, ra, mC[m], mP[m]));
+  }
+  __syncthreads();
+  for (int i = i0; i < i1; ++i) {
+    const int b = (i - i0) & 1;
+    if (i + 1 < nx) stage(i + 1, b ^ 1, i + 1 < i1, mN, sN);
+    if (own) {
+      const uint32_t p = (uint32_t)i * SI + (uint32_t)j * SJ + (uint32_t)k;
+      const double mkm = k > 0 ? sm[b][c0 - 1] : 0.0;
+      const double mkp = k + 4 < nz ? sm[b][c0 + 4] : 0.0;
+      const uint8_t skm = k > 0 ? ss[b][c0 - 1] : 0, skp = k + 4 < nz ? ss[b][c0 + 4] : 0;
+      // A quad away from the i and j walls whose cells and neighbours all
+      // carry the same solid flag needs none of the wall and body rules but
+      // the k walls' (a solid quad only scales c by 1e-12 and drops its
+      // couplings): the same values in far fewer instructions. Rows run
+      // along k, so a warp's quads mostly agree on the branch.
+      bool fast = i > 0 && i < nx - 1 && j > 0 && j < ny - 1;
+      const uint8_t sp0 = sC.x;
+      if (solid && fast) {
+        const uint32_t w4 = 0x01010101u * sp0;
+        bool same = *reinterpret_cast<const uint32_t *>(&sC) == w4 &&
+                    *reinterpret_cast<const uint32_t *>(&sP) == w4 &&
+                    *reinterpret_cast<const uint32_t *>(&sN) == w4 && (k == 0 || skm == sp0) &&
+                    (k + 4 == nz || skp == sp0);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) same = same && ss[b][c0 + m - WD] == sp0 && ss[b][c0 + m + WD] == sp0;
+        fast = same;
+      }
+      if (fast) {
+        // the quad with quotients from qin (interior faces) and qbnd (the k
+        // walls' faces)
+        double e[4], oc[4], ow[4], os[4], ob[4];
+        auto quad = [&](auto &&qin, auto &&qbnd) {
+          double bfx[5];
+          bfx[0] = k == 0 ? qbnd(face_of(hc, ra, mC[0], mC[0])) : qin(face_of(hc, ra, mC[0], mkm));
+#pragma unroll
+          for (int m = 1; m < 4; ++m) bfx[m] = qin(face_of(hc, ra, mC[m], mC[m - 1]));
+          bfx[4] = k + 4 == nz ? qbnd(face_of(hc, ra, mC[3], mC[3])) : qin(face_of(hc, ra, mkp, mC[3]));
+#pragma unroll
+          for (int m = 0; m < 4; ++m) {
+            const double a0 = aW[m];
+            const double a1 = qin(face_of(hc, ra, mN[m], mC[m]));
+            const double a2 = qin(face_of(hc, ra, mC[m], sm[b][c0 + m - WD]));
+            const double a3 = qin(face_of(hc, ra, sm[b][c0 + m + WD], mC[m]));
+            double a4 = bfx[m];
+            const double a5 = bfx[m + 1];
+            double c = __dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(a0, a1), a2), a3), a4), a5);
+            if (m == 0 && k == 0) {
+              if (bc[4] == PBG_BC_NEUMANN_) { c = __dsub_rn(c, a4); a4 = 0.0; }
+              else if (bc[4] == PBG_BC_DIRICHLET_) a4 = 0.0;
+            }
+            if (m == 3 && k + 4 == nz && bc[5] == PBG_BC_NEUMANN_) c = __dsub_rn(c, a5);
+            e[m] = a1;
+            if (sp0) {
+              c = __dmul_rn(c, 1.0e-12);
+              a4 = 0.0;
+            }
+            oc[m] = c; ow[m] = sp0 ? 0.0 : a0; os[m] = sp0 ? 0.0 : a2; ob[m] = a4;
+          }
+        };
+        bool miss = false;
+        quad([&](double f) { return QC.in(f, miss); }, [&](double f) { return QC.bnd(f, miss); });
+        // an interface face: the quad again, dividing where the cache misses
+        if (miss) quad([&](double f) { return Q(f); }, [&](double f) { return __ddiv_rn(hxb, f); });
+#pragma unroll
+        for (int m = 0; m < 4; ++m) aW[m] = e[m];
+        st4d(C, p, oc);
+        st4d(W, p, ow);
+        st4d(S, p, os);
+        st4d(B, p, ob);
+        const uint8_t fl = sp0 ? 0 : 1;
+        *reinterpret_cast<uchar4 *>(aflag + p) = make_uchar4(fl, fl, fl, fl);
+      } else {
+        double bf[5];
+        bf[0] = k == 0 ? __ddiv_rn(hxb, face_of(hc, ra, mC[0], mC[0])) : Q(face_of(hc, ra, mC[0], mkm));
+#pragma unroll
+        for (int m = 1; m < 4; ++m) bf[m] = Q(face_of(hc, ra, mC[m], mC[m - 1]));
+        bf[4] = k + 4 == nz ? __ddiv_rn(hxb, face_of(hc, ra, mC[3], mC[3])) : Q(face_of(hc, ra, mkp, mC[3]));
+        uchar4 af;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const int kk = k + m;
+          const double ms_ = sm[b][c0 + m - WD], mn_ = sm[b][c0 + m + WD];
+          double a[6];
+          a[0] = i > 0 ? aW[m] : __ddiv_rn(hxb, face_of(hc, ra, mC[m], mC[m]));
+          a[1] = i < nx - 1 ? Q(face_of(hc, ra, mN[m], mC[m])) : __ddiv_rn(hxb, face_of(hc, ra, mC[m], mC[m]));
+          aW[m] = a[1];  // the west face of the next plane's cell
+          a[2] = j > 0 ? Q(face_of(hc, ra, mC[m], ms_)) : __ddiv_rn(hxb, face_of(hc, ra, mC[m], mC[m]));
+          a[3] = j < ny - 1 ? Q(face_of(hc, ra, mn_, mC[m])) : __ddiv_rn(hxb, face_of(hc, ra, mC[m], mC[m]));
+          a[4] = bf[m];
+          a[5] = bf[m + 1];
+          double c = a[0];
+#pragma unroll
+          for (int f = 1; f < 6; ++f) c = __dadd_rn(c, a[f]);
+          const uint8_t sp = byte_of(sC, m);
+          if (solid) {
+            const uint8_t sbm = m > 0 ? byte_of(sC, m - 1) : skm, stp = m < 3 ? byte_of(sC, m + 1) : skp;
+            if (i > 0 && byte_of(sP, m) != sp) a[0] = 0.0;
+            if (i < nx - 1 && byte_of(sN, m) != sp) a[1] = 0.0;
+            if (j > 0 && ss[b][c0 + m - WD] != sp) a[2] = 0.0;
+            if (j < ny - 1 && ss[b][c0 + m + WD] != sp) a[3] = 0.0;
+            if (kk > 0 && sbm != sp) a[4] = 0.0;
+            if (kk < nz - 1 && stp != sp) a[5] = 0.0;
+            if (!sp) {
+              c = a[0];
+#pragma unroll
+              for (int f = 1; f < 6; ++f) c = __dadd_rn(c, a[f]);
+            }
+          }
+          const bool onb[6] = {i == 0, i == nx - 1, j == 0, j == ny - 1, kk == 0, kk == nz - 1};
+#pragma unroll
+          for (int f = 0; f < 6; ++f) {
+            if (!onb[f] || bc[f] != PBG_BC_NEUMANN_) continue;
+            c = __dsub_rn(c, a[f]);
+            a[f] = 0.0;
+          }
+#pragma unroll
+          for (int f = 0; f < 6; ++f)
+            if (onb[f] && bc[f] == PBG_BC_DIRICHLET_) a[f] = 0.0;
+          if (sp) {
+            c = __dmul_rn(c, 1.0e-12);
+#pragma unroll
+            for (int f = 0; f < 6; ++f) a[f] = 0.0;
+          }
+          // one cell at a time (8-byte stores; the four of a thread fill
+          // whole sectors together) keeps the outputs out of registers
+          C[p + m] = c;
+          W[p + m] = a[0];
+          S[p + m] = a[2];
+          B[p + m] = a[4];
+          const uint8_t fl = sp ? 0 : 1;
+          if (m == 0) af.x = fl; else if (m == 1) af.y = fl; else if (m == 2) af.z = fl; else af.w = fl;
+        }
+        *reinterpret_cast<uchar4 *>(aflag + p) = af;
+      }
+    }
+    __syncthreads();
+    sP = sC;
+    sC = sN;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) mC[m] = mN[m];
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    km_project(int nx, int ny, int nz, int KQ, int LEN, double h, double dt, const double *__restrict__ pr,
+               const double *__restrict__ col, double ra, double rb, const uint8_t *__restrict__ solid,
+               double *__restrict__ u, double *__restrict__ v, double *__restrict__ w) {
+  __shared__ double sq_[2][kMarchSmP], sm_[2][kMarchSmP];
+  __shared__ uint8_t ss_[2][kMarchSmP];
+  const int TJ = kThreads / KQ, WD = 4 * KQ + 1;
+  const int tx = (int)threadIdx.x % KQ, ty = (int)threadIdx.x / KQ;
+  const int k = (int)blockIdx.x * 4 * KQ + 4 * tx, j = (int)blockIdx.y * TJ + ty;
+  const int i0 = (int)blockIdx.z * LEN, i1 = min(nx, i0 + LEN);
+  const bool own = j < ny && k < nz;
+  const uint32_t SI = (uint32_t)ny * nz, SJ = (uint32_t)nz;
+  const bool body = solid != nullptr;
+  const bool hc = col != nullptr;
+  const PhaseDiv D(ra, rb, h);
+  const ProjFast PF(D);
+  const uchar4 z4 = make_uchar4(0, 0, 0, 0);
+  // own cells from index c0; the halo row j0 - 1 (row 0) is loaded by the
+  // threads of the first row, the halo column k0 - 1 (column 0) by the first
+  // thread of each row
+  const int c0 = (ty + 1) * WD + 4 * tx + 1;
+  double pP[4] = {0.0, 0.0, 0.0, 0.0}, mP[4] = {0.0, 0.0, 0.0, 0.0};
+  uchar4 sP = z4;
+  if (own && i0 > 0) {
+    const uint32_t p = (uint32_t)(i0 - 1) * SI + (uint32_t)j * SJ + (uint32_t)k;
+    ld4d(pr, p, pP);
+    mix4(col, ra, rb, p, mP);
+    sP = body ? ld4b(solid, p) : z4;
+  }
+  for (int i = i0; i < i1; ++i) {
+    const int b = (i - i0) & 1;
+    const uint32_t base = (uint32_t)i * SI;
+    const uint32_t p = base + (uint32_t)j * SJ + (uint32_t)k;
+    double pC[4] = {0.0, 0.0, 0.0, 0.0}, mC[4] = {0.0, 0.0, 0.0, 0.0};
+    uchar4 sC = z4;
+    if (own) {
+      ld4d(pr, p, pC);
+      mix4(col, ra, rb, p, mC);
+      if (body) sC = ld4b(solid, p);
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        sq_[b][c0 + m] = pC[m];
+        sm_[b][c0 + m] = mC[m];
+        ss_[b][c0 + m] = byte_of(sC, m);
+      }
+      if (tx == 0 && k > 0) {
+        sq_[b][c0 - 1] = pr[p - 1];
+        sm_[b][c0 - 1] = mix1(col, ra, rb, (long long)p - 1);
+        ss_[b][c0 - 1] = body ? solid[p - 1] : 0;
+      }
+    }
+    if (ty == 0 && j > 0 && k < nz) {
+      const uint32_t ph = p - SJ;
+      double hp[4], hm[4];
+      ld4d(pr, ph, hp);
+      mix4(col, ra, rb, ph, hm);
+      const uchar4 hs = body ? ld4b(solid, ph) : z4;
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        sq_[b][4 * tx + 1 + m] = hp[m];
+        sm_[b][4 * tx + 1 + m] = hm[m];
+        ss_[b][4 * tx + 1 + m] = byte_of(hs, m);
+      }
+    }
+    __syncthreads();
+    // A quad of solid cells updates no face at all. A quad with all three
+    // lower neighbours inside the domain and no solid cell in it or below it
+    // on any axis updates every face, with both divisions by Markstein's
+    // correction when every face density is a pure phase's; a face it does
+    // not cover sends the quad to the general code.
+    bool fast = own && i > 0 && j > 0 && k > 0;
+    bool skip = false;
+    if (body && own) {
+      skip = sC.x && sC.y && sC.z && sC.w;
+      if (fast) {
+        uint32_t any = *reinterpret_cast<const uint32_t *>(&sC) | *reinterpret_cast<const uint32_t *>(&sP) |
+                       ss_[b][c0 - 1];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) any |= ss_[b][c0 + m - WD];
+        fast = any == 0;
+      }
+    }
+    if (skip) {
+    } else if (fast) {
+      const uint32_t iv = ((uint32_t)i * (ny + 1) + j) * nz + k;
+      const long long iw = ((long long)i * ny + j) * (nz + 1) + k;
+      bool miss = false;
+      double uo[4], vo[4], wo[4];
+      ld4d(u, p, uo);
+      ld4d(v, iv, vo);
+#pragma unroll
+      for (int m = 0; m < 4; ++m) wo[m] = w[iw + m];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        uo[m] = __dadd_rn(uo[m], PF.inc(pP[m], pC[m], face_of(hc, ra, mC[m], mP[m]), dt, body, miss));
+        vo[m] = __dadd_rn(vo[m], PF.inc(sq_[b][c0 + m - WD], pC[m], face_of(hc, ra, mC[m], sm_[b][c0 + m - WD]),
+                                        dt, body, miss));
+        const double pb = m > 0 ? pC[m - 1] : sq_[b][c0 - 1];
+        const double mb = m > 0 ? mC[m - 1] : sm_[b][c0 - 1];
+        wo[m] = __dadd_rn(wo[m], PF.inc(pb, pC[m], face_of(hc, ra, mC[m], mb), dt, body, miss));
+      }
+      if (!miss) {
+        st4d(u, p, uo);
+        st4d(v, iv, vo);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) w[iw + m] = wo[m];
+      }
+      fast = !miss;
+    }
+    if (!skip && !fast && own) {
+      if (i > 0) {
+        double uo[4];
+        ld4d(u, p, uo);
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+          if (!(body && (byte_of(sC, m) || byte_of(sP, m))))
+            uo[m] = __dadd_rn(uo[m], project_increment_k(pP[m], pC[m], face_of(hc, ra, mC[m], mP[m]), dt, D, body));
+        st4d(u, p, uo);
+      }
+      if (j > 0) {
+        const uint32_t iv = ((uint32_t)i * (ny + 1) + j) * nz + k;
+        double vo[4];
+        ld4d(v, iv, vo);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const double ps = sq_[b][c0 + m - WD], mS = sm_[b][c0 + m - WD];
+          if (!(body && (byte_of(sC, m) || ss_[b][c0 + m - WD])))
+            vo[m] = __dadd_rn(vo[m], project_increment_k(ps, pC[m], face_of(hc, ra, mC[m], mS), dt, D, body));
+        }
+        st4d(v, iv, vo);
+      }
+      if (nz > 1) {
+        const long long iw = ((long long)i * ny + j) * (nz + 1) + k;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const int kk = k + m;
+          if (kk == 0) continue;
+          const uint8_t sbm = m > 0 ? byte_of(sC, m - 1) : ss_[b][c0 - 1];
+          if (body && (byte_of(sC, m) || sbm)) continue;
+          const double pb = m > 0 ? pC[m - 1] : sq_[b][c0 - 1];
+          const double mb = m > 0 ? mC[m - 1] : sm_[b][c0 - 1];
+          w[iw + m] = __dadd_rn(w[iw + m], project_increment_k(pb, pC[m], face_of(hc, ra, mC[m], mb), dt, D, body));
+        }
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      pP[m] = pC[m];
+      mP[m] = mC[m];
+    }
+    sP = sC;
   }
 }
 

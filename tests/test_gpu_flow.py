@@ -23,7 +23,7 @@ pytestmark = pytest.mark.gpu
 
 CASES = [(0, dict(n=16)), (0, dict(n=12)), (1, dict(n=20, nb=3, rmin=2.0, rmax=3.0, rc=4.0)),
          (2, dict(index=0, n2d=1, s2=(32, 32))), (2, dict(index=3, n2d=1, s2=(20, 40))),
-         # nz % 4 == 0 grids run the row-vector kernels, others the one-cell ones
+         # nz % 4 == 0 grids run the 4-cells-a-thread kernels, others the one-cell ones
          (1, dict(n=28, nb=4, rmin=2.0, rmax=4.0, rc=6.0)), (0, dict(n=13))]
 
 
@@ -74,6 +74,55 @@ def test_divergence_and_project_bit_exact(engine, oracle, kind, kw, dt):
                 uu, vv, ww = u.copy(), v.copy(), w.copy()
                 s.project(p, c, ra, rb, dt, uu, vv, ww, solid=sol)
                 ru, rv, rw = flow.project(P.dims, P.h, dt, p, c, ra, rb, u, v, w, solid=sol)
+                assert np.array_equal(uu, ru) and np.array_equal(vv, rv) and np.array_equal(ww, rw)
+
+
+# Grids whose marching tiles are partial or several: k rows longer than one
+# 256-cell tile (264), j beyond one tile of rows, i over several walks, and
+# odd extents; a colour field with two ramped bubbles, a solid box, spacings
+# that are not powers of two and densities 1000 and 0.8.
+TILE_DIMS = [(37, 41, 264), (19, 9, 12), (33, 70, 20)]
+
+
+def _tile_state(dims, seed=11):
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = dims
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    col = np.ones(dims)
+    for ci, cj, ck, r in ((0.3, 0.4, 0.5, 0.25), (0.7, 0.7, 0.2, 0.2)):
+        d = np.sqrt((i - ci * nx) ** 2 + (j - cj * ny) ** 2 + (k - ck * nz) ** 2)
+        col = np.minimum(col, np.clip((d - r * min(dims)) / 3.0 + 0.5, 0.0, 1.0))
+    solid = np.zeros(dims, dtype=np.uint8)
+    solid[nx // 2:nx // 2 + 3, ny // 3:ny // 3 + 4, :max(1, nz // 4)] = 1
+    u = rng.uniform(-0.5, 0.5, (nx + 1, ny, nz))
+    v = rng.uniform(-0.5, 0.5, (nx, ny + 1, nz))
+    w = rng.uniform(-0.5, 0.5, (nx, ny, nz + 1))
+    u[0] = u[-1] = 0.0
+    v[:, 0] = v[:, -1] = 0.0
+    w[:, :, 0] = w[:, :, -1] = 0.0
+    return col, solid.reshape(-1), u, v, w, 1.0 / (nx + 0.5)
+
+
+@pytest.mark.parametrize("dims", TILE_DIMS)
+def test_flow_tiles_bit_exact(engine, dims):
+    col, solid, u, v, w, h = _tile_state(dims)
+    ra, rb = 1000.0, 0.8
+    bc = [0, 0, 0, 0, 0, 1]
+    N = int(np.prod(dims))
+    p = np.random.default_rng(4).standard_normal(N)
+    with engine.Session(*dims, h, bc=bc) as s:
+        for sol in (None, solid):
+            s.assemble_mix(col, ra, rb, solid=sol)
+            M = s.download_matrix()
+            ref = flow.assemble_mix(dims, h, bc, col, ra, rb, solid=sol)
+            for key in "cwesnbt":
+                assert np.array_equal(M[key], ref[key]), key
+            rhs = s.divergence(u, v, w, 0.0037, np.zeros(N), solid=sol)
+            assert np.array_equal(rhs, flow.divergence(dims, h, 0.0037, u, v, w, solid=sol))
+            for c in (col, None):
+                uu, vv, ww = u.copy(), v.copy(), w.copy()
+                s.project(p, c, ra, rb, 0.0037, uu, vv, ww, solid=sol)
+                ru, rv, rw = flow.project(dims, h, 0.0037, p, c, ra, rb, u, v, w, solid=sol)
                 assert np.array_equal(uu, ru) and np.array_equal(vv, rv) and np.array_equal(ww, rw)
 
 
