@@ -113,7 +113,14 @@ struct BCtx {
   T omega;
 };
 
-#define BTILE_LOOP(C, l, t) for (int t = (C).lbeg[l] + (int)blockIdx.x; t < (C).lbeg[(l) + 1]; t += (int)gridDim.x)
+// Tiles of level l, grid-strided, with the next tile's record loaded one
+// iteration ahead: a CTA's chain of dependent descriptor loads (tile ->
+// slot state and problem -> arrays) then starts from a record already in
+// registers. `continue` in the body moves to the next tile.
+#define BTILE_FOR(C, l, t, tl)                                                                     \
+  for (int t = (C).lbeg[l] + (int)blockIdx.x, e_##t = (C).lbeg[(l) + 1]; t < e_##t; t = e_##t)   \
+    for (BTile tl = (C).tiles[t], n_##t = tl; t < e_##t; t += (int)gridDim.x, tl = n_##t)          \
+      if (n_##t = t + (int)gridDim.x < e_##t ? (C).tiles[t + (int)gridDim.x] : tl, true)
 #define BCELL_LOOP(T_, p) for (uint32_t p = (T_).p0 + threadIdx.x; p < (T_).p0 + (T_).n; p += blockDim.x)
 
 // Is slot s running its inner solve (this launch's work applies)?
@@ -210,8 +217,7 @@ __device__ bool b_reduce(const BCtx<T> &C, int l, int t, int slot, double (&v)[K
 // keep the uploaded one).
 template <typename T>
 __global__ void kb_assemble(BCtx<T> C) {
-  BTILE_LOOP(C, 0, t) {
-    const BTile tl = C.tiles[t];
+  BTILE_FOR(C, 0, t, tl) {
     if (!C.st[tl.slot].setup) continue;
     const BProb<T> &P = C.prob[tl.slot];
     if (!P.rho) continue;
@@ -231,8 +237,7 @@ __global__ void kb_assemble(BCtx<T> C) {
 // k_galerkin), FP64.
 template <typename T>
 __global__ void kb_galerkin(BCtx<T> C, int l) {
-  BTILE_LOOP(C, l, t) {
-    const BTile tl = C.tiles[t];
+  BTILE_FOR(C, l, t, tl) {
     if (!C.st[tl.slot].setup) continue;
     const BProb<T> &P = C.prob[tl.slot];
     const BLev<T> &F = P.L[l - 1], &V = P.L[l];
@@ -266,8 +271,7 @@ __global__ void kb_finish(BCtx<T> C, int l) {
     if (l == 0) {
       // padded level 0: compact FP64 in, padded T out (2-D: the j coupling
       // goes to the fast axis, b); pad cells keep their zeros
-      BTILE_LOOP(C, 0, t) {
-        const BTile tl = C.tiles[t];
+      BTILE_FOR(C, 0, t, tl) {
         if (!C.st[tl.slot].setup) continue;
         const BProb<T> &P = C.prob[tl.slot];
         const BLev<T> &V = P.L[0];
@@ -295,8 +299,7 @@ __global__ void kb_finish(BCtx<T> C, int l) {
       return;
     }
   }
-  BTILE_LOOP(C, l, t) {
-    const BTile tl = C.tiles[t];
+  BTILE_FOR(C, l, t, tl) {
     if (!C.st[tl.slot].setup) continue;
     const BLev<T> &V = C.prob[tl.slot].L[l];
     const EMat<T> &A = V.A;
@@ -383,8 +386,7 @@ __global__ void kb_dense_inverse(BCtx<T> C, double rel_tol) {
 // x += e for slots whose inner solve just finished.
 template <typename T>
 __global__ void kb_outer_corr(BCtx<T> C) {
-  BTILE_LOOP(C, 0, t) {
-    const BTile tl = C.tiles[t];
+  BTILE_FOR(C, 0, t, tl) {
     const BState &S = C.st[tl.slot];
     if (!(S.phase == BP_RUN && S.f.done)) continue;
     const BProb<T> &P = C.prob[tl.slot];
@@ -401,8 +403,7 @@ __global__ void kb_outer_corr(BCtx<T> C) {
 // solve_fp64).
 template <typename T>
 __global__ void kb_outer_resid(BCtx<T> C) {
-  BTILE_LOOP(C, 0, t) {
-    const BTile tl = C.tiles[t];
+  BTILE_FOR(C, 0, t, tl) {
     BState &S = C.st[tl.slot];
     if (!(S.phase == BP_INIT || (S.phase == BP_RUN && S.f.done))) continue;
     const BProb<T> &P = C.prob[tl.slot];
@@ -745,8 +746,7 @@ __device__ __forceinline__ void vgroup_jac(const BProb<T> &P, const BLev<T> &V, 
 // ---------------------------------------------------------------- K-cycle: tile kernels
 template <typename T>
 __global__ void BPAD_BOUNDS kb_jac2(BCtx<T> C, int l, int kc) {
-  BTILE_LOOP(C, l, t) {
-    const BTile tl = C.tiles[t];
+  BTILE_FOR(C, l, t, tl) {
     const BState &S = C.st[tl.slot];
     const BProb<T> &P = C.prob[tl.slot];
     if (!b_tile_level(S, P, l)) continue;
@@ -765,8 +765,7 @@ __global__ void BPAD_BOUNDS kb_jac2(BCtx<T> C, int l, int kc) {
 // GPU, so the eight-lane form is kept for the single-CTA tail.
 template <typename T>
 __global__ void kb_restrict(BCtx<T> C, int l, int kc) {
-  BTILE_LOOP(C, l + 1, t) {
-    const BTile tl = C.tiles[t];
+  BTILE_FOR(C, l + 1, t, tl) {
     const BState &S = C.st[tl.slot];
     const BProb<T> &P = C.prob[tl.slot];
     if (!b_tile_level(S, P, l)) continue;
@@ -784,8 +783,7 @@ __global__ void kb_restrict(BCtx<T> C, int l, int kc) {
 template <typename T>
 __global__ void BPAD_BOUNDS kb_resid0(BCtx<T> C) {
   if constexpr (kBPad<T>) {
-    BTILE_LOOP(C, 0, t) {
-      const BTile tl = C.tiles[t];
+    BTILE_FOR(C, 0, t, tl) {
       const BState &S = C.st[tl.slot];
       const BProb<T> &P = C.prob[tl.slot];
       if (!b_tile_level(S, P, 0)) continue;
@@ -810,8 +808,7 @@ __global__ void kb_dense(BCtx<T> C, int L) {
 
 template <typename T>
 __global__ void BPAD_BOUNDS kb_prolong_jac(BCtx<T> C, int l, int kc) {
-  BTILE_LOOP(C, l, t) {
-    const BTile tl = C.tiles[t];
+  BTILE_FOR(C, l, t, tl) {
     const BState &S = C.st[tl.slot];
     const BProb<T> &P = C.prob[tl.slot];
     if (!b_tile_level(S, P, l)) continue;
@@ -832,8 +829,7 @@ __global__ void BPAD_BOUNDS kb_prolong_jac(BCtx<T> C, int l, int kc) {
 // previous FCG iteration) into the slot's FCG scalars.
 template <typename T>
 __global__ void BPAD_BOUNDS kb_jac(BCtx<T> C, int l, int kc) {
-  BTILE_LOOP(C, l, t) {
-    const BTile tl = C.tiles[t];
+  BTILE_FOR(C, l, t, tl) {
     BState &S = C.st[tl.slot];
     const BProb<T> &P = C.prob[tl.slot];
     if (!b_tile_level(S, P, l)) continue;
@@ -863,8 +859,7 @@ __global__ void BPAD_BOUNDS kb_jac(BCtx<T> C, int l, int kc) {
 
 template <typename T>
 __global__ void kb_kc_q1(BCtx<T> C, int l) {
-  BTILE_LOOP(C, l, t) {
-    const BTile tl = C.tiles[t];
+  BTILE_FOR(C, l, t, tl) {
     BState &S = C.st[tl.slot];
     const BProb<T> &P = C.prob[tl.slot];
     if (!b_tile_level(S, P, l)) continue;
@@ -877,8 +872,7 @@ __global__ void kb_kc_q1(BCtx<T> C, int l) {
 
 template <typename T>
 __global__ void kb_kc_q2(BCtx<T> C, int l) {
-  BTILE_LOOP(C, l, t) {
-    const BTile tl = C.tiles[t];
+  BTILE_FOR(C, l, t, tl) {
     BState &S = C.st[tl.slot];
     const BProb<T> &P = C.prob[tl.slot];
     if (!b_tile_level(S, P, l)) continue;
@@ -1008,8 +1002,7 @@ __global__ void __launch_bounds__(kBThreadsMax) kb_tail(BCtx<T> C, int l) {
 // p = z - beta p_old, q = A p, alpha = p.r / p.q (k_fcg_pq)
 template <typename T>
 __global__ void BPAD_BOUNDS kb_fcg_pq(BCtx<T> C) {
-  BTILE_LOOP(C, 0, t) {
-    const BTile tl = C.tiles[t];
+  BTILE_FOR(C, 0, t, tl) {
     BState &S = C.st[tl.slot];
     if (!b_running(S)) continue;
     const BProb<T> &P = C.prob[tl.slot];
@@ -1073,8 +1066,7 @@ __global__ void BPAD_BOUNDS kb_fcg_pq(BCtx<T> C) {
 // x += alpha p, r -= alpha q; inner convergence (k_fcg_xr)
 template <typename T>
 __global__ void BPAD_BOUNDS kb_fcg_xr(BCtx<T> C) {
-  BTILE_LOOP(C, 0, t) {
-    const BTile tl = C.tiles[t];
+  BTILE_FOR(C, 0, t, tl) {
     BState &S = C.st[tl.slot];
     if (!b_running(S)) continue;
     const BProb<T> &P = C.prob[tl.slot];
