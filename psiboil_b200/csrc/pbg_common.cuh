@@ -171,12 +171,20 @@ template <typename T>
 __device__ __forceinline__ NbIdx nb_index(const MatView<T> &A, long long p, Pos q) {
   const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
   NbIdx o;
-  o.w = q.i > 0 ? p - SI : ((A.per & 1) ? p + (long long)(A.nx - 1) * SI : -1);
-  o.e = q.i < A.nx - 1 ? p + SI : ((A.per & 1) ? p - (long long)(A.nx - 1) * SI : -1);
-  o.s = q.j > 0 ? p - SJ : ((A.per & 2) ? p + (long long)(A.ny - 1) * SJ : -1);
-  o.n = q.j < A.ny - 1 ? p + SJ : ((A.per & 2) ? p - (long long)(A.ny - 1) * SJ : -1);
-  o.b = q.k > 0 ? p - 1 : ((A.per & 4) ? p + (long long)(A.nz - 1) : -1);
-  o.t = q.k < A.nz - 1 ? p + 1 : ((A.per & 4) ? p - (long long)(A.nz - 1) : -1);
+  o.w = q.i > 0 ? p - SI : -1;
+  o.e = q.i < A.nx - 1 ? p + SI : -1;
+  o.s = q.j > 0 ? p - SJ : -1;
+  o.n = q.j < A.ny - 1 ? p + SJ : -1;
+  o.b = q.k > 0 ? p - 1 : -1;
+  o.t = q.k < A.nz - 1 ? p + 1 : -1;
+  if (A.per) {  // uniform: the wrap only for a periodic matrix
+    if ((A.per & 1) && q.i == 0) o.w = p + (long long)(A.nx - 1) * SI;
+    if ((A.per & 1) && q.i == A.nx - 1) o.e = p - (long long)(A.nx - 1) * SI;
+    if ((A.per & 2) && q.j == 0) o.s = p + (long long)(A.ny - 1) * SJ;
+    if ((A.per & 2) && q.j == A.ny - 1) o.n = p - (long long)(A.ny - 1) * SJ;
+    if ((A.per & 4) && q.k == 0) o.b = p + (long long)(A.nz - 1);
+    if ((A.per & 4) && q.k == A.nz - 1) o.t = p - (long long)(A.nz - 1);
+  }
   return o;
 }
 

@@ -240,6 +240,9 @@ __global__ void k_cg_pq(MatView<double> A, const double *__restrict__ r, double 
   }
 }
 
+// Seq = false: tree-order sums only (the split path), without the
+// exact-order reduction's code and shared memory
+template <bool Seq>
 __global__ void k_cg_xr(long long N, const double *__restrict__ mc, double *__restrict__ x,
                         double *__restrict__ r, const double *pA, const double *pB,
                         const double *__restrict__ qv, KrylovState *st, double *hist,
@@ -258,7 +261,7 @@ __global__ void k_cg_xr(long long N, const double *__restrict__ mc, double *__re
     v[1] += __dmul_rn(rv, __dmul_rn(rv, mc[p]));
   }
   double o[2];
-  if (grid_reduce<2>(v, part, count, o, st->seq, N)) {
+  if (grid_reduce<2>(v, part, count, o, Seq ? st->seq : nullptr, N)) {
     double res = res_of(o[0], st);
     st->res = res;
     if (hist && it < st->hist_cap) hist[it] = res;
@@ -1259,15 +1262,15 @@ void enqueue_ref_iters(const MatView<double> &A, double *x, int solver, int coun
       ic_apply(A, M, w.r.p, w.z.p, st, s);
       k_cg_rho<<<g, kThreads, 0, s>>>(N, w.r.p, w.z.p, st, P0, C0); note_launch();
       k_cg_pq<<<g, kThreads, 0, s>>>(A, w.r.p, w.pA.p, w.pB.p, w.q.p, st, P0, C0, w.z.p, w.mcd.p); note_launch();
-      k_cg_xr<<<g, kThreads, 0, s>>>(N, w.mcd.p, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1, 1); note_launch();
+      k_cg_xr<true><<<g, kThreads, 0, s>>>(N, w.mcd.p, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1, 1); note_launch();
     } else if (solver == 0 && !exact && A.nz % 2 == 0 && !A.per) {
       const int gq = grid_for(N / 2);
       k_cg_p<<<gq, kThreads, 0, s>>>(N, w.r.p, w.mcd.p, w.pA.p, st); note_launch();
       k_cg_q<<<gq, kThreads, 0, s>>>(A, Geo(A.nx, A.ny, A.nz), w.pA.p, w.q.p, st, P0, C0); note_launch();
-      k_cg_xr<<<g, kThreads, 0, s>>>(N, w.mcd.p, x, w.r.p, w.pA.p, w.pA.p, w.q.p, st, hist, P1, C1, 0); note_launch();
+      k_cg_xr<false><<<g, kThreads, 0, s>>>(N, w.mcd.p, x, w.r.p, w.pA.p, w.pA.p, w.q.p, st, hist, P1, C1, 0); note_launch();
     } else if (solver == 0) {
       k_cg_pq<<<g, kThreads, 0, s>>>(A, w.r.p, w.pA.p, w.pB.p, w.q.p, st, P0, C0, nullptr, w.mcd.p); note_launch();
-      k_cg_xr<<<g, kThreads, 0, s>>>(N, w.mcd.p, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1, 0); note_launch();
+      k_cg_xr<true><<<g, kThreads, 0, s>>>(N, w.mcd.p, x, w.r.p, w.pA.p, w.pB.p, w.q.p, st, hist, P1, C1, 0); note_launch();
     } else if (solver == 1) {
       k_bi_rho<<<g, kThreads, 0, s>>>(N, w.rt.p, w.r.p, st, P0, C0); note_launch();
       k_bi_p<<<g, kThreads, 0, s>>>(N, w.mcd.p, w.r.p, w.pA.p, w.v.p, w.ph.p, st, diag); note_launch();
