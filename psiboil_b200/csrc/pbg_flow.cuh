@@ -237,19 +237,22 @@ struct KnownDiv {
     const double m = fabs(b_);
     ok = m >= 0x1p-60 && m <= 0x1p60;
   }
-  // a / b
+  // a / b (a zero dividend: a b, the signed zero a / b is)
   __device__ __forceinline__ double operator()(double a) const {
     const double m = fabs(a);
     if (ok && m > 0x1p-900 && m < 0x1p900) {
       const double q0 = __dmul_rn(a, y);
       return __fma_rn(__fma_rn(-q0, b, a), y, q0);
     }
+    if (ok && m == 0.0) return __dmul_rn(a, b);
     return __ddiv_rn(a, b);
   }
   // a / d for any d: the corrected product when d is b (b nonzero, so d == b
-  // means the same bits), else the division
+  // means the same bits), else the division (a zero dividend over a finite
+  // nonzero d: a d, the same signed zero)
   __device__ __forceinline__ double by(double a, double d) const {
     if (d == b && ok) return (*this)(a);
+    if (a == 0.0 && d != 0.0 && isfinite(d)) return __dmul_rn(a, d);
     return __ddiv_rn(a, d);
   }
 };
@@ -275,10 +278,11 @@ __device__ __forceinline__ double project_increment_k(double pm, double pp, doub
 }
 
 // project_increment for the fast quads of the marching projection: both
-// divisions by Markstein's correction with no fallback; a face density that
-// is not a pure phase's, a dividend outside the range where the correction
-// is exact (+0 included, -0 not), or a divisor outside [2^-60, 2^60] sets
-// miss, and the quad is redone by the general code.
+// divisions by Markstein's correction with no fallback (exact for +0 too;
+// -0 would come out +0); a face density that is not a pure phase's, a
+// dividend outside the range where the correction is exact (+0 included,
+// -0 not), or a divisor outside [2^-60, 2^60] sets miss, and the quad is
+// redone by the general code.
 struct ProjFast {
   double ka, kb, ra, rb, ya, yb, h, yh;
   bool hok;
