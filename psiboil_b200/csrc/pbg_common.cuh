@@ -198,6 +198,11 @@ __device__ __forceinline__ Nb<T> coeffs(const MatView<T> &A, long long p, Pos q)
     o.e = A.e[p];
     o.n = A.n[p];
     o.t = A.t[p];
+  } else if (!A.per) {
+    const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
+    o.e = q.i < A.nx - 1 ? A.w[p + SI] : T(0);
+    o.n = q.j < A.ny - 1 ? A.s[p + SJ] : T(0);
+    o.t = q.k < A.nz - 1 ? A.b[p + 1] : T(0);
   } else {
     const NbIdx m = nb_index(A, p, q);
     o.e = m.e >= 0 ? A.w[m.e] : T(0);

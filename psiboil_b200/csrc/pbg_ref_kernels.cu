@@ -22,10 +22,18 @@ __device__ __forceinline__ double ld0(const double *x, long long p, bool ok) {
 template <typename XF>
 __device__ __forceinline__ double ref_ax(const MatView<double> &A, long long p, Pos q, XF xv) {
   Nb<double> a = coeffs(A, p, q);
-  const NbIdx m = nb_index(A, p, q);
-  double xw = m.w >= 0 ? xv(m.w) : 0.0, xe = m.e >= 0 ? xv(m.e) : 0.0;
-  double xs = m.s >= 0 ? xv(m.s) : 0.0, xn = m.n >= 0 ? xv(m.n) : 0.0;
-  double xb = m.b >= 0 ? xv(m.b) : 0.0, xt = m.t >= 0 ? xv(m.t) : 0.0;
+  double xw, xe, xs, xn, xb, xt;
+  if (!A.per) {  // uniform: the plain neighbour form unless the matrix is periodic
+    const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
+    xw = q.i > 0 ? xv(p - SI) : 0.0; xe = q.i < A.nx - 1 ? xv(p + SI) : 0.0;
+    xs = q.j > 0 ? xv(p - SJ) : 0.0; xn = q.j < A.ny - 1 ? xv(p + SJ) : 0.0;
+    xb = q.k > 0 ? xv(p - 1) : 0.0; xt = q.k < A.nz - 1 ? xv(p + 1) : 0.0;
+  } else {
+    const NbIdx m = nb_index(A, p, q);
+    xw = m.w >= 0 ? xv(m.w) : 0.0; xe = m.e >= 0 ? xv(m.e) : 0.0;
+    xs = m.s >= 0 ? xv(m.s) : 0.0; xn = m.n >= 0 ? xv(m.n) : 0.0;
+    xb = m.b >= 0 ? xv(m.b) : 0.0; xt = m.t >= 0 ? xv(m.t) : 0.0;
+  }
   double v = __dmul_rn(A.c[p], xv(p));
   v = __dsub_rn(v, __dadd_rn(__dmul_rn(a.w, xw), __dmul_rn(a.e, xe)));
   v = __dsub_rn(v, __dadd_rn(__dmul_rn(a.s, xs), __dmul_rn(a.n, xn)));
@@ -39,10 +47,18 @@ __device__ __forceinline__ double ref_ax(const MatView<double> &A, long long p, 
 __device__ __forceinline__ double ref_bmax(const MatView<double> &A, long long p, Pos q,
                                            const double *x, double bp) {
   Nb<double> a = coeffs(A, p, q);
-  const NbIdx m = nb_index(A, p, q);
-  double xw = ld0(x, m.w, m.w >= 0), xe = ld0(x, m.e, m.e >= 0);
-  double xs = ld0(x, m.s, m.s >= 0), xn = ld0(x, m.n, m.n >= 0);
-  double xb = ld0(x, m.b, m.b >= 0), xt = ld0(x, m.t, m.t >= 0);
+  double xw, xe, xs, xn, xb, xt;
+  if (!A.per) {
+    const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
+    xw = ld0(x, p - SI, q.i > 0); xe = ld0(x, p + SI, q.i < A.nx - 1);
+    xs = ld0(x, p - SJ, q.j > 0); xn = ld0(x, p + SJ, q.j < A.ny - 1);
+    xb = ld0(x, p - 1, q.k > 0); xt = ld0(x, p + 1, q.k < A.nz - 1);
+  } else {
+    const NbIdx m = nb_index(A, p, q);
+    xw = ld0(x, m.w, m.w >= 0); xe = ld0(x, m.e, m.e >= 0);
+    xs = ld0(x, m.s, m.s >= 0); xn = ld0(x, m.n, m.n >= 0);
+    xb = ld0(x, m.b, m.b >= 0); xt = ld0(x, m.t, m.t >= 0);
+  }
   double v = __dsub_rn(bp, __dmul_rn(A.c[p], x[p]));
   v = __dadd_rn(v, __dadd_rn(__dmul_rn(a.w, xw), __dmul_rn(a.e, xe)));
   v = __dadd_rn(v, __dadd_rn(__dmul_rn(a.s, xs), __dmul_rn(a.n, xn)));

@@ -28,7 +28,7 @@ CASES = [
     ("single16", O.KIND_SINGLE, dict(n=16), ["cg", "bicgs", "ac", "cg_ic0", "cg_ic2", "cg_ic3", "cgs",
                                              "bicgs_ic2", "cgs_ic0"]),
     ("single12", O.KIND_SINGLE, dict(n=12), ["cg", "ac_w", "ac_f", "ac_noguard", "jacobi", "gs",
-                                             "acsm_gs", "acsm_bicgs"]),
+                                             "acsm_gs", "acsm_bicgs", "acsm_cgs", "acsm_cg-ic0"]),
     ("cyl24", O.KIND_CYL, dict(n=24, nb=3, rmin=2.0, rmax=4.0, rc=5.0), ["cg", "ac", "cg_ic2", "jacobi",
                                                                           "gs", "acsm_gs", "acsm_jacobi"]),
     ("odd15", O.KIND_BATCH, dict(index=40, n2d=0, s3=(15, 16)), ["cg", "ac", "jacobi", "gs",
@@ -133,7 +133,11 @@ def main():
             elif run == "ac_noguard":
                 extra = dict(guard=0, maxcyc=6)
             elif run.startswith("acsm_"):  # AC with the Pressure's solver of that kind
-                extra = dict(acsm=run.split("_")[1])
+                # "acsm_<solver>" or "acsm_<solver>-<preconditioner>"
+                sm, _, pr = run.split("_")[1].partition("-")
+                extra = dict(acsm=sm)
+                if pr:
+                    extra["prec"] = pr
             kw_run = dict(resrat=1e-8)
             if solver in ("jacobi", "gs"):
                 kw_run = dict(STATIONARY)

@@ -181,21 +181,40 @@ ACSM_RUNS = [(n, k) for n in NAMES for k in load(n) if k.startswith("acsm_") and
 @pytest.mark.parametrize("name,key", ACSM_RUNS)
 def test_ac_with_other_smoothers(engine, oracle, name, key):
     """AC whose levels are smoothed by the Centered object's own solver:
-    Gauss-Seidel, Jacobi or BiCGS instead of CG (ref_harness --acsm). With
-    exact sums the cycles, the residual history and the iterate are the
-    compiled reference's."""
+    Gauss-Seidel, Jacobi, BiCGS, CGS or IC0-preconditioned CG instead of CG
+    (ref_harness --acsm, --prec). With exact sums the cycles, the residual
+    history and the iterate are the compiled reference's."""
     run = key[:-2]
     g = load(name)
     P = problem_of(g, oracle)
     x = np.zeros(P.N)
+    sm, _, pr = run.split("_")[1].partition("-")
     with session_for(engine, P) as s:
         s.upload_ci(g["ci"])
-        ac = engine.AC(s, exact_sums=True, smoother=run.split("_")[1])
+        ac = engine.AC(s, exact_sums=True, smoother=sm, prec=pr or "di")
         ok, ncyc = ac.cycle(x, P.b.copy(), loop=engine.CYCLE_V, factor=1e-8)
         hist = s.history()
     assert ok == bool(g[run + "_converged"])
     assert ncyc == int(g[run + "_cycles"])
     np.testing.assert_allclose(hist, g[run + "_hist"], rtol=1e-13)
+    assert np.array_equal(x, g[run + "_x"])
+
+
+@pytest.mark.parametrize("run", ["acsm_gs", "acsm_cg-ic0"])
+def test_ac_smoother_without_uploaded_ci(engine, oracle, run):
+    """Without an uploaded ci the level-0 smoother takes 1/c for the
+    reference's ci; on a fixture whose ci is exactly 1/c (no solid cells)
+    the run is the reference's bit for bit."""
+    g = load("single12")
+    assert np.array_equal(g["ci"], 1.0 / g["A_c"])
+    P = problem_of(g, oracle)
+    x = np.zeros(P.N)
+    sm, _, pr = run.split("_")[1].partition("-")
+    with session_for(engine, P) as s:
+        ac = engine.AC(s, exact_sums=True, smoother=sm, prec=pr or "di")
+        ok, ncyc = ac.cycle(x, P.b.copy(), loop=engine.CYCLE_V, factor=1e-8)
+    assert ok == bool(g[run + "_converged"])
+    assert ncyc == int(g[run + "_cycles"])
     assert np.array_equal(x, g[run + "_x"])
 
 

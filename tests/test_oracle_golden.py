@@ -67,12 +67,14 @@ def test_ac_bit_exact(oracle, name, run):
 @pytest.mark.parametrize("name,run", [(n, k[:-2]) for n in NAMES for k in load(n)
                                       if k.startswith("acsm_") and k.endswith("_x")])
 def test_ac_other_smoothers_bit_exact(oracle, name, run):
-    """AC whose levels are smoothed by Gauss-Seidel, Jacobi or BiCGS (the
-    reference's Pressure solver of that kind): cycles, history and iterate."""
+    """AC whose levels are smoothed by Gauss-Seidel, Jacobi, BiCGS, CGS or
+    IC0-preconditioned CG (the reference's Pressure solver of that kind):
+    cycles, history and iterate."""
     g = load(name)
     P = problem_of(g, oracle)
     assert np.array_equal(P.ci, g["ci"])
-    ac = oracle.AC(P, smoother=run.split("_")[1])
+    sm, _, pr = run.split("_")[1].partition("-")
+    ac = oracle.AC(P, smoother=sm, prec=pr or "di")
     x, st = ac.cycle(factor=1e-8, loop=1)
     assert st["cycles"] == int(g[run + "_cycles"])
     assert st["converged"] == int(g[run + "_converged"])
