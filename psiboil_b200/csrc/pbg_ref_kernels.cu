@@ -224,7 +224,7 @@ __global__ void k_cg_init(MatView<double> A, const double *__restrict__ x,
   }
 }
 
-__global__ void k_cg_pq(MatView<double> A, const double *__restrict__ r, double *pA, double *pB,
+__global__ void __launch_bounds__(kThreads, 3) k_cg_pq(MatView<double> A, const double *__restrict__ r, double *pA, double *pB,
                         double *__restrict__ qv, KrylovState *st, double *part, unsigned *count,
                         const double *__restrict__ zarr, const double *__restrict__ mc) {
   if (st->done) return;
@@ -259,7 +259,7 @@ __global__ void k_cg_pq(MatView<double> A, const double *__restrict__ r, double 
 // Seq = false: tree-order sums only (the split path), without the
 // exact-order reduction's code and shared memory
 template <bool Seq>
-__global__ void k_cg_xr(long long N, const double *__restrict__ mc, double *__restrict__ x,
+__global__ void __launch_bounds__(kThreads, 3) k_cg_xr(long long N, const double *__restrict__ mc, double *__restrict__ x,
                         double *__restrict__ r, const double *pA, const double *pB,
                         const double *__restrict__ qv, KrylovState *st, double *hist,
                         double *part, unsigned *count, int ic) {
@@ -336,7 +336,7 @@ __global__ void k_cg_p(long long N, const double *__restrict__ r, const double *
 }
 
 // q = A p for two cells of one k-row (nz even), in ref_ax's order
-__global__ void k_cg_q(MatView<double> A, Geo G, const double *__restrict__ p, double *__restrict__ qv,
+__global__ void __launch_bounds__(kThreads, 4) k_cg_q(MatView<double> A, Geo G, const double *__restrict__ p, double *__restrict__ qv,
                        KrylovState *st, double *part, unsigned *count) {
   if (st->done) return;
   const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
@@ -1076,7 +1076,6 @@ __global__ void k_gs_plane(MatView<double> A, const double *__restrict__ ci,
                            const double *__restrict__ b, double *x, int h, const KrylovState *st,
                            const double *__restrict__ xold) {
   if (st->done) return;
-  const long long SI = (long long)A.ny * A.nz, SJ = A.nz;
   const long long nij = (long long)A.nx * A.ny;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nij;
        t += (long long)gridDim.x * blockDim.x) {
