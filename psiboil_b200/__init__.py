@@ -16,6 +16,7 @@ reference's BW=3 Scalar blocks. Every compute call runs the CUDA library; if
 it cannot be loaded, importing a solver raises — there is no CPU fallback.
 """
 import ctypes
+import functools
 import os
 
 import numpy as np
@@ -296,6 +297,58 @@ def device_count():
     return n.value if rc == PBG_OK else 0
 
 
+def _first_cuda_tensor(values):
+    for a in values:
+        if isinstance(a, dict):
+            t = _first_cuda_tensor(a.values())
+            if t is not None:
+                return t
+        elif getattr(a, "is_cuda", False) and hasattr(a, "data_ptr"):
+            return a
+    return None
+
+
+def _stream_ordered(fn):
+    """For Session methods that take CUDA tensors. torch wrote those tensors
+    on its current stream; the library works on the session's own
+    (non-blocking) stream. So the session's stream first waits for torch's
+    current stream, and torch's current stream then waits for the session's:
+    the call sees the tensors' values, and later torch work sees its
+    results. Nothing is done when the session's stream is the current one
+    (work issued inside `torch.cuda.stream(ExternalStream(stream_handle()))`)."""
+    @functools.wraps(fn)
+    def wrap(self, *args, **kw):
+        t = _first_cuda_tensor(list(args) + list(kw.values()))
+        if t is None:
+            return fn(self, *args, **kw)
+        import torch
+        cur = torch.cuda.current_stream(t.device)
+        h = self.stream_handle()
+        if cur.cuda_stream == h:
+            return fn(self, *args, **kw)
+        own = torch.cuda.ExternalStream(h, device=t.device)
+        own.wait_stream(cur)
+        out = fn(self, *args, **kw)
+        cur.wait_stream(own)
+        return out
+    return wrap
+
+
+def _inputs_ready(fn):
+    """For batch and server calls that take CUDA tensors: those copy or read
+    device inputs on the library's own streams, which torch's stream does
+    not order; the host first waits for the work torch has queued, so the
+    tensors hold their values when the library reads them."""
+    @functools.wraps(fn)
+    def wrap(self, *args, **kw):
+        t = _first_cuda_tensor(list(args) + list(kw.values()))
+        if t is not None:
+            import torch
+            torch.cuda.current_stream(t.device).synchronize()
+        return fn(self, *args, **kw)
+    return wrap
+
+
 class Session:
     """One grid, its matrix, hierarchies and scratch on one GPU.
 
@@ -338,6 +391,7 @@ class Session:
         self.close()
 
     # -- matrix -----------------------------------------------------------
+    @_stream_ordered
     def upload_matrix(self, A, strides=None, offset=0):
         """A: mapping with c, w, e, s, n, b, t (the reference's Matrix)."""
         ptrs = [_ptr(A[k]) for k in "cwesnbt"]
@@ -351,12 +405,14 @@ class Session:
         _check(lib().pbg_matrix_download(self._h, *[out[k].ctypes.data for k in "cwesnbt"], HOST))
         return out
 
+    @_stream_ordered
     def upload_active(self, aflag, strides=None, offset=0):
         a = np.ascontiguousarray(aflag, dtype=np.int32)
         nx, ny, nz = self.dims
         si, sj, sk = strides if strides else (ny * nz, nz, 1)
         _check(lib().pbg_active_upload(self._h, a.ctypes.data, si, sj, sk, offset, HOST))
 
+    @_stream_ordered
     def upload_ci(self, ci, strides=None, offset=0):
         """The matrix's stored inverse central coefficient A.ci, read by Jacobi
         and Gauss-Seidel (1/c until it is uploaded, and after every matrix change)."""
@@ -365,6 +421,7 @@ class Session:
         si, sj, sk = strides if strides else (ny * nz, nz, 1)
         _check(lib().pbg_ci_upload(self._h, p, si, sj, sk, offset, where))
 
+    @_stream_ordered
     def assemble_pressure(self, rho, solid):
         """Pressure::discretize on the device (harmonic face density)."""
         pr, where = _ptr(rho)
@@ -373,6 +430,7 @@ class Session:
             raise ValueError("rho and solid must live in the same memory")
         _check(lib().pbg_assemble_pressure(self._h, pr, ps, where))
 
+    @_stream_ordered
     def assemble_mix(self, col, rho_a, rho_b=1.0, solid=None):
         """Pressure::discretize of a two-phase mixture on the device
         (arithmetic face density from the colour; col None: one fluid)."""
@@ -384,6 +442,7 @@ class Session:
             where = where2
         _check(lib().pbg_assemble_mix(self._h, pc, rho_a, rho_b, ps, where))
 
+    @_stream_ordered
     def divergence(self, u, v, w, dt, rhs, solid=None):
         """Pressure::update_rhs: rhs from the face velocities (solid: a
         voxel body, the immersed-body branch)."""
@@ -392,6 +451,7 @@ class Session:
                                     _ptr(rhs)[0], where))
         return rhs
 
+    @_stream_ordered
     def project(self, p, col, rho_a, rho_b, dt, u, v, w, solid=None):
         """Momentum::project: u, v, w updated in place."""
         pp, where = _ptr(p)
@@ -399,6 +459,7 @@ class Session:
                                  _ptr(u)[0], _ptr(v)[0], _ptr(w)[0], where))
         return u, v, w
 
+    @_stream_ordered
     def upload_body(self, fV, fS):
         """A cut immersed body for the flow functions (the reference's Body:
         fV per cell, fS the six face fractions per cell, planes w e s n b t);
@@ -416,6 +477,7 @@ class Session:
             raise ValueError("fV and fS must live in the same memory")
         _check(lib().pbg_body_upload(self._h, pv, ps, where))
 
+    @_stream_ordered
     def pressure_step(self, col, rho_a, rho_b, dt, u, v, w, p, params, solid=None):
         """Assemble, divergence, solve and project in one call; u, v, w and
         p updated in place. Returns the solver's Result."""
@@ -432,23 +494,27 @@ class Session:
         return bool(sym.value)
 
     # -- operators ---------------------------------------------------------
+    @_stream_ordered
     def spmv(self, x, y):
         px, w = _ptrn(x, self.ncell)
         py, _ = _ptrn(y, self.ncell)
         _check(lib().pbg_spmv(self._h, px, py, w))
         return y
 
+    @_stream_ordered
     def residual(self, x, b, r):
         px, w = _ptrn(x, self.ncell)
         _check(lib().pbg_residual(self._h, px, _ptrn(b, self.ncell)[0], _ptrn(r, self.ncell)[0], w))
         return r
 
+    @_stream_ordered
     def dot(self, x, y):
         out = (ctypes.c_double * 2)()
         px, w = _ptrn(x, self.ncell)
         _check(lib().pbg_dot(self._h, px, _ptrn(y, self.ncell)[0], w, out))
         return out[0], out[1]
 
+    @_stream_ordered
     def seq_sum(self, a, b=None):
         """Sequential sums in index order (pbg_seq_sum): the rounded
         left-to-right sum of a (and of b)."""
@@ -476,6 +542,7 @@ class Session:
         return {k: out[q * n:(q + 1) * n] for q, k in enumerate("cwesnbt")}
 
     # -- solve -------------------------------------------------------------
+    @_stream_ordered
     def solve(self, x, b, params, strides=None, offset=0):
         need = self.ncell if strides is None else 0
         px, where = _ptrn(x, need)
@@ -786,6 +853,7 @@ class Batch:
         _check(lib().pbg_batch_problem_bytes(self._h, nx, ny, nz, ctypes.byref(v)))
         return v.value
 
+    @_inputs_ready
     def add(self, dims, h, rho=None, solid=None, b=None, x=None, bc=None):
         """A new problem; returns its id."""
         if bc is None:  # Dirichlet top: kmax in 3-D, jmax in 2-D (as Session)
@@ -807,6 +875,7 @@ class Batch:
         _check(lib().pbg_batch_remove(self._h, i))
         self.dims.pop(i, None)
 
+    @_inputs_ready
     def set_fields(self, i, rho, solid):
         pr, wr = _ptr(rho)
         ps, ws = _ptr(solid, "uint8")
@@ -814,10 +883,12 @@ class Batch:
             raise ValueError("rho and solid must live on the same side")
         _check(lib().pbg_batch_set_fields(self._h, i, pr, ps, wr))
 
+    @_inputs_ready
     def set_rhs(self, i, b):
         pb_, w = _ptr(b)
         _check(lib().pbg_batch_set_rhs(self._h, i, pb_, w))
 
+    @_inputs_ready
     def set_x(self, i, x=None):
         px, w = _ptr(x)
         _check(lib().pbg_batch_set_x(self._h, i, px, w))
@@ -904,6 +975,7 @@ class Server:
         _check(lib().pbg_server_close_session(self._h, sid))
         self.dims.pop(sid, None)
 
+    @_inputs_ready
     def submit(self, sid, rhs, rho=None, solid=None):
         pb_, w = _ptr(rhs)
         pr, _ = _ptr(rho)
