@@ -32,7 +32,12 @@
  * offset = 3*(si+sj+sk).
  *
  * `where` says whether caller pointers are host (PBG_HOST) or device
- * (PBG_DEVICE, on the session's device) memory.
+ * (PBG_DEVICE, on the session's device) memory. A session works on its own
+ * non-blocking stream (pbg_session_stream), which other streams' work is
+ * not ordered against: device inputs must be complete before the call
+ * (make the session's stream wait on an event of the stream that wrote
+ * them, or synchronise that stream). A call returns with its results
+ * complete.
  */
 #ifndef PSIBOIL_B200_H
 #define PSIBOIL_B200_H
