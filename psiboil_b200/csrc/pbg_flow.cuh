@@ -453,18 +453,19 @@ __global__ void __launch_bounds__(kThreads)
 // Marching forms of the assembly and the projection (nz % 4 == 0, no cut
 // body, fewer than 2^31 cells). A block of 256 threads owns a tile of the
 // (j, k) plane, TJ rows of 4 KQ cells (KQ threads a row, 4 cells a thread,
-// TJ = 256 / KQ), and walks it through LEN consecutive i planes. The
-// colour, mixture density, pressure and solid flag of a cell are read and
-// formed once per walk (plus the plane before the walk and the tile's
-// one-cell halo); the row and k neighbours in a plane come from shared
-// memory, the previous plane from registers, and the coefficient of the
-// face between planes i and i+1 is formed once, as the east face of i and
-// the west face of i+1. Every value is the same operations in the same
-// order as the one-cell kernels, so the outputs are bit for bit theirs.
+// TJ = 256 / KQ), and walks it through LEN consecutive i planes, the
+// previous plane in registers. The assembly forms each cell's mixture
+// density once per walk (plus the plane before the walk and the tile's
+// one-cell halo) and takes the row and k neighbours of a plane from shared
+// memory; the coefficient of the face between planes i and i+1 is formed
+// once, as the east face of i and the west face of i+1. The projection
+// reads its south row directly and takes its k neighbour from the lane
+// before, without shared memory or barriers. Every value is the same
+// operations in the same order as the one-cell kernels, so the outputs are
+// bit for bit theirs.
 // ---------------------------------------------------------------------------
 constexpr int kMarchI = 8;       // planes a walk, at most
 constexpr int kMarchSmA = 1548;  // assembly: (TJ + 2) (4 KQ + 2) cells at most, TJ KQ = 256
-constexpr int kMarchSmP = 1285;  // projection: (TJ + 1) (4 KQ + 1) cells at most
 
 // threads a row: the smallest power of two with 4 KQ >= nz, at most 64
 inline int march_kq(int nz) {
@@ -751,14 +752,23 @@ __global__ void __launch_bounds__(kThreads, 2)
   }
 }
 
-__global__ void __launch_bounds__(kThreads)
+// The projection's walk, without shared memory or barriers: the previous
+// plane in registers, the south row (j - 1) read directly (from L1/L2: it is
+// another thread's own row), the k - 1 neighbour from the previous lane when
+// that lane holds the row's previous quad, else read. Faces follow the
+// one-cell kernel's rules and arithmetic:
+//  * a quad of solid cells updates no face at all;
+//  * a quad with all three lower neighbours inside the domain and no solid
+//    cell in it or below it on any axis updates every face, both divisions
+//    by Markstein's correction when every face density is a pure phase's;
+//  * any other quad (or one whose correction misses) takes the general
+//    per-face rules with KnownDiv's divisions.
+__global__ void __launch_bounds__(kThreads, 2)
     km_project(int nx, int ny, int nz, int KQ, int LEN, double h, double dt, const double *__restrict__ pr,
                const double *__restrict__ col, double ra, double rb, const uint8_t *__restrict__ solid,
                double *__restrict__ u, double *__restrict__ v, double *__restrict__ w) {
-  __shared__ double sq_[2][kMarchSmP], sm_[2][kMarchSmP];
-  __shared__ uint8_t ss_[2][kMarchSmP];
-  const int TJ = kThreads / KQ, WD = 4 * KQ + 1;
-  const int tx = (int)threadIdx.x % KQ, ty = (int)threadIdx.x / KQ;
+  const int TJ = kThreads / KQ;
+  const int tx = (int)threadIdx.x % KQ, ty = (int)threadIdx.x / KQ, lane = (int)threadIdx.x & 31;
   const int k = (int)blockIdx.x * 4 * KQ + 4 * tx, j = (int)blockIdx.y * TJ + ty;
   const int i0 = (int)blockIdx.z * LEN, i1 = min(nx, i0 + LEN);
   const bool own = j < ny && k < nz;
@@ -768,10 +778,7 @@ __global__ void __launch_bounds__(kThreads)
   const PhaseDiv D(ra, rb, h);
   const ProjFast PF(D);
   const uchar4 z4 = make_uchar4(0, 0, 0, 0);
-  // own cells from index c0; the halo row j0 - 1 (row 0) is loaded by the
-  // threads of the first row, the halo column k0 - 1 (column 0) by the first
-  // thread of each row
-  const int c0 = (ty + 1) * WD + 4 * tx + 1;
+  const bool kshfl = lane > 0 && tx > 0;  // the previous lane holds the quad before
   double pP[4] = {0.0, 0.0, 0.0, 0.0}, mP[4] = {0.0, 0.0, 0.0, 0.0};
   uchar4 sP = z4;
   if (own && i0 > 0) {
@@ -781,55 +788,35 @@ __global__ void __launch_bounds__(kThreads)
     sP = body ? ld4b(solid, p) : z4;
   }
   for (int i = i0; i < i1; ++i) {
-    const int b = (i - i0) & 1;
-    const uint32_t base = (uint32_t)i * SI;
-    const uint32_t p = base + (uint32_t)j * SJ + (uint32_t)k;
+    const uint32_t p = (uint32_t)i * SI + (uint32_t)j * SJ + (uint32_t)k;
     double pC[4] = {0.0, 0.0, 0.0, 0.0}, mC[4] = {0.0, 0.0, 0.0, 0.0};
-    uchar4 sC = z4;
+    double pS[4] = {0.0, 0.0, 0.0, 0.0}, mS[4] = {0.0, 0.0, 0.0, 0.0};
+    uchar4 sC = z4, sS = z4;
     if (own) {
       ld4d(pr, p, pC);
       mix4(col, ra, rb, p, mC);
       if (body) sC = ld4b(solid, p);
-#pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        sq_[b][c0 + m] = pC[m];
-        sm_[b][c0 + m] = mC[m];
-        ss_[b][c0 + m] = byte_of(sC, m);
-      }
-      if (tx == 0 && k > 0) {
-        sq_[b][c0 - 1] = pr[p - 1];
-        sm_[b][c0 - 1] = mix1(col, ra, rb, (long long)p - 1);
-        ss_[b][c0 - 1] = body ? solid[p - 1] : 0;
+      if (j > 0) {
+        ld4d(pr, p - SJ, pS);
+        mix4(col, ra, rb, p - SJ, mS);
+        if (body) sS = ld4b(solid, p - SJ);
       }
     }
-    if (ty == 0 && j > 0 && k < nz) {
-      const uint32_t ph = p - SJ;
-      double hp[4], hm[4];
-      ld4d(pr, ph, hp);
-      mix4(col, ra, rb, ph, hm);
-      const uchar4 hs = body ? ld4b(solid, ph) : z4;
-#pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        sq_[b][4 * tx + 1 + m] = hp[m];
-        sm_[b][4 * tx + 1 + m] = hm[m];
-        ss_[b][4 * tx + 1 + m] = byte_of(hs, m);
-      }
+    double pk = __shfl_up_sync(0xffffffffu, pC[3], 1);
+    double mk = __shfl_up_sync(0xffffffffu, mC[3], 1);
+    unsigned sk = __shfl_up_sync(0xffffffffu, (unsigned)sC.w, 1);
+    if (!kshfl && own && k > 0) {
+      pk = pr[p - 1];
+      mk = mix1(col, ra, rb, (long long)p - 1);
+      sk = body ? solid[p - 1] : 0u;
     }
-    __syncthreads();
-    // A quad of solid cells updates no face at all. A quad with all three
-    // lower neighbours inside the domain and no solid cell in it or below it
-    // on any axis updates every face, with both divisions by Markstein's
-    // correction when every face density is a pure phase's; a face it does
-    // not cover sends the quad to the general code.
     bool fast = own && i > 0 && j > 0 && k > 0;
     bool skip = false;
     if (body && own) {
       skip = sC.x && sC.y && sC.z && sC.w;
       if (fast) {
-        uint32_t any = *reinterpret_cast<const uint32_t *>(&sC) | *reinterpret_cast<const uint32_t *>(&sP) |
-                       ss_[b][c0 - 1];
-#pragma unroll
-        for (int m = 0; m < 4; ++m) any |= ss_[b][c0 + m - WD];
+        const uint32_t any = *reinterpret_cast<const uint32_t *>(&sC) | *reinterpret_cast<const uint32_t *>(&sP) |
+                             *reinterpret_cast<const uint32_t *>(&sS) | sk;
         fast = any == 0;
       }
     }
@@ -846,10 +833,9 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
       for (int m = 0; m < 4; ++m) {
         uo[m] = __dadd_rn(uo[m], PF.inc(pP[m], pC[m], face_of(hc, ra, mC[m], mP[m]), dt, body, miss));
-        vo[m] = __dadd_rn(vo[m], PF.inc(sq_[b][c0 + m - WD], pC[m], face_of(hc, ra, mC[m], sm_[b][c0 + m - WD]),
-                                        dt, body, miss));
-        const double pb = m > 0 ? pC[m - 1] : sq_[b][c0 - 1];
-        const double mb = m > 0 ? mC[m - 1] : sm_[b][c0 - 1];
+        vo[m] = __dadd_rn(vo[m], PF.inc(pS[m], pC[m], face_of(hc, ra, mC[m], mS[m]), dt, body, miss));
+        const double pb = m > 0 ? pC[m - 1] : pk;
+        const double mb = m > 0 ? mC[m - 1] : mk;
         wo[m] = __dadd_rn(wo[m], PF.inc(pb, pC[m], face_of(hc, ra, mC[m], mb), dt, body, miss));
       }
       if (!miss) {
@@ -875,11 +861,9 @@ __global__ void __launch_bounds__(kThreads)
         double vo[4];
         ld4d(v, iv, vo);
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-          const double ps = sq_[b][c0 + m - WD], mS = sm_[b][c0 + m - WD];
-          if (!(body && (byte_of(sC, m) || ss_[b][c0 + m - WD])))
-            vo[m] = __dadd_rn(vo[m], project_increment_k(ps, pC[m], face_of(hc, ra, mC[m], mS), dt, D, body));
-        }
+        for (int m = 0; m < 4; ++m)
+          if (!(body && (byte_of(sC, m) || byte_of(sS, m))))
+            vo[m] = __dadd_rn(vo[m], project_increment_k(pS[m], pC[m], face_of(hc, ra, mC[m], mS[m]), dt, D, body));
         st4d(v, iv, vo);
       }
       if (nz > 1) {
@@ -888,10 +872,10 @@ __global__ void __launch_bounds__(kThreads)
         for (int m = 0; m < 4; ++m) {
           const int kk = k + m;
           if (kk == 0) continue;
-          const uint8_t sbm = m > 0 ? byte_of(sC, m - 1) : ss_[b][c0 - 1];
+          const unsigned sbm = m > 0 ? byte_of(sC, m - 1) : sk;
           if (body && (byte_of(sC, m) || sbm)) continue;
-          const double pb = m > 0 ? pC[m - 1] : sq_[b][c0 - 1];
-          const double mb = m > 0 ? mC[m - 1] : sm_[b][c0 - 1];
+          const double pb = m > 0 ? pC[m - 1] : pk;
+          const double mb = m > 0 ? mC[m - 1] : mk;
           w[iw + m] = __dadd_rn(w[iw + m], project_increment_k(pb, pC[m], face_of(hc, ra, mC[m], mb), dt, D, body));
         }
       }
