@@ -454,18 +454,15 @@ __global__ void __launch_bounds__(kThreads)
 // body, fewer than 2^31 cells). A block of 256 threads owns a tile of the
 // (j, k) plane, TJ rows of 4 KQ cells (KQ threads a row, 4 cells a thread,
 // TJ = 256 / KQ), and walks it through LEN consecutive i planes, the
-// previous plane in registers. The assembly forms each cell's mixture
-// density once per walk (plus the plane before the walk and the tile's
-// one-cell halo) and takes the row and k neighbours of a plane from shared
-// memory; the coefficient of the face between planes i and i+1 is formed
-// once, as the east face of i and the west face of i+1. The projection
-// reads its south row directly and takes its k neighbour from the lane
-// before, without shared memory or barriers. Every value is the same
+// previous plane in registers, without shared memory or barriers: the rows
+// beside a thread's own (other threads' own rows) are read directly, from
+// L1/L2, and the k neighbours come from the lanes around it. The assembly's
+// coefficient of the face between planes i and i+1 is formed once, as the
+// east face of i and the west face of i+1. Every value is the same
 // operations in the same order as the one-cell kernels, so the outputs are
 // bit for bit theirs.
 // ---------------------------------------------------------------------------
 constexpr int kMarchI = 8;       // planes a walk, at most
-constexpr int kMarchSmA = 1548;  // assembly: (TJ + 2) (4 KQ + 2) cells at most, TJ KQ = 256
 
 // threads a row: the smallest power of two with 4 KQ >= nz, at most 64
 inline int march_kq(int nz) {
@@ -544,10 +541,8 @@ __global__ void __launch_bounds__(kThreads, 2)
                     const double *__restrict__ col, double ra, double rb, const uint8_t *__restrict__ solid,
                     double *__restrict__ C, double *__restrict__ W, double *__restrict__ S,
                     double *__restrict__ B, uint8_t *__restrict__ aflag) {
-  __shared__ double sm[2][kMarchSmA];
-  __shared__ uint8_t ss[2][kMarchSmA];
   const int bc[6] = {bc03.x, bc03.y, bc03.z, bc03.w, bc45.x, bc45.y};
-  const int TJ = kThreads / KQ, WD = 4 * KQ + 2;
+  const int TJ = kThreads / KQ;
   const int tx = (int)threadIdx.x % KQ, ty = (int)threadIdx.x / KQ;
   const int k = (int)blockIdx.x * 4 * KQ + 4 * tx, j = (int)blockIdx.y * TJ + ty;
   const int i0 = (int)blockIdx.z * LEN, i1 = min(nx, i0 + LEN);
@@ -560,48 +555,20 @@ __global__ void __launch_bounds__(kThreads, 2)
   const QuotCache Q(hx, ra, rb);
   const QuotOnly QC(hx, hxb, ra, rb);
   const uchar4 z4 = make_uchar4(0, 0, 0, 0);
-  // shared-memory index of the thread's first cell; the halo rows (j0 - 1
-  // and j0 + TJ) are loaded by the threads of the first and last row, the
-  // halo columns (k0 - 1, k0 + 4 KQ) by the first and last thread of a row
-  const int c0 = (ty + 1) * WD + 4 * tx + 1;
-  const int hj = ty == 0 ? j - 1 : (ty == TJ - 1 ? j + 1 : -1);
-  const int hc0 = ty == 0 ? 4 * tx + 1 : (TJ + 1) * WD + 4 * tx + 1;
-  auto stage = [&](int ip, int b, bool halo, double (&mq)[4], uchar4 &sq) {
-    const uint32_t base = (uint32_t)ip * SI;
+  // the lanes before and after hold the row's previous and next quads
+  const int lane = (int)threadIdx.x & 31;
+  const bool kdn = lane > 0 && tx > 0, kup = lane < 31 && tx < KQ - 1;
+  // the thread's own quad of plane ip: mixture densities and solid flags
+  auto stage = [&](int ip, double (&mq)[4], uchar4 &sq) {
     if (own) {
-      const uint32_t p = base + (uint32_t)j * SJ + (uint32_t)k;
+      const uint32_t p = (uint32_t)ip * SI + (uint32_t)j * SJ + (uint32_t)k;
       mix4(col, ra, rb, p, mq);
       sq = solid ? ld4b(solid, p) : z4;
-      if (!halo) return;
-#pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        sm[b][c0 + m] = mq[m];
-        ss[b][c0 + m] = byte_of(sq, m);
-      }
-      if (tx == 0 && k > 0) {
-        sm[b][c0 - 1] = mix1(col, ra, rb, (long long)p - 1);
-        ss[b][c0 - 1] = solid ? solid[p - 1] : 0;
-      }
-      if (tx == KQ - 1 && k + 4 < nz) {
-        sm[b][c0 + 4] = mix1(col, ra, rb, (long long)p + 4);
-        ss[b][c0 + 4] = solid ? solid[p + 4] : 0;
-      }
-    }
-    if (halo && hj >= 0 && hj < ny && k < nz) {
-      const uint32_t ph = base + (uint32_t)hj * SJ + (uint32_t)k;
-      double hq[4];
-      mix4(col, ra, rb, ph, hq);
-      const uchar4 hs = solid ? ld4b(solid, ph) : z4;
-#pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        sm[b][hc0 + m] = hq[m];
-        ss[b][hc0 + m] = byte_of(hs, m);
-      }
     }
   };
-  double mC[4], mN[4], aW[4] = {0.0, 0.0, 0.0, 0.0};
+  double mC[4] = {0.0, 0.0, 0.0, 0.0}, mN[4] = {0.0, 0.0, 0.0, 0.0}, aW[4] = {0.0, 0.0, 0.0, 0.0};
   uchar4 sP = z4, sC = z4, sN = z4;
-  stage(i0, 0, true, mC, sC);
+  stage(i0, mC, sC);
   if (own && i0 > 0) {
     double mP[4];
     const uint32_t p = (uint32_t)(i0 - 1) * SI + (uint32_t)j * SJ + (uint32_t)k;
@@ -610,15 +577,23 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll
     for (int m = 0; m < 4; ++m) aW[m] = Q(face_of(hc, ra, mC[m], mP[m]));
   }
-  __syncthreads();
   for (int i = i0; i < i1; ++i) {
-    const int b = (i - i0) & 1;
-    if (i + 1 < nx) stage(i + 1, b ^ 1, i + 1 < i1, mN, sN);
+    if (i + 1 < nx) stage(i + 1, mN, sN);
+    // the row's k neighbours from the lanes around, else read; the south
+    // and north rows read directly
+    double mkm = __shfl_up_sync(0xffffffffu, mC[3], 1), mkp = __shfl_down_sync(0xffffffffu, mC[0], 1);
+    unsigned skm_ = __shfl_up_sync(0xffffffffu, (unsigned)sC.w, 1), skp_ = __shfl_down_sync(0xffffffffu, (unsigned)sC.x, 1);
     if (own) {
       const uint32_t p = (uint32_t)i * SI + (uint32_t)j * SJ + (uint32_t)k;
-      const double mkm = k > 0 ? sm[b][c0 - 1] : 0.0;
-      const double mkp = k + 4 < nz ? sm[b][c0 + 4] : 0.0;
-      const uint8_t skm = k > 0 ? ss[b][c0 - 1] : 0, skp = k + 4 < nz ? ss[b][c0 + 4] : 0;
+      if (!kdn) { mkm = k > 0 ? mix1(col, ra, rb, (long long)p - 1) : 0.0; skm_ = (k > 0 && solid) ? solid[p - 1] : 0u; }
+      if (!kup) { mkp = k + 4 < nz ? mix1(col, ra, rb, (long long)p + 4) : 0.0; skp_ = (k + 4 < nz && solid) ? solid[p + 4] : 0u; }
+      if (k == 0) { mkm = 0.0; skm_ = 0u; }
+      if (k + 4 >= nz) { mkp = 0.0; skp_ = 0u; }
+      const uint8_t skm = (uint8_t)skm_, skp = (uint8_t)skp_;
+      double mS[4] = {0.0, 0.0, 0.0, 0.0}, mNo[4] = {0.0, 0.0, 0.0, 0.0};
+      uchar4 sS = z4, sNo = z4;
+      if (j > 0) { mix4(col, ra, rb, p - SJ, mS); if (solid) sS = ld4b(solid, p - SJ); }
+      if (j < ny - 1) { mix4(col, ra, rb, p + SJ, mNo); if (solid) sNo = ld4b(solid, p + SJ); }
       // A quad away from the i and j walls whose cells and neighbours all
       // carry the same solid flag needs none of the wall and body rules but
       // the k walls' (a solid quad only scales c by 1e-12 and drops its
@@ -633,7 +608,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                     *reinterpret_cast<const uint32_t *>(&sN) == w4 && (k == 0 || skm == sp0) &&
                     (k + 4 == nz || skp == sp0);
 #pragma unroll
-        for (int m = 0; m < 4; ++m) same = same && ss[b][c0 + m - WD] == sp0 && ss[b][c0 + m + WD] == sp0;
+        for (int m = 0; m < 4; ++m) same = same && byte_of(sS, m) == sp0 && byte_of(sNo, m) == sp0;
         fast = same;
       }
       if (fast) {
@@ -650,8 +625,8 @@ __global__ void __launch_bounds__(kThreads, 2)
           for (int m = 0; m < 4; ++m) {
             const double a0 = aW[m];
             const double a1 = qin(face_of(hc, ra, mN[m], mC[m]));
-            const double a2 = qin(face_of(hc, ra, mC[m], sm[b][c0 + m - WD]));
-            const double a3 = qin(face_of(hc, ra, sm[b][c0 + m + WD], mC[m]));
+            const double a2 = qin(face_of(hc, ra, mC[m], mS[m]));
+            const double a3 = qin(face_of(hc, ra, mNo[m], mC[m]));
             double a4 = bfx[m];
             const double a5 = bfx[m + 1];
             double c = __dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(a0, a1), a2), a3), a4), a5);
@@ -690,7 +665,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
           const int kk = k + m;
-          const double ms_ = sm[b][c0 + m - WD], mn_ = sm[b][c0 + m + WD];
+          const double ms_ = mS[m], mn_ = mNo[m];
           double a[6];
           a[0] = i > 0 ? aW[m] : __ddiv_rn(hxb, face_of(hc, ra, mC[m], mC[m]));
           a[1] = i < nx - 1 ? Q(face_of(hc, ra, mN[m], mC[m])) : __ddiv_rn(hxb, face_of(hc, ra, mC[m], mC[m]));
@@ -707,8 +682,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             const uint8_t sbm = m > 0 ? byte_of(sC, m - 1) : skm, stp = m < 3 ? byte_of(sC, m + 1) : skp;
             if (i > 0 && byte_of(sP, m) != sp) a[0] = 0.0;
             if (i < nx - 1 && byte_of(sN, m) != sp) a[1] = 0.0;
-            if (j > 0 && ss[b][c0 + m - WD] != sp) a[2] = 0.0;
-            if (j < ny - 1 && ss[b][c0 + m + WD] != sp) a[3] = 0.0;
+            if (j > 0 && byte_of(sS, m) != sp) a[2] = 0.0;
+            if (j < ny - 1 && byte_of(sNo, m) != sp) a[3] = 0.0;
             if (kk > 0 && sbm != sp) a[4] = 0.0;
             if (kk < nz - 1 && stp != sp) a[5] = 0.0;
             if (!sp) {
@@ -744,7 +719,6 @@ __global__ void __launch_bounds__(kThreads, 2)
         *reinterpret_cast<uchar4 *>(aflag + p) = af;
       }
     }
-    __syncthreads();
     sP = sC;
     sC = sN;
 #pragma unroll
