@@ -277,11 +277,11 @@ __device__ __forceinline__ double project_increment_k(double pm, double pp, doub
   return D.h(__dmul_rn(D.by_rho(dp, rho), dt));
 }
 
-// project_increment for the fast quads of the marching projection: both
+// project_increment for the fast groups of the marching projection: both
 // divisions by Markstein's correction with no fallback (exact for +0 too;
 // -0 would come out +0); a face density that is not a pure phase's, a
 // dividend outside the range where the correction is exact (+0 included,
-// -0 not), or a divisor outside [2^-60, 2^60] sets miss, and the quad is
+// -0 not), or a divisor outside [2^-60, 2^60] sets miss, and the group is
 // redone by the general code.
 struct ProjFast {
   double ka, kb, ra, rb, ya, yb, h, yh;
@@ -386,6 +386,55 @@ __device__ __forceinline__ void mix4(const double *__restrict__ col, double ra, 
 __device__ __forceinline__ double mix1(const double *__restrict__ col, double ra, double rb, long long p) {
   return col ? mix_cell(col, ra, rb, p) : ra;
 }
+// V cells of a row (V = 2 or 4), for the marching kernels: doubles in
+// 16-byte pairs, solid flags as one V-byte word (byte m is cell m's)
+template <int V>
+__device__ __forceinline__ void ldvd(const double *__restrict__ a, uint32_t p, double (&o)[V]) {
+#pragma unroll
+  for (int q = 0; q < V; q += 2) {
+    const double2 t = *reinterpret_cast<const double2 *>(a + p + q);
+    o[q] = t.x;
+    o[q + 1] = t.y;
+  }
+}
+template <int V>
+__device__ __forceinline__ void stvd(double *__restrict__ a, uint32_t p, const double (&o)[V]) {
+#pragma unroll
+  for (int q = 0; q < V; q += 2) *reinterpret_cast<double2 *>(a + p + q) = make_double2(o[q], o[q + 1]);
+}
+template <int V>
+__device__ __forceinline__ uint32_t ldvb(const uint8_t *__restrict__ a, uint32_t p) {
+  if constexpr (V == 4) return *reinterpret_cast<const uint32_t *>(a + p);
+  else return *reinterpret_cast<const uint16_t *>(a + p);
+}
+template <int V>
+__device__ __forceinline__ void stvb(uint8_t *__restrict__ a, uint32_t p, uint32_t f) {
+  if constexpr (V == 4) *reinterpret_cast<uint32_t *>(a + p) = f;
+  else *reinterpret_cast<uint16_t *>(a + p) = (uint16_t)f;
+}
+// every byte of a V-byte word set to b
+template <int V>
+__device__ __forceinline__ uint32_t bytes_all(uint32_t b) { return b * (V == 4 ? 0x01010101u : 0x0101u); }
+__device__ __forceinline__ uint32_t byte_at(uint32_t x, int m) { return (x >> (8 * m)) & 0xffu; }
+// mixture densities of V cells of a row (mix_cell), or ra without colour
+template <int V>
+__device__ __forceinline__ void mixv(const double *__restrict__ col, double ra, double rb, uint32_t p,
+                                     double (&o)[V]) {
+  if (!col) {
+#pragma unroll
+    for (int m = 0; m < V; ++m) o[m] = ra;
+    return;
+  }
+  double c[V];
+  ldvd<V>(col, p, c);
+#pragma unroll
+  for (int m = 0; m < V; ++m) {
+    double v = c[m];
+    if (v > 1.0) v = 1.0;
+    if (v < 0.0) v = 0.0;
+    o[m] = __dadd_rn(__dmul_rn(ra, v), __dmul_rn(rb, __dsub_rn(1.0, v)));
+  }
+}
 // 0.5 * (value(first) + value(second)), mix_face's order; a constant
 // density without colour
 __device__ __forceinline__ double face_of(bool col, double ra, double m1, double m2) {
@@ -451,42 +500,50 @@ __global__ void __launch_bounds__(kThreads)
 
 // ---------------------------------------------------------------------------
 // Marching forms of the assembly and the projection (nz % 4 == 0, no cut
-// body, fewer than 2^31 cells). A block of 256 threads owns a tile of the
-// (j, k) plane, TJ rows of 4 KQ cells (KQ threads a row, 4 cells a thread,
-// TJ = 256 / KQ), and walks it through LEN consecutive i planes, the
-// previous plane in registers, without shared memory or barriers: the rows
-// beside a thread's own (other threads' own rows) are read directly, from
-// L1/L2, and the k neighbours come from the lanes around it. The assembly's
+// body, fewer than 2^31 cells). A thread owns a group of V consecutive
+// cells of a row (V = kAsmV = 4 in the assembly; kProjV = 2 in the
+// projection, whose fewer registers a thread let four blocks share an SM
+// instead of two). A block of 256 threads owns a tile of the (j, k) plane,
+// TJ rows of V KQ cells (KQ threads a row, TJ = 256 / KQ), and walks it
+// through LEN consecutive i planes, the previous plane in registers, without
+// shared memory or barriers: the rows beside a thread's own (other threads'
+// own rows) are read directly, from L1/L2, and the k neighbours come from
+// the lanes around it. The assembly's
 // coefficient of the face between planes i and i+1 is formed once, as the
 // east face of i and the west face of i+1. Every value is the same
 // operations in the same order as the one-cell kernels, so the outputs are
 // bit for bit theirs.
 // ---------------------------------------------------------------------------
-constexpr int kMarchI = 8;       // planes a walk, at most
+constexpr int kMarchI = 8;  // planes a walk, at most
+constexpr int kAsmV = 4;    // cells a thread, assembly
+constexpr int kProjV = 2;   // cells a thread, projection
 
-// threads a row: the smallest power of two with 4 KQ >= nz, at most 64
-inline int march_kq(int nz) {
+// threads a row: the smallest power of two with v KQ >= nz, at most 256 / v
+inline int march_kq(int nz, int v) {
   int q = 1;
-  while (q < 64 && 4 * q < nz) q *= 2;
+  while (q < kThreads / v && v * q < nz) q *= 2;
   return q;
 }
 // planes a walk: kMarchI, halved (down to 2) while the grid would hold
 // fewer than four blocks an SM of a 148-SM GPU
-inline int march_len(int nx, int ny, int nz) {
-  const int kq = march_kq(nz), tj = kThreads / kq;
-  const long long tiles = (long long)((nz + 4 * kq - 1) / (4 * kq)) * ((ny + tj - 1) / tj);
+inline int march_len(int nx, int ny, int nz, int v) {
+  const int kq = march_kq(nz, v), tj = kThreads / kq;
+  const long long tiles = (long long)((nz + v * kq - 1) / (v * kq)) * ((ny + tj - 1) / tj);
   int len = kMarchI;
   while (len > 2 && tiles * ((nx + len - 1) / len) < 4 * 148) len /= 2;
   return len;
 }
-inline dim3 march_grid(int nx, int ny, int nz) {
-  const int kq = march_kq(nz), tj = kThreads / kq, len = march_len(nx, ny, nz);
-  return dim3((unsigned)((nz + 4 * kq - 1) / (4 * kq)), (unsigned)((ny + tj - 1) / tj),
+inline dim3 march_grid(int nx, int ny, int nz, int v) {
+  const int kq = march_kq(nz, v), tj = kThreads / kq, len = march_len(nx, ny, nz, v);
+  return dim3((unsigned)((nz + v * kq - 1) / (v * kq)), (unsigned)((ny + tj - 1) / tj),
               (unsigned)((nx + len - 1) / len));
 }
 inline bool march_fits(int nx, int ny, int nz) {
-  const dim3 g = march_grid(nx, ny, nz);
-  return g.y <= 65535u && g.z <= 65535u;
+  for (int v : {kAsmV, kProjV}) {
+    const dim3 g = march_grid(nx, ny, nz, v);
+    if (g.y > 65535u || g.z > 65535u) return false;
+  }
+  return true;
 }
 
 // hx / f for a face density f, with hx / ra and hx / rb formed once: away
@@ -509,7 +566,7 @@ struct QuotCache {
   }
 };
 
-// Cache-only quotients for the fast quads of the marching assembly: hx and
+// Cache-only quotients for the fast groups of the marching assembly: hx and
 // hxb (the wall faces' numerator) over either pure-phase density. A face
 // density that is neither (an interface face), or a zero density, sets
 // miss and returns a placeholder.
@@ -536,7 +593,8 @@ struct QuotOnly {
   }
 };
 
-__global__ void __launch_bounds__(kThreads, 2)
+template <int V>
+__global__ void __launch_bounds__(kThreads, V == 2 ? 4 : 2)
     km_assemble_mix(int nx, int ny, int nz, int KQ, int LEN, double h, int4 bc03, int2 bc45,
                     const double *__restrict__ col, double ra, double rb, const uint8_t *__restrict__ solid,
                     double *__restrict__ C, double *__restrict__ W, double *__restrict__ S,
@@ -544,7 +602,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int bc[6] = {bc03.x, bc03.y, bc03.z, bc03.w, bc45.x, bc45.y};
   const int TJ = kThreads / KQ;
   const int tx = (int)threadIdx.x % KQ, ty = (int)threadIdx.x / KQ;
-  const int k = (int)blockIdx.x * 4 * KQ + 4 * tx, j = (int)blockIdx.y * TJ + ty;
+  const int k = (int)blockIdx.x * V * KQ + V * tx, j = (int)blockIdx.y * TJ + ty;
   const int i0 = (int)blockIdx.z * LEN, i1 = min(nx, i0 + LEN);
   const bool own = j < ny && k < nz;
   const uint32_t SI = (uint32_t)ny * nz, SJ = (uint32_t)nz;
@@ -554,75 +612,70 @@ __global__ void __launch_bounds__(kThreads, 2)
   const bool hc = col != nullptr;
   const QuotCache Q(hx, ra, rb);
   const QuotOnly QC(hx, hxb, ra, rb);
-  const uchar4 z4 = make_uchar4(0, 0, 0, 0);
-  // the lanes before and after hold the row's previous and next quads
+  // the lanes before and after hold the row's previous and next groups
   const int lane = (int)threadIdx.x & 31;
   const bool kdn = lane > 0 && tx > 0, kup = lane < 31 && tx < KQ - 1;
-  // the thread's own quad of plane ip: mixture densities and solid flags
-  auto stage = [&](int ip, double (&mq)[4], uchar4 &sq) {
+  // the thread's own group of plane ip: mixture densities and solid flags
+  auto stage = [&](int ip, double (&mq)[V], uint32_t &sq) {
     if (own) {
       const uint32_t p = (uint32_t)ip * SI + (uint32_t)j * SJ + (uint32_t)k;
-      mix4(col, ra, rb, p, mq);
-      sq = solid ? ld4b(solid, p) : z4;
+      mixv<V>(col, ra, rb, p, mq);
+      sq = solid ? ldvb<V>(solid, p) : 0u;
     }
   };
-  double mC[4] = {0.0, 0.0, 0.0, 0.0}, mN[4] = {0.0, 0.0, 0.0, 0.0}, aW[4] = {0.0, 0.0, 0.0, 0.0};
-  uchar4 sP = z4, sC = z4, sN = z4;
+  double mC[V] = {}, mN[V] = {}, aW[V] = {};
+  uint32_t sP = 0u, sC = 0u, sN = 0u;
   stage(i0, mC, sC);
   if (own && i0 > 0) {
-    double mP[4];
+    double mP[V];
     const uint32_t p = (uint32_t)(i0 - 1) * SI + (uint32_t)j * SJ + (uint32_t)k;
-    mix4(col, ra, rb, p, mP);
-    sP = solid ? ld4b(solid, p) : z4;
+    mixv<V>(col, ra, rb, p, mP);
+    sP = solid ? ldvb<V>(solid, p) : 0u;
 #pragma unroll
-    for (int m = 0; m < 4; ++m) aW[m] = Q(face_of(hc, ra, mC[m], mP[m]));
+    for (int m = 0; m < V; ++m) aW[m] = Q(face_of(hc, ra, mC[m], mP[m]));
   }
   for (int i = i0; i < i1; ++i) {
     if (i + 1 < nx) stage(i + 1, mN, sN);
     // the row's k neighbours from the lanes around, else read; the south
     // and north rows read directly
-    double mkm = __shfl_up_sync(0xffffffffu, mC[3], 1), mkp = __shfl_down_sync(0xffffffffu, mC[0], 1);
-    unsigned skm_ = __shfl_up_sync(0xffffffffu, (unsigned)sC.w, 1), skp_ = __shfl_down_sync(0xffffffffu, (unsigned)sC.x, 1);
+    double mkm = __shfl_up_sync(0xffffffffu, mC[V - 1], 1), mkp = __shfl_down_sync(0xffffffffu, mC[0], 1);
+    unsigned skm_ = __shfl_up_sync(0xffffffffu, byte_at(sC, V - 1), 1), skp_ = __shfl_down_sync(0xffffffffu, byte_at(sC, 0), 1);
     if (own) {
       const uint32_t p = (uint32_t)i * SI + (uint32_t)j * SJ + (uint32_t)k;
       if (!kdn) { mkm = k > 0 ? mix1(col, ra, rb, (long long)p - 1) : 0.0; skm_ = (k > 0 && solid) ? solid[p - 1] : 0u; }
-      if (!kup) { mkp = k + 4 < nz ? mix1(col, ra, rb, (long long)p + 4) : 0.0; skp_ = (k + 4 < nz && solid) ? solid[p + 4] : 0u; }
+      if (!kup) { mkp = k + V < nz ? mix1(col, ra, rb, (long long)p + V) : 0.0; skp_ = (k + V < nz && solid) ? solid[p + V] : 0u; }
       if (k == 0) { mkm = 0.0; skm_ = 0u; }
-      if (k + 4 >= nz) { mkp = 0.0; skp_ = 0u; }
+      if (k + V >= nz) { mkp = 0.0; skp_ = 0u; }
       const uint8_t skm = (uint8_t)skm_, skp = (uint8_t)skp_;
-      double mS[4] = {0.0, 0.0, 0.0, 0.0}, mNo[4] = {0.0, 0.0, 0.0, 0.0};
-      uchar4 sS = z4, sNo = z4;
-      if (j > 0) { mix4(col, ra, rb, p - SJ, mS); if (solid) sS = ld4b(solid, p - SJ); }
-      if (j < ny - 1) { mix4(col, ra, rb, p + SJ, mNo); if (solid) sNo = ld4b(solid, p + SJ); }
-      // A quad away from the i and j walls whose cells and neighbours all
+      double mS[V] = {}, mNo[V] = {};
+      uint32_t sS = 0u, sNo = 0u;
+      if (j > 0) { mixv<V>(col, ra, rb, p - SJ, mS); if (solid) sS = ldvb<V>(solid, p - SJ); }
+      if (j < ny - 1) { mixv<V>(col, ra, rb, p + SJ, mNo); if (solid) sNo = ldvb<V>(solid, p + SJ); }
+      // A group away from the i and j walls whose cells and neighbours all
       // carry the same solid flag needs none of the wall and body rules but
-      // the k walls' (a solid quad only scales c by 1e-12 and drops its
+      // the k walls' (a solid group only scales c by 1e-12 and drops its
       // couplings): the same values in far fewer instructions. Rows run
-      // along k, so a warp's quads mostly agree on the branch.
+      // along k, so a warp's groups mostly agree on the branch.
       bool fast = i > 0 && i < nx - 1 && j > 0 && j < ny - 1;
-      const uint8_t sp0 = sC.x;
+      const uint32_t sp0 = byte_at(sC, 0);
       if (solid && fast) {
-        const uint32_t w4 = 0x01010101u * sp0;
-        bool same = *reinterpret_cast<const uint32_t *>(&sC) == w4 &&
-                    *reinterpret_cast<const uint32_t *>(&sP) == w4 &&
-                    *reinterpret_cast<const uint32_t *>(&sN) == w4 && (k == 0 || skm == sp0) &&
-                    (k + 4 == nz || skp == sp0);
-#pragma unroll
-        for (int m = 0; m < 4; ++m) same = same && byte_of(sS, m) == sp0 && byte_of(sNo, m) == sp0;
+        const uint32_t wv = bytes_all<V>(sp0);
+        bool same = sC == wv && sP == wv && sN == wv && sS == wv && sNo == wv && (k == 0 || skm == sp0) &&
+                    (k + V == nz || skp == sp0);
         fast = same;
       }
       if (fast) {
-        // the quad with quotients from qin (interior faces) and qbnd (the k
+        // the group with quotients from qin (interior faces) and qbnd (the k
         // walls' faces)
-        double e[4], oc[4], ow[4], os[4], ob[4];
-        auto quad = [&](auto &&qin, auto &&qbnd) {
-          double bfx[5];
+        double e[V], oc[V], ow[V], os[V], ob[V];
+        auto group = [&](auto &&qin, auto &&qbnd) {
+          double bfx[V + 1];
           bfx[0] = k == 0 ? qbnd(face_of(hc, ra, mC[0], mC[0])) : qin(face_of(hc, ra, mC[0], mkm));
 #pragma unroll
-          for (int m = 1; m < 4; ++m) bfx[m] = qin(face_of(hc, ra, mC[m], mC[m - 1]));
-          bfx[4] = k + 4 == nz ? qbnd(face_of(hc, ra, mC[3], mC[3])) : qin(face_of(hc, ra, mkp, mC[3]));
+          for (int m = 1; m < V; ++m) bfx[m] = qin(face_of(hc, ra, mC[m], mC[m - 1]));
+          bfx[V] = k + V == nz ? qbnd(face_of(hc, ra, mC[V - 1], mC[V - 1])) : qin(face_of(hc, ra, mkp, mC[V - 1]));
 #pragma unroll
-          for (int m = 0; m < 4; ++m) {
+          for (int m = 0; m < V; ++m) {
             const double a0 = aW[m];
             const double a1 = qin(face_of(hc, ra, mN[m], mC[m]));
             const double a2 = qin(face_of(hc, ra, mC[m], mS[m]));
@@ -634,7 +687,7 @@ __global__ void __launch_bounds__(kThreads, 2)
               if (bc[4] == PBG_BC_NEUMANN_) { c = __dsub_rn(c, a4); a4 = 0.0; }
               else if (bc[4] == PBG_BC_DIRICHLET_) a4 = 0.0;
             }
-            if (m == 3 && k + 4 == nz && bc[5] == PBG_BC_NEUMANN_) c = __dsub_rn(c, a5);
+            if (m == V - 1 && k + V == nz && bc[5] == PBG_BC_NEUMANN_) c = __dsub_rn(c, a5);
             e[m] = a1;
             if (sp0) {
               c = __dmul_rn(c, 1.0e-12);
@@ -644,26 +697,25 @@ __global__ void __launch_bounds__(kThreads, 2)
           }
         };
         bool miss = false;
-        quad([&](double f) { return QC.in(f, miss); }, [&](double f) { return QC.bnd(f, miss); });
-        // an interface face: the quad again, dividing where the cache misses
-        if (miss) quad([&](double f) { return Q(f); }, [&](double f) { return __ddiv_rn(hxb, f); });
+        group([&](double f) { return QC.in(f, miss); }, [&](double f) { return QC.bnd(f, miss); });
+        // an interface face: the group again, dividing where the cache misses
+        if (miss) group([&](double f) { return Q(f); }, [&](double f) { return __ddiv_rn(hxb, f); });
 #pragma unroll
-        for (int m = 0; m < 4; ++m) aW[m] = e[m];
-        st4d(C, p, oc);
-        st4d(W, p, ow);
-        st4d(S, p, os);
-        st4d(B, p, ob);
-        const uint8_t fl = sp0 ? 0 : 1;
-        *reinterpret_cast<uchar4 *>(aflag + p) = make_uchar4(fl, fl, fl, fl);
+        for (int m = 0; m < V; ++m) aW[m] = e[m];
+        stvd<V>(C, p, oc);
+        stvd<V>(W, p, ow);
+        stvd<V>(S, p, os);
+        stvd<V>(B, p, ob);
+        stvb<V>(aflag, p, bytes_all<V>(sp0 ? 0u : 1u));
       } else {
-        double bf[5];
+        double bf[V + 1];
         bf[0] = k == 0 ? __ddiv_rn(hxb, face_of(hc, ra, mC[0], mC[0])) : Q(face_of(hc, ra, mC[0], mkm));
 #pragma unroll
-        for (int m = 1; m < 4; ++m) bf[m] = Q(face_of(hc, ra, mC[m], mC[m - 1]));
-        bf[4] = k + 4 == nz ? __ddiv_rn(hxb, face_of(hc, ra, mC[3], mC[3])) : Q(face_of(hc, ra, mkp, mC[3]));
-        uchar4 af;
+        for (int m = 1; m < V; ++m) bf[m] = Q(face_of(hc, ra, mC[m], mC[m - 1]));
+        bf[V] = k + V == nz ? __ddiv_rn(hxb, face_of(hc, ra, mC[V - 1], mC[V - 1])) : Q(face_of(hc, ra, mkp, mC[V - 1]));
+        uint32_t af = 0u;
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
+        for (int m = 0; m < V; ++m) {
           const int kk = k + m;
           const double ms_ = mS[m], mn_ = mNo[m];
           double a[6];
@@ -677,13 +729,13 @@ __global__ void __launch_bounds__(kThreads, 2)
           double c = a[0];
 #pragma unroll
           for (int f = 1; f < 6; ++f) c = __dadd_rn(c, a[f]);
-          const uint8_t sp = byte_of(sC, m);
+          const uint32_t sp = byte_at(sC, m);
           if (solid) {
-            const uint8_t sbm = m > 0 ? byte_of(sC, m - 1) : skm, stp = m < 3 ? byte_of(sC, m + 1) : skp;
-            if (i > 0 && byte_of(sP, m) != sp) a[0] = 0.0;
-            if (i < nx - 1 && byte_of(sN, m) != sp) a[1] = 0.0;
-            if (j > 0 && byte_of(sS, m) != sp) a[2] = 0.0;
-            if (j < ny - 1 && byte_of(sNo, m) != sp) a[3] = 0.0;
+            const uint32_t sbm = m > 0 ? byte_at(sC, m - 1) : skm, stp = m < V - 1 ? byte_at(sC, m + 1) : skp;
+            if (i > 0 && byte_at(sP, m) != sp) a[0] = 0.0;
+            if (i < nx - 1 && byte_at(sN, m) != sp) a[1] = 0.0;
+            if (j > 0 && byte_at(sS, m) != sp) a[2] = 0.0;
+            if (j < ny - 1 && byte_at(sNo, m) != sp) a[3] = 0.0;
             if (kk > 0 && sbm != sp) a[4] = 0.0;
             if (kk < nz - 1 && stp != sp) a[5] = 0.0;
             if (!sp) {
@@ -707,43 +759,43 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll
             for (int f = 0; f < 6; ++f) a[f] = 0.0;
           }
-          // one cell at a time (8-byte stores; the four of a thread fill
-          // whole sectors together) keeps the outputs out of registers
+          // one cell at a time (8-byte stores; a thread's cells fill whole
+          // 16-byte pairs together) keeps the outputs out of registers
           C[p + m] = c;
           W[p + m] = a[0];
           S[p + m] = a[2];
           B[p + m] = a[4];
-          const uint8_t fl = sp ? 0 : 1;
-          if (m == 0) af.x = fl; else if (m == 1) af.y = fl; else if (m == 2) af.z = fl; else af.w = fl;
+          af |= (sp ? 0u : 1u) << (8 * m);
         }
-        *reinterpret_cast<uchar4 *>(aflag + p) = af;
+        stvb<V>(aflag, p, af);
       }
     }
     sP = sC;
     sC = sN;
 #pragma unroll
-    for (int m = 0; m < 4; ++m) mC[m] = mN[m];
+    for (int m = 0; m < V; ++m) mC[m] = mN[m];
   }
 }
 
 // The projection's walk, without shared memory or barriers: the previous
 // plane in registers, the south row (j - 1) read directly (from L1/L2: it is
 // another thread's own row), the k - 1 neighbour from the previous lane when
-// that lane holds the row's previous quad, else read. Faces follow the
+// that lane holds the row's previous group, else read. Faces follow the
 // one-cell kernel's rules and arithmetic:
-//  * a quad of solid cells updates no face at all;
-//  * a quad with all three lower neighbours inside the domain and no solid
+//  * a group of solid cells updates no face at all;
+//  * a group with all three lower neighbours inside the domain and no solid
 //    cell in it or below it on any axis updates every face, both divisions
 //    by Markstein's correction when every face density is a pure phase's;
-//  * any other quad (or one whose correction misses) takes the general
+//  * any other group (or one whose correction misses) takes the general
 //    per-face rules with KnownDiv's divisions.
-__global__ void __launch_bounds__(kThreads, 2)
+template <int V>
+__global__ void __launch_bounds__(kThreads, V == 2 ? 4 : 2)
     km_project(int nx, int ny, int nz, int KQ, int LEN, double h, double dt, const double *__restrict__ pr,
                const double *__restrict__ col, double ra, double rb, const uint8_t *__restrict__ solid,
                double *__restrict__ u, double *__restrict__ v, double *__restrict__ w) {
   const int TJ = kThreads / KQ;
   const int tx = (int)threadIdx.x % KQ, ty = (int)threadIdx.x / KQ, lane = (int)threadIdx.x & 31;
-  const int k = (int)blockIdx.x * 4 * KQ + 4 * tx, j = (int)blockIdx.y * TJ + ty;
+  const int k = (int)blockIdx.x * V * KQ + V * tx, j = (int)blockIdx.y * TJ + ty;
   const int i0 = (int)blockIdx.z * LEN, i1 = min(nx, i0 + LEN);
   const bool own = j < ny && k < nz;
   const uint32_t SI = (uint32_t)ny * nz, SJ = (uint32_t)nz;
@@ -751,34 +803,33 @@ __global__ void __launch_bounds__(kThreads, 2)
   const bool hc = col != nullptr;
   const PhaseDiv D(ra, rb, h);
   const ProjFast PF(D);
-  const uchar4 z4 = make_uchar4(0, 0, 0, 0);
-  const bool kshfl = lane > 0 && tx > 0;  // the previous lane holds the quad before
-  double pP[4] = {0.0, 0.0, 0.0, 0.0}, mP[4] = {0.0, 0.0, 0.0, 0.0};
-  uchar4 sP = z4;
+  const bool kshfl = lane > 0 && tx > 0;  // the previous lane holds the group before
+  double pP[V] = {}, mP[V] = {};
+  uint32_t sP = 0u;
   if (own && i0 > 0) {
     const uint32_t p = (uint32_t)(i0 - 1) * SI + (uint32_t)j * SJ + (uint32_t)k;
-    ld4d(pr, p, pP);
-    mix4(col, ra, rb, p, mP);
-    sP = body ? ld4b(solid, p) : z4;
+    ldvd<V>(pr, p, pP);
+    mixv<V>(col, ra, rb, p, mP);
+    sP = body ? ldvb<V>(solid, p) : 0u;
   }
   for (int i = i0; i < i1; ++i) {
     const uint32_t p = (uint32_t)i * SI + (uint32_t)j * SJ + (uint32_t)k;
-    double pC[4] = {0.0, 0.0, 0.0, 0.0}, mC[4] = {0.0, 0.0, 0.0, 0.0};
-    double pS[4] = {0.0, 0.0, 0.0, 0.0}, mS[4] = {0.0, 0.0, 0.0, 0.0};
-    uchar4 sC = z4, sS = z4;
+    double pC[V] = {}, mC[V] = {};
+    double pS[V] = {}, mS[V] = {};
+    uint32_t sC = 0u, sS = 0u;
     if (own) {
-      ld4d(pr, p, pC);
-      mix4(col, ra, rb, p, mC);
-      if (body) sC = ld4b(solid, p);
+      ldvd<V>(pr, p, pC);
+      mixv<V>(col, ra, rb, p, mC);
+      if (body) sC = ldvb<V>(solid, p);
       if (j > 0) {
-        ld4d(pr, p - SJ, pS);
-        mix4(col, ra, rb, p - SJ, mS);
-        if (body) sS = ld4b(solid, p - SJ);
+        ldvd<V>(pr, p - SJ, pS);
+        mixv<V>(col, ra, rb, p - SJ, mS);
+        if (body) sS = ldvb<V>(solid, p - SJ);
       }
     }
-    double pk = __shfl_up_sync(0xffffffffu, pC[3], 1);
-    double mk = __shfl_up_sync(0xffffffffu, mC[3], 1);
-    unsigned sk = __shfl_up_sync(0xffffffffu, (unsigned)sC.w, 1);
+    double pk = __shfl_up_sync(0xffffffffu, pC[V - 1], 1);
+    double mk = __shfl_up_sync(0xffffffffu, mC[V - 1], 1);
+    unsigned sk = __shfl_up_sync(0xffffffffu, byte_at(sC, V - 1), 1);
     if (!kshfl && own && k > 0) {
       pk = pr[p - 1];
       mk = mix1(col, ra, rb, (long long)p - 1);
@@ -787,10 +838,11 @@ __global__ void __launch_bounds__(kThreads, 2)
     bool fast = own && i > 0 && j > 0 && k > 0;
     bool skip = false;
     if (body && own) {
-      skip = sC.x && sC.y && sC.z && sC.w;
+      skip = true;
+#pragma unroll
+      for (int m = 0; m < V; ++m) skip = skip && byte_at(sC, m) != 0u;
       if (fast) {
-        const uint32_t any = *reinterpret_cast<const uint32_t *>(&sC) | *reinterpret_cast<const uint32_t *>(&sP) |
-                             *reinterpret_cast<const uint32_t *>(&sS) | sk;
+        const uint32_t any = sC | sP | sS | sk;
         fast = any == 0;
       }
     }
@@ -799,13 +851,13 @@ __global__ void __launch_bounds__(kThreads, 2)
       const uint32_t iv = ((uint32_t)i * (ny + 1) + j) * nz + k;
       const long long iw = ((long long)i * ny + j) * (nz + 1) + k;
       bool miss = false;
-      double uo[4], vo[4], wo[4];
-      ld4d(u, p, uo);
-      ld4d(v, iv, vo);
+      double uo[V], vo[V], wo[V];
+      ldvd<V>(u, p, uo);
+      ldvd<V>(v, iv, vo);
 #pragma unroll
-      for (int m = 0; m < 4; ++m) wo[m] = w[iw + m];
+      for (int m = 0; m < V; ++m) wo[m] = w[iw + m];
 #pragma unroll
-      for (int m = 0; m < 4; ++m) {
+      for (int m = 0; m < V; ++m) {
         uo[m] = __dadd_rn(uo[m], PF.inc(pP[m], pC[m], face_of(hc, ra, mC[m], mP[m]), dt, body, miss));
         vo[m] = __dadd_rn(vo[m], PF.inc(pS[m], pC[m], face_of(hc, ra, mC[m], mS[m]), dt, body, miss));
         const double pb = m > 0 ? pC[m - 1] : pk;
@@ -813,41 +865,41 @@ __global__ void __launch_bounds__(kThreads, 2)
         wo[m] = __dadd_rn(wo[m], PF.inc(pb, pC[m], face_of(hc, ra, mC[m], mb), dt, body, miss));
       }
       if (!miss) {
-        st4d(u, p, uo);
-        st4d(v, iv, vo);
+        stvd<V>(u, p, uo);
+        stvd<V>(v, iv, vo);
 #pragma unroll
-        for (int m = 0; m < 4; ++m) w[iw + m] = wo[m];
+        for (int m = 0; m < V; ++m) w[iw + m] = wo[m];
       }
       fast = !miss;
     }
     if (!skip && !fast && own) {
       if (i > 0) {
-        double uo[4];
-        ld4d(u, p, uo);
+        double uo[V];
+        ldvd<V>(u, p, uo);
 #pragma unroll
-        for (int m = 0; m < 4; ++m)
-          if (!(body && (byte_of(sC, m) || byte_of(sP, m))))
+        for (int m = 0; m < V; ++m)
+          if (!(body && (byte_at(sC, m) || byte_at(sP, m))))
             uo[m] = __dadd_rn(uo[m], project_increment_k(pP[m], pC[m], face_of(hc, ra, mC[m], mP[m]), dt, D, body));
-        st4d(u, p, uo);
+        stvd<V>(u, p, uo);
       }
       if (j > 0) {
         const uint32_t iv = ((uint32_t)i * (ny + 1) + j) * nz + k;
-        double vo[4];
-        ld4d(v, iv, vo);
+        double vo[V];
+        ldvd<V>(v, iv, vo);
 #pragma unroll
-        for (int m = 0; m < 4; ++m)
-          if (!(body && (byte_of(sC, m) || byte_of(sS, m))))
+        for (int m = 0; m < V; ++m)
+          if (!(body && (byte_at(sC, m) || byte_at(sS, m))))
             vo[m] = __dadd_rn(vo[m], project_increment_k(pS[m], pC[m], face_of(hc, ra, mC[m], mS[m]), dt, D, body));
-        st4d(v, iv, vo);
+        stvd<V>(v, iv, vo);
       }
       if (nz > 1) {
         const long long iw = ((long long)i * ny + j) * (nz + 1) + k;
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
+        for (int m = 0; m < V; ++m) {
           const int kk = k + m;
           if (kk == 0) continue;
-          const unsigned sbm = m > 0 ? byte_of(sC, m - 1) : sk;
-          if (body && (byte_of(sC, m) || sbm)) continue;
+          const unsigned sbm = m > 0 ? byte_at(sC, m - 1) : sk;
+          if (body && (byte_at(sC, m) || sbm)) continue;
           const double pb = m > 0 ? pC[m - 1] : pk;
           const double mb = m > 0 ? mC[m - 1] : mk;
           w[iw + m] = __dadd_rn(w[iw + m], project_increment_k(pb, pC[m], face_of(hc, ra, mC[m], mb), dt, D, body));
@@ -855,7 +907,7 @@ __global__ void __launch_bounds__(kThreads, 2)
       }
     }
 #pragma unroll
-    for (int m = 0; m < 4; ++m) {
+    for (int m = 0; m < V; ++m) {
       pP[m] = pC[m];
       mP[m] = mC[m];
     }
