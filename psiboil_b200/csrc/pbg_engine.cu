@@ -472,7 +472,8 @@ void Engine::precond(int l, const T *r, T *z, bool dots, const T *u, double *out
   const bool vec = A.nz % VecTraits<T>::V == 0;
   const int gv = grid_for(A.ncell() / VecTraits<T>::V, kThreads, kVecBlocks);
   const KScal *ksl = kc ? w.ks.p + l : nullptr;
-  launch_pdl(vec ? kv_jac2<T> : k_jac2<T>, vec ? gv : g, kThreads, s, A, r, (const T *)v.b.p,
+  const int gw = grid_for(A.ncell() / VecTraits<T>::V, kThreads, kVecWideBlocks<T>);
+  launch_pdl(vec ? kv_jac2<T> : k_jac2<T>, vec ? gw : g, kThreads, s, A, r, (const T *)v.b.p,
              (const T *)v.q1.p, ksl, v.r1.p, v.xb.p, om, stop);
   const long long rthreads = H.ncell() >= kRestrictSerialMin ? H.ncell() : H.ncell() * 8;
   launch_pdl(k_resid_restrict<T>, grid_for(rthreads), kThreads, s, A, rr, (const T *)v.xb.p,
@@ -541,7 +542,8 @@ int Engine::fcg(EWork<T> &w, const T *b, double tol, int maxit, RedPool &red, cu
     precond<T>(0, w.r0.p, w.z0.p, true, w.q0.p, &fs->zr, w, red, stop, s, false);
     if (A.nz % VecTraits<T>::V == 0 && (int)L.size() > 1) {
       const int gv = grid_for(N / VecTraits<T>::V, kThreads, kVecBlocks);
-      launch_pdl(kv_fcg_pq<T>, gv, kThreads, s, A, (const T *)w.z0.p, w.pA.p, w.pB.p, w.q0.p, w.q0b.p, fs,
+      const int gw = grid_for(N / VecTraits<T>::V, kThreads, kVecWideBlocks<T>);
+      launch_pdl(kv_fcg_pq<T>, gw, kThreads, s, A, (const T *)w.z0.p, w.pA.p, w.pB.p, w.q0.p, w.q0b.p, fs,
                  red.slot_part(0), red.slot_count(0));
       launch_pdl(kv_fcg_xr<T>, gv, kThreads, s, N, w.x0.p, w.r0.p, (const T *)w.pA.p, (const T *)w.pB.p,
                  (const T *)w.q0.p, (const T *)w.q0b.p, fs, red.slot_part(0), red.slot_count(0));

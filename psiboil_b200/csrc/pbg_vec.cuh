@@ -159,6 +159,12 @@ struct FJac0Kc {
 
 // one wave of the 64-register vector kernels: 4 blocks of 256 per SM
 constexpr int kVecBlocks = 148 * 4;
+// blocks an SM of the two-sweep and FCG direction kernels: their float4
+// neighbourhoods (FP32) need up to 80 registers a thread, which at four
+// blocks an SM (64) would spill to local memory, so FP32 runs three; FP64
+// (double2) keeps four
+template <typename T> constexpr int kVecWideSm = sizeof(T) == 4 ? 3 : 4;
+template <typename T> constexpr int kVecWideBlocks = 148 * kVecWideSm<T>;
 
 #define VGRID_LOOP(g, NG)                                                       \
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < (uint32_t)(NG); \
@@ -166,7 +172,7 @@ constexpr int kVecBlocks = 148 * 4;
 
 // two sweeps from zero (k_jac2)
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, kVecWideSm<T>)
     kv_jac2(EMat<T> A, const T *__restrict__ r, const T *__restrict__ b2, const T *__restrict__ q2,
             const KScal *ks, T *__restrict__ r_out, T *__restrict__ xo, T omega, const int *stop) {
   PBG_PDL_ENTRY();
@@ -315,7 +321,7 @@ __device__ __forceinline__ T axv(const T c, const CoefV<T> &C, const HoodV<T> &X
 // FCG direction: p = z - beta p_old, q = A z - beta q_old (A p = A z - beta
 // A p_old), p.q. Reads z at the stencil, p_old and q_old once per cell.
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, kVecWideSm<T>)
     kv_fcg_pq(EMat<T> A, const T *__restrict__ z, T *pA, T *pB, T *qA, T *qB, FcgScal *fs,
               double *part, unsigned *count) {
   PBG_PDL_ENTRY();
