@@ -660,7 +660,8 @@ int pbg_assemble_mix(pbg_session *s, const double *col, double rho_a, double rho
     else if (A.e.n != (size_t)N) { A.e.alloc(N); A.n.alloc(N); A.t.alloc(N); }
     if (flow_vec(s, bd.idx != nullptr)) {
       km_assemble_mix<kAsmV><<<march_grid(s->nx, s->ny, s->nz, kAsmV), kThreads, 0, s->stream>>>(
-          s->nx, s->ny, s->nz, march_kq(s->nz, kAsmV), march_len(s->nx, s->ny, s->nz, kAsmV), s->h,
+          s->nx, s->ny, s->nz, march_kq(s->nz, kAsmV), march_len(s->nx, s->ny, s->nz, kAsmV),
+          asm_const(s->h, rho_a, rho_b),
           make_int4(s->bc[0], s->bc[1], s->bc[2], s->bc[3]), make_int2(s->bc[4], s->bc[5]), cp, rho_a, rho_b,
           bd.off, A.c.p, A.w.p, A.s.p, A.b.p, s->aflag.p);
     } else {
@@ -800,7 +801,8 @@ int pbg_project(pbg_session *s, const double *p, const double *col, double rho_a
     if (int rc = body_args(s, sp, bd)) return rc;
     if (flow_vec(s, false))
       km_project<kProjV><<<march_grid(s->nx, s->ny, s->nz, kProjV), kThreads, 0, s->stream>>>(
-          s->nx, s->ny, s->nz, march_kq(s->nz, kProjV), march_len(s->nx, s->ny, s->nz, kProjV), s->h, dt, pp, cp,
+          s->nx, s->ny, s->nz, march_kq(s->nz, kProjV), march_len(s->nx, s->ny, s->nz, kProjV),
+          proj_const(rho_a, rho_b, s->h), dt, pp, cp,
           rho_a, rho_b,
           bd.off, fa.d[0], fa.d[1], fa.d[2]);
     else

@@ -12,6 +12,7 @@
 // and f, so the west face of cell (i,j,k) is u[(i*ny + j)*nz + k].
 #pragma once
 #include <cstdint>
+#include <cstring>
 
 #include "../../include/psiboil_b200.h"
 #include "pbg_common.cuh"
@@ -211,6 +212,35 @@ __global__ void k_divergence(Geo G, int nx, int ny, int nz, double a, const doub
   }
 }
 
+// Correctly rounded IEEE double operations on the host and the device, for
+// constants that the host forms once per launch (the host's double
+// arithmetic is IEEE binary64 with round to nearest, as __ddiv_rn is).
+__host__ __device__ __forceinline__ double div_rn(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __ddiv_rn(a, b);
+#else
+  return a / b;
+#endif
+}
+__host__ __device__ __forceinline__ double mul_rn(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
+__host__ __device__ __forceinline__ double quiet_nan() {
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double(0x7ff8000000000000LL);
+#else
+  const unsigned long long u = 0x7ff8000000000000ULL;
+  double d;
+  memcpy(&d, &u, sizeof d);
+  return d;
+#endif
+}
+
+
 // Momentum::project (Src/Equation/Staggered/Momentum/momentum_project.cpp:
 // 11-80) on every interior face: without a body (:26-45)
 // u += (p[i-1] - p[i]) / rho_face * dt / dxc; with a solid mask, the
@@ -232,8 +262,9 @@ __global__ void k_divergence(Geo G, int nx, int ny, int nz, double a, const doub
 struct KnownDiv {
   double b, y;
   bool ok;
-  __device__ __forceinline__ explicit KnownDiv(double b_) : b(b_) {
-    y = __ddiv_rn(1.0, b_);
+  KnownDiv() = default;
+  __host__ __device__ __forceinline__ explicit KnownDiv(double b_) : b(b_) {
+    y = div_rn(1.0, b_);
     const double m = fabs(b_);
     ok = m >= 0x1p-60 && m <= 0x1p60;
   }
@@ -261,7 +292,8 @@ struct KnownDiv {
 // the divisors the projection meets on every face away from an interface.
 struct PhaseDiv {
   KnownDiv a, b, h;
-  __device__ __forceinline__ PhaseDiv(double ra, double rb, double h_) : a(ra), b(rb), h(h_) {}
+  PhaseDiv() = default;
+  __host__ __device__ __forceinline__ PhaseDiv(double ra, double rb, double h_) : a(ra), b(rb), h(h_) {}
   __device__ __forceinline__ double by_rho(double x, double rho) const {
     if (rho == a.b && a.ok) return a(x);
     return b.by(x, rho);
@@ -286,8 +318,9 @@ __device__ __forceinline__ double project_increment_k(double pm, double pp, doub
 struct ProjFast {
   double ka, kb, ra, rb, ya, yb, h, yh;
   bool hok;
-  __device__ __forceinline__ explicit ProjFast(const PhaseDiv &D) {
-    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+  ProjFast() = default;
+  __host__ __device__ __forceinline__ explicit ProjFast(const PhaseDiv &D) {
+    const double nan = quiet_nan();
     ka = D.a.ok ? D.a.b : nan;
     kb = D.b.ok ? D.b.b : nan;
     ra = D.a.b; rb = D.b.b; ya = D.a.y; yb = D.b.y;
@@ -501,21 +534,20 @@ __global__ void __launch_bounds__(kThreads)
 // ---------------------------------------------------------------------------
 // Marching forms of the assembly and the projection (nz % 4 == 0, no cut
 // body, fewer than 2^31 cells). A thread owns a group of V consecutive
-// cells of a row (V = kAsmV = 4 in the assembly; kProjV = 2 in the
-// projection, whose fewer registers a thread let four blocks share an SM
-// instead of two). A block of 256 threads owns a tile of the (j, k) plane,
-// TJ rows of V KQ cells (KQ threads a row, TJ = 256 / KQ), and walks it
-// through LEN consecutive i planes, the previous plane in registers, without
-// shared memory or barriers: the rows beside a thread's own (other threads'
-// own rows) are read directly, from L1/L2, and the k neighbours come from
-// the lanes around it. The assembly's
-// coefficient of the face between planes i and i+1 is formed once, as the
-// east face of i and the west face of i+1. Every value is the same
-// operations in the same order as the one-cell kernels, so the outputs are
-// bit for bit theirs.
+// cells of a row (V = 2 in both kernels: at 64 registers a thread four
+// blocks share an SM, against two at V = 4). A block of 256 threads owns a
+// tile of the (j, k) plane, TJ rows of V KQ cells (KQ threads a row,
+// TJ = 256 / KQ), and walks it through LEN consecutive i planes, the
+// previous plane in registers, without shared memory or barriers: the rows
+// beside a thread's own (other threads' own rows) are read directly, from
+// L1/L2, and the k neighbours come from the lanes around it. The
+// assembly's coefficient of the face between planes i and i+1 is formed
+// once, as the east face of i and the west face of i+1. Every value is the
+// same operations in the same order as the one-cell kernels, so the outputs
+// are bit for bit theirs.
 // ---------------------------------------------------------------------------
 constexpr int kMarchI = 8;  // planes a walk, at most
-constexpr int kAsmV = 4;    // cells a thread, assembly
+constexpr int kAsmV = 2;    // cells a thread, assembly
 constexpr int kProjV = 2;   // cells a thread, projection
 
 // threads a row: the smallest power of two with v KQ >= nz, at most 256 / v
@@ -553,9 +585,10 @@ inline bool march_fits(int nx, int ny, int nz) {
 // wrong sign of infinity).
 struct QuotCache {
   double hx, ra, rb, qa, qb;
-  __device__ __forceinline__ QuotCache(double hx_, double ra_, double rb_) : hx(hx_), ra(ra_), rb(rb_) {
-    qa = __ddiv_rn(hx_, ra_);
-    qb = __ddiv_rn(hx_, rb_);
+  QuotCache() = default;
+  __host__ __device__ __forceinline__ QuotCache(double hx_, double ra_, double rb_) : hx(hx_), ra(ra_), rb(rb_) {
+    qa = div_rn(hx_, ra_);
+    qb = div_rn(hx_, rb_);
   }
   __device__ __forceinline__ double operator()(double f) const {
     if (f != 0.0) {
@@ -572,14 +605,15 @@ struct QuotCache {
 // miss and returns a placeholder.
 struct QuotOnly {
   double ka, kb, qa, qb, qba, qbb;
-  __device__ __forceinline__ QuotOnly(double hx, double hxb, double ra, double rb) {
-    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+  QuotOnly() = default;
+  __host__ __device__ __forceinline__ QuotOnly(double hx, double hxb, double ra, double rb) {
+    const double nan = quiet_nan();
     ka = ra != 0.0 ? ra : nan;
     kb = rb != 0.0 ? rb : nan;
-    qa = __ddiv_rn(hx, ra);
-    qb = __ddiv_rn(hx, rb);
-    qba = __ddiv_rn(hxb, ra);
-    qbb = __ddiv_rn(hxb, rb);
+    qa = div_rn(hx, ra);
+    qb = div_rn(hx, rb);
+    qba = div_rn(hxb, ra);
+    qbb = div_rn(hxb, rb);
   }
   __device__ __forceinline__ double in(double f, bool &miss) const {
     const bool isa = f == ka;
@@ -593,9 +627,40 @@ struct QuotOnly {
   }
 };
 
+// Per-launch constants of the marching kernels, formed on the host with the
+// same correctly rounded operations the one-cell kernels use (hx = h^2 / h;
+// hxb = h^2 / (h / 2), the wall faces' numerator; the cached quotients and
+// reciprocals). Passed as __grid_constant__ parameters, they are read from
+// the constant bank rather than held in every thread's registers.
+struct AsmConst {
+  double hx, hxb;
+  QuotCache Q;
+  QuotOnly QC;
+};
+inline AsmConst asm_const(double h, double ra, double rb) {
+  AsmConst K;
+  const double hh = mul_rn(h, h);
+  K.hx = div_rn(hh, h);
+  K.hxb = div_rn(hh, mul_rn(0.5, h));
+  K.Q = QuotCache(K.hx, ra, rb);
+  K.QC = QuotOnly(K.hx, K.hxb, ra, rb);
+  return K;
+}
+struct ProjConst {
+  PhaseDiv D;
+  ProjFast PF;
+};
+inline ProjConst proj_const(double ra, double rb, double h) {
+  ProjConst K;
+  K.D = PhaseDiv(ra, rb, h);
+  K.PF = ProjFast(K.D);
+  return K;
+}
+
 template <int V>
 __global__ void __launch_bounds__(kThreads, V == 2 ? 4 : 2)
-    km_assemble_mix(int nx, int ny, int nz, int KQ, int LEN, double h, int4 bc03, int2 bc45,
+    km_assemble_mix(int nx, int ny, int nz, int KQ, int LEN, const __grid_constant__ AsmConst K, int4 bc03,
+                    int2 bc45,
                     const double *__restrict__ col, double ra, double rb, const uint8_t *__restrict__ solid,
                     double *__restrict__ C, double *__restrict__ W, double *__restrict__ S,
                     double *__restrict__ B, uint8_t *__restrict__ aflag) {
@@ -606,12 +671,10 @@ __global__ void __launch_bounds__(kThreads, V == 2 ? 4 : 2)
   const int i0 = (int)blockIdx.z * LEN, i1 = min(nx, i0 + LEN);
   const bool own = j < ny && k < nz;
   const uint32_t SI = (uint32_t)ny * nz, SJ = (uint32_t)nz;
-  const double hh = __dmul_rn(h, h);
-  const double hx = __ddiv_rn(hh, h);
-  const double hxb = __ddiv_rn(hh, __dmul_rn(0.5, h));
+  const double &hxb = K.hxb;
   const bool hc = col != nullptr;
-  const QuotCache Q(hx, ra, rb);
-  const QuotOnly QC(hx, hxb, ra, rb);
+  const QuotCache &Q = K.Q;
+  const QuotOnly &QC = K.QC;
   // the lanes before and after hold the row's previous and next groups
   const int lane = (int)threadIdx.x & 31;
   const bool kdn = lane > 0 && tx > 0, kup = lane < 31 && tx < KQ - 1;
@@ -790,7 +853,8 @@ __global__ void __launch_bounds__(kThreads, V == 2 ? 4 : 2)
 //    per-face rules with KnownDiv's divisions.
 template <int V>
 __global__ void __launch_bounds__(kThreads, V == 2 ? 4 : 2)
-    km_project(int nx, int ny, int nz, int KQ, int LEN, double h, double dt, const double *__restrict__ pr,
+    km_project(int nx, int ny, int nz, int KQ, int LEN, const __grid_constant__ ProjConst K, double dt,
+               const double *__restrict__ pr,
                const double *__restrict__ col, double ra, double rb, const uint8_t *__restrict__ solid,
                double *__restrict__ u, double *__restrict__ v, double *__restrict__ w) {
   const int TJ = kThreads / KQ;
@@ -801,8 +865,8 @@ __global__ void __launch_bounds__(kThreads, V == 2 ? 4 : 2)
   const uint32_t SI = (uint32_t)ny * nz, SJ = (uint32_t)nz;
   const bool body = solid != nullptr;
   const bool hc = col != nullptr;
-  const PhaseDiv D(ra, rb, h);
-  const ProjFast PF(D);
+  const PhaseDiv &D = K.D;
+  const ProjFast &PF = K.PF;
   const bool kshfl = lane > 0 && tx > 0;  // the previous lane holds the group before
   double pP[V] = {}, mP[V] = {};
   uint32_t sP = 0u;
