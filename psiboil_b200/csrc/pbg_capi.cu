@@ -753,7 +753,7 @@ int pbg_divergence(pbg_session *s, const double *u, const double *v, const doubl
     const double dti = 1.0 / dt;
     const double a = (s->h * s->h) * dti;
     if (flow_vec(s, bd.idx != nullptr))
-      kv_divergence<<<grid_for(N / kFlowV), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, a,
+      kv_divergence<kFlowV><<<grid_for(N / kFlowV), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, a,
                                                                       fa.d[0], fa.d[1], fa.d[2], bd.off, r);
     else
       k_divergence<<<grid_for(N), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, a, fa.d[0], fa.d[1],
