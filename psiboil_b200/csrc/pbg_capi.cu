@@ -661,9 +661,8 @@ int pbg_assemble_mix(pbg_session *s, const double *col, double rho_a, double rho
     if (flow_vec(s, bd.idx != nullptr)) {
       km_assemble_mix<kAsmV><<<march_grid(s->nx, s->ny, s->nz, kAsmV), kThreads, 0, s->stream>>>(
           s->nx, s->ny, s->nz, march_kq(s->nz, kAsmV), march_len(s->nx, s->ny, s->nz, kAsmV),
-          asm_const(s->h, rho_a, rho_b),
-          make_int4(s->bc[0], s->bc[1], s->bc[2], s->bc[3]), make_int2(s->bc[4], s->bc[5]), cp, rho_a, rho_b,
-          bd.off, A.c.p, A.w.p, A.s.p, A.b.p, s->aflag.p);
+          asm_const(s->h, rho_a, rho_b), make_int4(s->bc[0], s->bc[1], s->bc[2], s->bc[3]),
+          make_int2(s->bc[4], s->bc[5]), cp, rho_a, rho_b, bd.off, A.c.p, A.w.p, A.s.p, A.b.p, s->aflag.p);
     } else {
       k_assemble_mix<<<grid_for(N), kThreads, 0, s->stream>>>(
           flow_geo(s), s->nx, s->ny, s->nz, s->h, make_int4(s->bc[0], s->bc[1], s->bc[2], s->bc[3]),
@@ -753,8 +752,8 @@ int pbg_divergence(pbg_session *s, const double *u, const double *v, const doubl
     const double dti = 1.0 / dt;
     const double a = (s->h * s->h) * dti;
     if (flow_vec(s, bd.idx != nullptr))
-      kv_divergence<kFlowV><<<grid_for(N / kFlowV), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, a,
-                                                                      fa.d[0], fa.d[1], fa.d[2], bd.off, r);
+      kv_divergence<kFlowV><<<grid_for(N / kFlowV), kThreads, 0, s->stream>>>(
+          flow_geo(s), s->nx, s->ny, s->nz, a, fa.d[0], fa.d[1], fa.d[2], bd.off, r);
     else
       k_divergence<<<grid_for(N), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, a, fa.d[0], fa.d[1],
                                                             fa.d[2], bd.off, bd.idx, bd.fs, r);
@@ -802,9 +801,7 @@ int pbg_project(pbg_session *s, const double *p, const double *col, double rho_a
     if (flow_vec(s, false))
       km_project<kProjV><<<march_grid(s->nx, s->ny, s->nz, kProjV), kThreads, 0, s->stream>>>(
           s->nx, s->ny, s->nz, march_kq(s->nz, kProjV), march_len(s->nx, s->ny, s->nz, kProjV),
-          proj_const(rho_a, rho_b, s->h), dt, pp, cp,
-          rho_a, rho_b,
-          bd.off, fa.d[0], fa.d[1], fa.d[2]);
+          proj_const(rho_a, rho_b, s->h), dt, pp, cp, rho_a, rho_b, bd.off, fa.d[0], fa.d[1], fa.d[2]);
     else
       k_project<<<grid_for(N), kThreads, 0, s->stream>>>(flow_geo(s), s->nx, s->ny, s->nz, s->h, dt, pp, cp, rho_a,
                                                          rho_b, bd.off, fa.d[0], fa.d[1], fa.d[2]);
